@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Training iterations per second of the tile-based differentiable Gaussian
+rasterizer on B200, on the workload the headline metric is quoted on: 1M
+Gaussians, SH degree 3, 1237x822 views (the Mip-NeRF 360 "bicycle" images_4
+size), 64 cameras on a hemisphere of radius 5. The photos themselves are not
+available here, so the scene and the targets are seeded synthetic data of
+those shapes (means in [-2, 2]^3, log-scales N(-4, 0.5), opacity logits
+N(-1, 1.5), unit quaternions from N(0,1)^4, DC colour U(0,1), higher SH
+N(0, 0.05), 60 degree horizontal field of view).
+
+One step = one training iteration (forward, SSIM + L1 loss, backward, Adam)
+on one view, views in turn. Reported:
+  value  iterations/s with the targets resident in HBM (device-timed, CUDA
+         events on the trainer's stream, max over ranks, times the ranks);
+  e2e    the same through the public step() call with host (numpy) targets:
+         the host->device copy of each target and the stats read-back are
+         inside the timed region;
+  plain  the plain FP32 form (FP32 SH and Adam state, the reference's
+         two-sort order, host read-back of the entry count, no CUDA graph,
+         deterministic exp/log) on the same views, for the 2x target;
+  roofline, cpu_baseline, clocks, gpu_launches.
+With --gpus N > 1 every rank trains its own replica (the path does not shard:
+replicas only), and value is the sum over ranks.
+--impl reference times the reference's own FP64 CPU twin (src/train/
+reference.cpp, compiled from the reference's sources into oracle/_ref) on the
+host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+WIDTH, HEIGHT = 1237, 822
+GAUSSIANS = 1_000_000
+DEGREE = 3
+VIEWS = 64
+SEED = 3
+SH_C0 = 0.28209479177387814
+
+
+def make_scene(n: int = GAUSSIANS, degree: int = DEGREE, seed: int = SEED):
+    """The seeded synthetic scene: GaussianCloud arrays (float32)."""
+    rng = np.random.default_rng(seed)
+    coeffs = (degree + 1) ** 2
+    positions = rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32)
+    scales = rng.normal(-4.0, 0.5, (n, 3)).astype(np.float32)
+    q = rng.normal(0.0, 1.0, (n, 4))
+    rotations = (q / np.linalg.norm(q, axis=1, keepdims=True)).astype(np.float32)
+    opacities = rng.normal(-1.0, 1.5, n).astype(np.float32)
+    sh = np.zeros((n, coeffs, 3), np.float32)
+    sh[:, 0, :] = (rng.uniform(0.0, 1.0, (n, 3)) - 0.5) / SH_C0
+    if coeffs > 1:
+        sh[:, 1:, :] = rng.normal(0.0, 0.05, (n, coeffs - 1, 3))
+    return positions.ravel(), scales.ravel(), rotations.ravel(), opacities, sh.ravel()
+
+
+def hemisphere_views(count: int = VIEWS, radius: float = 5.0, width: int = WIDTH, height: int = HEIGHT):
+    """Cameras on the upper hemisphere (z >= 0.15 r) looking at the origin:
+    (view 4x4 world->camera, centre, fx, fy, cx, cy, W, H)."""
+    fx = (width / 2) / math.tan(math.radians(30.0))
+    golden = math.pi * (3.0 - math.sqrt(5.0))
+    out = []
+    for k in range(count):
+        z = 0.15 + 0.85 * (k + 0.5) / count
+        r = math.sqrt(1.0 - z * z)
+        eye = radius * np.array([r * math.cos(golden * k), r * math.sin(golden * k), z])
+        forward = -eye / np.linalg.norm(eye)
+        right = np.cross(forward, np.array([0.0, 0.0, 1.0]))
+        right /= np.linalg.norm(right)
+        down = np.cross(forward, right)
+        rot = np.stack([right, down, forward])
+        view = np.eye(4)
+        view[:3, :3] = rot
+        view[:3, 3] = -rot @ eye
+        out.append((view.astype(np.float32), eye.astype(np.float32), fx, fx, width / 2, height / 2, width, height))
+    return out
+
+
+def make_targets(count: int = VIEWS, width: int = WIDTH, height: int = HEIGHT, seed: int = SEED):
+    rng = np.random.default_rng(seed + 1)
+    t = rng.integers(0, 256, (count, height * width * 4), dtype=np.uint8)
+    t[:, 3::4] = 255
+    return t
+
+
+def cpu_count() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- CPU reference
+
+
+def reference_iterations(oracle, cloud, views, targets, threads: int, rows_per_band: int | None = None) -> tuple:
+    """One training iteration's forward + loss + backward of the reference's
+    FP64 twin per view, the image split into `threads` horizontal bands that
+    run in parallel (each band a camera on those rows; every band projects all
+    Gaussians, as reference_render must). Returns (seconds, views done)."""
+    import concurrent.futures
+
+    def band_jobs(view, target):
+        W, H = view.width, view.height
+        rows = rows_per_band or math.ceil(H / threads)
+        jobs = []
+        for y0 in range(0, H, rows):
+            h = min(rows, H - y0)
+            v = oracle.View(view.view, view.position, view.fx, view.fy, view.cx, view.cy - y0, W, h)
+            t = target.reshape(H, W, 4)[y0:y0 + h].ravel()
+            jobs.append((v, t))
+        return jobs
+
+    def work(job):
+        v, t = job
+        rgb, _, _ = oracle.ref_render(cloud, v)
+        _, _, _, adjoint = oracle.ref_loss(rgb, v.width, v.height, t, 0.2)
+        oracle.ref_gradients(cloud, v, adjoint)
+
+    jobs = []
+    for view, target in zip(views, targets):
+        jobs.extend(band_jobs(view, target))
+    start = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as pool:
+        list(pool.map(work, jobs))
+    return time.perf_counter() - start, len(views)
+
+
+def reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    if not O.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsplatref.so was not built "
+                          "(the reference's src/train/reference.cpp compiles only where its tree is present)"}))
+        return
+    pos, sc, rot, op, sh = make_scene()
+    cloud = O.Cloud(DEGREE, pos, sc, rot, op, sh)
+    cams = hemisphere_views()
+    targets = make_targets(8)
+    threads = cpu_count()
+    views = [O.View(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in cams]
+    for i in range(args.warmup if args.reference_warmup else 0):
+        reference_iterations(O, cloud, [views[i % VIEWS]], [targets[i % 8]], threads)
+    total_s, done = 0.0, 0
+    for i in range(args.steps):
+        s, d = reference_iterations(O, cloud, [views[i % VIEWS]], [targets[i % 8]], threads)
+        total_s += s
+        done += d
+    value = done / total_s
+    sample = (f"{args.steps} full training iterations (1M Gaussians, SH degree 3, 1237x822), each split into "
+              f"{threads} row bands run on {threads} threads; reference_render + reference_loss + "
+              "reference_gradients (which renders again) per band")
+    print(json.dumps({
+        "impl": "reference", "metric": "train iters/s @1M Gaussians 1237x822", "value": value, "unit": "iters/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "1M Gaussians, SH degree 3, 1237x822, 64 hemisphere views (synthetic bicycle shapes)"},
+        "cpu_baseline": {"value": value, "unit": "iters/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ----------------------------------------------------------------- our arm
+
+
+def chosen_options(splat):
+    return splat.TrainerOptions(sh_storage=splat.SH_BF16, state_storage=splat.STATE_BF16_PAIR,
+                                sort_form=splat.SORT_TILE_DEPTH_64, exact_math=False, use_graph=True, digit_bits=8)
+
+
+def plain_options(splat):
+    return splat.TrainerOptions(sh_storage=splat.SH_F32, state_storage=splat.STATE_F32,
+                                sort_form=splat.SORT_DEPTH_THEN_TILE, exact_math=True, use_graph=False, digit_bits=8)
+
+
+def time_steps(torch, trainer, step_fn, steps: int, stream_handle: int) -> float:
+    """Device milliseconds for `steps` calls of step_fn, by CUDA events on the trainer's stream."""
+    stream = torch.cuda.ExternalStream(stream_handle)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for i in range(steps):
+        step_fn(i)
+    end.record(stream)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def our_arm(args) -> None:
+    import torch
+
+    splat = importlib.import_module("vibe-splat_b200")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    pos, sc, rot, op, sh = make_scene()
+    cloud = splat.GaussianCloud(DEGREE, pos, sc, rot, op, sh)
+    cams = [splat.Camera(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in hemisphere_views()]
+    host_targets = make_targets()
+    device_targets = torch.from_numpy(host_targets).cuda()
+    rates = splat.LearningRates()
+    nbytes = WIDTH * HEIGHT * 4
+
+    def run_form(options, label: str):
+        trainer = splat.Trainer(cloud, options)
+        stream = trainer.stream()
+
+        def resident(i):
+            k = i % VIEWS
+            return trainer.step_device_target(cams[k], device_targets[k].data_ptr(), rates)
+
+        for i in range(args.warmup):
+            resident(i)
+        if dist is not None:
+            dist.barrier()
+        with ClockSampler(local) as clocks:
+            ms = time_steps(torch, trainer, lambda i: resident(args.warmup + i), args.steps, stream)
+        stats = resident(0)
+        return trainer, ms, clocks.summary(), stats
+
+    trainer, ms, clocks, stats = run_form(chosen_options(splat), "chosen")
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * 1000.0 / ms_per_step
+
+    # e2e: the public step() with host targets (H2D of the target and the stats
+    # read-back in the timed region).
+    stream = trainer.stream()
+    e2e_ms = time_steps(torch, trainer, lambda i: trainer.step(cams[i % VIEWS], host_targets[i % VIEWS], rates),
+                        args.steps, stream)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * 1000.0 * args.steps / e2e_ms
+
+    # Per-stage device times (serialising events, plain launches) for the roofline.
+    trainer.set_timing(True)
+    for i in range(max(3, min(args.steps, 10))):
+        trainer.step_device_target(cams[i % VIEWS], device_targets[i % VIEWS].data_ptr(), rates)
+    stages = dict(trainer.timings())
+    trainer.set_timing(False)
+    entries, visible = stats.tile_entries, stats.visible_splats
+    pixels = WIDTH * HEIGHT
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    dominant = max(stages, key=stages.get) if stages else None
+    # Algorithmic bytes of the backward pass per launch: each tile entry's index
+    # and 48-byte splat (52 B), per pixel its image, adjoint, stop (36 B), and
+    # 56 B of sums per visible splat.
+    algorithmic = {
+        "backward": 52.0 * entries + 36.0 * pixels + 56.0 * visible,
+        "composite": 52.0 * entries + 20.0 * pixels,
+        "project": 288.0 * GAUSSIANS,
+        "chain rule and step": 528.0 * GAUSSIANS,
+    }
+    roof = None
+    if dominant is not None:
+        b = algorithmic.get(dominant, 0.0)
+        achieved = b / (stages[dominant] * 1e-3) / 1e9 if stages[dominant] > 0 else 0.0
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None, "ms": stages[dominant],
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
+
+    plain = None
+    if not args.no_plain:
+        del trainer
+        torch.cuda.empty_cache()
+        p_trainer, p_ms, p_clocks, _ = run_form(plain_options(splat), "plain")
+        plain = {"iters_per_s": 1000.0 * args.steps / p_ms, "ms_per_step": p_ms / args.steps,
+                 "form": "FP32 SH and Adam state, depth-then-tile sort, host read-back, no graph, exact exp/log"}
+        del p_trainer
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        if O.have_reference():
+            c = O.Cloud(DEGREE, pos, sc, rot, op, sh)
+            (v, p, fx, fy, cx, cy, w, h) = hemisphere_views()[0]
+            threads = cpu_count()
+            secs, done = reference_iterations(O, c, [O.View(v, p, fx, fy, cx, cy, w, h)], [host_targets[0]], threads)
+            cpu = {"value": done / secs, "unit": "iters/s", "cores": threads, "kind": "reference",
+                   "sample": f"1 training iteration of the reference's FP64 twin on the same workload, split into "
+                             f"{threads} row bands on {threads} threads ({secs:.1f} s)"}
+
+    h2d = nbytes + 1240 + 128
+    d2h = 160
+    launches_per_step = 22
+    out = {
+        "metric": "train iters/s @1M Gaussians 1237x822 (fwd+bwd+Adam per view)",
+        "value": value, "unit": "iters/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "fwd_bwd_ms": sum(stages.get(k, 0.0) for k in ("composite", "loss", "backward")),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; the bicycle photos are not available)",
+        "config": {"workload": "1M Gaussians, SH degree 3 (BF16 above DC), 1237x822, 64 cameras on a radius-5 hemisphere, "
+                               "60 deg horizontal fov", "form": "chosen: BF16 SH + BF16-pair Adam state, 64-bit tile|depth "
+                               "keys, CUDA graph, SFU exp/log", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (1M-Gaussian parameters and state, 64 x 4 MB targets)",
+                   "tile_entries": entries, "visible_splats": visible},
+        "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roof,
+        "stages_ms": stages,
+        "plain_fp32": plain,
+        "speedup_vs_plain": (value / world) / plain["iters_per_s"] if plain else None,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches_per_step * args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=30)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
+    parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
+    parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
+    args = parser.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,254 @@
+/*
+ * splat_b200: the training step of a tile-based differentiable Gaussian
+ * rasterizer on one NVIDIA B200 (sm_100a), behind a plain C ABI.
+ *
+ * The entry points mirror the reference trainer's class API, splat::Trainer
+ * (src/train/trainer.hpp:89-270), method for method, so that the reference's
+ * session loop (src/train/train.cpp:474-860) can drive this library through a
+ * thin shim (include/splat_trainer.hpp) instead of its Vulkan trainer. Each
+ * declaration names the reference interface it replaces.
+ *
+ * Conventions, as in the reference:
+ *   - Gaussian clouds are given as the reference's GaussianCloud arrays
+ *     (src/splat/gaussian_cloud.hpp:138-151): positions 3 floats per Gaussian,
+ *     scales 3 (log of the standard deviations), rotations 4 (quaternion
+ *     w, x, y, z, not necessarily normalised), opacities 1 (logit), SH
+ *     3 * (degree + 1)^2 floats per Gaussian, ordered [coefficient][rgb].
+ *   - Cameras are the reference's Camera (src/render/camera.hpp:84-89):
+ *     OpenCV pinhole (x right, y down, z forward), a world->camera matrix
+ *     stored column-major (view[column * 4 + row]), pixel (0,0) the top-left
+ *     corner with pixel centres at +0.5.
+ *   - Targets are RGBA8, width * height * 4 bytes.
+ *   - Host pointers passed in are read during the call only, except the
+ *     prefetched next target (see splat_trainer_step).
+ *   - Every call returns a status (SPLAT_OK or an error below); the message of
+ *     the last error on this thread is splat_last_error(). The reference
+ *     throws instead: BudgetExceeded (trainer.hpp:46-49) maps to
+ *     SPLAT_ERR_BUDGET, std::runtime_error on bad input (trainer.cpp:174,276,
+ *     281,571) to SPLAT_ERR_INVALID, std::logic_error (trainer.cpp:853) to
+ *     SPLAT_ERR_STATE.
+ *   - A handle is used by one thread at a time, as the reference's Trainer.
+ * Options the reference has but this library has no kernel for (the Mip
+ * filters, SH dropout, second-order steps, pose gradients, position noise,
+ * exposure, scoring) are refused with SPLAT_ERR_UNSUPPORTED; nothing falls
+ * back to the CPU.
+ */
+#ifndef SPLAT_B200_H
+#define SPLAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum splat_status {
+  SPLAT_OK = 0,
+  SPLAT_ERR_INVALID = 1,     /* bad argument: sizes, counts, mismatched target */
+  SPLAT_ERR_BUDGET = 2,      /* a view needs more memory than the budget allows (BudgetExceeded) */
+  SPLAT_ERR_UNSUPPORTED = 3, /* an option this library has no kernel for */
+  SPLAT_ERR_DEVICE = 4,      /* a CUDA error, or a device-side check that failed */
+  SPLAT_ERR_NONFINITE = 5,   /* the loss came out NaN or infinite */
+  SPLAT_ERR_STATE = 6,       /* called in the wrong order (e.g. gradients before compute_gradients) */
+  SPLAT_ERR_NOMEM = 7        /* device allocation failed */
+};
+
+/* How the step is computed. The reference has one form; this library keeps the
+ * reference's layout and arithmetic as the default and adds the B200 forms. */
+enum splat_sh_storage {
+  SPLAT_SH_F32 = 0,  /* SH above degree 0 in FP32 */
+  SPLAT_SH_BF16 = 1, /* in bfloat16, rounded at random after each step */
+  SPLAT_SH_F16 = 2   /* in FP16 as the reference (gaussian_cloud.hpp:164-173), rounded at random */
+};
+enum splat_state_storage {
+  SPLAT_STATE_F32 = 0,      /* Adam moments in two FP32 words per parameter */
+  SPLAT_STATE_BF16_PAIR = 1 /* one word of two bfloat16 per parameter, as the reference (train_gradient.comp:33-35) */
+};
+enum splat_sort_form {
+  SPLAT_SORT_DEPTH_THEN_TILE = 0, /* the reference's order: 32-bit depth sort, then a stable sort by tile */
+  SPLAT_SORT_TILE_DEPTH_64 = 1    /* one sort of 64-bit (tile << 32 | depth) keys */
+};
+
+/* TrainerOptions (src/train/trainer.hpp:24-42), plus the B200 knobs. */
+typedef struct splat_trainer_options {
+  float lambda_ssim;          /* 0.2 */
+  float background[3];        /* 0, 0, 0 */
+  float near_plane;           /* 0.01 */
+  int32_t force_fixed_point;  /* 0: float atomics, 1: the bit-reproducible fixed-point backward */
+  int32_t selective_adam;     /* 1 */
+  float opacity_reg;          /* 0 */
+  float scale_reg;            /* 0 */
+  float position_noise;       /* 0; anything else is SPLAT_ERR_UNSUPPORTED */
+  int32_t mip_filter_2d;      /* 0; 1 is SPLAT_ERR_UNSUPPORTED */
+  int32_t pose_gradients;     /* 0; 1 is SPLAT_ERR_UNSUPPORTED */
+  uint64_t memory_budget;     /* bytes; UINT64_MAX for none */
+  /* B200 knobs. */
+  int32_t sh_storage;         /* splat_sh_storage, default SPLAT_SH_F16 (the reference's) */
+  int32_t state_storage;      /* splat_state_storage, default SPLAT_STATE_BF16_PAIR (the reference's) */
+  int32_t sort_form;          /* splat_sort_form, default SPLAT_SORT_DEPTH_THEN_TILE */
+  int32_t exact_math;         /* 1: deterministic exp/log, bit-reproducible by the CPU restatement; 0: SFU */
+  int32_t use_graph;          /* 1: capture the step as a CUDA graph, entry count kept on the device */
+  int32_t digit_bits;         /* radix digit width, 6..8 (0 picks 8) */
+} splat_trainer_options;
+
+/* LearningRates (src/train/trainer.hpp:51-61); trust_region must be 0. */
+typedef struct splat_learning_rates {
+  float position;      /* 1.6e-4 */
+  float scale;         /* 0.005 */
+  float rotation;      /* 0.001 */
+  float opacity;       /* 0.05 */
+  float sh;            /* 0.025 */
+  float sh_rest_scale; /* 0.05 */
+  float trust_region;  /* 0 */
+} splat_learning_rates;
+
+/* StepStats (src/train/trainer.hpp:63-73). */
+typedef struct splat_step_stats {
+  float loss;
+  float l1;
+  float ssim;
+  uint32_t visible_splats;
+  uint32_t tile_entries;
+  float exposure_gradient[12];
+  float pose_gradient[6];
+} splat_step_stats;
+
+/* Camera (src/render/camera.hpp:84-89). */
+typedef struct splat_camera {
+  float view[16];     /* world -> camera, column-major */
+  float position[3];  /* camera centre in world space */
+  float fx, fy, cx, cy;
+  int32_t width, height;
+} splat_camera;
+
+/* GaussianCloud (src/splat/gaussian_cloud.hpp:145-162), as host arrays. */
+typedef struct splat_cloud {
+  int32_t count;
+  int32_t sh_degree;         /* 0..3 */
+  const float *positions;    /* 3 * count */
+  const float *scales;       /* 3 * count */
+  const float *rotations;    /* 4 * count */
+  const float *opacities;    /* count */
+  const float *sh;           /* 3 * (sh_degree + 1)^2 * count */
+} splat_cloud;
+
+typedef struct splat_trainer splat_trainer;
+
+/* The message of the last failed call on this thread ("" if none). */
+const char *splat_last_error(void);
+
+/* Fills the reference's defaults (TrainerOptions{}, LearningRates{}). */
+void splat_trainer_options_default(splat_trainer_options *options);
+void splat_learning_rates_default(splat_learning_rates *rates);
+
+/* Trainer::Trainer (trainer.hpp:91, trainer.cpp:157-208). Uploads the cloud. */
+int splat_trainer_create(const splat_cloud *cloud, const splat_trainer_options *options, splat_trainer **out);
+/* Trainer::~Trainer. */
+int splat_trainer_destroy(splat_trainer *trainer);
+
+/* Trainer::render (trainer.hpp:98): width * height * 4 floats, rgb and the log transmittance. */
+int splat_trainer_render(splat_trainer *trainer, const splat_camera *camera, float *out_pixels);
+
+/* Trainer::compute_gradients (trainer.hpp:104): forward, loss, backward, and
+ * gradients stored for splat_trainer_get_gradients. */
+int splat_trainer_compute_gradients(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
+                                    size_t target_bytes, splat_step_stats *stats);
+/* Trainer::collect_statistics (trainer.hpp:106). */
+int splat_trainer_collect_statistics(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
+                                     size_t target_bytes, splat_step_stats *stats);
+/* Trainer::apply_gradients (trainer.hpp:121): one Adam step from the sums the last
+ * compute_gradients left. */
+int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_rates *rates);
+/* Trainer::step (trainer.hpp:125-126). next_target (may be NULL) is copied to
+ * pinned staging memory while the GPU works on this step and must stay valid
+ * until the next call that uses it. */
+int splat_trainer_step(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
+                       const splat_learning_rates *rates, const uint8_t *next_target, size_t next_target_bytes,
+                       splat_step_stats *stats);
+/* Trainer::step with the target already in device memory (device_target is a
+ * device pointer of width * height * 4 bytes, read during the call). For
+ * callers that keep their photos resident in HBM. New in this library. */
+int splat_trainer_step_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
+                                     size_t target_bytes, const splat_learning_rates *rates, splat_step_stats *stats);
+/* The CUDA stream (cudaStream_t) the trainer's work runs on, for callers that
+ * time it with events or order their own work after it. */
+int splat_trainer_stream(splat_trainer *trainer, void **stream);
+/* Several views (up to 8, of any sizes) in one step: their forward and backward
+ * passes share one set of launches, their gradients are summed and one Adam
+ * step is taken. New in this library; stats receives one entry per view. */
+int splat_trainer_step_batch(splat_trainer *trainer, const splat_camera *cameras, const uint8_t *const *targets,
+                             int32_t views, const splat_learning_rates *rates, splat_step_stats *stats);
+/* Trainer::prefetch_target (trainer.hpp:129). */
+int splat_trainer_prefetch_target(splat_trainer *trainer, const uint8_t *target, size_t target_bytes);
+
+/* Trainer::gradients (trainer.hpp:141-144), in GaussianCloud layout. */
+int splat_trainer_get_gradients(splat_trainer *trainer, float *positions, float *scales, float *rotations, float *opacities,
+                                float *sh);
+/* Trainer::cloud (trainer.hpp:131). Arrays sized as the cloud given to create
+ * (after splat_trainer_apply_changes, as the last cloud given). */
+int splat_trainer_get_cloud(splat_trainer *trainer, float *positions, float *scales, float *rotations, float *opacities,
+                            float *sh);
+/* Trainer::set_active_sh_degree (trainer.hpp:151). */
+int splat_trainer_set_active_sh_degree(splat_trainer *trainer, int32_t degree);
+/* Trainer::densify_stats (trainer.hpp:176, trainer.cpp:686-708): 8 floats per
+ * Gaussian: gradient sum, visits, largest radius, contribution, absolute
+ * gradient sum, marked pixels, marked loss, edge score. */
+int splat_trainer_get_densify_stats(splat_trainer *trainer, float *out);
+/* Trainer::reset_densify_stats (trainer.hpp:178). */
+int splat_trainer_reset_densify_stats(splat_trainer *trainer);
+/* Trainer::reset_opacity (trainer.hpp:163, trainer.cpp:810-819). */
+int splat_trainer_reset_opacity(splat_trainer *trainer, float maximum);
+/* Trainer::apply_changes (trainer.cpp:749-787): replaces the Gaussians by
+ * `cloud`; source[i] is the old index whose optimiser state Gaussian i keeps,
+ * or -1 for a new one. */
+int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud, const int32_t *source);
+
+/* Trainer::gaussian_count, sh_degree, active_sh_degree, uses_fixed_point,
+ * gpu_bytes, bytes_per_gaussian (trainer.hpp:138-193). */
+int splat_trainer_info(splat_trainer *trainer, int64_t *gaussians, int32_t *sh_degree, int32_t *active_sh_degree,
+                       int32_t *uses_fixed_point, uint64_t *gpu_bytes, uint64_t *bytes_per_gaussian);
+/* Trainer::timings (trainer.hpp:186): average milliseconds per training
+ * iteration by stage, in order. Fills up to `capacity` (name, ms) pairs; names
+ * are static strings. *count gets the number of stages. */
+int splat_trainer_timings(splat_trainer *trainer, const char **names, double *ms, int32_t capacity, int32_t *count);
+/* Turns per-stage CUDA-event timing on or off (off by default: it serialises). */
+int splat_trainer_set_timing(splat_trainer *trainer, int32_t enabled);
+/* Trainer::parameters (trainer.hpp:137): the device address of a parameter
+ * group (0 positions, 1 scales, 2 rotations, 3 opacities, 4 SH DC planes,
+ * 5 SH rest planes), valid until the Gaussians change in number. */
+int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint64_t *device_address, uint64_t *bytes);
+
+/* Debug access to the device buffers of the last step, for parity tests:
+ * which: 0 splats (12 floats per Gaussian), 1 reach (1 float), 2 depth keys
+ * (u32, in Gaussian order), 3 entry tile keys (u32 or u64 by sort form, sorted),
+ * 4 entry values (u32, sorted), 5 tile ranges (2 u32 per tile), 6 image
+ * (4 floats per pixel), 7 stops (u32 per pixel), 8 adjoint (4 floats per
+ * pixel), 9 raw sums (16 words per Gaussian: int32 fixed point or float),
+ * 10 counters (visible, total entries, used entries, 0), 11 loss partials
+ * (2 floats per tile), 12 error word. Copies min(bytes, size) bytes; *size
+ * gets the buffer's size in bytes. */
+int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size);
+
+/* Stage-level entry points on device memory, for the reference's operator
+ * tests (tests/test_radix_sort.cpp) and for callers with their own buffers. */
+
+/* RadixSorter::record (src/core/radix_sort.hpp, radix_sort.cpp:70-97): stable
+ * ascending sort of count (u32 key, u32 value) pairs over the low key_bits
+ * bits. keys, values, tmp_keys, tmp_values are device pointers of count
+ * elements; the result is in keys/values. Allocates its scratch. stream may be 0. */
+int splat_radix_sort_u32(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, uint32_t *tmp_values, uint32_t count,
+                         int32_t key_bits, int32_t digit_bits, void *stream);
+/* The same for 64-bit keys over key_bits bits (the (tile << 32 | depth) keys). */
+int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, uint32_t *tmp_values, uint32_t count,
+                         int32_t key_bits, int32_t digit_bits, void *stream);
+
+/* Evaluates the deterministic exp and log of splat_detmath.h on the device, for
+ * the check that they agree bit for bit with the host. Device pointers. */
+int splat_debug_detmath(const float *in, float *out_exp, float *out_log, uint32_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPLAT_B200_H */

@@ -1,0 +1,161 @@
+// ORACLE (test infrastructure only; never linked into the product).
+//
+// A plain C interface over the reference trainer's own FP64 CPU twin,
+// src/train/reference.cpp (reference_render :238, reference_contributions :242,
+// reference_loss :276, reference_gradients :343), which oracle/Makefile
+// compiles unmodified from the reference's sources into oracle/_ref/. Python
+// tests load the result with ctypes. Arrays are the reference's GaussianCloud
+// layout (src/splat/gaussian_cloud.hpp:138-151): positions 3/Gaussian,
+// log-scales 3, quaternions (w,x,y,z) 4, opacity logits 1, SH [k][rgb].
+// The camera is the reference's Camera (src/render/camera.hpp:84-89): a
+// column-major world->camera matrix, the camera centre, fx, fy, cx, cy, size.
+#include "train/reference.hpp"
+
+#include <cstdint>
+#include <cstring>
+#include <exception>
+
+using namespace splat;
+
+namespace {
+
+GaussianCloud make_cloud(int n, int degree, const float *positions, const float *scales, const float *rotations,
+                         const float *opacities, const float *sh) {
+  GaussianCloud cloud;
+  cloud.shDegree = degree;
+  const std::size_t count = static_cast<std::size_t>(n);
+  const std::size_t floats = count * 3 * static_cast<std::size_t>((degree + 1) * (degree + 1));
+  cloud.positions.assign(positions, positions + count * 3);
+  cloud.scales.assign(scales, scales + count * 3);
+  cloud.rotations.assign(rotations, rotations + count * 4);
+  cloud.opacities.assign(opacities, opacities + count);
+  cloud.sh.assign(sh, sh + floats);
+  return cloud;
+}
+
+Camera make_camera(const float *view16, const float *position3, const float *intrinsics4, int width, int height) {
+  Camera camera;
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) camera.view[c][r] = view16[c * 4 + r];
+  camera.position = glm::vec3(position3[0], position3[1], position3[2]);
+  camera.fx = intrinsics4[0];
+  camera.fy = intrinsics4[1];
+  camera.cx = intrinsics4[2];
+  camera.cy = intrinsics4[3];
+  camera.width = width;
+  camera.height = height;
+  return camera;
+}
+
+// flags: 1 noCutoffs, 2 mipFilter2d. background 3 floats. filter3d may be null.
+ReferenceOptions make_options(const float *background, float nearPlane, int flags, float opacityReg, float scaleReg,
+                              const float *filter3d, int n) {
+  ReferenceOptions options;
+  for (int c = 0; c < 3; ++c) options.background[static_cast<std::size_t>(c)] = background[c];
+  options.nearPlane = nearPlane;
+  options.noCutoffs = (flags & 1) != 0;
+  options.mipFilter2d = (flags & 2) != 0;
+  options.opacityReg = opacityReg;
+  options.scaleReg = scaleReg;
+  if (filter3d != nullptr) options.filter3d.assign(filter3d, filter3d + n);
+  return options;
+}
+
+} // namespace
+
+extern "C" {
+
+// rgb: 3 doubles per pixel, logT: 1 per pixel, stop: 1 uint64 per pixel.
+int ref_render(int n, int degree, const float *positions, const float *scales, const float *rotations, const float *opacities,
+               const float *sh, const float *view16, const float *position3, const float *intrinsics4, int width, int height,
+               const float *background, float nearPlane, int flags, const float *filter3d, double *rgb, double *logT,
+               std::uint64_t *stop) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    const Camera camera = make_camera(view16, position3, intrinsics4, width, height);
+    const ReferenceImage image =
+        reference_render(cloud, camera, make_options(background, nearPlane, flags, 0.f, 0.f, filter3d, n));
+    for (std::size_t i = 0; i < image.rgb.size(); ++i) {
+      rgb[i * 3] = image.rgb[i].r;
+      rgb[i * 3 + 1] = image.rgb[i].g;
+      rgb[i * 3 + 2] = image.rgb[i].b;
+      logT[i] = image.logTransmittance[i];
+      stop[i] = image.stop[i];
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+int ref_contributions(int n, int degree, const float *positions, const float *scales, const float *rotations,
+                      const float *opacities, const float *sh, const float *view16, const float *position3,
+                      const float *intrinsics4, int width, int height, const float *background, float nearPlane, int flags,
+                      double *out) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    const Camera camera = make_camera(view16, position3, intrinsics4, width, height);
+    const std::vector<double> c =
+        reference_contributions(cloud, camera, make_options(background, nearPlane, flags, 0.f, 0.f, nullptr, n));
+    std::memcpy(out, c.data(), c.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// rgb: 3 doubles per pixel; target RGBA8; adjoint out: 3 doubles per pixel; totals out: loss, l1, ssim.
+int ref_loss(int width, int height, const double *rgb, const std::uint8_t *target, double lambda, double *adjoint,
+             double *totals) {
+  try {
+    ReferenceImage image;
+    image.width = width;
+    image.height = height;
+    const std::size_t pixels = static_cast<std::size_t>(width) * height;
+    image.rgb.resize(pixels);
+    for (std::size_t i = 0; i < pixels; ++i) image.rgb[i] = glm::dvec3(rgb[i * 3], rgb[i * 3 + 1], rgb[i * 3 + 2]);
+    image.logTransmittance.assign(pixels, 0.0);
+    image.stop.assign(pixels, 0);
+    const std::vector<std::uint8_t> t(target, target + pixels * 4);
+    const ReferenceLoss loss = reference_loss(image, t, lambda);
+    for (std::size_t i = 0; i < pixels; ++i) {
+      adjoint[i * 3] = loss.adjoint[i].r;
+      adjoint[i * 3 + 1] = loss.adjoint[i].g;
+      adjoint[i * 3 + 2] = loss.adjoint[i].b;
+    }
+    totals[0] = loss.loss;
+    totals[1] = loss.l1;
+    totals[2] = loss.ssim;
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// adjoint: 3 doubles per pixel. Outputs are the reference's ParameterGradients arrays.
+int ref_gradients(int n, int degree, const float *positions, const float *scales, const float *rotations, const float *opacities,
+                  const float *sh, const float *view16, const float *position3, const float *intrinsics4, int width, int height,
+                  const double *adjoint, const float *background, float nearPlane, int flags, float opacityReg, float scaleReg,
+                  const float *filter3d, double *gPositions, double *gScales, double *gRotations, double *gOpacities,
+                  double *gSh, double *absoluteCentre) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    const Camera camera = make_camera(view16, position3, intrinsics4, width, height);
+    const std::size_t pixels = static_cast<std::size_t>(width) * height;
+    std::vector<glm::dvec3> a(pixels);
+    for (std::size_t i = 0; i < pixels; ++i) a[i] = glm::dvec3(adjoint[i * 3], adjoint[i * 3 + 1], adjoint[i * 3 + 2]);
+    const ParameterGradients g = reference_gradients(
+        cloud, camera, a, make_options(background, nearPlane, flags, opacityReg, scaleReg, filter3d, n));
+    std::memcpy(gPositions, g.positions.data(), g.positions.size() * sizeof(double));
+    std::memcpy(gScales, g.scales.data(), g.scales.size() * sizeof(double));
+    std::memcpy(gRotations, g.rotations.data(), g.rotations.size() * sizeof(double));
+    std::memcpy(gOpacities, g.opacities.data(), g.opacities.size() * sizeof(double));
+    std::memcpy(gSh, g.sh.data(), g.sh.size() * sizeof(double));
+    std::memcpy(absoluteCentre, g.absoluteCentre.data(), g.absoluteCentre.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+} // extern "C"

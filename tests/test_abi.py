@@ -1,0 +1,103 @@
+"""CPU tests of the drop-in boundary: the C-ABI library loads without a GPU,
+exports every entry point include/*.h declares, and refuses bad arguments and
+unsupported options before it touches a device (the reference throws for
+these: trainer.cpp:174,276,571)."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from tests.conftest import ROOT, splat_module
+
+
+def declared_functions() -> list[str]:
+    """Entry points of the headers that declare an extern "C" ABI (header-only
+    inline helpers such as splat_detmath.h export nothing)."""
+    names = []
+    for header in sorted((ROOT / "include").glob("*.h")):
+        text = header.read_text()
+        if 'extern "C"' not in text:
+            continue
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s*(splat_[a-z_0-9]+)\s*\(", text, flags=re.M):
+            names.append(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_entry_point():
+    lib = ctypes.CDLL(str(ROOT / "vibe-splat_b200" / "libsplat_b200.so"))
+    public = declared_functions()
+    assert len(public) >= 29
+    missing = [n for n in public if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_defaults_are_the_reference_defaults():
+    s = splat_module()
+    o = s._Options()
+    s._lib.splat_trainer_options_default(ctypes.byref(o))
+    assert abs(o.lambda_ssim - 0.2) < 1e-7 and abs(o.near_plane - 0.01) < 1e-9 and o.selective_adam == 1
+    assert o.memory_budget == 2**64 - 1 and o.force_fixed_point == 0
+    r = s._Rates()
+    s._lib.splat_learning_rates_default(ctypes.byref(r))
+    got = [r.position, r.scale, r.rotation, r.opacity, r.sh, r.sh_rest_scale, r.trust_region]
+    np.testing.assert_allclose(got, [1.6e-4, 0.005, 0.001, 0.05, 0.025, 0.05, 0.0], rtol=1e-6)
+
+
+def _tiny_cloud(s, n=4, degree=0):
+    f = 3 * (degree + 1) ** 2
+    return s.GaussianCloud(degree, np.zeros(n * 3, np.float32), np.zeros(n * 3, np.float32),
+                           np.tile(np.array([1, 0, 0, 0], np.float32), n), np.zeros(n, np.float32),
+                           np.zeros(n * f, np.float32))
+
+
+def test_empty_cloud_is_refused():
+    s = splat_module()
+    empty = _tiny_cloud(s, 0)
+    with pytest.raises(RuntimeError, match="empty"):
+        s.Trainer(empty)
+    c, keep = empty._c()
+    h = s._P()
+    status = s._lib.splat_trainer_create(ctypes.byref(c), None, ctypes.byref(h))
+    assert status == s.SPLAT_ERR_INVALID and b"empty" in s._lib.splat_last_error()
+
+
+def test_unsupported_options_are_refused_not_emulated():
+    s = splat_module()
+    for opts in (s.TrainerOptions(mip_filter_2d=True), s.TrainerOptions(position_noise=0.1),
+                 s.TrainerOptions(pose_gradients=True)):
+        with pytest.raises(s.UnsupportedOption):
+            s.Trainer(_tiny_cloud(s), opts)
+
+
+def test_inconsistent_cloud_is_refused():
+    s = splat_module()
+    bad = _tiny_cloud(s)
+    bad.sh = np.zeros(5, np.float32)
+    with pytest.raises(RuntimeError, match="inconsistent"):
+        s.Trainer(bad)
+    bad = _tiny_cloud(s)
+    bad.sh_degree = 4
+    with pytest.raises(RuntimeError):
+        s.Trainer(bad)
+
+
+def test_bad_digit_width_is_refused():
+    s = splat_module()
+    with pytest.raises(s.SplatError) as e:
+        s.Trainer(_tiny_cloud(s), s.TrainerOptions(digit_bits=5))
+    assert e.value.status == s.SPLAT_ERR_INVALID
+
+
+def test_stage_entry_points_check_arguments():
+    s = splat_module()
+    with pytest.raises(s.SplatError):
+        s.radix_sort_device(0, 0, 0, 0, 10, 0)
+    with pytest.raises(s.SplatError):
+        s.radix_sort_device(0, 0, 0, 0, 10, 65, key_bytes=8)
+    # One key needs no work and touches no memory.
+    s.radix_sort_device(0, 0, 0, 0, 1, 32)

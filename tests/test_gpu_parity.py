@@ -1,0 +1,306 @@
+"""GPU parity: the CUDA step against the reference's FP64 twin (with the
+reference's own tolerances, tests/test_train.cpp) and against the FP32 CPU
+restatement (bit for bit on integer results, given the device's own projected
+splats). Every call goes through the C ABI."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.conftest import check_close
+from tests.helpers import device_projection, oracle_entries, tile_count, to_camera, to_cloud
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_oracle_forward(oracle, trainer, cloud, view, n):
+    splats, reach, keys = device_projection(trainer, n)
+    tiles, values, ranges = oracle_entries(oracle, splats, reach, keys, view)
+    image, stops = oracle.forward(splats, values, ranges, view)
+    return splats, reach, keys, tiles, values, ranges, image, stops
+
+
+@pytest.mark.parametrize("sort_form", [0, 1])
+def test_forward_matches_reference_and_restatement(splat, oracle, sort_form):
+    # tests/test_train.cpp:218-235: 100x75, 300 Gaussians, degree 1, seed 7.
+    view = oracle.train_camera(100, 75)
+    cloud = oracle.random_cloud(300, 1, 7)
+    opts = splat.TrainerOptions(sort_form=sort_form)
+    trainer = splat.Trainer(to_cloud(cloud), opts)
+    gpu = trainer.render(to_camera(view)).reshape(-1, 4)
+    rgb, logT, _ = oracle.ref_render(cloud, view)
+    worst = np.abs(gpu[:, :3] - rgb).max()
+    worst_log = np.abs(gpu[:, 3] - logT).max()
+    print(f"  forward: worst difference from CPU {worst:.6f}, log transmittance {worst_log:.6f}")
+    assert worst < 1e-3 and worst_log < 1e-2
+
+    # Bit for bit against the restatement, given the device's own splats.
+    n = cloud.count
+    splats, reach, keys, tiles, values, ranges, image, stops = _run_oracle_forward(oracle, trainer, cloud, view, n)
+    dev_ranges = trainer.debug_download(splat.DEBUG_RANGES, np.uint32).reshape(-1, 2)[: tile_count(view)]
+    dev_values = trainer.debug_download(splat.DEBUG_ENTRY_VALUES, np.uint32)
+    dev_keys = trainer.debug_download(splat.DEBUG_ENTRY_KEYS, np.uint64 if sort_form == 1 else np.uint32)
+    assert dev_values.size == values.size
+    np.testing.assert_array_equal(dev_values, values)
+    dev_tiles = (dev_keys >> np.uint64(32)).astype(np.uint32) if sort_form == 1 else dev_keys
+    np.testing.assert_array_equal(dev_tiles, tiles)
+    np.testing.assert_array_equal(dev_ranges, ranges)
+    np.testing.assert_array_equal(trainer.debug_download(splat.DEBUG_STOPS, np.uint32), stops)
+    np.testing.assert_array_equal(gpu.view(np.uint32), image.view(np.uint32))
+
+
+def test_preprocess_matches_restatement(splat, oracle):
+    view = oracle.train_camera(100, 75)
+    cloud = oracle.random_cloud(300, 3, 21)
+    trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(sh_storage=splat.SH_F32))
+    trainer.render(to_camera(view))
+    splats, reach, keys = device_projection(trainer, cloud.count)
+    o_splats, o_reach, o_keys = oracle.preprocess(cloud, view, sh_storage="f32")
+    np.testing.assert_array_equal(keys, o_keys)
+    visible = keys != 0xFFFFFFFF
+    assert visible.sum() > 100
+    np.testing.assert_array_equal(splats[visible].view(np.uint32), o_splats[visible].view(np.uint32))
+    np.testing.assert_array_equal(reach[visible].view(np.uint32), o_reach[visible].view(np.uint32))
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+def test_loss_and_gradients_match_reference(splat, oracle, fixed):
+    # tests/test_train.cpp:256-293: 72x56, 60 Gaussians degree 1 seed 13,
+    # target seed 11, penalties 0.01; float atomics cosine > 0.999 and length
+    # within 2%, fixed point cosine > 0.97 and length within 10%.
+    view = oracle.train_camera(72, 56)
+    target = oracle.smooth_target(72, 56, 11)
+    cloud = oracle.random_cloud(60, 1, 13)
+    rgb, _, _ = oracle.ref_render(cloud, view)
+    loss, l1, ssim, adjoint = oracle.ref_loss(rgb, 72, 56, target, 0.2)
+    cpu = oracle.ref_gradients(cloud, view, adjoint, opacity_reg=0.01, scale_reg=0.01)
+    opts = splat.TrainerOptions(force_fixed_point=fixed, opacity_reg=0.01, scale_reg=0.01)
+    trainer = splat.Trainer(to_cloud(cloud), opts)
+    assert trainer.uses_fixed_point() == fixed
+    stats = trainer.compute_gradients(to_camera(view), target)
+    assert abs(stats.loss - loss) < 1e-3
+    assert abs(stats.l1 - l1) < 1e-3
+    assert abs(stats.ssim - ssim) < 1e-3
+    g = trainer.gradients()
+    cos, ratio = (0.97, 0.1) if fixed else (0.999, 0.02)
+    check_close(g.positions, cpu.positions, "positions", cos, ratio)
+    check_close(g.scales, cpu.scales, "scales", cos, ratio)
+    check_close(g.rotations, cpu.rotations, "rotations", cos, ratio)
+    check_close(g.opacities, cpu.opacities, "opacities", cos, ratio)
+    check_close(g.sh, cpu.sh, "sh", cos, ratio)
+
+
+def test_fixed_point_sums_are_bit_exact(splat, oracle):
+    # Fixed-point sums: the same integers as the restatement's per-warp
+    # quantisation, given the device's splats, image, stops and adjoint.
+    view = oracle.train_camera(80, 60)
+    target = oracle.smooth_target(80, 60, 19)
+    cloud = oracle.random_cloud(400, 1, 17)
+    cloud.opacities[:] = 2.0
+    trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=True))
+    trainer.compute_gradients(to_camera(view), target)
+    n = cloud.count
+    splats, reach, keys = device_projection(trainer, n)
+    tiles, values, ranges = oracle_entries(oracle, splats, reach, keys, view)
+    image = trainer.debug_download(splat.DEBUG_IMAGE, np.float32).reshape(-1, 4)
+    stops = trainer.debug_download(splat.DEBUG_STOPS, np.uint32)
+    adjoint = trainer.debug_download(splat.DEBUG_ADJOINT, np.float32).reshape(-1, 4)
+    o_image, o_stops = oracle.forward(splats, values, ranges, view)
+    np.testing.assert_array_equal(image.view(np.uint32), o_image.view(np.uint32))
+    np.testing.assert_array_equal(stops, o_stops)
+    raw = trainer.debug_download(splat.DEBUG_RAW, np.int32)[: n * 16].reshape(n, 16)
+    o_raw = oracle.backward(splats, values, ranges, view, image, adjoint, stops, True, n)
+    assert np.count_nonzero(raw) > 100
+    np.testing.assert_array_equal(raw[:, :14], o_raw[:, :14])
+    # The adjoint against the restatement's loss (floats, order of sums differs).
+    o_adj, _, _ = oracle.loss(image, target, view, 0.2)
+    np.testing.assert_allclose(adjoint[:, :3], o_adj[:, :3], rtol=1e-4, atol=1e-9)
+
+
+def test_early_stop_case(splat, oracle):
+    # tests/test_train.cpp:353-403: opaque Gaussians, most pixels stop early.
+    view = oracle.train_camera(80, 60)
+    target = oracle.smooth_target(80, 60, 19)
+    cloud = oracle.random_cloud(400, 1, 17)
+    cloud.opacities[:] = 5.0
+    rgb, logT, stop = oracle.ref_render(cloud, view)
+    assert (stop > 0).sum() > stop.size // 10
+    loss, _, _, adjoint = oracle.ref_loss(rgb, 80, 60, target, 0.2)
+    cpu = oracle.ref_gradients(cloud, view, adjoint)
+    contributions = oracle.ref_contributions(cloud, view)
+    for fixed in (False, True):
+        trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=fixed))
+        gpu = trainer.render(to_camera(view)).reshape(-1, 4)
+        assert np.abs(gpu[:, :3] - rgb).max() < 1e-3
+        assert np.abs(gpu[:, 3] - logT).max() < 1e-2
+        stats = trainer.compute_gradients(to_camera(view), target)
+        assert abs(stats.loss - loss) < 1e-3
+        g = trainer.gradients()
+        d = trainer.densify_stats()
+        cos, ratio = (0.97, 0.1) if fixed else (0.999, 0.02)
+        check_close(d.contribution, contributions, "contribution", cos, ratio)
+        absolute = np.hypot(cpu.absolute_centre[0::2] * 0.5 * 80, cpu.absolute_centre[1::2] * 0.5 * 60)
+        check_close(d.absolute_gradient_sum, absolute, "absolute", cos, ratio)
+        check_close(g.positions, cpu.positions, "positions", cos, ratio)
+        check_close(g.scales, cpu.scales, "scales", cos, ratio)
+        check_close(g.rotations, cpu.rotations, "rotations", cos, ratio)
+        check_close(g.opacities, cpu.opacities, "opacities", cos, ratio)
+        check_close(g.sh, cpu.sh, "sh", cos, ratio)
+
+
+def test_adam_first_step_and_unseen_view(splat, oracle):
+    # tests/test_train.cpp:450-491.
+    view = oracle.train_camera(40, 32)
+    target = oracle.smooth_target(40, 32, 2)
+    cloud = oracle.random_cloud(8, 1, 5)
+    trainer = splat.Trainer(to_cloud(cloud))
+    trainer.compute_gradients(to_camera(view), target)
+    g = trainer.gradients()
+    rates = splat.LearningRates(sh=0.02, sh_rest_scale=0.05)
+    trainer.apply_gradients(rates)
+    after = trainer.cloud()
+    moved = 0
+    for i in range(cloud.sh.size):
+        if g.sh[i] == 0.0:
+            continue
+        dc = i % 12 < 3
+        rate = rates.sh if dc else rates.sh * rates.sh_rest_scale
+        expected = cloud.sh[i] - (rate if g.sh[i] > 0 else -rate)
+        tol = 2e-5 if dc else max(2e-5, abs(expected) / 512.0)
+        assert abs(after.sh[i] - expected) <= tol
+        moved += 1
+    assert moved > 0
+    for i in range(cloud.count):
+        if g.opacities[i] == 0.0:
+            continue
+        assert abs(after.opacities[i] - (cloud.opacities[i] - (rates.opacity if g.opacities[i] > 0 else -rates.opacity))) < 2e-5
+    # A view that sees none of them moves nothing, despite the momentum.
+    away = to_camera(view)
+    rot = np.diag([-1.0, 1.0, -1.0, 1.0]).astype(np.float32)  # 180 degrees about y
+    away.view = rot @ away.view
+    trainer.compute_gradients(away, target)
+    trainer.apply_gradients(rates)
+    unseen = trainer.cloud()
+    np.testing.assert_array_equal(unseen.positions, after.positions)
+    np.testing.assert_array_equal(unseen.opacities, after.opacities)
+    np.testing.assert_array_equal(unseen.sh, after.sh)
+
+
+def test_degenerate_gaussians_do_not_spread(splat, oracle):
+    # tests/test_train.cpp:544-586.
+    view = oracle.train_camera(72, 56)
+    target = oracle.smooth_target(72, 56, 37)
+    healthy = oracle.random_cloud(40, 1, 41)
+    clean = splat.Trainer(to_cloud(healthy))
+    expected = clean.render(to_camera(view))
+    bad = healthy.copy()
+    n, f = healthy.count, 12
+    extra = 5
+    bad.positions = np.concatenate([healthy.positions, np.zeros(extra * 3, np.float32)])
+    bad.scales = np.concatenate([healthy.scales, np.full(extra * 3, np.log(0.3), np.float32)])
+    bad.rotations = np.concatenate([healthy.rotations, np.tile(np.array([1, 0, 0, 0], np.float32), extra)])
+    bad.opacities = np.concatenate([healthy.opacities, np.full(extra, 2.0, np.float32)])
+    bad.sh = np.concatenate([healthy.sh, np.zeros(extra * f, np.float32)])
+    for i in range(n, n + extra):
+        bad.positions[i * 3 + 2] = 4.0
+    bad.positions[n * 3] = np.nan
+    bad.scales[(n + 1) * 3] = 200.0
+    bad.rotations[(n + 2) * 4] = 1e-5
+    bad.opacities[n + 3] = np.nan
+    bad.sh[(n + 4) * f] = np.nan
+    trainer = splat.Trainer(to_cloud(bad))
+    rendered = trainer.render(to_camera(view))
+    np.testing.assert_array_equal(rendered.view(np.uint32), expected.view(np.uint32))
+    stats = trainer.compute_gradients(to_camera(view), target)
+    assert np.isfinite(stats.loss)
+    g = trainer.gradients()
+    assert np.isfinite(g.positions).all() and np.isfinite(g.sh).all()
+
+
+def test_graph_form_matches_plain_form(splat, oracle):
+    view = oracle.train_camera(96, 80)
+    target = oracle.smooth_target(96, 80, 3)
+    cloud = oracle.random_cloud(500, 2, 23)
+    rates = splat.LearningRates(position=1e-3)
+    results = []
+    for graph in (False, True):
+        opts = splat.TrainerOptions(force_fixed_point=True, use_graph=graph, sh_storage=splat.SH_F32,
+                                    state_storage=splat.STATE_F32)
+        t = splat.Trainer(to_cloud(cloud), opts)
+        losses = [t.step(to_camera(view), target, rates).loss for _ in range(5)]
+        results.append((losses, t.cloud()))
+    assert results[0][0] == results[1][0]
+    for a, b in zip((results[0][1].positions, results[0][1].sh), (results[1][1].positions, results[1][1].sh)):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_training_lowers_the_loss(splat, oracle):
+    # In the spirit of tests/test_train.cpp:493-520: fit a rendered view.
+    view = oracle.train_camera(96, 72)
+    truth = oracle.random_cloud(300, 1, 99)
+    ref_rgb, _, _ = oracle.ref_render(truth, view)
+    target = np.concatenate([np.clip(np.rint(ref_rgb * 255), 0, 255), np.full((ref_rgb.shape[0], 1), 255)], axis=1)
+    target = target.astype(np.uint8).ravel()
+    start = oracle.random_cloud(300, 1, 5)
+    trainer = splat.Trainer(to_cloud(start))
+    rates = splat.LearningRates(position=1e-3)
+    first = last = None
+    for it in range(300):
+        s = trainer.step(to_camera(view), target, rates)
+        assert np.isfinite(s.loss)
+        first = s.loss if first is None else first
+        last = s.loss
+    print(f"  overfitting one view: loss {first:.4f} -> {last:.4f}")
+    assert last < first * 0.6
+
+
+def test_detmath_bit_exact_on_device(splat, oracle):
+    import torch
+
+    x = np.concatenate([np.linspace(-90, 90, 100001), np.linspace(1e-6, 2, 100001),
+                        np.random.default_rng(1).normal(0, 5, 100000)]).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    e, l = torch.empty_like(xd), torch.empty_like(xd)
+    splat.detmath_device(xd.data_ptr(), e.data_ptr(), l.data_ptr(), x.size)
+    he, hl = oracle.detmath(x)
+    np.testing.assert_array_equal(e.cpu().numpy().view(np.uint32), he.view(np.uint32))
+    np.testing.assert_array_equal(l.cpu().numpy().view(np.uint32), hl.view(np.uint32))
+
+
+@pytest.mark.parametrize("count", [2, 255, 256, 4096, 4097, 100_000, (1 << 20) + 7])
+@pytest.mark.parametrize("key_bits", [8, 32])
+def test_radix_sort_matches_stable_sort(splat, oracle, count, key_bits):
+    # tests/test_radix_sort.cpp:15-60.
+    import torch
+
+    mask = 0xFFFFFFFF if key_bits == 32 else 0x0F
+    keys = oracle.mt19937(count * 31 + key_bits, count) & np.uint32(mask)
+    order = oracle.stable_order(keys)
+    k = torch.from_numpy(keys.view(np.int32)).cuda()
+    v = torch.arange(count, dtype=torch.int32, device="cuda")
+    tk, tv = torch.empty_like(k), torch.empty_like(v)
+    splat.radix_sort_device(k.data_ptr(), v.data_ptr(), tk.data_ptr(), tv.data_ptr(), count, key_bits)
+    got_k = k.cpu().numpy().view(np.uint32)
+    got_v = v.cpu().numpy().view(np.uint32)
+    np.testing.assert_array_equal(got_k, keys[order])
+    np.testing.assert_array_equal(got_v, order)
+
+
+@pytest.mark.parametrize("digit_bits", [6, 7, 8])
+def test_radix_sort_u64_tile_depth_keys(splat, digit_bits):
+    import torch
+
+    rng = np.random.default_rng(digit_bits)
+    count = 300_001
+    tiles = rng.integers(0, 4056, count, dtype=np.uint64)
+    depth = rng.integers(0, 1 << 32, count, dtype=np.uint64) | np.uint64(0xFFFF0000)  # many ties in the high bits
+    depth[::7] = depth[0]
+    keys = (tiles << np.uint64(32)) | depth
+    order = np.argsort(keys, kind="stable").astype(np.uint32)
+    k = torch.from_numpy(keys.view(np.int64)).cuda()
+    v = torch.arange(count, dtype=torch.int32, device="cuda")
+    tk, tv = torch.empty_like(k), torch.empty_like(v)
+    splat.radix_sort_device(k.data_ptr(), v.data_ptr(), tk.data_ptr(), tv.data_ptr(), count, 44, key_bytes=8,
+                            digit_bits=digit_bits)
+    np.testing.assert_array_equal(k.cpu().numpy().view(np.uint64), keys[order])
+    np.testing.assert_array_equal(v.cpu().numpy().view(np.uint32), order)

@@ -1,0 +1,604 @@
+"""splat_b200: the training step of vibe-splat's tile-based differentiable
+Gaussian rasterizer, on one B200, behind the C ABI of include/splat_b200.h.
+
+This module mirrors the reference's C++ trainer interface (splat::Trainer,
+src/train/trainer.hpp:89-270; TrainerOptions :24-42, LearningRates :51-61,
+StepStats :63-73; GaussianCloud src/splat/gaussian_cloud.hpp:145-162; Camera
+src/render/camera.hpp:84-93) with the same names, argument meanings and error
+behaviour: the reference throws BudgetExceeded, std::runtime_error and
+std::logic_error, and so does this module (BudgetExceeded, RuntimeError,
+StateError). The compute runs only in the CUDA library libsplat_b200.so; if it
+is missing, importing this module fails.
+
+The package directory name has a hyphen, so import it with
+importlib.import_module("vibe-splat_b200").
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = _HERE / "libsplat_b200.so"
+
+if not LIBRARY_PATH.exists():
+    raise ImportError(
+        f"{LIBRARY_PATH} is missing: build it with `python vibe-splat_b200/_build.py` "
+        "(or __graft_entry__.build()); there is no CPU fallback"
+    )
+
+_lib = ctypes.CDLL(str(LIBRARY_PATH))
+
+# ----------------------------------------------------------------- C structs
+
+SPLAT_OK = 0
+SPLAT_ERR_INVALID = 1
+SPLAT_ERR_BUDGET = 2
+SPLAT_ERR_UNSUPPORTED = 3
+SPLAT_ERR_DEVICE = 4
+SPLAT_ERR_NONFINITE = 5
+SPLAT_ERR_STATE = 6
+SPLAT_ERR_NOMEM = 7
+
+SH_F32, SH_BF16, SH_F16 = 0, 1, 2
+STATE_F32, STATE_BF16_PAIR = 0, 1
+SORT_DEPTH_THEN_TILE, SORT_TILE_DEPTH_64 = 0, 1
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [
+        ("lambda_ssim", ctypes.c_float),
+        ("background", ctypes.c_float * 3),
+        ("near_plane", ctypes.c_float),
+        ("force_fixed_point", ctypes.c_int32),
+        ("selective_adam", ctypes.c_int32),
+        ("opacity_reg", ctypes.c_float),
+        ("scale_reg", ctypes.c_float),
+        ("position_noise", ctypes.c_float),
+        ("mip_filter_2d", ctypes.c_int32),
+        ("pose_gradients", ctypes.c_int32),
+        ("memory_budget", ctypes.c_uint64),
+        ("sh_storage", ctypes.c_int32),
+        ("state_storage", ctypes.c_int32),
+        ("sort_form", ctypes.c_int32),
+        ("exact_math", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+        ("digit_bits", ctypes.c_int32),
+    ]
+
+
+class _Rates(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_float) for name in
+                ("position", "scale", "rotation", "opacity", "sh", "sh_rest_scale", "trust_region")]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [
+        ("loss", ctypes.c_float),
+        ("l1", ctypes.c_float),
+        ("ssim", ctypes.c_float),
+        ("visible_splats", ctypes.c_uint32),
+        ("tile_entries", ctypes.c_uint32),
+        ("exposure_gradient", ctypes.c_float * 12),
+        ("pose_gradient", ctypes.c_float * 6),
+    ]
+
+
+class _Camera(ctypes.Structure):
+    _fields_ = [
+        ("view", ctypes.c_float * 16),
+        ("position", ctypes.c_float * 3),
+        ("fx", ctypes.c_float),
+        ("fy", ctypes.c_float),
+        ("cx", ctypes.c_float),
+        ("cy", ctypes.c_float),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+    ]
+
+
+_FP = ctypes.POINTER(ctypes.c_float)
+
+
+class _Cloud(ctypes.Structure):
+    _fields_ = [
+        ("count", ctypes.c_int32),
+        ("sh_degree", ctypes.c_int32),
+        ("positions", _FP),
+        ("scales", _FP),
+        ("rotations", _FP),
+        ("opacities", _FP),
+        ("sh", _FP),
+    ]
+
+
+_P = ctypes.c_void_p
+_lib.splat_last_error.restype = ctypes.c_char_p
+_lib.splat_trainer_options_default.argtypes = [ctypes.POINTER(_Options)]
+_lib.splat_learning_rates_default.argtypes = [ctypes.POINTER(_Rates)]
+_lib.splat_trainer_create.argtypes = [ctypes.POINTER(_Cloud), ctypes.POINTER(_Options), ctypes.POINTER(_P)]
+_lib.splat_trainer_destroy.argtypes = [_P]
+_lib.splat_trainer_render.argtypes = [_P, ctypes.POINTER(_Camera), _FP]
+_lib.splat_trainer_compute_gradients.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Stats)]
+_lib.splat_trainer_collect_statistics.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Stats)]
+_lib.splat_trainer_apply_gradients.argtypes = [_P, ctypes.POINTER(_Rates)]
+_lib.splat_trainer_step.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Rates), _P,
+                                    ctypes.c_size_t, ctypes.POINTER(_Stats)]
+_lib.splat_trainer_step_batch.argtypes = [_P, ctypes.POINTER(_Camera), ctypes.POINTER(_P), ctypes.c_int32,
+                                          ctypes.POINTER(_Rates), ctypes.POINTER(_Stats)]
+_lib.splat_trainer_prefetch_target.argtypes = [_P, _P, ctypes.c_size_t]
+_lib.splat_trainer_step_device_target.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Rates),
+                                                  ctypes.POINTER(_Stats)]
+_lib.splat_trainer_stream.argtypes = [_P, ctypes.POINTER(_P)]
+_lib.splat_trainer_get_gradients.argtypes = [_P, _FP, _FP, _FP, _FP, _FP]
+_lib.splat_trainer_get_cloud.argtypes = [_P, _FP, _FP, _FP, _FP, _FP]
+_lib.splat_trainer_set_active_sh_degree.argtypes = [_P, ctypes.c_int32]
+_lib.splat_trainer_get_densify_stats.argtypes = [_P, _FP]
+_lib.splat_trainer_reset_densify_stats.argtypes = [_P]
+_lib.splat_trainer_reset_opacity.argtypes = [_P, ctypes.c_float]
+_lib.splat_trainer_apply_changes.argtypes = [_P, ctypes.POINTER(_Cloud), ctypes.POINTER(ctypes.c_int32)]
+_lib.splat_trainer_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+_lib.splat_trainer_timings.argtypes = [_P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
+                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+_lib.splat_trainer_set_timing.argtypes = [_P, ctypes.c_int32]
+_lib.splat_trainer_device_parameters.argtypes = [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64),
+                                                 ctypes.POINTER(ctypes.c_uint64)]
+_lib.splat_trainer_debug_download.argtypes = [_P, ctypes.c_int32, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+_lib.splat_radix_sort_u32.argtypes = [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, _P]
+_lib.splat_radix_sort_u64.argtypes = [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, _P]
+_lib.splat_debug_detmath.argtypes = [_P, _P, _P, ctypes.c_uint32]
+
+# ----------------------------------------------------------------- errors
+
+
+class SplatError(RuntimeError):
+    """A failed call; .status is the splat_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class BudgetExceeded(SplatError):
+    """A view would need more memory than the budget allows (trainer.hpp:46-49). The
+    trainer is still usable: remove Gaussians and try again."""
+
+
+class UnsupportedOption(SplatError):
+    """An option of the reference that this library has no kernel for."""
+
+
+class DeviceError(SplatError):
+    """A CUDA error or a failed device-side check."""
+
+
+class NonFiniteLoss(SplatError):
+    """The loss came out NaN or infinite."""
+
+
+class StateError(SplatError):
+    """Called in the wrong order, as the reference's std::logic_error (trainer.cpp:853)."""
+
+
+_ERRORS = {
+    SPLAT_ERR_BUDGET: BudgetExceeded,
+    SPLAT_ERR_UNSUPPORTED: UnsupportedOption,
+    SPLAT_ERR_DEVICE: DeviceError,
+    SPLAT_ERR_NONFINITE: NonFiniteLoss,
+    SPLAT_ERR_STATE: StateError,
+    SPLAT_ERR_NOMEM: DeviceError,
+}
+
+
+def _check(status: int) -> None:
+    if status != SPLAT_OK:
+        message = _lib.splat_last_error().decode()
+        raise _ERRORS.get(status, SplatError)(status, message)
+
+
+# ----------------------------------------------------------------- value types
+
+
+@dataclass
+class GaussianCloud:
+    """The reference's GaussianCloud: raw parameters as in a 3DGS .ply."""
+
+    sh_degree: int = 0
+    positions: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+    scales: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+    rotations: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+    opacities: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+    sh: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+
+    def size(self) -> int:
+        return int(np.asarray(self.opacities).size)
+
+    def sh_coeffs(self) -> int:
+        return (self.sh_degree + 1) ** 2
+
+    def validate(self) -> None:
+        n = self.size()
+        if not 0 <= self.sh_degree <= 3:
+            raise RuntimeError("GaussianCloud: SH degree must be 0..3")
+        sizes = (self.positions.size, self.scales.size, self.rotations.size, self.sh.size)
+        if sizes != (n * 3, n * 3, n * 4, n * 3 * self.sh_coeffs()):
+            raise RuntimeError("GaussianCloud: inconsistent array sizes")
+
+    def _c(self):
+        arrays = [np.ascontiguousarray(np.asarray(a, dtype=np.float32).ravel())
+                  for a in (self.positions, self.scales, self.rotations, self.opacities, self.sh)]
+        c = _Cloud(self.size(), self.sh_degree, *[a.ctypes.data_as(_FP) for a in arrays])
+        return c, arrays
+
+    def copy(self) -> "GaussianCloud":
+        return GaussianCloud(self.sh_degree, *(np.array(a, dtype=np.float32, copy=True) for a in
+                                               (self.positions, self.scales, self.rotations, self.opacities, self.sh)))
+
+
+@dataclass
+class Camera:
+    """The reference's Camera: OpenCV pinhole, world->camera view matrix (4x4,
+    as a numpy array indexed [row, column])."""
+
+    view: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
+    position: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
+    fx: float = 1.0
+    fy: float = 1.0
+    cx: float = 0.0
+    cy: float = 0.0
+    width: int = 1
+    height: int = 1
+
+    def _c(self) -> _Camera:
+        c = _Camera()
+        view = np.asarray(self.view, dtype=np.float32)
+        for col in range(4):
+            for row in range(4):
+                c.view[col * 4 + row] = float(view[row, col])
+        for a in range(3):
+            c.position[a] = float(self.position[a])
+        c.fx, c.fy, c.cx, c.cy = float(self.fx), float(self.fy), float(self.cx), float(self.cy)
+        c.width, c.height = int(self.width), int(self.height)
+        return c
+
+    @staticmethod
+    def look_at(eye, target, up, fx: float, width: int, height: int, fy: float | None = None) -> "Camera":
+        """A camera at `eye` looking at `target` (x right, y down, z forward)."""
+        eye = np.asarray(eye, np.float64)
+        forward = np.asarray(target, np.float64) - eye
+        forward /= np.linalg.norm(forward)
+        right = np.cross(forward, np.asarray(up, np.float64))
+        if np.linalg.norm(right) < 1e-9:
+            right = np.cross(forward, np.array([1.0, 0.0, 0.0]))
+        right /= np.linalg.norm(right)
+        down = np.cross(forward, right)
+        rot = np.stack([right, down, forward])
+        view = np.eye(4)
+        view[:3, :3] = rot
+        view[:3, 3] = -rot @ eye
+        return Camera(view.astype(np.float32), eye.astype(np.float32), fx, fy if fy is not None else fx,
+                      width * 0.5, height * 0.5, width, height)
+
+
+@dataclass
+class TrainerOptions:
+    """TrainerOptions (trainer.hpp:24-42), plus the B200 knobs: SH and optimiser
+    storage, sort form, exact (CPU-reproducible) or SFU exp/log, CUDA graph, and
+    the radix digit width. The defaults are the reference's layout and arithmetic."""
+
+    lambda_ssim: float = 0.2
+    background: tuple = (0.0, 0.0, 0.0)
+    near_plane: float = 0.01
+    force_fixed_point: bool = False
+    selective_adam: bool = True
+    opacity_reg: float = 0.0
+    scale_reg: float = 0.0
+    position_noise: float = 0.0
+    mip_filter_2d: bool = False
+    pose_gradients: bool = False
+    memory_budget: int = 2**64 - 1
+    sh_storage: int = SH_F16
+    state_storage: int = STATE_BF16_PAIR
+    sort_form: int = SORT_DEPTH_THEN_TILE
+    exact_math: bool = True
+    use_graph: bool = False
+    digit_bits: int = 8
+
+    def _c(self) -> _Options:
+        o = _Options()
+        o.lambda_ssim = self.lambda_ssim
+        for c in range(3):
+            o.background[c] = float(self.background[c])
+        o.near_plane = self.near_plane
+        o.force_fixed_point = int(self.force_fixed_point)
+        o.selective_adam = int(self.selective_adam)
+        o.opacity_reg, o.scale_reg, o.position_noise = self.opacity_reg, self.scale_reg, self.position_noise
+        o.mip_filter_2d, o.pose_gradients = int(self.mip_filter_2d), int(self.pose_gradients)
+        o.memory_budget = int(self.memory_budget)
+        o.sh_storage, o.state_storage, o.sort_form = self.sh_storage, self.state_storage, self.sort_form
+        o.exact_math, o.use_graph, o.digit_bits = int(self.exact_math), int(self.use_graph), self.digit_bits
+        return o
+
+
+@dataclass
+class LearningRates:
+    """LearningRates (trainer.hpp:51-61)."""
+
+    position: float = 1.6e-4
+    scale: float = 0.005
+    rotation: float = 0.001
+    opacity: float = 0.05
+    sh: float = 0.025
+    sh_rest_scale: float = 0.05
+    trust_region: float = 0.0
+
+    def _c(self) -> _Rates:
+        return _Rates(self.position, self.scale, self.rotation, self.opacity, self.sh, self.sh_rest_scale,
+                      self.trust_region)
+
+
+@dataclass
+class StepStats:
+    """StepStats (trainer.hpp:63-73)."""
+
+    loss: float = 0.0
+    l1: float = 0.0
+    ssim: float = 0.0
+    visible_splats: int = 0
+    tile_entries: int = 0
+
+    @staticmethod
+    def _from(c: _Stats) -> "StepStats":
+        return StepStats(c.loss, c.l1, c.ssim, c.visible_splats, c.tile_entries)
+
+
+@dataclass
+class Gradients:
+    positions: np.ndarray
+    scales: np.ndarray
+    rotations: np.ndarray
+    opacities: np.ndarray
+    sh: np.ndarray
+
+
+@dataclass
+class DensifyStats:
+    """DensifyStats as Trainer::densify_stats() downloads it (trainer.cpp:686-708)."""
+
+    gradient_sum: np.ndarray
+    visits: np.ndarray
+    max_radius: np.ndarray
+    contribution: np.ndarray
+    absolute_gradient_sum: np.ndarray
+    marked_pixels: np.ndarray
+    marked_loss: np.ndarray
+    edge_score: np.ndarray
+
+
+# Buffers splat_trainer_debug_download knows.
+DEBUG_SPLATS, DEBUG_REACH, DEBUG_DEPTH_KEYS, DEBUG_ENTRY_KEYS, DEBUG_ENTRY_VALUES, DEBUG_RANGES = range(6)
+DEBUG_IMAGE, DEBUG_STOPS, DEBUG_ADJOINT, DEBUG_RAW, DEBUG_COUNTERS, DEBUG_PARTIALS, DEBUG_ERROR = range(6, 13)
+
+
+def _target_ptr(target) -> tuple:
+    t = np.ascontiguousarray(np.asarray(target, dtype=np.uint8).ravel())
+    return t, t.ctypes.data_as(_P), t.nbytes
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(_FP)
+
+
+class Trainer:
+    """Trains Gaussians on one B200: the reference's splat::Trainer, method for method."""
+
+    def __init__(self, initial: GaussianCloud, options: TrainerOptions | None = None):
+        initial.validate()
+        if initial.size() == 0:
+            raise RuntimeError("nothing to train: the cloud is empty")
+        self.options = options or TrainerOptions()
+        c, self._keep = initial._c()
+        handle = _P()
+        _check(_lib.splat_trainer_create(ctypes.byref(c), ctypes.byref(self.options._c()), ctypes.byref(handle)))
+        self._h = handle
+        self._count = initial.size()
+        self._degree = initial.sh_degree
+        self._prefetch_keep = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _check(_lib.splat_trainer_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- the step
+
+    def render(self, camera: Camera) -> np.ndarray:
+        """width * height * 4 floats: rgb and the log transmittance."""
+        out = np.empty(camera.width * camera.height * 4, np.float32)
+        _check(_lib.splat_trainer_render(self._h, ctypes.byref(camera._c()), _fptr(out)))
+        return out
+
+    def compute_gradients(self, camera: Camera, target) -> StepStats:
+        t, p, n = _target_ptr(target)
+        s = _Stats()
+        _check(_lib.splat_trainer_compute_gradients(self._h, ctypes.byref(camera._c()), p, n, ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def collect_statistics(self, camera: Camera, target) -> StepStats:
+        t, p, n = _target_ptr(target)
+        s = _Stats()
+        _check(_lib.splat_trainer_collect_statistics(self._h, ctypes.byref(camera._c()), p, n, ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def apply_gradients(self, rates: LearningRates) -> None:
+        _check(_lib.splat_trainer_apply_gradients(self._h, ctypes.byref(rates._c())))
+
+    def step(self, camera: Camera, target, rates: LearningRates, next_target=None) -> StepStats:
+        t, p, n = _target_ptr(target)
+        s = _Stats()
+        if next_target is not None:
+            nt, np_, nn = _target_ptr(next_target)
+            self._prefetch_keep = nt
+        else:
+            np_, nn = None, 0
+        _check(_lib.splat_trainer_step(self._h, ctypes.byref(camera._c()), p, n, ctypes.byref(rates._c()), np_, nn,
+                                       ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def step_device_target(self, camera: Camera, device_target_ptr: int, rates: LearningRates) -> StepStats:
+        """Trainer::step with the target already in device memory (a device address
+        of width * height * 4 bytes)."""
+        s = _Stats()
+        _check(_lib.splat_trainer_step_device_target(self._h, ctypes.byref(camera._c()), _P(device_target_ptr),
+                                                     camera.width * camera.height * 4, ctypes.byref(rates._c()),
+                                                     ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def stream(self) -> int:
+        """The cudaStream_t the trainer runs on, as an integer handle."""
+        out = _P()
+        _check(_lib.splat_trainer_stream(self._h, ctypes.byref(out)))
+        return out.value or 0
+
+    def step_batch(self, cameras: list, targets: list, rates: LearningRates) -> list:
+        """Several views in one step (new in this library): one Adam step from
+        the summed gradients. Needs sort_form SORT_TILE_DEPTH_64."""
+        k = len(cameras)
+        cams = (_Camera * k)(*[c._c() for c in cameras])
+        kept = [np.ascontiguousarray(np.asarray(t, np.uint8).ravel()) for t in targets]
+        ptrs = (_P * k)(*[a.ctypes.data_as(_P) for a in kept])
+        stats = (_Stats * k)()
+        _check(_lib.splat_trainer_step_batch(self._h, cams, ptrs, k, ctypes.byref(rates._c()), stats))
+        return [StepStats._from(s) for s in stats]
+
+    def prefetch_target(self, target) -> None:
+        t, p, n = _target_ptr(target)
+        self._prefetch_keep = t
+        _check(_lib.splat_trainer_prefetch_target(self._h, p, n))
+
+    # -- state
+
+    def gradients(self) -> Gradients:
+        n, f = self._count, 3 * (self._degree + 1) ** 2
+        g = Gradients(*(np.empty(k, np.float32) for k in (n * 3, n * 3, n * 4, n, n * f)))
+        _check(_lib.splat_trainer_get_gradients(self._h, _fptr(g.positions), _fptr(g.scales), _fptr(g.rotations),
+                                                _fptr(g.opacities), _fptr(g.sh)))
+        return g
+
+    def cloud(self) -> GaussianCloud:
+        n, f = self._count, 3 * (self._degree + 1) ** 2
+        c = GaussianCloud(self._degree, *(np.empty(k, np.float32) for k in (n * 3, n * 3, n * 4, n, n * f)))
+        _check(_lib.splat_trainer_get_cloud(self._h, _fptr(c.positions), _fptr(c.scales), _fptr(c.rotations),
+                                            _fptr(c.opacities), _fptr(c.sh)))
+        return c
+
+    def set_active_sh_degree(self, degree: int) -> None:
+        _check(_lib.splat_trainer_set_active_sh_degree(self._h, int(degree)))
+
+    def densify_stats(self) -> DensifyStats:
+        raw = np.empty(self._count * 8, np.float32)
+        _check(_lib.splat_trainer_get_densify_stats(self._h, _fptr(raw)))
+        r = raw.reshape(-1, 8)
+        return DensifyStats(*(r[:, k].copy() for k in range(8)))
+
+    def reset_densify_stats(self) -> None:
+        _check(_lib.splat_trainer_reset_densify_stats(self._h))
+
+    def reset_opacity(self, maximum: float) -> None:
+        _check(_lib.splat_trainer_reset_opacity(self._h, float(maximum)))
+
+    def apply_changes(self, cloud: GaussianCloud, source) -> None:
+        """Replaces the Gaussians; source[i] is the old index whose optimiser
+        state Gaussian i keeps, -1 for new ones (Trainer::apply_changes)."""
+        cloud.validate()
+        c, keep = cloud._c()
+        src = np.ascontiguousarray(np.asarray(source, np.int32))
+        _check(_lib.splat_trainer_apply_changes(self._h, ctypes.byref(c), src.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        self._count = cloud.size()
+
+    def _info(self):
+        g, d, a, f = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        gb, bpg = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(_lib.splat_trainer_info(self._h, ctypes.byref(g), ctypes.byref(d), ctypes.byref(a), ctypes.byref(f),
+                                       ctypes.byref(gb), ctypes.byref(bpg)))
+        return g.value, d.value, a.value, bool(f.value), gb.value, bpg.value
+
+    def gaussian_count(self) -> int:
+        return self._info()[0]
+
+    def sh_degree(self) -> int:
+        return self._info()[1]
+
+    def active_sh_degree(self) -> int:
+        return self._info()[2]
+
+    def uses_fixed_point(self) -> bool:
+        return self._info()[3]
+
+    def gpu_bytes(self) -> int:
+        return self._info()[4]
+
+    def bytes_per_gaussian(self) -> int:
+        return self._info()[5]
+
+    def set_timing(self, enabled: bool) -> None:
+        _check(_lib.splat_trainer_set_timing(self._h, int(enabled)))
+
+    def timings(self) -> list:
+        names = (ctypes.c_char_p * 16)()
+        ms = (ctypes.c_double * 16)()
+        count = ctypes.c_int32()
+        _check(_lib.splat_trainer_timings(self._h, names, ms, 16, ctypes.byref(count)))
+        return [(names[i].decode(), ms[i]) for i in range(count.value)]
+
+    def device_parameters(self, group: int) -> tuple:
+        addr, size = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(_lib.splat_trainer_device_parameters(self._h, group, ctypes.byref(addr), ctypes.byref(size)))
+        return addr.value, size.value
+
+    def debug_download(self, which: int, dtype=np.uint8) -> np.ndarray:
+        size = ctypes.c_size_t()
+        _check(_lib.splat_trainer_debug_download(self._h, which, None, 0, ctypes.byref(size)))
+        out = np.empty(size.value, np.uint8)
+        if size.value:
+            _check(_lib.splat_trainer_debug_download(self._h, which, out.ctypes.data_as(_P), size.value, ctypes.byref(size)))
+        return out.view(dtype)
+
+
+# ----------------------------------------------------------------- stage entry points
+
+
+def radix_sort_device(keys_ptr: int, values_ptr: int, tmp_keys_ptr: int, tmp_values_ptr: int, count: int,
+                      key_bits: int, key_bytes: int = 4, digit_bits: int = 8, stream: int = 0) -> None:
+    """RadixSorter::record on device pointers (u32 or u64 keys, u32 values)."""
+    fn = _lib.splat_radix_sort_u64 if key_bytes == 8 else _lib.splat_radix_sort_u32
+    _check(fn(_P(keys_ptr), _P(values_ptr), _P(tmp_keys_ptr), _P(tmp_values_ptr), count, key_bits, digit_bits,
+              _P(stream) if stream else None))
+
+
+def detmath_device(in_ptr: int, exp_ptr: int, log_ptr: int, count: int) -> None:
+    _check(_lib.splat_debug_detmath(_P(in_ptr), _P(exp_ptr), _P(log_ptr), count))
+
+
+def library():
+    """The loaded ctypes library, for callers that bind more entry points."""
+    return _lib

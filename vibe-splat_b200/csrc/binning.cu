@@ -1,0 +1,252 @@
+// Tile binning: coverage count with a fused single-pass exclusive scan, entry
+// emission, and tile ranges. Restates shaders/train_bin_count.comp:18-38,
+// shaders/train_bin_emit.comp:18-38, shaders/train_tile_ranges.comp:11-23 and
+// the tile tests of shaders/train_types.glsl:34-77 (splat_tiles,
+// splat_reaches_tile). The reach 2 log(255 opacity) comes from the preprocess
+// pass, so the test here is exact IEEE arithmetic only.
+#include "kernels.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr unsigned long long kScanAggregate = 1ull << 32;
+constexpr unsigned long long kScanInclusive = 2ull << 32;
+constexpr int kScanSpinLimit = 1 << 20;
+
+struct TileRect {
+  uint32_t x0, y0, x1, y1; // inclusive
+};
+
+// Covered tiles of a splat, inclusive (splat_tiles).
+__device__ __forceinline__ TileRect splat_tiles(const float4 ce, int gridW, int gridH) {
+  const float lastX = (float)(gridW - 1), lastY = (float)(gridH - 1);
+  const float lx = fminf(fmaxf(floorf((ce.x - ce.z - 1.0f) / 16.0f), 0.0f), lastX);
+  const float ly = fminf(fmaxf(floorf((ce.y - ce.w - 1.0f) / 16.0f), 0.0f), lastY);
+  const float hx = fminf(fmaxf(floorf((ce.x + ce.z + 1.0f) / 16.0f), 0.0f), lastX);
+  const float hy = fminf(fmaxf(floorf((ce.y + ce.w + 1.0f) / 16.0f), 0.0f), lastY);
+  return {(uint32_t)lx, (uint32_t)ly, (uint32_t)hx, (uint32_t)hy};
+}
+
+// Whether the splat reaches any pixel centre of tile (tx, ty) (splat_reaches_tile).
+__device__ __forceinline__ bool splat_reaches_tile(const float4 q, const float4 ce, float reach, uint32_t tx, uint32_t ty) {
+  const float lowX = ((float)tx * 16.0f + 0.5f) - ce.x, lowY = ((float)ty * 16.0f + 0.5f) - ce.y;
+  const float highX = lowX + 15.0f, highY = lowY + 15.0f;
+  if (lowX <= 0.0f && lowY <= 0.0f && highX >= 0.0f && highY >= 0.0f) return true;
+  float least = 1e30f;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const float x = side == 0 ? lowX : highX;
+    const float y = fminf(fmaxf(-q.y * x / q.z, lowY), highY);
+    least = fminf(least, q.x * x * x + 2.0f * q.y * x * y + q.z * y * y);
+    const float v = side == 0 ? lowY : highY;
+    const float u = fminf(fmaxf(-q.y * v / q.x, lowX), highX);
+    least = fminf(least, q.x * u * u + 2.0f * q.y * u * v + q.z * v * v);
+  }
+  return least <= reach * 1.001f + 1e-3f;
+}
+
+__device__ __forceinline__ uint32_t count_tiles(const float4 q, const float4 ce, float reach, int gridW, int gridH) {
+  const TileRect t = splat_tiles(ce, gridW, gridH);
+  uint32_t n = 0;
+  for (uint32_t y = t.y0; y <= t.y1; ++y)
+    for (uint32_t x = t.x0; x <= t.x1; ++x) n += splat_reaches_tile(q, ce, reach, x, y) ? 1u : 0u;
+  return n;
+}
+
+__device__ __forceinline__ unsigned long long load_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void store_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ int item_view(uint32_t splatIndex, uint32_t n, int views) {
+  return views == 1 ? 0 : (int)(splatIndex / n);
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_bin_count_scan(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
+                     const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
+                     uint32_t *__restrict__ offsets, uint32_t *counters, uint32_t capacity, unsigned long long *status,
+                     uint32_t *ticket, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ unsigned long long s_exclusive;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  if (t == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t numTiles = div_up(items, kScanTile);
+  if (tile >= numTiles) return;
+
+  uint32_t counts[kScanItems];
+  uint32_t threadSum = 0, visible = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    const uint32_t r = tile * kScanTile + t * kScanItems + j;
+    uint32_t c = 0;
+    if (r < items && itemKeys[r] != kInvisible) {
+      const uint32_t s = itemSplat != nullptr ? itemSplat[r] : r;
+      const ViewParams &cam = views.v[item_view(s, n, views.count)];
+      const Splat sp = splats[s];
+      c = count_tiles(sp.conicOpacity, sp.centerExtent, reach[s], cam.gridW, cam.gridH);
+      ++visible;
+    }
+    counts[j] = c;
+    threadSum += c;
+  }
+  // Block scan of the thread sums.
+  uint32_t inclusive = threadSum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, inclusive, o);
+    if (lane >= (uint32_t)o) inclusive += x;
+  }
+  uint32_t warpVisible = __reduce_add_sync(0xFFFFFFFFu, visible);
+  if (lane == 31) s_warp[warp] = inclusive;
+  if (lane == 0 && warpVisible != 0) atomicAdd(&counters[0], warpVisible);
+  __syncthreads();
+  uint32_t before = 0, tileSum = 0;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    before += (uint32_t)w < warp ? s_warp[w] : 0u;
+    tileSum += s_warp[w];
+  }
+  // Decoupled look-back over the tiles before this one.
+  if (t == 0) {
+    unsigned long long exclusive = 0;
+    if (tile == 0) {
+      store_u64(&status[0], kScanInclusive | tileSum);
+    } else {
+      store_u64(&status[tile], kScanAggregate | tileSum);
+      int64_t pred = (int64_t)tile - 1;
+      int spins = 0;
+      while (pred >= 0) {
+        const unsigned long long v = load_u64(&status[pred]);
+        const unsigned long long flag = v & 0xFFFFFFFF00000000ull;
+        if (flag == 0) {
+          if (++spins > kScanSpinLimit) {
+            atomicOr(error, kErrLookbackTimeout);
+            break;
+          }
+          continue;
+        }
+        exclusive += v & 0xFFFFFFFFull;
+        if (flag == kScanInclusive) break;
+        --pred;
+      }
+      store_u64(&status[tile], kScanInclusive | ((exclusive + tileSum) & 0xFFFFFFFFull));
+    }
+    s_exclusive = exclusive;
+    if (tile == numTiles - 1) {
+      const unsigned long long total = exclusive + tileSum;
+      const uint32_t clipped = total > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)total;
+      counters[1] = clipped;
+      counters[2] = clipped < capacity ? clipped : capacity;
+      if (clipped > capacity) atomicOr(error, kErrEntryOverflow);
+    }
+  }
+  __syncthreads();
+  uint32_t running = (uint32_t)s_exclusive + before + inclusive - threadSum;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    const uint32_t r = tile * kScanTile + t * kScanItems + j;
+    if (r < items) offsets[r] = running;
+    running += counts[j];
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    k_bin_emit(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
+               const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
+               const uint32_t *__restrict__ offsets, uint32_t capacity, uint32_t *__restrict__ tileKeys32,
+               unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= items) return;
+  const uint32_t depthKey = itemKeys[r];
+  if (depthKey == kInvisible) return;
+  const uint32_t s = itemSplat != nullptr ? itemSplat[r] : r;
+  const ViewParams &cam = views.v[item_view(s, n, views.count)];
+  const Splat sp = splats[s];
+  const float rc = reach[s];
+  const TileRect t = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+  uint32_t slot = offsets[r];
+  bool overflow = false;
+  for (uint32_t y = t.y0; y <= t.y1; ++y) {
+    for (uint32_t x = t.x0; x <= t.x1; ++x) {
+      if (!splat_reaches_tile(sp.conicOpacity, sp.centerExtent, rc, x, y)) continue;
+      if (slot < capacity) {
+        const uint32_t tileId = y * (uint32_t)cam.gridW + x;
+        if (tileKeys64 != nullptr) {
+          tileKeys64[slot] = ((unsigned long long)((uint32_t)cam.tileBase + tileId) << 32) | depthKey;
+        } else {
+          tileKeys32[slot] = tileId;
+        }
+        entryValues[slot] = s;
+      } else {
+        overflow = true;
+      }
+      ++slot;
+    }
+  }
+  if (overflow) atomicOr(error, kErrEntryOverflow);
+}
+
+__global__ void __launch_bounds__(256) k_tile_ranges(const uint32_t *__restrict__ keys32, const unsigned long long *__restrict__ keys64,
+                                                     const uint32_t *deviceCount, uint32_t tileLimit, uint2 *__restrict__ ranges,
+                                                     uint32_t *error) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t count = *deviceCount;
+  if (k >= count) return;
+  auto tile_of = [&](uint32_t i) { return keys64 != nullptr ? (uint32_t)(keys64[i] >> 32) : keys32[i]; };
+  const uint32_t tile = tile_of(k);
+  if (tile >= tileLimit) {
+    atomicOr(error, kErrBadIndex);
+    return;
+  }
+  if (k == 0 || tile_of(k - 1) != tile) ranges[tile].x = k;
+  if (k + 1 == count || tile_of(k + 1) != tile) ranges[tile].y = k + 1;
+}
+
+} // namespace
+
+size_t bin_scan_scratch_bytes(uint32_t items) {
+  return (size_t)(div_up(items, kScanTile) + 1) * sizeof(unsigned long long) + 256;
+}
+
+void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
+                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *counters,
+                           uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
+  if (items == 0) return;
+  const uint32_t tiles = div_up(items, kScanTile);
+  unsigned long long *status = static_cast<unsigned long long *>(scratch);
+  uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
+  cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
+  k_bin_count_scan<<<tiles, kScanThreads, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, counters,
+                                                       capacity, status, ticket, error);
+}
+
+void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
+                     uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets, uint32_t capacity,
+                     uint32_t *tileKeys32, unsigned long long *tileKeys64, uint32_t *entryValues, uint32_t *error,
+                     cudaStream_t stream) {
+  if (items == 0) return;
+  k_bin_emit<<<div_up(items, 256), 256, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, capacity,
+                                                     tileKeys32, tileKeys64, entryValues, error);
+}
+
+void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *tileKeys64, const uint32_t *deviceCount,
+                        uint32_t capacity, uint32_t tileLimit, uint2 *ranges, uint32_t *error, cudaStream_t stream) {
+  if (capacity == 0) return;
+  k_tile_ranges<<<div_up(capacity, 256), 256, 0, stream>>>(tileKeys32, tileKeys64, deviceCount, tileLimit, ranges, error);
+}
+
+} // namespace sb

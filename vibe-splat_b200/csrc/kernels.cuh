@@ -1,0 +1,130 @@
+// Launch wrappers of the training kernels (host side). Each names the
+// reference shader it replaces.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace sb {
+
+constexpr int kMaxViews = 8;
+struct ViewSet {
+  ViewParams v[kMaxViews];
+  int count;
+  int totalTiles;
+  long long totalPixels;
+};
+
+// SH storage of the coefficients above degree 0 (the DC term is always FP32).
+enum class ShStore : int { F32 = 0, BF16 = 1, F16 = 2 };
+// Adam's moments: two FP32 words per parameter, or the reference's word of two
+// bfloat16 (first moment rounded to nearest, second stochastically).
+enum class StateStore : int { F32 = 0, BF16Pair = 1 };
+
+// Trainable parameters, in this library's HBM layout: positions, log-scales and
+// quaternions per Gaussian (12, 12, 16 bytes), opacity logits (4 bytes), SH
+// planar: shDc[c * n + i] and shRest[((k - 1) * 3 + c) * n + i].
+struct Params {
+  float *positions;
+  float *scales;
+  float *rotations;
+  float *opacities;
+  float *shDc;
+  void *shRest;
+  ShStore shStore;
+  uint32_t n;
+  int shDegree;
+  int shCoeffs;
+};
+
+// train_preprocess.comp: projects every Gaussian into every view. Writes
+// splats[v n + i], reach[v n + i], depthKeys[v n + i] (kInvisible when culled)
+// and, if values is not null, values[v n + i] = i.
+void launch_preprocess(const Params &p, const ViewSet &views, const ViewSet *dViews, Splat *splats, float *reach, uint32_t *depthKeys,
+                       uint32_t *values, cudaStream_t stream);
+
+// train_bin_count.comp + record_scan(coverage): for every item r (a sorted
+// splat in the depth-sorted form, v n + i in the single-sort form) counts the
+// tiles the splat reaches and writes their exclusive scan to offsets[r].
+// counters[0] += visible items, counters[1] = total entries, counters[2] =
+// min(total, capacity). itemSplat: if not null, the splat of item r is
+// itemSplat[r] (sorted values); itemKeys: kInvisible marks culled items.
+void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
+                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *counters,
+                           uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream);
+size_t bin_scan_scratch_bytes(uint32_t items);
+
+// train_bin_emit.comp. Depth-sorted form: tileKeys32[slot] = tile, entryValues[slot]
+// = splat. Single-sort form (tileKeys64 not null): tileKeys64[slot] = (global
+// tile << 32) | depth key.
+void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
+                     uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets, uint32_t capacity,
+                     uint32_t *tileKeys32, unsigned long long *tileKeys64, uint32_t *entryValues, uint32_t *error,
+                     cudaStream_t stream);
+
+// train_tile_ranges.comp over the sorted keys; ranges (2 u32 per global tile)
+// must be cleared first. count is read from deviceCount.
+void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *tileKeys64, const uint32_t *deviceCount,
+                        uint32_t capacity, uint32_t tileLimit, uint2 *ranges, uint32_t *error, cudaStream_t stream);
+
+struct RasterConfig {
+  int exactMath = 1;   // deterministic exp/log (bit-reproducible by the CPU restatement)
+  float background[3] = {0.f, 0.f, 0.f};
+};
+
+// train_forward.comp: one block per tile of 16x16 pixels. image: 4 floats per
+// pixel (rgb, log transmittance), stops: 1 u32 per pixel, both indexed by
+// view pixelBase + y W + x.
+void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
+                    const RasterConfig &cfg, float4 *image, uint32_t *stops, uint32_t splatLimit, uint32_t *error,
+                    cudaStream_t stream);
+
+// train_ssim.comp + train_loss.comp: SSIM fields, then the adjoint and L1.
+// partials: 2 floats per global tile (SSIM sum, L1 sum).
+void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
+                 cudaStream_t stream);
+void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
+                 float4 *adjoint, float2 *partials, cudaStream_t stream);
+// FP64 sums of the per-tile partials into stats (see LossTotals).
+struct LossTotals {
+  double ssimSum[kMaxViews];
+  double l1Sum[kMaxViews];
+};
+void launch_loss_totals(const float2 *partials, const ViewSet &views, const ViewSet *dViews, LossTotals *totals, cudaStream_t stream);
+
+// train_backward_{fixed,float}.comp: raw sums, kRawStride per splat per view
+// (int32 fixed point with each view's fixedScale, or float).
+void launch_backward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
+                     const RasterConfig &cfg, const float4 *image, const float4 *adjoint, const uint32_t *stops,
+                     bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream);
+
+// train_gradient.comp + train_sh_step.comp, fused: the chain rule from the raw
+// sums of every view, then (mode) gradients stored, or Adam's step.
+enum class ChainMode : int { Statistics = 0, Gradients = 1, Step = 2 };
+struct ChainArgs {
+  ChainMode mode;
+  bool statistics;     // add to the densification statistics
+  bool selective;      // Adam leaves parameters without a gradient alone
+  bool fixedPoint;
+  float rates[5];      // position, scale, rotation, opacity, SH
+  float restScale;
+  float beta1, beta2, epsilon, correction1, correction2;
+  uint32_t seed;
+  float opacityReg, scaleReg; // per Gaussian: the option over the count
+};
+struct OptimState {
+  void *state[5];      // per group: F32 {m, v} pairs or BF16 pair words
+  StateStore store;
+};
+struct GradientsOut {
+  float *g[5];         // positions, scales, rotations, opacities, sh (GaussianCloud layout)
+};
+void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
+                  const ChainArgs *dArgs,
+                  OptimState &state, const GradientsOut *grads, float *densifyStats, const uint32_t *error,
+                  cudaStream_t stream);
+
+} // namespace sb

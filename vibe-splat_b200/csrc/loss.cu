@@ -1,0 +1,254 @@
+// Loss: SSIM fields (shaders/train_ssim.comp:42-123), then the adjoint
+// dL/dImage and L1 (shaders/train_loss.comp:52-113), for
+//   L = (1 - lambda) mean|image - target| + lambda (1 - mean SSIM)
+// over pixels and channels, 11x11 Gaussian window (sigma 1.5) cut off and
+// renormalised at the image border. Both kernels run one block per 16x16
+// tile: a horizontal pass over the tile plus 5 rows above and below into
+// shared memory, then a vertical pass out of it. The fields are stored as 9
+// FP32 planes (P, Q, R per channel; 36 bytes per pixel instead of the
+// reference's 48). Per-tile partial sums are added in FP64 on the GPU.
+#include "kernels.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr int kHalo = 5;
+constexpr int kRows = kTileSize + 2 * kHalo;
+constexpr int kSpan = kRows * kTileSize;
+constexpr float kC1 = 0.0001f, kC2 = 0.0009f;
+
+__constant__ float c_weights[11] = {0.00102838f, 0.00759876f, 0.03600077f, 0.10936069f, 0.21300554f, 0.26601172f,
+                                    0.21300554f, 0.10936069f, 0.03600077f, 0.00759876f, 0.00102838f};
+
+__device__ __forceinline__ float window_norm(int at, int size) {
+  float norm = 0.0f;
+  for (int i = max(at - 5, 0); i <= min(at + 5, size - 1); ++i) norm += c_weights[i - at + 5];
+  return norm;
+}
+
+__device__ __forceinline__ float3 unpack_unorm(uint32_t v) {
+  return make_float3((float)(v & 0xFFu) / 255.0f, (float)((v >> 8) & 0xFFu) / 255.0f, (float)((v >> 16) & 0xFFu) / 255.0f);
+}
+
+__device__ __forceinline__ int view_of_tile(const ViewSet &views, int tile) {
+  int v = 0;
+  while (v + 1 < views.count && tile >= views.v[v + 1].tileBase) ++v;
+  return v;
+}
+
+// Sum over the block of 256 threads; valid in thread 0.
+__device__ __forceinline__ float block_sum(float v, float *s_warp) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  if ((threadIdx.x & 31u) == 0) s_warp[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float total = 0.0f;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kTilePixels / 32; ++w) total += s_warp[w];
+  return total;
+}
+
+__global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
+                                                      const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
+                                                      float2 *__restrict__ partials) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ float s_h[5][3][kSpan];
+  __shared__ float s_warp[kTilePixels / 32];
+  const int tile = blockIdx.x;
+  const ViewParams &cam = views.v[view_of_tile(views, tile)];
+  const int local = tile - cam.tileBase;
+  const int W = cam.width, H = cam.height;
+  const int x0 = (local % cam.gridW) * kTileSize, y0 = (local / cam.gridW) * kTileSize;
+  const size_t base = (size_t)cam.pixelBase;
+  const size_t plane = (size_t)views.totalPixels;
+
+  for (int i = threadIdx.x; i < kSpan; i += kTilePixels) {
+    const int r = i / kTileSize, c = i % kTileSize;
+    const int y = y0 + r - kHalo, x = x0 + c;
+    float m[5][3] = {};
+    if (y >= 0 && y < H && x < W) {
+      float norm = 0.0f;
+      const int u0 = max(x - 5, 0), u1 = min(x + 5, W - 1);
+      for (int u = u0; u <= u1; ++u) {
+        const float w = c_weights[u - x + 5];
+        const size_t at = base + (size_t)y * W + u;
+        const float4 a4 = image[at];
+        const float3 b3 = unpack_unorm(target[at]);
+        const float a[3] = {a4.x, a4.y, a4.z}, b[3] = {b3.x, b3.y, b3.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          m[0][k] = fmaf(w, a[k], m[0][k]);
+          m[1][k] = fmaf(w, b[k], m[1][k]);
+          m[2][k] = fmaf(w * a[k], a[k], m[2][k]);
+          m[3][k] = fmaf(w * b[k], b[k], m[3][k]);
+          m[4][k] = fmaf(w * a[k], b[k], m[4][k]);
+        }
+        norm += w;
+      }
+#pragma unroll
+      for (int q = 0; q < 5; ++q)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) m[q][k] = m[q][k] / norm;
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s_h[q][k][i] = m[q][k];
+  }
+  __syncthreads();
+
+  const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
+  float own = 0.0f;
+  if (px < W && py < H) {
+    const float rowNorm = window_norm(py, H);
+    float m[5][3] = {};
+    const int v0 = max(py - 5, 0), v1 = min(py + 5, H - 1);
+    for (int v = v0; v <= v1; ++v) {
+      const float w = c_weights[v - py + 5];
+      const int at = (v - y0 + kHalo) * kTileSize + (threadIdx.x & 15);
+#pragma unroll
+      for (int q = 0; q < 5; ++q)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_h[q][k][at], m[q][k]);
+    }
+    const float norm = rowNorm * window_norm(px, W);
+    const size_t pixel = base + (size_t)py * W + px;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float mx = m[0][k] / rowNorm, my = m[1][k] / rowNorm;
+      const float vx = m[2][k] / rowNorm - mx * mx, vy = m[3][k] / rowNorm - my * my, cxy = m[4][k] / rowNorm - mx * my;
+      const float n1 = 2.0f * mx * my + kC1, n2 = 2.0f * cxy + kC2;
+      const float d1 = mx * mx + my * my + kC1, d2 = vx + vy + kC2;
+      const float s = (n1 * n2) / (d1 * d2);
+      own += s;
+      // n1 and n2 cancelled by hand, as the reference does: n2 can be zero.
+      const float dMu = 2.0f * my * n2 / (d1 * d2) - s * 2.0f * mx / d1;
+      const float dVar = -s / d2;
+      const float dCov = 2.0f * n1 / (d1 * d2);
+      fields[(0 * 3 + k) * plane + pixel] = (dMu - 2.0f * mx * dVar - my * dCov) / norm;
+      fields[(1 * 3 + k) * plane + pixel] = dVar / norm;
+      fields[(2 * 3 + k) * plane + pixel] = dCov / norm;
+    }
+  }
+  const float total = block_sum(own, s_warp);
+  if (threadIdx.x == 0) partials[tile].x = total;
+}
+
+__global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
+                                                      const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
+                                                      float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ float s_h[3][3][kSpan];
+  __shared__ float s_warp[kTilePixels / 32];
+  const int tile = blockIdx.x;
+  const ViewParams &cam = views.v[view_of_tile(views, tile)];
+  const int local = tile - cam.tileBase;
+  const int W = cam.width, H = cam.height;
+  const int x0 = (local % cam.gridW) * kTileSize, y0 = (local / cam.gridW) * kTileSize;
+  const size_t base = (size_t)cam.pixelBase;
+  const size_t plane = (size_t)views.totalPixels;
+
+  for (int i = threadIdx.x; i < kSpan; i += kTilePixels) {
+    const int r = i / kTileSize, c = i % kTileSize;
+    const int y = y0 + r - kHalo, x = x0 + c;
+    float m[3][3] = {};
+    if (y >= 0 && y < H && x < W) {
+      const int u0 = max(x - 5, 0), u1 = min(x + 5, W - 1);
+      for (int u = u0; u <= u1; ++u) {
+        const float w = c_weights[u - x + 5];
+        const size_t at = base + (size_t)y * W + u;
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, fields[(q * 3 + k) * plane + at], m[q][k]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s_h[q][k][i] = m[q][k];
+  }
+  __syncthreads();
+
+  const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
+  float own = 0.0f;
+  if (px < W && py < H) {
+    const float perValue = cam.perPixel;
+    const size_t pixel = base + (size_t)py * W + px;
+    const float4 x4 = image[pixel];
+    const float3 y3 = unpack_unorm(target[pixel]);
+    const float xv[3] = {x4.x, x4.y, x4.z}, yv[3] = {y3.x, y3.y, y3.z};
+    float m[3][3] = {};
+    const int v0 = max(py - 5, 0), v1 = min(py + 5, H - 1);
+    for (int v = v0; v <= v1; ++v) {
+      const float w = c_weights[v - py + 5];
+      const int at = (v - y0 + kHalo) * kTileSize + (threadIdx.x & 15);
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_h[q][k][at], m[q][k]);
+    }
+    float result[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float d = xv[k] - yv[k];
+      own += fabsf(d);
+      const float sgn = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
+      const float ssimPart = m[0][k] + 2.0f * xv[k] * m[1][k] + yv[k] * m[2][k];
+      result[k] = ((1.0f - lambda) * sgn - lambda * ssimPart) * perValue;
+    }
+    adjoint[pixel] = make_float4(result[0], result[1], result[2], 0.0f);
+  }
+  const float total = block_sum(own, s_warp);
+  if (threadIdx.x == 0) partials[tile].y = total;
+}
+
+__global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ partials, const ViewSet *__restrict__ viewsPtr,
+                                                     LossTotals *totals) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ double s_ssim[256], s_l1[256];
+  const int v = blockIdx.x;
+  const ViewParams &cam = views.v[v];
+  double ssim = 0.0, l1 = 0.0;
+  for (int i = threadIdx.x; i < cam.tileCount; i += 256) {
+    const float2 p = partials[cam.tileBase + i];
+    ssim += (double)p.x;
+    l1 += (double)p.y;
+  }
+  s_ssim[threadIdx.x] = ssim;
+  s_l1[threadIdx.x] = l1;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < (unsigned)o) {
+      s_ssim[threadIdx.x] += s_ssim[threadIdx.x + o];
+      s_l1[threadIdx.x] += s_l1[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    totals->ssimSum[v] = s_ssim[0];
+    totals->l1Sum[v] = s_l1[0];
+  }
+}
+
+} // namespace
+
+void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
+                 cudaStream_t stream) {
+  if (views.totalTiles == 0) return;
+  k_ssim<<<views.totalTiles, kTilePixels, 0, stream>>>(image, target, dViews, reinterpret_cast<float *>(fields), partials);
+}
+
+void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
+                 float4 *adjoint, float2 *partials, cudaStream_t stream) {
+  if (views.totalTiles == 0) return;
+  k_loss<<<views.totalTiles, kTilePixels, 0, stream>>>(image, target, reinterpret_cast<const float *>(fields), dViews, lambda,
+                                                       adjoint, partials);
+}
+
+void launch_loss_totals(const float2 *partials, const ViewSet &views, const ViewSet *dViews, LossTotals *totals, cudaStream_t stream) {
+  k_loss_totals<<<views.count, 256, 0, stream>>>(partials, dViews, totals);
+}
+
+} // namespace sb

@@ -1,0 +1,374 @@
+// Forward compositing and its hand-written adjoint, one block of 16x16 threads
+// per tile, one thread per pixel (shaders/train_forward.comp:38-100,
+// shaders/train_backward.glsl:78-157).
+//
+// What differs from the reference, and why it changes no result:
+//   * When a batch of splats is staged into shared memory, the staging thread
+//     folds splat_pixels() and the radius test of splat_at()
+//     (train_types.glsl:43-48,82-86) into two 16-bit masks, one bit per column
+//     and per row of the tile, evaluated with the very expressions a pixel
+//     would use. The per-pixel test becomes one AND; a warp whose two rows the
+//     splat misses skips it without divergence.
+//   * The backward pass reduces each splat's 14 sums over a warp with the
+//     reference's transposed butterfly (reduce_and_add, train_backward.glsl
+//     :51-76), lanes grouped exactly as the reference's 32-wide subgroups (two
+//     rows of 16). Fixed point: each warp total is quantised as the reference
+//     quantises it, then the warps of the tile add their integers in shared
+//     memory and one global atomic per (tile, splat, value) adds the result.
+//     Integer addition is associative, so the sums are bit-identical to the
+//     reference's per-warp global atomics, with up to 8 times fewer of them.
+//     Float: the same shared-memory pre-aggregation (float atomics are not
+//     order-deterministic in the reference either).
+#include "kernels.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr int kBatch = kTilePixels; // splats staged per round, one per thread
+constexpr int kAccStride = 15;      // shared accumulator words per staged splat (odd: no bank conflicts)
+
+// A staged splat, 48 bytes: centre, -qxx/2, -qxy, -qyy/2 (exact rescalings of
+// the conic), opacity, colour, and the tile's column (bits 0-15) and row (bits
+// 16-31) masks.
+struct __align__(16) Staged {
+  float cx, cy, hqx, nqy;
+  float hqz, opacity, r, g;
+  float b;
+  uint32_t mask;
+  uint32_t index;
+  float pad;
+};
+
+__device__ __forceinline__ uint32_t to_u32_clamped(float v) { return (uint32_t)fminf(v, 4294967040.0f); }
+
+// The global tile's view.
+__device__ __forceinline__ int view_of_tile(const ViewSet &views, int tile) {
+  int v = 0;
+  while (v + 1 < views.count && tile >= views.v[v + 1].tileBase) ++v;
+  return v;
+}
+
+// splat_pixels() and the radius test of splat_at(), per column and per row.
+__device__ __forceinline__ uint32_t pixel_masks(const Splat &s, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+  const float cx = s.centerExtent.x, cy = s.centerExtent.y, ex = s.centerExtent.z, ey = s.centerExtent.w;
+  const float r = s.colorRadius.w;
+  const uint32_t ax0 = max(to_u32_clamped(fmaxf(cx - ex - 0.5f, 0.0f)), x0);
+  const uint32_t ay0 = max(to_u32_clamped(fmaxf(cy - ey - 0.5f, 0.0f)), y0);
+  const uint32_t ax1 = min(to_u32_clamped(fmaxf(cx + ex + 0.5f, 0.0f)) + 1u, x1);
+  const uint32_t ay1 = min(to_u32_clamped(fmaxf(cy + ey + 0.5f, 0.0f)) + 1u, y1);
+  uint32_t mask = 0;
+#pragma unroll
+  for (int l = 0; l < kTileSize; ++l) {
+    const uint32_t x = x0 + l, y = y0 + l;
+    const float dx = ((float)x + 0.5f) - cx, dy = ((float)y + 0.5f) - cy;
+    if (x >= ax0 && x < ax1 && !(fabsf(dx) > r)) mask |= 1u << l;
+    if (y >= ay0 && y < ay1 && !(fabsf(dy) > r)) mask |= 1u << (16 + l);
+  }
+  return mask;
+}
+
+__device__ __forceinline__ Staged stage(const Splat &s, uint32_t index, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+  Staged out;
+  out.cx = s.centerExtent.x;
+  out.cy = s.centerExtent.y;
+  out.hqx = -0.5f * s.conicOpacity.x;
+  out.nqy = -s.conicOpacity.y;
+  out.hqz = -0.5f * s.conicOpacity.z;
+  out.opacity = s.conicOpacity.w;
+  out.r = s.colorRadius.x;
+  out.g = s.colorRadius.y;
+  out.b = s.colorRadius.z;
+  out.mask = pixel_masks(s, x0, y0, x1, y1);
+  out.index = index;
+  out.pad = 0.0f;
+  return out;
+}
+
+// -0.5 (qxx dx^2 + qyy dy^2) - qxy dx dy, in this rounding order.
+__device__ __forceinline__ float splat_power(const Staged &s, float dx, float dy) {
+  const float pxy = fmaf(s.nqy, dy, s.hqx * dx);
+  return fmaf(s.hqz * dy, dy, pxy * dx);
+}
+
+struct TileGeometry {
+  int view;
+  uint32_t x0, y0, x1, y1; // pixels of the tile, upper bounds exclusive
+};
+
+__device__ __forceinline__ TileGeometry tile_geometry(const ViewSet &views, int tile) {
+  TileGeometry g;
+  g.view = view_of_tile(views, tile);
+  const ViewParams &cam = views.v[g.view];
+  const int local = tile - cam.tileBase;
+  const uint32_t tx = local % cam.gridW, ty = local / cam.gridW;
+  g.x0 = tx * kTileSize;
+  g.y0 = ty * kTileSize;
+  g.x1 = min(g.x0 + kTileSize, (uint32_t)cam.width);
+  g.y1 = min(g.y0 + kTileSize, (uint32_t)cam.height);
+  return g;
+}
+
+// An index outside the splat array can only come from a broken earlier stage:
+// record it and stage a splat that covers no pixel.
+__device__ __forceinline__ Staged stage_checked(const Splat *__restrict__ splats, uint32_t s, uint32_t splatLimit,
+                                                const TileGeometry &geo, uint32_t *error) {
+  if (s >= splatLimit) {
+    atomicOr(error, kErrBadIndex);
+    Staged empty{};
+    empty.mask = 0u;
+    empty.index = 0u;
+    return empty;
+  }
+  return stage(splats[s], s, geo.x0, geo.y0, geo.x1, geo.y1);
+}
+
+template <class M>
+__global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
+                                                         const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
+                                                         float bgR, float bgG, float bgB, float4 *__restrict__ image,
+                                                         uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ Staged s_batch[kBatch];
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const int tile = blockIdx.x;
+  const TileGeometry geo = tile_geometry(views, tile);
+  const ViewParams &cam = views.v[geo.view];
+  const uint32_t t = threadIdx.x, lx = t & 15u, ly = t >> 4;
+  const uint32_t x = geo.x0 + lx, y = geo.y0 + ly;
+  const bool inside = x < (uint32_t)cam.width && y < (uint32_t)cam.height;
+  const uint32_t myBits = (1u << lx) | (1u << (16 + ly));
+  const uint32_t warpRows = 3u << (16 + 2 * (t >> 5));
+  const float pxf = (float)x + 0.5f, pyf = (float)y + 0.5f;
+
+  const uint2 range = ranges[tile];
+  float cr = 0.0f, cg = 0.0f, cb = 0.0f, T = 1.0f, logT = 0.0f;
+  uint32_t stop = range.x;
+  bool done = !inside;
+  for (uint32_t end = range.y; end > range.x;) {
+    const uint32_t count = min((uint32_t)kBatch, end - range.x);
+    end -= count;
+    if (__syncthreads_count(done) == kTilePixels) break;
+    if (t < count) {
+      const uint32_t s = entryValues[end + t];
+      s_batch[t] = stage_checked(splats, s, splatLimit, geo, error);
+    }
+    __syncthreads();
+    if (done) continue;
+    for (int k = (int)count - 1; k >= 0; --k) {
+      const Staged &s = s_batch[k];
+      const uint32_t mask = s.mask;
+      if ((mask & warpRows) == 0u || (mask & 0xFFFFu) == 0u) continue; // warp-uniform
+      if ((mask & myBits) != myBits) continue;
+      const float dx = pxf - s.cx, dy = pyf - s.cy;
+      const float power = splat_power(s, dx, dy);
+      if (power > 0.0f) continue;
+      const float alpha = fminf(kAlphaMax, s.opacity * M::exp(power));
+      if (!(alpha >= kAlphaMin)) continue;
+      const float oneMinus = 1.0f - alpha;
+      const float logRest = M::log(oneMinus);
+      if (logT + logRest < kLogMinTransmittance) {
+        stop = end + (uint32_t)k + 1u;
+        done = true;
+        break;
+      }
+      const float w = T * alpha;
+      cr = fmaf(w, s.r, cr);
+      cg = fmaf(w, s.g, cg);
+      cb = fmaf(w, s.b, cb);
+      T = T * oneMinus;
+      logT = logT + logRest;
+    }
+  }
+  if (inside) {
+    const size_t at = (size_t)cam.pixelBase + (size_t)y * cam.width + x;
+    image[at] = make_float4(fmaf(T, bgR, cr), fmaf(T, bgG, cg), fmaf(T, bgB, cb), logT);
+    stops[at] = stop;
+  }
+}
+
+// Lane l (< 16) ends up with the warp total of value bitreverse4(l).
+__device__ __forceinline__ float butterfly(float v[16]) {
+  const uint32_t lane = threadIdx.x & 31u;
+#define SB_HALVE(offset, count)                                           \
+  {                                                                       \
+    const bool upper = (lane & (offset)) != 0u;                           \
+    _Pragma("unroll") for (int i = 0; i < (count) / 2; ++i) {             \
+      const float send = upper ? v[i] : v[i + (count) / 2];               \
+      const float keep = upper ? v[i + (count) / 2] : v[i];               \
+      v[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, (offset));         \
+    }                                                                     \
+  }
+  SB_HALVE(1, 16)
+  SB_HALVE(2, 8)
+  SB_HALVE(4, 4)
+  SB_HALVE(8, 2)
+#undef SB_HALVE
+  return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 16);
+}
+
+template <class M, bool FIXED>
+__global__ void __launch_bounds__(kTilePixels, 3)
+    k_backward(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
+               const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
+               const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, void *__restrict__ rawOut,
+               uint32_t splatLimit, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ Staged s_batch[kBatch];
+  __shared__ uint32_t s_acc[kBatch * kAccStride];
+  __shared__ uint32_t s_min[kTilePixels / 32];
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const int tile = blockIdx.x;
+  const TileGeometry geo = tile_geometry(views, tile);
+  const ViewParams &cam = views.v[geo.view];
+  const uint32_t t = threadIdx.x, lane = t & 31u, lx = t & 15u, ly = t >> 4;
+  const uint32_t x = geo.x0 + lx, y = geo.y0 + ly;
+  const bool inside = x < (uint32_t)cam.width && y < (uint32_t)cam.height;
+  const uint32_t myBits = (1u << lx) | (1u << (16 + ly));
+  const uint32_t warpRows = 3u << (16 + 2 * (t >> 5));
+  const float pxf = (float)x + 0.5f, pyf = (float)y + 0.5f;
+  const size_t at = inside ? (size_t)cam.pixelBase + (size_t)y * cam.width + x : 0;
+  const float logTotal = inside ? image[at].w : 0.0f;
+  float4 A = inside ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float perPixel = cam.perPixel;
+  const float scale = cam.fixedScale;
+  const uint2 range = ranges[tile];
+  const uint32_t stop = inside ? stops[at] : range.y;
+  const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, stop);
+  if (lane == 0) s_min[t >> 5] = warpMin;
+  for (int i = t; i < kBatch * kAccStride; i += kTilePixels) s_acc[i] = 0u;
+  __syncthreads();
+  uint32_t tileStop = s_min[0];
+#pragma unroll
+  for (int w = 1; w < kTilePixels / 32; ++w) tileStop = min(tileStop, s_min[w]);
+
+  // The composite behind the current splat, and its log transmittance.
+  float Br = bgR, Bg = bgG, Bb = bgB, logBehind = 0.0f;
+  // Index of value bitreverse4(lane) held by this lane after the butterfly.
+  const uint32_t held = __brev(lane) >> 28;
+  uint32_t *raw32 = static_cast<uint32_t *>(rawOut);
+
+  for (uint32_t start = tileStop; start < range.y; start += kBatch) {
+    const uint32_t count = min((uint32_t)kBatch, range.y - start);
+    __syncthreads();
+    if (t < count) {
+      const uint32_t s = entryValues[start + t];
+      s_batch[t] = stage_checked(splats, s, splatLimit, geo, error);
+    }
+    __syncthreads();
+    for (uint32_t k = 0; k < count; ++k) {
+      const Staged &s = s_batch[k];
+      const uint32_t mask = s.mask;
+      if ((mask & warpRows) == 0u || (mask & 0xFFFFu) == 0u) continue; // warp-uniform: no lane has anything
+      float g[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) g[j] = 0.0f;
+      bool any = false;
+      if (start + k >= stop && (mask & myBits) == myBits) {
+        const float dx = pxf - s.cx, dy = pyf - s.cy;
+        const float power = splat_power(s, dx, dy);
+        if (!(power > 0.0f)) {
+          const float ep = M::exp(power);
+          const float oe = s.opacity * ep;
+          const float alpha = fminf(kAlphaMax, oe);
+          if (alpha >= kAlphaMin) {
+            const float logRest = M::log(1.0f - alpha);
+            const float T = M::exp((logTotal - logBehind) - logRest);
+            const float wA = T * alpha;
+            g[6] = wA * A.x;
+            g[7] = wA * A.y;
+            g[8] = wA * A.z;
+            g[9] = wA * perPixel;
+            // At the 0.99 clamp alpha no longer depends on the parameters.
+            if (oe < kAlphaMax) {
+              const float dAlpha = T * fmaf(A.z, s.b - Bb, fmaf(A.y, s.g - Bg, A.x * (s.r - Br)));
+              g[0] = dAlpha * ep;
+              const float dPower = dAlpha * alpha;
+              const float qx = -2.0f * s.hqx, qy = -s.nqy, qz = -2.0f * s.hqz;
+              const float vx = fmaf(qy, dy, qx * dx), vy = fmaf(qz, dy, qy * dx);
+              g[1] = dPower * vx;
+              g[2] = dPower * vy;
+              g[10] = fabsf(g[1]);
+              g[11] = fabsf(g[2]);
+              const float h = dPower * 0.5f;
+              g[3] = h * vx * vx;
+              g[4] = h * vx * vy;
+              g[5] = h * vy * vy;
+            }
+            any = true;
+            Br = fmaf(alpha, s.r - Br, Br);
+            Bg = fmaf(alpha, s.g - Bg, Bg);
+            Bb = fmaf(alpha, s.b - Bb, Bb);
+            logBehind = logBehind + logRest;
+          }
+        }
+      }
+      if (!__any_sync(0xFFFFFFFFu, any)) continue;
+      const float total = butterfly(g);
+      if (lane < 16 && held < (uint32_t)kRawPerSplat && total != 0.0f) {
+        uint32_t *slot = &s_acc[k * kAccStride + held];
+        if (FIXED) {
+          atomicAdd(reinterpret_cast<int *>(slot), __float2int_rn(fminf(fmaxf(total * scale, -1.0e9f), 1.0e9f)));
+        } else {
+          atomicAdd(reinterpret_cast<float *>(slot), total);
+        }
+      }
+    }
+    __syncthreads();
+    // One global atomic per (splat, value) for the whole tile.
+    if (t < count && s_batch[t].mask != 0u) {
+      const size_t base = ((size_t)s_batch[t].index) * kRawStride;
+#pragma unroll
+      for (int j = 0; j < kRawPerSplat; ++j) {
+        const uint32_t v = s_acc[t * kAccStride + j];
+        if (v != 0u) {
+          if (FIXED) {
+            atomicAdd(reinterpret_cast<int *>(raw32 + base + j), (int)v);
+          } else {
+            atomicAdd(reinterpret_cast<float *>(raw32 + base + j), __uint_as_float(v));
+          }
+          s_acc[t * kAccStride + j] = 0u;
+        }
+      }
+    }
+  }
+}
+
+} // namespace
+
+void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
+                    const RasterConfig &cfg, float4 *image, uint32_t *stops, uint32_t splatLimit, uint32_t *error,
+                    cudaStream_t stream) {
+  if (views.totalTiles == 0) return;
+  if (cfg.exactMath) {
+    k_forward<ExactMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, cfg.background[0],
+                                                                      cfg.background[1], cfg.background[2], image, stops, splatLimit, error);
+  } else {
+    k_forward<FastMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, cfg.background[0],
+                                                                     cfg.background[1], cfg.background[2], image, stops, splatLimit, error);
+  }
+}
+
+void launch_backward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
+                     const RasterConfig &cfg, const float4 *image, const float4 *adjoint, const uint32_t *stops,
+                     bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream) {
+  if (views.totalTiles == 0) return;
+  const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
+  if (cfg.exactMath) {
+    if (fixedPoint)
+      k_backward<ExactMath, true><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
+                                                                               image, adjoint, stops, raw, splatLimit, error);
+    else
+      k_backward<ExactMath, false><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
+                                                                                image, adjoint, stops, raw, splatLimit, error);
+  } else {
+    if (fixedPoint)
+      k_backward<FastMath, true><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
+                                                                              image, adjoint, stops, raw, splatLimit, error);
+    else
+      k_backward<FastMath, false><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
+                                                                               image, adjoint, stops, raw, splatLimit, error);
+  }
+}
+
+} // namespace sb

@@ -1,0 +1,379 @@
+// Onesweep radix sort: see sort.cuh.
+#include "sort.cuh"
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;                        // keys per thread
+constexpr int kSortTileKeys = kSortThreads * kSortItems; // 4096 keys per tile
+constexpr int kMaxPasses = 11;                        // 64 bits at 6-bit digits
+constexpr uint32_t kFlagAggregate = 1u << 30;
+constexpr uint32_t kFlagInclusive = 2u << 30;
+constexpr uint32_t kValueMask = (1u << 30) - 1u;
+constexpr int kLookbackSpinLimit = 1 << 20;
+constexpr int kHistogramItems = 16;
+
+struct ScratchLayout {
+  size_t hist;      // [passes][bins] u32 digit totals
+  size_t counters;  // [passes] u32 tile tickets
+  size_t lookback;  // [passes][tiles][bins] u32 flagged partial sums
+  size_t total;
+};
+
+ScratchLayout sort_scratch_layout(size_t capacity, int bits, int digitBits) {
+  const int passes = (bits + digitBits - 1) / digitBits;
+  const size_t bins = size_t{1} << digitBits;
+  const size_t tiles = (capacity + kSortTileKeys - 1) / kSortTileKeys;
+  ScratchLayout l{};
+  l.hist = 0;
+  l.counters = l.hist + passes * bins * 4;
+  l.lookback = (l.counters + passes * 4 + 255) / 256 * 256;
+  l.total = l.lookback + passes * (tiles > 0 ? tiles : 1) * bins * 4;
+  return l;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t load_volatile(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void store_volatile(uint32_t *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Exclusive prefix sum over the 256 threads of the block; `total` gets the sum.
+// s_warp needs kSortWarps words. Contains two barriers.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_warp, uint32_t &total) {
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  uint32_t inclusive = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t n = __shfl_up_sync(0xFFFFFFFFu, inclusive, o);
+    if (lane >= (uint32_t)o) inclusive += n;
+  }
+  if (lane == 31) s_warp[warp] = inclusive;
+  __syncthreads();
+  uint32_t before = 0, sum = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) {
+    const uint32_t t = s_warp[w];
+    before += (uint32_t)w < warp ? t : 0u;
+    sum += t;
+  }
+  __syncthreads();
+  total = sum;
+  return before + inclusive - v;
+}
+
+template <typename K> __device__ __forceinline__ uint32_t digit_of(K key, int shift, uint32_t mask) {
+  return (uint32_t)(key >> shift) & mask;
+}
+
+// Counts the digits of every pass in one read of the keys. Keys are read as
+// 16-byte vectors; a warp's same-digit keys are added once through match.any.
+template <typename K, int BITS>
+__global__ void __launch_bounds__(kSortThreads) k_histogram(const K *__restrict__ keys, const uint32_t *deviceCount,
+                                                            uint32_t hostCount, int firstBit, int passes,
+                                                            uint32_t *__restrict__ hist) {
+  constexpr int kBins = 1 << BITS;
+  constexpr uint32_t kMask = kBins - 1;
+  constexpr int kPerVec = 16 / sizeof(K);
+  __shared__ uint32_t s_hist[kMaxPasses * kBins];
+  for (int i = threadIdx.x; i < passes * kBins; i += kSortThreads) s_hist[i] = 0;
+  __syncthreads();
+  const uint32_t count = deviceCount != nullptr ? *deviceCount : hostCount;
+  const uint32_t lane = lane_id();
+  const size_t vecs = count / kPerVec;
+  const size_t stride = (size_t)gridDim.x * kSortThreads;
+  for (size_t base = (size_t)blockIdx.x * kSortThreads; base < vecs + (count % kPerVec != 0); base += stride) {
+    const size_t v = base + threadIdx.x;
+    K items[kPerVec];
+    bool valid[kPerVec];
+    if (v < vecs) {
+      const uint4 raw = reinterpret_cast<const uint4 *>(keys)[v];
+      const K *k = reinterpret_cast<const K *>(&raw);
+#pragma unroll
+      for (int e = 0; e < kPerVec; ++e) {
+        items[e] = k[e];
+        valid[e] = true;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < kPerVec; ++e) {
+        const size_t i = v * kPerVec + e;
+        valid[e] = i < count;
+        items[e] = valid[e] ? keys[i] : K(0);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < kPerVec; ++e) {
+      for (int p = 0; p < passes; ++p) {
+        const uint32_t d = valid[e] ? digit_of(items[e], firstBit + p * BITS, kMask) : (uint32_t)kBins;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        if (d < (uint32_t)kBins && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_hist[p * kBins + d], __popc(peers));
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kBins; i += kSortThreads) {
+    if (s_hist[i] != 0) atomicAdd(&hist[i], s_hist[i]);
+  }
+}
+
+// One pass: rank, look back, scatter. Dynamic shared memory holds the tile's
+// keys (later its values) and one digit byte per key.
+template <typename K, int BITS>
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const K *__restrict__ keysIn, const uint32_t *__restrict__ valsIn,
+                                                           K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
+                                                           const uint32_t *deviceCount, uint32_t hostCount,
+                                                           const uint32_t *__restrict__ passHist, uint32_t *lookback,
+                                                           uint32_t *tileCounter, int shift, uint32_t *error) {
+  constexpr int kBins = 1 << BITS;
+  constexpr uint32_t kMask = kBins - 1;
+  extern __shared__ __align__(16) unsigned char s_dynamic[];
+  K *s_keys = reinterpret_cast<K *>(s_dynamic);
+  uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_dynamic);
+  uint8_t *s_digit = s_dynamic + kSortTileKeys * sizeof(K);
+  __shared__ uint32_t s_warpHist[kSortWarps][kBins];
+  __shared__ uint32_t s_digitBase[kBins];
+  __shared__ uint32_t s_globalBase[kBins];
+  __shared__ uint32_t s_scan[kSortWarps];
+  __shared__ uint32_t s_tile;
+
+  const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
+  if (t == 0) s_tile = atomicAdd(tileCounter, 1u);
+  for (int i = t; i < kSortWarps * kBins; i += kSortThreads) (&s_warpHist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t count = deviceCount != nullptr ? *deviceCount : hostCount;
+  const size_t tileStart = (size_t)tile * kSortTileKeys;
+  if (tileStart >= count) return; // Every CTA of the block leaves together.
+  const uint32_t tileKeys = count - tileStart < (size_t)kSortTileKeys ? (uint32_t)(count - tileStart) : (uint32_t)kSortTileKeys;
+
+  // The pass's global digit offsets: an exclusive scan of its histogram.
+  uint32_t binTotal = 0;
+  const uint32_t passOffset = block_exclusive_scan(t < (uint32_t)kBins ? passHist[t] : 0u, s_scan, binTotal);
+
+  // Load the tile linearly with 16-byte vectors, then read it back warp-striped:
+  // warp w owns keys [w*kSortItems*32, (w+1)*kSortItems*32), item j of lane l is
+  // at j*32 + l inside that chunk, so (warp, item, lane) is the input order.
+  constexpr int kPerVec = 16 / sizeof(K);
+  if (tileKeys == kSortTileKeys) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(keysIn + tileStart);
+    uint4 *dst = reinterpret_cast<uint4 *>(s_keys);
+#pragma unroll
+    for (int i = 0; i < kSortTileKeys / kPerVec / kSortThreads; ++i) dst[i * kSortThreads + t] = src[i * kSortThreads + t];
+  } else {
+    for (uint32_t i = t; i < tileKeys; i += kSortThreads) s_keys[i] = keysIn[tileStart + i];
+  }
+  __syncthreads();
+  K key[kSortItems];
+  uint32_t rank[kSortItems];
+  const uint32_t chunk = warp * kSortItems * 32;
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = chunk + j * 32 + lane;
+    key[j] = i < tileKeys ? s_keys[i] : K(0);
+  }
+
+  // Warp-level multi-split ranking, item by item in input order.
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = chunk + j * 32 + lane;
+    const bool valid = i < tileKeys;
+    const uint32_t d = valid ? digit_of(key[j], shift, kMask) : (uint32_t)kBins;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t before = __popc(peers & ((1u << lane) - 1u));
+    const uint32_t prior = valid ? s_warpHist[warp][d] : 0u;
+    __syncwarp();
+    if (valid && lane == (uint32_t)(31 - __clz(peers))) s_warpHist[warp][d] = prior + __popc(peers);
+    __syncwarp();
+    rank[j] = prior + before;
+  }
+  __syncthreads();
+
+  // Per digit: exclusive offsets across warps, and the tile's total.
+  uint32_t digitTotal = 0;
+  if (t < (uint32_t)kBins) {
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = s_warpHist[w][t];
+      s_warpHist[w][t] = digitTotal;
+      digitTotal += c;
+    }
+    // Publish this tile's aggregate (or, for tile 0, its inclusive prefix) early.
+    store_volatile(&lookback[(size_t)tile * kBins + t], (tile == 0 ? kFlagInclusive : kFlagAggregate) | digitTotal);
+  }
+  uint32_t tileTotal;
+  const uint32_t digitBase = block_exclusive_scan(t < (uint32_t)kBins ? digitTotal : 0u, s_scan, tileTotal);
+
+  // Decoupled look-back, one thread per digit.
+  if (t < (uint32_t)kBins) {
+    uint32_t exclusive = 0;
+    if (tile > 0) {
+      int64_t pred = (int64_t)tile - 1;
+      int spins = 0;
+      while (pred >= 0) {
+        const uint32_t v = load_volatile(&lookback[(size_t)pred * kBins + t]);
+        const uint32_t flag = v & ~kValueMask;
+        if (flag == 0u) {
+          if (++spins > kLookbackSpinLimit) {
+            atomicOr(error, kErrLookbackTimeout);
+            break;
+          }
+          continue;
+        }
+        exclusive += v & kValueMask;
+        if (flag == kFlagInclusive) break;
+        --pred;
+      }
+      store_volatile(&lookback[(size_t)tile * kBins + t], kFlagInclusive | ((exclusive + digitTotal) & kValueMask));
+    }
+    s_digitBase[t] = digitBase;
+    s_globalBase[t] = passOffset + exclusive - digitBase;
+  }
+  __syncthreads();
+
+  // Scatter keys into shared memory in digit order, then write them out: the
+  // threads of a warp write consecutive addresses within each digit's run.
+  uint32_t slot[kSortItems];
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = chunk + j * 32 + lane;
+    if (i < tileKeys) {
+      const uint32_t d = digit_of(key[j], shift, kMask);
+      slot[j] = s_digitBase[d] + s_warpHist[warp][d] + rank[j];
+      s_keys[slot[j]] = key[j];
+      s_digit[slot[j]] = (uint8_t)d;
+    }
+  }
+  __syncthreads();
+  // A position outside [0, count) can only come from a look-back that gave up
+  // (kErrLookbackTimeout is set then): skip the write rather than fault.
+  for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
+    const uint32_t dst = s_globalBase[s_digit[i]] + i;
+    if (dst < count) keysOut[dst] = s_keys[i];
+  }
+  __syncthreads();
+
+  // The same permutation for the values.
+  if (tileKeys == kSortTileKeys) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(valsIn + tileStart);
+    uint4 *dst = reinterpret_cast<uint4 *>(s_vals);
+#pragma unroll
+    for (int i = 0; i < kSortTileKeys / 4 / kSortThreads; ++i) dst[i * kSortThreads + t] = src[i * kSortThreads + t];
+  } else {
+    for (uint32_t i = t; i < tileKeys; i += kSortThreads) s_vals[i] = valsIn[tileStart + i];
+  }
+  __syncthreads();
+  uint32_t val[kSortItems];
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = chunk + j * 32 + lane;
+    val[j] = i < tileKeys ? s_vals[i] : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = chunk + j * 32 + lane;
+    if (i < tileKeys) s_vals[slot[j]] = val[j];
+  }
+  __syncthreads();
+  for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
+    const uint32_t dst = s_globalBase[s_digit[i]] + i;
+    if (dst < count) valsOut[dst] = s_vals[i];
+  }
+}
+
+template <typename K, int BITS> size_t onesweep_smem() { return kSortTileKeys * sizeof(K) + kSortTileKeys; }
+
+template <typename K, int BITS>
+int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, size_t capacity, uint32_t hostCount,
+                    const uint32_t *deviceCount, int firstBit, int bits, void *scratch, uint32_t *error,
+                    cudaStream_t stream) {
+  constexpr int kBins = 1 << BITS;
+  const int passes = (bits + BITS - 1) / BITS;
+  if (capacity == 0 || passes == 0) return 0;
+  if (deviceCount == nullptr && hostCount <= 1) return 0;
+  const ScratchLayout l = sort_scratch_layout(capacity, bits, BITS);
+  unsigned char *base = static_cast<unsigned char *>(scratch);
+  uint32_t *hist = reinterpret_cast<uint32_t *>(base + l.hist);
+  uint32_t *counters = reinterpret_cast<uint32_t *>(base + l.counters);
+  uint32_t *lookback = reinterpret_cast<uint32_t *>(base + l.lookback);
+  cudaMemsetAsync(scratch, 0, l.total, stream);
+
+  const uint32_t launchKeys = deviceCount != nullptr ? (uint32_t)capacity : hostCount;
+  const uint32_t tiles = div_up(launchKeys, kSortTileKeys);
+  const uint32_t histBlocks = std::min<uint32_t>(div_up(launchKeys, kSortThreads * kHistogramItems), 148u * 8u);
+  k_histogram<K, BITS><<<std::max(histBlocks, 1u), kSortThreads, 0, stream>>>(keys, deviceCount, hostCount, firstBit, passes, hist);
+
+  static bool configured = false;
+  const size_t smem = onesweep_smem<K, BITS>();
+  if (!configured) {
+    cudaFuncSetAttribute(k_onesweep<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = true;
+  }
+  K *srcK = keys, *dstK = tmpKeys;
+  uint32_t *srcV = values, *dstV = tmpValues;
+  for (int p = 0; p < passes; ++p) {
+    k_onesweep<K, BITS><<<tiles, kSortThreads, smem, stream>>>(srcK, srcV, dstK, dstV, deviceCount, hostCount,
+                                                               hist + p * kBins, lookback + (size_t)p * tiles * kBins,
+                                                               counters + p, firstBit + p * BITS, error);
+    K *tk = srcK;
+    srcK = dstK;
+    dstK = tk;
+    uint32_t *tv = srcV;
+    srcV = dstV;
+    dstV = tv;
+  }
+  return srcK == keys ? 0 : 1;
+}
+
+} // namespace
+
+size_t sort_scratch_bytes(size_t capacity, int /*keyBytes*/, int bits, int digitBits) {
+  return sort_scratch_layout(capacity, bits, digitBits).total;
+}
+
+int sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t *tmpKeys, uint32_t *tmpValues, size_t capacity,
+                   uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits, void *scratch,
+                   uint32_t *error, cudaStream_t stream) {
+  switch (digitBits) {
+  case 6:
+    return sort_pairs_impl<uint32_t, 6>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount, firstBit, bits,
+                                        scratch, error, stream);
+  case 7:
+    return sort_pairs_impl<uint32_t, 7>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount, firstBit, bits,
+                                        scratch, error, stream);
+  default:
+    return sort_pairs_impl<uint32_t, 8>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount, firstBit, bits,
+                                        scratch, error, stream);
+  }
+}
+
+int sort_pairs_u64(unsigned long long *keys, uint32_t *values, unsigned long long *tmpKeys, uint32_t *tmpValues,
+                   size_t capacity, uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
+                   void *scratch, uint32_t *error, cudaStream_t stream) {
+  switch (digitBits) {
+  case 6:
+    return sort_pairs_impl<unsigned long long, 6>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount,
+                                                  firstBit, bits, scratch, error, stream);
+  case 7:
+    return sort_pairs_impl<unsigned long long, 7>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount,
+                                                  firstBit, bits, scratch, error, stream);
+  default:
+    return sort_pairs_impl<unsigned long long, 8>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount,
+                                                  firstBit, bits, scratch, error, stream);
+  }
+}
+
+} // namespace sb

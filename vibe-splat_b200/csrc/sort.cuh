@@ -1,0 +1,49 @@
+// Onesweep-style stable LSD radix sort of (key, u32 value) pairs.
+//
+// Replaces the reference's three-kernel-per-pass sort (RadixSorter::record,
+// src/core/radix_sort.cpp:70-97, with shaders/radix_histogram.comp,
+// scan_blocks/scan_add.comp and radix_scatter.comp) with the single-pass
+// scheme of Adinets and Merrill ("Onesweep", 2022):
+//   1. one histogram kernel counts the digits of every pass at once;
+//   2. one kernel per pass ranks a tile of keys with warp-level match.any,
+//      finds its global offsets through a decoupled look-back over the tiles
+//      before it, and scatters through shared memory so that each warp writes
+//      contiguous runs.
+// Keys are read once per pass and written once; the reference reads them
+// twice per pass (histogram and scatter) and runs a recursive scan between.
+// Stability matches std::stable_sort (tests/test_radix_sort.cpp:48-59 in the
+// reference): keys of equal digit keep their input order inside a tile (ranks
+// follow warp, then item, then lane order over a warp-contiguous chunk), and
+// tiles are ordered by their id, which is claimed in launch order through an
+// atomic counter, so a tile only ever waits on tiles that already run.
+//
+// Every look-back wait is bounded: after kLookbackSpinLimit polls the kernel
+// sets kErrLookbackTimeout in the error word, takes what it has and finishes.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sb {
+
+// Scratch one sort needs, in bytes, for `capacity` keys of `keyBytes` bytes,
+// sorted over `bits` significant bits (from bit `firstBit`) with `digitBits`-bit
+// digits. The layout is fixed by sort_scratch_layout() in sort.cu.
+size_t sort_scratch_bytes(size_t capacity, int keyBytes, int bits, int digitBits);
+
+// Sorts count pairs, ascending by bits [firstBit, firstBit + bits) of the keys.
+// keys/values hold the input; tmpKeys/tmpValues are the same size. Returns 0 if
+// the sorted pairs ended in keys/values, 1 if in tmpKeys/tmpValues. The count is
+// read from *deviceCount when it is not null (CUDA-graph friendly; capacity
+// bounds the launch), else hostCount is used. scratch must hold
+// sort_scratch_bytes(capacity, ...) bytes; error is a device word that gets
+// kErrLookbackTimeout if a wait ran out. Supported digitBits: 6, 7, 8.
+int sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t *tmpKeys, uint32_t *tmpValues, size_t capacity,
+                   uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
+                   void *scratch, uint32_t *error, cudaStream_t stream);
+int sort_pairs_u64(unsigned long long *keys, uint32_t *values, unsigned long long *tmpKeys, uint32_t *tmpValues,
+                   size_t capacity, uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
+                   void *scratch, uint32_t *error, cudaStream_t stream);
+
+} // namespace sb

@@ -1,0 +1,1237 @@
+// The trainer behind the C ABI of include/splat_b200.h: device buffers, the
+// order of the step's launches, the host reads, and the CUDA-graph form.
+//
+// Mirrors splat::Trainer (src/train/trainer.cpp). The reference records two
+// Vulkan submissions per step with a host wait between them, to read the tile
+// entry count and size the entry buffers (trainer.cpp:328-375, 593-602). This
+// trainer does the same in its plain form. In its graph form the entry count
+// stays on the device: the entry pool is sized from earlier steps, the
+// kernels after the emission skip their work when a step would overflow it
+// (an error bit, never an out-of-bounds write), and the host grows the pool
+// and runs that step again. With no host wait inside, the whole step is one
+// CUDA graph.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_fp16.h>
+
+#include "kernels.cuh"
+#include "sort.cuh"
+#include "splat_b200.h"
+
+namespace sb {
+
+thread_local std::string g_lastError;
+
+struct Failure {
+  int status;
+  std::string message;
+};
+
+#define SB_CUDA(call)                                                                                  \
+  do {                                                                                                 \
+    const cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) throw Failure{SPLAT_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+class DeviceBuffer {
+public:
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (ptr_ != nullptr) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+  }
+  // Makes the buffer at least `bytes` long; the contents are lost when it grows.
+  void ensure(size_t bytes) {
+    if (bytes <= bytes_ && ptr_ != nullptr) return;
+    release();
+    const size_t want = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(&ptr_, want) != cudaSuccess) {
+      cudaGetLastError();
+      ptr_ = nullptr;
+      throw Failure{SPLAT_ERR_NOMEM, "device allocation of " + std::to_string(want) + " bytes failed"};
+    }
+    bytes_ = want;
+  }
+  template <class T = void> T *get() const { return static_cast<T *>(ptr_); }
+  size_t bytes() const { return bytes_; }
+
+private:
+  void *ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+class PinnedBuffer {
+public:
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer &) = delete;
+  PinnedBuffer &operator=(const PinnedBuffer &) = delete;
+  friend void swap(PinnedBuffer &a, PinnedBuffer &b) noexcept {
+    std::swap(a.ptr_, b.ptr_);
+    std::swap(a.bytes_, b.bytes_);
+  }
+  ~PinnedBuffer() {
+    if (ptr_ != nullptr) cudaFreeHost(ptr_);
+  }
+  void ensure(size_t bytes) {
+    if (bytes <= bytes_ && ptr_ != nullptr) return;
+    if (ptr_ != nullptr) cudaFreeHost(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+    if (cudaMallocHost(&ptr_, std::max<size_t>(bytes, 64)) != cudaSuccess) {
+      cudaGetLastError();
+      throw Failure{SPLAT_ERR_NOMEM, "pinned host allocation failed"};
+    }
+    bytes_ = std::max<size_t>(bytes, 64);
+  }
+  template <class T = void> T *get() const { return static_cast<T *>(ptr_); }
+  size_t bytes() const { return bytes_; }
+
+private:
+  void *ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// What the host reads back at the end of a step.
+struct StepReadback {
+  uint32_t counters[4];
+  uint32_t error;
+  uint32_t pad[3];
+  LossTotals totals;
+};
+
+constexpr int kStages = 8;
+const char *const kStageNames[kStages] = {"project", "depth sort", "count tiles", "tile lists",
+                                          "composite", "loss", "backward", "chain rule and step"};
+
+uint32_t bits_for(uint32_t values) {
+  uint32_t b = 0;
+  while (b < 32 && (1ull << b) < values) ++b;
+  return std::max<uint32_t>(b, 1);
+}
+
+class Trainer {
+public:
+  Trainer(const splat_cloud &cloud, const splat_trainer_options &options);
+  ~Trainer();
+
+  splat_trainer_options opt;
+  uint32_t n = 0;
+  int shDegree = 0, shCoeffs = 1, activeDegree = 0;
+  ShStore shStore = ShStore::F16;
+  StateStore stateStore = StateStore::BF16Pair;
+  bool fixedPoint = false, oneSort = false, exactMath = true, useGraph = false;
+  int digitBits = 8;
+  cudaStream_t stream = nullptr;
+
+  DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
+  DeviceBuffer state[5], grads[5], densifyStats;
+  bool haveGradients = false, haveRaw = false;
+
+  // Per (view, Gaussian).
+  int viewSlots = 0;
+  DeviceBuffer splats, reach, depthKeys, values, tmpKeys, tmpValues, offsets, raw;
+  // Tile entries.
+  uint32_t entryCapacity = 0;
+  DeviceBuffer entryKeys, entryValues, tmpEntryKeys, tmpEntryValues;
+  bool entriesInTmp = false, depthInTmp = false;
+  // Per pixel and per tile of the views of a step.
+  DeviceBuffer image, stops, adjoint, fields, target, ranges, partials;
+  // Small things.
+  DeviceBuffer dViews, dArgs, dReadback, sortScratchDepth, sortScratchEntries, scanScratch;
+  PinnedBuffer hViews, hArgs, hReadback, staging, stagingNext;
+  const uint8_t *prefetched = nullptr;
+  size_t prefetchedBytes = 0;
+
+  ViewSet views{};
+  uint32_t adamStep = 0;
+  ChainArgs lastArgs{};
+
+  // Graph form: one instantiated graph per shape of step.
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::map<std::string, GraphEntry> graphs;
+
+  // Timings.
+  bool timing = false;
+  cudaEvent_t events[kStages + 1] = {};
+  double stageTotals[kStages] = {};
+  uint64_t timedIterations = 0;
+
+  void set_views(const splat_camera *cameras, int count);
+  void ensure_view_buffers();
+  void ensure_entries(uint32_t total);
+  uint64_t entry_bytes(uint64_t entries) const;
+  uint64_t gpu_bytes() const;
+  uint64_t bytes_per_gaussian() const;
+  Params params() const;
+  OptimState optim_state();
+  void upload_targets(const uint8_t *const *targets, const size_t *bytes, int count);
+  void record_prepare();
+  void record_forward();
+  void record_backward_and_chain(ChainMode mode, bool statistics);
+  void record_readback();
+  void mark(int stage);
+  void clear_graphs();
+  std::string graph_key(ChainMode mode, bool statistics) const;
+  void run(const splat_camera *cameras, const uint8_t *const *targets, const size_t *bytes, int count, ChainMode mode,
+           const splat_learning_rates *rates, bool statistics, splat_step_stats *stats, bool deviceTargets = false);
+  void render(const splat_camera *camera, float *out);
+  void finish_stats(splat_step_stats *stats, int count);
+  void fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates);
+};
+
+// ---------------------------------------------------------------- set-up
+
+Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options) : opt(options) {
+  if (cloud.count <= 0) throw Failure{SPLAT_ERR_INVALID, "nothing to train: the cloud is empty"};
+  if (cloud.sh_degree < 0 || cloud.sh_degree > 3) throw Failure{SPLAT_ERR_INVALID, "GaussianCloud: SH degree must be 0..3"};
+  if (cloud.positions == nullptr || cloud.scales == nullptr || cloud.rotations == nullptr || cloud.opacities == nullptr ||
+      cloud.sh == nullptr) {
+    throw Failure{SPLAT_ERR_INVALID, "GaussianCloud: inconsistent array sizes"};
+  }
+  if (opt.position_noise != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "position noise has no kernel in this library"};
+  if (opt.mip_filter_2d != 0) throw Failure{SPLAT_ERR_UNSUPPORTED, "the Mip 2D filter has no kernel in this library"};
+  if (opt.pose_gradients != 0) throw Failure{SPLAT_ERR_UNSUPPORTED, "pose gradients have no kernel in this library"};
+  if (opt.sh_storage < 0 || opt.sh_storage > 2 || opt.state_storage < 0 || opt.state_storage > 1 || opt.sort_form < 0 ||
+      opt.sort_form > 1) {
+    throw Failure{SPLAT_ERR_INVALID, "unknown storage or sort form"};
+  }
+  n = (uint32_t)cloud.count;
+  shDegree = cloud.sh_degree;
+  activeDegree = shDegree;
+  shCoeffs = (shDegree + 1) * (shDegree + 1);
+  shStore = (ShStore)opt.sh_storage;
+  stateStore = (StateStore)opt.state_storage;
+  // The reference picks fixed point on GPUs without float atomics (trainer.cpp:181); a B200 has them.
+  fixedPoint = opt.force_fixed_point != 0;
+  oneSort = opt.sort_form == SPLAT_SORT_TILE_DEPTH_64;
+  exactMath = opt.exact_math != 0;
+  useGraph = opt.use_graph != 0;
+  digitBits = opt.digit_bits == 0 ? 8 : opt.digit_bits;
+  if (digitBits < 6 || digitBits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
+  SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
+
+  const size_t nn = n;
+  positions.ensure(nn * 12);
+  scales.ensure(nn * 12);
+  rotations.ensure(nn * 16);
+  opacities.ensure(nn * 4);
+  shDc.ensure(nn * 12);
+  const size_t rest = nn * 3 * (shCoeffs - 1);
+  shRest.ensure(std::max<size_t>(rest * (shStore == ShStore::F32 ? 4 : 2), 4));
+  SB_CUDA(cudaMemcpy(positions.get(), cloud.positions, nn * 12, cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(scales.get(), cloud.scales, nn * 12, cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(rotations.get(), cloud.rotations, nn * 16, cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(opacities.get(), cloud.opacities, nn * 4, cudaMemcpyHostToDevice));
+  // SH to planes: DC as FP32, the rest in the chosen storage, rounded to nearest.
+  {
+    const int floats = 3 * shCoeffs;
+    std::vector<float> dc(nn * 3);
+    for (size_t i = 0; i < nn; ++i)
+      for (int c = 0; c < 3; ++c) dc[c * nn + i] = cloud.sh[i * floats + c];
+    SB_CUDA(cudaMemcpy(shDc.get(), dc.data(), nn * 12, cudaMemcpyHostToDevice));
+    if (rest > 0) {
+      std::vector<float> planes(rest);
+      for (size_t i = 0; i < nn; ++i)
+        for (int j = 3; j < floats; ++j) planes[(size_t)(j - 3) * nn + i] = cloud.sh[i * floats + j];
+      if (shStore == ShStore::F32) {
+        SB_CUDA(cudaMemcpy(shRest.get(), planes.data(), rest * 4, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<uint16_t> half(rest);
+        for (size_t k = 0; k < rest; ++k) {
+          if (shStore == ShStore::BF16) {
+            uint32_t bits;
+            std::memcpy(&bits, &planes[k], 4);
+            half[k] = (uint16_t)((bits + 0x7FFFu + ((bits >> 16) & 1u)) >> 16);
+          } else {
+            half[k] = __half_as_ushort(__float2half_rn(planes[k]));
+          }
+        }
+        SB_CUDA(cudaMemcpy(shRest.get(), half.data(), rest * 2, cudaMemcpyHostToDevice));
+      }
+    }
+  }
+  const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, nn * 3 * shCoeffs};
+  for (int g = 0; g < 5; ++g) {
+    const size_t bytes = groupCounts[g] * (stateStore == StateStore::F32 ? 8 : 4);
+    state[g].ensure(bytes);
+    SB_CUDA(cudaMemset(state[g].get(), 0, bytes));
+  }
+  densifyStats.ensure(nn * kStatStride * 4);
+  SB_CUDA(cudaMemset(densifyStats.get(), 0, nn * kStatStride * 4));
+  dViews.ensure(sizeof(ViewSet));
+  dArgs.ensure(sizeof(ChainArgs));
+  dReadback.ensure(sizeof(StepReadback));
+  hViews.ensure(sizeof(ViewSet));
+  hArgs.ensure(sizeof(ChainArgs));
+  hReadback.ensure(sizeof(StepReadback));
+}
+
+Trainer::~Trainer() {
+  if (stream != nullptr) cudaStreamSynchronize(stream);
+  clear_graphs();
+  for (auto &e : events)
+    if (e != nullptr) cudaEventDestroy(e);
+  if (stream != nullptr) cudaStreamDestroy(stream);
+}
+
+void Trainer::clear_graphs() {
+  for (auto &g : graphs)
+    if (g.second.exec != nullptr) cudaGraphExecDestroy(g.second.exec);
+  graphs.clear();
+}
+
+Params Trainer::params() const {
+  Params p;
+  p.positions = positions.get<float>();
+  p.scales = scales.get<float>();
+  p.rotations = rotations.get<float>();
+  p.opacities = opacities.get<float>();
+  p.shDc = shDc.get<float>();
+  p.shRest = shRest.get();
+  p.shStore = shStore;
+  p.n = n;
+  p.shDegree = shDegree;
+  p.shCoeffs = shCoeffs;
+  return p;
+}
+
+OptimState Trainer::optim_state() {
+  OptimState s;
+  for (int g = 0; g < 5; ++g) s.state[g] = state[g].get();
+  s.store = stateStore;
+  return s;
+}
+
+uint64_t Trainer::bytes_per_gaussian() const {
+  const uint64_t rest = 3ull * (shCoeffs - 1) * (shStore == ShStore::F32 ? 4 : 2);
+  const uint64_t floats = 3 + 3 + 4 + 1 + 3ull * shCoeffs;
+  const uint64_t params = (3 + 3 + 4 + 1 + 3) * 4 + rest;
+  const uint64_t optimiser = floats * (stateStore == StateStore::F32 ? 8 : 4);
+  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets 4, raw 64.
+  const uint64_t perView = sizeof(Splat) + 4 + 16 + 4 + kRawStride * 4;
+  return params + optimiser + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
+}
+
+uint64_t Trainer::entry_bytes(uint64_t entries) const {
+  // Keys and values with their copies, plus the sort's look-back words.
+  return entries * ((oneSort ? 16 : 8) + 8) + entries / 16;
+}
+
+uint64_t Trainer::gpu_bytes() const {
+  uint64_t total = bytes_per_gaussian() * n;
+  for (const DeviceBuffer *b : {&image, &stops, &adjoint, &fields, &target, &ranges, &partials, &entryKeys, &entryValues,
+                                &tmpEntryKeys, &tmpEntryValues, &sortScratchDepth, &sortScratchEntries, &scanScratch})
+    total += b->bytes();
+  return total;
+}
+
+// ---------------------------------------------------------------- views
+
+void Trainer::set_views(const splat_camera *cameras, int count) {
+  if (count < 1 || count > kMaxViews) throw Failure{SPLAT_ERR_INVALID, "between 1 and 8 views per step"};
+  ViewSet vs{};
+  vs.count = count;
+  int tileBase = 0;
+  long long pixelBase = 0;
+  for (int k = 0; k < count; ++k) {
+    const splat_camera &c = cameras[k];
+    if (c.width <= 0 || c.height <= 0) throw Failure{SPLAT_ERR_INVALID, "bad image size"};
+    ViewParams &v = vs.v[k];
+    for (int r = 0; r < 3; ++r) {
+      for (int col = 0; col < 3; ++col) v.R[r * 3 + col] = c.view[col * 4 + r];
+      v.T[r] = c.view[12 + r];
+    }
+    for (int a = 0; a < 3; ++a) v.pos[a] = c.position[a];
+    v.nearPlane = opt.near_plane;
+    v.fx = c.fx;
+    v.fy = c.fy;
+    v.cx = c.cx;
+    v.cy = c.cy;
+    v.widthF = (float)c.width;
+    v.heightF = (float)c.height;
+    v.tanX = 0.5f * (float)c.width / c.fx;
+    v.tanY = 0.5f * (float)c.height / c.fy;
+    v.width = c.width;
+    v.height = c.height;
+    v.gridW = (int)div_up((uint32_t)c.width, kTileSize);
+    v.gridH = (int)div_up((uint32_t)c.height, kTileSize);
+    v.tileBase = tileBase;
+    v.tileCount = v.gridW * v.gridH;
+    v.pixelBase = pixelBase;
+    v.perPixel = 1.0f / (3.0f * (float)c.width * (float)c.height);
+    v.fixedScale = 3.0f * (float)c.width * (float)c.height * 64.0f;
+    v.activeDegree = activeDegree;
+    v.activeCoeffs = (activeDegree + 1) * (activeDegree + 1);
+    tileBase += v.tileCount;
+    pixelBase += (long long)c.width * c.height;
+  }
+  // The depth-sorted form sorts entries by as many bits as the tile count needs.
+  if (!oneSort && tileBase > (1 << 24)) throw Failure{SPLAT_ERR_INVALID, "too many tiles for one step"};
+  vs.totalTiles = tileBase;
+  vs.totalPixels = pixelBase;
+  views = vs;
+}
+
+void Trainer::ensure_view_buffers() {
+  const int count = views.count;
+  if (count > viewSlots) {
+    const size_t items = (size_t)n * count;
+    splats.ensure(items * sizeof(Splat));
+    reach.ensure(items * 4);
+    depthKeys.ensure(items * 4);
+    values.ensure(items * 4);
+    tmpKeys.ensure(items * 4);
+    tmpValues.ensure(items * 4);
+    offsets.ensure(items * 4);
+    raw.ensure(items * kRawStride * 4);
+    SB_CUDA(cudaMemset(raw.get(), 0, items * kRawStride * 4));
+    viewSlots = count;
+    clear_graphs();
+  }
+  const size_t pixels = (size_t)views.totalPixels, tiles = (size_t)views.totalTiles;
+  const size_t before = image.bytes() + target.bytes() + ranges.bytes();
+  image.ensure(pixels * 16);
+  stops.ensure(pixels * 4);
+  adjoint.ensure(pixels * 16);
+  fields.ensure(pixels * 36);
+  target.ensure(pixels * 4);
+  ranges.ensure(tiles * 8);
+  partials.ensure(tiles * 8);
+  if (image.bytes() + target.bytes() + ranges.bytes() != before) clear_graphs();
+  const size_t items = (size_t)n * (oneSort ? count : 1);
+  if (scanScratch.bytes() < bin_scan_scratch_bytes((uint32_t)items)) {
+    scanScratch.ensure(bin_scan_scratch_bytes((uint32_t)items));
+    clear_graphs();
+  }
+  if (!oneSort) {
+    const size_t need = sort_scratch_bytes(n, 4, 32, digitBits);
+    if (sortScratchDepth.bytes() < need) {
+      sortScratchDepth.ensure(need);
+      clear_graphs();
+    }
+  }
+}
+
+void Trainer::ensure_entries(uint32_t total) {
+  if (total <= entryCapacity && entryKeys.get() != nullptr) return;
+  const uint64_t others = gpu_bytes() - (entryKeys.bytes() + entryValues.bytes() + tmpEntryKeys.bytes() +
+                                         tmpEntryValues.bytes() + sortScratchEntries.bytes());
+  if (others + entry_bytes(total) > opt.memory_budget) {
+    throw Failure{SPLAT_ERR_BUDGET, std::to_string(total) + " tile entries do not fit the memory budget"};
+  }
+  // Room to grow as splats change, as far as the budget lets it (trainer.cpp:361-364).
+  const uint64_t wanted = (uint64_t)total + total / 2 + 1024;
+  const uint64_t affordable =
+      opt.memory_budget == ~0ull ? wanted : (opt.memory_budget - others) / std::max<uint64_t>(entry_bytes(1), 1);
+  const uint64_t cap = std::max<uint64_t>(std::min(wanted, affordable), total);
+  if (cap > 0xFFFFFFF0ull) throw Failure{SPLAT_ERR_BUDGET, "more tile entries than 32-bit indices hold"};
+  const size_t keyBytes = oneSort ? 8 : 4;
+  entryKeys.release();
+  entryValues.release();
+  tmpEntryKeys.release();
+  tmpEntryValues.release();
+  sortScratchEntries.release();
+  entryKeys.ensure(cap * keyBytes);
+  entryValues.ensure(cap * 4);
+  tmpEntryKeys.ensure(cap * keyBytes);
+  tmpEntryValues.ensure(cap * 4);
+  const uint32_t bits = oneSort ? 32 + bits_for((uint32_t)views.totalTiles) : bits_for((uint32_t)views.totalTiles);
+  sortScratchEntries.ensure(sort_scratch_bytes(cap, (int)keyBytes, std::max<uint32_t>(bits, 32 + 24), digitBits));
+  entryCapacity = (uint32_t)cap;
+  clear_graphs();
+}
+
+void Trainer::upload_targets(const uint8_t *const *targets, const size_t *bytes, int count) {
+  size_t total = 0;
+  for (int k = 0; k < count; ++k) {
+    const size_t want = (size_t)views.v[k].width * views.v[k].height * 4;
+    if (bytes[k] != want || targets[k] == nullptr) throw Failure{SPLAT_ERR_INVALID, "the target image does not match the camera"};
+    total += want;
+  }
+  if (count == 1 && prefetched == targets[0] && prefetchedBytes == bytes[0]) {
+    // Staged during the previous step.
+    swap(staging, stagingNext);
+    prefetched = nullptr;
+  } else {
+    staging.ensure(total);
+    size_t off = 0;
+    for (int k = 0; k < count; ++k) {
+      std::memcpy(staging.get<uint8_t>() + off, targets[k], bytes[k]);
+      off += bytes[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- recording
+
+void Trainer::mark(int stage) {
+  if (timing) SB_CUDA(cudaEventRecord(events[stage], stream));
+}
+
+void Trainer::record_prepare() {
+  const Params p = params();
+  SB_CUDA(cudaMemcpyAsync(dViews.get(), hViews.get(), sizeof(ViewSet), cudaMemcpyHostToDevice, stream));
+  SB_CUDA(cudaMemsetAsync(dReadback.get(), 0, sizeof(StepReadback), stream));
+  StepReadback *rb = dReadback.get<StepReadback>();
+  uint32_t *counters = rb->counters, *error = &rb->error;
+  mark(0);
+  launch_preprocess(p, views, dViews.get<ViewSet>(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
+                    oneSort ? nullptr : values.get<uint32_t>(), stream);
+  mark(1);
+  if (!oneSort) {
+    depthInTmp = sort_pairs_u32(depthKeys.get<uint32_t>(), values.get<uint32_t>(), tmpKeys.get<uint32_t>(),
+                                tmpValues.get<uint32_t>(), n, n, nullptr, 0, 32, digitBits, sortScratchDepth.get(), error,
+                                stream) == 1;
+  }
+  mark(2);
+  const uint32_t *itemKeys = oneSort ? depthKeys.get<uint32_t>() : (depthInTmp ? tmpKeys.get<uint32_t>() : depthKeys.get<uint32_t>());
+  const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
+  const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
+  launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
+                        offsets.get<uint32_t>(), counters, entryCapacity, scanScratch.get(), error, stream);
+}
+
+void Trainer::record_forward() {
+  StepReadback *rb = dReadback.get<StepReadback>();
+  uint32_t *counters = rb->counters, *error = &rb->error;
+  const uint32_t *itemKeys = oneSort ? depthKeys.get<uint32_t>() : (depthInTmp ? tmpKeys.get<uint32_t>() : depthKeys.get<uint32_t>());
+  const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
+  const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
+  mark(3);
+  launch_bin_emit(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
+                  offsets.get<uint32_t>(), entryCapacity, oneSort ? nullptr : entryKeys.get<uint32_t>(),
+                  oneSort ? entryKeys.get<unsigned long long>() : nullptr, entryValues.get<uint32_t>(), error, stream);
+  if (oneSort) {
+    const int bits = 32 + (int)bits_for((uint32_t)views.totalTiles);
+    entriesInTmp = sort_pairs_u64(entryKeys.get<unsigned long long>(), entryValues.get<uint32_t>(),
+                                  tmpEntryKeys.get<unsigned long long>(), tmpEntryValues.get<uint32_t>(), entryCapacity, 0,
+                                  &counters[2], 0, bits, digitBits, sortScratchEntries.get(), error, stream) == 1;
+  } else {
+    const int bits = (int)bits_for((uint32_t)views.totalTiles);
+    entriesInTmp = sort_pairs_u32(entryKeys.get<uint32_t>(), entryValues.get<uint32_t>(), tmpEntryKeys.get<uint32_t>(),
+                                  tmpEntryValues.get<uint32_t>(), entryCapacity, 0, &counters[2], 0, bits, digitBits,
+                                  sortScratchEntries.get(), error, stream) == 1;
+  }
+  SB_CUDA(cudaMemsetAsync(ranges.get(), 0, (size_t)views.totalTiles * 8, stream));
+  const void *keys = entriesInTmp ? tmpEntryKeys.get() : entryKeys.get();
+  launch_tile_ranges(oneSort ? nullptr : static_cast<const uint32_t *>(keys),
+                     oneSort ? static_cast<const unsigned long long *>(keys) : nullptr, &counters[2], entryCapacity,
+                     (uint32_t)views.totalTiles, ranges.get<uint2>(), error, stream);
+  mark(4);
+  RasterConfig cfg;
+  cfg.exactMath = exactMath ? 1 : 0;
+  for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
+  const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
+  launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                 stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
+}
+
+void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
+  StepReadback *rb = dReadback.get<StepReadback>();
+  uint32_t *error = &rb->error;
+  mark(5);
+  launch_ssim(image.get<float4>(), target.get<uint32_t>(), views, dViews.get<ViewSet>(), fields.get<float4>(),
+              partials.get<float2>(), stream);
+  launch_loss(image.get<float4>(), target.get<uint32_t>(), fields.get<float4>(), views, dViews.get<ViewSet>(), opt.lambda_ssim,
+              adjoint.get<float4>(), partials.get<float2>(), stream);
+  launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, stream);
+  mark(6);
+  SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, stream));
+  RasterConfig cfg;
+  cfg.exactMath = exactMath ? 1 : 0;
+  for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
+  const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
+  launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                  adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
+                  stream);
+  mark(7);
+  ChainArgs args{};
+  std::memcpy(&args, hArgs.get(), sizeof(ChainArgs));
+  (void)mode;
+  (void)statistics;
+  SB_CUDA(cudaMemcpyAsync(dArgs.get(), hArgs.get(), sizeof(ChainArgs), cudaMemcpyHostToDevice, stream));
+  OptimState st = optim_state();
+  GradientsOut g{};
+  const GradientsOut *gp = nullptr;
+  if (args.mode == ChainMode::Gradients) {
+    for (int k = 0; k < 5; ++k) g.g[k] = grads[k].get<float>();
+    gp = &g;
+  }
+  launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
+               densifyStats.get<float>(), error, stream);
+}
+
+void Trainer::record_readback() {
+  mark(8);
+  SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+}
+
+void Trainer::fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates) {
+  ChainArgs a{};
+  a.mode = mode;
+  a.statistics = statistics;
+  a.selective = opt.selective_adam != 0;
+  a.fixedPoint = fixedPoint;
+  a.beta1 = 0.9f;
+  a.beta2 = 0.999f;
+  a.epsilon = 1e-15f;
+  a.opacityReg = opt.opacity_reg / (float)n;
+  a.scaleReg = opt.scale_reg / (float)n;
+  if (mode == ChainMode::Step) {
+    ++adamStep;
+    a.rates[0] = rates->position;
+    a.rates[1] = rates->scale;
+    a.rates[2] = rates->rotation;
+    a.rates[3] = rates->opacity;
+    a.rates[4] = rates->sh;
+    a.restScale = rates->sh_rest_scale;
+    a.correction1 = 1.f - std::pow(0.9f, (float)adamStep);
+    a.correction2 = 1.f - std::pow(0.999f, (float)adamStep);
+    a.seed = adamStep;
+  } else if (mode == ChainMode::Gradients) {
+    for (int g = 0; g < 5; ++g) {
+      const size_t counts[5] = {(size_t)n * 3, (size_t)n * 3, (size_t)n * 4, n, (size_t)n * 3 * shCoeffs};
+      if (grads[g].bytes() < counts[g] * 4) {
+        grads[g].ensure(counts[g] * 4);
+        clear_graphs();
+      }
+    }
+  }
+  std::memcpy(hArgs.get(), &a, sizeof(ChainArgs));
+  lastArgs = a;
+}
+
+std::string Trainer::graph_key(ChainMode mode, bool statistics) const {
+  std::string key = std::to_string((int)mode) + (statistics ? "s" : "-") + std::to_string(views.count);
+  for (int k = 0; k < views.count; ++k) key += ":" + std::to_string(views.v[k].width) + "x" + std::to_string(views.v[k].height);
+  return key;
+}
+
+void Trainer::finish_stats(splat_step_stats *stats, int count) {
+  const StepReadback *rb = hReadback.get<StepReadback>();
+  for (int k = 0; k < count; ++k) {
+    splat_step_stats s{};
+    const double perValue = 1.0 / (3.0 * (double)views.v[k].width * views.v[k].height);
+    s.l1 = (float)(rb->totals.l1Sum[k] * perValue);
+    s.ssim = (float)(rb->totals.ssimSum[k] * perValue);
+    s.loss = (1.f - opt.lambda_ssim) * s.l1 + opt.lambda_ssim * (1.f - s.ssim);
+    s.visible_splats = rb->counters[0];
+    s.tile_entries = rb->counters[1];
+    if (stats != nullptr) stats[k] = s;
+  }
+}
+
+void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, const size_t *bytes, int count, ChainMode mode,
+                  const splat_learning_rates *rates, bool statistics, splat_step_stats *stats, bool deviceTargets) {
+  set_views(cameras, count);
+  if (count > 1 && !oneSort) throw Failure{SPLAT_ERR_UNSUPPORTED, "several views per step need sort_form SPLAT_SORT_TILE_DEPTH_64"};
+  ensure_view_buffers();
+  std::memcpy(hViews.get(), &views, sizeof(ViewSet));
+  fill_chain_args(mode, statistics, rates);
+  // The targets reach the device before the step's launches (and outside the graph).
+  if (deviceTargets) {
+    size_t off = 0;
+    for (int k = 0; k < count; ++k) {
+      const size_t want = (size_t)views.v[k].width * views.v[k].height * 4;
+      if (bytes[k] != want || targets[k] == nullptr) throw Failure{SPLAT_ERR_INVALID, "the target image does not match the camera"};
+      SB_CUDA(cudaMemcpyAsync(target.get<uint8_t>() + off, targets[k], want, cudaMemcpyDeviceToDevice, stream));
+      off += want;
+    }
+  } else {
+    upload_targets(targets, bytes, count);
+    SB_CUDA(cudaMemcpyAsync(target.get(), staging.get(), (size_t)views.totalPixels * 4, cudaMemcpyHostToDevice, stream));
+  }
+
+  bool graphDone = false;
+  if (useGraph && entryKeys.get() != nullptr && !timing) {
+    for (int attempt = 0; attempt < 3 && !graphDone; ++attempt) {
+      const std::string key = graph_key(mode, statistics);
+      auto it = graphs.find(key);
+      if (it == graphs.end()) {
+        cudaGraph_t graph = nullptr;
+        SB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          record_prepare();
+          record_forward();
+          record_backward_and_chain(mode, statistics);
+          record_readback();
+        } catch (...) {
+          cudaStreamEndCapture(stream, &graph);
+          if (graph != nullptr) cudaGraphDestroy(graph);
+          throw;
+        }
+        SB_CUDA(cudaStreamEndCapture(stream, &graph));
+        GraphEntry e;
+        const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) throw Failure{SPLAT_ERR_DEVICE, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie)};
+        it = graphs.emplace(key, e).first;
+      }
+      SB_CUDA(cudaGraphLaunch(it->second.exec, stream));
+      SB_CUDA(cudaStreamSynchronize(stream));
+      const StepReadback *rb = hReadback.get<StepReadback>();
+      if ((rb->error & kErrEntryOverflow) != 0u) {
+        // The kernels after the emission skipped their work: grow and run again.
+        ensure_entries(rb->counters[1]);
+        continue;
+      }
+      graphDone = true;
+    }
+    if (!graphDone) throw Failure{SPLAT_ERR_DEVICE, "the entry pool kept overflowing"};
+  } else {
+    record_prepare();
+    // The reference's host wait: read the entry count and size the entry buffers.
+    SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+    SB_CUDA(cudaStreamSynchronize(stream));
+    const uint32_t total = hReadback.get<StepReadback>()->counters[1];
+    if (total > entryCapacity || entryKeys.get() == nullptr) {
+      ensure_entries(total);
+      // The count-and-scan pass wrote the clipped count for the old capacity.
+      const uint32_t fix[2] = {total, total};
+      SB_CUDA(cudaMemcpyAsync(&dReadback.get<StepReadback>()->counters[1], fix, sizeof(fix), cudaMemcpyHostToDevice, stream));
+      uint32_t *err = &dReadback.get<StepReadback>()->error;
+      SB_CUDA(cudaMemsetAsync(err, 0, 4, stream));
+      SB_CUDA(cudaStreamSynchronize(stream));
+    }
+    record_forward();
+    record_backward_and_chain(mode, statistics);
+    record_readback();
+    SB_CUDA(cudaStreamSynchronize(stream));
+  }
+  const StepReadback *rb = hReadback.get<StepReadback>();
+  if (rb->error != 0u) {
+    char msg[96];
+    std::snprintf(msg, sizeof msg, "device check failed (error bits 0x%x)", rb->error);
+    throw Failure{SPLAT_ERR_DEVICE, msg};
+  }
+  if (timing) {
+    for (int s = 0; s < kStages; ++s) {
+      float ms = 0.f;
+      SB_CUDA(cudaEventElapsedTime(&ms, events[s], events[s + 1]));
+      stageTotals[s] += ms;
+    }
+    ++timedIterations;
+  }
+  haveRaw = true;
+  if (mode == ChainMode::Gradients) haveGradients = true;
+  finish_stats(stats, count);
+  for (int k = 0; k < count; ++k) {
+    if (stats != nullptr && !std::isfinite(stats[k].loss)) throw Failure{SPLAT_ERR_NONFINITE, "the loss is not finite"};
+  }
+}
+
+void Trainer::render(const splat_camera *camera, float *out) {
+  set_views(camera, 1);
+  ensure_view_buffers();
+  std::memcpy(hViews.get(), &views, sizeof(ViewSet));
+  record_prepare();
+  SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+  SB_CUDA(cudaStreamSynchronize(stream));
+  const uint32_t total = hReadback.get<StepReadback>()->counters[1];
+  if (total > entryCapacity || entryKeys.get() == nullptr) {
+    ensure_entries(total);
+    const uint32_t fix[2] = {total, total};
+    SB_CUDA(cudaMemcpyAsync(&dReadback.get<StepReadback>()->counters[1], fix, sizeof(fix), cudaMemcpyHostToDevice, stream));
+    SB_CUDA(cudaMemsetAsync(&dReadback.get<StepReadback>()->error, 0, 4, stream));
+  }
+  const bool wasTiming = timing;
+  timing = false;
+  record_forward();
+  timing = wasTiming;
+  record_readback();
+  SB_CUDA(cudaStreamSynchronize(stream));
+  if (hReadback.get<StepReadback>()->error != 0u) throw Failure{SPLAT_ERR_DEVICE, "device check failed during render"};
+  const size_t pixels = (size_t)camera->width * camera->height;
+  SB_CUDA(cudaMemcpy(out, image.get(), pixels * 16, cudaMemcpyDeviceToHost));
+}
+
+// ---------------------------------------------------------------- small kernels
+
+__global__ void k_detmath(const float *in, float *outExp, float *outLog, uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  outExp[i] = splat_expf(in[i]);
+  outLog[i] = in[i] > 0.0f ? splat_logf(in[i]) : 0.0f;
+}
+
+} // namespace sb
+
+// ---------------------------------------------------------------- C ABI
+
+using sb::Failure;
+using sb::Trainer;
+
+struct splat_trainer {
+  Trainer *impl;
+};
+
+namespace {
+
+int fail(int status, const std::string &message) {
+  sb::g_lastError = message;
+  return status;
+}
+
+template <class F> int guarded(F &&f) {
+  try {
+    f();
+    sb::g_lastError.clear();
+    return SPLAT_OK;
+  } catch (const Failure &e) {
+    return fail(e.status, e.message);
+  } catch (const std::bad_alloc &) {
+    return fail(SPLAT_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(SPLAT_ERR_INVALID, e.what());
+  }
+}
+
+Trainer *impl_of(splat_trainer *t) {
+  if (t == nullptr || t->impl == nullptr) throw Failure{SPLAT_ERR_INVALID, "null trainer"};
+  return t->impl;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *splat_last_error(void) { return sb::g_lastError.c_str(); }
+
+void splat_trainer_options_default(splat_trainer_options *o) {
+  if (o == nullptr) return;
+  std::memset(o, 0, sizeof(*o));
+  o->lambda_ssim = 0.2f;
+  o->near_plane = 0.01f;
+  o->selective_adam = 1;
+  o->memory_budget = ~0ull;
+  o->sh_storage = SPLAT_SH_F16;
+  o->state_storage = SPLAT_STATE_BF16_PAIR;
+  o->sort_form = SPLAT_SORT_DEPTH_THEN_TILE;
+  o->exact_math = 1;
+  o->use_graph = 0;
+  o->digit_bits = 8;
+}
+
+void splat_learning_rates_default(splat_learning_rates *r) {
+  if (r == nullptr) return;
+  r->position = 1.6e-4f;
+  r->scale = 0.005f;
+  r->rotation = 0.001f;
+  r->opacity = 0.05f;
+  r->sh = 0.025f;
+  r->sh_rest_scale = 0.05f;
+  r->trust_region = 0.f;
+}
+
+int splat_trainer_create(const splat_cloud *cloud, const splat_trainer_options *options, splat_trainer **out) {
+  return guarded([&] {
+    if (cloud == nullptr || out == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    splat_trainer_options o;
+    if (options != nullptr) o = *options;
+    else splat_trainer_options_default(&o);
+    *out = nullptr;
+    Trainer *t = new Trainer(*cloud, o);
+    *out = new splat_trainer{t};
+  });
+}
+
+int splat_trainer_destroy(splat_trainer *trainer) {
+  return guarded([&] {
+    if (trainer == nullptr) return;
+    delete trainer->impl;
+    delete trainer;
+  });
+}
+
+int splat_trainer_render(splat_trainer *trainer, const splat_camera *camera, float *out_pixels) {
+  return guarded([&] {
+    if (camera == nullptr || out_pixels == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    impl_of(trainer)->render(camera, out_pixels);
+  });
+}
+
+static int run_one(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t bytes,
+                   sb::ChainMode mode, const splat_learning_rates *rates, bool statistics, splat_step_stats *stats) {
+  return guarded([&] {
+    if (camera == nullptr) throw Failure{SPLAT_ERR_INVALID, "null camera"};
+    if (mode == sb::ChainMode::Step && (rates == nullptr || rates->trust_region != 0.f))
+      throw Failure{rates == nullptr ? SPLAT_ERR_INVALID : SPLAT_ERR_UNSUPPORTED, "rates missing, or a trust region (second order)"};
+    const uint8_t *targets[1] = {target};
+    const size_t sizes[1] = {bytes};
+    impl_of(trainer)->run(camera, targets, sizes, 1, mode, rates, statistics, stats);
+  });
+}
+
+int splat_trainer_compute_gradients(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
+                                    size_t target_bytes, splat_step_stats *stats) {
+  return run_one(trainer, camera, target, target_bytes, sb::ChainMode::Gradients, nullptr, true, stats);
+}
+
+int splat_trainer_collect_statistics(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
+                                     size_t target_bytes, splat_step_stats *stats) {
+  return run_one(trainer, camera, target, target_bytes, sb::ChainMode::Statistics, nullptr, true, stats);
+}
+
+int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_rates *rates) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (rates == nullptr) throw Failure{SPLAT_ERR_INVALID, "null rates"};
+    if (rates->trust_region != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
+    if (!t->haveRaw) throw Failure{SPLAT_ERR_STATE, "no gradients: compute_gradients() leaves the sums apply_gradients() uses"};
+    t->fill_chain_args(sb::ChainMode::Step, false, rates);
+    SB_CUDA(cudaMemcpyAsync(t->dArgs.get(), t->hArgs.get(), sizeof(sb::ChainArgs), cudaMemcpyHostToDevice, t->stream));
+    sb::OptimState st = t->optim_state();
+    sb::launch_chain(t->params(), t->views, t->dViews.get<sb::ViewSet>(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
+                     t->dArgs.get<sb::ChainArgs>(), st, nullptr, t->densifyStats.get<float>(), nullptr, t->stream);
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+  });
+}
+
+int splat_trainer_step(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
+                       const splat_learning_rates *rates, const uint8_t *next_target, size_t next_target_bytes,
+                       splat_step_stats *stats) {
+  const int status = run_one(trainer, camera, target, target_bytes, sb::ChainMode::Step, rates, true, stats);
+  if (status == SPLAT_OK && next_target != nullptr) return splat_trainer_prefetch_target(trainer, next_target, next_target_bytes);
+  return status;
+}
+
+int splat_trainer_step_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
+                                     size_t target_bytes, const splat_learning_rates *rates, splat_step_stats *stats) {
+  return guarded([&] {
+    if (camera == nullptr || rates == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    if (rates->trust_region != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
+    const uint8_t *targets[1] = {device_target};
+    const size_t sizes[1] = {target_bytes};
+    impl_of(trainer)->run(camera, targets, sizes, 1, sb::ChainMode::Step, rates, true, stats, true);
+  });
+}
+
+int splat_trainer_stream(splat_trainer *trainer, void **stream) {
+  return guarded([&] {
+    if (stream == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    *stream = impl_of(trainer)->stream;
+  });
+}
+
+int splat_trainer_step_batch(splat_trainer *trainer, const splat_camera *cameras, const uint8_t *const *targets,
+                             int32_t views, const splat_learning_rates *rates, splat_step_stats *stats) {
+  return guarded([&] {
+    if (cameras == nullptr || targets == nullptr || rates == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    if (rates->trust_region != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
+    if (views < 1 || views > sb::kMaxViews) throw Failure{SPLAT_ERR_INVALID, "between 1 and 8 views per step"};
+    size_t sizes[sb::kMaxViews];
+    for (int k = 0; k < views; ++k) sizes[k] = (size_t)cameras[k].width * cameras[k].height * 4;
+    impl_of(trainer)->run(cameras, targets, sizes, views, sb::ChainMode::Step, rates, true, stats);
+  });
+}
+
+int splat_trainer_prefetch_target(splat_trainer *trainer, const uint8_t *target, size_t target_bytes) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null target"};
+    t->stagingNext.ensure(target_bytes);
+    std::memcpy(t->stagingNext.get(), target, target_bytes);
+    t->prefetched = target;
+    t->prefetchedBytes = target_bytes;
+  });
+}
+
+int splat_trainer_get_gradients(splat_trainer *trainer, float *positions, float *scales, float *rotations, float *opacities,
+                                float *sh) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (!t->haveGradients) throw Failure{SPLAT_ERR_STATE, "no gradients: compute_gradients() stores them"};
+    const size_t n = t->n;
+    float *outs[5] = {positions, scales, rotations, opacities, sh};
+    const size_t counts[5] = {n * 3, n * 3, n * 4, n, n * 3 * t->shCoeffs};
+    for (int g = 0; g < 5; ++g)
+      if (outs[g] != nullptr) SB_CUDA(cudaMemcpy(outs[g], t->grads[g].get(), counts[g] * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+int splat_trainer_get_cloud(splat_trainer *trainer, float *positions, float *scales, float *rotations, float *opacities,
+                            float *sh) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    const size_t n = t->n;
+    if (positions) SB_CUDA(cudaMemcpy(positions, t->positions.get(), n * 12, cudaMemcpyDeviceToHost));
+    if (scales) SB_CUDA(cudaMemcpy(scales, t->scales.get(), n * 12, cudaMemcpyDeviceToHost));
+    if (rotations) SB_CUDA(cudaMemcpy(rotations, t->rotations.get(), n * 16, cudaMemcpyDeviceToHost));
+    if (opacities) SB_CUDA(cudaMemcpy(opacities, t->opacities.get(), n * 4, cudaMemcpyDeviceToHost));
+    if (sh) {
+      const int floats = 3 * t->shCoeffs;
+      std::vector<float> dc(n * 3);
+      SB_CUDA(cudaMemcpy(dc.data(), t->shDc.get(), n * 12, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) sh[i * floats + c] = dc[c * n + i];
+      const size_t rest = n * 3 * (t->shCoeffs - 1);
+      if (rest > 0) {
+        std::vector<float> planes(rest);
+        if (t->shStore == sb::ShStore::F32) {
+          SB_CUDA(cudaMemcpy(planes.data(), t->shRest.get(), rest * 4, cudaMemcpyDeviceToHost));
+        } else {
+          std::vector<uint16_t> half(rest);
+          SB_CUDA(cudaMemcpy(half.data(), t->shRest.get(), rest * 2, cudaMemcpyDeviceToHost));
+          for (size_t k = 0; k < rest; ++k) {
+            if (t->shStore == sb::ShStore::BF16) {
+              const uint32_t bits = (uint32_t)half[k] << 16;
+              std::memcpy(&planes[k], &bits, 4);
+            } else {
+              planes[k] = __half2float(__ushort_as_half(half[k]));
+            }
+          }
+        }
+        for (size_t i = 0; i < n; ++i)
+          for (int j = 3; j < floats; ++j) sh[i * floats + j] = planes[(size_t)(j - 3) * n + i];
+      }
+    }
+  });
+}
+
+int splat_trainer_set_active_sh_degree(splat_trainer *trainer, int32_t degree) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    t->activeDegree = std::clamp<int>(degree, 0, t->shDegree);
+  });
+}
+
+int splat_trainer_get_densify_stats(splat_trainer *trainer, float *out) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (out == nullptr) throw Failure{SPLAT_ERR_INVALID, "null output"};
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    SB_CUDA(cudaMemcpy(out, t->densifyStats.get(), (size_t)t->n * sb::kStatStride * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+int splat_trainer_reset_densify_stats(splat_trainer *trainer) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    SB_CUDA(cudaMemsetAsync(t->densifyStats.get(), 0, (size_t)t->n * sb::kStatStride * 4, t->stream));
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+  });
+}
+
+int splat_trainer_reset_opacity(splat_trainer *trainer, float maximum) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    const float limit = std::log(maximum / (1.f - maximum));
+    std::vector<float> values(t->n);
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    SB_CUDA(cudaMemcpy(values.data(), t->opacities.get(), (size_t)t->n * 4, cudaMemcpyDeviceToHost));
+    for (float &v : values) v = std::min(v, limit);
+    SB_CUDA(cudaMemcpy(t->opacities.get(), values.data(), (size_t)t->n * 4, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemset(t->state[3].get(), 0, t->state[3].bytes()));
+  });
+}
+
+int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud, const int32_t *source) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (cloud == nullptr || source == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    if (cloud->count <= 0) throw Failure{SPLAT_ERR_INVALID, "densification removed every Gaussian"};
+    if (cloud->sh_degree != t->shDegree) throw Failure{SPLAT_ERR_INVALID, "the SH degree cannot change"};
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    // The survivors keep their optimiser state: gathered on the host here (the
+    // GPU gather of train_gather.comp is the next component to build).
+    const size_t oldN = t->n, newN = (size_t)cloud->count;
+    const int floats = 3 * t->shCoeffs;
+    const size_t wordBytes = t->stateStore == sb::StateStore::F32 ? 8 : 4;
+    std::vector<std::vector<uint8_t>> moved(5);
+    const size_t strides[5] = {3, 3, 4, 1, (size_t)floats};
+    for (int g = 0; g < 5; ++g) {
+      const size_t oldCount = oldN * strides[g], newCount = newN * strides[g];
+      std::vector<uint8_t> old(oldCount * wordBytes);
+      SB_CUDA(cudaMemcpy(old.data(), t->state[g].get(), old.size(), cudaMemcpyDeviceToHost));
+      moved[g].assign(newCount * wordBytes, 0);
+      for (size_t i = 0; i < newN; ++i) {
+        const int32_t s = source[i];
+        if (s < 0 || (size_t)s >= oldN) continue;
+        for (size_t a = 0; a < strides[g]; ++a) {
+          // State index of element a of Gaussian i: AoS for groups 0-3, planes for SH.
+          const size_t from = g == 4 ? a * oldN + (size_t)s : (size_t)s * strides[g] + a;
+          const size_t to = g == 4 ? a * newN + i : i * strides[g] + a;
+          if (wordBytes == 8) {
+            std::memcpy(&moved[g][to * 4], &old[from * 4], 4);
+            std::memcpy(&moved[g][(newCount + to) * 4], &old[(oldCount + from) * 4], 4);
+          } else {
+            std::memcpy(&moved[g][to * 4], &old[from * 4], 4);
+          }
+        }
+      }
+    }
+    splat_trainer_options o = t->opt;
+    const uint32_t step = t->adamStep;
+    const int active = t->activeDegree;
+    Trainer *fresh = new Trainer(*cloud, o);
+    fresh->adamStep = step;
+    fresh->activeDegree = active;
+    for (int g = 0; g < 5; ++g) SB_CUDA(cudaMemcpy(fresh->state[g].get(), moved[g].data(), moved[g].size(), cudaMemcpyHostToDevice));
+    delete t;
+    trainer->impl = fresh;
+  });
+}
+
+int splat_trainer_info(splat_trainer *trainer, int64_t *gaussians, int32_t *sh_degree, int32_t *active_sh_degree,
+                       int32_t *uses_fixed_point, uint64_t *gpu_bytes, uint64_t *bytes_per_gaussian) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (gaussians) *gaussians = t->n;
+    if (sh_degree) *sh_degree = t->shDegree;
+    if (active_sh_degree) *active_sh_degree = t->activeDegree;
+    if (uses_fixed_point) *uses_fixed_point = t->fixedPoint ? 1 : 0;
+    if (gpu_bytes) *gpu_bytes = t->gpu_bytes();
+    if (bytes_per_gaussian) *bytes_per_gaussian = t->bytes_per_gaussian();
+  });
+}
+
+int splat_trainer_timings(splat_trainer *trainer, const char **names, double *ms, int32_t capacity, int32_t *count) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (count) *count = t->timedIterations > 0 ? sb::kStages : 0;
+    if (t->timedIterations == 0) return;
+    for (int s = 0; s < sb::kStages && s < capacity; ++s) {
+      if (names) names[s] = sb::kStageNames[s];
+      if (ms) ms[s] = t->stageTotals[s] / (double)t->timedIterations;
+    }
+  });
+}
+
+int splat_trainer_set_timing(splat_trainer *trainer, int32_t enabled) {
+  return guarded([&] { impl_of(trainer)->timing = enabled != 0; });
+}
+
+int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint64_t *device_address, uint64_t *bytes) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    const sb::DeviceBuffer *b[6] = {&t->positions, &t->scales, &t->rotations, &t->opacities, &t->shDc, &t->shRest};
+    if (group < 0 || group > 5) throw Failure{SPLAT_ERR_INVALID, "group must be 0..5"};
+    if (device_address) *device_address = (uint64_t)(uintptr_t)b[group]->get();
+    if (bytes) *bytes = b[group]->bytes();
+  });
+}
+
+int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    const size_t items = (size_t)t->n * std::max(t->views.count, 1);
+    const void *src = nullptr;
+    size_t have = 0;
+    sb::StepReadback *rb = t->dReadback.get<sb::StepReadback>();
+    switch (which) {
+    case 0: src = t->splats.get(); have = items * sizeof(sb::Splat); break;
+    case 1: src = t->reach.get(); have = items * 4; break;
+    case 2:
+      if (!t->oneSort) {
+        // The depth sort permuted the keys in place: put them back in Gaussian order.
+        const size_t n = t->n;
+        std::vector<uint32_t> k(n), v(n), g(n);
+        const uint32_t *sk = t->depthInTmp ? t->tmpKeys.get<uint32_t>() : t->depthKeys.get<uint32_t>();
+        const uint32_t *sv = t->depthInTmp ? t->tmpValues.get<uint32_t>() : t->values.get<uint32_t>();
+        SB_CUDA(cudaMemcpy(k.data(), sk, n * 4, cudaMemcpyDeviceToHost));
+        SB_CUDA(cudaMemcpy(v.data(), sv, n * 4, cudaMemcpyDeviceToHost));
+        for (size_t r = 0; r < n; ++r)
+          if (v[r] < n) g[v[r]] = k[r];
+        if (size) *size = n * 4;
+        if (out != nullptr) std::memcpy(out, g.data(), std::min(bytes, n * 4));
+        return;
+      }
+      src = t->depthKeys.get();
+      have = items * 4;
+      break;
+    case 3: src = t->entriesInTmp ? t->tmpEntryKeys.get() : t->entryKeys.get(); have = (size_t)t->hReadback.get<sb::StepReadback>()->counters[2] * (t->oneSort ? 8 : 4); break;
+    case 4: src = t->entriesInTmp ? t->tmpEntryValues.get() : t->entryValues.get(); have = (size_t)t->hReadback.get<sb::StepReadback>()->counters[2] * 4; break;
+    case 5: src = t->ranges.get(); have = (size_t)t->views.totalTiles * 8; break;
+    case 6: src = t->image.get(); have = (size_t)t->views.totalPixels * 16; break;
+    case 7: src = t->stops.get(); have = (size_t)t->views.totalPixels * 4; break;
+    case 8: src = t->adjoint.get(); have = (size_t)t->views.totalPixels * 16; break;
+    case 9: src = t->raw.get(); have = items * sb::kRawStride * 4; break;
+    case 10: src = rb->counters; have = 16; break;
+    case 11: src = t->partials.get(); have = (size_t)t->views.totalTiles * 8; break;
+    case 12: src = &rb->error; have = 4; break;
+    default: throw Failure{SPLAT_ERR_INVALID, "unknown buffer"};
+    }
+    if (size) *size = have;
+    if (out != nullptr && bytes > 0 && src != nullptr) SB_CUDA(cudaMemcpy(out, src, std::min(bytes, have), cudaMemcpyDeviceToHost));
+  });
+}
+
+int splat_radix_sort_u32(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, uint32_t *tmp_values, uint32_t count,
+                         int32_t key_bits, int32_t digit_bits, void *stream) {
+  return guarded([&] {
+    if (key_bits < 1 || key_bits > 32) throw Failure{SPLAT_ERR_INVALID, "key_bits must be 1..32"};
+    const int digits = digit_bits == 0 ? 8 : digit_bits;
+    if (digits < 6 || digits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
+    if (count <= 1) return;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    sb::DeviceBuffer scratch, error;
+    scratch.ensure(sb::sort_scratch_bytes(count, 4, key_bits, digits));
+    error.ensure(4);
+    SB_CUDA(cudaMemsetAsync(error.get(), 0, 4, s));
+    const int where = sb::sort_pairs_u32(keys, values, tmp_keys, tmp_values, count, count, nullptr, 0, key_bits, digits,
+                                         scratch.get(), error.get<uint32_t>(), s);
+    if (where == 1) {
+      SB_CUDA(cudaMemcpyAsync(keys, tmp_keys, (size_t)count * 4, cudaMemcpyDeviceToDevice, s));
+      SB_CUDA(cudaMemcpyAsync(values, tmp_values, (size_t)count * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    uint32_t err = 0;
+    SB_CUDA(cudaMemcpyAsync(&err, error.get(), 4, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (err != 0) throw Failure{SPLAT_ERR_DEVICE, "the sort's look-back gave up waiting"};
+  });
+}
+
+int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, uint32_t *tmp_values, uint32_t count,
+                         int32_t key_bits, int32_t digit_bits, void *stream) {
+  return guarded([&] {
+    if (key_bits < 1 || key_bits > 64) throw Failure{SPLAT_ERR_INVALID, "key_bits must be 1..64"};
+    const int digits = digit_bits == 0 ? 8 : digit_bits;
+    if (digits < 6 || digits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
+    if (count <= 1) return;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    sb::DeviceBuffer scratch, error;
+    scratch.ensure(sb::sort_scratch_bytes(count, 8, key_bits, digits));
+    error.ensure(4);
+    SB_CUDA(cudaMemsetAsync(error.get(), 0, 4, s));
+    auto *k = reinterpret_cast<unsigned long long *>(keys);
+    auto *tk = reinterpret_cast<unsigned long long *>(tmp_keys);
+    const int where = sb::sort_pairs_u64(k, values, tk, tmp_values, count, count, nullptr, 0, key_bits, digits, scratch.get(),
+                                         error.get<uint32_t>(), s);
+    if (where == 1) {
+      SB_CUDA(cudaMemcpyAsync(keys, tmp_keys, (size_t)count * 8, cudaMemcpyDeviceToDevice, s));
+      SB_CUDA(cudaMemcpyAsync(values, tmp_values, (size_t)count * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    uint32_t err = 0;
+    SB_CUDA(cudaMemcpyAsync(&err, error.get(), 4, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (err != 0) throw Failure{SPLAT_ERR_DEVICE, "the sort's look-back gave up waiting"};
+  });
+}
+
+int splat_debug_detmath(const float *in, float *out_exp, float *out_log, uint32_t count) {
+  return guarded([&] {
+    if (count == 0) return;
+    sb::k_detmath<<<sb::div_up(count, 256), 256>>>(in, out_exp, out_log, count);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaDeviceSynchronize());
+  });
+}
+
+} // extern "C"
