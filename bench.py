@@ -276,10 +276,10 @@ def our_arm(args) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    pos, sc, rot, op, sh = make_scene()
+    pos, sc, rot, op, sh = make_scene(args.gaussians)
     cloud = splat.GaussianCloud(DEGREE, pos, sc, rot, op, sh)
-    cams = [splat.Camera(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in hemisphere_views()]
-    host_targets = make_targets()
+    cams = [splat.Camera(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in hemisphere_views()][: args.views]
+    host_targets = make_targets(args.views)
     device_targets = torch.from_numpy(host_targets).cuda()
     rates = splat.LearningRates()
     nbytes = WIDTH * HEIGHT * 4
@@ -289,7 +289,7 @@ def our_arm(args) -> None:
         stream = trainer.stream()
 
         def resident(i):
-            k = i % VIEWS
+            k = i % len(cams)
             return trainer.step_device_target(cams[k], device_targets[k].data_ptr(), rates)
 
         for i in range(args.warmup):
@@ -312,7 +312,7 @@ def our_arm(args) -> None:
     # e2e: the public step() with host targets (H2D of the target and the stats
     # read-back in the timed region).
     stream = trainer.stream()
-    e2e_ms = time_steps(torch, trainer, lambda i: trainer.step(cams[i % VIEWS], host_targets[i % VIEWS], rates),
+    e2e_ms = time_steps(torch, trainer, lambda i: trainer.step(cams[i % len(cams)], host_targets[i % len(cams)], rates),
                         args.steps, stream)
     if dist is not None:
         t = torch.tensor([e2e_ms], device="cuda")
@@ -323,7 +323,7 @@ def our_arm(args) -> None:
     # Per-stage device times (serialising events, plain launches) for the roofline.
     trainer.set_timing(True)
     for i in range(max(3, min(args.steps, 10))):
-        trainer.step_device_target(cams[i % VIEWS], device_targets[i % VIEWS].data_ptr(), rates)
+        trainer.step_device_target(cams[i % len(cams)], device_targets[i % len(cams)].data_ptr(), rates)
     stages = dict(trainer.timings())
     trainer.set_timing(False)
     entries, visible = stats.tile_entries, stats.visible_splats
@@ -341,8 +341,8 @@ def our_arm(args) -> None:
     algorithmic = {
         "backward": 52.0 * entries + 36.0 * pixels + 56.0 * visible,
         "composite": 52.0 * entries + 20.0 * pixels,
-        "project": 288.0 * GAUSSIANS,
-        "chain rule and step": 528.0 * GAUSSIANS,
+        "project": 288.0 * args.gaussians,
+        "chain rule and step": 528.0 * args.gaussians,
     }
     roof = None
     if dominant is not None:
@@ -412,6 +412,10 @@ def main() -> None:
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
+    parser.add_argument("--views", type=int, default=VIEWS,
+                        help="cameras cycled through (default 64; fewer keep ncu captures small)")
+    parser.add_argument("--gaussians", type=int, default=GAUSSIANS,
+                        help="scene size (default 1M, the headline workload; smaller cases are for ncu captures)")
     args = parser.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -101,8 +101,9 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
                      const RasterConfig &cfg, const float4 *image, const float4 *adjoint, const uint32_t *stops,
                      bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream);
 
-// train_gradient.comp + train_sh_step.comp, fused: the chain rule from the raw
-// sums of every view, then (mode) gradients stored, or Adam's step.
+// train_gradient.comp + train_sh_step.comp: the chain rule from the raw sums of
+// every view, then (mode) gradients stored, or Adam's step. shGrad holds 2
+// float4 per (view, Gaussian) between the two kernels.
 enum class ChainMode : int { Statistics = 0, Gradients = 1, Step = 2 };
 struct ChainArgs {
   ChainMode mode;
@@ -123,8 +124,7 @@ struct GradientsOut {
   float *g[5];         // positions, scales, rotations, opacities, sh (GaussianCloud layout)
 };
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
-                  const ChainArgs *dArgs,
-                  OptimState &state, const GradientsOut *grads, float *densifyStats, const uint32_t *error,
-                  cudaStream_t stream);
+                  const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad,
+                  float *densifyStats, const uint32_t *error, cudaStream_t stream);
 
 } // namespace sb

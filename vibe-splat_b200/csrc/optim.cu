@@ -109,217 +109,276 @@ __device__ __forceinline__ void store_sh_rest(void *p, size_t idx, float value, 
   }
 }
 
-template <ShStore S, bool FIXED>
-__global__ void __launch_bounds__(128) k_chain(Params p, const ViewSet *__restrict__ viewsPtr, const void *__restrict__ rawIn,
-                                               const Splat *__restrict__ splats, const ChainArgs *__restrict__ argsPtr, OptimState state,
-                                               GradientsOut grads, bool storeGradients, float *__restrict__ densifyStats,
-                                               const uint32_t *error) {
+// One SH basis function and its gradient, for a coefficient index the caller
+// unrolls (so the switch folds away). Formulas as sh_basis / sh_basis_gradient.
+__device__ __forceinline__ float basis_one(int k, float x, float y, float z) {
+  switch (k) {
+  case 0: return 0.28209479177387814f;
+  case 1: return -0.4886025119029199f * y;
+  case 2: return 0.4886025119029199f * z;
+  case 3: return -0.4886025119029199f * x;
+  case 4: return 1.0925484305920792f * x * y;
+  case 5: return -1.0925484305920792f * y * z;
+  case 6: return 0.31539156525252005f * (2.0f * (z * z) - x * x - y * y);
+  case 7: return -1.0925484305920792f * x * z;
+  case 8: return 0.5462742152960396f * (x * x - y * y);
+  case 9: return -0.5900435899266435f * y * (3.0f * (x * x) - y * y);
+  case 10: return 2.890611442640554f * x * y * z;
+  case 11: return -0.4570457994644658f * y * (4.0f * (z * z) - x * x - y * y);
+  case 12: return 0.3731763325901154f * z * (2.0f * (z * z) - 3.0f * (x * x) - 3.0f * (y * y));
+  case 13: return -0.4570457994644658f * x * (4.0f * (z * z) - x * x - y * y);
+  case 14: return 1.445305721320277f * z * (x * x - y * y);
+  default: return -0.5900435899266435f * x * (x * x - 3.0f * (y * y));
+  }
+}
+
+__device__ __forceinline__ void basis_gradient_one(int k, float x, float y, float z, float g[3]) {
+  const float C1 = 0.4886025119029199f, A = 1.0925484305920792f, K = 0.31539156525252005f, L = 0.5462742152960396f;
+  const float C = -0.5900435899266435f, E = 2.890611442640554f, F = -0.4570457994644658f, G = 0.3731763325901154f,
+              H = 1.445305721320277f;
+  const float xx = x * x, yy = y * y, zz = z * z;
+  switch (k) {
+  case 1: g[0] = 0.f; g[1] = -C1; g[2] = 0.f; break;
+  case 2: g[0] = 0.f; g[1] = 0.f; g[2] = C1; break;
+  case 3: g[0] = -C1; g[1] = 0.f; g[2] = 0.f; break;
+  case 4: g[0] = A * y; g[1] = A * x; g[2] = 0.f; break;
+  case 5: g[0] = -A * 0.f; g[1] = -A * z; g[2] = -A * y; break;
+  case 6: g[0] = K * (-2.0f * x); g[1] = K * (-2.0f * y); g[2] = K * (4.0f * z); break;
+  case 7: g[0] = -A * z; g[1] = -A * 0.f; g[2] = -A * x; break;
+  case 8: g[0] = L * (2.0f * x); g[1] = L * (-2.0f * y); g[2] = 0.f; break;
+  case 9: g[0] = C * (6.0f * x * y); g[1] = C * (3.0f * xx - 3.0f * yy); g[2] = 0.f; break;
+  case 10: g[0] = E * (y * z); g[1] = E * (x * z); g[2] = E * (x * y); break;
+  case 11: g[0] = F * (-2.0f * x * y); g[1] = F * (4.0f * zz - xx - 3.0f * yy); g[2] = F * (8.0f * y * z); break;
+  case 12: g[0] = G * (-6.0f * x * z); g[1] = G * (-6.0f * y * z); g[2] = G * (6.0f * zz - 3.0f * xx - 3.0f * yy); break;
+  case 13: g[0] = F * (4.0f * zz - 3.0f * xx - yy); g[1] = F * (-2.0f * x * y); g[2] = F * (8.0f * x * z); break;
+  case 14: g[0] = H * (2.0f * x * z); g[1] = H * (-2.0f * y * z); g[2] = H * (xx - yy); break;
+  case 15: g[0] = C * (3.0f * xx - 3.0f * yy); g[1] = C * (-6.0f * x * y); g[2] = 0.f; break;
+  default: g[0] = g[1] = g[2] = 0.f; break;
+  }
+}
+
+// The chain rule of one view for Gaussian i (train_gradient.comp:165-275):
+// adds its position, scale, rotation and opacity gradients, and returns the
+// colour gradient where the colour was not clamped and the view direction.
+template <ShStore S>
+__device__ __forceinline__ void chain_view(const Params &p, uint32_t i, const ViewParams &cam, const float raw[kRawPerSplat],
+                                           const float4 col, const float pos[3], const float logScale[3], float opacity,
+                                           float4 rq, float gP[3], float gScale[3], float gRot[4], float &gOpacity,
+                                           float gColour[3], float dir[3]) {
+  const float px = pos[0], py = pos[1], pz = pos[2];
+  const float quatLength = sqrtf(fmaf(rq.w, rq.w, fmaf(rq.z, rq.z, fmaf(rq.y, rq.y, rq.x * rq.x))));
+  float q[4] = {1.f, 0.f, 0.f, 0.f};
+  if (quatLength > 0.0f) {
+    q[0] = rq.x / quatLength;
+    q[1] = rq.y / quatLength;
+    q[2] = rq.z / quatLength;
+    q[3] = rq.w / quatLength;
+  }
+  const float t[3] = {fmaf(cam.R[2], pz, fmaf(cam.R[1], py, fmaf(cam.R[0], px, cam.T[0]))),
+                      fmaf(cam.R[5], pz, fmaf(cam.R[4], py, fmaf(cam.R[3], px, cam.T[1]))),
+                      fmaf(cam.R[8], pz, fmaf(cam.R[7], py, fmaf(cam.R[6], px, cam.T[2])))};
+  const float fx = cam.fx, fy = cam.fy;
+  const float z = t[2], iz = 1.0f / z, iz2 = iz * iz;
+  const float G[2][2] = {{raw[3], raw[4]}, {raw[4], raw[5]}};
+  float Rv[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Rv[r][c] = cam.R[r * 3 + c];
+  float R[3][3];
+  quat_to_matrix(q[0], q[1], q[2], q[3], R);
+  const float s2[3] = {splat_expf(2.0f * logScale[0]), splat_expf(2.0f * logScale[1]), splat_expf(2.0f * logScale[2])};
+  float sigma[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      sigma[r][c] = fmaf(R[r][2] * s2[2], R[c][2], fmaf(R[r][1] * s2[1], R[c][1], R[r][0] * s2[0] * R[c][0]));
+  float X[3][3];
+  {
+    float RS[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) RS[r][c] = fmaf(Rv[r][2], sigma[2][c], fmaf(Rv[r][1], sigma[1][c], Rv[r][0] * sigma[0][c]));
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) X[r][c] = fmaf(RS[r][2], Rv[c][2], fmaf(RS[r][1], Rv[c][1], RS[r][0] * Rv[c][0]));
+  }
+  const float limX = 1.3f * cam.tanX, limY = 1.3f * cam.tanY;
+  const float rx = t[0] * iz, ry = t[1] * iz;
+  const bool clampedX = fabsf(rx) > limX, clampedY = fabsf(ry) > limY;
+  const float tx = fminf(fmaxf(rx, -limX), limX) * z, ty = fminf(fmaxf(ry, -limY), limY) * z;
+  const float J[2][3] = {{fx * iz, 0.f, -fx * tx * iz2}, {0.f, fy * iz, -fy * ty * iz2}};
+  const float Jc[2][3] = {{fx * iz, 0.f, -fx * t[0] * iz2}, {0.f, fy * iz, -fy * t[1] * iz2}};
+  float gT[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) gT[k] = fmaf(Jc[1][k], raw[2], Jc[0][k] * raw[1]);
+  const float dJx[2][3] = {{0.f, 0.f, clampedX ? 0.0f : -fx * iz2}, {0.f, 0.f, 0.f}};
+  const float dJy[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, clampedY ? 0.0f : -fy * iz2}};
+  const float dJz[2][3] = {{-fx * iz2, 0.f, clampedX ? fx * tx * iz2 * iz : 2.0f * fx * tx * iz2 * iz},
+                           {0.f, -fy * iz2, clampedY ? fy * ty * iz2 * iz : 2.0f * fy * ty * iz2 * iz}};
+  gT[0] += 2.0f * trace_term(G, dJx, X, J);
+  gT[1] += 2.0f * trace_term(G, dJy, X, J);
+  gT[2] += 2.0f * trace_term(G, dJz, X, J);
+  float gPv[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) gPv[c] = fmaf(Rv[2][c], gT[2], fmaf(Rv[1][c], gT[1], Rv[0][c] * gT[0]));
+
+  // T2 = J Rv (2x3), G3 = T2^T G T2.
+  float T2[2][3];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) T2[r][c] = fmaf(J[r][2], Rv[2][c], fmaf(J[r][1], Rv[1][c], J[r][0] * Rv[0][c]));
+  float G3[3][3];
+  {
+    float GT[2][3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) GT[r][c] = fmaf(G[r][1], T2[1][c], G[r][0] * T2[0][c]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) G3[a][b] = fmaf(T2[1][a], GT[1][b], T2[0][a] * GT[0][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float ax[3] = {R[0][a], R[1][a], R[2][a]};
+    float Ga[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) Ga[r] = fmaf(G3[r][2], ax[2], fmaf(G3[r][1], ax[1], G3[r][0] * ax[0]));
+    gScale[a] += 2.0f * s2[a] * fmaf(ax[2], Ga[2], fmaf(ax[1], Ga[1], ax[0] * Ga[0]));
+  }
+  // Rotation: P = 2 G3 R D, gq_k = <P, dR/dq_k> (the GLSL column constructors, transposed to rows).
+  float P[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) P[r][c] = 2.0f * fmaf(G3[r][2], R[2][c], fmaf(G3[r][1], R[1][c], G3[r][0] * R[0][c])) * s2[c];
+  const float w = q[0], x = q[1], y = q[2], zq = q[3];
+  const float gq[4] = {
+      2.0f * (-P[0][1] * zq + P[0][2] * y + P[1][0] * zq - P[1][2] * x - P[2][0] * y + P[2][1] * x),
+      2.0f * (P[0][1] * y + P[0][2] * zq + P[1][0] * y - 2.0f * P[1][1] * x - P[1][2] * w + P[2][0] * zq + P[2][1] * w -
+              2.0f * P[2][2] * x),
+      2.0f * (-2.0f * P[0][0] * y + P[0][1] * x + P[0][2] * w + P[1][0] * x + P[1][2] * zq - P[2][0] * w + P[2][1] * zq -
+              2.0f * P[2][2] * y),
+      2.0f * (-2.0f * P[0][0] * zq - P[0][1] * w + P[0][2] * x + P[1][0] * w - 2.0f * P[1][1] * zq + P[1][2] * y +
+              P[2][0] * x + P[2][1] * y)};
+  const float qg = fmaf(q[3], gq[3], fmaf(q[2], gq[2], fmaf(q[1], gq[1], q[0] * gq[0])));
+  const float inv = fmaxf(quatLength, 1e-12f);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) gRot[k] += (gq[k] - q[k] * qg) / inv;
+  gOpacity += raw[0] * opacity * (1.0f - opacity);
+
+  // Colour: the gradient reaches the coefficients in use where the colour was
+  // not clamped at zero (the splat keeps the clamped colour).
+  gColour[0] = col.x > 0.0f ? raw[6] : 0.0f;
+  gColour[1] = col.y > 0.0f ? raw[7] : 0.0f;
+  gColour[2] = col.z > 0.0f ? raw[8] : 0.0f;
+  const float ddx = px - cam.pos[0], ddy = py - cam.pos[1], ddz = pz - cam.pos[2];
+  const float distance = sqrtf(fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx)));
+  dir[0] = ddx / distance;
+  dir[1] = ddy / distance;
+  dir[2] = ddz / distance;
+  // Position also changes the view direction, and with it the colour.
+  if (cam.activeDegree > 0) {
+    float gDir[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 1; k < kMaxCoeffs; ++k) {
+      if (k < cam.activeCoeffs) {
+        const float c0 = sh_coefficient<S>(p, i, k, 0), c1 = sh_coefficient<S>(p, i, k, 1), c2 = sh_coefficient<S>(p, i, k, 2);
+        const float d = fmaf(gColour[2], c2, fmaf(gColour[1], c1, gColour[0] * c0));
+        float bg[3];
+        basis_gradient_one(k, dir[0], dir[1], dir[2], bg);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) gDir[c] = fmaf(d, bg[c], gDir[c]);
+      }
+    }
+    const float dd = fmaf(dir[2], gDir[2], fmaf(dir[1], gDir[1], dir[0] * gDir[0]));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gPv[c] += (gDir[c] - dir[c] * dd) / distance;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
+}
+
+// Geometry part of the chain rule and Adam for positions, scales, rotations
+// and opacities (train_gradient.comp:105-315), one thread per Gaussian. For the
+// SH step that follows it leaves, per view, the colour gradient where the colour
+// was not clamped and the number of coefficients in use (0: the view did not
+// reach the Gaussian), then the view direction: shGrad[(v n + i) * 2 + {0, 1}],
+// as the reference leaves them in its sums for train_sh_step.comp.
+template <ShStore S, bool FIXED, bool MULTI>
+__global__ void __launch_bounds__(128, 4) k_chain(Params p, const ViewSet *__restrict__ viewsPtr, const void *__restrict__ rawIn,
+                                                  const Splat *__restrict__ splats, const ChainArgs *__restrict__ argsPtr,
+                                                  OptimState state, GradientsOut grads, bool storeGradients,
+                                                  float4 *__restrict__ shGrad, float *__restrict__ densifyStats,
+                                                  const uint32_t *error) {
   const ViewSet &views = *viewsPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.n) return;
   const ChainArgs args = *argsPtr;
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
   const size_t n = p.n;
-  const int shFloats = 3 * p.shCoeffs;
   const bool zeros = args.mode == ChainMode::Gradients || (args.mode == ChainMode::Step && !args.selective);
   const bool penalties = args.opacityReg > 0.0f || args.scaleReg > 0.0f;
 
-  // Accumulated over views.
   float gP[3] = {0.f, 0.f, 0.f}, gScale[3] = {0.f, 0.f, 0.f}, gRot[4] = {0.f, 0.f, 0.f, 0.f}, gOpacity = 0.f;
-  float gSh[kMaxCoeffs][3];
-#pragma unroll
-  for (int k = 0; k < kMaxCoeffs; ++k) gSh[k][0] = gSh[k][1] = gSh[k][2] = 0.f;
   bool anyTouched = false;
-  int activeCoeffs = 0;
-
+  const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
   const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
   const float opacity = 1.0f / (1.0f + splat_expf(-p.opacities[i]));
+  const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
 
-  for (int v = 0; v < views.count; ++v) {
+  const int viewCount = MULTI ? views.count : 1;
+  for (int v = 0; v < viewCount; ++v) {
     const ViewParams &cam = views.v[v];
-    const size_t at = ((size_t)v * n + i) * kRawStride;
+    const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + ((size_t)v * n + i) * (kRawStride / 4);
+    uint32_t words[16];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4 w4 = r4[q];
+      words[q * 4] = w4.x;
+      words[q * 4 + 1] = w4.y;
+      words[q * 4 + 2] = w4.z;
+      words[q * 4 + 3] = w4.w;
+    }
     float raw[kRawPerSplat];
     bool touched = false;
 #pragma unroll
     for (int k = 0; k < kRawPerSplat; ++k) {
-      if (FIXED) {
-        const int q = static_cast<const int *>(rawIn)[at + k];
-        raw[k] = (float)q / cam.fixedScale;
-        touched = touched || q != 0;
-      } else {
-        raw[k] = static_cast<const float *>(rawIn)[at + k];
-        touched = touched || raw[k] != 0.0f;
-      }
+      raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
+      touched = touched || raw[k] != 0.0f;
     }
-    if (!touched) continue;
+    float4 *sg = shGrad + ((size_t)v * n + i) * 2;
+    if (!touched || args.mode == ChainMode::Statistics) {
+      if (args.mode != ChainMode::Statistics) sg[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (!touched) continue;
+    }
     anyTouched = true;
+    const float4 col = splats[(size_t)v * n + i].colorRadius;
     if (args.statistics) {
-      float *st = densifyStats + (size_t)i * kStatStride;
+      float4 *st = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
+      float4 a = st[0], b = st[1];
       const float hx = 0.5f * cam.widthF, hy = 0.5f * cam.heightF;
       const float ax = raw[1] * hx, ay = raw[2] * hy;
-      st[0] += sqrtf(fmaf(ay, ay, ax * ax));
-      st[1] += 1.0f;
-      st[2] = fmaxf(st[2], splats[(size_t)v * n + i].colorRadius.w);
-      st[3] += raw[9] * 3.0f * cam.widthF * cam.heightF;
+      a.x += sqrtf(fmaf(ay, ay, ax * ax));
+      a.y += 1.0f;
+      a.z = fmaxf(a.z, col.w);
+      a.w += raw[9] * 3.0f * cam.widthF * cam.heightF;
       const float bx = raw[10] * hx, by = raw[11] * hy;
-      st[4] += sqrtf(fmaf(by, by, bx * bx));
+      b.x += sqrtf(fmaf(by, by, bx * bx));
+      st[0] = a;
+      st[1] = b;
     }
     if (args.mode == ChainMode::Statistics) continue;
-
-    const float px = p.positions[i * 3], py = p.positions[i * 3 + 1], pz = p.positions[i * 3 + 2];
-    const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
-    const float quatLength = sqrtf(fmaf(rq.w, rq.w, fmaf(rq.z, rq.z, fmaf(rq.y, rq.y, rq.x * rq.x))));
-    float q[4] = {1.f, 0.f, 0.f, 0.f};
-    if (quatLength > 0.0f) {
-      q[0] = rq.x / quatLength;
-      q[1] = rq.y / quatLength;
-      q[2] = rq.z / quatLength;
-      q[3] = rq.w / quatLength;
-    }
-    const float t[3] = {fmaf(cam.R[2], pz, fmaf(cam.R[1], py, fmaf(cam.R[0], px, cam.T[0]))),
-                        fmaf(cam.R[5], pz, fmaf(cam.R[4], py, fmaf(cam.R[3], px, cam.T[1]))),
-                        fmaf(cam.R[8], pz, fmaf(cam.R[7], py, fmaf(cam.R[6], px, cam.T[2])))};
-    const float fx = cam.fx, fy = cam.fy;
-    const float z = t[2], iz = 1.0f / z, iz2 = iz * iz;
-    const float gCentre[2] = {raw[1], raw[2]};
-    const float G[2][2] = {{raw[3], raw[4]}, {raw[4], raw[5]}};
-
-    float Rv[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) Rv[r][c] = cam.R[r * 3 + c];
-    float R[3][3];
-    quat_to_matrix(q[0], q[1], q[2], q[3], R);
-    const float s2[3] = {splat_expf(2.0f * logScale[0]), splat_expf(2.0f * logScale[1]), splat_expf(2.0f * logScale[2])};
-    // sigma = R D R^T, X = Rv sigma Rv^T.
-    float sigma[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        sigma[r][c] = fmaf(R[r][2] * s2[2], R[c][2], fmaf(R[r][1] * s2[1], R[c][1], R[r][0] * s2[0] * R[c][0]));
-    float RS[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) RS[r][c] = fmaf(Rv[r][2], sigma[2][c], fmaf(Rv[r][1], sigma[1][c], Rv[r][0] * sigma[0][c]));
-    float X[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) X[r][c] = fmaf(RS[r][2], Rv[c][2], fmaf(RS[r][1], Rv[c][1], RS[r][0] * Rv[c][0]));
-
-    const float limX = 1.3f * cam.tanX, limY = 1.3f * cam.tanY;
-    const float rx = t[0] * iz, ry = t[1] * iz;
-    const bool clampedX = fabsf(rx) > limX, clampedY = fabsf(ry) > limY;
-    const float tx = fminf(fmaxf(rx, -limX), limX) * z, ty = fminf(fmaxf(ry, -limY), limY) * z;
-    const float J[2][3] = {{fx * iz, 0.f, -fx * tx * iz2}, {0.f, fy * iz, -fy * ty * iz2}};
-    const float Jc[2][3] = {{fx * iz, 0.f, -fx * t[0] * iz2}, {0.f, fy * iz, -fy * t[1] * iz2}};
-    float gT[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) gT[k] = fmaf(Jc[1][k], gCentre[1], Jc[0][k] * gCentre[0]);
-    const float dJx[2][3] = {{0.f, 0.f, clampedX ? 0.0f : -fx * iz2}, {0.f, 0.f, 0.f}};
-    const float dJy[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, clampedY ? 0.0f : -fy * iz2}};
-    const float dJz[2][3] = {{-fx * iz2, 0.f, clampedX ? fx * tx * iz2 * iz : 2.0f * fx * tx * iz2 * iz},
-                             {0.f, -fy * iz2, clampedY ? fy * ty * iz2 * iz : 2.0f * fy * ty * iz2 * iz}};
-    gT[0] += 2.0f * trace_term(G, dJx, X, J);
-    gT[1] += 2.0f * trace_term(G, dJy, X, J);
-    gT[2] += 2.0f * trace_term(G, dJz, X, J);
-    float gPv[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gPv[c] = fmaf(Rv[2][c], gT[2], fmaf(Rv[1][c], gT[1], Rv[0][c] * gT[0]));
-
-    // T2 = J Rv (2x3), G3 = T2^T G T2.
-    float T2[2][3];
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) T2[r][c] = fmaf(J[r][2], Rv[2][c], fmaf(J[r][1], Rv[1][c], J[r][0] * Rv[0][c]));
-    float GT[2][3];
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) GT[r][c] = fmaf(G[r][1], T2[1][c], G[r][0] * T2[0][c]);
-    float G3[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) G3[a][b] = fmaf(T2[1][a], GT[1][b], T2[0][a] * GT[0][b]);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float ax[3] = {R[0][a], R[1][a], R[2][a]};
-      float Ga[3];
-#pragma unroll
-      for (int r = 0; r < 3; ++r) Ga[r] = fmaf(G3[r][2], ax[2], fmaf(G3[r][1], ax[1], G3[r][0] * ax[0]));
-      gScale[a] += 2.0f * s2[a] * fmaf(ax[2], Ga[2], fmaf(ax[1], Ga[1], ax[0] * Ga[0]));
-    }
-    // Rotation: P = 2 G3 R D, gq_k = <P, dR/dq_k>.
-    float P[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) P[r][c] = 2.0f * fmaf(G3[r][2], R[2][c], fmaf(G3[r][1], R[1][c], G3[r][0] * R[0][c])) * s2[c];
-    const float w = q[0], x = q[1], y = q[2], zq = q[3];
-    // dR/dq as rows (transposed from the GLSL column constructors).
-    const float dR[4][3][3] = {
-        {{0.f, -2.0f * zq, 2.0f * y}, {2.0f * zq, 0.f, -2.0f * x}, {-2.0f * y, 2.0f * x, 0.f}},
-        {{0.f, 2.0f * y, 2.0f * zq}, {2.0f * y, -4.0f * x, -2.0f * w}, {2.0f * zq, 2.0f * w, -4.0f * x}},
-        {{-4.0f * y, 2.0f * x, 2.0f * w}, {2.0f * x, 0.f, 2.0f * zq}, {-2.0f * w, 2.0f * zq, -4.0f * y}},
-        {{-4.0f * zq, -2.0f * w, 2.0f * x}, {2.0f * w, -4.0f * zq, 2.0f * y}, {2.0f * x, 2.0f * y, 0.f}}};
-    float gq[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      float acc = 0.0f;
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int r = 0; r < 3; ++r) acc = fmaf(P[r][c], dR[k][r][c], acc);
-      gq[k] = acc;
-    }
-    const float qg = fmaf(q[3], gq[3], fmaf(q[2], gq[2], fmaf(q[1], gq[1], q[0] * gq[0])));
-    const float inv = fmaxf(quatLength, 1e-12f);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) gRot[k] += (gq[k] - q[k] * qg) / inv;
-    gOpacity += raw[0] * opacity * (1.0f - opacity);
-
-    // Colour: the gradient reaches the coefficients in use where the colour
-    // was not clamped at zero (the splat keeps the clamped colour).
-    const float4 col = splats[(size_t)v * n + i].colorRadius;
-    const float gColour[3] = {col.x > 0.0f ? raw[6] : 0.0f, col.y > 0.0f ? raw[7] : 0.0f, col.z > 0.0f ? raw[8] : 0.0f};
-    const float ddx = px - cam.pos[0], ddy = py - cam.pos[1], ddz = pz - cam.pos[2];
-    const float distance = sqrtf(fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx)));
-    const float dir[3] = {ddx / distance, ddy / distance, ddz / distance};
-    float basis[16];
-    sh_basis(dir[0], dir[1], dir[2], cam.activeDegree, basis);
-    activeCoeffs = max(activeCoeffs, cam.activeCoeffs);
-#pragma unroll
-    for (int k = 0; k < kMaxCoeffs; ++k) {
-      if (k < cam.activeCoeffs) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) gSh[k][c] += basis[k] * gColour[c];
-      }
-    }
-    // Position also changes the view direction, and with it the colour.
-    if (cam.activeDegree > 0) {
-      float bg[16][3];
-      sh_basis_gradient(dir[0], dir[1], dir[2], cam.activeDegree, bg);
-      float gDir[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-      for (int k = 1; k < kMaxCoeffs; ++k) {
-        if (k < cam.activeCoeffs) {
-          const float c0 = sh_coefficient<S>(p, i, k, 0), c1 = sh_coefficient<S>(p, i, k, 1), c2 = sh_coefficient<S>(p, i, k, 2);
-          const float d = fmaf(gColour[2], c2, fmaf(gColour[1], c1, gColour[0] * c0));
-#pragma unroll
-          for (int c = 0; c < 3; ++c) gDir[c] = fmaf(d, bg[k][c], gDir[c]);
-        }
-      }
-      const float dd = fmaf(dir[2], gDir[2], fmaf(dir[1], gDir[1], dir[0] * gDir[0]));
-#pragma unroll
-      for (int c = 0; c < 3; ++c) gPv[c] += (gDir[c] - dir[c] * dd) / distance;
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
+    float gColour[3], dir[3];
+    chain_view<S>(p, i, cam, raw, col, pos, logScale, opacity, rq, gP, gScale, gRot, gOpacity, gColour, dir);
+    sg[0] = make_float4(gColour[0], gColour[1], gColour[2], __uint_as_float((uint32_t)cam.activeCoeffs));
+    sg[1] = make_float4(dir[0], dir[1], dir[2], 0.0f);
   }
 
   if (args.mode == ChainMode::Statistics) return;
@@ -330,7 +389,6 @@ __global__ void __launch_bounds__(128) k_chain(Params p, const ViewSet *__restri
     for (int a = 0; a < 3; ++a) gScale[a] += args.scaleReg * splat_expf(logScale[a]);
     gOpacity += args.opacityReg * opacity * (1.0f - opacity);
   }
-
   if (storeGradients) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -340,32 +398,29 @@ __global__ void __launch_bounds__(128) k_chain(Params p, const ViewSet *__restri
 #pragma unroll
     for (int a = 0; a < 4; ++a) grads.g[2][i * 4 + a] = gRot[a];
     grads.g[3][i] = gOpacity;
-    for (int k = 0; k < p.shCoeffs; ++k)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) grads.g[4][(size_t)i * shFloats + k * 3 + c] = k < kMaxCoeffs ? gSh[k][c] : 0.0f;
     return;
   }
-
   // Adam. A parameter with a zero gradient is left alone when selective.
   const AdamArgs a{args.beta1, args.beta2, args.epsilon, args.correction1, args.correction2, args.seed};
   const bool stepZeros = !args.selective;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (gP[c] != 0.0f || stepZeros) {
-      float value = p.positions[i * 3 + c];
+      float value = pos[c];
       step_state(value, state.state[0], state.store, n * 3, i * 3 + c, gP[c], args.rates[0], a, (i * 3 + c) * 5u + 0u);
       p.positions[i * 3 + c] = value;
     }
     if (gScale[c] != 0.0f || stepZeros) {
-      float value = p.scales[i * 3 + c];
+      float value = logScale[c];
       step_state(value, state.state[1], state.store, n * 3, i * 3 + c, gScale[c], args.rates[1], a, (i * 3 + c) * 5u + 1u);
       p.scales[i * 3 + c] = value;
     }
   }
+  const float rv[4] = {rq.x, rq.y, rq.z, rq.w};
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     if (gRot[c] != 0.0f || stepZeros) {
-      float value = p.rotations[i * 4 + c];
+      float value = rv[c];
       step_state(value, state.state[2], state.store, n * 4, i * 4 + c, gRot[c], args.rates[2], a, (i * 4 + c) * 5u + 2u);
       p.rotations[i * 4 + c] = value;
     }
@@ -375,58 +430,101 @@ __global__ void __launch_bounds__(128) k_chain(Params p, const ViewSet *__restri
     step_state(value, state.state[3], state.store, n, i, gOpacity, args.rates[3], a, i * 5u + 3u);
     p.opacities[i] = value;
   }
-  // SH: planar element (k, c) of Gaussian i; GaussianCloud index i*shFloats + 3k + c.
-  if (!anyTouched && !stepZeros) return;
-  for (int k = 0; k < p.shCoeffs; ++k) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float g = (k < activeCoeffs && k < kMaxCoeffs) ? gSh[k][c] : 0.0f;
-      if (g == 0.0f && !stepZeros) continue;
-      const size_t plane = (size_t)(k * 3 + c) * n + i;
-      const uint32_t hashIndex = ((uint32_t)(i * shFloats + k * 3 + c)) * 5u + 4u;
-      const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
-      if (k == 0) {
-        float value = p.shDc[(size_t)c * n + i];
-        step_state(value, state.state[4], state.store, n * shFloats, plane, g, rate, a, hashIndex);
-        p.shDc[(size_t)c * n + i] = value;
-      } else {
-        const size_t idx = ((size_t)(k - 1) * 3 + c) * n + i;
-        float value = load_sh_rest<S>(p.shRest, idx);
-        step_state(value, state.state[4], state.store, n * shFloats, plane, g, rate, a, hashIndex);
-        store_sh_rest<S>(p.shRest, idx, value, hashIndex, args.seed);
-      }
+}
+
+// The SH step (train_sh_step.comp:19-70), one thread per SH element: element
+// (k, c) of Gaussian i is thread (3k + c) n + i, so a warp touches one plane and
+// neighbouring Gaussians. The gradient of coefficient k is basis_k(direction)
+// times the colour gradient the chain-rule kernel left, summed over the views.
+template <ShStore S, bool MULTI>
+__global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__restrict__ viewsPtr, const float4 *__restrict__ shGrad,
+                                                 const ChainArgs *__restrict__ argsPtr, OptimState state, GradientsOut grads,
+                                                 bool storeGradients, const uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  const size_t n = p.n;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int shFloats = 3 * p.shCoeffs;
+  if (t >= n * shFloats) return;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const ChainArgs args = *argsPtr;
+  const uint32_t plane = (uint32_t)(t / n), i = (uint32_t)(t - (size_t)plane * n);
+  const int k = (int)plane / 3, c = (int)plane - 3 * k;
+  float g = 0.0f;
+  bool touched = false;
+  const int viewCount = MULTI ? views.count : 1;
+  for (int v = 0; v < viewCount; ++v) {
+    const float4 a = shGrad[((size_t)v * n + i) * 2];
+    const uint32_t coeffs = __float_as_uint(a.w);
+    if (coeffs == 0u) continue;
+    touched = true;
+    if ((uint32_t)k < coeffs) {
+      const float4 d = shGrad[((size_t)v * n + i) * 2 + 1];
+      g = fmaf(basis_one(k, d.x, d.y, d.z), c == 0 ? a.x : (c == 1 ? a.y : a.z), g);
     }
+  }
+  if (storeGradients) {
+    grads.g[4][(size_t)i * shFloats + plane] = g;
+    return;
+  }
+  // Only Adam, when not selective, steps parameters without a gradient.
+  const bool stepZeros = !args.selective;
+  if (!touched && !stepZeros) return;
+  if (g == 0.0f && !stepZeros) return;
+  const AdamArgs a{args.beta1, args.beta2, args.epsilon, args.correction1, args.correction2, args.seed};
+  const uint32_t hashIndex = ((uint32_t)(i * shFloats + plane)) * 5u + 4u;
+  const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
+  if (k == 0) {
+    float value = p.shDc[(size_t)c * n + i];
+    step_state(value, state.state[4], state.store, n * shFloats, t, g, rate, a, hashIndex);
+    p.shDc[(size_t)c * n + i] = value;
+  } else {
+    const size_t idx = t - 3 * n;
+    float value = load_sh_rest<S>(p.shRest, idx);
+    step_state(value, state.state[4], state.store, n * shFloats, t, g, rate, a, hashIndex);
+    store_sh_rest<S>(p.shRest, idx, value, hashIndex, args.seed);
   }
 }
 
 template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
-                    const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float *densifyStats, const uint32_t *error,
-                    cudaStream_t stream) {
+                    const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
+                    const uint32_t *error, cudaStream_t stream) {
   const GradientsOut g = grads != nullptr ? *grads : GradientsOut{};
   const bool store = grads != nullptr && args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
-  if (args.fixedPoint)
-    k_chain<S, true><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, g, store, densifyStats, error);
-  else
-    k_chain<S, false><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, g, store, densifyStats, error);
+  const bool multi = views.count > 1;
+#define SB_CHAIN(F, M) \
+  k_chain<S, F, M><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, g, store, shGrad, densifyStats, error)
+  if (args.fixedPoint) {
+    if (multi) SB_CHAIN(true, true);
+    else SB_CHAIN(true, false);
+  } else {
+    if (multi) SB_CHAIN(false, true);
+    else SB_CHAIN(false, false);
+  }
+#undef SB_CHAIN
+  if (args.mode == ChainMode::Statistics) return;
+  const size_t elements = (size_t)p.n * 3 * p.shCoeffs;
+  const uint32_t shBlocks = (uint32_t)((elements + 255) / 256);
+  if (multi) k_sh_step<S, true><<<shBlocks, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
+  else k_sh_step<S, false><<<shBlocks, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
 }
 
 } // namespace
 
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
-                  const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float *densifyStats, const uint32_t *error,
-                  cudaStream_t stream) {
+                  const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
+                  const uint32_t *error, cudaStream_t stream) {
   if (p.n == 0) return;
   switch (p.shStore) {
   case ShStore::BF16:
-    launch_chain_s<ShStore::BF16>(p, views, dViews, raw, splats, args, dArgs, state, grads, densifyStats, error, stream);
+    launch_chain_s<ShStore::BF16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
     break;
   case ShStore::F16:
-    launch_chain_s<ShStore::F16>(p, views, dViews, raw, splats, args, dArgs, state, grads, densifyStats, error, stream);
+    launch_chain_s<ShStore::F16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
     break;
   default:
-    launch_chain_s<ShStore::F32>(p, views, dViews, raw, splats, args, dArgs, state, grads, densifyStats, error, stream);
+    launch_chain_s<ShStore::F32>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
     break;
   }
 }

@@ -141,7 +141,7 @@ public:
 
   // Per (view, Gaussian).
   int viewSlots = 0;
-  DeviceBuffer splats, reach, depthKeys, values, tmpKeys, tmpValues, offsets, raw;
+  DeviceBuffer splats, reach, depthKeys, values, tmpKeys, tmpValues, offsets, raw, shGrad;
   // Tile entries.
   uint32_t entryCapacity = 0;
   DeviceBuffer entryKeys, entryValues, tmpEntryKeys, tmpEntryValues;
@@ -322,8 +322,9 @@ uint64_t Trainer::bytes_per_gaussian() const {
   const uint64_t floats = 3 + 3 + 4 + 1 + 3ull * shCoeffs;
   const uint64_t params = (3 + 3 + 4 + 1 + 3) * 4 + rest;
   const uint64_t optimiser = floats * (stateStore == StateStore::F32 ? 8 : 4);
-  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets 4, raw 64.
-  const uint64_t perView = sizeof(Splat) + 4 + 16 + 4 + kRawStride * 4;
+  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets 4,
+  // raw sums 64, colour gradient and direction for the SH step 32.
+  const uint64_t perView = sizeof(Splat) + 4 + 16 + 4 + kRawStride * 4 + 32;
   return params + optimiser + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
 }
 
@@ -399,6 +400,7 @@ void Trainer::ensure_view_buffers() {
     tmpValues.ensure(items * 4);
     offsets.ensure(items * 4);
     raw.ensure(items * kRawStride * 4);
+    shGrad.ensure(items * 32);
     SB_CUDA(cudaMemset(raw.get(), 0, items * kRawStride * 4));
     viewSlots = count;
     clear_graphs();
@@ -573,7 +575,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
     gp = &g;
   }
   launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
-               densifyStats.get<float>(), error, stream);
+               shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
 }
 
 void Trainer::record_readback() {
@@ -897,7 +899,8 @@ int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_r
     SB_CUDA(cudaMemcpyAsync(t->dArgs.get(), t->hArgs.get(), sizeof(sb::ChainArgs), cudaMemcpyHostToDevice, t->stream));
     sb::OptimState st = t->optim_state();
     sb::launch_chain(t->params(), t->views, t->dViews.get<sb::ViewSet>(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
-                     t->dArgs.get<sb::ChainArgs>(), st, nullptr, t->densifyStats.get<float>(), nullptr, t->stream);
+                     t->dArgs.get<sb::ChainArgs>(), st, nullptr, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
+                     t->stream);
     SB_CUDA(cudaStreamSynchronize(t->stream));
   });
 }
