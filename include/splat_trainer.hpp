@@ -1,0 +1,192 @@
+// Header-only C++ face of the C ABI in splat_b200.h with the reference
+// trainer's class shape (splat::Trainer, src/train/trainer.hpp:89-270 of the
+// reference), so that code written against the reference's trainer can switch
+// to this library by changing its include and its construction. Errors become
+// the exceptions the reference throws: BudgetExceeded (trainer.hpp:46-49),
+// std::runtime_error, std::logic_error (trainer.cpp:853).
+//
+// Types are this header's own plain structs; a caller with the reference's
+// GaussianCloud and Camera converts with the two adapters at the end, which
+// compile only where the reference's headers are included first.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <cstring>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "splat_b200.h"
+
+namespace splat_b200 {
+
+class BudgetExceeded : public std::runtime_error {
+public:
+  using std::runtime_error::runtime_error;
+};
+
+inline void check(int status) {
+  if (status == SPLAT_OK) return;
+  const std::string message = splat_last_error();
+  if (status == SPLAT_ERR_BUDGET) throw BudgetExceeded(message);
+  if (status == SPLAT_ERR_STATE) throw std::logic_error(message);
+  if (status == SPLAT_ERR_INVALID) throw std::invalid_argument(message);
+  throw std::runtime_error(message);
+}
+
+struct Cloud {
+  int shDegree = 0;
+  std::vector<float> positions, scales, rotations, opacities, sh;
+  [[nodiscard]] std::size_t size() const noexcept { return opacities.size(); }
+  [[nodiscard]] splat_cloud view() const {
+    return splat_cloud{static_cast<int32_t>(size()), shDegree, positions.data(), scales.data(), rotations.data(),
+                       opacities.data(), sh.data()};
+  }
+};
+
+inline splat_trainer_options default_options() {
+  splat_trainer_options o;
+  splat_trainer_options_default(&o);
+  return o;
+}
+
+inline splat_learning_rates default_rates() {
+  splat_learning_rates r;
+  splat_learning_rates_default(&r);
+  return r;
+}
+
+class Trainer {
+public:
+  explicit Trainer(const Cloud &initial, const splat_trainer_options &options = default_options())
+      : shDegree_(initial.shDegree), count_(initial.size()) {
+    const splat_cloud c = initial.view();
+    check(splat_trainer_create(&c, &options, &handle_));
+  }
+  ~Trainer() { splat_trainer_destroy(handle_); }
+  Trainer(const Trainer &) = delete;
+  Trainer &operator=(const Trainer &) = delete;
+
+  [[nodiscard]] std::vector<float> render(const splat_camera &camera) {
+    std::vector<float> out(static_cast<std::size_t>(camera.width) * camera.height * 4);
+    check(splat_trainer_render(handle_, &camera, out.data()));
+    return out;
+  }
+  splat_step_stats compute_gradients(const splat_camera &camera, std::span<const std::uint8_t> target) {
+    splat_step_stats s{};
+    check(splat_trainer_compute_gradients(handle_, &camera, target.data(), target.size(), &s));
+    return s;
+  }
+  splat_step_stats collect_statistics(const splat_camera &camera, std::span<const std::uint8_t> target) {
+    splat_step_stats s{};
+    check(splat_trainer_collect_statistics(handle_, &camera, target.data(), target.size(), &s));
+    return s;
+  }
+  void apply_gradients(const splat_learning_rates &rates) { check(splat_trainer_apply_gradients(handle_, &rates)); }
+  splat_step_stats step(const splat_camera &camera, std::span<const std::uint8_t> target, const splat_learning_rates &rates,
+                        std::span<const std::uint8_t> nextTarget = {}) {
+    splat_step_stats s{};
+    check(splat_trainer_step(handle_, &camera, target.data(), target.size(), &rates,
+                             nextTarget.empty() ? nullptr : nextTarget.data(), nextTarget.size(), &s));
+    return s;
+  }
+  void prefetch_target(std::span<const std::uint8_t> target) {
+    check(splat_trainer_prefetch_target(handle_, target.data(), target.size()));
+  }
+
+  struct Gradients {
+    std::vector<float> positions, scales, rotations, opacities, sh;
+  };
+  [[nodiscard]] Gradients gradients() const {
+    Gradients g;
+    const std::size_t n = count_, f = 3u * static_cast<std::size_t>((shDegree_ + 1) * (shDegree_ + 1));
+    g.positions.resize(n * 3);
+    g.scales.resize(n * 3);
+    g.rotations.resize(n * 4);
+    g.opacities.resize(n);
+    g.sh.resize(n * f);
+    check(splat_trainer_get_gradients(handle_, g.positions.data(), g.scales.data(), g.rotations.data(), g.opacities.data(),
+                                      g.sh.data()));
+    return g;
+  }
+  [[nodiscard]] Cloud cloud() const {
+    Cloud c;
+    c.shDegree = shDegree_;
+    const std::size_t n = count_, f = 3u * static_cast<std::size_t>((shDegree_ + 1) * (shDegree_ + 1));
+    c.positions.resize(n * 3);
+    c.scales.resize(n * 3);
+    c.rotations.resize(n * 4);
+    c.opacities.resize(n);
+    c.sh.resize(n * f);
+    check(splat_trainer_get_cloud(handle_, c.positions.data(), c.scales.data(), c.rotations.data(), c.opacities.data(),
+                                  c.sh.data()));
+    return c;
+  }
+  void set_active_sh_degree(int degree) { check(splat_trainer_set_active_sh_degree(handle_, degree)); }
+  void reset_densify_stats() { check(splat_trainer_reset_densify_stats(handle_)); }
+  void reset_opacity(float maximum) { check(splat_trainer_reset_opacity(handle_, maximum)); }
+  // Trainer::apply_changes: source[i] is the old index whose optimiser state
+  // Gaussian i keeps, or -1.
+  void apply_changes(const Cloud &next, std::span<const std::int32_t> source) {
+    const splat_cloud c = next.view();
+    check(splat_trainer_apply_changes(handle_, &c, source.data()));
+    count_ = next.size();
+  }
+  [[nodiscard]] std::vector<float> densify_stats() const {
+    std::vector<float> out(count_ * 8);
+    check(splat_trainer_get_densify_stats(handle_, out.data()));
+    return out;
+  }
+  [[nodiscard]] std::size_t gaussian_count() const noexcept { return count_; }
+  [[nodiscard]] int sh_degree() const noexcept { return shDegree_; }
+  [[nodiscard]] bool uses_fixed_point() const {
+    int32_t fixed = 0;
+    check(splat_trainer_info(handle_, nullptr, nullptr, nullptr, &fixed, nullptr, nullptr));
+    return fixed != 0;
+  }
+  [[nodiscard]] std::uint64_t gpu_bytes() const {
+    uint64_t bytes = 0;
+    check(splat_trainer_info(handle_, nullptr, nullptr, nullptr, nullptr, &bytes, nullptr));
+    return bytes;
+  }
+  [[nodiscard]] splat_trainer *handle() const noexcept { return handle_; }
+
+private:
+  splat_trainer *handle_ = nullptr;
+  int shDegree_ = 0;
+  std::size_t count_ = 0;
+};
+
+} // namespace splat_b200
+
+// Adapters from the reference's own types, available where its headers come first.
+#if defined(SPLAT_B200_WITH_REFERENCE_TYPES)
+namespace splat_b200 {
+inline Cloud from_reference(const splat::GaussianCloud &c) {
+  Cloud out;
+  out.shDegree = c.shDegree;
+  out.positions = c.positions;
+  out.scales = c.scales;
+  out.rotations = c.rotations;
+  out.opacities = c.opacities;
+  out.sh = c.sh;
+  return out;
+}
+inline splat_camera from_reference(const splat::Camera &c) {
+  splat_camera out{};
+  std::memcpy(out.view, &c.view[0][0], sizeof(out.view));
+  out.position[0] = c.position.x;
+  out.position[1] = c.position.y;
+  out.position[2] = c.position.z;
+  out.fx = c.fx;
+  out.fy = c.fy;
+  out.cx = c.cx;
+  out.cy = c.cy;
+  out.width = c.width;
+  out.height = c.height;
+  return out;
+}
+} // namespace splat_b200
+#endif
