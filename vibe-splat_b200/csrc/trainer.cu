@@ -30,6 +30,13 @@ namespace sb {
 
 thread_local std::string g_lastError;
 
+// For entry points outside this file. An empty message clears without
+// allocating.
+void set_last_error(const char *message) {
+  if (message == nullptr || message[0] == '\0') g_lastError.clear();
+  else g_lastError.assign(message);
+}
+
 struct Failure {
   int status;
   std::string message;
