@@ -284,7 +284,9 @@ def our_arm(args) -> None:
     rates = splat.LearningRates()
     nbytes = WIDTH * HEIGHT * 4
 
-    def run_form(options, label: str):
+    tuned = {}
+
+    def run_form(options, label: str, tune: bool = False):
         trainer = splat.Trainer(cloud, options)
         stream = trainer.stream()
 
@@ -292,6 +294,9 @@ def our_arm(args) -> None:
             k = i % len(cams)
             return trainer.step_device_target(cams[k], device_targets[k].data_ptr(), rates)
 
+        if tune:
+            # The autotuner picks the sort form and digit width (gradient passes, no parameter change).
+            tuned.update(trainer.autotune(cams[0], host_targets[0], repeats=3))
         for i in range(args.warmup):
             resident(i)
         if dist is not None:
@@ -301,7 +306,10 @@ def our_arm(args) -> None:
         stats = resident(0)
         return trainer, ms, clocks.summary(), stats
 
-    trainer, ms, clocks, stats = run_form(chosen_options(splat), "chosen")
+    chosen = chosen_options(splat)
+    if args.sort_form is not None:
+        chosen.sort_form = args.sort_form
+    trainer, ms, clocks, stats = run_form(chosen, "chosen", tune=args.sort_form is None and not args.no_autotune)
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -376,7 +384,16 @@ def our_arm(args) -> None:
 
     h2d = nbytes + 1240 + 128
     d2h = 160
-    launches_per_step = 22
+    form = tuned.get("sort_form", chosen.sort_form)
+    digits = tuned.get("digit_bits", chosen.digit_bits)
+    tile_bits = max(1, math.ceil(math.log2(((WIDTH + 15) // 16) * ((HEIGHT + 15) // 16))))
+    # Kernels of one step: preprocess, [histogram + passes of the depth sort],
+    # count+scan, emit, histogram + passes of the entry sort, ranges, forward,
+    # SSIM, loss, loss totals, backward, chain, geometry Adam, SH step.
+    depth_launches = (1 + math.ceil(32 / digits)) if form == 0 else 0
+    entry_launches = 1 + math.ceil((tile_bits + (32 if form == 1 else 0)) / digits)
+    launches_per_step = 12 + depth_launches + entry_launches
+    form_name = "depth then tile sort" if form == 0 else "64-bit tile|depth keys"
     out = {
         "metric": "train iters/s @1M Gaussians 1237x822 (fwd+bwd+Adam per view)",
         "value": value, "unit": "iters/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -384,8 +401,10 @@ def our_arm(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; the bicycle photos are not available)",
         "config": {"workload": "1M Gaussians, SH degree 3 (BF16 above DC), 1237x822, 64 cameras on a radius-5 hemisphere, "
-                               "60 deg horizontal fov", "form": "chosen: BF16 SH + BF16-pair Adam state, 64-bit tile|depth "
-                               "keys, CUDA graph, SFU exp/log", "parallelism": f"replicas x{world}",
+                               "60 deg horizontal fov",
+                   "form": f"chosen: BF16 SH + BF16-pair Adam state, {form_name} with {digits}-bit digits "
+                           f"({'autotuned' if tuned else 'fixed'}), CUDA graph, SFU exp/log",
+                   "autotune_ms": tuned.get("ms"), "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (1M-Gaussian parameters and state, 64 x 4 MB targets)",
                    "tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -412,6 +431,9 @@ def main() -> None:
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
+    parser.add_argument("--no-autotune", action="store_true", help="keep the chosen form's sort settings")
+    parser.add_argument("--sort-form", type=int, choices=[0, 1], default=None,
+                        help="override the chosen form's tile sort (0: depth then tile, 1: 64-bit tile|depth keys)")
     parser.add_argument("--views", type=int, default=VIEWS,
                         help="cameras cycled through (default 64; fewer keep ncu captures small)")
     parser.add_argument("--gaussians", type=int, default=GAUSSIANS,

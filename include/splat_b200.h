@@ -212,6 +212,20 @@ int splat_trainer_info(splat_trainer *trainer, int64_t *gaussians, int32_t *sh_d
  * iteration by stage, in order. Fills up to `capacity` (name, ms) pairs; names
  * are static strings. *count gets the number of stages. */
 int splat_trainer_timings(splat_trainer *trainer, const char **names, double *ms, int32_t capacity, int32_t *count);
+/* What splat_trainer_autotune measured and chose. */
+typedef struct splat_autotune_result {
+  int32_t sort_form;    /* the splat_sort_form kept */
+  int32_t digit_bits;   /* the radix digit width kept */
+  double ms[2][3];      /* milliseconds per gradient pass, [sort form][digit bits - 6] */
+} splat_autotune_result;
+
+/* The autotuner (new in this library; the reference has fixed 16x16 tiles and
+ * 8-bit digits): times every tile-sort form and radix digit width on this view
+ * with gradient passes (which change neither the parameters, the optimiser
+ * state nor the densification statistics), `repeats` passes each, and keeps
+ * the fastest for the following steps. */
+int splat_trainer_autotune(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
+                           int32_t repeats, splat_autotune_result *result);
 /* Turns per-stage CUDA-event timing on or off (off by default: it serialises). */
 int splat_trainer_set_timing(splat_trainer *trainer, int32_t enabled);
 /* Trainer::parameters (trainer.hpp:137): the device address of a parameter

@@ -304,3 +304,24 @@ def test_radix_sort_u64_tile_depth_keys(splat, digit_bits):
                             digit_bits=digit_bits)
     np.testing.assert_array_equal(k.cpu().numpy().view(np.uint64), keys[order])
     np.testing.assert_array_equal(v.cpu().numpy().view(np.uint32), order)
+
+
+def test_autotune_changes_nothing_but_the_sort_settings(splat, oracle):
+    view = oracle.train_camera(96, 80)
+    target = oracle.smooth_target(96, 80, 3)
+    cloud = oracle.random_cloud(400, 2, 31)
+    opts = splat.TrainerOptions(force_fixed_point=True, use_graph=True)
+    tuned = splat.Trainer(to_cloud(cloud), opts)
+    result = tuned.autotune(to_camera(view), target, repeats=1)
+    assert result["sort_form"] in (0, 1) and result["digit_bits"] in (6, 7, 8)
+    assert all(v > 0 for v in result["ms"].values())
+    after = tuned.cloud()
+    np.testing.assert_array_equal(after.positions, cloud.positions)
+    assert np.all(tuned.densify_stats().visits == 0)
+    plain = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=True))
+    rates = splat.LearningRates(position=1e-3)
+    for _ in range(3):
+        a = tuned.step(to_camera(view), target, rates)
+        b = plain.step(to_camera(view), target, rates)
+        assert a.loss == b.loss and a.tile_entries == b.tile_entries
+    np.testing.assert_array_equal(tuned.cloud().positions, plain.cloud().positions)

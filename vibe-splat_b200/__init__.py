@@ -135,6 +135,14 @@ _lib.splat_trainer_prefetch_target.argtypes = [_P, _P, ctypes.c_size_t]
 _lib.splat_trainer_step_device_target.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Rates),
                                                   ctypes.POINTER(_Stats)]
 _lib.splat_trainer_stream.argtypes = [_P, ctypes.POINTER(_P)]
+
+
+class _Autotune(ctypes.Structure):
+    _fields_ = [("sort_form", ctypes.c_int32), ("digit_bits", ctypes.c_int32), ("ms", (ctypes.c_double * 3) * 2)]
+
+
+_lib.splat_trainer_autotune.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_int32,
+                                        ctypes.POINTER(_Autotune)]
 _lib.splat_trainer_get_gradients.argtypes = [_P, _FP, _FP, _FP, _FP, _FP]
 _lib.splat_trainer_get_cloud.argtypes = [_P, _FP, _FP, _FP, _FP, _FP]
 _lib.splat_trainer_set_active_sh_degree.argtypes = [_P, ctypes.c_int32]
@@ -472,6 +480,15 @@ class Trainer:
                                                      camera.width * camera.height * 4, ctypes.byref(rates._c()),
                                                      ctypes.byref(s)))
         return StepStats._from(s)
+
+    def autotune(self, camera: Camera, target, repeats: int = 3) -> dict:
+        """Times each tile-sort form and radix digit width on this view with
+        gradient passes (no parameter changes) and keeps the fastest."""
+        t, p, n = _target_ptr(target)
+        r = _Autotune()
+        _check(_lib.splat_trainer_autotune(self._h, ctypes.byref(camera._c()), p, n, int(repeats), ctypes.byref(r)))
+        return {"sort_form": r.sort_form, "digit_bits": r.digit_bits,
+                "ms": {f"form{f}/digits{d + 6}": r.ms[f][d] for f in range(2) for d in range(3)}}
 
     def stream(self) -> int:
         """The cudaStream_t the trainer runs on, as an integer handle."""

@@ -53,15 +53,22 @@ __device__ __forceinline__ __half half_stochastic(float x, uint32_t index, uint3
 }
 
 struct AdamArgs {
-  float beta1, beta2, epsilon, correction1, correction2;
+  float beta1, beta2, epsilon, invCorrection1, invCorrection2;
   uint32_t seed;
 };
 
-// Adam on one parameter (step_parameter with radius < 0).
+__device__ __forceinline__ AdamArgs adam_args(const ChainArgs &c) {
+  return AdamArgs{c.beta1, c.beta2, c.epsilon, 1.0f / c.correction1, 1.0f / c.correction2, c.seed};
+}
+
+// Adam on one parameter (step_parameter with radius < 0): the bias
+// corrections as multiplications by their reciprocals, the step's division
+// by the SFU reciprocal (the reference's GLSL division is not correctly
+// rounded either).
 __device__ __forceinline__ void adam(float &value, float &m, float &v, float g, float rate, const AdamArgs &a) {
   m = a.beta1 * m + (1.0f - a.beta1) * g;
   v = a.beta2 * v + (1.0f - a.beta2) * g * g;
-  value -= rate * (m / a.correction1) / (sqrtf(v / a.correction2) + a.epsilon);
+  value -= __fdividef(rate * (m * a.invCorrection1), sqrtf(v * a.invCorrection2) + a.epsilon);
 }
 
 // Steps parameter `at` of a group whose state is `state` (F32: m then v planes
@@ -382,74 +389,84 @@ __global__ void __launch_bounds__(128, 4) k_chain(Params p, const ViewSet *__res
   }
 
   if (args.mode == ChainMode::Statistics) return;
-  if (!anyTouched && !zeros && !penalties) return;
   // The penalties (3DGS-MCMC) apply to every Gaussian, seen or not.
   if (penalties) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) gScale[a] += args.scaleReg * splat_expf(logScale[a]);
     gOpacity += args.opacityReg * opacity * (1.0f - opacity);
   }
-  if (storeGradients) {
+  (void)zeros;
+  (void)anyTouched;
+  (void)state;
+  (void)storeGradients;
+  // The geometry gradients, zeros for a Gaussian no view reached; the Adam
+  // kernel steps them (or they are the stored gradients).
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      grads.g[0][i * 3 + a] = gP[a];
-      grads.g[1][i * 3 + a] = gScale[a];
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) grads.g[2][i * 4 + a] = gRot[a];
-    grads.g[3][i] = gOpacity;
-    return;
+  for (int a = 0; a < 3; ++a) {
+    grads.g[0][i * 3 + a] = gP[a];
+    grads.g[1][i * 3 + a] = gScale[a];
   }
-  // Adam. A parameter with a zero gradient is left alone when selective.
-  const AdamArgs a{args.beta1, args.beta2, args.epsilon, args.correction1, args.correction2, args.seed};
-  const bool stepZeros = !args.selective;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    if (gP[c] != 0.0f || stepZeros) {
-      float value = pos[c];
-      step_state(value, state.state[0], state.store, n * 3, i * 3 + c, gP[c], args.rates[0], a, (i * 3 + c) * 5u + 0u);
-      p.positions[i * 3 + c] = value;
-    }
-    if (gScale[c] != 0.0f || stepZeros) {
-      float value = logScale[c];
-      step_state(value, state.state[1], state.store, n * 3, i * 3 + c, gScale[c], args.rates[1], a, (i * 3 + c) * 5u + 1u);
-      p.scales[i * 3 + c] = value;
-    }
-  }
-  const float rv[4] = {rq.x, rq.y, rq.z, rq.w};
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    if (gRot[c] != 0.0f || stepZeros) {
-      float value = rv[c];
-      step_state(value, state.state[2], state.store, n * 4, i * 4 + c, gRot[c], args.rates[2], a, (i * 4 + c) * 5u + 2u);
-      p.rotations[i * 4 + c] = value;
-    }
-  }
-  if (gOpacity != 0.0f || stepZeros) {
-    float value = p.opacities[i];
-    step_state(value, state.state[3], state.store, n, i, gOpacity, args.rates[3], a, i * 5u + 3u);
-    p.opacities[i] = value;
-  }
+  reinterpret_cast<float4 *>(grads.g[2])[i] = make_float4(gRot[0], gRot[1], gRot[2], gRot[3]);
+  grads.g[3][i] = gOpacity;
 }
 
-// The SH step (train_sh_step.comp:19-70), one thread per SH element: element
-// (k, c) of Gaussian i is thread (3k + c) n + i, so a warp touches one plane and
-// neighbouring Gaussians. The gradient of coefficient k is basis_k(direction)
-// times the colour gradient the chain-rule kernel left, summed over the views.
+// Adam on positions, scales, rotations and opacities (EMITTER,
+// train_gradient.comp:57-76), one thread per element of the four arrays taken
+// as one: [positions 3n | scales 3n | rotations 4n | opacities n].
+__global__ void __launch_bounds__(256) k_adam_geometry(Params p, const ChainArgs *__restrict__ argsPtr, OptimState state,
+                                                       GradientsOut grads, const uint32_t *error) {
+  const size_t n = p.n;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 11 * n) return;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const ChainArgs args = *argsPtr;
+  uint32_t group;
+  size_t idx, count;
+  float *values;
+  const float *gradient;
+  void *st;
+  float rate;
+  if (t < 3 * n) {
+    group = 0, idx = t, count = 3 * n, values = p.positions, gradient = grads.g[0], st = state.state[0], rate = args.rates[0];
+  } else if (t < 6 * n) {
+    group = 1, idx = t - 3 * n, count = 3 * n, values = p.scales, gradient = grads.g[1], st = state.state[1], rate = args.rates[1];
+  } else if (t < 10 * n) {
+    group = 2, idx = t - 6 * n, count = 4 * n, values = p.rotations, gradient = grads.g[2], st = state.state[2], rate = args.rates[2];
+  } else {
+    group = 3, idx = t - 10 * n, count = n, values = p.opacities, gradient = grads.g[3], st = state.state[3], rate = args.rates[3];
+  }
+  const float g = gradient[idx];
+  // A parameter with a zero gradient is left alone when selective.
+  if (g == 0.0f && args.selective) return;
+  const AdamArgs a = adam_args(args);
+  float value = values[idx];
+  step_state(value, st, state.store, count, idx, g, rate, a, (uint32_t)idx * 5u + group);
+  values[idx] = value;
+}
+
+// The SH step (train_sh_step.comp:19-70): blocks along y are groups of four
+// coefficients, along x the Gaussians; a thread steps the 12 elements (4
+// coefficients x 3 channels) of one Gaussian, so it reads the colour gradient
+// and direction the chain-rule kernel left once per group rather than once
+// per element, and each warp's accesses to an SH plane cover 32 neighbouring
+// Gaussians. The gradient of coefficient k is basis_k(direction) times the
+// colour gradient, summed over the views.
+constexpr int kShGroup = 4;
+
 template <ShStore S, bool MULTI>
 __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__restrict__ viewsPtr, const float4 *__restrict__ shGrad,
                                                  const ChainArgs *__restrict__ argsPtr, OptimState state, GradientsOut grads,
                                                  bool storeGradients, const uint32_t *error) {
   const ViewSet &views = *viewsPtr;
-  const size_t n = p.n;
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int shFloats = 3 * p.shCoeffs;
-  if (t >= n * shFloats) return;
+  const uint32_t n = p.n;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  const ChainArgs args = *argsPtr;
-  const uint32_t plane = (uint32_t)(t / n), i = (uint32_t)(t - (size_t)plane * n);
-  const int k = (int)plane / 3, c = (int)plane - 3 * k;
-  float g = 0.0f;
+  const int k0 = (int)blockIdx.y * kShGroup;
+  const int shFloats = 3 * p.shCoeffs;
+  float g[kShGroup][3];
+#pragma unroll
+  for (int kk = 0; kk < kShGroup; ++kk) g[kk][0] = g[kk][1] = g[kk][2] = 0.0f;
   bool touched = false;
   const int viewCount = MULTI ? views.count : 1;
   for (int v = 0; v < viewCount; ++v) {
@@ -457,31 +474,55 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
     const uint32_t coeffs = __float_as_uint(a.w);
     if (coeffs == 0u) continue;
     touched = true;
-    if ((uint32_t)k < coeffs) {
-      const float4 d = shGrad[((size_t)v * n + i) * 2 + 1];
-      g = fmaf(basis_one(k, d.x, d.y, d.z), c == 0 ? a.x : (c == 1 ? a.y : a.z), g);
+    const float4 d = shGrad[((size_t)v * n + i) * 2 + 1];
+#pragma unroll
+    for (int kk = 0; kk < kShGroup; ++kk) {
+      const int k = k0 + kk;
+      if ((uint32_t)k < coeffs) {
+        const float b = basis_one(k, d.x, d.y, d.z);
+        g[kk][0] = fmaf(b, a.x, g[kk][0]);
+        g[kk][1] = fmaf(b, a.y, g[kk][1]);
+        g[kk][2] = fmaf(b, a.z, g[kk][2]);
+      }
     }
   }
   if (storeGradients) {
-    grads.g[4][(size_t)i * shFloats + plane] = g;
+#pragma unroll
+    for (int kk = 0; kk < kShGroup; ++kk) {
+      if (k0 + kk < p.shCoeffs) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) grads.g[4][(size_t)i * shFloats + (k0 + kk) * 3 + c] = g[kk][c];
+      }
+    }
     return;
   }
+  const ChainArgs args = *argsPtr;
   // Only Adam, when not selective, steps parameters without a gradient.
   const bool stepZeros = !args.selective;
   if (!touched && !stepZeros) return;
-  if (g == 0.0f && !stepZeros) return;
-  const AdamArgs a{args.beta1, args.beta2, args.epsilon, args.correction1, args.correction2, args.seed};
-  const uint32_t hashIndex = ((uint32_t)(i * shFloats + plane)) * 5u + 4u;
-  const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
-  if (k == 0) {
-    float value = p.shDc[(size_t)c * n + i];
-    step_state(value, state.state[4], state.store, n * shFloats, t, g, rate, a, hashIndex);
-    p.shDc[(size_t)c * n + i] = value;
-  } else {
-    const size_t idx = t - 3 * n;
-    float value = load_sh_rest<S>(p.shRest, idx);
-    step_state(value, state.state[4], state.store, n * shFloats, t, g, rate, a, hashIndex);
-    store_sh_rest<S>(p.shRest, idx, value, hashIndex, args.seed);
+  const AdamArgs a = adam_args(args);
+#pragma unroll
+  for (int kk = 0; kk < kShGroup; ++kk) {
+    const int k = k0 + kk;
+    if (k >= p.shCoeffs) continue;
+    const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (g[kk][c] == 0.0f && !stepZeros) continue;
+      const uint32_t plane = (uint32_t)(k * 3 + c);
+      const size_t t = (size_t)plane * n + i;
+      const uint32_t hashIndex = (i * (uint32_t)shFloats + plane) * 5u + 4u;
+      if (k == 0) {
+        float value = p.shDc[t];
+        step_state(value, state.state[4], state.store, (size_t)n * shFloats, t, g[kk][c], rate, a, hashIndex);
+        p.shDc[t] = value;
+      } else {
+        const size_t idx = t - 3 * (size_t)n;
+        float value = load_sh_rest<S>(p.shRest, idx);
+        step_state(value, state.state[4], state.store, (size_t)n * shFloats, t, g[kk][c], rate, a, hashIndex);
+        store_sh_rest<S>(p.shRest, idx, value, hashIndex, args.seed);
+      }
+    }
   }
 }
 
@@ -489,8 +530,8 @@ template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                     const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
                     const uint32_t *error, cudaStream_t stream) {
-  const GradientsOut g = grads != nullptr ? *grads : GradientsOut{};
-  const bool store = grads != nullptr && args.mode == ChainMode::Gradients;
+  const GradientsOut g = *grads;
+  const bool store = args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
   const bool multi = views.count > 1;
 #define SB_CHAIN(F, M) \
@@ -504,10 +545,10 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
   }
 #undef SB_CHAIN
   if (args.mode == ChainMode::Statistics) return;
-  const size_t elements = (size_t)p.n * 3 * p.shCoeffs;
-  const uint32_t shBlocks = (uint32_t)((elements + 255) / 256);
-  if (multi) k_sh_step<S, true><<<shBlocks, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
-  else k_sh_step<S, false><<<shBlocks, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
+  if (!store) k_adam_geometry<<<(uint32_t)((11 * (size_t)p.n + 255) / 256), 256, 0, stream>>>(p, dArgs, state, g, error);
+  const dim3 shGrid(div_up(p.n, 256), div_up(p.shCoeffs, kShGroup));
+  if (multi) k_sh_step<S, true><<<shGrid, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
+  else k_sh_step<S, false><<<shGrid, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
 }
 
 } // namespace

@@ -26,18 +26,22 @@ namespace sb {
 namespace {
 
 constexpr int kBatch = kTilePixels; // splats staged per round, one per thread
-constexpr int kAccStride = 15;      // shared accumulator words per staged splat (odd: no bank conflicts)
+constexpr int kGradValues = 12;     // sums per splat without scoring (values 12, 13 need the scoring pass)
+constexpr int kAccStride = 13;      // shared accumulator words per staged splat (odd: no bank conflicts)
 
-// A staged splat, 48 bytes: centre, -qxx/2, -qxy, -qyy/2 (exact rescalings of
-// the conic), opacity, colour, and the tile's column (bits 0-15) and row (bits
-// 16-31) masks.
+// A staged splat, 64 bytes in four 16-byte words so that a pixel reads only
+// what it needs: first the tile's column (bits 0-15) and row (bits 16-31)
+// masks with the centre and opacity, then -qxx/2, -qxy, -qyy/2 (exact
+// rescalings of the conic) and the colour, then the conic itself for the
+// backward pass.
 struct __align__(16) Staged {
-  float cx, cy, hqx, nqy;
-  float hqz, opacity, r, g;
-  float b;
   uint32_t mask;
+  float cx, cy, opacity;
+  float hqx, nqy, hqz, r;
+  float g, b, qx, qy;
+  float qz;
   uint32_t index;
-  float pad;
+  float pad0, pad1;
 };
 
 __device__ __forceinline__ uint32_t to_u32_clamped(float v) { return (uint32_t)fminf(v, 4294967040.0f); }
@@ -79,9 +83,13 @@ __device__ __forceinline__ Staged stage(const Splat &s, uint32_t index, uint32_t
   out.r = s.colorRadius.x;
   out.g = s.colorRadius.y;
   out.b = s.colorRadius.z;
+  out.qx = s.conicOpacity.x;
+  out.qy = s.conicOpacity.y;
+  out.qz = s.conicOpacity.z;
   out.mask = pixel_masks(s, x0, y0, x1, y1);
   out.index = index;
-  out.pad = 0.0f;
+  out.pad0 = 0.0f;
+  out.pad1 = 0.0f;
   return out;
 }
 
@@ -187,9 +195,26 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
   }
 }
 
-// Lane l (< 16) ends up with the warp total of value bitreverse4(l).
-__device__ __forceinline__ float butterfly(float v[16]) {
+// The reference's transposed butterfly (reduce_and_add) over the 12 values the
+// backward pass produces without scoring; lane l (< 16) ends up with the warp
+// total of value bitreverse4(l). The reference pads to 16 values with zeros.
+// In its first level the partners of values 4-7 are pads (12-15): a lower lane
+// adds the same two numbers as the reference without selecting, and an upper
+// lane's sum there stands for a pad total that no lane ever reads. Every total
+// that is read is made of the same additions in the same order.
+__device__ __forceinline__ float butterfly12(float v[12]) {
   const uint32_t lane = threadIdx.x & 31u;
+  {
+    const bool upper = (lane & 1u) != 0u;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float send = upper ? v[i] : v[i + 8];
+      const float keep = upper ? v[i + 8] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 1);
+    }
+#pragma unroll
+    for (int i = 4; i < 8; ++i) v[i] = v[i] + __shfl_xor_sync(0xFFFFFFFFu, v[i], 1);
+  }
 #define SB_HALVE(offset, count)                                           \
   {                                                                       \
     const bool upper = (lane & (offset)) != 0u;                           \
@@ -199,7 +224,6 @@ __device__ __forceinline__ float butterfly(float v[16]) {
       v[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, (offset));         \
     }                                                                     \
   }
-  SB_HALVE(1, 16)
   SB_HALVE(2, 8)
   SB_HALVE(4, 4)
   SB_HALVE(8, 2)
@@ -260,52 +284,47 @@ __global__ void __launch_bounds__(kTilePixels, 3)
       const Staged &s = s_batch[k];
       const uint32_t mask = s.mask;
       if ((mask & warpRows) == 0u || (mask & 0xFFFFu) == 0u) continue; // warp-uniform: no lane has anything
-      float g[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) g[j] = 0.0f;
-      bool any = false;
-      if (start + k >= stop && (mask & myBits) == myBits) {
-        const float dx = pxf - s.cx, dy = pyf - s.cy;
-        const float power = splat_power(s, dx, dy);
-        if (!(power > 0.0f)) {
-          const float ep = M::exp(power);
-          const float oe = s.opacity * ep;
-          const float alpha = fminf(kAlphaMax, oe);
-          if (alpha >= kAlphaMin) {
-            const float logRest = M::log(1.0f - alpha);
-            const float T = M::exp((logTotal - logBehind) - logRest);
-            const float wA = T * alpha;
-            g[6] = wA * A.x;
-            g[7] = wA * A.y;
-            g[8] = wA * A.z;
-            g[9] = wA * perPixel;
-            // At the 0.99 clamp alpha no longer depends on the parameters.
-            if (oe < kAlphaMax) {
-              const float dAlpha = T * fmaf(A.z, s.b - Bb, fmaf(A.y, s.g - Bg, A.x * (s.r - Br)));
-              g[0] = dAlpha * ep;
-              const float dPower = dAlpha * alpha;
-              const float qx = -2.0f * s.hqx, qy = -s.nqy, qz = -2.0f * s.hqz;
-              const float vx = fmaf(qy, dy, qx * dx), vy = fmaf(qz, dy, qy * dx);
-              g[1] = dPower * vx;
-              g[2] = dPower * vy;
-              g[10] = fabsf(g[1]);
-              g[11] = fabsf(g[2]);
-              const float h = dPower * 0.5f;
-              g[3] = h * vx * vx;
-              g[4] = h * vx * vy;
-              g[5] = h * vy * vy;
-            }
-            any = true;
-            Br = fmaf(alpha, s.r - Br, Br);
-            Bg = fmaf(alpha, s.g - Bg, Bg);
-            Bb = fmaf(alpha, s.b - Bb, Bb);
-            logBehind = logBehind + logRest;
-          }
-        }
-      }
-      if (!__any_sync(0xFFFFFFFFu, any)) continue;
-      const float total = butterfly(g);
-      if (lane < 16 && held < (uint32_t)kRawPerSplat && total != 0.0f) {
+      // The tests of splat_at() first; one vote decides whether the warp has work.
+      const float dx = pxf - s.cx, dy = pyf - s.cy;
+      const float power = splat_power(s, dx, dy);
+      // exp of a clamped power: an inactive lane may have power > 0, and its
+      // exp must stay finite because it is multiplied by zero below.
+      const float ep = M::exp(fminf(power, 0.0f));
+      const float oe = s.opacity * ep;
+      const float alpha = fminf(kAlphaMax, oe);
+      const bool act = start + k >= stop && (mask & myBits) == myBits && !(power > 0.0f) && alpha >= kAlphaMin;
+      if (!__any_sync(0xFFFFFFFFu, act)) continue;
+      // The warp's arithmetic without branches: an inactive lane takes alpha
+      // and the weights as exact zeros, which leaves its B and log T behind as
+      // they were and adds zeros to the sums.
+      const float aAct = act ? alpha : 0.0f;
+      const float logRest = M::log(1.0f - aAct);
+      const float T = M::exp((logTotal - logBehind) - logRest);
+      const float wA = act ? T * alpha : 0.0f;
+      float g[12];
+      g[6] = wA * A.x;
+      g[7] = wA * A.y;
+      g[8] = wA * A.z;
+      g[9] = wA * perPixel;
+      // At the 0.99 clamp alpha no longer depends on the parameters.
+      const float dAlpha = (act && oe < kAlphaMax) ? T * fmaf(A.z, s.b - Bb, fmaf(A.y, s.g - Bg, A.x * (s.r - Br))) : 0.0f;
+      g[0] = dAlpha * ep;
+      const float dPower = dAlpha * alpha;
+      const float vx = fmaf(s.qy, dy, s.qx * dx), vy = fmaf(s.qz, dy, s.qy * dx);
+      g[1] = dPower * vx;
+      g[2] = dPower * vy;
+      g[10] = fabsf(g[1]);
+      g[11] = fabsf(g[2]);
+      const float h = dPower * 0.5f;
+      g[3] = h * vx * vx;
+      g[4] = h * vx * vy;
+      g[5] = h * vy * vy;
+      Br = fmaf(aAct, s.r - Br, Br);
+      Bg = fmaf(aAct, s.g - Bg, Bg);
+      Bb = fmaf(aAct, s.b - Bb, Bb);
+      logBehind = logBehind + logRest;
+      const float total = butterfly12(g);
+      if (lane < 16 && held < (uint32_t)kGradValues && total != 0.0f) {
         uint32_t *slot = &s_acc[k * kAccStride + held];
         if (FIXED) {
           atomicAdd(reinterpret_cast<int *>(slot), __float2int_rn(fminf(fmaxf(total * scale, -1.0e9f), 1.0e9f)));
@@ -319,7 +338,7 @@ __global__ void __launch_bounds__(kTilePixels, 3)
     if (t < count && s_batch[t].mask != 0u) {
       const size_t base = ((size_t)s_batch[t].index) * kRawStride;
 #pragma unroll
-      for (int j = 0; j < kRawPerSplat; ++j) {
+      for (int j = 0; j < kGradValues; ++j) {
         const uint32_t v = s_acc[t * kAccStride + j];
         if (v != 0u) {
           if (FIXED) {

@@ -198,6 +198,8 @@ public:
   void render(const splat_camera *camera, float *out);
   void finish_stats(splat_step_stats *stats, int count);
   void fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates);
+  void set_sort(bool single, int digits);
+  void autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats, splat_autotune_result *out);
 };
 
 // ---------------------------------------------------------------- set-up
@@ -278,6 +280,9 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
     state[g].ensure(bytes);
     SB_CUDA(cudaMemset(state[g].get(), 0, bytes));
   }
+  // Geometry gradients pass through these on their way to Adam; the SH ones
+  // are made only when compute_gradients() stores them (fill_chain_args).
+  for (int g = 0; g < 4; ++g) grads[g].ensure(groupCounts[g] * 4);
   densifyStats.ensure(nn * kStatStride * 4);
   SB_CUDA(cudaMemset(densifyStats.get(), 0, nn * kStatStride * 4));
   dViews.ensure(sizeof(ViewSet));
@@ -332,7 +337,8 @@ uint64_t Trainer::bytes_per_gaussian() const {
   // Per view: splat 48, reach 4, keys/values and their copies 16, offsets 4,
   // raw sums 64, colour gradient and direction for the SH step 32.
   const uint64_t perView = sizeof(Splat) + 4 + 16 + 4 + kRawStride * 4 + 32;
-  return params + optimiser + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
+  // Geometry gradients between the chain rule and Adam: 11 floats.
+  return params + optimiser + 11 * 4 + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
 }
 
 uint64_t Trainer::entry_bytes(uint64_t entries) const {
@@ -575,12 +581,11 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   (void)statistics;
   SB_CUDA(cudaMemcpyAsync(dArgs.get(), hArgs.get(), sizeof(ChainArgs), cudaMemcpyHostToDevice, stream));
   OptimState st = optim_state();
+  // The geometry gradients always pass through these buffers on their way to
+  // Adam; compute_gradients() also keeps the SH ones there.
   GradientsOut g{};
-  const GradientsOut *gp = nullptr;
-  if (args.mode == ChainMode::Gradients) {
-    for (int k = 0; k < 5; ++k) g.g[k] = grads[k].get<float>();
-    gp = &g;
-  }
+  for (int k = 0; k < 5; ++k) g.g[k] = grads[k].get<float>();
+  const GradientsOut *gp = &g;
   launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
                shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
 }
@@ -744,6 +749,65 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
   }
 }
 
+// Switches the tile sort's form and digit width; the entry buffers (whose key
+// width may change) and the captured graphs are rebuilt on the next step.
+void Trainer::set_sort(bool single, int digits) {
+  if (single == oneSort && digits == digitBits) return;
+  SB_CUDA(cudaStreamSynchronize(stream));
+  oneSort = single;
+  digitBits = digits;
+  entryKeys.release();
+  entryValues.release();
+  tmpEntryKeys.release();
+  tmpEntryValues.release();
+  sortScratchEntries.release();
+  sortScratchDepth.release();
+  entryCapacity = 0;
+  clear_graphs();
+}
+
+// The autotuner: times every sort form and digit width on one view with
+// gradient passes, which change neither the parameters, the optimiser state
+// nor the densification statistics, and keeps the fastest. The tile size (16)
+// and the batch depth (one staged splat per pixel thread, 256) are fixed by
+// the kernels' thread-per-pixel design.
+void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats,
+                       splat_autotune_result *out) {
+  if (repeats < 1) repeats = 1;
+  const bool oldSingle = oneSort;
+  const int oldDigits = digitBits;
+  double best = 1e30;
+  int bestForm = oneSort ? 1 : 0, bestDigits = digitBits;
+  const uint8_t *targets[1] = {target};
+  const size_t sizes[1] = {bytes};
+  splat_autotune_result result{};
+  for (int form = 0; form < 2; ++form) {
+    for (int digits = 6; digits <= 8; ++digits) {
+      set_sort(form == 1, digits);
+      splat_step_stats s{};
+      // The first runs size the entry pool and capture the graph.
+      run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+      run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+      const auto t0 = std::chrono::steady_clock::now();
+      for (int r = 0; r < repeats; ++r) run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
+      result.ms[form][digits - 6] = ms;
+      if (ms < best) {
+        best = ms;
+        bestForm = form;
+        bestDigits = digits;
+      }
+    }
+  }
+  (void)oldSingle;
+  (void)oldDigits;
+  set_sort(bestForm == 1, bestDigits);
+  result.sort_form = bestForm;
+  result.digit_bits = bestDigits;
+  if (out != nullptr) *out = result;
+}
+
 void Trainer::render(const splat_camera *camera, float *out) {
   set_views(camera, 1);
   ensure_view_buffers();
@@ -905,8 +969,10 @@ int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_r
     t->fill_chain_args(sb::ChainMode::Step, false, rates);
     SB_CUDA(cudaMemcpyAsync(t->dArgs.get(), t->hArgs.get(), sizeof(sb::ChainArgs), cudaMemcpyHostToDevice, t->stream));
     sb::OptimState st = t->optim_state();
+    sb::GradientsOut g{};
+    for (int k = 0; k < 5; ++k) g.g[k] = t->grads[k].get<float>();
     sb::launch_chain(t->params(), t->views, t->dViews.get<sb::ViewSet>(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
-                     t->dArgs.get<sb::ChainArgs>(), st, nullptr, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
+                     t->dArgs.get<sb::ChainArgs>(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
                      t->stream);
     SB_CUDA(cudaStreamSynchronize(t->stream));
   });
@@ -1120,6 +1186,14 @@ int splat_trainer_timings(splat_trainer *trainer, const char **names, double *ms
       if (names) names[s] = sb::kStageNames[s];
       if (ms) ms[s] = t->stageTotals[s] / (double)t->timedIterations;
     }
+  });
+}
+
+int splat_trainer_autotune(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
+                           int32_t repeats, splat_autotune_result *result) {
+  return guarded([&] {
+    if (camera == nullptr || target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    impl_of(trainer)->autotune(camera, target, target_bytes, repeats, result);
   });
 }
 
