@@ -325,3 +325,22 @@ def test_autotune_changes_nothing_but_the_sort_settings(splat, oracle):
         b = plain.step(to_camera(view), target, rates)
         assert a.loss == b.loss and a.tile_entries == b.tile_entries
     np.testing.assert_array_equal(tuned.cloud().positions, plain.cloud().positions)
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_pixel_layouts_agree(splat, oracle, exact):
+    # One or two pixels per thread: the same per-pixel arithmetic, so the same
+    # image bit for bit; float sums in another order, so gradients to rounding.
+    view = oracle.train_camera(100, 75)
+    target = oracle.smooth_target(100, 75, 5)
+    cloud = oracle.random_cloud(500, 1, 37)
+    out = []
+    for layout in (1, 2):
+        t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(exact_math=exact, pixels_per_thread=layout))
+        image = t.render(to_camera(view))
+        stats = t.compute_gradients(to_camera(view), target)
+        out.append((image, stats, t.gradients()))
+    np.testing.assert_array_equal(out[0][0].view(np.uint32), out[1][0].view(np.uint32))
+    assert abs(out[0][1].loss - out[1][1].loss) < 1e-6
+    for name in ("positions", "scales", "rotations", "opacities", "sh"):
+        check_close(getattr(out[0][2], name), getattr(out[1][2], name), name, 0.99999, 1e-4)

@@ -119,33 +119,45 @@ __global__ void __launch_bounds__(kScanThreads)
     before += (uint32_t)w < warp ? s_warp[w] : 0u;
     tileSum += s_warp[w];
   }
-  // Decoupled look-back over the tiles before this one.
-  if (t == 0) {
+  // Decoupled look-back over the tiles before this one, by warp 0: each poll
+  // reads the 32 nearest predecessors at once (lane j the tile j + 1 back),
+  // takes the nearest inclusive prefix, and adds the aggregates in between.
+  if (warp == 0) {
     unsigned long long exclusive = 0;
     if (tile == 0) {
-      store_u64(&status[0], kScanInclusive | tileSum);
+      if (lane == 0) store_u64(&status[0], kScanInclusive | tileSum);
     } else {
-      store_u64(&status[tile], kScanAggregate | tileSum);
-      int64_t pred = (int64_t)tile - 1;
+      if (lane == 0) store_u64(&status[tile], kScanAggregate | tileSum);
+      int64_t window = (int64_t)tile - 1;
       int spins = 0;
-      while (pred >= 0) {
-        const unsigned long long v = load_u64(&status[pred]);
+      for (;;) {
+        const int64_t pred = window - (int64_t)lane;
+        // Before the first tile there is nothing: an inclusive prefix of zero.
+        const unsigned long long v = pred >= 0 ? load_u64(&status[pred]) : kScanInclusive;
         const unsigned long long flag = v & 0xFFFFFFFF00000000ull;
-        if (flag == 0) {
+        const uint32_t inclusiveLanes = __ballot_sync(0xFFFFFFFFu, flag == kScanInclusive);
+        const uint32_t pendingLanes = __ballot_sync(0xFFFFFFFFu, flag == 0);
+        const int nearest = inclusiveLanes != 0u ? __ffs(inclusiveLanes) - 1 : 32;
+        const uint32_t needed = nearest >= 31 ? 0xFFFFFFFFu : ((2u << nearest) - 1u);
+        if ((pendingLanes & needed) != 0u) {
           if (++spins > kScanSpinLimit) {
-            atomicOr(error, kErrLookbackTimeout);
+            if (lane == 0) atomicOr(error, kErrLookbackTimeout);
             break;
           }
           continue;
         }
-        exclusive += v & 0xFFFFFFFFull;
-        if (flag == kScanInclusive) break;
-        --pred;
+        const unsigned long long mine = (int)lane <= nearest ? (v & 0xFFFFFFFFull) : 0ull;
+        unsigned long long sum = mine;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+        exclusive += sum;
+        if (nearest < 32) break;
+        window -= 32;
       }
-      store_u64(&status[tile], kScanInclusive | ((exclusive + tileSum) & 0xFFFFFFFFull));
+      if (lane == 0) store_u64(&status[tile], kScanInclusive | ((exclusive + tileSum) & 0xFFFFFFFFull));
     }
-    s_exclusive = exclusive;
-    if (tile == numTiles - 1) {
+    if (lane == 0) s_exclusive = exclusive;
+    if (lane == 0 && tile == numTiles - 1) {
       const unsigned long long total = exclusive + tileSum;
       const uint32_t clipped = total > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)total;
       counters[1] = clipped;

@@ -72,6 +72,7 @@ void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *ti
 
 struct RasterConfig {
   int exactMath = 1;   // deterministic exp/log (bit-reproducible by the CPU restatement)
+  int pixelsPerThread = 2; // 2: 8x8-pixel warps, two pixels per lane; 1: the reference's 2x16-pixel warps
   float background[3] = {0.f, 0.f, 0.f};
 };
 

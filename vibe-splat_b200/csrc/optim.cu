@@ -501,6 +501,32 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
   const bool stepZeros = !args.selective;
   if (!touched && !stepZeros) return;
   const AdamArgs a = adam_args(args);
+  const size_t count = (size_t)n * shFloats;
+  // Every load first, then the arithmetic, then the stores: the values and the
+  // state are reached through plain pointers, so a load placed after a store
+  // could not be moved before it, and the 12 updates would run one by one.
+  float value[kShGroup][3], m[kShGroup][3], vv[kShGroup][3];
+  uint32_t word[kShGroup][3];
+#pragma unroll
+  for (int kk = 0; kk < kShGroup; ++kk) {
+    const int k = k0 + kk;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      value[kk][c] = m[kk][c] = vv[kk][c] = 0.0f;
+      word[kk][c] = 0u;
+      if (k >= p.shCoeffs) continue;
+      const size_t t = (size_t)(k * 3 + c) * n + i;
+      value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3 * (size_t)n);
+      if (state.store == StateStore::F32) {
+        m[kk][c] = static_cast<const float *>(state.state[4])[t];
+        vv[kk][c] = static_cast<const float *>(state.state[4])[count + t];
+      } else {
+        word[kk][c] = static_cast<const uint32_t *>(state.state[4])[t];
+        m[kk][c] = bf16_load(word[kk][c], 0);
+        vv[kk][c] = bf16_load(word[kk][c], 1);
+      }
+    }
+  }
 #pragma unroll
   for (int kk = 0; kk < kShGroup; ++kk) {
     const int k = k0 + kk;
@@ -512,15 +538,18 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       const uint32_t plane = (uint32_t)(k * 3 + c);
       const size_t t = (size_t)plane * n + i;
       const uint32_t hashIndex = (i * (uint32_t)shFloats + plane) * 5u + 4u;
-      if (k == 0) {
-        float value = p.shDc[t];
-        step_state(value, state.state[4], state.store, (size_t)n * shFloats, t, g[kk][c], rate, a, hashIndex);
-        p.shDc[t] = value;
+      adam(value[kk][c], m[kk][c], vv[kk][c], g[kk][c], rate, a);
+      if (state.store == StateStore::F32) {
+        static_cast<float *>(state.state[4])[t] = m[kk][c];
+        static_cast<float *>(state.state[4])[count + t] = vv[kk][c];
       } else {
-        const size_t idx = t - 3 * (size_t)n;
-        float value = load_sh_rest<S>(p.shRest, idx);
-        step_state(value, state.state[4], state.store, (size_t)n * shFloats, t, g[kk][c], rate, a, hashIndex);
-        store_sh_rest<S>(p.shRest, idx, value, hashIndex, args.seed);
+        static_cast<uint32_t *>(state.state[4])[t] =
+            bf16_store(bf16_store(word[kk][c], 0, bf16_round(m[kk][c])), 1, bf16_stochastic(vv[kk][c], hashIndex, a.seed));
+      }
+      if (k == 0) {
+        p.shDc[t] = value[kk][c];
+      } else {
+        store_sh_rest<S>(p.shRest, t - 3 * (size_t)n, value[kk][c], hashIndex, args.seed);
       }
     }
   }

@@ -353,18 +353,243 @@ __global__ void __launch_bounds__(kTilePixels, 3)
   }
 }
 
+// Two pixels per thread, for the forms whose sums need not follow the
+// reference's 32-lane groups: 128 threads per tile, warp w covering the 8x8
+// quadrant (w & 1, w >> 1) of the tile, lane l its pixels (l & 7, l >> 3) and
+// (l & 7, (l >> 3) + 4). The per-pixel arithmetic is that of k_forward and
+// k_backward; what changes is that a warp skips a splat that misses its 8x8
+// block, and that a staged splat's record and (backward) its reduction serve
+// two pixels per lane.
+constexpr int kHalfTile = kTilePixels / 2;
+
+struct PixelPair {
+  uint32_t x[2], y[2], bits[2];
+  float px[2], py[2];
+  bool inside[2];
+  uint32_t warpCols, warpRows;
+};
+
+__device__ __forceinline__ PixelPair pixel_pair(const TileGeometry &geo, const ViewParams &cam, uint32_t t) {
+  PixelPair pp;
+  const uint32_t warp = t >> 5, lane = t & 31u;
+  const uint32_t bx = (warp & 1u) * 8u, by = (warp >> 1) * 8u;
+  const uint32_t lx = bx + (lane & 7u), ly = by + (lane >> 3);
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const uint32_t yy = ly + 4u * q;
+    pp.x[q] = geo.x0 + lx;
+    pp.y[q] = geo.y0 + yy;
+    pp.bits[q] = (1u << lx) | (1u << (16 + yy));
+    pp.px[q] = (float)pp.x[q] + 0.5f;
+    pp.py[q] = (float)pp.y[q] + 0.5f;
+    pp.inside[q] = pp.x[q] < (uint32_t)cam.width && pp.y[q] < (uint32_t)cam.height;
+  }
+  pp.warpCols = 0xFFu << bx;
+  pp.warpRows = 0xFFu << (16 + by);
+  return pp;
+}
+
+template <class M>
+__global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
+                                                        const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
+                                                        float bgR, float bgG, float bgB, float4 *__restrict__ image,
+                                                        uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ Staged s_batch[kBatch];
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const int tile = blockIdx.x;
+  const TileGeometry geo = tile_geometry(views, tile);
+  const ViewParams &cam = views.v[geo.view];
+  const uint32_t t = threadIdx.x;
+  const PixelPair pp = pixel_pair(geo, cam, t);
+  const uint2 range = ranges[tile];
+  float cr[2] = {0.f, 0.f}, cg[2] = {0.f, 0.f}, cb[2] = {0.f, 0.f}, T[2] = {1.f, 1.f}, logT[2] = {0.f, 0.f};
+  uint32_t stop[2] = {range.x, range.x};
+  bool done[2] = {!pp.inside[0], !pp.inside[1]};
+  for (uint32_t end = range.y; end > range.x;) {
+    const uint32_t count = min((uint32_t)kBatch, end - range.x);
+    end -= count;
+    if (__syncthreads_count(done[0] && done[1]) == kHalfTile) break;
+    for (uint32_t j = t; j < count; j += kHalfTile) s_batch[j] = stage_checked(splats, entryValues[end + j], splatLimit, geo, error);
+    __syncthreads();
+    if (done[0] && done[1]) continue;
+    for (int k = (int)count - 1; k >= 0; --k) {
+      const Staged &s = s_batch[k];
+      const uint32_t mask = s.mask;
+      if ((mask & pp.warpRows) == 0u || (mask & pp.warpCols) == 0u) continue; // warp-uniform
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (done[q] || (mask & pp.bits[q]) != pp.bits[q]) continue;
+        const float dx = pp.px[q] - s.cx, dy = pp.py[q] - s.cy;
+        const float power = splat_power(s, dx, dy);
+        if (power > 0.0f) continue;
+        const float alpha = fminf(kAlphaMax, s.opacity * M::exp(power));
+        if (!(alpha >= kAlphaMin)) continue;
+        const float oneMinus = 1.0f - alpha;
+        const float logRest = M::log(oneMinus);
+        if (logT[q] + logRest < kLogMinTransmittance) {
+          stop[q] = end + (uint32_t)k + 1u;
+          done[q] = true;
+          continue;
+        }
+        const float w = T[q] * alpha;
+        cr[q] = fmaf(w, s.r, cr[q]);
+        cg[q] = fmaf(w, s.g, cg[q]);
+        cb[q] = fmaf(w, s.b, cb[q]);
+        T[q] = T[q] * oneMinus;
+        logT[q] = logT[q] + logRest;
+      }
+      if (done[0] && done[1]) break;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (!pp.inside[q]) continue;
+    const size_t at = (size_t)cam.pixelBase + (size_t)pp.y[q] * cam.width + pp.x[q];
+    image[at] = make_float4(fmaf(T[q], bgR, cr[q]), fmaf(T[q], bgG, cg[q]), fmaf(T[q], bgB, cb[q]), logT[q]);
+    stops[at] = stop[q];
+  }
+}
+
+// Float sums only: each lane adds its two pixels' values before one butterfly.
+template <class M>
+__global__ void __launch_bounds__(kHalfTile, 6)
+    k_backward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
+                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
+                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
+                uint32_t splatLimit, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ Staged s_batch[kBatch];
+  __shared__ float s_acc[kBatch * kAccStride];
+  __shared__ uint32_t s_min[kHalfTile / 32];
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const int tile = blockIdx.x;
+  const TileGeometry geo = tile_geometry(views, tile);
+  const ViewParams &cam = views.v[geo.view];
+  const uint32_t t = threadIdx.x, lane = t & 31u;
+  const PixelPair pp = pixel_pair(geo, cam, t);
+  const uint2 range = ranges[tile];
+  float logTotal[2], Ax[2], Ay[2], Az[2], Br[2], Bg[2], Bb[2], logBehind[2];
+  uint32_t stop[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const size_t at = pp.inside[q] ? (size_t)cam.pixelBase + (size_t)pp.y[q] * cam.width + pp.x[q] : 0;
+    logTotal[q] = pp.inside[q] ? image[at].w : 0.0f;
+    const float4 a = pp.inside[q] ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
+    Ax[q] = a.x;
+    Ay[q] = a.y;
+    Az[q] = a.z;
+    stop[q] = pp.inside[q] ? stops[at] : range.y;
+    Br[q] = bgR;
+    Bg[q] = bgG;
+    Bb[q] = bgB;
+    logBehind[q] = 0.0f;
+  }
+  const float perPixel = cam.perPixel;
+  const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
+  if (lane == 0) s_min[t >> 5] = warpMin;
+  for (int i = t; i < kBatch * kAccStride; i += kHalfTile) s_acc[i] = 0.0f;
+  __syncthreads();
+  uint32_t tileStop = s_min[0];
+#pragma unroll
+  for (int w = 1; w < kHalfTile / 32; ++w) tileStop = min(tileStop, s_min[w]);
+  const uint32_t held = __brev(lane) >> 28;
+
+  for (uint32_t start = tileStop; start < range.y; start += kBatch) {
+    const uint32_t count = min((uint32_t)kBatch, range.y - start);
+    __syncthreads();
+    for (uint32_t j = t; j < count; j += kHalfTile) s_batch[j] = stage_checked(splats, entryValues[start + j], splatLimit, geo, error);
+    __syncthreads();
+    for (uint32_t k = 0; k < count; ++k) {
+      const Staged &s = s_batch[k];
+      const uint32_t mask = s.mask;
+      if ((mask & pp.warpRows) == 0u || (mask & pp.warpCols) == 0u) continue; // warp-uniform
+      float dx[2], dy[2], ep[2], oe[2], alpha[2];
+      bool act[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        dx[q] = pp.px[q] - s.cx;
+        dy[q] = pp.py[q] - s.cy;
+        const float power = splat_power(s, dx[q], dy[q]);
+        ep[q] = M::exp(fminf(power, 0.0f));
+        oe[q] = s.opacity * ep[q];
+        alpha[q] = fminf(kAlphaMax, oe[q]);
+        act[q] = start + k >= stop[q] && (mask & pp.bits[q]) == pp.bits[q] && !(power > 0.0f) && alpha[q] >= kAlphaMin;
+      }
+      if (!__any_sync(0xFFFFFFFFu, act[0] || act[1])) continue;
+      float g[12];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) g[j] = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const float aAct = act[q] ? alpha[q] : 0.0f;
+        const float logRest = M::log(1.0f - aAct);
+        const float T = M::exp((logTotal[q] - logBehind[q]) - logRest);
+        const float wA = act[q] ? T * alpha[q] : 0.0f;
+        g[6] += wA * Ax[q];
+        g[7] += wA * Ay[q];
+        g[8] += wA * Az[q];
+        g[9] += wA * perPixel;
+        const float dAlpha =
+            (act[q] && oe[q] < kAlphaMax) ? T * fmaf(Az[q], s.b - Bb[q], fmaf(Ay[q], s.g - Bg[q], Ax[q] * (s.r - Br[q]))) : 0.0f;
+        g[0] += dAlpha * ep[q];
+        const float dPower = dAlpha * alpha[q];
+        const float vx = fmaf(s.qy, dy[q], s.qx * dx[q]), vy = fmaf(s.qz, dy[q], s.qy * dx[q]);
+        const float g1 = dPower * vx, g2 = dPower * vy;
+        g[1] += g1;
+        g[2] += g2;
+        g[10] += fabsf(g1);
+        g[11] += fabsf(g2);
+        const float h = dPower * 0.5f;
+        g[3] += h * vx * vx;
+        g[4] += h * vx * vy;
+        g[5] += h * vy * vy;
+        Br[q] = fmaf(aAct, s.r - Br[q], Br[q]);
+        Bg[q] = fmaf(aAct, s.g - Bg[q], Bg[q]);
+        Bb[q] = fmaf(aAct, s.b - Bb[q], Bb[q]);
+        logBehind[q] = logBehind[q] + logRest;
+      }
+      const float total = butterfly12(g);
+      if (lane < 16 && held < (uint32_t)kGradValues && total != 0.0f) atomicAdd(&s_acc[k * kAccStride + held], total);
+    }
+    __syncthreads();
+    // One global atomic per (splat, value) for the whole tile.
+    for (uint32_t j = t; j < count; j += kHalfTile) {
+      if (s_batch[j].mask == 0u) continue;
+      float *dst = raw + (size_t)s_batch[j].index * kRawStride;
+#pragma unroll
+      for (int v = 0; v < kGradValues; ++v) {
+        const float x = s_acc[j * kAccStride + v];
+        if (x != 0.0f) {
+          atomicAdd(dst + v, x);
+          s_acc[j * kAccStride + v] = 0.0f;
+        }
+      }
+    }
+  }
+}
+
 } // namespace
 
 void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
                     const RasterConfig &cfg, float4 *image, uint32_t *stops, uint32_t splatLimit, uint32_t *error,
                     cudaStream_t stream) {
   if (views.totalTiles == 0) return;
-  if (cfg.exactMath) {
-    k_forward<ExactMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, cfg.background[0],
-                                                                      cfg.background[1], cfg.background[2], image, stops, splatLimit, error);
+  const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
+  if (cfg.pixelsPerThread == 2) {
+    if (cfg.exactMath)
+      k_forward2<ExactMath><<<views.totalTiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
+                                                                       splatLimit, error);
+    else
+      k_forward2<FastMath><<<views.totalTiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
+                                                                      splatLimit, error);
   } else {
-    k_forward<FastMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, cfg.background[0],
-                                                                     cfg.background[1], cfg.background[2], image, stops, splatLimit, error);
+    if (cfg.exactMath)
+      k_forward<ExactMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
+                                                                        splatLimit, error);
+    else
+      k_forward<FastMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
+                                                                       splatLimit, error);
   }
 }
 
@@ -373,21 +598,29 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
                      bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream) {
   if (views.totalTiles == 0) return;
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
-  if (cfg.exactMath) {
-    if (fixedPoint)
-      k_backward<ExactMath, true><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
-                                                                               image, adjoint, stops, raw, splatLimit, error);
+  const uint32_t tiles = views.totalTiles;
+  // The fixed-point sums keep the reference's 32-lane groups: one pixel per thread.
+  if (!fixedPoint && cfg.pixelsPerThread == 2) {
+    float *rawF = static_cast<float *>(raw);
+    if (cfg.exactMath)
+      k_backward2<ExactMath><<<tiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
+                                                             rawF, splatLimit, error);
     else
-      k_backward<ExactMath, false><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
-                                                                                image, adjoint, stops, raw, splatLimit, error);
-  } else {
-    if (fixedPoint)
-      k_backward<FastMath, true><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
-                                                                              image, adjoint, stops, raw, splatLimit, error);
-    else
-      k_backward<FastMath, false><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b,
-                                                                               image, adjoint, stops, raw, splatLimit, error);
+      k_backward2<FastMath><<<tiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
+                                                            rawF, splatLimit, error);
+    return;
   }
+#define SB_BACKWARD(MATH, FIX) \
+  k_backward<MATH, FIX><<<tiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops, \
+                                                          raw, splatLimit, error)
+  if (cfg.exactMath) {
+    if (fixedPoint) SB_BACKWARD(ExactMath, true);
+    else SB_BACKWARD(ExactMath, false);
+  } else {
+    if (fixedPoint) SB_BACKWARD(FastMath, true);
+    else SB_BACKWARD(FastMath, false);
+  }
+#undef SB_BACKWARD
 }
 
 } // namespace sb

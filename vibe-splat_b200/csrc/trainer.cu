@@ -140,6 +140,7 @@ public:
   StateStore stateStore = StateStore::BF16Pair;
   bool fixedPoint = false, oneSort = false, exactMath = true, useGraph = false;
   int digitBits = 8;
+  int pixelsPerThread = 2;
   cudaStream_t stream = nullptr;
 
   DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
@@ -173,7 +174,7 @@ public:
 
   // Timings.
   bool timing = false;
-  cudaEvent_t events[kStages + 1] = {};
+  cudaEvent_t events[2 * kStages] = {};
   double stageTotals[kStages] = {};
   uint64_t timedIterations = 0;
 
@@ -190,7 +191,8 @@ public:
   void record_forward();
   void record_backward_and_chain(ChainMode mode, bool statistics);
   void record_readback();
-  void mark(int stage);
+  void begin(int stage);
+  void end(int stage);
   void clear_graphs();
   std::string graph_key(ChainMode mode, bool statistics) const;
   void run(const splat_camera *cameras, const uint8_t *const *targets, const size_t *bytes, int count, ChainMode mode,
@@ -231,6 +233,8 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   useGraph = opt.use_graph != 0;
   digitBits = opt.digit_bits == 0 ? 8 : opt.digit_bits;
   if (digitBits < 6 || digitBits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
+  pixelsPerThread = opt.pixels_per_thread == 0 ? 2 : opt.pixels_per_thread;
+  if (pixelsPerThread != 1 && pixelsPerThread != 2) throw Failure{SPLAT_ERR_INVALID, "pixels_per_thread must be 1 or 2"};
   SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
 
@@ -494,8 +498,13 @@ void Trainer::upload_targets(const uint8_t *const *targets, const size_t *bytes,
 
 // ---------------------------------------------------------------- recording
 
-void Trainer::mark(int stage) {
-  if (timing) SB_CUDA(cudaEventRecord(events[stage], stream));
+// Per-stage timing: a pair of events around each stage's kernels, so host
+// waits and small copies between stages are not counted.
+void Trainer::begin(int stage) {
+  if (timing) SB_CUDA(cudaEventRecord(events[2 * stage], stream));
+}
+void Trainer::end(int stage) {
+  if (timing) SB_CUDA(cudaEventRecord(events[2 * stage + 1], stream));
 }
 
 void Trainer::record_prepare() {
@@ -504,21 +513,24 @@ void Trainer::record_prepare() {
   SB_CUDA(cudaMemsetAsync(dReadback.get(), 0, sizeof(StepReadback), stream));
   StepReadback *rb = dReadback.get<StepReadback>();
   uint32_t *counters = rb->counters, *error = &rb->error;
-  mark(0);
+  begin(0);
   launch_preprocess(p, views, dViews.get<ViewSet>(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
                     oneSort ? nullptr : values.get<uint32_t>(), stream);
-  mark(1);
+  end(0);
+  begin(1);
   if (!oneSort) {
     depthInTmp = sort_pairs_u32(depthKeys.get<uint32_t>(), values.get<uint32_t>(), tmpKeys.get<uint32_t>(),
                                 tmpValues.get<uint32_t>(), n, n, nullptr, 0, 32, digitBits, sortScratchDepth.get(), error,
                                 stream) == 1;
   }
-  mark(2);
+  end(1);
+  begin(2);
   const uint32_t *itemKeys = oneSort ? depthKeys.get<uint32_t>() : (depthInTmp ? tmpKeys.get<uint32_t>() : depthKeys.get<uint32_t>());
   const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
   launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
                         offsets.get<uint32_t>(), counters, entryCapacity, scanScratch.get(), error, stream);
+  end(2);
 }
 
 void Trainer::record_forward() {
@@ -527,7 +539,7 @@ void Trainer::record_forward() {
   const uint32_t *itemKeys = oneSort ? depthKeys.get<uint32_t>() : (depthInTmp ? tmpKeys.get<uint32_t>() : depthKeys.get<uint32_t>());
   const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
-  mark(3);
+  begin(3);
   launch_bin_emit(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
                   offsets.get<uint32_t>(), entryCapacity, oneSort ? nullptr : entryKeys.get<uint32_t>(),
                   oneSort ? entryKeys.get<unsigned long long>() : nullptr, entryValues.get<uint32_t>(), error, stream);
@@ -547,34 +559,39 @@ void Trainer::record_forward() {
   launch_tile_ranges(oneSort ? nullptr : static_cast<const uint32_t *>(keys),
                      oneSort ? static_cast<const unsigned long long *>(keys) : nullptr, &counters[2], entryCapacity,
                      (uint32_t)views.totalTiles, ranges.get<uint2>(), error, stream);
-  mark(4);
+  end(3);
   RasterConfig cfg;
   cfg.exactMath = exactMath ? 1 : 0;
+  cfg.pixelsPerThread = pixelsPerThread;
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
+  begin(4);
   launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
                  stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
+  end(4);
 }
 
 void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   StepReadback *rb = dReadback.get<StepReadback>();
   uint32_t *error = &rb->error;
-  mark(5);
+  begin(5);
   launch_ssim(image.get<float4>(), target.get<uint32_t>(), views, dViews.get<ViewSet>(), fields.get<float4>(),
               partials.get<float2>(), stream);
   launch_loss(image.get<float4>(), target.get<uint32_t>(), fields.get<float4>(), views, dViews.get<ViewSet>(), opt.lambda_ssim,
               adjoint.get<float4>(), partials.get<float2>(), stream);
   launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, stream);
-  mark(6);
+  end(5);
   SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, stream));
   RasterConfig cfg;
   cfg.exactMath = exactMath ? 1 : 0;
+  cfg.pixelsPerThread = pixelsPerThread;
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
+  begin(6);
   launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
                   adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
                   stream);
-  mark(7);
+  end(6);
   ChainArgs args{};
   std::memcpy(&args, hArgs.get(), sizeof(ChainArgs));
   (void)mode;
@@ -586,12 +603,13 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   GradientsOut g{};
   for (int k = 0; k < 5; ++k) g.g[k] = grads[k].get<float>();
   const GradientsOut *gp = &g;
+  begin(7);
   launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
                shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
+  end(7);
 }
 
 void Trainer::record_readback() {
-  mark(8);
   SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
 }
 
@@ -736,7 +754,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
   if (timing) {
     for (int s = 0; s < kStages; ++s) {
       float ms = 0.f;
-      SB_CUDA(cudaEventElapsedTime(&ms, events[s], events[s + 1]));
+      SB_CUDA(cudaEventElapsedTime(&ms, events[2 * s], events[2 * s + 1]));
       stageTotals[s] += ms;
     }
     ++timedIterations;
@@ -805,6 +823,26 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
   set_sort(bestForm == 1, bestDigits);
   result.sort_form = bestForm;
   result.digit_bits = bestDigits;
+  // Then the rasterizer's layout with that sort.
+  const int oldLayout = pixelsPerThread;
+  int bestLayout = oldLayout;
+  double bestLayoutMs = 1e30;
+  for (int layout = 1; layout <= 2; ++layout) {
+    pixelsPerThread = layout;
+    splat_step_stats s{};
+    run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < repeats; ++r) run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
+    result.layout_ms[layout - 1] = ms;
+    if (ms < bestLayoutMs) {
+      bestLayoutMs = ms;
+      bestLayout = layout;
+    }
+  }
+  pixelsPerThread = bestLayout;
+  clear_graphs();
+  result.pixels_per_thread = bestLayout;
   if (out != nullptr) *out = result;
 }
 
@@ -898,6 +936,7 @@ void splat_trainer_options_default(splat_trainer_options *o) {
   o->exact_math = 1;
   o->use_graph = 0;
   o->digit_bits = 8;
+  o->pixels_per_thread = 2;
 }
 
 void splat_learning_rates_default(splat_learning_rates *r) {
