@@ -245,7 +245,8 @@ def chosen_options(splat):
 
 def plain_options(splat):
     return splat.TrainerOptions(sh_storage=splat.SH_F32, state_storage=splat.STATE_F32,
-                                sort_form=splat.SORT_DEPTH_THEN_TILE, exact_math=True, use_graph=False, digit_bits=8)
+                                sort_form=splat.SORT_DEPTH_THEN_TILE, exact_math=True, use_graph=False, digit_bits=8,
+                                forward_pixels_per_thread=1, backward_pixels_per_thread=1)
 
 
 def time_steps(torch, trainer, step_fn, steps: int, stream_handle: int) -> float:

@@ -90,9 +90,13 @@ typedef struct splat_trainer_options {
   int32_t exact_math;         /* 1: deterministic exp/log, bit-reproducible by the CPU restatement; 0: SFU */
   int32_t use_graph;          /* 1: capture the step as a CUDA graph, entry count kept on the device */
   int32_t digit_bits;         /* radix digit width, 6..8 (0 picks 8) */
-  int32_t pixels_per_thread;  /* 2: 8x8-pixel warps, two pixels per lane (0 picks 2); 1: the reference's 2x16-pixel
-                                 warps. The fixed-point backward always uses 1, as its sums follow the reference's
-                                 32-lane groups. */
+  int32_t forward_pixels_per_thread;  /* compositing layout. 1: the reference's 2x16-pixel warps (0 picks 1);
+                                         2: 8x8-pixel warps, two pixels per lane */
+  int32_t backward_pixels_per_thread; /* float backward layout, 1 or 2 as above (0 picks 2). The fixed-point
+                                         backward always uses 1, as its sums follow the reference's 32-lane
+                                         groups. */
+  int32_t split_step;         /* 0: a one-view Adam step is one fused kernel (chain rule, geometry and SH
+                                 step); 1: three kernels, as for batches. The results are the same bits. */
 } splat_trainer_options;
 
 /* LearningRates (src/train/trainer.hpp:51-61); trust_region must be 0. */
@@ -219,9 +223,10 @@ int splat_trainer_timings(splat_trainer *trainer, const char **names, double *ms
 typedef struct splat_autotune_result {
   int32_t sort_form;    /* the splat_sort_form kept */
   int32_t digit_bits;   /* the radix digit width kept */
-  int32_t pixels_per_thread; /* the rasterizer layout kept */
-  double ms[2][3];      /* milliseconds per gradient pass, [sort form][digit bits - 6], with 2 pixels per thread */
-  double layout_ms[2];  /* milliseconds per gradient pass with 1 and 2 pixels per thread, best sort */
+  int32_t forward_pixels_per_thread;  /* the compositing layout kept */
+  int32_t backward_pixels_per_thread; /* the backward layout kept */
+  double ms[2][3];         /* milliseconds per gradient pass, [sort form][digit bits - 6], starting layouts */
+  double layout_ms[2][2];  /* milliseconds per gradient pass, [forward pixels - 1][backward pixels - 1], best sort */
 } splat_autotune_result;
 
 /* The autotuner (new in this library; the reference has fixed 16x16 tiles and

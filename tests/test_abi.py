@@ -42,6 +42,7 @@ def test_defaults_are_the_reference_defaults():
     s._lib.splat_trainer_options_default(ctypes.byref(o))
     assert abs(o.lambda_ssim - 0.2) < 1e-7 and abs(o.near_plane - 0.01) < 1e-9 and o.selective_adam == 1
     assert o.memory_budget == 2**64 - 1 and o.force_fixed_point == 0
+    assert o.forward_pixels_per_thread == 1 and o.backward_pixels_per_thread == 2 and o.digit_bits == 8
     r = s._Rates()
     s._lib.splat_learning_rates_default(ctypes.byref(r))
     got = [r.position, r.scale, r.rotation, r.opacity, r.sh, r.sh_rest_scale, r.trust_region]

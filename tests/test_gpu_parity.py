@@ -234,6 +234,34 @@ def test_graph_form_matches_plain_form(splat, oracle):
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("sh_storage,state_storage,selective", [
+    ("SH_F16", "STATE_BF16_PAIR", True),
+    ("SH_BF16", "STATE_BF16_PAIR", False),
+    ("SH_F32", "STATE_F32", True),
+])
+def test_fused_step_matches_split_step(splat, oracle, sh_storage, state_storage, selective):
+    # The one-kernel step and the three-kernel step: the same bits, including
+    # non-selective Adam (momentum on unseen Gaussians) and the penalties.
+    # Fixed-point sums, so that both runs start from the same gradients (float
+    # atomics add in an order that changes from run to run).
+    view = oracle.train_camera(96, 80)
+    target = oracle.smooth_target(96, 80, 3)
+    cloud = oracle.random_cloud(700, 3, 41)
+    rates = splat.LearningRates(position=1e-3)
+    results = []
+    for split in (False, True):
+        opts = splat.TrainerOptions(sh_storage=getattr(splat, sh_storage), state_storage=getattr(splat, state_storage),
+                                    selective_adam=selective, force_fixed_point=True, split_step=split,
+                                    opacity_reg=0.0 if selective else 0.01, scale_reg=0.0 if selective else 0.01)
+        t = splat.Trainer(to_cloud(cloud), opts)
+        t.set_active_sh_degree(2)
+        losses = [t.step(to_camera(view), target, rates).loss for _ in range(4)]
+        results.append((losses, t.cloud()))
+    assert results[0][0] == results[1][0]
+    for name in ("positions", "scales", "rotations", "opacities", "sh"):
+        np.testing.assert_array_equal(getattr(results[0][1], name), getattr(results[1][1], name), err_msg=name)
+
+
 def test_training_lowers_the_loss(splat, oracle):
     # In the spirit of tests/test_train.cpp:493-520: fit a rendered view.
     view = oracle.train_camera(96, 72)
@@ -336,7 +364,8 @@ def test_pixel_layouts_agree(splat, oracle, exact):
     cloud = oracle.random_cloud(500, 1, 37)
     out = []
     for layout in (1, 2):
-        t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(exact_math=exact, pixels_per_thread=layout))
+        t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(exact_math=exact, forward_pixels_per_thread=layout,
+                                                                backward_pixels_per_thread=layout))
         image = t.render(to_camera(view))
         stats = t.compute_gradients(to_camera(view), target)
         out.append((image, stats, t.gradients()))

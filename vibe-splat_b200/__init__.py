@@ -69,7 +69,9 @@ class _Options(ctypes.Structure):
         ("exact_math", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
         ("digit_bits", ctypes.c_int32),
-        ("pixels_per_thread", ctypes.c_int32),
+        ("forward_pixels_per_thread", ctypes.c_int32),
+        ("backward_pixels_per_thread", ctypes.c_int32),
+        ("split_step", ctypes.c_int32),
     ]
 
 
@@ -139,8 +141,9 @@ _lib.splat_trainer_stream.argtypes = [_P, ctypes.POINTER(_P)]
 
 
 class _Autotune(ctypes.Structure):
-    _fields_ = [("sort_form", ctypes.c_int32), ("digit_bits", ctypes.c_int32), ("pixels_per_thread", ctypes.c_int32),
-                ("ms", (ctypes.c_double * 3) * 2), ("layout_ms", ctypes.c_double * 2)]
+    _fields_ = [("sort_form", ctypes.c_int32), ("digit_bits", ctypes.c_int32),
+                ("forward_pixels_per_thread", ctypes.c_int32), ("backward_pixels_per_thread", ctypes.c_int32),
+                ("ms", (ctypes.c_double * 3) * 2), ("layout_ms", (ctypes.c_double * 2) * 2)]
 
 
 _lib.splat_trainer_autotune.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_int32,
@@ -320,7 +323,9 @@ class TrainerOptions:
     exact_math: bool = True
     use_graph: bool = False
     digit_bits: int = 8
-    pixels_per_thread: int = 2
+    forward_pixels_per_thread: int = 1
+    backward_pixels_per_thread: int = 2
+    split_step: bool = False
 
     def _c(self) -> _Options:
         o = _Options()
@@ -335,7 +340,9 @@ class TrainerOptions:
         o.memory_budget = int(self.memory_budget)
         o.sh_storage, o.state_storage, o.sort_form = self.sh_storage, self.state_storage, self.sort_form
         o.exact_math, o.use_graph, o.digit_bits = int(self.exact_math), int(self.use_graph), self.digit_bits
-        o.pixels_per_thread = self.pixels_per_thread
+        o.forward_pixels_per_thread = self.forward_pixels_per_thread
+        o.backward_pixels_per_thread = self.backward_pixels_per_thread
+        o.split_step = int(self.split_step)
         return o
 
 
@@ -486,14 +493,17 @@ class Trainer:
         return StepStats._from(s)
 
     def autotune(self, camera: Camera, target, repeats: int = 3) -> dict:
-        """Times each tile-sort form and radix digit width on this view with
-        gradient passes (no parameter changes) and keeps the fastest."""
+        """Times each tile-sort form and radix digit width, then each forward and
+        backward pixel layout, on this view with gradient passes (no parameter
+        changes) and keeps the fastest."""
         t, p, n = _target_ptr(target)
         r = _Autotune()
         _check(_lib.splat_trainer_autotune(self._h, ctypes.byref(camera._c()), p, n, int(repeats), ctypes.byref(r)))
-        return {"sort_form": r.sort_form, "digit_bits": r.digit_bits, "pixels_per_thread": r.pixels_per_thread,
+        return {"sort_form": r.sort_form, "digit_bits": r.digit_bits,
+                "forward_pixels_per_thread": r.forward_pixels_per_thread,
+                "backward_pixels_per_thread": r.backward_pixels_per_thread,
                 "ms": {f"form{f}/digits{d + 6}": r.ms[f][d] for f in range(2) for d in range(3)},
-                "layout_ms": {"1px": r.layout_ms[0], "2px": r.layout_ms[1]}}
+                "layout_ms": {f"fwd{f + 1}/bwd{b + 1}": r.layout_ms[f][b] for f in range(2) for b in range(2)}}
 
     def stream(self) -> int:
         """The cudaStream_t the trainer runs on, as an integer handle."""

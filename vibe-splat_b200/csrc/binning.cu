@@ -49,12 +49,33 @@ __device__ __forceinline__ bool splat_reaches_tile(const float4 q, const float4 
   return least <= reach * 1.001f + 1e-3f;
 }
 
-__device__ __forceinline__ uint32_t count_tiles(const float4 q, const float4 ce, float reach, int gridW, int gridH) {
-  const TileRect t = splat_tiles(ce, gridW, gridH);
+// Splats whose tile rectangle holds more than this many tiles are tested by a
+// whole warp, one tile per lane, so that no thread walks a large splat's
+// rectangle alone while its block (and, through the scan, every later block)
+// waits for it.
+constexpr uint32_t kWarpTiles = 16;
+
+__device__ __forceinline__ uint32_t rect_area(const TileRect &t) { return (t.x1 - t.x0 + 1u) * (t.y1 - t.y0 + 1u); }
+
+__device__ __forceinline__ uint32_t count_tiles(const float4 q, const float4 ce, float reach, const TileRect &t) {
   uint32_t n = 0;
   for (uint32_t y = t.y0; y <= t.y1; ++y)
     for (uint32_t x = t.x0; x <= t.x1; ++x) n += splat_reaches_tile(q, ce, reach, x, y) ? 1u : 0u;
   return n;
+}
+
+// The tiles of the rectangle in row-major order, 32 at a time: lane l tests
+// tile base + l. Returns the lanes whose tile the splat reaches.
+__device__ __forceinline__ uint32_t warp_reach(const float4 q, const float4 ce, float reach, const TileRect &t, uint32_t width,
+                                               uint32_t area, uint32_t base, uint32_t lane, uint32_t &x, uint32_t &y) {
+  const uint32_t li = base + lane;
+  bool hit = false;
+  if (li < area) {
+    y = t.y0 + li / width;
+    x = t.x0 + li % width;
+    hit = splat_reaches_tile(q, ce, reach, x, y);
+  }
+  return __ballot_sync(0xFFFFFFFFu, hit);
 }
 
 __device__ __forceinline__ unsigned long long load_u64(const unsigned long long *p) {
@@ -91,13 +112,30 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
-    uint32_t c = 0;
+    uint32_t c = 0, s = 0;
+    bool big = false;
     if (r < items && itemKeys[r] != kInvisible) {
-      const uint32_t s = itemSplat != nullptr ? itemSplat[r] : r;
+      s = itemSplat != nullptr ? itemSplat[r] : r;
       const ViewParams &cam = views.v[item_view(s, n, views.count)];
       const Splat sp = splats[s];
-      c = count_tiles(sp.conicOpacity, sp.centerExtent, reach[s], cam.gridW, cam.gridH);
+      const TileRect rect = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+      big = rect_area(rect) > kWarpTiles;
+      if (!big) c = count_tiles(sp.conicOpacity, sp.centerExtent, reach[s], rect);
       ++visible;
+    }
+    // Large rectangles: the whole warp, one after another.
+    for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
+      const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
+      const uint32_t bs = __shfl_sync(0xFFFFFFFFu, s, src);
+      const ViewParams &cam = views.v[item_view(bs, n, views.count)];
+      const Splat sp = splats[bs];
+      const float rc = reach[bs];
+      const TileRect rect = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+      const uint32_t width = rect.x1 - rect.x0 + 1u, area = rect_area(rect);
+      uint32_t total = 0, x = 0, y = 0;
+      for (uint32_t base = 0; base < area; base += 32u)
+        total += (uint32_t)__popc(warp_reach(sp.conicOpacity, sp.centerExtent, rc, rect, width, area, base, lane, x, y));
+      if (lane == src) c = total;
     }
     counts[j] = c;
     threadSum += c;
@@ -181,32 +219,59 @@ __global__ void __launch_bounds__(256)
                const uint32_t *__restrict__ offsets, uint32_t capacity, uint32_t *__restrict__ tileKeys32,
                unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues, uint32_t *error) {
   const ViewSet &views = *viewsPtr;
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= items) return;
-  const uint32_t depthKey = itemKeys[r];
-  if (depthKey == kInvisible) return;
-  const uint32_t s = itemSplat != nullptr ? itemSplat[r] : r;
-  const ViewParams &cam = views.v[item_view(s, n, views.count)];
-  const Splat sp = splats[s];
-  const float rc = reach[s];
-  const TileRect t = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
-  uint32_t slot = offsets[r];
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
+  // Whole warps stay to the end: large rectangles are emitted by all 32 lanes.
+  const bool valid = r < items && itemKeys[r] != kInvisible;
+  const uint32_t depthKey = valid ? itemKeys[r] : 0u;
+  const uint32_t s = valid ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
   bool overflow = false;
-  for (uint32_t y = t.y0; y <= t.y1; ++y) {
-    for (uint32_t x = t.x0; x <= t.x1; ++x) {
-      if (!splat_reaches_tile(sp.conicOpacity, sp.centerExtent, rc, x, y)) continue;
-      if (slot < capacity) {
-        const uint32_t tileId = y * (uint32_t)cam.gridW + x;
-        if (tileKeys64 != nullptr) {
-          tileKeys64[slot] = ((unsigned long long)((uint32_t)cam.tileBase + tileId) << 32) | depthKey;
-        } else {
-          tileKeys32[slot] = tileId;
-        }
-        entryValues[slot] = s;
+  auto put = [&](uint32_t slot, const ViewParams &cam, uint32_t x, uint32_t y, uint32_t key, uint32_t splat) {
+    if (slot < capacity) {
+      const uint32_t tileId = y * (uint32_t)cam.gridW + x;
+      if (tileKeys64 != nullptr) {
+        tileKeys64[slot] = ((unsigned long long)((uint32_t)cam.tileBase + tileId) << 32) | key;
       } else {
-        overflow = true;
+        tileKeys32[slot] = tileId;
       }
-      ++slot;
+      entryValues[slot] = splat;
+    } else {
+      overflow = true;
+    }
+  };
+  bool big = false;
+  if (valid) {
+    const ViewParams &cam = views.v[item_view(s, n, views.count)];
+    const Splat sp = splats[s];
+    const TileRect t = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    big = rect_area(t) > kWarpTiles;
+    if (!big) {
+      const float rc = reach[s];
+      uint32_t slot = offsets[r];
+      for (uint32_t y = t.y0; y <= t.y1; ++y) {
+        for (uint32_t x = t.x0; x <= t.x1; ++x) {
+          if (!splat_reaches_tile(sp.conicOpacity, sp.centerExtent, rc, x, y)) continue;
+          put(slot++, cam, x, y, depthKey, s);
+        }
+      }
+    }
+  }
+  // Large rectangles: row-major order kept by counting the lower lanes' hits.
+  for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
+    const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
+    const uint32_t bs = __shfl_sync(0xFFFFFFFFu, s, src);
+    const uint32_t key = __shfl_sync(0xFFFFFFFFu, depthKey, src);
+    const uint32_t first = __shfl_sync(0xFFFFFFFFu, r, src);
+    const ViewParams &cam = views.v[item_view(bs, n, views.count)];
+    const Splat sp = splats[bs];
+    const float rc = reach[bs];
+    const TileRect t = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    const uint32_t width = t.x1 - t.x0 + 1u, area = rect_area(t);
+    uint32_t slot = offsets[first];
+    for (uint32_t base = 0; base < area; base += 32u) {
+      uint32_t x = 0, y = 0;
+      const uint32_t hits = warp_reach(sp.conicOpacity, sp.centerExtent, rc, t, width, area, base, lane, x, y);
+      if ((hits >> lane) & 1u) put(slot + (uint32_t)__popc(hits & ((1u << lane) - 1u)), cam, x, y, key, bs);
+      slot += (uint32_t)__popc(hits);
     }
   }
   if (overflow) atomicOr(error, kErrEntryOverflow);

@@ -72,7 +72,9 @@ void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *ti
 
 struct RasterConfig {
   int exactMath = 1;   // deterministic exp/log (bit-reproducible by the CPU restatement)
-  int pixelsPerThread = 2; // 2: 8x8-pixel warps, two pixels per lane; 1: the reference's 2x16-pixel warps
+  // Pixels per thread. 1: the reference's 2x16-pixel warps; 2: 8x8-pixel warps, two pixels per lane.
+  int forwardPixels = 1;
+  int backwardPixels = 2; // float backward only; the fixed-point sums keep 1
   float background[3] = {0.f, 0.f, 0.f};
 };
 
@@ -116,6 +118,7 @@ struct ChainArgs {
   float beta1, beta2, epsilon, correction1, correction2;
   uint32_t seed;
   float opacityReg, scaleReg; // per Gaussian: the option over the count
+  bool splitStep;      // host side: three kernels even for one view
 };
 struct OptimState {
   void *state[5];      // per group: F32 {m, v} pairs or BF16 pair words

@@ -6,11 +6,13 @@
 // shaders/train_sh_step.comp:19-70 (the SH step, with half_stochastic,
 // train_step.glsl:140-150).
 //
-// One thread per Gaussian does all of it, the SH step included: SH lives in
-// planes (coefficient-major), so neighbouring threads touch neighbouring words
-// for every coefficient, which is what the reference's separate one-thread-
-// per-word SH pass was for. With several views in a batch, the chain rule runs
-// per view and the gradients are summed before one step.
+// SH lives in planes (coefficient-major), so neighbouring threads touch
+// neighbouring words for every coefficient, which is what the reference's
+// separate one-thread-per-word SH pass was for. A one-view Adam step is one
+// kernel, one thread per Gaussian (k_chain_step). The other cases run the
+// chain rule (k_chain), then Adam on the geometry (k_adam_geometry) and the
+// SH step (k_sh_step); with several views in a batch the chain rule runs per
+// view and the gradients are summed before one step.
 // Out of scope and rejected by the host: the Mip 2D filter, the 3D filter,
 // SH dropout, second-order steps, pose gradients, position noise.
 #include <cuda_bf16.h>
@@ -165,13 +167,15 @@ __device__ __forceinline__ void basis_gradient_one(int k, float x, float y, floa
 }
 
 // The chain rule of one view for Gaussian i (train_gradient.comp:165-275):
-// adds its position, scale, rotation and opacity gradients, and returns the
-// colour gradient where the colour was not clamped and the view direction.
-template <ShStore S>
-__device__ __forceinline__ void chain_view(const Params &p, uint32_t i, const ViewParams &cam, const float raw[kRawPerSplat],
-                                           const float4 col, const float pos[3], const float logScale[3], float opacity,
-                                           float4 rq, float gP[3], float gScale[3], float gRot[4], float &gOpacity,
-                                           float gColour[3], float dir[3]) {
+// adds its scale, rotation and opacity gradients, and returns the position
+// gradient of this view without the view-direction term (gPv), the colour
+// gradient where the colour was not clamped, the view direction and the
+// distance. The direction term needs the SH coefficients: add_direction_term
+// finishes gPv with it.
+__device__ __forceinline__ void chain_view(const ViewParams &cam, const float raw[kRawPerSplat], const float4 col,
+                                           const float pos[3], const float logScale[3], float opacity, float4 rq,
+                                           float gPv[3], float gScale[3], float gRot[4], float &gOpacity, float gColour[3],
+                                           float dir[3], float &distance) {
   const float px = pos[0], py = pos[1], pz = pos[2];
   const float quatLength = sqrtf(fmaf(rq.w, rq.w, fmaf(rq.z, rq.z, fmaf(rq.y, rq.y, rq.x * rq.x))));
   float q[4] = {1.f, 0.f, 0.f, 0.f};
@@ -229,7 +233,6 @@ __device__ __forceinline__ void chain_view(const Params &p, uint32_t i, const Vi
   gT[0] += 2.0f * trace_term(G, dJx, X, J);
   gT[1] += 2.0f * trace_term(G, dJy, X, J);
   gT[2] += 2.0f * trace_term(G, dJz, X, J);
-  float gPv[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) gPv[c] = fmaf(Rv[2][c], gT[2], fmaf(Rv[1][c], gT[1], Rv[0][c] * gT[0]));
 
@@ -286,30 +289,27 @@ __device__ __forceinline__ void chain_view(const Params &p, uint32_t i, const Vi
   gColour[1] = col.y > 0.0f ? raw[7] : 0.0f;
   gColour[2] = col.z > 0.0f ? raw[8] : 0.0f;
   const float ddx = px - cam.pos[0], ddy = py - cam.pos[1], ddz = pz - cam.pos[2];
-  const float distance = sqrtf(fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx)));
+  distance = sqrtf(fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx)));
   dir[0] = ddx / distance;
   dir[1] = ddy / distance;
   dir[2] = ddz / distance;
-  // Position also changes the view direction, and with it the colour.
-  if (cam.activeDegree > 0) {
-    float gDir[3] = {0.f, 0.f, 0.f};
+}
+
+// Position also changes the view direction, and with it the colour: the
+// gradient through the coefficients 1..active-1 of each channel, in order.
+// c[3] are coefficient k's values before any step.
+__device__ __forceinline__ void direction_term(int k, const float c[3], const float gColour[3], const float dir[3], float gDir[3]) {
+  const float d = fmaf(gColour[2], c[2], fmaf(gColour[1], c[1], gColour[0] * c[0]));
+  float bg[3];
+  basis_gradient_one(k, dir[0], dir[1], dir[2], bg);
 #pragma unroll
-    for (int k = 1; k < kMaxCoeffs; ++k) {
-      if (k < cam.activeCoeffs) {
-        const float c0 = sh_coefficient<S>(p, i, k, 0), c1 = sh_coefficient<S>(p, i, k, 1), c2 = sh_coefficient<S>(p, i, k, 2);
-        const float d = fmaf(gColour[2], c2, fmaf(gColour[1], c1, gColour[0] * c0));
-        float bg[3];
-        basis_gradient_one(k, dir[0], dir[1], dir[2], bg);
+  for (int a = 0; a < 3; ++a) gDir[a] = fmaf(d, bg[a], gDir[a]);
+}
+
+__device__ __forceinline__ void add_direction_term(const float gDir[3], const float dir[3], float distance, float gPv[3]) {
+  const float dd = fmaf(dir[2], gDir[2], fmaf(dir[1], gDir[1], dir[0] * gDir[0]));
 #pragma unroll
-        for (int c = 0; c < 3; ++c) gDir[c] = fmaf(d, bg[c], gDir[c]);
-      }
-    }
-    const float dd = fmaf(dir[2], gDir[2], fmaf(dir[1], gDir[1], dir[0] * gDir[0]));
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gPv[c] += (gDir[c] - dir[c] * dd) / distance;
-  }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
+  for (int c = 0; c < 3; ++c) gPv[c] += (gDir[c] - dir[c] * dd) / distance;
 }
 
 // Geometry part of the chain rule and Adam for positions, scales, rotations
@@ -382,8 +382,21 @@ __global__ void __launch_bounds__(128, 4) k_chain(Params p, const ViewSet *__res
       st[1] = b;
     }
     if (args.mode == ChainMode::Statistics) continue;
-    float gColour[3], dir[3];
-    chain_view<S>(p, i, cam, raw, col, pos, logScale, opacity, rq, gP, gScale, gRot, gOpacity, gColour, dir);
+    float gColour[3], dir[3], gPv[3], distance;
+    chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
+    if (cam.activeDegree > 0) {
+      float gDir[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 1; k < kMaxCoeffs; ++k) {
+        if (k < cam.activeCoeffs) {
+          const float c[3] = {sh_coefficient<S>(p, i, k, 0), sh_coefficient<S>(p, i, k, 1), sh_coefficient<S>(p, i, k, 2)};
+          direction_term(k, c, gColour, dir, gDir);
+        }
+      }
+      add_direction_term(gDir, dir, distance, gPv);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
     sg[0] = make_float4(gColour[0], gColour[1], gColour[2], __uint_as_float((uint32_t)cam.activeCoeffs));
     sg[1] = make_float4(dir[0], dir[1], dir[2], 0.0f);
   }
@@ -555,6 +568,197 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
   }
 }
 
+// One view, Adam step: the chain rule, Adam on the geometry and the SH step
+// in one pass, one thread per Gaussian. The SH coefficients are read once,
+// for the direction term and for their own step, and no gradient leaves
+// registers. Element by element the arithmetic, the hash indices and the
+// order of the sums are those of k_chain, k_adam_geometry and k_sh_step, so
+// the results are the same bits. Loads are issued a chunk of coefficients at a
+// time ahead of the arithmetic (the stores to the same arrays would otherwise
+// keep each load behind the previous element's store).
+constexpr int kStepChunk = 4;
+
+__device__ __forceinline__ void load_state(const void *st, StateStore store, uint32_t count, uint32_t at, float &m, float &v,
+                                           uint32_t &word) {
+  if (store == StateStore::F32) {
+    m = static_cast<const float *>(st)[at];
+    v = static_cast<const float *>(st)[count + at];
+    word = 0u;
+  } else {
+    word = static_cast<const uint32_t *>(st)[at];
+    m = bf16_load(word, 0);
+    v = bf16_load(word, 1);
+  }
+}
+
+__device__ __forceinline__ void store_state(void *st, StateStore store, uint32_t count, uint32_t at, float m, float v,
+                                            uint32_t word, uint32_t hashIndex, uint32_t seed) {
+  if (store == StateStore::F32) {
+    static_cast<float *>(st)[at] = m;
+    static_cast<float *>(st)[count + at] = v;
+  } else {
+    static_cast<uint32_t *>(st)[at] = bf16_store(bf16_store(word, 0, bf16_round(m)), 1, bf16_stochastic(v, hashIndex, seed));
+  }
+}
+
+template <ShStore S, bool FIXED>
+__global__ void __launch_bounds__(128, 4) k_chain_step(Params p, const ViewSet *__restrict__ viewsPtr, const void *__restrict__ rawIn,
+                                                       const Splat *__restrict__ splats, const ChainArgs *__restrict__ argsPtr,
+                                                       OptimState state, float *__restrict__ densifyStats, const uint32_t *error) {
+  const ViewParams &cam = viewsPtr->v[0];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n) return;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const ChainArgs args = *argsPtr;
+  const uint32_t n = p.n;
+  const AdamArgs a = adam_args(args);
+
+  const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
+  const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
+  const float rawOpacity = p.opacities[i];
+  const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
+  float raw[kRawPerSplat];
+  bool touched = false;
+  {
+    const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
+    uint32_t words[16];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4 w4 = r4[q];
+      words[q * 4] = w4.x;
+      words[q * 4 + 1] = w4.y;
+      words[q * 4 + 2] = w4.z;
+      words[q * 4 + 3] = w4.w;
+    }
+#pragma unroll
+    for (int k = 0; k < kRawPerSplat; ++k) {
+      raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
+      touched = touched || raw[k] != 0.0f;
+    }
+  }
+  const float opacity = 1.0f / (1.0f + splat_expf(-rawOpacity));
+
+  float gP[3] = {0.f, 0.f, 0.f}, gScale[3] = {0.f, 0.f, 0.f}, gRot[4] = {0.f, 0.f, 0.f, 0.f}, gOpacity = 0.f;
+  float gColour[3] = {0.f, 0.f, 0.f}, dir[3] = {0.f, 0.f, 0.f}, gPv[3] = {0.f, 0.f, 0.f}, distance = 1.0f;
+  if (touched) {
+    const float4 col = splats[i].colorRadius;
+    if (args.statistics) {
+      float4 *st = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
+      float4 sa = st[0], sb = st[1];
+      const float hx = 0.5f * cam.widthF, hy = 0.5f * cam.heightF;
+      const float ax = raw[1] * hx, ay = raw[2] * hy;
+      sa.x += sqrtf(fmaf(ay, ay, ax * ax));
+      sa.y += 1.0f;
+      sa.z = fmaxf(sa.z, col.w);
+      sa.w += raw[9] * 3.0f * cam.widthF * cam.heightF;
+      const float bx = raw[10] * hx, by = raw[11] * hy;
+      sb.x += sqrtf(fmaf(by, by, bx * bx));
+      st[0] = sa;
+      st[1] = sb;
+    }
+    chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
+  }
+
+  // The SH step, with the direction term from the coefficients before it.
+  const bool stepZeros = !args.selective;
+  const int active = touched ? cam.activeCoeffs : 0;
+  float gDir[3] = {0.f, 0.f, 0.f};
+  if (touched || stepZeros) {
+    const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
+    const uint32_t count = n * shFloats;
+#pragma unroll
+    for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStepChunk) {
+      if (k0 >= p.shCoeffs) break;
+      float value[kStepChunk][3], m[kStepChunk][3], vv[kStepChunk][3];
+      uint32_t word[kStepChunk][3];
+#pragma unroll
+      for (int kk = 0; kk < kStepChunk; ++kk) {
+        const int k = k0 + kk;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          value[kk][c] = m[kk][c] = vv[kk][c] = 0.0f;
+          word[kk][c] = 0u;
+          if (k >= p.shCoeffs) continue;
+          const uint32_t t = (uint32_t)(k * 3 + c) * n + i;
+          value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3u * n);
+          load_state(state.state[4], state.store, count, t, m[kk][c], vv[kk][c], word[kk][c]);
+        }
+      }
+      if (touched && cam.activeDegree > 0) {
+#pragma unroll
+        for (int kk = 0; kk < kStepChunk; ++kk) {
+          const int k = k0 + kk;
+          if (k >= 1 && k < active) direction_term(k, value[kk], gColour, dir, gDir);
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < kStepChunk; ++kk) {
+        const int k = k0 + kk;
+        if (k >= p.shCoeffs) continue;
+        const float b = k < active ? basis_one(k, dir[0], dir[1], dir[2]) : 0.0f;
+        const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float g = k < active ? fmaf(b, gColour[c], 0.0f) : 0.0f;
+          if (g == 0.0f && !stepZeros) continue;
+          const uint32_t plane = (uint32_t)(k * 3 + c);
+          const uint32_t t = plane * n + i;
+          const uint32_t hashIndex = (i * shFloats + plane) * 5u + 4u;
+          adam(value[kk][c], m[kk][c], vv[kk][c], g, rate, a);
+          store_state(state.state[4], state.store, count, t, m[kk][c], vv[kk][c], word[kk][c], hashIndex, a.seed);
+          if (k == 0) {
+            p.shDc[t] = value[kk][c];
+          } else {
+            store_sh_rest<S>(p.shRest, t - 3u * n, value[kk][c], hashIndex, args.seed);
+          }
+        }
+      }
+    }
+  }
+  if (touched) {
+    if (cam.activeDegree > 0) add_direction_term(gDir, dir, distance, gPv);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
+  }
+  // The penalties (3DGS-MCMC) apply to every Gaussian, seen or not.
+  if (args.opacityReg > 0.0f || args.scaleReg > 0.0f) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gScale[c] += args.scaleReg * splat_expf(logScale[c]);
+    gOpacity += args.opacityReg * opacity * (1.0f - opacity);
+  }
+
+  // Adam on the 11 geometry elements: [positions 3 | scales 3 | rotations 4 | opacity 1].
+  float gv[11], value[11], m[11], vv[11];
+  uint32_t word[11];
+#pragma unroll
+  for (int e = 0; e < 11; ++e) {
+    const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+    const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+    const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+    const uint32_t idx = i * per + (uint32_t)a0;
+    gv[e] = group == 0 ? gP[a0] : group == 1 ? gScale[a0] : group == 2 ? gRot[a0] : gOpacity;
+    value[e] = group == 0 ? pos[a0] : group == 1 ? logScale[a0] : group == 3 ? rawOpacity
+             : a0 == 0 ? rq.x : a0 == 1 ? rq.y : a0 == 2 ? rq.z : rq.w;
+    m[e] = vv[e] = 0.0f;
+    word[e] = 0u;
+    if (gv[e] == 0.0f && args.selective) continue;
+    load_state(state.state[group], state.store, per * n, idx, m[e], vv[e], word[e]);
+  }
+#pragma unroll
+  for (int e = 0; e < 11; ++e) {
+    const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+    const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+    const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+    const uint32_t idx = i * per + (uint32_t)a0;
+    // A parameter with a zero gradient is left alone when selective.
+    if (gv[e] == 0.0f && args.selective) continue;
+    adam(value[e], m[e], vv[e], gv[e], args.rates[group], a);
+    store_state(state.state[group], state.store, per * n, idx, m[e], vv[e], word[e], idx * 5u + (uint32_t)group, a.seed);
+    float *values = group == 0 ? p.positions : group == 1 ? p.scales : group == 2 ? p.rotations : p.opacities;
+    values[idx] = value[e];
+  }
+}
+
 template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                     const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
@@ -563,6 +767,14 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
   const bool store = args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
   const bool multi = views.count > 1;
+  // The fused form indexes the F32 SH state (two planes of n * 48 floats) in 32 bits.
+  if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.n * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
+    if (args.fixedPoint)
+      k_chain_step<S, true><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+    else
+      k_chain_step<S, false><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+    return;
+  }
 #define SB_CHAIN(F, M) \
   k_chain<S, F, M><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, g, store, shGrad, densifyStats, error)
   if (args.fixedPoint) {

@@ -131,6 +131,31 @@ __device__ __forceinline__ Staged stage_checked(const Splat *__restrict__ splats
   return stage(splats[s], s, geo.x0, geo.y0, geo.x1, geo.y1);
 }
 
+// Per-warp lists of the staged splats, as bitmaps: word w of warp v has bit b
+// set when splat 32 w + b reaches a pixel of warp v's block. The warps then
+// walk only their own splats; a splat that no pixel of the warp can take is
+// one no lane would have taken, so nothing else changes. Every lane of the
+// staging warp calls this (mask 0 for lanes without a splat); warps of the
+// 1-pixel layout cover two rows of 16, those of the 2-pixel layout 8x8.
+template <int WARPS>
+__device__ __forceinline__ void publish_cover(uint32_t mask, uint32_t word, uint32_t lane, uint32_t (*cover)[kBatch / 32]) {
+  uint32_t mine = 0;
+#pragma unroll
+  for (int w = 0; w < WARPS; ++w) {
+    uint32_t cols, rows;
+    if (WARPS == 8) {
+      cols = 0xFFFFu;
+      rows = 3u << (16 + 2 * w);
+    } else {
+      cols = 0xFFu << (8 * (w & 1));
+      rows = 0xFFu << (16 + 8 * (w >> 1));
+    }
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, (mask & cols) != 0u && (mask & rows) != 0u);
+    if (lane == (uint32_t)w) mine = b;
+  }
+  if (lane < (uint32_t)WARPS) cover[lane][word] = mine;
+}
+
 template <class M>
 __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
                                                          const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
@@ -138,15 +163,15 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
                                                          uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
+  __shared__ uint32_t s_cover[kTilePixels / 32][kBatch / 32];
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
   const int tile = blockIdx.x;
   const TileGeometry geo = tile_geometry(views, tile);
   const ViewParams &cam = views.v[geo.view];
-  const uint32_t t = threadIdx.x, lx = t & 15u, ly = t >> 4;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5, lx = t & 15u, ly = t >> 4;
   const uint32_t x = geo.x0 + lx, y = geo.y0 + ly;
   const bool inside = x < (uint32_t)cam.width && y < (uint32_t)cam.height;
   const uint32_t myBits = (1u << lx) | (1u << (16 + ly));
-  const uint32_t warpRows = 3u << (16 + 2 * (t >> 5));
   const float pxf = (float)x + 0.5f, pyf = (float)y + 0.5f;
 
   const uint2 range = ranges[tile];
@@ -157,35 +182,41 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
     const uint32_t count = min((uint32_t)kBatch, end - range.x);
     end -= count;
     if (__syncthreads_count(done) == kTilePixels) break;
+    uint32_t stagedMask = 0u;
     if (t < count) {
-      const uint32_t s = entryValues[end + t];
-      s_batch[t] = stage_checked(splats, s, splatLimit, geo, error);
+      const Staged st = stage_checked(splats, entryValues[end + t], splatLimit, geo, error);
+      s_batch[t] = st;
+      stagedMask = st.mask;
     }
+    publish_cover<kTilePixels / 32>(stagedMask, warp, lane, s_cover);
     __syncthreads();
-    if (done) continue;
-    for (int k = (int)count - 1; k >= 0; --k) {
-      const Staged &s = s_batch[k];
-      const uint32_t mask = s.mask;
-      if ((mask & warpRows) == 0u || (mask & 0xFFFFu) == 0u) continue; // warp-uniform
-      if ((mask & myBits) != myBits) continue;
-      const float dx = pxf - s.cx, dy = pyf - s.cy;
-      const float power = splat_power(s, dx, dy);
-      if (power > 0.0f) continue;
-      const float alpha = fminf(kAlphaMax, s.opacity * M::exp(power));
-      if (!(alpha >= kAlphaMin)) continue;
-      const float oneMinus = 1.0f - alpha;
-      const float logRest = M::log(oneMinus);
-      if (logT + logRest < kLogMinTransmittance) {
-        stop = end + (uint32_t)k + 1u;
-        done = true;
-        break;
+    // Back to front within the batch: the highest index first.
+    for (int word = (int)((count - 1u) >> 5); word >= 0 && !done; --word) {
+      for (uint32_t bits = s_cover[warp][word]; bits != 0u;) {
+        const int bit = 31 - __clz(bits);
+        bits ^= 1u << bit;
+        const uint32_t k = (uint32_t)word * 32u + (uint32_t)bit;
+        const Staged &s = s_batch[k];
+        if ((s.mask & myBits) != myBits) continue;
+        const float dx = pxf - s.cx, dy = pyf - s.cy;
+        const float power = splat_power(s, dx, dy);
+        if (power > 0.0f) continue;
+        const float alpha = fminf(kAlphaMax, s.opacity * M::exp(power));
+        if (!(alpha >= kAlphaMin)) continue;
+        const float oneMinus = 1.0f - alpha;
+        const float logRest = M::log(oneMinus);
+        if (logT + logRest < kLogMinTransmittance) {
+          stop = end + k + 1u;
+          done = true;
+          break;
+        }
+        const float w = T * alpha;
+        cr = fmaf(w, s.r, cr);
+        cg = fmaf(w, s.g, cg);
+        cb = fmaf(w, s.b, cb);
+        T = T * oneMinus;
+        logT = logT + logRest;
       }
-      const float w = T * alpha;
-      cr = fmaf(w, s.r, cr);
-      cg = fmaf(w, s.g, cg);
-      cb = fmaf(w, s.b, cb);
-      T = T * oneMinus;
-      logT = logT + logRest;
     }
   }
   if (inside) {
@@ -232,7 +263,7 @@ __device__ __forceinline__ float butterfly12(float v[12]) {
 }
 
 template <class M, bool FIXED>
-__global__ void __launch_bounds__(kTilePixels, 3)
+__global__ void __launch_bounds__(kTilePixels, 4)
     k_backward(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, void *__restrict__ rawOut,
@@ -241,15 +272,15 @@ __global__ void __launch_bounds__(kTilePixels, 3)
   __shared__ Staged s_batch[kBatch];
   __shared__ uint32_t s_acc[kBatch * kAccStride];
   __shared__ uint32_t s_min[kTilePixels / 32];
+  __shared__ uint32_t s_cover[kTilePixels / 32][kBatch / 32];
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
   const int tile = blockIdx.x;
   const TileGeometry geo = tile_geometry(views, tile);
   const ViewParams &cam = views.v[geo.view];
-  const uint32_t t = threadIdx.x, lane = t & 31u, lx = t & 15u, ly = t >> 4;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5, lx = t & 15u, ly = t >> 4;
   const uint32_t x = geo.x0 + lx, y = geo.y0 + ly;
   const bool inside = x < (uint32_t)cam.width && y < (uint32_t)cam.height;
   const uint32_t myBits = (1u << lx) | (1u << (16 + ly));
-  const uint32_t warpRows = 3u << (16 + 2 * (t >> 5));
   const float pxf = (float)x + 0.5f, pyf = (float)y + 0.5f;
   const size_t at = inside ? (size_t)cam.pixelBase + (size_t)y * cam.width + x : 0;
   const float logTotal = inside ? image[at].w : 0.0f;
@@ -275,15 +306,20 @@ __global__ void __launch_bounds__(kTilePixels, 3)
   for (uint32_t start = tileStop; start < range.y; start += kBatch) {
     const uint32_t count = min((uint32_t)kBatch, range.y - start);
     __syncthreads();
+    uint32_t stagedMask = 0u;
     if (t < count) {
-      const uint32_t s = entryValues[start + t];
-      s_batch[t] = stage_checked(splats, s, splatLimit, geo, error);
+      const Staged st = stage_checked(splats, entryValues[start + t], splatLimit, geo, error);
+      s_batch[t] = st;
+      stagedMask = st.mask;
     }
+    publish_cover<kTilePixels / 32>(stagedMask, warp, lane, s_cover);
     __syncthreads();
-    for (uint32_t k = 0; k < count; ++k) {
+    // Front to back: the lowest index first. The walk is warp-uniform.
+    for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
+    for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
+      const uint32_t k = word * 32u + (uint32_t)(__ffs(bits) - 1);
       const Staged &s = s_batch[k];
       const uint32_t mask = s.mask;
-      if ((mask & warpRows) == 0u || (mask & 0xFFFFu) == 0u) continue; // warp-uniform: no lane has anything
       // The tests of splat_at() first; one vote decides whether the warp has work.
       const float dx = pxf - s.cx, dy = pyf - s.cy;
       const float power = splat_power(s, dx, dy);
@@ -366,7 +402,6 @@ struct PixelPair {
   uint32_t x[2], y[2], bits[2];
   float px[2], py[2];
   bool inside[2];
-  uint32_t warpCols, warpRows;
 };
 
 __device__ __forceinline__ PixelPair pixel_pair(const TileGeometry &geo, const ViewParams &cam, uint32_t t) {
@@ -384,9 +419,26 @@ __device__ __forceinline__ PixelPair pixel_pair(const TileGeometry &geo, const V
     pp.py[q] = (float)pp.y[q] + 0.5f;
     pp.inside[q] = pp.x[q] < (uint32_t)cam.width && pp.y[q] < (uint32_t)cam.height;
   }
-  pp.warpCols = 0xFFu << bx;
-  pp.warpRows = 0xFFu << (16 + by);
   return pp;
+}
+
+// Stages `count` splats with 128 threads, two rounds, and publishes the
+// 8x8-block bitmaps.
+__device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, const uint32_t *__restrict__ values, uint32_t count,
+                                            uint32_t splatLimit, const TileGeometry &geo, uint32_t *error, Staged *batch,
+                                            uint32_t (*cover)[kBatch / 32]) {
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+#pragma unroll
+  for (uint32_t round = 0; round < kBatch / kHalfTile; ++round) {
+    const uint32_t j = round * kHalfTile + t;
+    uint32_t mask = 0u;
+    if (j < count) {
+      const Staged st = stage_checked(splats, values[j], splatLimit, geo, error);
+      batch[j] = st;
+      mask = st.mask;
+    }
+    publish_cover<kHalfTile / 32>(mask, round * (kHalfTile / 32) + warp, lane, cover);
+  }
 }
 
 template <class M>
@@ -396,11 +448,12 @@ __global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict_
                                                         uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
+  __shared__ uint32_t s_cover[kHalfTile / 32][kBatch / 32];
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
   const int tile = blockIdx.x;
   const TileGeometry geo = tile_geometry(views, tile);
   const ViewParams &cam = views.v[geo.view];
-  const uint32_t t = threadIdx.x;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const PixelPair pp = pixel_pair(geo, cam, t);
   const uint2 range = ranges[tile];
   float cr[2] = {0.f, 0.f}, cg[2] = {0.f, 0.f}, cb[2] = {0.f, 0.f}, T[2] = {1.f, 1.f}, logT[2] = {0.f, 0.f};
@@ -410,13 +463,15 @@ __global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict_
     const uint32_t count = min((uint32_t)kBatch, end - range.x);
     end -= count;
     if (__syncthreads_count(done[0] && done[1]) == kHalfTile) break;
-    for (uint32_t j = t; j < count; j += kHalfTile) s_batch[j] = stage_checked(splats, entryValues[end + j], splatLimit, geo, error);
+    stage_pairs(splats, entryValues + end, count, splatLimit, geo, error, s_batch, s_cover);
     __syncthreads();
-    if (done[0] && done[1]) continue;
-    for (int k = (int)count - 1; k >= 0; --k) {
+    for (int word = (int)((count - 1u) >> 5); word >= 0 && !(done[0] && done[1]); --word) {
+    for (uint32_t bits = s_cover[warp][word]; bits != 0u;) {
+      const int bit = 31 - __clz(bits);
+      bits ^= 1u << bit;
+      const uint32_t k = (uint32_t)word * 32u + (uint32_t)bit;
       const Staged &s = s_batch[k];
       const uint32_t mask = s.mask;
-      if ((mask & pp.warpRows) == 0u || (mask & pp.warpCols) == 0u) continue; // warp-uniform
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         if (done[q] || (mask & pp.bits[q]) != pp.bits[q]) continue;
@@ -441,6 +496,7 @@ __global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict_
       }
       if (done[0] && done[1]) break;
     }
+    }
   }
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
@@ -462,11 +518,12 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   __shared__ Staged s_batch[kBatch];
   __shared__ float s_acc[kBatch * kAccStride];
   __shared__ uint32_t s_min[kHalfTile / 32];
+  __shared__ uint32_t s_cover[kHalfTile / 32][kBatch / 32];
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
   const int tile = blockIdx.x;
   const TileGeometry geo = tile_geometry(views, tile);
   const ViewParams &cam = views.v[geo.view];
-  const uint32_t t = threadIdx.x, lane = t & 31u;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const PixelPair pp = pixel_pair(geo, cam, t);
   const uint2 range = ranges[tile];
   float logTotal[2], Ax[2], Ay[2], Az[2], Br[2], Bg[2], Bb[2], logBehind[2];
@@ -498,12 +555,13 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   for (uint32_t start = tileStop; start < range.y; start += kBatch) {
     const uint32_t count = min((uint32_t)kBatch, range.y - start);
     __syncthreads();
-    for (uint32_t j = t; j < count; j += kHalfTile) s_batch[j] = stage_checked(splats, entryValues[start + j], splatLimit, geo, error);
+    stage_pairs(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover);
     __syncthreads();
-    for (uint32_t k = 0; k < count; ++k) {
+    for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
+    for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
+      const uint32_t k = word * 32u + (uint32_t)(__ffs(bits) - 1);
       const Staged &s = s_batch[k];
       const uint32_t mask = s.mask;
-      if ((mask & pp.warpRows) == 0u || (mask & pp.warpCols) == 0u) continue; // warp-uniform
       float dx[2], dy[2], ep[2], oe[2], alpha[2];
       bool act[2];
 #pragma unroll
@@ -576,7 +634,7 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
                     cudaStream_t stream) {
   if (views.totalTiles == 0) return;
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
-  if (cfg.pixelsPerThread == 2) {
+  if (cfg.forwardPixels == 2) {
     if (cfg.exactMath)
       k_forward2<ExactMath><<<views.totalTiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
                                                                        splatLimit, error);
@@ -600,7 +658,7 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
   const uint32_t tiles = views.totalTiles;
   // The fixed-point sums keep the reference's 32-lane groups: one pixel per thread.
-  if (!fixedPoint && cfg.pixelsPerThread == 2) {
+  if (!fixedPoint && cfg.backwardPixels == 2) {
     float *rawF = static_cast<float *>(raw);
     if (cfg.exactMath)
       k_backward2<ExactMath><<<tiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,

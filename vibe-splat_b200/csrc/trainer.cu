@@ -140,7 +140,7 @@ public:
   StateStore stateStore = StateStore::BF16Pair;
   bool fixedPoint = false, oneSort = false, exactMath = true, useGraph = false;
   int digitBits = 8;
-  int pixelsPerThread = 2;
+  int forwardPixels = 1, backwardPixels = 2; // pixels per thread of the compositing and float backward kernels
   cudaStream_t stream = nullptr;
 
   DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
@@ -233,8 +233,12 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   useGraph = opt.use_graph != 0;
   digitBits = opt.digit_bits == 0 ? 8 : opt.digit_bits;
   if (digitBits < 6 || digitBits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
-  pixelsPerThread = opt.pixels_per_thread == 0 ? 2 : opt.pixels_per_thread;
-  if (pixelsPerThread != 1 && pixelsPerThread != 2) throw Failure{SPLAT_ERR_INVALID, "pixels_per_thread must be 1 or 2"};
+  forwardPixels = opt.forward_pixels_per_thread == 0 ? 1 : opt.forward_pixels_per_thread;
+  backwardPixels = opt.backward_pixels_per_thread == 0 ? 2 : opt.backward_pixels_per_thread;
+  if (forwardPixels != 1 && forwardPixels != 2)
+    throw Failure{SPLAT_ERR_INVALID, "forward_pixels_per_thread must be 1 or 2"};
+  if (backwardPixels != 1 && backwardPixels != 2)
+    throw Failure{SPLAT_ERR_INVALID, "backward_pixels_per_thread must be 1 or 2"};
   SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
 
@@ -562,7 +566,8 @@ void Trainer::record_forward() {
   end(3);
   RasterConfig cfg;
   cfg.exactMath = exactMath ? 1 : 0;
-  cfg.pixelsPerThread = pixelsPerThread;
+  cfg.forwardPixels = forwardPixels;
+  cfg.backwardPixels = backwardPixels;
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
   begin(4);
@@ -584,7 +589,8 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, stream));
   RasterConfig cfg;
   cfg.exactMath = exactMath ? 1 : 0;
-  cfg.pixelsPerThread = pixelsPerThread;
+  cfg.forwardPixels = forwardPixels;
+  cfg.backwardPixels = backwardPixels;
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
   begin(6);
@@ -619,6 +625,7 @@ void Trainer::fill_chain_args(ChainMode mode, bool statistics, const splat_learn
   a.statistics = statistics;
   a.selective = opt.selective_adam != 0;
   a.fixedPoint = fixedPoint;
+  a.splitStep = opt.split_step != 0;
   a.beta1 = 0.9f;
   a.beta2 = 0.999f;
   a.epsilon = 1e-15f;
@@ -823,26 +830,34 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
   set_sort(bestForm == 1, bestDigits);
   result.sort_form = bestForm;
   result.digit_bits = bestDigits;
-  // Then the rasterizer's layout with that sort.
-  const int oldLayout = pixelsPerThread;
-  int bestLayout = oldLayout;
+  // Then the rasterizer's layouts with that sort (the graphs are keyed by
+  // shape only, so they are dropped before each change).
+  int bestForward = forwardPixels, bestBackward = backwardPixels;
   double bestLayoutMs = 1e30;
-  for (int layout = 1; layout <= 2; ++layout) {
-    pixelsPerThread = layout;
-    splat_step_stats s{};
-    run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
-    const auto t0 = std::chrono::steady_clock::now();
-    for (int r = 0; r < repeats; ++r) run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
-    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
-    result.layout_ms[layout - 1] = ms;
-    if (ms < bestLayoutMs) {
-      bestLayoutMs = ms;
-      bestLayout = layout;
+  for (int fwd = 1; fwd <= 2; ++fwd) {
+    for (int bwd = 1; bwd <= 2; ++bwd) {
+      forwardPixels = fwd;
+      backwardPixels = bwd;
+      clear_graphs();
+      splat_step_stats s{};
+      run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+      const auto t0 = std::chrono::steady_clock::now();
+      for (int r = 0; r < repeats; ++r) run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
+      result.layout_ms[fwd - 1][bwd - 1] = ms;
+      if (ms < bestLayoutMs) {
+        bestLayoutMs = ms;
+        bestForward = fwd;
+        bestBackward = bwd;
+      }
     }
   }
-  pixelsPerThread = bestLayout;
+  forwardPixels = bestForward;
+  backwardPixels = bestBackward;
   clear_graphs();
-  result.pixels_per_thread = bestLayout;
+  result.forward_pixels_per_thread = bestForward;
+  result.backward_pixels_per_thread = bestBackward;
   if (out != nullptr) *out = result;
 }
 
@@ -936,7 +951,8 @@ void splat_trainer_options_default(splat_trainer_options *o) {
   o->exact_math = 1;
   o->use_graph = 0;
   o->digit_bits = 8;
-  o->pixels_per_thread = 2;
+  o->forward_pixels_per_thread = 1;
+  o->backward_pixels_per_thread = 2;
 }
 
 void splat_learning_rates_default(splat_learning_rates *r) {
