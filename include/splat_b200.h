@@ -260,7 +260,9 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
 /* RadixSorter::record (src/core/radix_sort.hpp, radix_sort.cpp:70-97): stable
  * ascending sort of count (u32 key, u32 value) pairs over the low key_bits
  * bits. keys, values, tmp_keys, tmp_values are device pointers of count
- * elements; the result is in keys/values. Allocates its scratch. stream may be 0. */
+ * elements, each 16-byte aligned (cudaMalloc's are; others are refused with
+ * SPLAT_ERR_INVALID); the result is in keys/values. Allocates its scratch.
+ * stream may be 0. */
 int splat_radix_sort_u32(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, uint32_t *tmp_values, uint32_t count,
                          int32_t key_bits, int32_t digit_bits, void *stream);
 /* The same for 64-bit keys over key_bits bits (the (tile << 32 | depth) keys). */

@@ -102,3 +102,15 @@ def test_stage_entry_points_check_arguments():
         s.radix_sort_device(0, 0, 0, 0, 10, 65, key_bytes=8)
     # One key needs no work and touches no memory.
     s.radix_sort_device(0, 0, 0, 0, 1, 32)
+
+
+def test_sorts_refuse_unaligned_arrays():
+    # Vector loads and bulk copies need 16-byte aligned arrays; the check comes
+    # before any device work.
+    s = splat_module()
+    for key_bytes in (4, 8):
+        with pytest.raises(s.SplatError, match="16-byte aligned"):
+            s.radix_sort_device(0x1004, 0x2000, 0x3000, 0x4000, 10, 16, key_bytes=key_bytes)
+    fn = s._lib.splat_radix_sort_u32_noalloc
+    assert fn(s._P(0x1000), s._P(0x2008), s._P(0x3000), s._P(0x4000), 10, 16, 8, None) == s.SPLAT_ERR_INVALID
+    assert "16-byte aligned" in s._lib.splat_last_error().decode()

@@ -3,8 +3,11 @@
 //   L = (1 - lambda) mean|image - target| + lambda (1 - mean SSIM)
 // over pixels and channels, 11x11 Gaussian window (sigma 1.5) cut off and
 // renormalised at the image border. Both kernels run one block per 16x16
-// tile: a horizontal pass over the tile plus 5 rows above and below into
-// shared memory, then a vertical pass out of it. The fields are stored as 9
+// tile: the tile and a 5-pixel halo are staged into shared memory once, a
+// horizontal pass over the tile plus 5 rows above and below goes into shared
+// memory, then a vertical pass out of it. Normalisations are multiplications
+// by reciprocals (the reference's GLSL division is not correctly rounded
+// either). The fields are stored as 9
 // FP32 planes (P, Q, R per channel; 36 bytes per pixel instead of the
 // reference's 48). Per-tile partial sums are added in FP64 on the GPU.
 #include "kernels.cuh"
@@ -49,10 +52,17 @@ __device__ __forceinline__ float block_sum(float v, float *s_warp) {
   return total;
 }
 
+// The tile with a 5-pixel halo on every side, one float per pixel and
+// plane, zero outside the image: a tap there adds an exact zero, as if the
+// window had been cut at the border.
+constexpr int kSpanCols = kTileSize + 2 * kHalo;
+constexpr int kStage = kRows * kSpanCols;
+
 __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
                                                       const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
                                                       float2 *__restrict__ partials) {
   const ViewSet &views = *viewsPtr;
+  __shared__ float s_in[6][kStage]; // image r, g, b, then target r, g, b
   __shared__ float s_h[5][3][kSpan];
   __shared__ float s_warp[kTilePixels / 32];
   const int tile = blockIdx.x;
@@ -63,33 +73,50 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
   const size_t base = (size_t)cam.pixelBase;
   const size_t plane = (size_t)views.totalPixels;
 
+  for (int i = threadIdx.x; i < kStage; i += kTilePixels) {
+    const int y = y0 + i / kSpanCols - kHalo, x = x0 + i % kSpanCols - kHalo;
+    float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float3 b3 = make_float3(0.f, 0.f, 0.f);
+    if (y >= 0 && y < H && x >= 0 && x < W) {
+      const size_t at = base + (size_t)y * W + x;
+      a4 = image[at];
+      b3 = unpack_unorm(target[at]);
+    }
+    s_in[0][i] = a4.x;
+    s_in[1][i] = a4.y;
+    s_in[2][i] = a4.z;
+    s_in[3][i] = b3.x;
+    s_in[4][i] = b3.y;
+    s_in[5][i] = b3.z;
+  }
+  __syncthreads();
+
+  // Horizontal pass: tile columns, tile rows plus the halo rows.
   for (int i = threadIdx.x; i < kSpan; i += kTilePixels) {
     const int r = i / kTileSize, c = i % kTileSize;
     const int y = y0 + r - kHalo, x = x0 + c;
     float m[5][3] = {};
     if (y >= 0 && y < H && x < W) {
-      float norm = 0.0f;
-      const int u0 = max(x - 5, 0), u1 = min(x + 5, W - 1);
-      for (int u = u0; u <= u1; ++u) {
-        const float w = c_weights[u - x + 5];
-        const size_t at = base + (size_t)y * W + u;
-        const float4 a4 = image[at];
-        const float3 b3 = unpack_unorm(target[at]);
-        const float a[3] = {a4.x, a4.y, a4.z}, b[3] = {b3.x, b3.y, b3.z};
+#pragma unroll
+      for (int u = 0; u < 11; ++u) {
+        const float w = c_weights[u];
+        const int at = r * kSpanCols + c + u;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          m[0][k] = fmaf(w, a[k], m[0][k]);
-          m[1][k] = fmaf(w, b[k], m[1][k]);
-          m[2][k] = fmaf(w * a[k], a[k], m[2][k]);
-          m[3][k] = fmaf(w * b[k], b[k], m[3][k]);
-          m[4][k] = fmaf(w * a[k], b[k], m[4][k]);
+          const float a = s_in[k][at], b = s_in[3 + k][at];
+          const float wa = w * a;
+          m[0][k] = fmaf(w, a, m[0][k]);
+          m[1][k] = fmaf(w, b, m[1][k]);
+          m[2][k] = fmaf(wa, a, m[2][k]);
+          m[3][k] = fmaf(w * b, b, m[3][k]);
+          m[4][k] = fmaf(wa, b, m[4][k]);
         }
-        norm += w;
       }
+      const float inv = 1.0f / window_norm(x, W);
 #pragma unroll
       for (int q = 0; q < 5; ++q)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) m[q][k] = m[q][k] / norm;
+        for (int k = 0; k < 3; ++k) m[q][k] *= inv;
     }
 #pragma unroll
     for (int q = 0; q < 5; ++q)
@@ -112,23 +139,25 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
 #pragma unroll
         for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_h[q][k][at], m[q][k]);
     }
-    const float norm = rowNorm * window_norm(px, W);
+    const float invRow = 1.0f / rowNorm;
+    const float invNorm = 1.0f / (rowNorm * window_norm(px, W));
     const size_t pixel = base + (size_t)py * W + px;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const float mx = m[0][k] / rowNorm, my = m[1][k] / rowNorm;
-      const float vx = m[2][k] / rowNorm - mx * mx, vy = m[3][k] / rowNorm - my * my, cxy = m[4][k] / rowNorm - mx * my;
+      const float mx = m[0][k] * invRow, my = m[1][k] * invRow;
+      const float vx = m[2][k] * invRow - mx * mx, vy = m[3][k] * invRow - my * my, cxy = m[4][k] * invRow - mx * my;
       const float n1 = 2.0f * mx * my + kC1, n2 = 2.0f * cxy + kC2;
       const float d1 = mx * mx + my * my + kC1, d2 = vx + vy + kC2;
-      const float s = (n1 * n2) / (d1 * d2);
+      const float invD = 1.0f / (d1 * d2), invD1 = 1.0f / d1, invD2 = 1.0f / d2;
+      const float s = (n1 * n2) * invD;
       own += s;
       // n1 and n2 cancelled by hand, as the reference does: n2 can be zero.
-      const float dMu = 2.0f * my * n2 / (d1 * d2) - s * 2.0f * mx / d1;
-      const float dVar = -s / d2;
-      const float dCov = 2.0f * n1 / (d1 * d2);
-      fields[(0 * 3 + k) * plane + pixel] = (dMu - 2.0f * mx * dVar - my * dCov) / norm;
-      fields[(1 * 3 + k) * plane + pixel] = dVar / norm;
-      fields[(2 * 3 + k) * plane + pixel] = dCov / norm;
+      const float dMu = 2.0f * my * n2 * invD - s * 2.0f * mx * invD1;
+      const float dVar = -s * invD2;
+      const float dCov = 2.0f * n1 * invD;
+      fields[(0 * 3 + k) * plane + pixel] = (dMu - 2.0f * mx * dVar - my * dCov) * invNorm;
+      fields[(1 * 3 + k) * plane + pixel] = dVar * invNorm;
+      fields[(2 * 3 + k) * plane + pixel] = dCov * invNorm;
     }
   }
   const float total = block_sum(own, s_warp);
@@ -139,6 +168,7 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
                                                       const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
                                                       float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials) {
   const ViewSet &views = *viewsPtr;
+  __shared__ float s_in[9][kStage];
   __shared__ float s_h[3][3][kSpan];
   __shared__ float s_warp[kTilePixels / 32];
   const int tile = blockIdx.x;
@@ -149,19 +179,28 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   const size_t base = (size_t)cam.pixelBase;
   const size_t plane = (size_t)views.totalPixels;
 
+  for (int i = threadIdx.x; i < kStage; i += kTilePixels) {
+    const int y = y0 + i / kSpanCols - kHalo, x = x0 + i % kSpanCols - kHalo;
+    const bool in = y >= 0 && y < H && x >= 0 && x < W;
+    const size_t at = in ? base + (size_t)y * W + x : 0;
+#pragma unroll
+    for (int f = 0; f < 9; ++f) s_in[f][i] = in ? fields[f * plane + at] : 0.0f;
+  }
+  __syncthreads();
+
   for (int i = threadIdx.x; i < kSpan; i += kTilePixels) {
     const int r = i / kTileSize, c = i % kTileSize;
     const int y = y0 + r - kHalo, x = x0 + c;
     float m[3][3] = {};
     if (y >= 0 && y < H && x < W) {
-      const int u0 = max(x - 5, 0), u1 = min(x + 5, W - 1);
-      for (int u = u0; u <= u1; ++u) {
-        const float w = c_weights[u - x + 5];
-        const size_t at = base + (size_t)y * W + u;
+#pragma unroll
+      for (int u = 0; u < 11; ++u) {
+        const float w = c_weights[u];
+        const int at = r * kSpanCols + c + u;
 #pragma unroll
         for (int q = 0; q < 3; ++q)
 #pragma unroll
-          for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, fields[(q * 3 + k) * plane + at], m[q][k]);
+          for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_in[q * 3 + k][at], m[q][k]);
       }
     }
 #pragma unroll
@@ -170,7 +209,6 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
       for (int k = 0; k < 3; ++k) s_h[q][k][i] = m[q][k];
   }
   __syncthreads();
-
   const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
   float own = 0.0f;
   if (px < W && py < H) {

@@ -74,6 +74,9 @@ extern "C" int splat_radix_sort_u32_noalloc(uint32_t *keys, uint32_t *values, ui
   if (key_bits < 1 || key_bits > 32) return fail(SPLAT_ERR_INVALID, "key_bits must be 1..32");
   const int digits = digit_bits == 0 ? 8 : digit_bits;
   if (digits < 6 || digits > 8) return fail(SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8");
+  if (!sb::sort_aligned(keys, values, tmp_keys, tmp_values)) {
+    return fail(SPLAT_ERR_INVALID, "keys, values and temporaries must be 16-byte aligned");
+  }
   if (count > sb::kNoAllocMaxKeys) {
     return fail(SPLAT_ERR_INVALID, "count exceeds the no-allocation sort's maximum of 4194304 keys");
   }

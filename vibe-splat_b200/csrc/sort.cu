@@ -3,6 +3,7 @@
 
 #include <algorithm>
 
+#include "bulk.cuh"
 #include "common.cuh"
 
 namespace sb {
@@ -18,7 +19,6 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagInclusive = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
 constexpr int kLookbackSpinLimit = 1 << 20;
-constexpr int kHistogramItems = 16;
 
 struct ScratchLayout {
   size_t hist;      // [passes][bins] u32 digit totals
@@ -78,8 +78,13 @@ template <typename K> __device__ __forceinline__ uint32_t digit_of(K key, int sh
   return (uint32_t)(key >> shift) & mask;
 }
 
-// Counts the digits of every pass in one read of the keys. Keys are read as
-// 16-byte vectors; a warp's same-digit keys are added once through match.any.
+// Counts the digits of every pass in one read of the keys: 16-byte vector
+// loads, kHistogramVecs per thread, and shared-memory atomics on one
+// histogram copy per pair of warps (kHistogramCopies), added up and sent to
+// the global histogram once per block.
+constexpr int kHistogramVecs = 4;
+constexpr int kHistogramCopies = kSortWarps / 2;
+
 template <typename K, int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_histogram(const K *__restrict__ keys, const uint32_t *deviceCount,
                                                             uint32_t hostCount, int firstBit, int passes,
@@ -87,97 +92,116 @@ __global__ void __launch_bounds__(kSortThreads) k_histogram(const K *__restrict_
   constexpr int kBins = 1 << BITS;
   constexpr uint32_t kMask = kBins - 1;
   constexpr int kPerVec = 16 / sizeof(K);
-  __shared__ uint32_t s_hist[kMaxPasses * kBins];
-  for (int i = threadIdx.x; i < passes * kBins; i += kSortThreads) s_hist[i] = 0;
+  extern __shared__ uint32_t s_hist[]; // [kHistogramCopies][passes][kBins]
+  const int words = passes * kBins;
+  for (int i = threadIdx.x; i < kHistogramCopies * words; i += kSortThreads) s_hist[i] = 0u;
   __syncthreads();
   const uint32_t count = deviceCount != nullptr ? *deviceCount : hostCount;
-  const uint32_t lane = lane_id();
-  const size_t vecs = count / kPerVec;
-  const size_t stride = (size_t)gridDim.x * kSortThreads;
-  for (size_t base = (size_t)blockIdx.x * kSortThreads; base < vecs + (count % kPerVec != 0); base += stride) {
-    const size_t v = base + threadIdx.x;
-    K items[kPerVec];
-    bool valid[kPerVec];
-    if (v < vecs) {
-      const uint4 raw = reinterpret_cast<const uint4 *>(keys)[v];
-      const K *k = reinterpret_cast<const K *>(&raw);
+  uint32_t *mine = s_hist + ((threadIdx.x >> 5) % kHistogramCopies) * words;
+  const size_t vecs = div_up(count, kPerVec);
+  const size_t stride = (size_t)gridDim.x * kSortThreads * kHistogramVecs;
+  for (size_t base = (size_t)blockIdx.x * kSortThreads * kHistogramVecs; base < vecs; base += stride) {
+    // All loads first; the last, ragged vector element by element.
+    K items[kHistogramVecs][kPerVec];
 #pragma unroll
-      for (int e = 0; e < kPerVec; ++e) {
-        items[e] = k[e];
-        valid[e] = true;
-      }
-    } else {
+    for (int q = 0; q < kHistogramVecs; ++q) {
+      const size_t v = base + (size_t)q * kSortThreads + threadIdx.x;
+      if ((v + 1) * kPerVec <= count) {
+        const uint4 raw = reinterpret_cast<const uint4 *>(keys)[v];
+        const K *k = reinterpret_cast<const K *>(&raw);
 #pragma unroll
-      for (int e = 0; e < kPerVec; ++e) {
-        const size_t i = v * kPerVec + e;
-        valid[e] = i < count;
-        items[e] = valid[e] ? keys[i] : K(0);
+        for (int e = 0; e < kPerVec; ++e) items[q][e] = k[e];
+      } else {
+#pragma unroll
+        for (int e = 0; e < kPerVec; ++e) items[q][e] = v * kPerVec + e < count ? keys[v * kPerVec + e] : K(0);
       }
     }
 #pragma unroll
-    for (int e = 0; e < kPerVec; ++e) {
-      for (int p = 0; p < passes; ++p) {
-        const uint32_t d = valid[e] ? digit_of(items[e], firstBit + p * BITS, kMask) : (uint32_t)kBins;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        if (d < (uint32_t)kBins && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_hist[p * kBins + d], __popc(peers));
+    for (int q = 0; q < kHistogramVecs; ++q) {
+      const size_t v = base + (size_t)q * kSortThreads + threadIdx.x;
+#pragma unroll
+      for (int e = 0; e < kPerVec; ++e) {
+        if (v * kPerVec + e >= count) continue;
+        for (int p = 0; p < passes; ++p) atomicAdd(&mine[p * kBins + digit_of(items[q][e], firstBit + p * BITS, kMask)], 1u);
       }
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < passes * kBins; i += kSortThreads) {
-    if (s_hist[i] != 0) atomicAdd(&hist[i], s_hist[i]);
+  for (int i = threadIdx.x; i < words; i += kSortThreads) {
+    uint32_t total = 0;
+#pragma unroll
+    for (int c = 0; c < kHistogramCopies; ++c) total += s_hist[c * words + i];
+    if (total != 0u) atomicAdd(&hist[i], total);
   }
 }
 
+// Polls of a tile's bulk-copy barrier before the kernel gives up on it.
+constexpr int kBulkSpinLimit = 1 << 22;
+
 // One pass: rank, look back, scatter. Dynamic shared memory holds the tile's
-// keys (later its values) and one digit byte per key.
+// keys (later the keys, then the values, in digit order), its values as read,
+// and one digit byte per key. A full tile's keys and values arrive by bulk
+// copy, issued first so that the values land while the keys are ranked.
 template <typename K, int BITS>
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const K *__restrict__ keysIn, const uint32_t *__restrict__ valsIn,
-                                                           K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
-                                                           const uint32_t *deviceCount, uint32_t hostCount,
-                                                           const uint32_t *__restrict__ passHist, uint32_t *lookback,
-                                                           uint32_t *tileCounter, int shift, uint32_t *error) {
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restrict__ keysIn, const uint32_t *__restrict__ valsIn,
+                                                              K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
+                                                              const uint32_t *deviceCount, uint32_t hostCount,
+                                                              const uint32_t *__restrict__ passHist, uint32_t *lookback,
+                                                              uint32_t *tileCounter, int shift, uint32_t *error) {
   constexpr int kBins = 1 << BITS;
   constexpr uint32_t kMask = kBins - 1;
-  extern __shared__ __align__(16) unsigned char s_dynamic[];
+  extern __shared__ __align__(128) unsigned char s_dynamic[];
   K *s_keys = reinterpret_cast<K *>(s_dynamic);
-  uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_dynamic);
-  uint8_t *s_digit = s_dynamic + kSortTileKeys * sizeof(K);
+  uint32_t *s_out = reinterpret_cast<uint32_t *>(s_dynamic);
+  uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_dynamic + kSortTileKeys * sizeof(K));
+  uint8_t *s_digit = s_dynamic + kSortTileKeys * (sizeof(K) + 4);
   __shared__ uint32_t s_warpHist[kSortWarps][kBins];
   __shared__ uint32_t s_digitBase[kBins];
   __shared__ uint32_t s_globalBase[kBins];
   __shared__ uint32_t s_scan[kSortWarps];
   __shared__ uint32_t s_tile;
+  __shared__ __align__(8) uint64_t s_bar;
 
   const uint32_t t = threadIdx.x, lane = lane_id(), warp = t >> 5;
-  if (t == 0) s_tile = atomicAdd(tileCounter, 1u);
+  if (t == 0) {
+    s_tile = atomicAdd(tileCounter, 1u);
+    bulk_barrier_init(&s_bar, 1);
+  }
   for (int i = t; i < kSortWarps * kBins; i += kSortThreads) (&s_warpHist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t count = deviceCount != nullptr ? *deviceCount : hostCount;
   const size_t tileStart = (size_t)tile * kSortTileKeys;
-  if (tileStart >= count) return; // Every CTA of the block leaves together.
+  if (tileStart >= count) return; // the whole block leaves; no copy was issued
   const uint32_t tileKeys = count - tileStart < (size_t)kSortTileKeys ? (uint32_t)(count - tileStart) : (uint32_t)kSortTileKeys;
+  const bool bulk = tileKeys == kSortTileKeys;
+  if (bulk && t == 0) {
+    bulk_expect(&s_bar, kSortTileKeys * (uint32_t)(sizeof(K) + 4));
+    bulk_load(s_keys, keysIn + tileStart, kSortTileKeys * sizeof(K), &s_bar);
+    bulk_load(s_vals, valsIn + tileStart, kSortTileKeys * 4, &s_bar);
+  }
 
   // The pass's global digit offsets: an exclusive scan of its histogram.
   uint32_t binTotal = 0;
   const uint32_t passOffset = block_exclusive_scan(t < (uint32_t)kBins ? passHist[t] : 0u, s_scan, binTotal);
 
-  // Load the tile linearly with 16-byte vectors, then read it back warp-striped:
-  // warp w owns keys [w*kSortItems*32, (w+1)*kSortItems*32), item j of lane l is
-  // at j*32 + l inside that chunk, so (warp, item, lane) is the input order.
-  constexpr int kPerVec = 16 / sizeof(K);
-  if (tileKeys == kSortTileKeys) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(keysIn + tileStart);
-    uint4 *dst = reinterpret_cast<uint4 *>(s_keys);
-#pragma unroll
-    for (int i = 0; i < kSortTileKeys / kPerVec / kSortThreads; ++i) dst[i * kSortThreads + t] = src[i * kSortThreads + t];
+  if (bulk) {
+    if (!bulk_wait(&s_bar, 0, kBulkSpinLimit)) {
+      // Never leave with a copy still landing in this block's shared memory.
+      if (t == 0) atomicOr(error, kErrLookbackTimeout);
+      bulk_wait(&s_bar, 0, kBulkSpinLimit);
+    }
   } else {
-    for (uint32_t i = t; i < tileKeys; i += kSortThreads) s_keys[i] = keysIn[tileStart + i];
+    for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
+      s_keys[i] = keysIn[tileStart + i];
+      s_vals[i] = valsIn[tileStart + i];
+    }
   }
   __syncthreads();
+  // Warp w owns keys [w*kSortItems*32, (w+1)*kSortItems*32); item j of lane l
+  // is at j*32 + l inside that chunk, so (warp, item, lane) is the input order.
   K key[kSortItems];
-  uint32_t rank[kSortItems];
+  uint32_t slot[kSortItems];
   const uint32_t chunk = warp * kSortItems * 32;
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
@@ -197,7 +221,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K *__restrict__
     __syncwarp();
     if (valid && lane == (uint32_t)(31 - __clz(peers))) s_warpHist[warp][d] = prior + __popc(peers);
     __syncwarp();
-    rank[j] = prior + before;
+    slot[j] = prior + before;
   }
   __syncthreads();
 
@@ -243,15 +267,14 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K *__restrict__
   }
   __syncthreads();
 
-  // Scatter keys into shared memory in digit order, then write them out: the
-  // threads of a warp write consecutive addresses within each digit's run.
-  uint32_t slot[kSortItems];
+  // Keys into shared memory in digit order, then out: the threads of a warp
+  // write consecutive addresses within each digit's run.
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t i = chunk + j * 32 + lane;
     if (i < tileKeys) {
       const uint32_t d = digit_of(key[j], shift, kMask);
-      slot[j] = s_digitBase[d] + s_warpHist[warp][d] + rank[j];
+      slot[j] += s_digitBase[d] + s_warpHist[warp][d];
       s_keys[slot[j]] = key[j];
       s_digit[slot[j]] = (uint8_t)d;
     }
@@ -264,37 +287,20 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K *__restrict__
     if (dst < count) keysOut[dst] = s_keys[i];
   }
   __syncthreads();
-
-  // The same permutation for the values.
-  if (tileKeys == kSortTileKeys) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(valsIn + tileStart);
-    uint4 *dst = reinterpret_cast<uint4 *>(s_vals);
-#pragma unroll
-    for (int i = 0; i < kSortTileKeys / 4 / kSortThreads; ++i) dst[i * kSortThreads + t] = src[i * kSortThreads + t];
-  } else {
-    for (uint32_t i = t; i < tileKeys; i += kSortThreads) s_vals[i] = valsIn[tileStart + i];
-  }
-  __syncthreads();
-  uint32_t val[kSortItems];
+  // The same permutation for the values, straight from where they landed.
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t i = chunk + j * 32 + lane;
-    val[j] = i < tileKeys ? s_vals[i] : 0u;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < kSortItems; ++j) {
-    const uint32_t i = chunk + j * 32 + lane;
-    if (i < tileKeys) s_vals[slot[j]] = val[j];
+    if (i < tileKeys) s_out[slot[j]] = s_vals[i];
   }
   __syncthreads();
   for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
     const uint32_t dst = s_globalBase[s_digit[i]] + i;
-    if (dst < count) valsOut[dst] = s_vals[i];
+    if (dst < count) valsOut[dst] = s_out[i];
   }
 }
 
-template <typename K, int BITS> size_t onesweep_smem() { return kSortTileKeys * sizeof(K) + kSortTileKeys; }
+template <typename K, int BITS> size_t onesweep_smem() { return kSortTileKeys * (sizeof(K) + 4) + kSortTileKeys; }
 
 template <typename K, int BITS>
 int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, size_t capacity, uint32_t hostCount,
@@ -313,15 +319,20 @@ int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, 
 
   const uint32_t launchKeys = deviceCount != nullptr ? (uint32_t)capacity : hostCount;
   const uint32_t tiles = div_up(launchKeys, kSortTileKeys);
-  const uint32_t histBlocks = std::min<uint32_t>(div_up(launchKeys, kSortThreads * kHistogramItems), 148u * 8u);
-  k_histogram<K, BITS><<<std::max(histBlocks, 1u), kSortThreads, 0, stream>>>(keys, deviceCount, hostCount, firstBit, passes, hist);
-
+  constexpr uint32_t kPerVec = 16 / sizeof(K);
+  const uint32_t histBlocks =
+      std::min<uint32_t>(div_up(div_up(launchKeys, kPerVec), (uint32_t)(kSortThreads * kHistogramVecs)), 148u * 8u);
+  const size_t histSmem = (size_t)kHistogramCopies * passes * kBins * 4;
   static bool configured = false;
   const size_t smem = onesweep_smem<K, BITS>();
   if (!configured) {
     cudaFuncSetAttribute(k_onesweep<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_histogram<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kHistogramCopies * kMaxPasses * kBins * 4));
     configured = true;
   }
+  k_histogram<K, BITS><<<std::max(histBlocks, 1u), kSortThreads, histSmem, stream>>>(keys, deviceCount, hostCount, firstBit,
+                                                                                     passes, hist);
   K *srcK = keys, *dstK = tmpKeys;
   uint32_t *srcV = values, *dstV = tmpValues;
   for (int p = 0; p < passes; ++p) {

@@ -5,10 +5,12 @@
 // scan_blocks/scan_add.comp and radix_scatter.comp) with the single-pass
 // scheme of Adinets and Merrill ("Onesweep", 2022):
 //   1. one histogram kernel counts the digits of every pass at once;
-//   2. one kernel per pass ranks a tile of keys with warp-level match.any,
-//      finds its global offsets through a decoupled look-back over the tiles
-//      before it, and scatters through shared memory so that each warp writes
-//      contiguous runs.
+//   2. one kernel per pass brings a tile of 4096 keys and their values into
+//      shared memory by bulk asynchronous copy (cp.async.bulk, completed on an
+//      mbarrier), ranks the keys with warp-level match.any, finds its global
+//      offsets through a decoupled look-back over the tiles before it, and
+//      scatters through shared memory so that each warp writes contiguous
+//      runs. Keys, values and their temporaries must be 16-byte aligned.
 // Keys are read once per pass and written once; the reference reads them
 // twice per pass (histogram and scatter) and runs a recursive scan between.
 // Stability matches std::stable_sort (tests/test_radix_sort.cpp:48-59 in the
@@ -26,6 +28,14 @@
 #include <cuda_runtime.h>
 
 namespace sb {
+
+// Whether all four arrays start on a 16-byte boundary (vector loads and bulk
+// copies need it).
+inline bool sort_aligned(const void *a, const void *b, const void *c, const void *d) {
+  return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c) |
+           reinterpret_cast<uintptr_t>(d)) &
+          15u) == 0u;
+}
 
 // Scratch one sort needs, in bytes, for `capacity` keys of `keyBytes` bytes,
 // sorted over `bits` significant bits (from bit `firstBit`) with `digitBits`-bit

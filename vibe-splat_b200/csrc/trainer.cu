@@ -1318,6 +1318,8 @@ int splat_radix_sort_u32(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, u
     if (key_bits < 1 || key_bits > 32) throw Failure{SPLAT_ERR_INVALID, "key_bits must be 1..32"};
     const int digits = digit_bits == 0 ? 8 : digit_bits;
     if (digits < 6 || digits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
+    if (!sb::sort_aligned(keys, values, tmp_keys, tmp_values))
+      throw Failure{SPLAT_ERR_INVALID, "keys, values and temporaries must be 16-byte aligned"};
     if (count <= 1) return;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     sb::DeviceBuffer scratch, error;
@@ -1343,6 +1345,8 @@ int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, u
     if (key_bits < 1 || key_bits > 64) throw Failure{SPLAT_ERR_INVALID, "key_bits must be 1..64"};
     const int digits = digit_bits == 0 ? 8 : digit_bits;
     if (digits < 6 || digits > 8) throw Failure{SPLAT_ERR_INVALID, "digit_bits must be 6, 7 or 8"};
+    if (!sb::sort_aligned(keys, values, tmp_keys, tmp_values))
+      throw Failure{SPLAT_ERR_INVALID, "keys, values and temporaries must be 16-byte aligned"};
     if (count <= 1) return;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     sb::DeviceBuffer scratch, error;
