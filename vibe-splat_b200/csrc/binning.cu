@@ -31,10 +31,28 @@ __device__ __forceinline__ TileRect splat_tiles(const float4 ce, int gridW, int 
   return {(uint32_t)lx, (uint32_t)ly, (uint32_t)hx, (uint32_t)hy};
 }
 
-// Whether the splat reaches any pixel centre of tile (tx, ty) (splat_reaches_tile).
-__device__ __forceinline__ bool splat_reaches_tile(const float4 q, const float4 ce, float reach, uint32_t tx, uint32_t ty) {
-  const float lowX = ((float)tx * 16.0f + 0.5f) - ce.x, lowY = ((float)ty * 16.0f + 0.5f) - ce.y;
-  const float highX = lowX + 15.0f, highY = lowY + 15.0f;
+// Whether the splat reaches any pixel centre of tile (tx, ty)
+// (splat_reaches_tile). The closest point of each tile edge to the centre is
+// found by clamping the ellipse's tangent point; the two horizontal edges'
+// tangent points depend on the row only, so a caller that walks a row can
+// compute them once (row_tangents) and pass them in. Same operations, same
+// order as evaluating everything per tile.
+struct RowTangents {
+  float lowY, highY, uLow, uHigh; // edge offsets from the centre and their unclamped tangent x
+};
+
+__device__ __forceinline__ RowTangents row_tangents(const float4 q, const float4 ce, uint32_t ty) {
+  RowTangents r;
+  r.lowY = ((float)ty * 16.0f + 0.5f) - ce.y;
+  r.highY = r.lowY + 15.0f;
+  r.uLow = -q.y * r.lowY / q.x;
+  r.uHigh = -q.y * r.highY / q.x;
+  return r;
+}
+
+__device__ __forceinline__ bool reaches_tile_row(const float4 q, const float4 ce, float reach, uint32_t tx, const RowTangents &row) {
+  const float lowX = ((float)tx * 16.0f + 0.5f) - ce.x, lowY = row.lowY;
+  const float highX = lowX + 15.0f, highY = row.highY;
   if (lowX <= 0.0f && lowY <= 0.0f && highX >= 0.0f && highY >= 0.0f) return true;
   float least = 1e30f;
 #pragma unroll
@@ -43,10 +61,14 @@ __device__ __forceinline__ bool splat_reaches_tile(const float4 q, const float4 
     const float y = fminf(fmaxf(-q.y * x / q.z, lowY), highY);
     least = fminf(least, q.x * x * x + 2.0f * q.y * x * y + q.z * y * y);
     const float v = side == 0 ? lowY : highY;
-    const float u = fminf(fmaxf(-q.y * v / q.x, lowX), highX);
+    const float u = fminf(fmaxf(side == 0 ? row.uLow : row.uHigh, lowX), highX);
     least = fminf(least, q.x * u * u + 2.0f * q.y * u * v + q.z * v * v);
   }
   return least <= reach * 1.001f + 1e-3f;
+}
+
+__device__ __forceinline__ bool splat_reaches_tile(const float4 q, const float4 ce, float reach, uint32_t tx, uint32_t ty) {
+  return reaches_tile_row(q, ce, reach, tx, row_tangents(q, ce, ty));
 }
 
 // Splats whose tile rectangle holds more than this many tiles are tested by a
@@ -57,11 +79,16 @@ constexpr uint32_t kWarpTiles = 16;
 
 __device__ __forceinline__ uint32_t rect_area(const TileRect &t) { return (t.x1 - t.x0 + 1u) * (t.y1 - t.y0 + 1u); }
 
-__device__ __forceinline__ uint32_t count_tiles(const float4 q, const float4 ce, float reach, const TileRect &t) {
-  uint32_t n = 0;
-  for (uint32_t y = t.y0; y <= t.y1; ++y)
-    for (uint32_t x = t.x0; x <= t.x1; ++x) n += splat_reaches_tile(q, ce, reach, x, y) ? 1u : 0u;
-  return n;
+// The reached tiles of a rectangle of at most 32 tiles, bit (y - y0) * width
+// + (x - x0) for tile (x, y): row-major, the reference's emission order.
+__device__ __forceinline__ uint32_t reach_mask(const float4 q, const float4 ce, float reach, const TileRect &t) {
+  uint32_t mask = 0, bit = 1;
+  for (uint32_t y = t.y0; y <= t.y1; ++y) {
+    const RowTangents row = row_tangents(q, ce, y);
+    for (uint32_t x = t.x0; x <= t.x1; ++x, bit <<= 1)
+      if (reaches_tile_row(q, ce, reach, x, row)) mask |= bit;
+  }
+  return mask;
 }
 
 // The tiles of the rectangle in row-major order, 32 at a time: lane l tests
@@ -94,8 +121,8 @@ __device__ __forceinline__ int item_view(uint32_t splatIndex, uint32_t n, int vi
 __global__ void __launch_bounds__(kScanThreads)
     k_bin_count_scan(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
                      const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
-                     uint32_t *__restrict__ offsets, uint32_t *counters, uint32_t capacity, unsigned long long *status,
-                     uint32_t *ticket, uint32_t *error) {
+                     uint32_t *__restrict__ offsets, uint32_t *__restrict__ masks, uint32_t *counters, uint32_t capacity,
+                     unsigned long long *status, uint32_t *ticket, uint32_t *error) {
   const ViewSet &views = *viewsPtr;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanThreads / 32];
@@ -107,35 +134,63 @@ __global__ void __launch_bounds__(kScanThreads)
   const uint32_t numTiles = div_up(items, kScanTile);
   if (tile >= numTiles) return;
 
-  uint32_t counts[kScanItems];
-  uint32_t threadSum = 0, visible = 0;
+  // Loads first: the items' splats, then the tests.
+  uint32_t sIdx[kScanItems];
+  bool valid[kScanItems];
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
-    uint32_t c = 0, s = 0;
+    valid[j] = r < items && itemKeys[r] != kInvisible;
+    sIdx[j] = valid[j] ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
+  }
+  float4 ce[kScanItems], cq[kScanItems];
+  float rc[kScanItems];
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    if (valid[j]) {
+      ce[j] = splats[sIdx[j]].centerExtent;
+      cq[j] = splats[sIdx[j]].conicOpacity;
+      rc[j] = reach[sIdx[j]];
+    } else {
+      ce[j] = cq[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      rc[j] = 0.0f;
+    }
+  }
+  uint32_t counts[kScanItems], mask[kScanItems];
+  uint32_t threadSum = 0, visible = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    uint32_t c = 0;
     bool big = false;
-    if (r < items && itemKeys[r] != kInvisible) {
-      s = itemSplat != nullptr ? itemSplat[r] : r;
-      const ViewParams &cam = views.v[item_view(s, n, views.count)];
-      const Splat sp = splats[s];
-      const TileRect rect = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    mask[j] = 0u;
+    if (valid[j]) {
+      const ViewParams &cam = views.v[item_view(sIdx[j], n, views.count)];
+      const TileRect rect = splat_tiles(ce[j], cam.gridW, cam.gridH);
       big = rect_area(rect) > kWarpTiles;
-      if (!big) c = count_tiles(sp.conicOpacity, sp.centerExtent, reach[s], rect);
+      if (!big) {
+        mask[j] = reach_mask(cq[j], ce[j], rc[j], rect);
+        c = (uint32_t)__popc(mask[j]);
+      }
       ++visible;
     }
     // Large rectangles: the whole warp, one after another.
     for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
       const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
-      const uint32_t bs = __shfl_sync(0xFFFFFFFFu, s, src);
+      const uint32_t bs = __shfl_sync(0xFFFFFFFFu, sIdx[j], src);
       const ViewParams &cam = views.v[item_view(bs, n, views.count)];
       const Splat sp = splats[bs];
-      const float rc = reach[bs];
+      const float rcb = reach[bs];
       const TileRect rect = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
       const uint32_t width = rect.x1 - rect.x0 + 1u, area = rect_area(rect);
-      uint32_t total = 0, x = 0, y = 0;
-      for (uint32_t base = 0; base < area; base += 32u)
-        total += (uint32_t)__popc(warp_reach(sp.conicOpacity, sp.centerExtent, rc, rect, width, area, base, lane, x, y));
-      if (lane == src) c = total;
+      uint32_t total = 0, hits = 0, x = 0, y = 0;
+      for (uint32_t base = 0; base < area; base += 32u) {
+        hits = warp_reach(sp.conicOpacity, sp.centerExtent, rcb, rect, width, area, base, lane, x, y);
+        total += (uint32_t)__popc(hits);
+      }
+      if (lane == src) {
+        c = total;
+        mask[j] = area <= 32u ? hits : 0u; // the emission replays masks of one word only
+      }
     }
     counts[j] = c;
     threadSum += c;
@@ -208,7 +263,10 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
-    if (r < items) offsets[r] = running;
+    if (r < items) {
+      offsets[r] = running;
+      masks[r] = mask[j];
+    }
     running += counts[j];
   }
 }
@@ -216,7 +274,8 @@ __global__ void __launch_bounds__(kScanThreads)
 __global__ void __launch_bounds__(256)
     k_bin_emit(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
                const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
-               const uint32_t *__restrict__ offsets, uint32_t capacity, uint32_t *__restrict__ tileKeys32,
+               const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ masks, uint32_t capacity,
+               uint32_t *__restrict__ tileKeys32,
                unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues, uint32_t *error) {
   const ViewSet &views = *viewsPtr;
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
@@ -241,21 +300,20 @@ __global__ void __launch_bounds__(256)
   bool big = false;
   if (valid) {
     const ViewParams &cam = views.v[item_view(s, n, views.count)];
-    const Splat sp = splats[s];
-    const TileRect t = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
-    big = rect_area(t) > kWarpTiles;
+    const TileRect t = splat_tiles(splats[s].centerExtent, cam.gridW, cam.gridH);
+    const uint32_t width = t.x1 - t.x0 + 1u;
+    big = rect_area(t) > 32u;
     if (!big) {
-      const float rc = reach[s];
+      // The counting pass's tests, replayed from its mask in row-major order.
       uint32_t slot = offsets[r];
-      for (uint32_t y = t.y0; y <= t.y1; ++y) {
-        for (uint32_t x = t.x0; x <= t.x1; ++x) {
-          if (!splat_reaches_tile(sp.conicOpacity, sp.centerExtent, rc, x, y)) continue;
-          put(slot++, cam, x, y, depthKey, s);
-        }
+      for (uint32_t bits = masks[r]; bits != 0u; bits &= bits - 1u) {
+        const uint32_t b = (uint32_t)(__ffs(bits) - 1);
+        put(slot++, cam, t.x0 + b % width, t.y0 + b / width, depthKey, s);
       }
     }
   }
-  // Large rectangles: row-major order kept by counting the lower lanes' hits.
+  // Rectangles of more than 32 tiles are tested again, by the whole warp;
+  // row-major order kept by counting the lower lanes' hits.
   for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
     const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
     const uint32_t bs = __shfl_sync(0xFFFFFFFFu, s, src);
@@ -300,23 +358,23 @@ size_t bin_scan_scratch_bytes(uint32_t items) {
 }
 
 void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
-                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *counters,
-                           uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
+                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *masks,
+                           uint32_t *counters, uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
   if (items == 0) return;
   const uint32_t tiles = div_up(items, kScanTile);
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
   cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
-  k_bin_count_scan<<<tiles, kScanThreads, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, counters,
-                                                       capacity, status, ticket, error);
+  k_bin_count_scan<<<tiles, kScanThreads, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks,
+                                                       counters, capacity, status, ticket, error);
 }
 
 void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
-                     uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets, uint32_t capacity,
-                     uint32_t *tileKeys32, unsigned long long *tileKeys64, uint32_t *entryValues, uint32_t *error,
-                     cudaStream_t stream) {
+                     uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets,
+                     const uint32_t *masks, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
+                     uint32_t *entryValues, uint32_t *error, cudaStream_t stream) {
   if (items == 0) return;
-  k_bin_emit<<<div_up(items, 256), 256, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, capacity,
+  k_bin_emit<<<div_up(items, 256), 256, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks, capacity,
                                                      tileKeys32, tileKeys64, entryValues, error);
 }
 

@@ -52,18 +52,20 @@ void launch_preprocess(const Params &p, const ViewSet &views, const ViewSet *dVi
 // counters[0] += visible items, counters[1] = total entries, counters[2] =
 // min(total, capacity). itemSplat: if not null, the splat of item r is
 // itemSplat[r] (sorted values); itemKeys: kInvisible marks culled items.
+// masks[r]: the reached tiles of a rectangle of at most 32 tiles, bit
+// (y - y0) * width + (x - x0), for the emission to replay (0 for larger ones).
 void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
-                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *counters,
-                           uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream);
+                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *masks,
+                           uint32_t *counters, uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream);
 size_t bin_scan_scratch_bytes(uint32_t items);
 
 // train_bin_emit.comp. Depth-sorted form: tileKeys32[slot] = tile, entryValues[slot]
 // = splat. Single-sort form (tileKeys64 not null): tileKeys64[slot] = (global
 // tile << 32) | depth key.
 void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
-                     uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets, uint32_t capacity,
-                     uint32_t *tileKeys32, unsigned long long *tileKeys64, uint32_t *entryValues, uint32_t *error,
-                     cudaStream_t stream);
+                     uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets,
+                     const uint32_t *masks, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
+                     uint32_t *entryValues, uint32_t *error, cudaStream_t stream);
 
 // train_tile_ranges.comp over the sorted keys; ranges (2 u32 per global tile)
 // must be cleared first. count is read from deviceCount.

@@ -19,6 +19,7 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagInclusive = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
 constexpr int kLookbackSpinLimit = 1 << 20;
+constexpr int kLookbackWindow = 8;
 
 struct ScratchLayout {
   size_t hist;      // [passes][bins] u32 digit totals
@@ -240,25 +241,37 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
   uint32_t tileTotal;
   const uint32_t digitBase = block_exclusive_scan(t < (uint32_t)kBins ? digitTotal : 0u, s_scan, tileTotal);
 
-  // Decoupled look-back, one thread per digit.
+  // Decoupled look-back, one thread per digit, kLookbackWindow predecessors
+  // per poll: the aggregates up to the nearest inclusive prefix are added; a
+  // predecessor that has published nothing yet stops the walk there, and the
+  // next poll starts from it.
   if (t < (uint32_t)kBins) {
     uint32_t exclusive = 0;
     if (tile > 0) {
       int64_t pred = (int64_t)tile - 1;
       int spins = 0;
-      while (pred >= 0) {
-        const uint32_t v = load_volatile(&lookback[(size_t)pred * kBins + t]);
-        const uint32_t flag = v & ~kValueMask;
-        if (flag == 0u) {
-          if (++spins > kLookbackSpinLimit) {
-            atomicOr(error, kErrLookbackTimeout);
-            break;
-          }
-          continue;
+      for (;;) {
+        uint32_t v[kLookbackWindow];
+#pragma unroll
+        for (int k = 0; k < kLookbackWindow; ++k)
+          v[k] = pred - k >= 0 ? load_volatile(&lookback[(size_t)(pred - k) * kBins + t]) : kFlagInclusive;
+        int used = 0;
+        bool done = false;
+#pragma unroll
+        for (int k = 0; k < kLookbackWindow; ++k) {
+          if (done || used < k) continue; // stopped before k
+          const uint32_t flag = v[k] & ~kValueMask;
+          if (flag == 0u) continue;       // pending: the walk resumes here
+          exclusive += v[k] & kValueMask;
+          used = k + 1;
+          done = flag == kFlagInclusive;
         }
-        exclusive += v & kValueMask;
-        if (flag == kFlagInclusive) break;
-        --pred;
+        if (done) break;
+        pred -= used;
+        if (used < kLookbackWindow && ++spins > kLookbackSpinLimit) {
+          atomicOr(error, kErrLookbackTimeout);
+          break;
+        }
       }
       store_volatile(&lookback[(size_t)tile * kBins + t], kFlagInclusive | ((exclusive + digitTotal) & kValueMask));
     }

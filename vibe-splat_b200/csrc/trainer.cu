@@ -342,9 +342,9 @@ uint64_t Trainer::bytes_per_gaussian() const {
   const uint64_t floats = 3 + 3 + 4 + 1 + 3ull * shCoeffs;
   const uint64_t params = (3 + 3 + 4 + 1 + 3) * 4 + rest;
   const uint64_t optimiser = floats * (stateStore == StateStore::F32 ? 8 : 4);
-  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets 4,
-  // raw sums 64, colour gradient and direction for the SH step 32.
-  const uint64_t perView = sizeof(Splat) + 4 + 16 + 4 + kRawStride * 4 + 32;
+  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets and
+  // reached-tile masks 8, raw sums 64, colour gradient and direction for the SH step 32.
+  const uint64_t perView = sizeof(Splat) + 4 + 16 + 8 + kRawStride * 4 + 32;
   // Geometry gradients between the chain rule and Adam: 11 floats.
   return params + optimiser + 11 * 4 + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
 }
@@ -419,7 +419,7 @@ void Trainer::ensure_view_buffers() {
     values.ensure(items * 4);
     tmpKeys.ensure(items * 4);
     tmpValues.ensure(items * 4);
-    offsets.ensure(items * 4);
+    offsets.ensure(items * 8); // entry offsets, then the reached-tile masks
     raw.ensure(items * kRawStride * 4);
     shGrad.ensure(items * 32);
     SB_CUDA(cudaMemset(raw.get(), 0, items * kRawStride * 4));
@@ -533,7 +533,8 @@ void Trainer::record_prepare() {
   const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
   launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
-                        offsets.get<uint32_t>(), counters, entryCapacity, scanScratch.get(), error, stream);
+                        offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, counters, entryCapacity, scanScratch.get(),
+                        error, stream);
   end(2);
 }
 
@@ -545,7 +546,8 @@ void Trainer::record_forward() {
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
   begin(3);
   launch_bin_emit(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
-                  offsets.get<uint32_t>(), entryCapacity, oneSort ? nullptr : entryKeys.get<uint32_t>(),
+                  offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, entryCapacity,
+                  oneSort ? nullptr : entryKeys.get<uint32_t>(),
                   oneSort ? entryKeys.get<unsigned long long>() : nullptr, entryValues.get<uint32_t>(), error, stream);
   if (oneSort) {
     const int bits = 32 + (int)bits_for((uint32_t)views.totalTiles);
