@@ -63,14 +63,20 @@ __device__ __forceinline__ AdamArgs adam_args(const ChainArgs &c) {
   return AdamArgs{c.beta1, c.beta2, c.epsilon, 1.0f / c.correction1, 1.0f / c.correction2, c.seed};
 }
 
+__device__ __forceinline__ float sqrt_sfu(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Adam on one parameter (step_parameter with radius < 0): the bias
-// corrections as multiplications by their reciprocals, the step's division
-// by the SFU reciprocal (the reference's GLSL division is not correctly
-// rounded either).
+// corrections as multiplications by their reciprocals, the square root and
+// the step's division on the SFU (the reference's GLSL sqrt and division are
+// not correctly rounded either).
 __device__ __forceinline__ void adam(float &value, float &m, float &v, float g, float rate, const AdamArgs &a) {
   m = a.beta1 * m + (1.0f - a.beta1) * g;
   v = a.beta2 * v + (1.0f - a.beta2) * g * g;
-  value -= __fdividef(rate * (m * a.invCorrection1), sqrtf(v * a.invCorrection2) + a.epsilon);
+  value -= __fdividef(rate * (m * a.invCorrection1), sqrt_sfu(v * a.invCorrection2) + a.epsilon);
 }
 
 // Steps parameter `at` of a group whose state is `state` (F32: m then v planes
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
 // the results are the same bits. Loads are issued a chunk of coefficients at a
 // time ahead of the arithmetic (the stores to the same arrays would otherwise
 // keep each load behind the previous element's store).
-constexpr int kStepChunk = 4;
+constexpr int kStepChunk = 2;
 
 __device__ __forceinline__ void load_state(const void *st, StateStore store, uint32_t count, uint32_t at, float &m, float &v,
                                            uint32_t &word) {
@@ -660,35 +666,42 @@ __global__ void __launch_bounds__(128, 4) k_chain_step(Params p, const ViewSet *
   }
 
   // The SH step, with the direction term from the coefficients before it.
+  // Chunks of kStepChunk coefficients, double-buffered: the next chunk's
+  // loads are issued before this chunk's arithmetic.
   const bool stepZeros = !args.selective;
   const int active = touched ? cam.activeCoeffs : 0;
   float gDir[3] = {0.f, 0.f, 0.f};
   if (touched || stepZeros) {
     const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
     const uint32_t count = n * shFloats;
-#pragma unroll
-    for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStepChunk) {
-      if (k0 >= p.shCoeffs) break;
-      float value[kStepChunk][3], m[kStepChunk][3], vv[kStepChunk][3];
-      uint32_t word[kStepChunk][3];
+    float value[2][kStepChunk][3], m[2][kStepChunk][3], vv[2][kStepChunk][3];
+    uint32_t word[2][kStepChunk][3];
+    auto load_chunk = [&](int k0, int buf) {
 #pragma unroll
       for (int kk = 0; kk < kStepChunk; ++kk) {
         const int k = k0 + kk;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          value[kk][c] = m[kk][c] = vv[kk][c] = 0.0f;
-          word[kk][c] = 0u;
+          value[buf][kk][c] = m[buf][kk][c] = vv[buf][kk][c] = 0.0f;
+          word[buf][kk][c] = 0u;
           if (k >= p.shCoeffs) continue;
           const uint32_t t = (uint32_t)(k * 3 + c) * n + i;
-          value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3u * n);
-          load_state(state.state[4], state.store, count, t, m[kk][c], vv[kk][c], word[kk][c]);
+          value[buf][kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3u * n);
+          load_state(state.state[4], state.store, count, t, m[buf][kk][c], vv[buf][kk][c], word[buf][kk][c]);
         }
       }
+    };
+    load_chunk(0, 0);
+#pragma unroll
+    for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStepChunk) {
+      const int buf = (k0 / kStepChunk) & 1;
+      if (k0 >= p.shCoeffs) break;
+      if (k0 + kStepChunk < kMaxCoeffs && k0 + kStepChunk < p.shCoeffs) load_chunk(k0 + kStepChunk, buf ^ 1);
       if (touched && cam.activeDegree > 0) {
 #pragma unroll
         for (int kk = 0; kk < kStepChunk; ++kk) {
           const int k = k0 + kk;
-          if (k >= 1 && k < active) direction_term(k, value[kk], gColour, dir, gDir);
+          if (k >= 1 && k < active) direction_term(k, value[buf][kk], gColour, dir, gDir);
         }
       }
 #pragma unroll
@@ -704,12 +717,13 @@ __global__ void __launch_bounds__(128, 4) k_chain_step(Params p, const ViewSet *
           const uint32_t plane = (uint32_t)(k * 3 + c);
           const uint32_t t = plane * n + i;
           const uint32_t hashIndex = (i * shFloats + plane) * 5u + 4u;
-          adam(value[kk][c], m[kk][c], vv[kk][c], g, rate, a);
-          store_state(state.state[4], state.store, count, t, m[kk][c], vv[kk][c], word[kk][c], hashIndex, a.seed);
+          float val = value[buf][kk][c], mm = m[buf][kk][c], v2 = vv[buf][kk][c];
+          adam(val, mm, v2, g, rate, a);
+          store_state(state.state[4], state.store, count, t, mm, v2, word[buf][kk][c], hashIndex, a.seed);
           if (k == 0) {
-            p.shDc[t] = value[kk][c];
+            p.shDc[t] = val;
           } else {
-            store_sh_rest<S>(p.shRest, t - 3u * n, value[kk][c], hashIndex, args.seed);
+            store_sh_rest<S>(p.shRest, t - 3u * n, val, hashIndex, args.seed);
           }
         }
       }

@@ -583,14 +583,15 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         const float aAct = act[q] ? alpha[q] : 0.0f;
         const float logRest = M::log(1.0f - aAct);
         const float T = M::exp((logTotal[q] - logBehind[q]) - logRest);
+        // Float sums only, so fused multiply-adds throughout.
         const float wA = act[q] ? T * alpha[q] : 0.0f;
-        g[6] += wA * Ax[q];
-        g[7] += wA * Ay[q];
-        g[8] += wA * Az[q];
-        g[9] += wA * perPixel;
+        g[6] = fmaf(wA, Ax[q], g[6]);
+        g[7] = fmaf(wA, Ay[q], g[7]);
+        g[8] = fmaf(wA, Az[q], g[8]);
+        g[9] = fmaf(wA, perPixel, g[9]);
         const float dAlpha =
             (act[q] && oe[q] < kAlphaMax) ? T * fmaf(Az[q], s.b - Bb[q], fmaf(Ay[q], s.g - Bg[q], Ax[q] * (s.r - Br[q]))) : 0.0f;
-        g[0] += dAlpha * ep[q];
+        g[0] = fmaf(dAlpha, ep[q], g[0]);
         const float dPower = dAlpha * alpha[q];
         const float vx = fmaf(s.qy, dy[q], s.qx * dx[q]), vy = fmaf(s.qz, dy[q], s.qy * dx[q]);
         const float g1 = dPower * vx, g2 = dPower * vy;
@@ -599,9 +600,10 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         g[10] += fabsf(g1);
         g[11] += fabsf(g2);
         const float h = dPower * 0.5f;
-        g[3] += h * vx * vx;
-        g[4] += h * vx * vy;
-        g[5] += h * vy * vy;
+        const float hx = h * vx;
+        g[3] = fmaf(hx, vx, g[3]);
+        g[4] = fmaf(hx, vy, g[4]);
+        g[5] = fmaf(h * vy, vy, g[5]);
         Br[q] = fmaf(aAct, s.r - Br[q], Br[q]);
         Bg[q] = fmaf(aAct, s.g - Bg[q], Bg[q]);
         Bb[q] = fmaf(aAct, s.b - Bb[q], Bb[q]);
