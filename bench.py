@@ -238,6 +238,48 @@ def reference_arm(args) -> None:
 # ----------------------------------------------------------------- our arm
 
 
+def stage_bytes(n: int, visible: int, entries: int, pixels: int, depth_passes: int) -> dict:
+    """Algorithmic HBM bytes per step of each timed stage, for the chosen form
+    (BF16 SH above DC, BF16-pair Adam state): what each stage must read and
+    write at least once, not what it happens to move."""
+    sh_bytes = 12 + 45 * 2  # DC in FP32, 45 higher coefficients in BF16
+    return {
+        # positions, scales, rotations, opacity (44 B) and SH in; splat (48),
+        # reach, depth key and index (12) out.
+        "project": n * (44 + sh_bytes + 60),
+        # keys and values read and written per pass, plus the histogram's read.
+        "depth sort": n * (16 * depth_passes + 4),
+        # per item: key, index, splat centre and conic, reach in; offset and mask out.
+        "count tiles": n * 8 + visible * (32 + 4 + 8),
+        # emission (offset, mask, rectangle in; tile and index out), two sort
+        # passes and a histogram over the entries, ranges.
+        "tile lists": visible * 24 + entries * (8 + 2 * 16 + 4 + 4),
+        # per entry its index and 48-byte splat; per pixel colour, log T and stop out.
+        "composite": entries * 52 + pixels * 20,
+        # image and target in for SSIM, 9 field planes out and in, adjoint out.
+        "loss": pixels * (16 + 4 + 36 + 36 + 16 + 16 + 4),
+        # per entry index and splat; per pixel image, adjoint, stop; sums out.
+        "backward": entries * 52 + pixels * 36 + visible * 56,
+        # sums, parameters and colour in for every Gaussian; SH, Adam state (59
+        # words) and parameters read and written for the touched ones.
+        "chain rule and step": n * (64 + 44) + visible * (16 + 2 * (44 + sh_bytes + 59 * 4)),
+    }
+
+
+def measured_traffic(stage: str):
+    """DRAM bytes per launch of the stage's kernel from the committed ncu
+    summary of the bench workload (profiles/*.md, a line 'traffic <stage>: N'),
+    or None."""
+    for path in sorted((ROOT / "profiles").glob("*.md")):
+        for line in path.read_text().splitlines():
+            if line.startswith(f"traffic {stage}:"):
+                try:
+                    return int(line.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
 def chosen_options(splat):
     return splat.TrainerOptions(sh_storage=splat.SH_BF16, state_storage=splat.STATE_BF16_PAIR,
                                 sort_form=splat.SORT_TILE_DEPTH_64, exact_math=False, use_graph=True, digit_bits=8)
@@ -344,22 +386,27 @@ def our_arm(args) -> None:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     dominant = max(stages, key=stages.get) if stages else None
-    # Algorithmic bytes of the backward pass per launch: each tile entry's index
-    # and 48-byte splat (52 B), per pixel its image, adjoint, stop (36 B), and
-    # 56 B of sums per visible splat.
-    algorithmic = {
-        "backward": 52.0 * entries + 36.0 * pixels + 56.0 * visible,
-        "composite": 52.0 * entries + 20.0 * pixels,
-        "project": 288.0 * args.gaussians,
-        "chain rule and step": 528.0 * args.gaussians,
-    }
+    n = args.gaussians
+    digits_used = tuned.get("digit_bits", chosen.digit_bits)
+    depth_passes = math.ceil(32 / digits_used)
+    algorithmic = stage_bytes(n, visible, entries, pixels, depth_passes)
+    stage_roof = {}
+    for name, ms_stage in stages.items():
+        b = algorithmic.get(name)
+        if b is None or ms_stage <= 0:
+            continue
+        gbs = b / (ms_stage * 1e-3) / 1e9
+        stage_roof[name] = {"bytes": b, "ms": ms_stage, "GB/s": gbs, "frac": gbs / hbm_peak}
     roof = None
-    if dominant is not None:
-        b = algorithmic.get(dominant, 0.0)
-        achieved = b / (stages[dominant] * 1e-3) / 1e9 if stages[dominant] > 0 else 0.0
-        roof = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "ms": stages[dominant],
+    if dominant is not None and dominant in stage_roof:
+        r = stage_roof[dominant]
+        traffic = measured_traffic(dominant)
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": r["GB/s"], "peak": hbm_peak, "unit": "GB/s",
+                "frac": r["frac"], "traffic": traffic, "ms": r["ms"],
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
+        if dominant in ("backward", "composite"):
+            roof["note"] = ("issue-bound, not HBM-bound: the FP32/ALU issue rate is the limit (ncu summary under "
+                            "profiles/); the HBM fraction is given for the record")
 
     plain = None
     if not args.no_plain:
@@ -390,10 +437,10 @@ def our_arm(args) -> None:
     tile_bits = max(1, math.ceil(math.log2(((WIDTH + 15) // 16) * ((HEIGHT + 15) // 16))))
     # Kernels of one step: preprocess, [histogram + passes of the depth sort],
     # count+scan, emit, histogram + passes of the entry sort, ranges, forward,
-    # SSIM, loss, loss totals, backward, chain, geometry Adam, SH step.
+    # SSIM, loss, loss totals, backward, the fused chain rule + Adam + SH step.
     depth_launches = (1 + math.ceil(32 / digits)) if form == 0 else 0
     entry_launches = 1 + math.ceil((tile_bits + (32 if form == 1 else 0)) / digits)
-    launches_per_step = 12 + depth_launches + entry_launches
+    launches_per_step = 10 + depth_launches + entry_launches
     form_name = "depth then tile sort" if form == 0 else "64-bit tile|depth keys"
     out = {
         "metric": "train iters/s @1M Gaussians 1237x822 (fwd+bwd+Adam per view)",
@@ -410,6 +457,7 @@ def our_arm(args) -> None:
                    "tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roof,
+        "stage_roofline": stage_roof,
         "stages_ms": stages,
         "plain_fp32": plain,
         "speedup_vs_plain": (value / world) / plain["iters_per_s"] if plain else None,
