@@ -32,14 +32,27 @@ __device__ __forceinline__ TileRect splat_tiles(const float4 ce, int gridW, int 
 }
 
 // Whether the splat reaches any pixel centre of tile (tx, ty)
-// (splat_reaches_tile). The closest point of each tile edge to the centre is
-// found by clamping the ellipse's tangent point; the two horizontal edges'
-// tangent points depend on the row only, so a caller that walks a row can
-// compute them once (row_tangents) and pass them in. Same operations, same
-// order as evaluating everything per tile.
+// (splat_reaches_tile): the closest point of each tile edge to the centre is
+// found by clamping the ellipse's tangent point to the edge. The tangent
+// points on the two vertical edges depend on the column only, those on the
+// two horizontal edges on the row only, so they are computed per column and
+// per row (col_tangents, row_tangents) and the test combines them: the same
+// operations in the same order as evaluating everything per tile.
+struct ColTangents {
+  float lowX, highX, yLow, yHigh; // edge offsets from the centre and their unclamped tangent y
+};
 struct RowTangents {
   float lowY, highY, uLow, uHigh; // edge offsets from the centre and their unclamped tangent x
 };
+
+__device__ __forceinline__ ColTangents col_tangents(const float4 q, const float4 ce, uint32_t tx) {
+  ColTangents c;
+  c.lowX = ((float)tx * 16.0f + 0.5f) - ce.x;
+  c.highX = c.lowX + 15.0f;
+  c.yLow = -q.y * c.lowX / q.z;
+  c.yHigh = -q.y * c.highX / q.z;
+  return c;
+}
 
 __device__ __forceinline__ RowTangents row_tangents(const float4 q, const float4 ce, uint32_t ty) {
   RowTangents r;
@@ -50,15 +63,14 @@ __device__ __forceinline__ RowTangents row_tangents(const float4 q, const float4
   return r;
 }
 
-__device__ __forceinline__ bool reaches_tile_row(const float4 q, const float4 ce, float reach, uint32_t tx, const RowTangents &row) {
-  const float lowX = ((float)tx * 16.0f + 0.5f) - ce.x, lowY = row.lowY;
-  const float highX = lowX + 15.0f, highY = row.highY;
+__device__ __forceinline__ bool reaches_tile(const float4 q, float reach, const ColTangents &col, const RowTangents &row) {
+  const float lowX = col.lowX, highX = col.highX, lowY = row.lowY, highY = row.highY;
   if (lowX <= 0.0f && lowY <= 0.0f && highX >= 0.0f && highY >= 0.0f) return true;
   float least = 1e30f;
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
     const float x = side == 0 ? lowX : highX;
-    const float y = fminf(fmaxf(-q.y * x / q.z, lowY), highY);
+    const float y = fminf(fmaxf(side == 0 ? col.yLow : col.yHigh, lowY), highY);
     least = fminf(least, q.x * x * x + 2.0f * q.y * x * y + q.z * y * y);
     const float v = side == 0 ? lowY : highY;
     const float u = fminf(fmaxf(side == 0 ? row.uLow : row.uHigh, lowX), highX);
@@ -67,15 +79,14 @@ __device__ __forceinline__ bool reaches_tile_row(const float4 q, const float4 ce
   return least <= reach * 1.001f + 1e-3f;
 }
 
-__device__ __forceinline__ bool splat_reaches_tile(const float4 q, const float4 ce, float reach, uint32_t tx, uint32_t ty) {
-  return reaches_tile_row(q, ce, reach, tx, row_tangents(q, ce, ty));
-}
-
 // Splats whose tile rectangle holds more than this many tiles are tested by a
 // whole warp, one tile per lane, so that no thread walks a large splat's
 // rectangle alone while its block (and, through the scan, every later block)
 // waits for it.
 constexpr uint32_t kWarpTiles = 16;
+// Columns and rows of the per-warp tangent tables for those rectangles; a
+// larger rectangle computes its tangents tile by tile.
+constexpr uint32_t kTableMax = 64;
 
 __device__ __forceinline__ uint32_t rect_area(const TileRect &t) { return (t.x1 - t.x0 + 1u) * (t.y1 - t.y0 + 1u); }
 
@@ -86,21 +97,39 @@ __device__ __forceinline__ uint32_t reach_mask(const float4 q, const float4 ce, 
   for (uint32_t y = t.y0; y <= t.y1; ++y) {
     const RowTangents row = row_tangents(q, ce, y);
     for (uint32_t x = t.x0; x <= t.x1; ++x, bit <<= 1)
-      if (reaches_tile_row(q, ce, reach, x, row)) mask |= bit;
+      if (reaches_tile(q, reach, col_tangents(q, ce, x), row)) mask |= bit;
   }
   return mask;
 }
 
-// The tiles of the rectangle in row-major order, 32 at a time: lane l tests
-// tile base + l. Returns the lanes whose tile the splat reaches.
+// A large rectangle's tangent tables, filled by the whole warp. False (and
+// nothing filled) when the rectangle is wider or taller than the tables.
+__device__ __forceinline__ bool fill_tables(const float4 q, const float4 ce, const TileRect &t, uint32_t lane, ColTangents *cols,
+                                            RowTangents *rows) {
+  const uint32_t width = t.x1 - t.x0 + 1u, height = t.y1 - t.y0 + 1u;
+  if (width > kTableMax || height > kTableMax) return false;
+  for (uint32_t c = lane; c < width; c += 32u) cols[c] = col_tangents(q, ce, t.x0 + c);
+  for (uint32_t r = lane; r < height; r += 32u) rows[r] = row_tangents(q, ce, t.y0 + r);
+  __syncwarp();
+  return true;
+}
+
+// The tiles base .. base + 31 of the rectangle in row-major order: lane l
+// tests tile base + l. Returns the lanes whose tile the splat reaches. The
+// row is found with a float reciprocal: (i + 1/2) / width lies at least
+// 1/(2 width) from an integer, far more than the rounding error.
 __device__ __forceinline__ uint32_t warp_reach(const float4 q, const float4 ce, float reach, const TileRect &t, uint32_t width,
-                                               uint32_t area, uint32_t base, uint32_t lane, uint32_t &x, uint32_t &y) {
+                                               float invWidth, uint32_t area, uint32_t base, uint32_t lane,
+                                               const ColTangents *cols, const RowTangents *rows, uint32_t &x, uint32_t &y) {
   const uint32_t li = base + lane;
   bool hit = false;
   if (li < area) {
-    y = t.y0 + li / width;
-    x = t.x0 + li % width;
-    hit = splat_reaches_tile(q, ce, reach, x, y);
+    const uint32_t r = (uint32_t)(((float)li + 0.5f) * invWidth);
+    const uint32_t c = li - r * width;
+    x = t.x0 + c;
+    y = t.y0 + r;
+    hit = cols != nullptr ? reaches_tile(q, reach, cols[c], rows[r])
+                          : reaches_tile(q, reach, col_tangents(q, ce, x), row_tangents(q, ce, y));
   }
   return __ballot_sync(0xFFFFFFFFu, hit);
 }
@@ -127,6 +156,8 @@ __global__ void __launch_bounds__(kScanThreads)
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ unsigned long long s_exclusive;
+  __shared__ ColTangents s_cols[kScanThreads / 32][kTableMax];
+  __shared__ RowTangents s_rows[kScanThreads / 32][kTableMax];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   if (t == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
@@ -182,11 +213,15 @@ __global__ void __launch_bounds__(kScanThreads)
       const float rcb = reach[bs];
       const TileRect rect = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
       const uint32_t width = rect.x1 - rect.x0 + 1u, area = rect_area(rect);
+      const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, rect, lane, s_cols[warp], s_rows[warp]);
+      const float invWidth = 1.0f / (float)width;
       uint32_t total = 0, hits = 0, x = 0, y = 0;
       for (uint32_t base = 0; base < area; base += 32u) {
-        hits = warp_reach(sp.conicOpacity, sp.centerExtent, rcb, rect, width, area, base, lane, x, y);
+        hits = warp_reach(sp.conicOpacity, sp.centerExtent, rcb, rect, width, invWidth, area, base, lane,
+                          tables ? s_cols[warp] : nullptr, s_rows[warp], x, y);
         total += (uint32_t)__popc(hits);
       }
+      __syncwarp(); // the tables are read before the next rectangle fills them
       if (lane == src) {
         c = total;
         mask[j] = area <= 32u ? hits : 0u; // the emission replays masks of one word only
@@ -271,21 +306,35 @@ __global__ void __launch_bounds__(kScanThreads)
   }
 }
 
+// Emission. Rectangles of up to 32 tiles replay the counting pass's masks
+// with the warp's entries laid out flat: lane l writes entries l, l + 32, ...
+// of the warp's run, so consecutive lanes write consecutive slots. Larger
+// rectangles are tested again by the whole warp.
 __global__ void __launch_bounds__(256)
     k_bin_emit(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
                const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
                const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ masks, uint32_t capacity,
-               uint32_t *__restrict__ tileKeys32,
-               unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues, uint32_t *error) {
+               uint32_t *__restrict__ tileKeys32, unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues,
+               uint32_t *error) {
   const ViewSet &views = *viewsPtr;
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
-  // Whole warps stay to the end: large rectangles are emitted by all 32 lanes.
+  __shared__ ColTangents s_cols[8][kTableMax];
+  __shared__ RowTangents s_rows[8][kTableMax];
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  // Whole warps stay to the end: every loop below is warp-wide.
   const bool valid = r < items && itemKeys[r] != kInvisible;
   const uint32_t depthKey = valid ? itemKeys[r] : 0u;
   const uint32_t s = valid ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
+  const int view = valid ? item_view(s, n, views.count) : 0;
+  TileRect t{0u, 0u, 0u, 0u};
+  if (valid) t = splat_tiles(splats[s].centerExtent, views.v[view].gridW, views.v[view].gridH);
+  const uint32_t width = t.x1 - t.x0 + 1u, area = valid ? rect_area(t) : 0u;
+  const bool big = area > 32u;
+  const uint32_t mask = valid && !big ? masks[r] : 0u;
+  const uint32_t first = valid ? offsets[r] : 0u;
   bool overflow = false;
-  auto put = [&](uint32_t slot, const ViewParams &cam, uint32_t x, uint32_t y, uint32_t key, uint32_t splat) {
+  auto put = [&](uint32_t slot, int v, uint32_t x, uint32_t y, uint32_t key, uint32_t splat) {
     if (slot < capacity) {
+      const ViewParams &cam = views.v[v];
       const uint32_t tileId = y * (uint32_t)cam.gridW + x;
       if (tileKeys64 != nullptr) {
         tileKeys64[slot] = ((unsigned long long)((uint32_t)cam.tileBase + tileId) << 32) | key;
@@ -297,40 +346,71 @@ __global__ void __launch_bounds__(256)
       overflow = true;
     }
   };
-  bool big = false;
-  if (valid) {
-    const ViewParams &cam = views.v[item_view(s, n, views.count)];
-    const TileRect t = splat_tiles(splats[s].centerExtent, cam.gridW, cam.gridH);
-    const uint32_t width = t.x1 - t.x0 + 1u;
-    big = rect_area(t) > 32u;
-    if (!big) {
-      // The counting pass's tests, replayed from its mask in row-major order.
-      uint32_t slot = offsets[r];
-      for (uint32_t bits = masks[r]; bits != 0u; bits &= bits - 1u) {
-        const uint32_t b = (uint32_t)(__ffs(bits) - 1);
-        put(slot++, cam, t.x0 + b % width, t.y0 + b / width, depthKey, s);
+
+  // The small rectangles' entries, flat: an inclusive scan of their counts
+  // over the warp, then entry j belongs to the first lane whose prefix passes j.
+  const uint32_t count = (uint32_t)__popc(mask);
+  uint32_t inclusive = count;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inclusive, o);
+    if (lane >= (uint32_t)o) inclusive += v;
+  }
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, inclusive, 31);
+  const uint32_t exclusive = inclusive - count;
+  for (uint32_t base = 0; base < total; base += 32u) {
+    const uint32_t j = base + lane;
+    uint32_t owner = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1) {
+      const uint32_t v = __shfl_sync(0xFFFFFFFFu, inclusive, owner + step - 1u);
+      if (v <= j) owner += step;
+    }
+    const uint32_t oExclusive = __shfl_sync(0xFFFFFFFFu, exclusive, owner);
+    const uint32_t oMask = __shfl_sync(0xFFFFFFFFu, mask, owner);
+    const uint32_t oFirst = __shfl_sync(0xFFFFFFFFu, first, owner);
+    const uint32_t oX0 = __shfl_sync(0xFFFFFFFFu, t.x0, owner), oY0 = __shfl_sync(0xFFFFFFFFu, t.y0, owner);
+    const uint32_t oWidth = __shfl_sync(0xFFFFFFFFu, width, owner);
+    const uint32_t oSplat = __shfl_sync(0xFFFFFFFFu, s, owner), oKey = __shfl_sync(0xFFFFFFFFu, depthKey, owner);
+    const int oView = __shfl_sync(0xFFFFFFFFu, view, owner);
+    if (j < total) {
+      // The rank-th set bit of the owner's mask: the largest p with rank set bits below it.
+      const uint32_t rank = j - oExclusive;
+      uint32_t bit = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t p = bit + step;
+        if ((uint32_t)__popc(oMask & ((1u << p) - 1u)) <= rank) bit = p;
       }
+      const uint32_t row = bit / oWidth;
+      put(oFirst + rank, oView, oX0 + (bit - row * oWidth), oY0 + row, oKey, oSplat);
     }
   }
+
   // Rectangles of more than 32 tiles are tested again, by the whole warp;
   // row-major order kept by counting the lower lanes' hits.
   for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
     const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
     const uint32_t bs = __shfl_sync(0xFFFFFFFFu, s, src);
     const uint32_t key = __shfl_sync(0xFFFFFFFFu, depthKey, src);
-    const uint32_t first = __shfl_sync(0xFFFFFFFFu, r, src);
-    const ViewParams &cam = views.v[item_view(bs, n, views.count)];
+    const uint32_t bFirst = __shfl_sync(0xFFFFFFFFu, first, src);
+    const int bView = __shfl_sync(0xFFFFFFFFu, view, src);
+    const ViewParams &cam = views.v[bView];
     const Splat sp = splats[bs];
     const float rc = reach[bs];
-    const TileRect t = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
-    const uint32_t width = t.x1 - t.x0 + 1u, area = rect_area(t);
-    uint32_t slot = offsets[first];
-    for (uint32_t base = 0; base < area; base += 32u) {
+    const TileRect bt = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    const uint32_t bWidth = bt.x1 - bt.x0 + 1u, bArea = rect_area(bt);
+    const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, bt, lane, s_cols[warp], s_rows[warp]);
+    const float invWidth = 1.0f / (float)bWidth;
+    uint32_t slot = bFirst;
+    for (uint32_t base = 0; base < bArea; base += 32u) {
       uint32_t x = 0, y = 0;
-      const uint32_t hits = warp_reach(sp.conicOpacity, sp.centerExtent, rc, t, width, area, base, lane, x, y);
-      if ((hits >> lane) & 1u) put(slot + (uint32_t)__popc(hits & ((1u << lane) - 1u)), cam, x, y, key, bs);
+      const uint32_t hits = warp_reach(sp.conicOpacity, sp.centerExtent, rc, bt, bWidth, invWidth, bArea, base, lane,
+                                       tables ? s_cols[warp] : nullptr, s_rows[warp], x, y);
+      if ((hits >> lane) & 1u) put(slot + (uint32_t)__popc(hits & ((1u << lane) - 1u)), bView, x, y, key, bs);
       slot += (uint32_t)__popc(hits);
     }
+    __syncwarp(); // the tables are read before the next rectangle fills them
   }
   if (overflow) atomicOr(error, kErrEntryOverflow);
 }

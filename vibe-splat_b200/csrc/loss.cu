@@ -54,15 +54,19 @@ __device__ __forceinline__ float block_sum(float v, float *s_warp) {
 
 // The tile with a 5-pixel halo on every side, one float per pixel and
 // plane, zero outside the image: a tap there adds an exact zero, as if the
-// window had been cut at the border.
+// window had been cut at the border. The horizontal pass gives each thread
+// two neighbouring outputs of a row, which share 10 of their 11 taps.
 constexpr int kSpanCols = kTileSize + 2 * kHalo;
 constexpr int kStage = kRows * kSpanCols;
+constexpr int kStagePlane = kStage;
+constexpr int kPairs = kRows * kTileSize / 2; // horizontal work items
+__device__ __forceinline__ int stage_row(int r) { return r * kSpanCols; }
 
 __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
                                                       const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
                                                       float2 *__restrict__ partials) {
   const ViewSet &views = *viewsPtr;
-  __shared__ float s_in[6][kStage]; // image r, g, b, then target r, g, b
+  __shared__ float s_in[6][kStagePlane]; // image r, g, b, then target r, g, b
   __shared__ float s_h[5][3][kSpan];
   __shared__ float s_warp[kTilePixels / 32];
   const int tile = blockIdx.x;
@@ -74,7 +78,8 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
   const size_t plane = (size_t)views.totalPixels;
 
   for (int i = threadIdx.x; i < kStage; i += kTilePixels) {
-    const int y = y0 + i / kSpanCols - kHalo, x = x0 + i % kSpanCols - kHalo;
+    const int r = i / kSpanCols, c = i % kSpanCols;
+    const int y = y0 + r - kHalo, x = x0 + c - kHalo;
     float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
     float3 b3 = make_float3(0.f, 0.f, 0.f);
     if (y >= 0 && y < H && x >= 0 && x < W) {
@@ -82,46 +87,58 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
       a4 = image[at];
       b3 = unpack_unorm(target[at]);
     }
-    s_in[0][i] = a4.x;
-    s_in[1][i] = a4.y;
-    s_in[2][i] = a4.z;
-    s_in[3][i] = b3.x;
-    s_in[4][i] = b3.y;
-    s_in[5][i] = b3.z;
+    const int o = stage_row(r) + c;
+    s_in[0][o] = a4.x;
+    s_in[1][o] = a4.y;
+    s_in[2][o] = a4.z;
+    s_in[3][o] = b3.x;
+    s_in[4][o] = b3.y;
+    s_in[5][o] = b3.z;
   }
   __syncthreads();
 
-  // Horizontal pass: tile columns, tile rows plus the halo rows.
-  for (int i = threadIdx.x; i < kSpan; i += kTilePixels) {
-    const int r = i / kTileSize, c = i % kTileSize;
+  // Horizontal pass: tile columns, tile rows plus the halo rows, two
+  // neighbouring columns per thread.
+  for (int i = threadIdx.x; i < kPairs; i += kTilePixels) {
+    const int r = i / (kTileSize / 2), c = 2 * (i % (kTileSize / 2));
     const int y = y0 + r - kHalo, x = x0 + c;
-    float m[5][3] = {};
+    float m[2][5][3] = {};
     if (y >= 0 && y < H && x < W) {
+      const int row = stage_row(r) + c;
 #pragma unroll
-      for (int u = 0; u < 11; ++u) {
-        const float w = c_weights[u];
-        const int at = r * kSpanCols + c + u;
+      for (int u = 0; u < 12; ++u) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const float a = s_in[k][at], b = s_in[3 + k][at];
-          const float wa = w * a;
-          m[0][k] = fmaf(w, a, m[0][k]);
-          m[1][k] = fmaf(w, b, m[1][k]);
-          m[2][k] = fmaf(wa, a, m[2][k]);
-          m[3][k] = fmaf(w * b, b, m[3][k]);
-          m[4][k] = fmaf(wa, b, m[4][k]);
+          const float a = s_in[k][row + u], b = s_in[3 + k][row + u];
+#pragma unroll
+          for (int o = 0; o < 2; ++o) {
+            const int tap = u - o; // output c + o takes staged column c + o + tap
+            if (tap < 0 || tap > 10) continue;
+            const float w = c_weights[tap];
+            const float wa = w * a;
+            m[o][0][k] = fmaf(w, a, m[o][0][k]);
+            m[o][1][k] = fmaf(w, b, m[o][1][k]);
+            m[o][2][k] = fmaf(wa, a, m[o][2][k]);
+            m[o][3][k] = fmaf(w * b, b, m[o][3][k]);
+            m[o][4][k] = fmaf(wa, b, m[o][4][k]);
+          }
         }
       }
-      const float inv = 1.0f / window_norm(x, W);
+#pragma unroll
+      for (int o = 0; o < 2; ++o) {
+        const float inv = x + o < W ? 1.0f / window_norm(x + o, W) : 0.0f;
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) m[o][q][k] *= inv;
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < 2; ++o)
 #pragma unroll
       for (int q = 0; q < 5; ++q)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) m[q][k] *= inv;
-    }
-#pragma unroll
-    for (int q = 0; q < 5; ++q)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) s_h[q][k][i] = m[q][k];
+        for (int k = 0; k < 3; ++k) s_h[q][k][r * kTileSize + c + o] = m[o][q][k];
   }
   __syncthreads();
 
@@ -168,7 +185,7 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
                                                       const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
                                                       float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials) {
   const ViewSet &views = *viewsPtr;
-  __shared__ float s_in[9][kStage];
+  __shared__ float s_in[9][kStagePlane]; // the nine field planes
   __shared__ float s_h[3][3][kSpan];
   __shared__ float s_warp[kTilePixels / 32];
   const int tile = blockIdx.x;
@@ -180,35 +197,51 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   const size_t plane = (size_t)views.totalPixels;
 
   for (int i = threadIdx.x; i < kStage; i += kTilePixels) {
-    const int y = y0 + i / kSpanCols - kHalo, x = x0 + i % kSpanCols - kHalo;
+    const int r = i / kSpanCols, c = i % kSpanCols;
+    const int y = y0 + r - kHalo, x = x0 + c - kHalo;
     const bool in = y >= 0 && y < H && x >= 0 && x < W;
     const size_t at = in ? base + (size_t)y * W + x : 0;
+    const int o = stage_row(r) + c;
 #pragma unroll
-    for (int f = 0; f < 9; ++f) s_in[f][i] = in ? fields[f * plane + at] : 0.0f;
+    for (int f = 0; f < 9; ++f) s_in[f][o] = in ? fields[f * plane + at] : 0.0f;
   }
   __syncthreads();
 
-  for (int i = threadIdx.x; i < kSpan; i += kTilePixels) {
-    const int r = i / kTileSize, c = i % kTileSize;
+  for (int i = threadIdx.x; i < kPairs; i += kTilePixels) {
+    const int r = i / (kTileSize / 2), c = 2 * (i % (kTileSize / 2));
     const int y = y0 + r - kHalo, x = x0 + c;
-    float m[3][3] = {};
+    float m[2][3][3] = {};
     if (y >= 0 && y < H && x < W) {
+      const int row = stage_row(r) + c;
 #pragma unroll
-      for (int u = 0; u < 11; ++u) {
-        const float w = c_weights[u];
-        const int at = r * kSpanCols + c + u;
+      for (int u = 0; u < 12; ++u) {
+#pragma unroll
+        for (int f = 0; f < 9; ++f) {
+          const float v = s_in[f][row + u];
+#pragma unroll
+          for (int o = 0; o < 2; ++o) {
+            const int tap = u - o;
+            if (tap < 0 || tap > 10) continue;
+            m[o][f / 3][f % 3] = fmaf(c_weights[tap], v, m[o][f / 3][f % 3]);
+          }
+        }
+      }
+      if (x + 1 >= W) {
 #pragma unroll
         for (int q = 0; q < 3; ++q)
 #pragma unroll
-          for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_in[q * 3 + k][at], m[q][k]);
+          for (int k = 0; k < 3; ++k) m[1][q][k] = 0.0f;
       }
     }
 #pragma unroll
-    for (int q = 0; q < 3; ++q)
+    for (int o = 0; o < 2; ++o)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) s_h[q][k][i] = m[q][k];
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s_h[q][k][r * kTileSize + c + o] = m[o][q][k];
   }
   __syncthreads();
+
   const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
   float own = 0.0f;
   if (px < W && py < H) {

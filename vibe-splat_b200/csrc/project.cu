@@ -12,8 +12,10 @@ namespace sb {
 
 namespace {
 
+constexpr int kMaxShCoeffs = 16;
+
 template <ShStore S>
-__global__ void __launch_bounds__(256) k_preprocess(Params p, const ViewSet *__restrict__ viewsPtr, Splat *__restrict__ splats,
+__global__ void __launch_bounds__(256, 3) k_preprocess(Params p, const ViewSet *__restrict__ viewsPtr, Splat *__restrict__ splats,
                                                     float *__restrict__ reachOut, uint32_t *__restrict__ depthKeys,
                                                     uint32_t *__restrict__ values) {
   const ViewSet &views = *viewsPtr;
@@ -25,20 +27,23 @@ __global__ void __launch_bounds__(256) k_preprocess(Params p, const ViewSet *__r
   depthKeys[at] = kInvisible;
   if (values != nullptr) values[at] = i;
 
+  // Every parameter load first, so that they are in flight together.
   const float px = p.positions[i * 3], py = p.positions[i * 3 + 1], pz = p.positions[i * 3 + 2];
+  const float rawOpacity = p.opacities[i];
+  const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
+  const float rawScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
   const float tx = fmaf(cam.R[2], pz, fmaf(cam.R[1], py, fmaf(cam.R[0], px, cam.T[0])));
   const float ty = fmaf(cam.R[5], pz, fmaf(cam.R[4], py, fmaf(cam.R[3], px, cam.T[1])));
   const float tz = fmaf(cam.R[8], pz, fmaf(cam.R[7], py, fmaf(cam.R[6], px, cam.T[2])));
   // Written so that NaN fails, as in the reference.
   if (!(tz >= cam.nearPlane)) return;
-  const float opacity = 1.0f / (1.0f + splat_expf(-p.opacities[i]));
+  const float opacity = 1.0f / (1.0f + splat_expf(-rawOpacity));
   if (!(opacity >= kAlphaMin)) return;
 
-  const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
   const float len = sqrtf(fmaf(rq.w, rq.w, fmaf(rq.z, rq.z, fmaf(rq.y, rq.y, rq.x * rq.x))));
   if (!(len >= kMinQuaternionLength)) return;
   const float qw = rq.x / len, qx = rq.y / len, qy = rq.z / len, qz = rq.w / len;
-  const float s[3] = {splat_expf(p.scales[i * 3]), splat_expf(p.scales[i * 3 + 1]), splat_expf(p.scales[i * 3 + 2])};
+  const float s[3] = {splat_expf(rawScale[0]), splat_expf(rawScale[1]), splat_expf(rawScale[2])};
   float Rq[3][3];
   quat_to_matrix(qw, qx, qy, qz, Rq);
   // M = Rq diag(s); sigma = M M^T (no 3D filter).
@@ -98,10 +103,19 @@ __global__ void __launch_bounds__(256) k_preprocess(Params p, const ViewSet *__r
   const float dlen = sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
   float basis[16];
   sh_basis(dx / dlen, dy / dlen, dz / dlen, cam.activeDegree, basis);
-  float col[3] = {0.5f, 0.5f, 0.5f};
-  for (int k = 0; k < cam.activeCoeffs; ++k) {
+  // Unrolled to the largest count so that the coefficients' loads are issued
+  // together; the sums run in coefficient order as before.
+  float coef[kMaxShCoeffs][3];
 #pragma unroll
-    for (int ch = 0; ch < 3; ++ch) col[ch] = fmaf(basis[k], sh_coefficient<S>(p, i, k, ch), col[ch]);
+  for (int k = 0; k < kMaxShCoeffs; ++k)
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) coef[k][ch] = k < cam.activeCoeffs ? sh_coefficient<S>(p, i, k, ch) : 0.0f;
+  float col[3] = {0.5f, 0.5f, 0.5f};
+#pragma unroll
+  for (int k = 0; k < kMaxShCoeffs; ++k) {
+    if (k >= cam.activeCoeffs) break;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) col[ch] = fmaf(basis[k], coef[k][ch], col[ch]);
   }
   if (!(fabsf(col[0]) < 1e30f && fabsf(col[1]) < 1e30f && fabsf(col[2]) < 1e30f)) return;
 
