@@ -26,7 +26,11 @@ enum class StateStore : int { F32 = 0, BF16Pair = 1 };
 
 // Trainable parameters, in this library's HBM layout: positions, log-scales and
 // quaternions per Gaussian (12, 12, 16 bytes), opacity logits (4 bytes), SH
-// planar: shDc[c * n + i] and shRest[((k - 1) * 3 + c) * n + i].
+// planar: shDc[c * planeStride + i] and shRest[((k - 1) * 3 + c) * planeStride
+// + i]. planeStride is n rounded up to kPlaneAlign, so that every plane starts
+// 16-byte aligned at every multiple of kPlaneAlign Gaussians (bulk copies);
+// the SH Adam state uses the same planes.
+constexpr uint32_t kPlaneAlign = 128;
 struct Params {
   float *positions;
   float *scales;
@@ -36,6 +40,7 @@ struct Params {
   void *shRest;
   ShStore shStore;
   uint32_t n;
+  uint32_t planeStride;
   int shDegree;
   int shCoeffs;
 };
@@ -131,6 +136,6 @@ struct GradientsOut {
 };
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad,
-                  float *densifyStats, const uint32_t *error, cudaStream_t stream);
+                  float *densifyStats, uint32_t *error, cudaStream_t stream);
 
 } // namespace sb

@@ -18,6 +18,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include "bulk.cuh"
 #include "kernels.cuh"
 #include "shmath.cuh"
 
@@ -520,7 +521,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
   const bool stepZeros = !args.selective;
   if (!touched && !stepZeros) return;
   const AdamArgs a = adam_args(args);
-  const size_t count = (size_t)n * shFloats;
+  const size_t ps = p.planeStride, count = ps * shFloats;
   // Every load first, then the arithmetic, then the stores: the values and the
   // state are reached through plain pointers, so a load placed after a store
   // could not be moved before it, and the 12 updates would run one by one.
@@ -534,8 +535,8 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       value[kk][c] = m[kk][c] = vv[kk][c] = 0.0f;
       word[kk][c] = 0u;
       if (k >= p.shCoeffs) continue;
-      const size_t t = (size_t)(k * 3 + c) * n + i;
-      value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3 * (size_t)n);
+      const size_t t = (size_t)(k * 3 + c) * ps + i;
+      value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3 * ps);
       if (state.store == StateStore::F32) {
         m[kk][c] = static_cast<const float *>(state.state[4])[t];
         vv[kk][c] = static_cast<const float *>(state.state[4])[count + t];
@@ -555,7 +556,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
     for (int c = 0; c < 3; ++c) {
       if (g[kk][c] == 0.0f && !stepZeros) continue;
       const uint32_t plane = (uint32_t)(k * 3 + c);
-      const size_t t = (size_t)plane * n + i;
+      const size_t t = (size_t)plane * ps + i;
       const uint32_t hashIndex = (i * (uint32_t)shFloats + plane) * 5u + 4u;
       adam(value[kk][c], m[kk][c], vv[kk][c], g[kk][c], rate, a);
       if (state.store == StateStore::F32) {
@@ -568,7 +569,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       if (k == 0) {
         p.shDc[t] = value[kk][c];
       } else {
-        store_sh_rest<S>(p.shRest, t - 3 * (size_t)n, value[kk][c], hashIndex, args.seed);
+        store_sh_rest<S>(p.shRest, t - 3 * ps, value[kk][c], hashIndex, args.seed);
       }
     }
   }
@@ -579,10 +580,15 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
 // for the direction term and for their own step, and no gradient leaves
 // registers. Element by element the arithmetic, the hash indices and the
 // order of the sums are those of k_chain, k_adam_geometry and k_sh_step, so
-// the results are the same bits. Loads are issued a chunk of coefficients at a
-// time ahead of the arithmetic (the stores to the same arrays would otherwise
-// keep each load behind the previous element's store).
-constexpr int kStepChunk = 2;
+// the results are the same bits.
+//
+// A block's SH planes and SH Adam state (one 16-byte aligned segment of
+// kStepThreads elements per plane) are brought into shared memory by bulk
+// asynchronous copies issued first thing, so they land while the chain rule
+// runs; the SH step then reads them from shared memory.
+constexpr int kStepThreads = kPlaneAlign;
+// Polls of the staging barrier before the kernel gives up on it.
+constexpr int kStageSpinLimit = 1 << 22;
 
 __device__ __forceinline__ void load_state(const void *st, StateStore store, uint32_t count, uint32_t at, float &m, float &v,
                                            uint32_t &word) {
@@ -607,16 +613,66 @@ __device__ __forceinline__ void store_state(void *st, StateStore store, uint32_t
   }
 }
 
+// Shared-memory bytes of a block's staged SH planes and state.
+__host__ __device__ inline uint32_t step_stage_bytes(int coeffs, int shBytes, bool stateF32) {
+  const uint32_t planes = 3u * (uint32_t)coeffs;
+  return 3u * kStepThreads * 4u + (planes - 3u) * kStepThreads * (uint32_t)shBytes +
+         (stateF32 ? 2u : 1u) * planes * kStepThreads * 4u;
+}
+
+template <ShStore S> __device__ __forceinline__ float staged_sh_rest(const unsigned char *rest, uint32_t at) {
+  if constexpr (S == ShStore::F32) {
+    return reinterpret_cast<const float *>(rest)[at];
+  } else if constexpr (S == ShStore::BF16) {
+    return __uint_as_float((uint32_t)reinterpret_cast<const uint16_t *>(rest)[at] << 16);
+  } else {
+    return __half2float(reinterpret_cast<const __half *>(rest)[at]);
+  }
+}
+
 template <ShStore S, bool FIXED>
-__global__ void __launch_bounds__(128, 4) k_chain_step(Params p, const ViewSet *__restrict__ viewsPtr, const void *__restrict__ rawIn,
-                                                       const Splat *__restrict__ splats, const ChainArgs *__restrict__ argsPtr,
-                                                       OptimState state, float *__restrict__ densifyStats, const uint32_t *error) {
+__global__ void __launch_bounds__(kStepThreads, 4) k_chain_step(Params p, const ViewSet *__restrict__ viewsPtr,
+                                                                const void *__restrict__ rawIn, const Splat *__restrict__ splats,
+                                                                const ChainArgs *__restrict__ argsPtr, OptimState state,
+                                                                float *__restrict__ densifyStats, uint32_t *error) {
+  constexpr uint32_t kShBytes = S == ShStore::F32 ? 4u : 2u;
+  extern __shared__ __align__(128) unsigned char s_stage[];
+  __shared__ __align__(8) uint64_t s_bar;
   const ViewParams &cam = viewsPtr->v[0];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n) return;
-  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return; // the whole block, before any copy
+  const uint32_t n = p.n, ps = p.planeStride, tid = threadIdx.x;
+  const uint32_t i0 = blockIdx.x * kStepThreads, i = i0 + tid;
+  const uint32_t planes = 3u * (uint32_t)p.shCoeffs, restPlanes = planes - 3u;
+  const bool stateF32 = state.store == StateStore::F32;
+  float *s_dc = reinterpret_cast<float *>(s_stage);
+  unsigned char *s_rest = s_stage + 3u * kStepThreads * 4u;
+  unsigned char *s_state = s_rest + restPlanes * kStepThreads * kShBytes;
+  if (tid == 0) bulk_barrier_init(&s_bar, 1);
+  __syncthreads();
+  if (tid < 32u) {
+    // Warp 0 issues the copies: DC planes, rest planes, state planes (F32: m then v).
+    if (tid == 0) bulk_expect(&s_bar, step_stage_bytes(p.shCoeffs, (int)kShBytes, stateF32));
+    __syncwarp();
+    const uint32_t copies = planes + (stateF32 ? 2u : 1u) * planes;
+    for (uint32_t c = tid; c < copies; c += 32u) {
+      if (c < 3u) {
+        bulk_load(s_dc + c * kStepThreads, p.shDc + (size_t)c * ps + i0, kStepThreads * 4u, &s_bar);
+      } else if (c < planes) {
+        const uint32_t r = c - 3u;
+        bulk_load(s_rest + r * kStepThreads * kShBytes,
+                  static_cast<const unsigned char *>(p.shRest) + ((size_t)r * ps + i0) * kShBytes, kStepThreads * kShBytes,
+                  &s_bar);
+      } else {
+        const uint32_t q = c - planes; // F32: planes m, then planes v (at planes * ps)
+        bulk_load(s_state + q * kStepThreads * 4u,
+                  static_cast<const unsigned char *>(state.state[4]) + ((size_t)q * ps + i0) * 4u, kStepThreads * 4u, &s_bar);
+      }
+    }
+  }
+  // From here on a block's threads leave only after waiting for the copies,
+  // or when they have no Gaussian (the issuing thread always has one).
+  if (i >= n) return;
   const ChainArgs args = *argsPtr;
-  const uint32_t n = p.n;
   const AdamArgs a = adam_args(args);
 
   const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
@@ -665,66 +721,70 @@ __global__ void __launch_bounds__(128, 4) k_chain_step(Params p, const ViewSet *
     chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
   }
 
-  // The SH step, with the direction term from the coefficients before it.
-  // Chunks of kStepChunk coefficients, double-buffered: the next chunk's
-  // loads are issued before this chunk's arithmetic.
+  // The SH step, from the staged planes, with the direction term from the
+  // coefficients before it.
+  if (!bulk_wait(&s_bar, 0, kStageSpinLimit)) {
+    // Never leave with a copy still landing in this block's shared memory.
+    atomicOr(error, kErrLookbackTimeout);
+    bulk_wait(&s_bar, 0, kStageSpinLimit);
+  }
   const bool stepZeros = !args.selective;
   const int active = touched ? cam.activeCoeffs : 0;
   float gDir[3] = {0.f, 0.f, 0.f};
   if (touched || stepZeros) {
     const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
-    const uint32_t count = n * shFloats;
-    float value[2][kStepChunk][3], m[2][kStepChunk][3], vv[2][kStepChunk][3];
-    uint32_t word[2][kStepChunk][3];
-    auto load_chunk = [&](int k0, int buf) {
+    const uint32_t count = ps * shFloats;
+    const float *s_statef = reinterpret_cast<const float *>(s_state);
+    const uint32_t *s_statew = reinterpret_cast<const uint32_t *>(s_state);
+    // The direction term first, unrolled (its basis gradients fold per
+    // coefficient), from the staged values; then the step, one coefficient
+    // per trip of a rolled loop: unrolled, the step's code overflows the
+    // instruction cache.
+    if (touched && cam.activeDegree > 0) {
 #pragma unroll
-      for (int kk = 0; kk < kStepChunk; ++kk) {
-        const int k = k0 + kk;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          value[buf][kk][c] = m[buf][kk][c] = vv[buf][kk][c] = 0.0f;
-          word[buf][kk][c] = 0u;
-          if (k >= p.shCoeffs) continue;
-          const uint32_t t = (uint32_t)(k * 3 + c) * n + i;
-          value[buf][kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3u * n);
-          load_state(state.state[4], state.store, count, t, m[buf][kk][c], vv[buf][kk][c], word[buf][kk][c]);
-        }
+      for (int k = 1; k < kMaxCoeffs; ++k) {
+        if (k >= active) break;
+        const uint32_t r = (uint32_t)(k - 1) * 3u;
+        const float value[3] = {staged_sh_rest<S>(s_rest, r * kStepThreads + tid),
+                                staged_sh_rest<S>(s_rest, (r + 1u) * kStepThreads + tid),
+                                staged_sh_rest<S>(s_rest, (r + 2u) * kStepThreads + tid)};
+        direction_term(k, value, gColour, dir, gDir);
       }
-    };
-    load_chunk(0, 0);
+    }
+#pragma unroll 1
+    for (int k = 0; k < p.shCoeffs; ++k) {
+      float value[3];
 #pragma unroll
-    for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStepChunk) {
-      const int buf = (k0 / kStepChunk) & 1;
-      if (k0 >= p.shCoeffs) break;
-      if (k0 + kStepChunk < kMaxCoeffs && k0 + kStepChunk < p.shCoeffs) load_chunk(k0 + kStepChunk, buf ^ 1);
-      if (touched && cam.activeDegree > 0) {
-#pragma unroll
-        for (int kk = 0; kk < kStepChunk; ++kk) {
-          const int k = k0 + kk;
-          if (k >= 1 && k < active) direction_term(k, value[buf][kk], gColour, dir, gDir);
-        }
+      for (int c = 0; c < 3; ++c) {
+        const uint32_t plane = (uint32_t)(k * 3 + c);
+        value[c] = k == 0 ? s_dc[c * kStepThreads + tid] : staged_sh_rest<S>(s_rest, (plane - 3u) * kStepThreads + tid);
       }
+      const float b = k < active ? basis_one(k, dir[0], dir[1], dir[2]) : 0.0f;
+      const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
 #pragma unroll
-      for (int kk = 0; kk < kStepChunk; ++kk) {
-        const int k = k0 + kk;
-        if (k >= p.shCoeffs) continue;
-        const float b = k < active ? basis_one(k, dir[0], dir[1], dir[2]) : 0.0f;
-        const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float g = k < active ? fmaf(b, gColour[c], 0.0f) : 0.0f;
-          if (g == 0.0f && !stepZeros) continue;
-          const uint32_t plane = (uint32_t)(k * 3 + c);
-          const uint32_t t = plane * n + i;
-          const uint32_t hashIndex = (i * shFloats + plane) * 5u + 4u;
-          float val = value[buf][kk][c], mm = m[buf][kk][c], v2 = vv[buf][kk][c];
-          adam(val, mm, v2, g, rate, a);
-          store_state(state.state[4], state.store, count, t, mm, v2, word[buf][kk][c], hashIndex, a.seed);
-          if (k == 0) {
-            p.shDc[t] = val;
-          } else {
-            store_sh_rest<S>(p.shRest, t - 3u * n, val, hashIndex, args.seed);
-          }
+      for (int c = 0; c < 3; ++c) {
+        const float g = k < active ? fmaf(b, gColour[c], 0.0f) : 0.0f;
+        if (g == 0.0f && !stepZeros) continue;
+        const uint32_t plane = (uint32_t)(k * 3 + c);
+        const uint32_t t = plane * ps + i;
+        const uint32_t hashIndex = (i * shFloats + plane) * 5u + 4u;
+        float m, v;
+        uint32_t word = 0u;
+        if (stateF32) {
+          m = s_statef[plane * kStepThreads + tid];
+          v = s_statef[(planes + plane) * kStepThreads + tid];
+        } else {
+          word = s_statew[plane * kStepThreads + tid];
+          m = bf16_load(word, 0);
+          v = bf16_load(word, 1);
+        }
+        float val = value[c];
+        adam(val, m, v, g, rate, a);
+        store_state(state.state[4], state.store, count, t, m, v, word, hashIndex, a.seed);
+        if (k == 0) {
+          p.shDc[t] = val;
+        } else {
+          store_sh_rest<S>(p.shRest, t - 3u * ps, val, hashIndex, args.seed);
         }
       }
     }
@@ -776,17 +836,22 @@ __global__ void __launch_bounds__(128, 4) k_chain_step(Params p, const ViewSet *
 template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                     const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
-                    const uint32_t *error, cudaStream_t stream) {
+                    uint32_t *error, cudaStream_t stream) {
   const GradientsOut g = *grads;
   const bool store = args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
   const bool multi = views.count > 1;
   // The fused form indexes the F32 SH state (two planes of n * 48 floats) in 32 bits.
-  if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.n * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
-    if (args.fixedPoint)
-      k_chain_step<S, true><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
-    else
-      k_chain_step<S, false><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+  if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.planeStride * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
+    const uint32_t smem = step_stage_bytes(p.shCoeffs, S == ShStore::F32 ? 4 : 2, state.store == StateStore::F32);
+    const uint32_t stepBlocks = div_up(p.n, kStepThreads);
+    if (args.fixedPoint) {
+      cudaFuncSetAttribute(k_chain_step<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_chain_step<S, true><<<stepBlocks, kStepThreads, smem, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+    } else {
+      cudaFuncSetAttribute(k_chain_step<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_chain_step<S, false><<<stepBlocks, kStepThreads, smem, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+    }
     return;
   }
 #define SB_CHAIN(F, M) \
@@ -810,7 +875,7 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
 
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
-                  const uint32_t *error, cudaStream_t stream) {
+                  uint32_t *error, cudaStream_t stream) {
   if (p.n == 0) return;
   switch (p.shStore) {
   case ShStore::BF16:

@@ -103,8 +103,8 @@ template <> __device__ __forceinline__ float load_sh_rest<ShStore::F16>(const vo
 
 // Coefficient k (0 = DC), channel c, of Gaussian i.
 template <ShStore S> __device__ __forceinline__ float sh_coefficient(const Params &p, uint32_t i, int k, int c) {
-  if (k == 0) return p.shDc[(size_t)c * p.n + i];
-  return load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * p.n + i);
+  if (k == 0) return p.shDc[(size_t)c * p.planeStride + i];
+  return load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * p.planeStride + i);
 }
 
 } // namespace sb

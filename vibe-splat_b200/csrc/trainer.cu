@@ -136,6 +136,7 @@ public:
   splat_trainer_options opt;
   uint32_t n = 0;
   int shDegree = 0, shCoeffs = 1, activeDegree = 0;
+  uint32_t planeStride = 0; // elements between SH planes: n rounded up to kPlaneAlign
   ShStore shStore = ShStore::F16;
   StateStore stateStore = StateStore::BF16Pair;
   bool fixedPoint = false, oneSort = false, exactMath = true, useGraph = false;
@@ -243,13 +244,17 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
 
   const size_t nn = n;
+  planeStride = (uint32_t)(((nn + kPlaneAlign - 1) / kPlaneAlign) * kPlaneAlign);
+  const size_t ps = planeStride;
   positions.ensure(nn * 12);
   scales.ensure(nn * 12);
   rotations.ensure(nn * 16);
   opacities.ensure(nn * 4);
-  shDc.ensure(nn * 12);
-  const size_t rest = nn * 3 * (shCoeffs - 1);
+  shDc.ensure(ps * 12);
+  const size_t rest = ps * 3 * (shCoeffs - 1);
   shRest.ensure(std::max<size_t>(rest * (shStore == ShStore::F32 ? 4 : 2), 4));
+  SB_CUDA(cudaMemset(shDc.get(), 0, shDc.bytes()));
+  SB_CUDA(cudaMemset(shRest.get(), 0, shRest.bytes()));
   SB_CUDA(cudaMemcpy(positions.get(), cloud.positions, nn * 12, cudaMemcpyHostToDevice));
   SB_CUDA(cudaMemcpy(scales.get(), cloud.scales, nn * 12, cudaMemcpyHostToDevice));
   SB_CUDA(cudaMemcpy(rotations.get(), cloud.rotations, nn * 16, cudaMemcpyHostToDevice));
@@ -257,14 +262,14 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   // SH to planes: DC as FP32, the rest in the chosen storage, rounded to nearest.
   {
     const int floats = 3 * shCoeffs;
-    std::vector<float> dc(nn * 3);
+    std::vector<float> dc(ps * 3, 0.0f);
     for (size_t i = 0; i < nn; ++i)
-      for (int c = 0; c < 3; ++c) dc[c * nn + i] = cloud.sh[i * floats + c];
-    SB_CUDA(cudaMemcpy(shDc.get(), dc.data(), nn * 12, cudaMemcpyHostToDevice));
+      for (int c = 0; c < 3; ++c) dc[c * ps + i] = cloud.sh[i * floats + c];
+    SB_CUDA(cudaMemcpy(shDc.get(), dc.data(), ps * 12, cudaMemcpyHostToDevice));
     if (rest > 0) {
-      std::vector<float> planes(rest);
+      std::vector<float> planes(rest, 0.0f);
       for (size_t i = 0; i < nn; ++i)
-        for (int j = 3; j < floats; ++j) planes[(size_t)(j - 3) * nn + i] = cloud.sh[i * floats + j];
+        for (int j = 3; j < floats; ++j) planes[(size_t)(j - 3) * ps + i] = cloud.sh[i * floats + j];
       if (shStore == ShStore::F32) {
         SB_CUDA(cudaMemcpy(shRest.get(), planes.data(), rest * 4, cudaMemcpyHostToDevice));
       } else {
@@ -282,7 +287,7 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
       }
     }
   }
-  const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, nn * 3 * shCoeffs};
+  const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, ps * 3 * shCoeffs};
   for (int g = 0; g < 5; ++g) {
     const size_t bytes = groupCounts[g] * (stateStore == StateStore::F32 ? 8 : 4);
     state[g].ensure(bytes);
@@ -325,6 +330,7 @@ Params Trainer::params() const {
   p.shRest = shRest.get();
   p.shStore = shStore;
   p.n = n;
+  p.planeStride = planeStride;
   p.shDegree = shDegree;
   p.shCoeffs = shCoeffs;
   return p;
@@ -1109,11 +1115,12 @@ int splat_trainer_get_cloud(splat_trainer *trainer, float *positions, float *sca
     if (opacities) SB_CUDA(cudaMemcpy(opacities, t->opacities.get(), n * 4, cudaMemcpyDeviceToHost));
     if (sh) {
       const int floats = 3 * t->shCoeffs;
-      std::vector<float> dc(n * 3);
-      SB_CUDA(cudaMemcpy(dc.data(), t->shDc.get(), n * 12, cudaMemcpyDeviceToHost));
+      const size_t ps = t->planeStride;
+      std::vector<float> dc(ps * 3);
+      SB_CUDA(cudaMemcpy(dc.data(), t->shDc.get(), ps * 12, cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < n; ++i)
-        for (int c = 0; c < 3; ++c) sh[i * floats + c] = dc[c * n + i];
-      const size_t rest = n * 3 * (t->shCoeffs - 1);
+        for (int c = 0; c < 3; ++c) sh[i * floats + c] = dc[c * ps + i];
+      const size_t rest = ps * 3 * (t->shCoeffs - 1);
       if (rest > 0) {
         std::vector<float> planes(rest);
         if (t->shStore == sb::ShStore::F32) {
@@ -1131,7 +1138,7 @@ int splat_trainer_get_cloud(splat_trainer *trainer, float *positions, float *sca
           }
         }
         for (size_t i = 0; i < n; ++i)
-          for (int j = 3; j < floats; ++j) sh[i * floats + j] = planes[(size_t)(j - 3) * n + i];
+          for (int j = 3; j < floats; ++j) sh[i * floats + j] = planes[(size_t)(j - 3) * ps + i];
       }
     }
   });
@@ -1188,8 +1195,11 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
     const size_t wordBytes = t->stateStore == sb::StateStore::F32 ? 8 : 4;
     std::vector<std::vector<uint8_t>> moved(5);
     const size_t strides[5] = {3, 3, 4, 1, (size_t)floats};
+    // SH state planes are planeStride (n rounded up to kPlaneAlign) apart.
+    const size_t oldPlanes = t->planeStride;
+    const size_t newPlanes = ((newN + sb::kPlaneAlign - 1) / sb::kPlaneAlign) * sb::kPlaneAlign;
     for (int g = 0; g < 5; ++g) {
-      const size_t oldCount = oldN * strides[g], newCount = newN * strides[g];
+      const size_t oldCount = (g == 4 ? oldPlanes : oldN) * strides[g], newCount = (g == 4 ? newPlanes : newN) * strides[g];
       std::vector<uint8_t> old(oldCount * wordBytes);
       SB_CUDA(cudaMemcpy(old.data(), t->state[g].get(), old.size(), cudaMemcpyDeviceToHost));
       moved[g].assign(newCount * wordBytes, 0);
@@ -1198,8 +1208,8 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
         if (s < 0 || (size_t)s >= oldN) continue;
         for (size_t a = 0; a < strides[g]; ++a) {
           // State index of element a of Gaussian i: AoS for groups 0-3, planes for SH.
-          const size_t from = g == 4 ? a * oldN + (size_t)s : (size_t)s * strides[g] + a;
-          const size_t to = g == 4 ? a * newN + i : i * strides[g] + a;
+          const size_t from = g == 4 ? a * oldPlanes + (size_t)s : (size_t)s * strides[g] + a;
+          const size_t to = g == 4 ? a * newPlanes + i : i * strides[g] + a;
           if (wordBytes == 8) {
             std::memcpy(&moved[g][to * 4], &old[from * 4], 4);
             std::memcpy(&moved[g][(newCount + to) * 4], &old[(oldCount + from) * 4], 4);
