@@ -631,7 +631,7 @@ template <ShStore S> __device__ __forceinline__ float staged_sh_rest(const unsig
 }
 
 template <ShStore S, bool FIXED>
-__global__ void __launch_bounds__(kStepThreads, 4) k_chain_step(Params p, const ViewSet *__restrict__ viewsPtr,
+__global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const ViewSet *__restrict__ viewsPtr,
                                                                 const void *__restrict__ rawIn, const Splat *__restrict__ splats,
                                                                 const ChainArgs *__restrict__ argsPtr, OptimState state,
                                                                 float *__restrict__ densifyStats, uint32_t *error) {
