@@ -48,6 +48,9 @@ WIDTH, HEIGHT = 1237, 822
 GAUSSIANS = 1_000_000
 DEGREE = 3
 VIEWS = 64
+METRIC = "train iters/s @1M Gaussians 1237x822"
+WORKLOAD = ("1M Gaussians, SH degree 3, 1237x822, 64 cameras on a radius-5 hemisphere, 60 deg horizontal fov "
+            "(synthetic shapes of the bicycle scene)")
 SEED = 3
 SH_C0 = 0.28209479177387814
 
@@ -226,10 +229,11 @@ def reference_arm(args) -> None:
               f"{threads} row bands run on {threads} threads; reference_render + reference_loss + "
               "reference_gradients (which renders again) per band")
     print(json.dumps({
-        "impl": "reference", "metric": "train iters/s @1M Gaussians 1237x822", "value": value, "unit": "iters/s",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "iters/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / done,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "1M Gaussians, SH degree 3, 1237x822, 64 hemisphere views (synthetic bicycle shapes)"},
+        "config": {"workload": WORKLOAD, "form": "the reference's FP64 CPU twin (src/train/reference.cpp): render, "
+                                                "loss and gradients per view, no optimiser step"},
         "cpu_baseline": {"value": value, "unit": "iters/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -302,6 +306,38 @@ def time_steps(torch, trainer, step_fn, steps: int, stream_handle: int) -> float
     end.record(stream)
     torch.cuda.synchronize()
     return start.elapsed_time(end)
+
+
+def psnr(image: np.ndarray, reference: np.ndarray) -> float:
+    mse = float(np.mean((np.asarray(image, np.float64) - np.asarray(reference, np.float64)) ** 2))
+    return 10.0 * math.log10(1.0 / max(mse, 1e-30))
+
+
+def precision_check(splat, torch, cloud, cams, host_targets, rates, chosen, tuned, steps: int = 20) -> dict:
+    """The chosen form against the plain FP32 form from the same cloud: PSNR of
+    one's render against the other's, then, after `steps` identical training
+    steps (views in turn), each render's PSNR against the target and the
+    difference."""
+    tuned_opts = chosen
+    if tuned:
+        tuned_opts.sort_form = tuned.get("sort_form", chosen.sort_form)
+        tuned_opts.digit_bits = tuned.get("digit_bits", chosen.digit_bits)
+        tuned_opts.forward_pixels_per_thread = tuned.get("forward_pixels_per_thread", chosen.forward_pixels_per_thread)
+        tuned_opts.backward_pixels_per_thread = tuned.get("backward_pixels_per_thread", chosen.backward_pixels_per_thread)
+    forms = {"chosen": tuned_opts, "plain": plain_options(splat)}
+    renders, after = {}, {}
+    target0 = host_targets[0].reshape(-1, 4)[:, :3].astype(np.float64) / 255.0
+    for name, opts in forms.items():
+        trainer = splat.Trainer(cloud, opts)
+        renders[name] = trainer.render(cams[0]).reshape(-1, 4)[:, :3]
+        for i in range(steps):
+            trainer.step(cams[i % len(cams)], host_targets[i % len(cams)], rates)
+        after[name] = psnr(trainer.render(cams[0]).reshape(-1, 4)[:, :3], target0)
+        del trainer
+        torch.cuda.empty_cache()
+    return {"render_psnr_chosen_vs_plain_db": psnr(renders["chosen"], renders["plain"]),
+            "steps": steps, "psnr_vs_target_db": after,
+            "psnr_difference_db": abs(after["chosen"] - after["plain"])}
 
 
 def our_arm(args) -> None:
@@ -417,6 +453,10 @@ def our_arm(args) -> None:
                  "form": "FP32 SH and Adam state, depth-then-tile sort, host read-back, no graph, exact exp/log"}
         del p_trainer
 
+    precision = None
+    if not args.no_plain:
+        precision = precision_check(splat, torch, cloud, cams, host_targets, rates, chosen, tuned)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -443,16 +483,19 @@ def our_arm(args) -> None:
     launches_per_step = 10 + depth_launches + entry_launches
     form_name = "depth then tile sort" if form == 0 else "64-bit tile|depth keys"
     out = {
-        "metric": "train iters/s @1M Gaussians 1237x822 (fwd+bwd+Adam per view)",
+        "metric": METRIC,
         "value": value, "unit": "iters/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "fwd_bwd_ms": sum(stages.get(k, 0.0) for k in ("composite", "loss", "backward")),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; the bicycle photos are not available)",
-        "config": {"workload": "1M Gaussians, SH degree 3 (BF16 above DC), 1237x822, 64 cameras on a radius-5 hemisphere, "
-                               "60 deg horizontal fov",
-                   "form": f"chosen: BF16 SH + BF16-pair Adam state, {form_name} with {digits}-bit digits "
-                           f"({'autotuned' if tuned else 'fixed'}), CUDA graph, SFU exp/log",
-                   "autotune_ms": tuned.get("ms"), "parallelism": f"replicas x{world}",
+        "config": {"workload": WORKLOAD,
+                   "form": f"chosen: BF16 SH + BF16-pair Adam state, {form_name} with {digits}-bit digits, "
+                           f"{tuned.get('forward_pixels_per_thread', chosen.forward_pixels_per_thread)}-pixel compositing, "
+                           f"{tuned.get('backward_pixels_per_thread', chosen.backward_pixels_per_thread)}-pixel float "
+                           f"backward ({'autotuned' if tuned else 'fixed'}), fused one-view chain rule + Adam + SH "
+                           "step, CUDA graph, SFU exp/log",
+                   "autotune_ms": tuned.get("ms"), "layout_ms": tuned.get("layout_ms"),
+                   "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (1M-Gaussian parameters and state, 64 x 4 MB targets)",
                    "tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -460,6 +503,7 @@ def our_arm(args) -> None:
         "stage_roofline": stage_roof,
         "stages_ms": stages,
         "plain_fp32": plain,
+        "precision": precision,
         "speedup_vs_plain": (value / world) / plain["iters_per_s"] if plain else None,
         "cpu_baseline": cpu,
         "clocks": clocks,

@@ -373,3 +373,40 @@ def test_pixel_layouts_agree(splat, oracle, exact):
     assert abs(out[0][1].loss - out[1][1].loss) < 1e-6
     for name in ("positions", "scales", "rotations", "opacities", "sh"):
         check_close(getattr(out[0][2], name), getattr(out[1][2], name), name, 0.99999, 1e-4)
+
+
+def _relative_error(a, b) -> float:
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("layout", [1, 2])
+def test_chosen_form_against_fp64(splat, oracle, layout):
+    # The precision form (BF16 SH above DC, SFU exp/log, float sums) against the
+    # FP64 twin given the same BF16-rounded coefficients: rendered image PSNR
+    # and the relative error of every gradient group (norm of the difference
+    # over the norm of the FP64 gradient).
+    w, h = 160, 120
+    view = oracle.train_camera(w, h)
+    target = oracle.smooth_target(w, h, 29)
+    cloud = oracle.random_cloud(3000, 3, 31)
+    cloud.sh = oracle.round_sh_like_device(cloud.sh, 3, "bf16")
+    rgb, _, _ = oracle.ref_render(cloud, view)
+    _, _, _, adjoint = oracle.ref_loss(rgb, w, h, target, 0.2)
+    cpu = oracle.ref_gradients(cloud, view, adjoint)
+    opts = splat.TrainerOptions(sh_storage=splat.SH_BF16, exact_math=False, use_graph=True,
+                                forward_pixels_per_thread=layout, backward_pixels_per_thread=layout)
+    trainer = splat.Trainer(to_cloud(cloud), opts)
+    image = trainer.render(to_camera(view)).reshape(-1, 4)[:, :3].astype(np.float64)
+    mse = float(np.mean((image - rgb.reshape(-1, 3)) ** 2))
+    psnr = 10.0 * np.log10(1.0 / max(mse, 1e-30))
+    trainer.compute_gradients(to_camera(view), target)
+    g = trainer.gradients()
+    errors = {name: _relative_error(getattr(g, name), getattr(cpu, name))
+              for name in ("positions", "scales", "rotations", "opacities", "sh")}
+    print(f"  layout {layout}: render PSNR vs FP64 {psnr:.1f} dB; gradient relative errors "
+          + ", ".join(f"{k} {v:.2e}" for k, v in errors.items()))
+    assert psnr > 60.0
+    for name, err in errors.items():
+        assert err < 1e-3, f"{name}: relative error {err}"
