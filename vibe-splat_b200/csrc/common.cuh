@@ -71,13 +71,27 @@ struct __align__(16) Splat {
 // Fast: the SFU approximations (ex2.approx / lg2.approx), for the forms that
 // trade bit-reproducibility on the CPU for speed; the GPU results are still
 // deterministic run to run.
+// The rasterizer's exp/log and the base of its log transmittance. The exact
+// form works in natural logs with the deterministic exp/log; the SFU form in
+// base 2, so that ex2/lg2 need no change of base: the staged conic is scaled
+// by kLogScale = log2(e) instead, and log T (image.w) is in bits.
 struct ExactMath {
+  static constexpr float kLogScale = 1.0f;
   static __device__ __forceinline__ float exp(float x) { return splat_expf(x); }
   static __device__ __forceinline__ float log(float x) { return splat_logf(x); }
 };
 struct FastMath {
-  static __device__ __forceinline__ float exp(float x) { return __expf(x); }
-  static __device__ __forceinline__ float log(float x) { return __logf(x); }
+  static constexpr float kLogScale = 1.4426950408889634f;
+  static __device__ __forceinline__ float exp(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  }
+  static __device__ __forceinline__ float log(float x) {
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  }
 };
 
 __host__ __device__ __forceinline__ uint32_t div_up(uint32_t a, uint32_t b) { return (a + b - 1) / b; }

@@ -72,13 +72,15 @@ __device__ __forceinline__ uint32_t pixel_masks(const Splat &s, uint32_t x0, uin
   return mask;
 }
 
+template <class M>
 __device__ __forceinline__ Staged stage(const Splat &s, uint32_t index, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
   Staged out;
   out.cx = s.centerExtent.x;
   out.cy = s.centerExtent.y;
-  out.hqx = -0.5f * s.conicOpacity.x;
-  out.nqy = -s.conicOpacity.y;
-  out.hqz = -0.5f * s.conicOpacity.z;
+  // The exponent's coefficients in the form's log base (a factor of 1 for the exact form).
+  out.hqx = (-0.5f * s.conicOpacity.x) * M::kLogScale;
+  out.nqy = (-s.conicOpacity.y) * M::kLogScale;
+  out.hqz = (-0.5f * s.conicOpacity.z) * M::kLogScale;
   out.opacity = s.conicOpacity.w;
   out.r = s.colorRadius.x;
   out.g = s.colorRadius.y;
@@ -119,6 +121,7 @@ __device__ __forceinline__ TileGeometry tile_geometry(const ViewSet &views, int 
 
 // An index outside the splat array can only come from a broken earlier stage:
 // record it and stage a splat that covers no pixel.
+template <class M>
 __device__ __forceinline__ Staged stage_checked(const Splat *__restrict__ splats, uint32_t s, uint32_t splatLimit,
                                                 const TileGeometry &geo, uint32_t *error) {
   if (s >= splatLimit) {
@@ -128,7 +131,7 @@ __device__ __forceinline__ Staged stage_checked(const Splat *__restrict__ splats
     empty.index = 0u;
     return empty;
   }
-  return stage(splats[s], s, geo.x0, geo.y0, geo.x1, geo.y1);
+  return stage<M>(splats[s], s, geo.x0, geo.y0, geo.x1, geo.y1);
 }
 
 // Per-warp lists of the staged splats, as bitmaps: word w of warp v has bit b
@@ -184,7 +187,7 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
     if (__syncthreads_count(done) == kTilePixels) break;
     uint32_t stagedMask = 0u;
     if (t < count) {
-      const Staged st = stage_checked(splats, entryValues[end + t], splatLimit, geo, error);
+      const Staged st = stage_checked<M>(splats, entryValues[end + t], splatLimit, geo, error);
       s_batch[t] = st;
       stagedMask = st.mask;
     }
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
         if (!(alpha >= kAlphaMin)) continue;
         const float oneMinus = 1.0f - alpha;
         const float logRest = M::log(oneMinus);
-        if (logT + logRest < kLogMinTransmittance) {
+        if (logT + logRest < kLogMinTransmittance * M::kLogScale) {
           stop = end + k + 1u;
           done = true;
           break;
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(kTilePixels, 4)
     __syncthreads();
     uint32_t stagedMask = 0u;
     if (t < count) {
-      const Staged st = stage_checked(splats, entryValues[start + t], splatLimit, geo, error);
+      const Staged st = stage_checked<M>(splats, entryValues[start + t], splatLimit, geo, error);
       s_batch[t] = st;
       stagedMask = st.mask;
     }
@@ -424,6 +427,7 @@ __device__ __forceinline__ PixelPair pixel_pair(const TileGeometry &geo, const V
 
 // Stages `count` splats with 128 threads, two rounds, and publishes the
 // 8x8-block bitmaps.
+template <class M>
 __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, const uint32_t *__restrict__ values, uint32_t count,
                                             uint32_t splatLimit, const TileGeometry &geo, uint32_t *error, Staged *batch,
                                             uint32_t (*cover)[kBatch / 32]) {
@@ -433,7 +437,7 @@ __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, co
     const uint32_t j = round * kHalfTile + t;
     uint32_t mask = 0u;
     if (j < count) {
-      const Staged st = stage_checked(splats, values[j], splatLimit, geo, error);
+      const Staged st = stage_checked<M>(splats, values[j], splatLimit, geo, error);
       batch[j] = st;
       mask = st.mask;
     }
@@ -463,7 +467,7 @@ __global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict_
     const uint32_t count = min((uint32_t)kBatch, end - range.x);
     end -= count;
     if (__syncthreads_count(done[0] && done[1]) == kHalfTile) break;
-    stage_pairs(splats, entryValues + end, count, splatLimit, geo, error, s_batch, s_cover);
+    stage_pairs<M>(splats, entryValues + end, count, splatLimit, geo, error, s_batch, s_cover);
     __syncthreads();
     for (int word = (int)((count - 1u) >> 5); word >= 0 && !(done[0] && done[1]); --word) {
     for (uint32_t bits = s_cover[warp][word]; bits != 0u;) {
@@ -482,7 +486,7 @@ __global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict_
         if (!(alpha >= kAlphaMin)) continue;
         const float oneMinus = 1.0f - alpha;
         const float logRest = M::log(oneMinus);
-        if (logT[q] + logRest < kLogMinTransmittance) {
+        if (logT[q] + logRest < kLogMinTransmittance * M::kLogScale) {
           stop[q] = end + (uint32_t)k + 1u;
           done[q] = true;
           continue;
@@ -526,12 +530,14 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const PixelPair pp = pixel_pair(geo, cam, t);
   const uint2 range = ranges[tile];
-  float logTotal[2], Ax[2], Ay[2], Az[2], Br[2], Bg[2], Bb[2], logBehind[2];
+  // front: log T total minus the log transmittance of the splats already
+  // walked (those behind), kept as one running value.
+  float front[2], Ax[2], Ay[2], Az[2], Br[2], Bg[2], Bb[2];
   uint32_t stop[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const size_t at = pp.inside[q] ? (size_t)cam.pixelBase + (size_t)pp.y[q] * cam.width + pp.x[q] : 0;
-    logTotal[q] = pp.inside[q] ? image[at].w : 0.0f;
+    front[q] = pp.inside[q] ? image[at].w : 0.0f;
     const float4 a = pp.inside[q] ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
     Ax[q] = a.x;
     Ay[q] = a.y;
@@ -540,7 +546,6 @@ __global__ void __launch_bounds__(kHalfTile, 6)
     Br[q] = bgR;
     Bg[q] = bgG;
     Bb[q] = bgB;
-    logBehind[q] = 0.0f;
   }
   const float perPixel = cam.perPixel;
   const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
@@ -555,7 +560,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   for (uint32_t start = tileStop; start < range.y; start += kBatch) {
     const uint32_t count = min((uint32_t)kBatch, range.y - start);
     __syncthreads();
-    stage_pairs(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover);
+    stage_pairs<M>(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover);
     __syncthreads();
     for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
     for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
@@ -582,9 +587,9 @@ __global__ void __launch_bounds__(kHalfTile, 6)
       for (int q = 0; q < 2; ++q) {
         const float aAct = act[q] ? alpha[q] : 0.0f;
         const float logRest = M::log(1.0f - aAct);
-        const float T = M::exp((logTotal[q] - logBehind[q]) - logRest);
+        const float T = M::exp(front[q] - logRest);
         // Float sums only, so fused multiply-adds throughout.
-        const float wA = act[q] ? T * alpha[q] : 0.0f;
+        const float wA = T * aAct;
         g[6] = fmaf(wA, Ax[q], g[6]);
         g[7] = fmaf(wA, Ay[q], g[7]);
         g[8] = fmaf(wA, Az[q], g[8]);
@@ -607,7 +612,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         Br[q] = fmaf(aAct, s.r - Br[q], Br[q]);
         Bg[q] = fmaf(aAct, s.g - Bg[q], Bg[q]);
         Bb[q] = fmaf(aAct, s.b - Bb[q], Bb[q]);
-        logBehind[q] = logBehind[q] + logRest;
+        front[q] = front[q] - logRest;
       }
       const float total = butterfly12(g);
       if (lane < 16 && held < (uint32_t)kGradValues && total != 0.0f) atomicAdd(&s_acc[k * kAccStride + held], total);

@@ -892,6 +892,9 @@ void Trainer::render(const splat_camera *camera, float *out) {
   if (hReadback.get<StepReadback>()->error != 0u) throw Failure{SPLAT_ERR_DEVICE, "device check failed during render"};
   const size_t pixels = (size_t)camera->width * camera->height;
   SB_CUDA(cudaMemcpy(out, image.get(), pixels * 16, cudaMemcpyDeviceToHost));
+  // The SFU form keeps log T in base 2 on the device; the caller gets natural logs.
+  if (!exactMath)
+    for (size_t p = 0; p < pixels; ++p) out[p * 4 + 3] *= 0.6931471805599453f;
 }
 
 // ---------------------------------------------------------------- small kernels
