@@ -4,6 +4,8 @@
 // the tile tests of shaders/train_types.glsl:34-77 (splat_tiles,
 // splat_reaches_tile). The reach 2 log(255 opacity) comes from the preprocess
 // pass, so the test here is exact IEEE arithmetic only.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace sb {
@@ -415,20 +417,37 @@ __global__ void __launch_bounds__(256)
   if (overflow) atomicOr(error, kErrEntryOverflow);
 }
 
+// Tile ranges over the sorted keys: a grid of a few blocks per SM walks the
+// entries (the count lives on the device, so a grid sized by the capacity
+// would be mostly blocks with nothing to do), each thread four consecutive
+// entries and their right neighbour.
+constexpr uint32_t kRangesPerThread = 4;
+
 __global__ void __launch_bounds__(256) k_tile_ranges(const uint32_t *__restrict__ keys32, const unsigned long long *__restrict__ keys64,
                                                      const uint32_t *deviceCount, uint32_t tileLimit, uint2 *__restrict__ ranges,
                                                      uint32_t *error) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t count = *deviceCount;
-  if (k >= count) return;
   auto tile_of = [&](uint32_t i) { return keys64 != nullptr ? (uint32_t)(keys64[i] >> 32) : keys32[i]; };
-  const uint32_t tile = tile_of(k);
-  if (tile >= tileLimit) {
-    atomicOr(error, kErrBadIndex);
-    return;
+  const uint32_t stride = gridDim.x * blockDim.x * kRangesPerThread;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * kRangesPerThread; base < count; base += stride) {
+    uint32_t tiles[kRangesPerThread + 1];
+#pragma unroll
+    for (uint32_t j = 0; j <= kRangesPerThread; ++j) tiles[j] = base + j < count ? tile_of(base + j) : 0xFFFFFFFFu;
+    const uint32_t before = base > 0 ? tile_of(base - 1) : 0xFFFFFFFFu;
+#pragma unroll
+    for (uint32_t j = 0; j < kRangesPerThread; ++j) {
+      const uint32_t k = base + j;
+      if (k >= count) break;
+      const uint32_t tile = tiles[j];
+      if (tile >= tileLimit) {
+        atomicOr(error, kErrBadIndex);
+        continue;
+      }
+      const uint32_t prev = j == 0 ? before : tiles[j - 1];
+      if (k == 0 || prev != tile) ranges[tile].x = k;
+      if (k + 1 == count || tiles[j + 1] != tile) ranges[tile].y = k + 1;
+    }
   }
-  if (k == 0 || tile_of(k - 1) != tile) ranges[tile].x = k;
-  if (k + 1 == count || tile_of(k + 1) != tile) ranges[tile].y = k + 1;
 }
 
 } // namespace
@@ -461,7 +480,8 @@ void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *it
 void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *tileKeys64, const uint32_t *deviceCount,
                         uint32_t capacity, uint32_t tileLimit, uint2 *ranges, uint32_t *error, cudaStream_t stream) {
   if (capacity == 0) return;
-  k_tile_ranges<<<div_up(capacity, 256), 256, 0, stream>>>(tileKeys32, tileKeys64, deviceCount, tileLimit, ranges, error);
+  const uint32_t blocks = std::min<uint32_t>(div_up(div_up(capacity, kRangesPerThread), 256), 148u * 8u);
+  k_tile_ranges<<<blocks, 256, 0, stream>>>(tileKeys32, tileKeys64, deviceCount, tileLimit, ranges, error);
 }
 
 } // namespace sb

@@ -122,6 +122,15 @@ constexpr int kStages = 8;
 const char *const kStageNames[kStages] = {"project", "depth sort", "count tiles", "tile lists",
                                           "composite", "loss", "backward", "chain rule and step"};
 
+// The entry sort's digit width: no more passes than digitBits would take, the
+// key's bits spread evenly over them (12-bit tile ids: two 6-bit passes
+// rather than 8 + 4; fewer buckets per pass write longer runs).
+int entry_digits(int bits, int digitBits) {
+  const int passes = (bits + digitBits - 1) / digitBits;
+  const int even = (bits + passes - 1) / passes;
+  return even < 6 ? 6 : (even > 8 ? 8 : even);
+}
+
 uint32_t bits_for(uint32_t values) {
   uint32_t b = 0;
   while (b < 32 && (1ull << b) < values) ++b;
@@ -480,7 +489,9 @@ void Trainer::ensure_entries(uint32_t total) {
   tmpEntryKeys.ensure(cap * keyBytes);
   tmpEntryValues.ensure(cap * 4);
   const uint32_t bits = oneSort ? 32 + bits_for((uint32_t)views.totalTiles) : bits_for((uint32_t)views.totalTiles);
-  sortScratchEntries.ensure(sort_scratch_bytes(cap, (int)keyBytes, std::max<uint32_t>(bits, 32 + 24), digitBits));
+  size_t scratch = 0;
+  for (int d = 6; d <= 8; ++d) scratch = std::max(scratch, sort_scratch_bytes(cap, (int)keyBytes, std::max<uint32_t>(bits, 32 + 24), d));
+  sortScratchEntries.ensure(scratch);
   entryCapacity = (uint32_t)cap;
   clear_graphs();
 }
@@ -559,12 +570,13 @@ void Trainer::record_forward() {
     const int bits = 32 + (int)bits_for((uint32_t)views.totalTiles);
     entriesInTmp = sort_pairs_u64(entryKeys.get<unsigned long long>(), entryValues.get<uint32_t>(),
                                   tmpEntryKeys.get<unsigned long long>(), tmpEntryValues.get<uint32_t>(), entryCapacity, 0,
-                                  &counters[2], 0, bits, digitBits, sortScratchEntries.get(), error, stream) == 1;
+                                  &counters[2], 0, bits, entry_digits(bits, digitBits), sortScratchEntries.get(), error,
+                                  stream) == 1;
   } else {
     const int bits = (int)bits_for((uint32_t)views.totalTiles);
     entriesInTmp = sort_pairs_u32(entryKeys.get<uint32_t>(), entryValues.get<uint32_t>(), tmpEntryKeys.get<uint32_t>(),
-                                  tmpEntryValues.get<uint32_t>(), entryCapacity, 0, &counters[2], 0, bits, digitBits,
-                                  sortScratchEntries.get(), error, stream) == 1;
+                                  tmpEntryValues.get<uint32_t>(), entryCapacity, 0, &counters[2], 0, bits,
+                                  entry_digits(bits, digitBits), sortScratchEntries.get(), error, stream) == 1;
   }
   SB_CUDA(cudaMemsetAsync(ranges.get(), 0, (size_t)views.totalTiles * 8, stream));
   const void *keys = entriesInTmp ? tmpEntryKeys.get() : entryKeys.get();
