@@ -92,18 +92,6 @@ constexpr uint32_t kTableMax = 64;
 
 __device__ __forceinline__ uint32_t rect_area(const TileRect &t) { return (t.x1 - t.x0 + 1u) * (t.y1 - t.y0 + 1u); }
 
-// The reached tiles of a rectangle of at most 32 tiles, bit (y - y0) * width
-// + (x - x0) for tile (x, y): row-major, the reference's emission order.
-__device__ __forceinline__ uint32_t reach_mask(const float4 q, const float4 ce, float reach, const TileRect &t) {
-  uint32_t mask = 0, bit = 1;
-  for (uint32_t y = t.y0; y <= t.y1; ++y) {
-    const RowTangents row = row_tangents(q, ce, y);
-    for (uint32_t x = t.x0; x <= t.x1; ++x, bit <<= 1)
-      if (reaches_tile(q, reach, col_tangents(q, ce, x), row)) mask |= bit;
-  }
-  return mask;
-}
-
 // A large rectangle's tangent tables, filled by the whole warp. False (and
 // nothing filled) when the rectangle is wider or taller than the tables.
 __device__ __forceinline__ bool fill_tables(const float4 q, const float4 ce, const TileRect &t, uint32_t lane, ColTangents *cols,
@@ -160,6 +148,7 @@ __global__ void __launch_bounds__(kScanThreads)
   __shared__ unsigned long long s_exclusive;
   __shared__ ColTangents s_cols[kScanThreads / 32][kTableMax];
   __shared__ RowTangents s_rows[kScanThreads / 32][kTableMax];
+  __shared__ uint32_t s_mask[kScanThreads / 32][32];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   if (t == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
@@ -194,17 +183,57 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     uint32_t c = 0;
-    bool big = false;
     mask[j] = 0u;
+    TileRect rect{0u, 0u, 0u, 0u};
+    uint32_t area = 0;
     if (valid[j]) {
       const ViewParams &cam = views.v[item_view(sIdx[j], n, views.count)];
-      const TileRect rect = splat_tiles(ce[j], cam.gridW, cam.gridH);
-      big = rect_area(rect) > kWarpTiles;
-      if (!big) {
-        mask[j] = reach_mask(cq[j], ce[j], rc[j], rect);
+      rect = splat_tiles(ce[j], cam.gridW, cam.gridH);
+      area = rect_area(rect);
+      ++visible;
+    }
+    const bool big = area > kWarpTiles;
+    // Small rectangles: the warp's (splat, tile) pairs laid out flat, 32 tests
+    // per trip with every lane busy; each splat's mask (bit = row-major index
+    // in its rectangle) is assembled in shared memory.
+    {
+      const uint32_t own = big ? 0u : area;
+      uint32_t incl = own;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += x;
+      }
+      const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31), excl = incl - own;
+      const uint32_t width = rect.x1 - rect.x0 + 1u;
+      const float invWidth = 1.0f / (float)width;
+      s_mask[warp][lane] = 0u;
+      __syncwarp();
+      for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t f = base + lane;
+        uint32_t owner = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1)
+          if (__shfl_sync(0xFFFFFFFFu, incl, owner + step - 1u) <= f) owner += step;
+        const uint32_t li = f - __shfl_sync(0xFFFFFFFFu, excl, owner);
+        const float4 oce = make_float4(__shfl_sync(0xFFFFFFFFu, ce[j].x, owner), __shfl_sync(0xFFFFFFFFu, ce[j].y, owner), 0.f, 0.f);
+        const float4 oq = make_float4(__shfl_sync(0xFFFFFFFFu, cq[j].x, owner), __shfl_sync(0xFFFFFFFFu, cq[j].y, owner),
+                                      __shfl_sync(0xFFFFFFFFu, cq[j].z, owner), 0.f);
+        const float orc = __shfl_sync(0xFFFFFFFFu, rc[j], owner);
+        const uint32_t ox0 = __shfl_sync(0xFFFFFFFFu, rect.x0, owner), oy0 = __shfl_sync(0xFFFFFFFFu, rect.y0, owner);
+        const uint32_t ow = __shfl_sync(0xFFFFFFFFu, width, owner);
+        const float oinv = __shfl_sync(0xFFFFFFFFu, invWidth, owner);
+        if (f < total) {
+          const uint32_t r = (uint32_t)(((float)li + 0.5f) * oinv), col = li - r * ow;
+          if (reaches_tile(oq, orc, col_tangents(oq, oce, ox0 + col), row_tangents(oq, oce, oy0 + r)))
+            atomicOr(&s_mask[warp][owner], 1u << li);
+        }
+      }
+      __syncwarp();
+      if (!big && valid[j]) {
+        mask[j] = s_mask[warp][lane];
         c = (uint32_t)__popc(mask[j]);
       }
-      ++visible;
     }
     // Large rectangles: the whole warp, one after another.
     for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
