@@ -137,129 +137,135 @@ __device__ __forceinline__ int item_view(uint32_t splatIndex, uint32_t n, int vi
   return views == 1 ? 0 : (int)(splatIndex / n);
 }
 
-__global__ void __launch_bounds__(kScanThreads)
-    k_bin_count_scan(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
-                     const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
-                     uint32_t *__restrict__ offsets, uint32_t *__restrict__ masks, uint32_t *counters, uint32_t capacity,
-                     unsigned long long *status, uint32_t *ticket, uint32_t *error) {
+// Coverage count, one thread per item, no block-wide waits: counts[r] (in
+// the offsets array, scanned in place afterwards) and masks[r].
+constexpr int kCountThreads = 256;
+
+__global__ void __launch_bounds__(kCountThreads)
+    k_bin_count(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
+                const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
+                uint32_t *__restrict__ counts, uint32_t *__restrict__ masks, uint32_t *counters) {
   const ViewSet &views = *viewsPtr;
+  __shared__ ColTangents s_cols[kCountThreads / 32][kTableMax];
+  __shared__ RowTangents s_rows[kCountThreads / 32][kTableMax];
+  __shared__ uint32_t s_mask[kCountThreads / 32][32];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t r = blockIdx.x * kCountThreads + threadIdx.x;
+  // Whole warps stay to the end: the loops below are warp-wide.
+  const bool valid = r < items && itemKeys[r] != kInvisible;
+  const uint32_t s = valid ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
+  float4 ce = make_float4(0.f, 0.f, 0.f, 0.f), cq = ce;
+  float rc = 0.0f;
+  TileRect rect{0u, 0u, 0u, 0u};
+  uint32_t area = 0;
+  if (valid) {
+    ce = splats[s].centerExtent;
+    cq = splats[s].conicOpacity;
+    rc = reach[s];
+    const ViewParams &cam = views.v[item_view(s, n, views.count)];
+    rect = splat_tiles(ce, cam.gridW, cam.gridH);
+    area = rect_area(rect);
+  }
+  const uint32_t visibleLanes = __ballot_sync(0xFFFFFFFFu, valid);
+  if (lane == 0 && visibleLanes != 0u) atomicAdd(&counters[0], (uint32_t)__popc(visibleLanes));
+  const bool big = area > kWarpTiles;
+  uint32_t count = 0, mask = 0;
+
+  // Small rectangles: the warp's (splat, tile) pairs laid out flat, 32 tests
+  // per trip with every lane busy; each splat's mask (bit = row-major index in
+  // its rectangle) is assembled in shared memory.
+  {
+    const uint32_t own = big ? 0u : area;
+    uint32_t incl = own;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= (uint32_t)o) incl += x;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31), excl = incl - own;
+    const uint32_t width = rect.x1 - rect.x0 + 1u;
+    const float invWidth = 1.0f / (float)width;
+    s_mask[warp][lane] = 0u;
+    __syncwarp();
+    for (uint32_t base = 0; base < total; base += 32u) {
+      const uint32_t f = base + lane;
+      uint32_t owner = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1)
+        if (__shfl_sync(0xFFFFFFFFu, incl, owner + step - 1u) <= f) owner += step;
+      const uint32_t li = f - __shfl_sync(0xFFFFFFFFu, excl, owner);
+      const float4 oce = make_float4(__shfl_sync(0xFFFFFFFFu, ce.x, owner), __shfl_sync(0xFFFFFFFFu, ce.y, owner), 0.f, 0.f);
+      const float4 oq = make_float4(__shfl_sync(0xFFFFFFFFu, cq.x, owner), __shfl_sync(0xFFFFFFFFu, cq.y, owner),
+                                    __shfl_sync(0xFFFFFFFFu, cq.z, owner), 0.f);
+      const float orc = __shfl_sync(0xFFFFFFFFu, rc, owner);
+      const uint32_t ox0 = __shfl_sync(0xFFFFFFFFu, rect.x0, owner), oy0 = __shfl_sync(0xFFFFFFFFu, rect.y0, owner);
+      const uint32_t ow = __shfl_sync(0xFFFFFFFFu, width, owner);
+      const float oinv = __shfl_sync(0xFFFFFFFFu, invWidth, owner);
+      if (f < total) {
+        const uint32_t row = (uint32_t)(((float)li + 0.5f) * oinv), col = li - row * ow;
+        if (reaches_tile(oq, orc, col_tangents(oq, oce, ox0 + col), row_tangents(oq, oce, oy0 + row)))
+          atomicOr(&s_mask[warp][owner], 1u << li);
+      }
+    }
+    __syncwarp();
+    if (!big) {
+      mask = s_mask[warp][lane];
+      count = (uint32_t)__popc(mask);
+    }
+  }
+  // Large rectangles: the whole warp, one after another.
+  for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
+    const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
+    const uint32_t bs = __shfl_sync(0xFFFFFFFFu, s, src);
+    const ViewParams &cam = views.v[item_view(bs, n, views.count)];
+    const Splat sp = splats[bs];
+    const float rcb = reach[bs];
+    const TileRect bt = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    const uint32_t width = bt.x1 - bt.x0 + 1u, barea = rect_area(bt);
+    const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, bt, lane, s_cols[warp], s_rows[warp]);
+    const float invWidth = 1.0f / (float)width;
+    uint32_t total = 0, hits = 0, x = 0, y = 0;
+    for (uint32_t base = 0; base < barea; base += 32u) {
+      hits = warp_reach(sp.conicOpacity, sp.centerExtent, rcb, bt, width, invWidth, barea, base, lane,
+                        tables ? s_cols[warp] : nullptr, s_rows[warp], x, y);
+      total += (uint32_t)__popc(hits);
+    }
+    __syncwarp(); // the tables are read before the next rectangle fills them
+    if (lane == src) {
+      count = total;
+      mask = barea <= 32u ? hits : 0u; // the emission replays masks of one word only
+    }
+  }
+  if (r < items) {
+    counts[r] = count;
+    masks[r] = mask;
+  }
+}
+
+// Exclusive scan of the coverage counts, in place (counts become offsets):
+// a block of kScanThreads threads takes kScanTile consecutive items, claimed
+// in launch order through a ticket, and finds what precedes it by a
+// decoupled look-back. counters[1] gets the total, counters[2] the entries
+// that fit the capacity; a total above it sets kErrEntryOverflow.
+__global__ void __launch_bounds__(kScanThreads)
+    k_offsets_scan(uint32_t items, uint32_t *__restrict__ offsets, uint32_t *counters, uint32_t capacity,
+                   unsigned long long *status, uint32_t *ticket, uint32_t *error) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ unsigned long long s_exclusive;
-  __shared__ ColTangents s_cols[kScanThreads / 32][kTableMax];
-  __shared__ RowTangents s_rows[kScanThreads / 32][kTableMax];
-  __shared__ uint32_t s_mask[kScanThreads / 32][32];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   if (t == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t numTiles = div_up(items, kScanTile);
   if (tile >= numTiles) return;
-
-  // Loads first: the items' splats, then the tests.
-  uint32_t sIdx[kScanItems];
-  bool valid[kScanItems];
+  uint32_t counts[kScanItems];
+  uint32_t threadSum = 0;
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
-    valid[j] = r < items && itemKeys[r] != kInvisible;
-    sIdx[j] = valid[j] ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
-  }
-  float4 ce[kScanItems], cq[kScanItems];
-  float rc[kScanItems];
-#pragma unroll
-  for (int j = 0; j < kScanItems; ++j) {
-    if (valid[j]) {
-      ce[j] = splats[sIdx[j]].centerExtent;
-      cq[j] = splats[sIdx[j]].conicOpacity;
-      rc[j] = reach[sIdx[j]];
-    } else {
-      ce[j] = cq[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-      rc[j] = 0.0f;
-    }
-  }
-  uint32_t counts[kScanItems], mask[kScanItems];
-  uint32_t threadSum = 0, visible = 0;
-#pragma unroll
-  for (int j = 0; j < kScanItems; ++j) {
-    uint32_t c = 0;
-    mask[j] = 0u;
-    TileRect rect{0u, 0u, 0u, 0u};
-    uint32_t area = 0;
-    if (valid[j]) {
-      const ViewParams &cam = views.v[item_view(sIdx[j], n, views.count)];
-      rect = splat_tiles(ce[j], cam.gridW, cam.gridH);
-      area = rect_area(rect);
-      ++visible;
-    }
-    const bool big = area > kWarpTiles;
-    // Small rectangles: the warp's (splat, tile) pairs laid out flat, 32 tests
-    // per trip with every lane busy; each splat's mask (bit = row-major index
-    // in its rectangle) is assembled in shared memory.
-    {
-      const uint32_t own = big ? 0u : area;
-      uint32_t incl = own;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= (uint32_t)o) incl += x;
-      }
-      const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31), excl = incl - own;
-      const uint32_t width = rect.x1 - rect.x0 + 1u;
-      const float invWidth = 1.0f / (float)width;
-      s_mask[warp][lane] = 0u;
-      __syncwarp();
-      for (uint32_t base = 0; base < total; base += 32u) {
-        const uint32_t f = base + lane;
-        uint32_t owner = 0;
-#pragma unroll
-        for (uint32_t step = 16; step > 0; step >>= 1)
-          if (__shfl_sync(0xFFFFFFFFu, incl, owner + step - 1u) <= f) owner += step;
-        const uint32_t li = f - __shfl_sync(0xFFFFFFFFu, excl, owner);
-        const float4 oce = make_float4(__shfl_sync(0xFFFFFFFFu, ce[j].x, owner), __shfl_sync(0xFFFFFFFFu, ce[j].y, owner), 0.f, 0.f);
-        const float4 oq = make_float4(__shfl_sync(0xFFFFFFFFu, cq[j].x, owner), __shfl_sync(0xFFFFFFFFu, cq[j].y, owner),
-                                      __shfl_sync(0xFFFFFFFFu, cq[j].z, owner), 0.f);
-        const float orc = __shfl_sync(0xFFFFFFFFu, rc[j], owner);
-        const uint32_t ox0 = __shfl_sync(0xFFFFFFFFu, rect.x0, owner), oy0 = __shfl_sync(0xFFFFFFFFu, rect.y0, owner);
-        const uint32_t ow = __shfl_sync(0xFFFFFFFFu, width, owner);
-        const float oinv = __shfl_sync(0xFFFFFFFFu, invWidth, owner);
-        if (f < total) {
-          const uint32_t r = (uint32_t)(((float)li + 0.5f) * oinv), col = li - r * ow;
-          if (reaches_tile(oq, orc, col_tangents(oq, oce, ox0 + col), row_tangents(oq, oce, oy0 + r)))
-            atomicOr(&s_mask[warp][owner], 1u << li);
-        }
-      }
-      __syncwarp();
-      if (!big && valid[j]) {
-        mask[j] = s_mask[warp][lane];
-        c = (uint32_t)__popc(mask[j]);
-      }
-    }
-    // Large rectangles: the whole warp, one after another.
-    for (uint32_t bigLanes = __ballot_sync(0xFFFFFFFFu, big); bigLanes != 0u; bigLanes &= bigLanes - 1u) {
-      const uint32_t src = (uint32_t)__ffs(bigLanes) - 1u;
-      const uint32_t bs = __shfl_sync(0xFFFFFFFFu, sIdx[j], src);
-      const ViewParams &cam = views.v[item_view(bs, n, views.count)];
-      const Splat sp = splats[bs];
-      const float rcb = reach[bs];
-      const TileRect rect = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
-      const uint32_t width = rect.x1 - rect.x0 + 1u, area = rect_area(rect);
-      const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, rect, lane, s_cols[warp], s_rows[warp]);
-      const float invWidth = 1.0f / (float)width;
-      uint32_t total = 0, hits = 0, x = 0, y = 0;
-      for (uint32_t base = 0; base < area; base += 32u) {
-        hits = warp_reach(sp.conicOpacity, sp.centerExtent, rcb, rect, width, invWidth, area, base, lane,
-                          tables ? s_cols[warp] : nullptr, s_rows[warp], x, y);
-        total += (uint32_t)__popc(hits);
-      }
-      __syncwarp(); // the tables are read before the next rectangle fills them
-      if (lane == src) {
-        c = total;
-        mask[j] = area <= 32u ? hits : 0u; // the emission replays masks of one word only
-      }
-    }
-    counts[j] = c;
-    threadSum += c;
+    counts[j] = r < items ? offsets[r] : 0u;
+    threadSum += counts[j];
   }
   // Block scan of the thread sums.
   uint32_t inclusive = threadSum;
@@ -268,9 +274,7 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, inclusive, o);
     if (lane >= (uint32_t)o) inclusive += x;
   }
-  uint32_t warpVisible = __reduce_add_sync(0xFFFFFFFFu, visible);
   if (lane == 31) s_warp[warp] = inclusive;
-  if (lane == 0 && warpVisible != 0) atomicAdd(&counters[0], warpVisible);
   __syncthreads();
   uint32_t before = 0, tileSum = 0;
 #pragma unroll
@@ -329,10 +333,7 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
-    if (r < items) {
-      offsets[r] = running;
-      masks[r] = mask[j];
-    }
+    if (r < items) offsets[r] = running;
     running += counts[j];
   }
 }
@@ -493,8 +494,9 @@ void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
   cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
-  k_bin_count_scan<<<tiles, kScanThreads, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks,
-                                                       counters, capacity, status, ticket, error);
+  k_bin_count<<<div_up(items, kCountThreads), kCountThreads, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews,
+                                                                        offsets, masks, counters);
+  k_offsets_scan<<<tiles, kScanThreads, 0, stream>>>(items, offsets, counters, capacity, status, ticket, error);
 }
 
 void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
