@@ -410,3 +410,26 @@ def test_chosen_form_against_fp64(splat, oracle, layout):
     assert psnr > 60.0
     for name, err in errors.items():
         assert err < 1e-3, f"{name}: relative error {err}"
+
+
+def test_prefetched_targets_change_nothing(splat, oracle):
+    # step(next_target=...) copies the next target during the step; the results
+    # are those of plain steps, also when the next call uses another target.
+    view = oracle.train_camera(96, 80)
+    targets = [oracle.smooth_target(96, 80, s) for s in (3, 4, 5)]
+    cloud = oracle.random_cloud(500, 1, 43)
+    rates = splat.LearningRates(position=1e-3)
+    order = [0, 1, 2, 0, 1]
+    runs = []
+    for prefetch in (False, True):
+        opts = splat.TrainerOptions(force_fixed_point=True, use_graph=True)
+        t = splat.Trainer(to_cloud(cloud), opts)
+        losses = []
+        for i, k in enumerate(order):
+            # The prefetch names target (k + 1) % 3, which is not the next one at i = 2.
+            nxt = targets[(k + 1) % 3] if prefetch else None
+            losses.append(t.step(to_camera(view), targets[k], rates, next_target=nxt).loss)
+        runs.append((losses, t.cloud()))
+    assert runs[0][0] == runs[1][0]
+    np.testing.assert_array_equal(runs[0][1].positions, runs[1][1].positions)
+    np.testing.assert_array_equal(runs[0][1].sh, runs[1][1].sh)

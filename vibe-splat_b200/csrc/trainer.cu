@@ -171,6 +171,8 @@ public:
   PinnedBuffer hViews, hArgs, hReadback, staging, stagingNext;
   const uint8_t *prefetched = nullptr;
   size_t prefetchedBytes = 0;
+  const uint8_t *pendingPrefetch = nullptr; // the next step's target, copied during this step
+  size_t pendingPrefetchBytes = 0;
 
   ViewSet views{};
   uint32_t adamStep = 0;
@@ -197,6 +199,7 @@ public:
   Params params() const;
   OptimState optim_state();
   void upload_targets(const uint8_t *const *targets, const size_t *bytes, int count);
+  void stage_prefetch();
   void record_prepare();
   void record_forward();
   void record_backward_and_chain(ChainMode mode, bool statistics);
@@ -496,6 +499,17 @@ void Trainer::ensure_entries(uint32_t total) {
   clear_graphs();
 }
 
+// Copies the target named for the next step into the second pinned buffer;
+// run() calls it once the step's work is queued, so the copy overlaps it.
+void Trainer::stage_prefetch() {
+  if (pendingPrefetch == nullptr) return;
+  stagingNext.ensure(pendingPrefetchBytes);
+  std::memcpy(stagingNext.get(), pendingPrefetch, pendingPrefetchBytes);
+  prefetched = pendingPrefetch;
+  prefetchedBytes = pendingPrefetchBytes;
+  pendingPrefetch = nullptr;
+}
+
 void Trainer::upload_targets(const uint8_t *const *targets, const size_t *bytes, int count) {
   size_t total = 0;
   for (int k = 0; k < count; ++k) {
@@ -742,6 +756,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
         it = graphs.emplace(key, e).first;
       }
       SB_CUDA(cudaGraphLaunch(it->second.exec, stream));
+      stage_prefetch(); // host copy of the next target while the GPU runs the step
       SB_CUDA(cudaStreamSynchronize(stream));
       const StepReadback *rb = hReadback.get<StepReadback>();
       if ((rb->error & kErrEntryOverflow) != 0u) {
@@ -770,6 +785,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
     record_forward();
     record_backward_and_chain(mode, statistics);
     record_readback();
+    stage_prefetch();
     SB_CUDA(cudaStreamSynchronize(stream));
   }
   const StepReadback *rb = hReadback.get<StepReadback>();
@@ -1059,8 +1075,13 @@ int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_r
 int splat_trainer_step(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
                        const splat_learning_rates *rates, const uint8_t *next_target, size_t next_target_bytes,
                        splat_step_stats *stats) {
+  // The next target is copied to pinned memory while this step runs on the GPU.
+  if (trainer != nullptr && trainer->impl != nullptr && next_target != nullptr) {
+    impl_of(trainer)->pendingPrefetch = next_target;
+    impl_of(trainer)->pendingPrefetchBytes = next_target_bytes;
+  }
   const int status = run_one(trainer, camera, target, target_bytes, sb::ChainMode::Step, rates, true, stats);
-  if (status == SPLAT_OK && next_target != nullptr) return splat_trainer_prefetch_target(trainer, next_target, next_target_bytes);
+  if (trainer != nullptr && trainer->impl != nullptr) impl_of(trainer)->pendingPrefetch = nullptr;
   return status;
 }
 
