@@ -97,6 +97,12 @@ typedef struct splat_trainer_options {
                                          groups. */
   int32_t split_step;         /* 0: a one-view Adam step is one fused kernel (chain rule, geometry and SH
                                  step); 1: three kernels, as for batches. The results are the same bits. */
+  int32_t blend_lists;        /* 0: the backward recomputes each pixel's transmittance in a reverse sweep,
+                                 keeping 8 bytes per pixel (the reference's design). 1: store everything:
+                                 the forward records every blended (entry, alpha) pair per pixel, 8 bytes
+                                 each, and the backward walks those lists (float sums, one view, no CUDA
+                                 graph: the list total is read back before the recording pass). For
+                                 comparison of memory and speed. */
 } splat_trainer_options;
 
 /* LearningRates (src/train/trainer.hpp:51-61); trust_region must be 0. */

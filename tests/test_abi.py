@@ -70,7 +70,7 @@ def test_empty_cloud_is_refused():
 def test_unsupported_options_are_refused_not_emulated():
     s = splat_module()
     for opts in (s.TrainerOptions(mip_filter_2d=True), s.TrainerOptions(position_noise=0.1),
-                 s.TrainerOptions(pose_gradients=True)):
+                 s.TrainerOptions(pose_gradients=True), s.TrainerOptions(blend_lists=True, force_fixed_point=True)):
         with pytest.raises(s.UnsupportedOption):
             s.Trainer(_tiny_cloud(s), opts)
 

@@ -433,3 +433,54 @@ def test_prefetched_targets_change_nothing(splat, oracle):
     assert runs[0][0] == runs[1][0]
     np.testing.assert_array_equal(runs[0][1].positions, runs[1][1].positions)
     np.testing.assert_array_equal(runs[0][1].sh, runs[1][1].sh)
+
+
+def test_config1_plain_small_case(splat, oracle):
+    # The plain method's small case: L1 loss only, fixed-point backward, against
+    # the FP64 twin (the reference's tolerances) and, bit for bit, against the
+    # restatement's fixed-point sums.
+    from tests.helpers import config1_scene
+
+    cloud, view, target = config1_scene(oracle, 101)
+    rgb, _, _ = oracle.ref_render(cloud, view)
+    loss, l1, _, adjoint = oracle.ref_loss(rgb, 128, 128, target, 0.0)
+    cpu = oracle.ref_gradients(cloud, view, adjoint)
+    trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=True, lambda_ssim=0.0))
+    image = trainer.render(to_camera(view)).reshape(-1, 4)
+    assert np.max(np.abs(image[:, :3] - rgb.reshape(-1, 3))) < 1e-3
+    stats = trainer.compute_gradients(to_camera(view), target)
+    assert abs(stats.loss - loss) < 1e-3 and abs(stats.l1 - l1) < 1e-3
+    g = trainer.gradients()
+    for name in ("positions", "scales", "rotations", "opacities", "sh"):
+        check_close(getattr(g, name), getattr(cpu, name), name, 0.97, 0.1)
+    n = cloud.count
+    splats, reach, keys = device_projection(trainer, n)
+    tiles, values, ranges = oracle_entries(oracle, splats, reach, keys, view)
+    dimage = trainer.debug_download(splat.DEBUG_IMAGE, np.float32).reshape(-1, 4)
+    stops = trainer.debug_download(splat.DEBUG_STOPS, np.uint32)
+    dadjoint = trainer.debug_download(splat.DEBUG_ADJOINT, np.float32).reshape(-1, 4)
+    raw = trainer.debug_download(splat.DEBUG_RAW, np.int32)[: n * 16].reshape(n, 16)
+    o_raw = oracle.backward(splats, values, ranges, view, dimage, dadjoint, stops, True, n)
+    assert np.count_nonzero(raw) > 1000
+    np.testing.assert_array_equal(raw[:, :14], o_raw[:, :14])
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_blend_lists_match_recompute(splat, oracle, exact):
+    # The store-everything variant against the reverse-sweep recompute: the
+    # same image (the same compositing), the same gradients up to the order of
+    # float sums and the transmittance's rounding (division vs exp/log).
+    view = oracle.train_camera(128, 96)
+    target = oracle.smooth_target(128, 96, 7)
+    cloud = oracle.random_cloud(2000, 2, 53)
+    out = []
+    for lists in (False, True):
+        t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(exact_math=exact, blend_lists=lists,
+                                                                backward_pixels_per_thread=1))
+        image = t.render(to_camera(view))
+        stats = t.compute_gradients(to_camera(view), target)
+        out.append((image, stats, t.gradients()))
+    np.testing.assert_array_equal(out[0][0].view(np.uint32), out[1][0].view(np.uint32))
+    assert out[0][1].loss == out[1][1].loss
+    for name in ("positions", "scales", "rotations", "opacities", "sh"):
+        check_close(getattr(out[1][2], name), getattr(out[0][2], name), name, 0.99999, 1e-3)

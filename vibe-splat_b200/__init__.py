@@ -72,6 +72,7 @@ class _Options(ctypes.Structure):
         ("forward_pixels_per_thread", ctypes.c_int32),
         ("backward_pixels_per_thread", ctypes.c_int32),
         ("split_step", ctypes.c_int32),
+        ("blend_lists", ctypes.c_int32),
     ]
 
 
@@ -326,6 +327,7 @@ class TrainerOptions:
     forward_pixels_per_thread: int = 1
     backward_pixels_per_thread: int = 2
     split_step: bool = False
+    blend_lists: bool = False
 
     def _c(self) -> _Options:
         o = _Options()
@@ -343,6 +345,7 @@ class TrainerOptions:
         o.forward_pixels_per_thread = self.forward_pixels_per_thread
         o.backward_pixels_per_thread = self.backward_pixels_per_thread
         o.split_step = int(self.split_step)
+        o.blend_lists = int(self.blend_lists)
         return o
 
 

@@ -515,4 +515,14 @@ void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *ti
   k_tile_ranges<<<blocks, 256, 0, stream>>>(tileKeys32, tileKeys64, deviceCount, tileLimit, ranges, error);
 }
 
+void launch_exclusive_scan(uint32_t items, uint32_t *values, uint32_t *counters, void *scratch, uint32_t *error,
+                           cudaStream_t stream) {
+  if (items == 0) return;
+  const uint32_t tiles = div_up(items, kScanTile);
+  unsigned long long *status = static_cast<unsigned long long *>(scratch);
+  uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
+  cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
+  k_offsets_scan<<<tiles, kScanThreads, 0, stream>>>(items, values, counters, 0xFFFFFFFFu, status, ticket, error);
+}
+
 } // namespace sb

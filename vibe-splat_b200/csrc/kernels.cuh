@@ -77,6 +77,15 @@ void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *it
 void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *tileKeys64, const uint32_t *deviceCount,
                         uint32_t capacity, uint32_t tileLimit, uint2 *ranges, uint32_t *error, cudaStream_t stream);
 
+// Per-pixel blend lists of the store-everything variant: counts[p] splats
+// blended at pixel p, recorded front to back at pool[offsets[p] ...] as
+// (entry index, alpha bits).
+struct BlendLists {
+  uint32_t *counts = nullptr;
+  const uint32_t *offsets = nullptr;
+  uint2 *pool = nullptr;
+};
+
 struct RasterConfig {
   int exactMath = 1;   // deterministic exp/log (bit-reproducible by the CPU restatement)
   // Pixels per thread. 1: the reference's 2x16-pixel warps; 2: 8x8-pixel warps, two pixels per lane.
@@ -88,9 +97,11 @@ struct RasterConfig {
 // train_forward.comp: one block per tile of 16x16 pixels. image: 4 floats per
 // pixel (rgb, log transmittance), stops: 1 u32 per pixel, both indexed by
 // view pixelBase + y W + x.
+// listMode 1 also counts each pixel's blended splats into lists.counts, 2
+// also records them (store-everything variant; one pixel per thread).
 void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
                     const RasterConfig &cfg, float4 *image, uint32_t *stops, uint32_t splatLimit, uint32_t *error,
-                    cudaStream_t stream);
+                    cudaStream_t stream, int listMode = 0, BlendLists lists = BlendLists{});
 
 // train_ssim.comp + train_loss.comp: SSIM fields, then the adjoint and L1.
 // partials: 2 floats per global tile (SSIM sum, L1 sum).
@@ -110,6 +121,15 @@ void launch_loss_totals(const float2 *partials, const ViewSet &views, const View
 void launch_backward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
                      const RasterConfig &cfg, const float4 *image, const float4 *adjoint, const uint32_t *stops,
                      bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream);
+// The store-everything backward: float sums from the recorded blend lists.
+void launch_backward_lists(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views,
+                           const ViewSet *dViews, const RasterConfig &cfg, const float4 *image, const float4 *adjoint,
+                           const uint32_t *stops, BlendLists lists, float *raw, uint32_t splatLimit, uint32_t *error,
+                           cudaStream_t stream);
+// Exclusive scan of `items` u32 values in place; *total gets their sum.
+// scratch: bin_scan_scratch_bytes(items) bytes.
+void launch_exclusive_scan(uint32_t items, uint32_t *values, uint32_t *counters, void *scratch, uint32_t *error,
+                           cudaStream_t stream);
 
 // train_gradient.comp + train_sh_step.comp: the chain rule from the raw sums of
 // every view, then (mode) gradients stored, or Adam's step. shGrad holds 2

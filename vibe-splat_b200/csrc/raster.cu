@@ -159,11 +159,15 @@ __device__ __forceinline__ void publish_cover(uint32_t mask, uint32_t word, uint
   if (lane < (uint32_t)WARPS) cover[lane][word] = mine;
 }
 
-template <class M>
+// LISTS: 0 plain; 1 also counts each pixel's blended splats into
+// lists.counts; 2 also records them, front to back, as (entry index, alpha)
+// at lists.pool[lists.offsets[pixel] ...] (the store-everything variant).
+template <class M, int LISTS>
 __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
                                                          const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
                                                          float bgR, float bgG, float bgB, float4 *__restrict__ image,
-                                                         uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
+                                                         uint32_t *__restrict__ stops, BlendLists lists, uint32_t splatLimit,
+                                                         uint32_t *error) {
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
   __shared__ uint32_t s_cover[kTilePixels / 32][kBatch / 32];
@@ -181,6 +185,10 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
   float cr = 0.0f, cg = 0.0f, cb = 0.0f, T = 1.0f, logT = 0.0f;
   uint32_t stop = range.x;
   bool done = !inside;
+  const size_t pixel = inside ? (size_t)cam.pixelBase + (size_t)y * cam.width + x : 0;
+  uint32_t blended = 0;
+  uint2 *list = nullptr;
+  if (LISTS == 2 && inside) list = lists.pool + lists.offsets[pixel];
   for (uint32_t end = range.y; end > range.x;) {
     const uint32_t count = min((uint32_t)kBatch, end - range.x);
     end -= count;
@@ -219,13 +227,15 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
         cb = fmaf(w, s.b, cb);
         T = T * oneMinus;
         logT = logT + logRest;
+        if (LISTS == 2) list[blended] = make_uint2(end + k, __float_as_uint(alpha));
+        if (LISTS != 0) ++blended;
       }
     }
   }
   if (inside) {
-    const size_t at = (size_t)cam.pixelBase + (size_t)y * cam.width + x;
-    image[at] = make_float4(fmaf(T, bgR, cr), fmaf(T, bgG, cg), fmaf(T, bgB, cb), logT);
-    stops[at] = stop;
+    image[pixel] = make_float4(fmaf(T, bgR, cr), fmaf(T, bgG, cg), fmaf(T, bgB, cb), logT);
+    stops[pixel] = stop;
+    if (LISTS == 1) lists.counts[pixel] = blended;
   }
 }
 
@@ -386,6 +396,121 @@ __global__ void __launch_bounds__(kTilePixels, 4)
             atomicAdd(reinterpret_cast<float *>(raw32 + base + j), __uint_as_float(v));
           }
           s_acc[t * kAccStride + j] = 0u;
+        }
+      }
+    }
+  }
+}
+
+// The store-everything backward (float sums): each pixel walks the list of
+// (entry index, alpha) its forward recorded, from the back, instead of
+// recomputing alpha and the transmittance: T in front of a splat is the
+// transmittance behind it divided by (1 - alpha). One pixel per thread, the
+// reference's 16x2 warps and butterfly; the per-splat arithmetic of the
+// gradients is that of k_backward.
+template <class M>
+__global__ void __launch_bounds__(kTilePixels, 4)
+    k_backward_lists(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
+                     const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
+                     const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, BlendLists lists,
+                     float *__restrict__ raw, uint32_t splatLimit, uint32_t *error) {
+  const ViewSet &views = *viewsPtr;
+  __shared__ Staged s_batch[kBatch];
+  __shared__ float s_acc[kBatch * kAccStride];
+  __shared__ uint32_t s_min[kTilePixels / 32];
+  __shared__ uint32_t s_cover[kTilePixels / 32][kBatch / 32];
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const int tile = blockIdx.x;
+  const TileGeometry geo = tile_geometry(views, tile);
+  const ViewParams &cam = views.v[geo.view];
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5, lx = t & 15u, ly = t >> 4;
+  const uint32_t x = geo.x0 + lx, y = geo.y0 + ly;
+  const bool inside = x < (uint32_t)cam.width && y < (uint32_t)cam.height;
+  const uint32_t myBits = (1u << lx) | (1u << (16 + ly));
+  const float pxf = (float)x + 0.5f, pyf = (float)y + 0.5f;
+  const size_t at = inside ? (size_t)cam.pixelBase + (size_t)y * cam.width + x : 0;
+  // Transmittance behind everything the pixel blended.
+  float Tcur = inside ? M::exp(image[at].w) : 1.0f;
+  const float4 A = inside ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float perPixel = cam.perPixel;
+  const uint2 range = ranges[tile];
+  const uint32_t stop = inside ? stops[at] : range.y;
+  // The list, walked from its end (the farthest blended splat).
+  const uint2 *list = lists.pool + (inside ? lists.offsets[at] : 0u);
+  int cursor = inside ? (int)lists.counts[at] - 1 : -1;
+  uint2 next = cursor >= 0 ? list[cursor] : make_uint2(0xFFFFFFFFu, 0u);
+  const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, stop);
+  if (lane == 0) s_min[warp] = warpMin;
+  for (int i = t; i < kBatch * kAccStride; i += kTilePixels) s_acc[i] = 0.0f;
+  __syncthreads();
+  uint32_t tileStop = s_min[0];
+#pragma unroll
+  for (int w = 1; w < kTilePixels / 32; ++w) tileStop = min(tileStop, s_min[w]);
+
+  float Br = bgR, Bg = bgG, Bb = bgB;
+  const uint32_t held = __brev(lane) >> 28;
+
+  for (uint32_t start = tileStop; start < range.y; start += kBatch) {
+    const uint32_t count = min((uint32_t)kBatch, range.y - start);
+    __syncthreads();
+    uint32_t stagedMask = 0u;
+    if (t < count) {
+      const Staged st = stage_checked<M>(splats, entryValues[start + t], splatLimit, geo, error);
+      s_batch[t] = st;
+      stagedMask = st.mask;
+    }
+    publish_cover<kTilePixels / 32>(stagedMask, warp, lane, s_cover);
+    __syncthreads();
+    for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
+    for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
+      const uint32_t k = word * 32u + (uint32_t)(__ffs(bits) - 1);
+      const bool act = next.x == start + k;
+      if (!__any_sync(0xFFFFFFFFu, act)) continue;
+      const Staged &s = s_batch[k];
+      const float alpha = act ? __uint_as_float(next.y) : 0.0f;
+      const float Tf = Tcur * __frcp_rn(1.0f - alpha);
+      const float wA = Tf * alpha;
+      const float dx = pxf - s.cx, dy = pyf - s.cy;
+      float g[12];
+      g[6] = wA * A.x;
+      g[7] = wA * A.y;
+      g[8] = wA * A.z;
+      g[9] = wA * perPixel;
+      // At the 0.99 clamp alpha no longer depends on the parameters; below it
+      // alpha = opacity * exp(power).
+      const float dAlpha = (act && alpha < kAlphaMax) ? Tf * fmaf(A.z, s.b - Bb, fmaf(A.y, s.g - Bg, A.x * (s.r - Br))) : 0.0f;
+      g[0] = dAlpha * (alpha / s.opacity);
+      const float dPower = dAlpha * alpha;
+      const float vx = fmaf(s.qy, dy, s.qx * dx), vy = fmaf(s.qz, dy, s.qy * dx);
+      g[1] = dPower * vx;
+      g[2] = dPower * vy;
+      g[10] = fabsf(g[1]);
+      g[11] = fabsf(g[2]);
+      const float h = dPower * 0.5f;
+      g[3] = h * vx * vx;
+      g[4] = h * vx * vy;
+      g[5] = h * vy * vy;
+      Br = fmaf(alpha, s.r - Br, Br);
+      Bg = fmaf(alpha, s.g - Bg, Bg);
+      Bb = fmaf(alpha, s.b - Bb, Bb);
+      if (act) {
+        Tcur = Tf;
+        --cursor;
+        next = cursor >= 0 ? list[cursor] : make_uint2(0xFFFFFFFFu, 0u);
+      }
+      const float total = butterfly12(g);
+      if (lane < 16 && held < (uint32_t)kGradValues && total != 0.0f) atomicAdd(&s_acc[k * kAccStride + held], total);
+    }
+    __syncthreads();
+    // One global atomic per (splat, value) for the whole tile.
+    if (t < count && s_batch[t].mask != 0u) {
+      float *dst = raw + (size_t)s_batch[t].index * kRawStride;
+#pragma unroll
+      for (int j = 0; j < kGradValues; ++j) {
+        const float v = s_acc[t * kAccStride + j];
+        if (v != 0.0f) {
+          atomicAdd(dst + j, v);
+          s_acc[t * kAccStride + j] = 0.0f;
         }
       }
     }
@@ -638,9 +763,23 @@ __global__ void __launch_bounds__(kHalfTile, 6)
 
 void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
                     const RasterConfig &cfg, float4 *image, uint32_t *stops, uint32_t splatLimit, uint32_t *error,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, int listMode, BlendLists lists) {
   if (views.totalTiles == 0) return;
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
+  if (listMode != 0) {
+#define SB_FORWARD_LISTS(MATH, MODE)                                                                                         \
+  k_forward<MATH, MODE><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops, \
+                                                                     lists, splatLimit, error)
+    if (cfg.exactMath) {
+      if (listMode == 1) SB_FORWARD_LISTS(ExactMath, 1);
+      else SB_FORWARD_LISTS(ExactMath, 2);
+    } else {
+      if (listMode == 1) SB_FORWARD_LISTS(FastMath, 1);
+      else SB_FORWARD_LISTS(FastMath, 2);
+    }
+#undef SB_FORWARD_LISTS
+    return;
+  }
   if (cfg.forwardPixels == 2) {
     if (cfg.exactMath)
       k_forward2<ExactMath><<<views.totalTiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
@@ -650,11 +789,11 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
                                                                       splatLimit, error);
   } else {
     if (cfg.exactMath)
-      k_forward<ExactMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
-                                                                        splatLimit, error);
+      k_forward<ExactMath, 0><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+                                                                           stops, BlendLists{}, splatLimit, error);
     else
-      k_forward<FastMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
-                                                                       splatLimit, error);
+      k_forward<FastMath, 0><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+                                                                          stops, BlendLists{}, splatLimit, error);
   }
 }
 
@@ -686,6 +825,20 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
     else SB_BACKWARD(FastMath, false);
   }
 #undef SB_BACKWARD
+}
+
+void launch_backward_lists(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views,
+                           const ViewSet *dViews, const RasterConfig &cfg, const float4 *image, const float4 *adjoint,
+                           const uint32_t *stops, BlendLists lists, float *raw, uint32_t splatLimit, uint32_t *error,
+                           cudaStream_t stream) {
+  if (views.totalTiles == 0) return;
+  const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
+  if (cfg.exactMath)
+    k_backward_lists<ExactMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+                                                                             adjoint, stops, lists, raw, splatLimit, error);
+  else
+    k_backward_lists<FastMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+                                                                            adjoint, stops, lists, raw, splatLimit, error);
 }
 
 } // namespace sb

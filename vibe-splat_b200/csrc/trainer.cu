@@ -149,6 +149,7 @@ public:
   ShStore shStore = ShStore::F16;
   StateStore stateStore = StateStore::BF16Pair;
   bool fixedPoint = false, oneSort = false, exactMath = true, useGraph = false;
+  bool blendLists = false; // store-everything backward
   int digitBits = 8;
   int forwardPixels = 1, backwardPixels = 2; // pixels per thread of the compositing and float backward kernels
   cudaStream_t stream = nullptr;
@@ -166,6 +167,8 @@ public:
   bool entriesInTmp = false, depthInTmp = false;
   // Per pixel and per tile of the views of a step.
   DeviceBuffer image, stops, adjoint, fields, target, ranges, partials;
+  // Store-everything variant: per-pixel blend counts, list offsets, the list pool, scan scratch and counters.
+  DeviceBuffer listCounts, listOffsets, listPool, listScratch, listCounters;
   // Small things.
   DeviceBuffer dViews, dArgs, dReadback, sortScratchDepth, sortScratchEntries, scanScratch;
   PinnedBuffer hViews, hArgs, hReadback, staging, stagingNext;
@@ -241,6 +244,8 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   stateStore = (StateStore)opt.state_storage;
   // The reference picks fixed point on GPUs without float atomics (trainer.cpp:181); a B200 has them.
   fixedPoint = opt.force_fixed_point != 0;
+  blendLists = opt.blend_lists != 0;
+  if (blendLists && fixedPoint) throw Failure{SPLAT_ERR_UNSUPPORTED, "blend lists keep float sums: no fixed-point form"};
   oneSort = opt.sort_form == SPLAT_SORT_TILE_DEPTH_64;
   exactMath = opt.exact_math != 0;
   useGraph = opt.use_graph != 0;
@@ -375,7 +380,8 @@ uint64_t Trainer::entry_bytes(uint64_t entries) const {
 uint64_t Trainer::gpu_bytes() const {
   uint64_t total = bytes_per_gaussian() * n;
   for (const DeviceBuffer *b : {&image, &stops, &adjoint, &fields, &target, &ranges, &partials, &entryKeys, &entryValues,
-                                &tmpEntryKeys, &tmpEntryValues, &sortScratchDepth, &sortScratchEntries, &scanScratch})
+                                &tmpEntryKeys, &tmpEntryValues, &sortScratchDepth, &sortScratchEntries, &scanScratch,
+                                &listCounts, &listOffsets, &listPool, &listScratch, &listCounters})
     total += b->bytes();
   return total;
 }
@@ -454,6 +460,12 @@ void Trainer::ensure_view_buffers() {
   ranges.ensure(tiles * 8);
   partials.ensure(tiles * 8);
   if (image.bytes() + target.bytes() + ranges.bytes() != before) clear_graphs();
+  if (blendLists) {
+    listCounts.ensure(pixels * 4);
+    listOffsets.ensure(pixels * 4);
+    listScratch.ensure(bin_scan_scratch_bytes((uint32_t)pixels));
+    listCounters.ensure(16);
+  }
   const size_t items = (size_t)n * (oneSort ? count : 1);
   if (scanScratch.bytes() < bin_scan_scratch_bytes((uint32_t)items)) {
     scanScratch.ensure(bin_scan_scratch_bytes((uint32_t)items));
@@ -605,8 +617,34 @@ void Trainer::record_forward() {
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
   begin(4);
-  launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
-                 stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
+  if (blendLists) {
+    // Store everything: count each pixel's blended splats, scan the counts
+    // into list offsets, read the total back, then composite again recording
+    // the lists.
+    BlendLists lists;
+    lists.counts = listCounts.get<uint32_t>();
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                   stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream, 1, lists);
+    const size_t pixels = (size_t)views.totalPixels;
+    SB_CUDA(cudaMemcpyAsync(listOffsets.get(), listCounts.get(), pixels * 4, cudaMemcpyDeviceToDevice, stream));
+    launch_exclusive_scan((uint32_t)pixels, listOffsets.get<uint32_t>(), listCounters.get<uint32_t>(), listScratch.get(), error,
+                          stream);
+    uint32_t counters[4] = {0, 0, 0, 0};
+    SB_CUDA(cudaMemcpyAsync(counters, listCounters.get(), sizeof(counters), cudaMemcpyDeviceToHost, stream));
+    SB_CUDA(cudaStreamSynchronize(stream));
+    const size_t pool = (size_t)counters[1] * sizeof(uint2);
+    if (listPool.bytes() < pool) {
+      listPool.release();
+      listPool.ensure(pool + pool / 2 + 4096);
+    }
+    lists.offsets = listOffsets.get<uint32_t>();
+    lists.pool = listPool.get<uint2>();
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                   stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream, 2, lists);
+  } else {
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                   stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
+  }
   end(4);
 }
 
@@ -628,9 +666,19 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
   begin(6);
-  launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
-                  adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
-                  stream);
+  if (blendLists) {
+    BlendLists lists;
+    lists.counts = listCounts.get<uint32_t>();
+    lists.offsets = listOffsets.get<uint32_t>();
+    lists.pool = listPool.get<uint2>();
+    launch_backward_lists(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                          adjoint.get<float4>(), stops.get<uint32_t>(), lists, raw.get<float>(), n * (uint32_t)views.count,
+                          error, stream);
+  } else {
+    launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+                    adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
+                    stream);
+  }
   end(6);
   ChainArgs args{};
   std::memcpy(&args, hArgs.get(), sizeof(ChainArgs));
@@ -713,6 +761,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
                   const splat_learning_rates *rates, bool statistics, splat_step_stats *stats, bool deviceTargets) {
   set_views(cameras, count);
   if (count > 1 && !oneSort) throw Failure{SPLAT_ERR_UNSUPPORTED, "several views per step need sort_form SPLAT_SORT_TILE_DEPTH_64"};
+  if (count > 1 && blendLists) throw Failure{SPLAT_ERR_UNSUPPORTED, "blend lists are for one view per step"};
   ensure_view_buffers();
   std::memcpy(hViews.get(), &views, sizeof(ViewSet));
   fill_chain_args(mode, statistics, rates);
@@ -731,7 +780,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
   }
 
   bool graphDone = false;
-  if (useGraph && entryKeys.get() != nullptr && !timing) {
+  if (useGraph && !blendLists && entryKeys.get() != nullptr && !timing) {
     for (int attempt = 0; attempt < 3 && !graphDone; ++attempt) {
       const std::string key = graph_key(mode, statistics);
       auto it = graphs.find(key);
