@@ -55,12 +55,12 @@ SEED = 3
 SH_C0 = 0.28209479177387814
 
 
-def make_scene(n: int = GAUSSIANS, degree: int = DEGREE, seed: int = SEED):
+def make_scene(n: int = GAUSSIANS, degree: int = DEGREE, seed: int = SEED, log_scale=(-4.0, 0.5)):
     """The seeded synthetic scene: GaussianCloud arrays (float32)."""
     rng = np.random.default_rng(seed)
     coeffs = (degree + 1) ** 2
     positions = rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32)
-    scales = rng.normal(-4.0, 0.5, (n, 3)).astype(np.float32)
+    scales = rng.normal(log_scale[0], log_scale[1], (n, 3)).astype(np.float32)
     q = rng.normal(0.0, 1.0, (n, 4))
     rotations = (q / np.linalg.norm(q, axis=1, keepdims=True)).astype(np.float32)
     opacities = rng.normal(-1.0, 1.5, n).astype(np.float32)
@@ -340,6 +340,63 @@ def precision_check(splat, torch, cloud, cams, host_targets, rates, chosen, tune
             "psnr_difference_db": abs(after["chosen"] - after["plain"])}
 
 
+def memory_adjoint_workload(args) -> None:
+    """The memory-bound adjoint: 6M Gaussians of SH degree 3 (BF16 above DC),
+    3840x2160 views, log-scales N(-4.5, 0.6) for heavy per-tile overlap. The
+    reverse-sweep recompute (8 bytes of per-pixel state) against the
+    store-everything variant (every blended (entry, alpha) pair kept per pixel):
+    iterations/s, device memory held, per-pixel state. One JSON line."""
+    import torch
+
+    splat = importlib.import_module("vibe-splat_b200")
+    n = 6_000_000 if args.gaussians == GAUSSIANS else args.gaussians
+    width, height, views = 3840, 2160, 4
+    pos, sc, rot, op, sh = make_scene(n, log_scale=(-4.5, 0.6))
+    cloud = splat.GaussianCloud(DEGREE, pos, sc, rot, op, sh)
+    cams = [splat.Camera(v, p, fx, fy, cx, cy, w, h)
+            for (v, p, fx, fy, cx, cy, w, h) in hemisphere_views(views, width=width, height=height)]
+    targets = torch.from_numpy(make_targets(views, width, height)).cuda()
+    rates = splat.LearningRates()
+    pixels = width * height
+    tiles = ((width + 15) // 16) * ((height + 15) // 16)
+    out = {"metric": "memory-bound adjoint: recompute vs store-everything", "unit": "iters/s",
+           "config": {"workload": f"{n} Gaussians, SH degree 3 (BF16 above DC), {width}x{height}, log-scales N(-4.5, 0.6), "
+                                  f"{views} cameras on a radius-5 hemisphere, 60 deg horizontal fov (synthetic)"},
+           "steps": args.steps, "warmup": args.warmup}
+    for name, lists in (("recompute", False), ("store_everything", True)):
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        free0, _ = torch.cuda.mem_get_info()
+        opts = chosen_options(splat)
+        opts.sort_form = splat.SORT_DEPTH_THEN_TILE
+        opts.blend_lists = lists
+        opts.use_graph = not lists
+        if lists:
+            opts.backward_pixels_per_thread = 1
+        trainer = splat.Trainer(cloud, opts)
+        for i in range(args.warmup):
+            stats = trainer.step_device_target(cams[i % views], targets[i % views].data_ptr(), rates)
+        ms = time_steps(torch, trainer, lambda i: trainer.step_device_target(cams[i % views], targets[i % views].data_ptr(),
+                                                                              rates), args.steps, trainer.stream())
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        entry = {"iters_per_s": 1000.0 * args.steps / ms, "ms_per_step": ms / args.steps,
+                 "device_bytes_held": free0 - free1, "tile_entries": stats.tile_entries,
+                 "mean_entries_per_tile": stats.tile_entries / tiles, "per_pixel_state_bytes": 8.0}
+        if lists:
+            counts = trainer.debug_download(splat.DEBUG_BLEND_COUNTS, np.uint32)[:pixels]
+            blended = int(counts.astype(np.uint64).sum())
+            entry["blended_pairs"] = blended
+            entry["mean_blended_per_pixel"] = blended / pixels
+            entry["per_pixel_state_bytes"] = 8.0 + 8.0 + 8.0 * blended / pixels
+        out[name] = entry
+        del trainer
+    r, s = out["recompute"], out["store_everything"]
+    out["memory_saved_bytes"] = s["device_bytes_held"] - r["device_bytes_held"]
+    out["speed_ratio_recompute_over_store"] = r["iters_per_s"] / s["iters_per_s"]
+    print(json.dumps(out))
+
+
 def our_arm(args) -> None:
     import torch
 
@@ -524,6 +581,9 @@ def main() -> None:
     parser.add_argument("--steps", type=int, default=30)
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--workload", choices=["step", "memory-adjoint"], default="step",
+                        help="step: the headline one-view training step; memory-adjoint: 6M Gaussians at 3840x2160, "
+                             "recompute vs store-everything backward")
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
@@ -535,7 +595,9 @@ def main() -> None:
     parser.add_argument("--gaussians", type=int, default=GAUSSIANS,
                         help="scene size (default 1M, the headline workload; smaller cases are for ncu captures)")
     args = parser.parse_args()
-    if args.impl == "reference":
+    if args.workload == "memory-adjoint":
+        memory_adjoint_workload(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         our_arm(args)

@@ -259,8 +259,9 @@ int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint6
  * (4 floats per pixel), 7 stops (u32 per pixel), 8 adjoint (4 floats per
  * pixel), 9 raw sums (16 words per Gaussian: int32 fixed point or float),
  * 10 counters (visible, total entries, used entries, 0), 11 loss partials
- * (2 floats per tile), 12 error word. Copies min(bytes, size) bytes; *size
- * gets the buffer's size in bytes. */
+ * (2 floats per tile), 12 error word, 13 blended splats per pixel (u32; with
+ * blend_lists only, else empty). Copies min(bytes, size) bytes; *size gets the
+ * buffer's size in bytes. */
 int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size);
 
 /* Stage-level entry points on device memory, for the reference's operator

@@ -1402,6 +1402,7 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     case 10: src = rb->counters; have = 16; break;
     case 11: src = t->partials.get(); have = (size_t)t->views.totalTiles * 8; break;
     case 12: src = &rb->error; have = 4; break;
+    case 13: src = t->listCounts.get(); have = t->blendLists ? (size_t)t->views.totalPixels * 4 : 0; break;
     default: throw Failure{SPLAT_ERR_INVALID, "unknown buffer"};
     }
     if (size) *size = have;
