@@ -397,6 +397,67 @@ def memory_adjoint_workload(args) -> None:
     print(json.dumps(out))
 
 
+def batched_workload(args) -> None:
+    """The batched form: 3M Gaussians of SH degree 3 (BF16 above DC), 8 views of
+    uneven sizes per step (one launch per stage for all of them, 64-bit
+    tile|depth keys, CUDA graph), cameras at random points of a sphere of radius
+    4 to 8 looking at the origin. Against the same views one per step. Views/s,
+    one JSON line."""
+    import torch
+
+    splat = importlib.import_module("vibe-splat_b200")
+    n = 3_000_000 if args.gaussians == GAUSSIANS else args.gaussians
+    sizes = [(640, 480), (800, 600), (1024, 768), (1237, 822), (1280, 720), (1600, 1200), (960, 540), (1920, 1080)]
+    rng = np.random.default_rng(SEED + 7)
+    cams, targets = [], []
+    for (w, h) in sizes:
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        eye = d * rng.uniform(4.0, 8.0)
+        forward = -eye / np.linalg.norm(eye)
+        up = np.array([0.0, 0.0, 1.0]) if abs(forward[2]) < 0.99 else np.array([0.0, 1.0, 0.0])
+        right = np.cross(forward, up)
+        right /= np.linalg.norm(right)
+        down = np.cross(forward, right)
+        rot = np.stack([right, down, forward])
+        view = np.eye(4)
+        view[:3, :3] = rot
+        view[:3, 3] = -rot @ eye
+        fx = (w / 2) / math.tan(math.radians(30.0))
+        cams.append(splat.Camera(view.astype(np.float32), eye.astype(np.float32), fx, fx, w / 2, h / 2, w, h))
+        t = rng.integers(0, 256, h * w * 4, dtype=np.uint8)
+        t[3::4] = 255
+        targets.append(t)
+    pos, sc, rot_, op, sh = make_scene(n)
+    cloud = splat.GaussianCloud(DEGREE, pos, sc, rot_, op, sh)
+    rates = splat.LearningRates()
+    out = {"metric": "train views/s, 8 uneven views per step", "unit": "views/s",
+           "config": {"workload": f"{n} Gaussians, SH degree 3 (BF16 above DC), 8 views "
+                                  + ", ".join(f"{w}x{h}" for w, h in sizes)
+                                  + ", random poses on a sphere of radius 4-8, 60 deg horizontal fov (synthetic)"},
+           "steps": args.steps, "warmup": args.warmup}
+    opts = chosen_options(splat)
+    opts.sort_form = splat.SORT_TILE_DEPTH_64
+    trainer = splat.Trainer(cloud, opts)
+    for _ in range(args.warmup):
+        stats = trainer.step_batch(cams, targets, rates)
+    ms = time_steps(torch, trainer, lambda i: trainer.step_batch(cams, targets, rates), args.steps, trainer.stream())
+    out["batched"] = {"views_per_s": 1000.0 * args.steps * len(cams) / ms, "ms_per_step": ms / args.steps,
+                      "tile_entries": stats[0].tile_entries}  # every view's stats carry the batch's total
+    del trainer
+    torch.cuda.empty_cache()
+    single = splat.Trainer(cloud, chosen_options(splat))
+    for i in range(args.warmup * len(cams)):
+        single.step(cams[i % len(cams)], targets[i % len(cams)], rates)
+    k = len(cams)
+    ms1 = time_steps(torch, single, lambda i: single.step(cams[i % k], targets[i % k], rates,
+                                                          next_target=targets[(i + 1) % k]),
+                     args.steps * k, single.stream())
+    out["one_view_per_step"] = {"views_per_s": 1000.0 * args.steps * k / ms1, "ms_per_view": ms1 / (args.steps * k)}
+    out["value"] = out["batched"]["views_per_s"]
+    print(json.dumps(out))
+
+
 def our_arm(args) -> None:
     import torch
 
@@ -581,9 +642,9 @@ def main() -> None:
     parser.add_argument("--steps", type=int, default=30)
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    parser.add_argument("--workload", choices=["step", "memory-adjoint"], default="step",
+    parser.add_argument("--workload", choices=["step", "memory-adjoint", "batched"], default="step",
                         help="step: the headline one-view training step; memory-adjoint: 6M Gaussians at 3840x2160, "
-                             "recompute vs store-everything backward")
+                             "recompute vs store-everything backward; batched: 3M Gaussians, 8 uneven views per step")
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
@@ -597,6 +658,8 @@ def main() -> None:
     args = parser.parse_args()
     if args.workload == "memory-adjoint":
         memory_adjoint_workload(args)
+    elif args.workload == "batched":
+        batched_workload(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:

@@ -484,3 +484,36 @@ def test_blend_lists_match_recompute(splat, oracle, exact):
     assert out[0][1].loss == out[1][1].loss
     for name in ("positions", "scales", "rotations", "opacities", "sh"):
         check_close(getattr(out[1][2], name), getattr(out[0][2], name), name, 0.99999, 1e-3)
+
+
+def test_batched_step_sums_the_views(splat, oracle):
+    # Several views in one step (uneven sizes, 64-bit tile|depth keys): each
+    # view's loss equals its single-view loss, and the first Adam step moves
+    # every parameter by -lr * sign(sum over views of its gradient).
+    base = oracle.train_camera(96, 72)
+    views = [base,
+             oracle.View(base.view, base.position, 50.0, 50.0, 40.0, 30.0, 80, 60),
+             oracle.View(base.view, base.position, 70.0, 70.0, 56.0, 40.0, 112, 80)]
+    targets = [oracle.smooth_target(v.width, v.height, 60 + i) for i, v in enumerate(views)]
+    cloud = oracle.random_cloud(600, 1, 61)
+    opts = dict(force_fixed_point=True, sort_form=splat.SORT_TILE_DEPTH_64, sh_storage=splat.SH_F32,
+                state_storage=splat.STATE_F32)
+    single = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(**opts))
+    losses, total = [], None
+    for v, t in zip(views, targets):
+        losses.append(single.compute_gradients(to_camera(v), t).loss)
+        g = single.gradients()
+        parts = [np.asarray(getattr(g, name), np.float64) for name in ("positions", "opacities", "sh")]
+        total = parts if total is None else [a + b for a, b in zip(total, parts)]
+    rates = splat.LearningRates(position=1e-3, opacity=0.05, sh=0.02, sh_rest_scale=1.0)
+    batch = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(**opts, use_graph=True))
+    stats = batch.step_batch([to_camera(v) for v in views], targets, rates)
+    for s, l in zip(stats, losses):
+        assert abs(s.loss - l) < 1e-6
+    after = batch.cloud()
+    for name, g, lr in zip(("positions", "opacities", "sh"), total, (1e-3, 0.05, 0.02)):
+        before = np.asarray(getattr(cloud, name), np.float64)
+        moved = np.asarray(getattr(after, name), np.float64) - before
+        clear = np.abs(g) > 1e-3 * np.max(np.abs(g))
+        assert clear.sum() > 50, name
+        np.testing.assert_allclose(moved[clear], -lr * np.sign(g[clear]), rtol=1e-3, atol=1e-6, err_msg=name)
