@@ -214,7 +214,9 @@ int splat_trainer_reset_densify_stats(splat_trainer *trainer);
 int splat_trainer_reset_opacity(splat_trainer *trainer, float maximum);
 /* Trainer::apply_changes (trainer.cpp:749-787): replaces the Gaussians by
  * `cloud`; source[i] is the old index whose optimiser state Gaussian i keeps,
- * or -1 for a new one. */
+ * or -1 for a new one (fresh, zero state); an index past the old count is
+ * SPLAT_ERR_INVALID. The state is gathered on the GPU (train_gather.comp);
+ * the old trainer's other buffers are freed before the new ones are made. */
 int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud, const int32_t *source);
 
 /* Trainer::gaussian_count, sh_degree, active_sh_degree, uses_fixed_point,
@@ -260,7 +262,10 @@ int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint6
  * pixel), 9 raw sums (16 words per Gaussian: int32 fixed point or float),
  * 10 counters (visible, total entries, used entries, 0), 11 loss partials
  * (2 floats per tile), 12 error word, 13 blended splats per pixel (u32; with
- * blend_lists only, else empty). Copies min(bytes, size) bytes; *size gets the
+ * blend_lists only, else empty), 14-18 the Adam state of parameter groups 0-4
+ * (positions, scales, rotations, opacities, SH; u32 words: BF16 pairs, or FP32
+ * m values then v values; SH state in planes of the Gaussian count rounded up
+ * to 128). Copies min(bytes, size) bytes; *size gets the
  * buffer's size in bytes. */
 int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size);
 

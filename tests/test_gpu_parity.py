@@ -517,3 +517,39 @@ def test_batched_step_sums_the_views(splat, oracle):
         clear = np.abs(g) > 1e-3 * np.max(np.abs(g))
         assert clear.sum() > 50, name
         np.testing.assert_allclose(moved[clear], -lr * np.sign(g[clear]), rtol=1e-3, atol=1e-6, err_msg=name)
+
+
+@pytest.mark.parametrize("state", ["STATE_BF16_PAIR", "STATE_F32"])
+def test_apply_changes_gathers_the_state(splat, oracle, state):
+    # Densification keeps the survivors' Adam moments (gathered on the GPU
+    # through the source table), starts new Gaussians at zero, and takes the
+    # parameters from the new cloud.
+    view = oracle.train_camera(96, 80)
+    target = oracle.smooth_target(96, 80, 3)
+    cloud = oracle.random_cloud(500, 2, 71)
+    rates = splat.LearningRates(position=1e-3)
+    t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(state_storage=getattr(splat, state)))
+    for _ in range(3):
+        t.step(to_camera(view), target, rates)
+    old = [t.debug_download(splat.DEBUG_STATE + g, np.uint32) for g in range(5)]
+    source = np.array(list(range(0, 500, 2)) + [-1] * 30 + list(range(499, 300, -3)), np.int32)
+    new_n = source.size
+    fresh = oracle.random_cloud(new_n, 2, 72)
+    t.apply_changes(to_cloud(fresh), source)
+    np.testing.assert_array_equal(t.cloud().positions, fresh.positions)
+    new = [t.debug_download(splat.DEBUG_STATE + g, np.uint32) for g in range(5)]
+    copies = 2 if state == "STATE_F32" else 1
+    kept = source >= 0
+    for g, stride in enumerate((3, 3, 4, 1)):
+        o = old[g][: copies * 500 * stride].reshape(copies, 500, stride)
+        n = new[g][: copies * new_n * stride].reshape(copies, new_n, stride)
+        np.testing.assert_array_equal(n[:, kept], o[:, source[kept]])
+        assert not n[:, ~kept].any()
+    planes = 3 * 9 * copies
+    old_ps, new_ps = 512, ((new_n + 127) // 128) * 128
+    o = old[4][: planes * old_ps].reshape(planes, old_ps)
+    n = new[4][: planes * new_ps].reshape(planes, new_ps)
+    np.testing.assert_array_equal(n[:, :new_n][:, kept], o[:, source[kept]])
+    assert not n[:, :new_n][:, ~kept].any()
+    assert np.any(o[:, source[kept]])
+    assert np.isfinite(t.step(to_camera(view), target, rates).loss)

@@ -408,6 +408,7 @@ class DensifyStats:
 DEBUG_SPLATS, DEBUG_REACH, DEBUG_DEPTH_KEYS, DEBUG_ENTRY_KEYS, DEBUG_ENTRY_VALUES, DEBUG_RANGES = range(6)
 DEBUG_IMAGE, DEBUG_STOPS, DEBUG_ADJOINT, DEBUG_RAW, DEBUG_COUNTERS, DEBUG_PARTIALS, DEBUG_ERROR = range(6, 13)
 DEBUG_BLEND_COUNTS = 13
+DEBUG_STATE = 14  # + parameter group 0..4
 
 
 def _target_ptr(target) -> tuple:

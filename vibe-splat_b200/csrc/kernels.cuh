@@ -158,4 +158,14 @@ void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, 
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad,
                   float *densifyStats, uint32_t *error, cudaStream_t stream);
 
+// train_gather.comp: optimiser state of the new Gaussians from the old ones
+// through a source table (negative: fresh, zero state). Rows: `stride` words
+// per Gaussian, `copies` consecutive copies of the layout (2 for F32 m and v).
+// Planes: `planes` planes of one word per Gaussian, newStride / oldStride apart.
+void launch_gather_rows(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t oldCount,
+                        uint32_t stride, uint32_t copies, cudaStream_t stream);
+void launch_gather_planes(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t newStride,
+                          uint32_t oldStride, uint32_t planes, cudaStream_t stream);
+
 } // namespace sb
+

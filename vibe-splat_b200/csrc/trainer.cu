@@ -210,6 +210,7 @@ public:
   void begin(int stage);
   void end(int stage);
   void clear_graphs();
+  void release_transient();
   std::string graph_key(ChainMode mode, bool statistics) const;
   void run(const splat_camera *cameras, const uint8_t *const *targets, const size_t *bytes, int count, ChainMode mode,
            const splat_learning_rates *rates, bool statistics, splat_step_stats *stats, bool deviceTargets = false);
@@ -329,6 +330,20 @@ Trainer::~Trainer() {
   for (auto &e : events)
     if (e != nullptr) cudaEventDestroy(e);
   if (stream != nullptr) cudaStreamDestroy(stream);
+}
+
+// Frees every device buffer except the optimiser state (densification keeps
+// only that from the old Gaussians).
+void Trainer::release_transient() {
+  clear_graphs();
+  for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities, &shDc, &shRest, &grads[0], &grads[1], &grads[2], &grads[3],
+                          &grads[4], &densifyStats, &splats, &reach, &depthKeys, &values, &tmpKeys, &tmpValues, &offsets, &raw,
+                          &shGrad, &entryKeys, &entryValues, &tmpEntryKeys, &tmpEntryValues, &image, &stops, &adjoint, &fields,
+                          &target, &ranges, &partials, &listCounts, &listOffsets, &listPool, &listScratch, &sortScratchDepth,
+                          &sortScratchEntries, &scanScratch})
+    b->release();
+  entryCapacity = 0;
+  viewSlots = 0;
 }
 
 void Trainer::clear_graphs() {
@@ -1272,45 +1287,36 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
     if (cloud == nullptr || source == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
     if (cloud->count <= 0) throw Failure{SPLAT_ERR_INVALID, "densification removed every Gaussian"};
     if (cloud->sh_degree != t->shDegree) throw Failure{SPLAT_ERR_INVALID, "the SH degree cannot change"};
-    SB_CUDA(cudaStreamSynchronize(t->stream));
-    // The survivors keep their optimiser state: gathered on the host here (the
-    // GPU gather of train_gather.comp is the next component to build).
     const size_t oldN = t->n, newN = (size_t)cloud->count;
-    const int floats = 3 * t->shCoeffs;
-    const size_t wordBytes = t->stateStore == sb::StateStore::F32 ? 8 : 4;
-    std::vector<std::vector<uint8_t>> moved(5);
-    const size_t strides[5] = {3, 3, 4, 1, (size_t)floats};
-    // SH state planes are planeStride (n rounded up to kPlaneAlign) apart.
-    const size_t oldPlanes = t->planeStride;
-    const size_t newPlanes = ((newN + sb::kPlaneAlign - 1) / sb::kPlaneAlign) * sb::kPlaneAlign;
-    for (int g = 0; g < 5; ++g) {
-      const size_t oldCount = (g == 4 ? oldPlanes : oldN) * strides[g], newCount = (g == 4 ? newPlanes : newN) * strides[g];
-      std::vector<uint8_t> old(oldCount * wordBytes);
-      SB_CUDA(cudaMemcpy(old.data(), t->state[g].get(), old.size(), cudaMemcpyDeviceToHost));
-      moved[g].assign(newCount * wordBytes, 0);
-      for (size_t i = 0; i < newN; ++i) {
-        const int32_t s = source[i];
-        if (s < 0 || (size_t)s >= oldN) continue;
-        for (size_t a = 0; a < strides[g]; ++a) {
-          // State index of element a of Gaussian i: AoS for groups 0-3, planes for SH.
-          const size_t from = g == 4 ? a * oldPlanes + (size_t)s : (size_t)s * strides[g] + a;
-          const size_t to = g == 4 ? a * newPlanes + i : i * strides[g] + a;
-          if (wordBytes == 8) {
-            std::memcpy(&moved[g][to * 4], &old[from * 4], 4);
-            std::memcpy(&moved[g][(newCount + to) * 4], &old[(oldCount + from) * 4], 4);
-          } else {
-            std::memcpy(&moved[g][to * 4], &old[from * 4], 4);
-          }
-        }
-      }
-    }
-    splat_trainer_options o = t->opt;
-    const uint32_t step = t->adamStep;
-    const int active = t->activeDegree;
+    for (size_t i = 0; i < newN; ++i)
+      if (source[i] >= (int64_t)oldN) throw Failure{SPLAT_ERR_INVALID, "a source index is past the old Gaussians"};
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    // The survivors keep their optimiser state, gathered on the GPU through the
+    // source table (train_gather.comp) so that the moments never cross to the
+    // host. Everything else the old trainer holds is freed first, for the
+    // sake of the budget; the new trainer starts from the new cloud.
+    t->release_transient();
+    const splat_trainer_options o = t->opt;
     Trainer *fresh = new Trainer(*cloud, o);
-    fresh->adamStep = step;
-    fresh->activeDegree = active;
-    for (int g = 0; g < 5; ++g) SB_CUDA(cudaMemcpy(fresh->state[g].get(), moved[g].data(), moved[g].size(), cudaMemcpyHostToDevice));
+    fresh->adamStep = t->adamStep;
+    fresh->activeDegree = t->activeDegree;
+    try {
+      sb::DeviceBuffer table;
+      table.ensure(newN * sizeof(int32_t));
+      SB_CUDA(cudaMemcpyAsync(table.get(), source, newN * sizeof(int32_t), cudaMemcpyHostToDevice, fresh->stream));
+      const uint32_t copies = t->stateStore == sb::StateStore::F32 ? 2u : 1u;
+      const uint32_t strides[4] = {3, 3, 4, 1};
+      for (int g = 0; g < 4; ++g)
+        sb::launch_gather_rows(table.get<int32_t>(), t->state[g].get<uint32_t>(), fresh->state[g].get<uint32_t>(), (uint32_t)newN,
+                               (uint32_t)oldN, strides[g], copies, fresh->stream);
+      sb::launch_gather_planes(table.get<int32_t>(), t->state[4].get<uint32_t>(), fresh->state[4].get<uint32_t>(), (uint32_t)newN,
+                               fresh->planeStride, t->planeStride, 3u * (uint32_t)t->shCoeffs * copies, fresh->stream);
+      SB_CUDA(cudaGetLastError());
+      SB_CUDA(cudaStreamSynchronize(fresh->stream));
+    } catch (...) {
+      delete fresh;
+      throw;
+    }
     delete t;
     trainer->impl = fresh;
   });
@@ -1403,6 +1409,7 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     case 11: src = t->partials.get(); have = (size_t)t->views.totalTiles * 8; break;
     case 12: src = &rb->error; have = 4; break;
     case 13: src = t->listCounts.get(); have = t->blendLists ? (size_t)t->views.totalPixels * 4 : 0; break;
+    case 14: case 15: case 16: case 17: case 18: src = t->state[which - 14].get(); have = t->state[which - 14].bytes(); break;
     default: throw Failure{SPLAT_ERR_INVALID, "unknown buffer"};
     }
     if (size) *size = have;
