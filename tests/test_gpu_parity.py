@@ -553,3 +553,56 @@ def test_apply_changes_gathers_the_state(splat, oracle, state):
     assert not n[:, :new_n][:, ~kept].any()
     assert np.any(o[:, source[kept]])
     assert np.isfinite(t.step(to_camera(view), target, rates).loss)
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+def test_gradients_against_central_differences(splat, oracle, fixed):
+    # The adjoint against FP64 central differences of the twin's loss (h = 1e-4)
+    # on 256 randomly chosen parameters of a 20000-Gaussian, SH degree 3 scene
+    # (loss 0.8 L1 + 0.2 (1 - SSIM)); float sums against the reference's
+    # finite-difference criterion for its oracle (tests/test_train.cpp:99-112):
+    # cosine > 0.999, length within 1%.
+    import concurrent.futures
+    import os
+
+    w = h = 256
+    view = oracle.train_camera(w, h)
+    target = oracle.smooth_target(w, h, 91)
+    cloud = oracle.random_cloud(20000, 3, 93)
+    trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=fixed, sh_storage=splat.SH_F32))
+    trainer.compute_gradients(to_camera(view), target)
+    g = trainer.gradients()
+    names = ("positions", "scales", "rotations", "opacities", "sh")
+    rng = np.random.default_rng(95)
+    picks = []
+    for _ in range(256):
+        name = names[rng.integers(0, len(names))]
+        picks.append((name, int(rng.integers(0, getattr(cloud, name).size))))
+
+    def loss_at(name, index, delta):
+        c = cloud.copy()
+        arr = getattr(c, name)
+        arr[index] = np.float32(arr[index] + delta)
+        rgb, _, _ = oracle.ref_render(c, view)
+        return oracle.ref_loss(rgb, w, h, target, 0.2)[0], float(arr[index])
+
+    def central(pick, step):
+        name, index = pick
+        (lp, xp), (lm, xm) = loss_at(name, index, step), loss_at(name, index, -step)
+        return (lp - lm) / (xp - xm)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, len(os.sched_getaffinity(0)))) as pool:
+        fd = np.array(list(pool.map(lambda p: central(p, 1e-4), picks)))
+        fd_half = np.array(list(pool.map(lambda p: central(p, 5e-5), picks)))
+    # The loss jumps where a perturbation crosses a cutoff (alpha >= 1/255, the
+    # stop threshold, a tile edge); the reference checks its FP64 twin against
+    # differences with the cutoffs switched off. The kernels keep them, so the
+    # parameters whose differences at h and h/2 disagree by more than 1% (not
+    # locally smooth) are left out; most are kept.
+    smooth = np.abs(fd - fd_half) <= 0.01 * np.maximum(np.abs(fd), 1e-3 * np.max(np.abs(fd)))
+    print(f"  {smooth.sum()} of {len(picks)} parameters locally smooth")
+    assert smooth.sum() >= 200
+    ours = np.array([float(getattr(g, name)[index]) for name, index in picks])
+    # Fixed point: the reference's tolerance for its quantised sums (cosine > 0.97, 10%).
+    cos, ratio = (0.97, 0.1) if fixed else (0.999, 0.01)
+    check_close(ours[smooth], fd[smooth], "parameters vs central differences", cos, ratio)
