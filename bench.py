@@ -270,18 +270,22 @@ def stage_bytes(n: int, visible: int, entries: int, pixels: int, depth_passes: i
     }
 
 
-def measured_traffic(stage: str):
-    """DRAM bytes per launch of the stage's kernel from the committed ncu
-    summary of the bench workload (profiles/*.md, a line 'traffic <stage>: N'),
-    or None."""
+def profile_figure(kind: str, stage: str):
+    """A per-launch figure of the stage's kernel from the committed ncu summary
+    of the bench workload (profiles/*.md, a line '<kind> <stage>: N'): kind
+    'traffic' for DRAM bytes, 'instructions' for warp-instructions. Or None."""
     for path in sorted((ROOT / "profiles").glob("*.md")):
         for line in path.read_text().splitlines():
-            if line.startswith(f"traffic {stage}:"):
+            if line.startswith(f"{kind} {stage}:"):
                 try:
                     return int(line.split(":", 1)[1].strip().split()[0])
                 except ValueError:
                     return None
     return None
+
+
+def measured_traffic(stage: str):
+    return profile_figure("traffic", stage)
 
 
 def chosen_options(splat):
@@ -547,6 +551,10 @@ def our_arm(args) -> None:
     digits_used = tuned.get("digit_bits", chosen.digit_bits)
     depth_passes = math.ceil(32 / digits_used)
     algorithmic = stage_bytes(n, visible, entries, pixels, depth_passes)
+    # The SM issue rate: 148 SMs x 4 warp-instructions per clock, at the SM
+    # clock sampled during the timed steps (the maximum if none was sampled).
+    sm_mhz = (clocks.get("sm_mhz") if isinstance(clocks, dict) else None) or 1965.0
+    issue_peak = 148 * 4 * sm_mhz * 1e6
     stage_roof = {}
     for name, ms_stage in stages.items():
         b = algorithmic.get(name)
@@ -554,6 +562,11 @@ def our_arm(args) -> None:
             continue
         gbs = b / (ms_stage * 1e-3) / 1e9
         stage_roof[name] = {"bytes": b, "ms": ms_stage, "GB/s": gbs, "frac": gbs / hbm_peak}
+        inst = profile_figure("instructions", name)
+        if inst:
+            rate = inst / (ms_stage * 1e-3)
+            stage_roof[name]["issue"] = {"warp_inst_per_s": rate, "peak": issue_peak, "frac": rate / issue_peak,
+                                         "instructions": inst}
     roof = None
     if dominant is not None and dominant in stage_roof:
         r = stage_roof[dominant]
@@ -562,8 +575,11 @@ def our_arm(args) -> None:
                 "frac": r["frac"], "traffic": traffic, "ms": r["ms"],
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
         if dominant in ("backward", "composite"):
-            roof["note"] = ("issue-bound, not HBM-bound: the FP32/ALU issue rate is the limit (ncu summary under "
-                            "profiles/); the HBM fraction is given for the record")
+            roof["note"] = ("issue-bound, not HBM-bound: the SM instruction issue rate is the limit; 'issue' gives "
+                            "the kernel's warp-instructions (ncu, profiles/) over its live time against 148 SMs x 4 "
+                            "per clock; the HBM fraction is given for the record")
+            if "issue" in r:
+                roof["issue"] = r["issue"]
 
     plain = None
     if not args.no_plain:
