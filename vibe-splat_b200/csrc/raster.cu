@@ -141,7 +141,8 @@ __device__ __forceinline__ Staged stage_checked(const Splat *__restrict__ splats
 // staging warp calls this (mask 0 for lanes without a splat); warps of the
 // 1-pixel layout cover two rows of 16, those of the 2-pixel layout 8x8.
 template <int WARPS>
-__device__ __forceinline__ void publish_cover(uint32_t mask, uint32_t word, uint32_t lane, uint32_t (*cover)[kBatch / 32]) {
+__device__ __forceinline__ void publish_cover(uint32_t mask, uint32_t word, uint32_t lane, uint32_t (*cover)[kBatch / 32],
+                                              uint32_t warpsMet = 0xFFFFFFFFu) {
   uint32_t mine = 0;
 #pragma unroll
   for (int w = 0; w < WARPS; ++w) {
@@ -153,7 +154,7 @@ __device__ __forceinline__ void publish_cover(uint32_t mask, uint32_t word, uint
       cols = 0xFFu << (8 * (w & 1));
       rows = 0xFFu << (16 + 8 * (w >> 1));
     }
-    const uint32_t b = __ballot_sync(0xFFFFFFFFu, (mask & cols) != 0u && (mask & rows) != 0u);
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, (mask & cols) != 0u && (mask & rows) != 0u && ((warpsMet >> w) & 1u) != 0u);
     if (lane == (uint32_t)w) mine = b;
   }
   if (lane < (uint32_t)WARPS) cover[lane][word] = mine;
@@ -550,8 +551,31 @@ __device__ __forceinline__ PixelPair pixel_pair(const TileGeometry &geo, const V
   return pp;
 }
 
+// Whether the cutoff ellipse {d : d' Q d <= reach} (Q = [qx qy; qy qz], the
+// splat's conic) may reach a pixel centre of [lowX, highX] x [lowY, highY]
+// (offsets from the splat's centre): the least of the quadratic over the
+// rectangle lies on an edge, at the ellipse's tangent point clamped to it; the
+// binning's margin covers the rounding of these SFU divisions. A warp whose
+// pixel block fails it has no pixel with alpha >= 1/255 for that splat.
+__device__ __forceinline__ bool ellipse_meets_rect(float qx, float qy, float qz, float reach, float lowX, float highX, float lowY,
+                                                   float highY) {
+  if (lowX <= 0.0f && lowY <= 0.0f && highX >= 0.0f && highY >= 0.0f) return true;
+  float least = 1e30f;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const float x = side == 0 ? lowX : highX;
+    const float y = fminf(fmaxf(__fdividef(-qy * x, qz), lowY), highY);
+    least = fminf(least, qx * x * x + 2.0f * qy * x * y + qz * y * y);
+    const float v = side == 0 ? lowY : highY;
+    const float u = fminf(fmaxf(__fdividef(-qy * v, qx), lowX), highX);
+    least = fminf(least, qx * u * u + 2.0f * qy * u * v + qz * v * v);
+  }
+  return least <= reach * 1.001f + 1e-3f;
+}
+
 // Stages `count` splats with 128 threads, two rounds, and publishes the
-// 8x8-block bitmaps.
+// 8x8-block bitmaps: a block is listed when the splat's masks reach it and its
+// cutoff ellipse meets the block's pixel centres.
 template <class M>
 __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, const uint32_t *__restrict__ values, uint32_t count,
                                             uint32_t splatLimit, const TileGeometry &geo, uint32_t *error, Staged *batch,
@@ -560,13 +584,23 @@ __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, co
 #pragma unroll
   for (uint32_t round = 0; round < kBatch / kHalfTile; ++round) {
     const uint32_t j = round * kHalfTile + t;
-    uint32_t mask = 0u;
+    uint32_t mask = 0u, met = 0u;
     if (j < count) {
       const Staged st = stage_checked<M>(splats, values[j], splatLimit, geo, error);
       batch[j] = st;
       mask = st.mask;
+      if (mask != 0u) {
+        // 2 ln(255 opacity): alpha >= 1/255 exactly where d' Q d <= reach.
+        const float reach = 2.0f * __logf(255.0f * st.opacity);
+#pragma unroll
+        for (uint32_t w = 0; w < kHalfTile / 32; ++w) {
+          const float lowX = ((float)(geo.x0 + (w & 1u) * 8u) + 0.5f) - st.cx;
+          const float lowY = ((float)(geo.y0 + (w >> 1) * 8u) + 0.5f) - st.cy;
+          if (ellipse_meets_rect(st.qx, st.qy, st.qz, reach, lowX, lowX + 7.0f, lowY, lowY + 7.0f)) met |= 1u << w;
+        }
+      }
     }
-    publish_cover<kHalfTile / 32>(mask, round * (kHalfTile / 32) + warp, lane, cover);
+    publish_cover<kHalfTile / 32>(mask, round * (kHalfTile / 32) + warp, lane, cover, met);
   }
 }
 
