@@ -140,16 +140,24 @@ __device__ __forceinline__ Staged stage_checked(const Splat *__restrict__ splats
 // one no lane would have taken, so nothing else changes. Every lane of the
 // staging warp calls this (mask 0 for lanes without a splat); warps of the
 // 1-pixel layout cover two rows of 16, those of the 2-pixel layout 8x8.
-template <int WARPS>
+// Warp shapes: kStrips, 8 warps of two rows of 16 (the reference's groups);
+// kBlocks8x4, 8 warps of 8 columns by 4 rows; kBlocks8x8, 4 warps of 8x8.
+enum WarpShape { kStrips = 0, kBlocks8x4 = 1, kBlocks8x8 = 2 };
+
+template <int SHAPE>
 __device__ __forceinline__ void publish_cover(uint32_t mask, uint32_t word, uint32_t lane, uint32_t (*cover)[kBatch / 32],
                                               uint32_t warpsMet = 0xFFFFFFFFu) {
+  constexpr int WARPS = SHAPE == kBlocks8x8 ? 4 : 8;
   uint32_t mine = 0;
 #pragma unroll
   for (int w = 0; w < WARPS; ++w) {
     uint32_t cols, rows;
-    if (WARPS == 8) {
+    if (SHAPE == kStrips) {
       cols = 0xFFFFu;
       rows = 3u << (16 + 2 * w);
+    } else if (SHAPE == kBlocks8x4) {
+      cols = 0xFFu << (8 * (w & 1));
+      rows = 0xFu << (16 + 4 * (w >> 1));
     } else {
       cols = 0xFFu << (8 * (w & 1));
       rows = 0xFFu << (16 + 8 * (w >> 1));
@@ -176,7 +184,11 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
   const int tile = blockIdx.x;
   const TileGeometry geo = tile_geometry(views, tile);
   const ViewParams &cam = views.v[geo.view];
-  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5, lx = t & 15u, ly = t >> 4;
+  // Compositing needs no particular grouping of pixels into warps: warp w
+  // takes the 8x4 block (w & 1, w >> 1), lane l its pixel (l & 7, l >> 3), a
+  // shape that meets fewer splats than a strip of two rows.
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint32_t lx = (warp & 1u) * 8u + (lane & 7u), ly = (warp >> 1) * 4u + (lane >> 3);
   const uint32_t x = geo.x0 + lx, y = geo.y0 + ly;
   const bool inside = x < (uint32_t)cam.width && y < (uint32_t)cam.height;
   const uint32_t myBits = (1u << lx) | (1u << (16 + ly));
@@ -200,7 +212,7 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
       s_batch[t] = st;
       stagedMask = st.mask;
     }
-    publish_cover<kTilePixels / 32>(stagedMask, warp, lane, s_cover);
+    publish_cover<kBlocks8x4>(stagedMask, warp, lane, s_cover);
     __syncthreads();
     // Back to front within the batch: the highest index first.
     for (int word = (int)((count - 1u) >> 5); word >= 0 && !done; --word) {
@@ -326,7 +338,7 @@ __global__ void __launch_bounds__(kTilePixels, 4)
       s_batch[t] = st;
       stagedMask = st.mask;
     }
-    publish_cover<kTilePixels / 32>(stagedMask, warp, lane, s_cover);
+    publish_cover<kStrips>(stagedMask, warp, lane, s_cover);
     __syncthreads();
     // Front to back: the lowest index first. The walk is warp-uniform.
     for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
@@ -460,7 +472,7 @@ __global__ void __launch_bounds__(kTilePixels, 4)
       s_batch[t] = st;
       stagedMask = st.mask;
     }
-    publish_cover<kTilePixels / 32>(stagedMask, warp, lane, s_cover);
+    publish_cover<kStrips>(stagedMask, warp, lane, s_cover);
     __syncthreads();
     for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
     for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
@@ -600,12 +612,12 @@ __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, co
         }
       }
     }
-    publish_cover<kHalfTile / 32>(mask, round * (kHalfTile / 32) + warp, lane, cover, met);
+    publish_cover<kBlocks8x8>(mask, round * (kHalfTile / 32) + warp, lane, cover, met);
   }
 }
 
 template <class M>
-__global__ void __launch_bounds__(kHalfTile) k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
+__global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
                                                         const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
                                                         float bgR, float bgG, float bgB, float4 *__restrict__ image,
                                                         uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
