@@ -630,7 +630,7 @@ template <ShStore S> __device__ __forceinline__ float staged_sh_rest(const unsig
   }
 }
 
-template <ShStore S, bool FIXED>
+template <ShStore S, StateStore ST, bool FIXED>
 __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const ViewSet *__restrict__ viewsPtr,
                                                                 const void *__restrict__ rawIn, const Splat *__restrict__ splats,
                                                                 const ChainArgs *__restrict__ argsPtr, OptimState state,
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   const uint32_t n = p.n, ps = p.planeStride, tid = threadIdx.x;
   const uint32_t i0 = blockIdx.x * kStepThreads, i = i0 + tid;
   const uint32_t planes = 3u * (uint32_t)p.shCoeffs, restPlanes = planes - 3u;
-  const bool stateF32 = state.store == StateStore::F32;
+  constexpr bool stateF32 = ST == StateStore::F32;
   float *s_dc = reinterpret_cast<float *>(s_stage);
   unsigned char *s_rest = s_stage + 3u * kStepThreads * 4u;
   unsigned char *s_state = s_rest + restPlanes * kStepThreads * kShBytes;
@@ -721,8 +721,6 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
     chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
   }
 
-  // The SH step, from the staged planes, with the direction term from the
-  // coefficients before it.
   if (!bulk_wait(&s_bar, 0, kStageSpinLimit)) {
     // Never leave with a copy still landing in this block's shared memory.
     atomicOr(error, kErrLookbackTimeout);
@@ -730,67 +728,22 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   }
   const bool stepZeros = !args.selective;
   const int active = touched ? cam.activeCoeffs : 0;
-  float gDir[3] = {0.f, 0.f, 0.f};
-  if (touched || stepZeros) {
-    const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
-    const uint32_t count = ps * shFloats;
-    const float *s_statef = reinterpret_cast<const float *>(s_state);
-    const uint32_t *s_statew = reinterpret_cast<const uint32_t *>(s_state);
-    // The direction term first, unrolled (its basis gradients fold per
-    // coefficient), from the staged values; then the step, one coefficient
-    // per trip of a rolled loop: unrolled, the step's code overflows the
-    // instruction cache.
-    if (touched && cam.activeDegree > 0) {
+  // The direction term, unrolled (its basis gradients fold per coefficient),
+  // from the staged coefficients before any step.
+  if (touched && cam.activeDegree > 0) {
+    float gDir[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-      for (int k = 1; k < kMaxCoeffs; ++k) {
-        if (k >= active) break;
-        const uint32_t r = (uint32_t)(k - 1) * 3u;
-        const float value[3] = {staged_sh_rest<S>(s_rest, r * kStepThreads + tid),
-                                staged_sh_rest<S>(s_rest, (r + 1u) * kStepThreads + tid),
-                                staged_sh_rest<S>(s_rest, (r + 2u) * kStepThreads + tid)};
-        direction_term(k, value, gColour, dir, gDir);
-      }
+    for (int k = 1; k < kMaxCoeffs; ++k) {
+      if (k >= active) break;
+      const uint32_t r = (uint32_t)(k - 1) * 3u;
+      const float value[3] = {staged_sh_rest<S>(s_rest, r * kStepThreads + tid),
+                              staged_sh_rest<S>(s_rest, (r + 1u) * kStepThreads + tid),
+                              staged_sh_rest<S>(s_rest, (r + 2u) * kStepThreads + tid)};
+      direction_term(k, value, gColour, dir, gDir);
     }
-#pragma unroll 1
-    for (int k = 0; k < p.shCoeffs; ++k) {
-      float value[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const uint32_t plane = (uint32_t)(k * 3 + c);
-        value[c] = k == 0 ? s_dc[c * kStepThreads + tid] : staged_sh_rest<S>(s_rest, (plane - 3u) * kStepThreads + tid);
-      }
-      const float b = k < active ? basis_one(k, dir[0], dir[1], dir[2]) : 0.0f;
-      const float rate = k == 0 ? args.rates[4] : args.rates[4] * args.restScale;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float g = k < active ? fmaf(b, gColour[c], 0.0f) : 0.0f;
-        if (g == 0.0f && !stepZeros) continue;
-        const uint32_t plane = (uint32_t)(k * 3 + c);
-        const uint32_t t = plane * ps + i;
-        const uint32_t hashIndex = (i * shFloats + plane) * 5u + 4u;
-        float m, v;
-        uint32_t word = 0u;
-        if (stateF32) {
-          m = s_statef[plane * kStepThreads + tid];
-          v = s_statef[(planes + plane) * kStepThreads + tid];
-        } else {
-          word = s_statew[plane * kStepThreads + tid];
-          m = bf16_load(word, 0);
-          v = bf16_load(word, 1);
-        }
-        float val = value[c];
-        adam(val, m, v, g, rate, a);
-        store_state(state.state[4], state.store, count, t, m, v, word, hashIndex, a.seed);
-        if (k == 0) {
-          p.shDc[t] = val;
-        } else {
-          store_sh_rest<S>(p.shRest, t - 3u * ps, val, hashIndex, args.seed);
-        }
-      }
-    }
+    add_direction_term(gDir, dir, distance, gPv);
   }
   if (touched) {
-    if (cam.activeDegree > 0) add_direction_term(gDir, dir, distance, gPv);
 #pragma unroll
     for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
   }
@@ -801,35 +754,87 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
     gOpacity += args.opacityReg * opacity * (1.0f - opacity);
   }
 
-  // Adam on the 11 geometry elements: [positions 3 | scales 3 | rotations 4 | opacity 1].
-  float gv[11], value[11], m[11], vv[11];
-  uint32_t word[11];
+  // Adam on the 11 geometry elements: [positions 3 | scales 3 | rotations 4 |
+  // opacity 1], before the SH step so that none of it stays live through the
+  // SH loop.
+  {
+    float gv[11], value[11], m[11], vv[11];
+    uint32_t word[11];
 #pragma unroll
-  for (int e = 0; e < 11; ++e) {
-    const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
-    const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
-    const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
-    const uint32_t idx = i * per + (uint32_t)a0;
-    gv[e] = group == 0 ? gP[a0] : group == 1 ? gScale[a0] : group == 2 ? gRot[a0] : gOpacity;
-    value[e] = group == 0 ? pos[a0] : group == 1 ? logScale[a0] : group == 3 ? rawOpacity
-             : a0 == 0 ? rq.x : a0 == 1 ? rq.y : a0 == 2 ? rq.z : rq.w;
-    m[e] = vv[e] = 0.0f;
-    word[e] = 0u;
-    if (gv[e] == 0.0f && args.selective) continue;
-    load_state(state.state[group], state.store, per * n, idx, m[e], vv[e], word[e]);
+    for (int e = 0; e < 11; ++e) {
+      const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+      const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+      const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+      const uint32_t idx = i * per + (uint32_t)a0;
+      gv[e] = group == 0 ? gP[a0] : group == 1 ? gScale[a0] : group == 2 ? gRot[a0] : gOpacity;
+      value[e] = group == 0 ? pos[a0] : group == 1 ? logScale[a0] : group == 3 ? rawOpacity
+               : a0 == 0 ? rq.x : a0 == 1 ? rq.y : a0 == 2 ? rq.z : rq.w;
+      m[e] = vv[e] = 0.0f;
+      word[e] = 0u;
+      if (gv[e] == 0.0f && args.selective) continue;
+      load_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e]);
+    }
+#pragma unroll
+    for (int e = 0; e < 11; ++e) {
+      const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+      const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+      const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+      const uint32_t idx = i * per + (uint32_t)a0;
+      // A parameter with a zero gradient is left alone when selective.
+      if (gv[e] == 0.0f && args.selective) continue;
+      adam(value[e], m[e], vv[e], gv[e], args.rates[group], a);
+      store_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e], idx * 5u + (uint32_t)group, a.seed);
+      float *values = group == 0 ? p.positions : group == 1 ? p.scales : group == 2 ? p.rotations : p.opacities;
+      values[idx] = value[e];
+    }
   }
+
+  // The SH step from the staged planes: the DC planes, then one coefficient of
+  // the rest per trip of a rolled loop (unrolled, the step's code overflows
+  // the instruction cache).
+  if (!(touched || stepZeros)) return;
+  const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
+  const uint32_t hashBase = i * shFloats * 5u + 4u;
+  const float *s_statef = reinterpret_cast<const float *>(s_state);
+  const uint32_t *s_statew = reinterpret_cast<const uint32_t *>(s_statef);
+  uint32_t *stateOut = static_cast<uint32_t *>(state.state[4]) + i;
+  const size_t stateCount = (size_t)ps * shFloats; // F32: the v planes follow the m planes
+  // One element: Adam from the staged state, the new state and value returned.
+  auto element = [&](uint32_t plane, float &val, float g, float rate) {
+    if constexpr (ST == StateStore::F32) {
+      float m = s_statef[plane * kStepThreads + tid], v = s_statef[(planes + plane) * kStepThreads + tid];
+      adam(val, m, v, g, rate, a);
+      reinterpret_cast<float *>(stateOut)[(size_t)plane * ps] = m;
+      reinterpret_cast<float *>(stateOut)[stateCount + (size_t)plane * ps] = v;
+    } else {
+      const uint32_t word = s_statew[plane * kStepThreads + tid];
+      float m = bf16_load(word, 0), v = bf16_load(word, 1);
+      adam(val, m, v, g, rate, a);
+      stateOut[(size_t)plane * ps] = bf16_round(m) | (bf16_stochastic(v, hashBase + plane * 5u, a.seed) << 16);
+    }
+  };
 #pragma unroll
-  for (int e = 0; e < 11; ++e) {
-    const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
-    const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
-    const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
-    const uint32_t idx = i * per + (uint32_t)a0;
-    // A parameter with a zero gradient is left alone when selective.
-    if (gv[e] == 0.0f && args.selective) continue;
-    adam(value[e], m[e], vv[e], gv[e], args.rates[group], a);
-    store_state(state.state[group], state.store, per * n, idx, m[e], vv[e], word[e], idx * 5u + (uint32_t)group, a.seed);
-    float *values = group == 0 ? p.positions : group == 1 ? p.scales : group == 2 ? p.rotations : p.opacities;
-    values[idx] = value[e];
+  for (int c = 0; c < 3; ++c) {
+    const float g = active > 0 ? fmaf(basis_one(0, dir[0], dir[1], dir[2]), gColour[c], 0.0f) : 0.0f;
+    if (g == 0.0f && !stepZeros) continue;
+    float val = s_dc[c * kStepThreads + tid];
+    element((uint32_t)c, val, g, args.rates[4]);
+    p.shDc[(size_t)c * ps + i] = val;
+  }
+  const float restRate = args.rates[4] * args.restScale;
+#pragma unroll 1
+  for (int k = 1; k < p.shCoeffs; ++k) {
+    const float b = k < active ? basis_one(k, dir[0], dir[1], dir[2]) : 0.0f;
+    const uint32_t r = (uint32_t)(k - 1) * 3u;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float g = k < active ? fmaf(b, gColour[c], 0.0f) : 0.0f;
+      if (g == 0.0f && !stepZeros) continue;
+      const uint32_t plane = r + 3u + (uint32_t)c;
+      float val = staged_sh_rest<S>(s_rest, (r + (uint32_t)c) * kStepThreads + tid);
+      element(plane, val, g, restRate);
+      store_sh_rest<S>(p.shRest, (size_t)(r + (uint32_t)c) * ps + i, val, hashBase + plane * 5u, args.seed);
+    }
   }
 }
 
@@ -845,13 +850,19 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
   if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.planeStride * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
     const uint32_t smem = step_stage_bytes(p.shCoeffs, S == ShStore::F32 ? 4 : 2, state.store == StateStore::F32);
     const uint32_t stepBlocks = div_up(p.n, kStepThreads);
+#define SB_STEP(ST, FIX)                                                                                           \
+  {                                                                                                                  \
+    cudaFuncSetAttribute(k_chain_step<S, ST, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
+    k_chain_step<S, ST, FIX><<<stepBlocks, kStepThreads, smem, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, \
+                                                                        error);                                      \
+  }
+    const bool f32 = state.store == StateStore::F32;
     if (args.fixedPoint) {
-      cudaFuncSetAttribute(k_chain_step<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_chain_step<S, true><<<stepBlocks, kStepThreads, smem, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+      if (f32) SB_STEP(StateStore::F32, true) else SB_STEP(StateStore::BF16Pair, true)
     } else {
-      cudaFuncSetAttribute(k_chain_step<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_chain_step<S, false><<<stepBlocks, kStepThreads, smem, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, error);
+      if (f32) SB_STEP(StateStore::F32, false) else SB_STEP(StateStore::BF16Pair, false)
     }
+#undef SB_STEP
     return;
   }
 #define SB_CHAIN(F, M) \
