@@ -587,11 +587,14 @@ __device__ __forceinline__ bool ellipse_meets_rect(float qx, float qy, float qz,
 
 // Stages `count` splats with 128 threads, two rounds, and publishes the
 // 8x8-block bitmaps: a block is listed when the splat's masks reach it and its
-// cutoff ellipse meets the block's pixel centres.
+// cutoff ellipse meets the block's pixel centres. With minStops (the backward
+// pass), also only when the splat's entry (first + j) is at or after the
+// least stop of the block's pixels: before it, every pixel there has stopped.
 template <class M>
 __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, const uint32_t *__restrict__ values, uint32_t count,
                                             uint32_t splatLimit, const TileGeometry &geo, uint32_t *error, Staged *batch,
-                                            uint32_t (*cover)[kBatch / 32]) {
+                                            uint32_t (*cover)[kBatch / 32], const uint32_t *minStops = nullptr,
+                                            uint32_t first = 0u) {
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
 #pragma unroll
   for (uint32_t round = 0; round < kBatch / kHalfTile; ++round) {
@@ -606,6 +609,7 @@ __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, co
         const float reach = 2.0f * __logf(255.0f * st.opacity);
 #pragma unroll
         for (uint32_t w = 0; w < kHalfTile / 32; ++w) {
+          if (minStops != nullptr && first + j < minStops[w]) continue;
           const float lowX = ((float)(geo.x0 + (w & 1u) * 8u) + 0.5f) - st.cx;
           const float lowY = ((float)(geo.y0 + (w >> 1) * 8u) + 0.5f) - st.cy;
           if (ellipse_meets_rect(st.qx, st.qy, st.qz, reach, lowX, lowX + 7.0f, lowY, lowY + 7.0f)) met |= 1u << w;
@@ -702,8 +706,10 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   const PixelPair pp = pixel_pair(geo, cam, t);
   const uint2 range = ranges[tile];
   // front: log T total minus the log transmittance of the splats already
-  // walked (those behind), kept as one running value.
-  float front[2], Ax[2], Ay[2], Az[2], Br[2], Bg[2], Bb[2];
+  // walked (those behind), kept as one running value. behind: the adjoint
+  // dotted with the colour the splats behind (and the background) give, the
+  // one thing of that colour the alpha gradient needs.
+  float front[2], Ax[2], Ay[2], Az[2], behind[2];
   uint32_t stop[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
@@ -714,9 +720,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
     Ay[q] = a.y;
     Az[q] = a.z;
     stop[q] = pp.inside[q] ? stops[at] : range.y;
-    Br[q] = bgR;
-    Bg[q] = bgG;
-    Bb[q] = bgB;
+    behind[q] = fmaf(a.z, bgB, fmaf(a.y, bgG, a.x * bgR));
   }
   const float perPixel = cam.perPixel;
   const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   for (uint32_t start = tileStop; start < range.y; start += kBatch) {
     const uint32_t count = min((uint32_t)kBatch, range.y - start);
     __syncthreads();
-    stage_pairs<M>(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover);
+    stage_pairs<M>(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover, s_min, start);
     __syncthreads();
     for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
     for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
@@ -765,8 +769,8 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         g[7] = fmaf(wA, Ay[q], g[7]);
         g[8] = fmaf(wA, Az[q], g[8]);
         g[9] = fmaf(wA, perPixel, g[9]);
-        const float dAlpha =
-            (act[q] && oe[q] < kAlphaMax) ? T * fmaf(Az[q], s.b - Bb[q], fmaf(Ay[q], s.g - Bg[q], Ax[q] * (s.r - Br[q]))) : 0.0f;
+        const float ahead = fmaf(Az[q], s.b, fmaf(Ay[q], s.g, Ax[q] * s.r)) - behind[q];
+        const float dAlpha = (act[q] && oe[q] < kAlphaMax) ? T * ahead : 0.0f;
         g[0] = fmaf(dAlpha, ep[q], g[0]);
         const float dPower = dAlpha * alpha[q];
         const float vx = fmaf(s.qy, dy[q], s.qx * dx[q]), vy = fmaf(s.qz, dy[q], s.qy * dx[q]);
@@ -775,14 +779,11 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         g[2] += g2;
         g[10] += fabsf(g1);
         g[11] += fabsf(g2);
-        const float h = dPower * 0.5f;
-        const float hx = h * vx;
-        g[3] = fmaf(hx, vx, g[3]);
-        g[4] = fmaf(hx, vy, g[4]);
-        g[5] = fmaf(h * vy, vy, g[5]);
-        Br[q] = fmaf(aAct, s.r - Br[q], Br[q]);
-        Bg[q] = fmaf(aAct, s.g - Bg[q], Bg[q]);
-        Bb[q] = fmaf(aAct, s.b - Bb[q], Bb[q]);
+        // Twice the conic sums; the flush halves them (exactly).
+        g[3] = fmaf(g1, vx, g[3]);
+        g[4] = fmaf(g1, vy, g[4]);
+        g[5] = fmaf(g2, vy, g[5]);
+        behind[q] = fmaf(aAct, ahead, behind[q]);
         front[q] = front[q] - logRest;
       }
       const float total = butterfly12(g);
@@ -797,7 +798,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
       for (int v = 0; v < kGradValues; ++v) {
         const float x = s_acc[j * kAccStride + v];
         if (x != 0.0f) {
-          atomicAdd(dst + v, x);
+          atomicAdd(dst + v, v >= 3 && v <= 5 ? 0.5f * x : x);
           s_acc[j * kAccStride + v] = 0.0f;
         }
       }
