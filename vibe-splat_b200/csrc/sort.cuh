@@ -7,7 +7,8 @@
 //   1. one histogram kernel counts the digits of every pass at once;
 //   2. one kernel per pass brings a tile of 4096 keys and their values into
 //      shared memory by bulk asynchronous copy (cp.async.bulk, completed on an
-//      mbarrier), ranks the keys with warp-level match.any, finds its global
+//      mbarrier), ranks the keys warp by warp (ballots of the digit bits for
+//      6- and 7-bit digits, match.any for 8-bit ones), finds its global
 //      offsets through a decoupled look-back over the tiles before it, and
 //      scatters through shared memory so that each warp writes contiguous
 //      runs. Keys, values and their temporaries must be 16-byte aligned.
