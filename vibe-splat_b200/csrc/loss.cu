@@ -24,6 +24,15 @@ constexpr float kC1 = 0.0001f, kC2 = 0.0009f;
 __constant__ float c_weights[11] = {0.00102838f, 0.00759876f, 0.03600077f, 0.10936069f, 0.21300554f, 0.26601172f,
                                     0.21300554f, 0.10936069f, 0.03600077f, 0.00759876f, 0.00102838f};
 
+// The norm of a window that lies inside the image: the eleven weights added in
+// window_norm's order.
+__device__ __forceinline__ float c_weights_total() {
+  float norm = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 11; ++i) norm += c_weights[i];
+  return norm;
+}
+
 __device__ __forceinline__ float window_norm(int at, int size) {
   float norm = 0.0f;
   for (int i = max(at - 5, 0); i <= min(at + 5, size - 1); ++i) norm += c_weights[i - at + 5];
@@ -54,26 +63,119 @@ __device__ __forceinline__ float block_sum(float v, float *s_warp) {
 
 // The tile with a 5-pixel halo on every side, one float per pixel and
 // plane, zero outside the image: a tap there adds an exact zero, as if the
-// window had been cut at the border. The horizontal pass gives each thread
-// two neighbouring outputs of a row, which share 10 of their 11 taps.
+// window had been cut at the border, so every pass runs all 11 taps.
+//
+// The horizontal pass leaves unnormalised window sums: the horizontal norm
+// depends on the column only, so it leaves the double sum as a factor and is
+// applied, with the vertical one, in the epilogue. Both passes are register
+// blocked: a thread takes kGroup neighbouring outputs of one channel, which
+// share kGroup + 10 staged values per plane.
 constexpr int kSpanCols = kTileSize + 2 * kHalo;
 constexpr int kStage = kRows * kSpanCols;
-constexpr int kStagePlane = kStage;
-constexpr int kPairs = kRows * kTileSize / 2; // horizontal work items
-__device__ __forceinline__ int stage_row(int r) { return r * kSpanCols; }
+constexpr int kGroup = 4;
+constexpr int kGroups = kTileSize / kGroup;
+constexpr int kHorizontalItems = kRows * kGroups;      // per channel
+constexpr int kVerticalItems = kTileSize * kGroups;    // per channel
+static_assert(3 * kVerticalItems <= kTilePixels, "one vertical item per thread");
+
+// The window norms of a row or column (the sum of the taps inside the image).
+__device__ __forceinline__ float norm_of(int at, int size) {
+  return (at >= kHalo && at + kHalo < size) ? c_weights_total() : window_norm(at, size);
+}
+
+// Horizontal window sums of `planes` staged planes into s_h, kGroup outputs
+// per item: FIELD sums x (one plane each); SSIM sums x, y, x^2, y^2, xy.
+template <bool SSIM>
+__device__ __forceinline__ void horizontal_pass(const float (*s_in)[kStage], float (*s_h)[kSpan]) {
+  constexpr int kOut = SSIM ? 5 : 3;
+  for (int item = threadIdx.x; item < 3 * kHorizontalItems; item += kTilePixels) {
+    const int k = item / kHorizontalItems, rem = item % kHorizontalItems;
+    const int r = rem / kGroups, c = (rem % kGroups) * kGroup;
+    const int row = r * kSpanCols + c;
+    float m[kGroup][kOut];
+#pragma unroll
+    for (int o = 0; o < kGroup; ++o)
+#pragma unroll
+      for (int q = 0; q < kOut; ++q) m[o][q] = 0.0f;
+#pragma unroll
+    for (int u = 0; u < kGroup + 10; ++u) {
+      if constexpr (SSIM) {
+        const float a = s_in[k][row + u], b = s_in[3 + k][row + u];
+#pragma unroll
+        for (int o = 0; o < kGroup; ++o) {
+          const int tap = u - o; // output c + o takes staged column c + o + tap
+          if (tap < 0 || tap > 10) continue;
+          const float w = c_weights[tap];
+          const float wa = w * a, wb = w * b;
+          m[o][0] = fmaf(w, a, m[o][0]);
+          m[o][1] = fmaf(w, b, m[o][1]);
+          m[o][2] = fmaf(wa, a, m[o][2]);
+          m[o][3] = fmaf(wb, b, m[o][3]);
+          m[o][4] = fmaf(wa, b, m[o][4]);
+        }
+      } else {
+        const float v[3] = {s_in[k][row + u], s_in[3 + k][row + u], s_in[6 + k][row + u]};
+#pragma unroll
+        for (int o = 0; o < kGroup; ++o) {
+          const int tap = u - o;
+          if (tap < 0 || tap > 10) continue;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) m[o][q] = fmaf(c_weights[tap], v[q], m[o][q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < kGroup; ++o)
+#pragma unroll
+      for (int q = 0; q < kOut; ++q) s_h[q * 3 + k][r * kTileSize + c + o] = m[o][q];
+  }
+}
+
+// Vertical window sums of kOut planes of channel k for kGroup rows of column
+// c, from the horizontal sums.
+template <int kOut>
+__device__ __forceinline__ void vertical_sums(const float (*s_h)[kSpan], int k, int c, int row0, float m[kGroup][kOut]) {
+#pragma unroll
+  for (int o = 0; o < kGroup; ++o)
+#pragma unroll
+    for (int q = 0; q < kOut; ++q) m[o][q] = 0.0f;
+#pragma unroll
+  for (int v = 0; v < kGroup + 10; ++v) {
+    float h[kOut];
+#pragma unroll
+    for (int q = 0; q < kOut; ++q) h[q] = s_h[q * 3 + k][(row0 + v) * kTileSize + c];
+#pragma unroll
+    for (int o = 0; o < kGroup; ++o) {
+      const int tap = v - o;
+      if (tap < 0 || tap > 10) continue;
+#pragma unroll
+      for (int q = 0; q < kOut; ++q) m[o][q] = fmaf(c_weights[tap], h[q], m[o][q]);
+    }
+  }
+}
+
+struct TileOrigin {
+  const ViewParams *cam;
+  int x0, y0;
+};
+
+__device__ __forceinline__ TileOrigin tile_origin(const ViewSet &views, int tile) {
+  const ViewParams &cam = views.v[view_of_tile(views, tile)];
+  const int local = tile - cam.tileBase;
+  return TileOrigin{&cam, (local % cam.gridW) * kTileSize, (local / cam.gridW) * kTileSize};
+}
 
 __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
                                                       const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
                                                       float2 *__restrict__ partials) {
   const ViewSet &views = *viewsPtr;
-  __shared__ float s_in[6][kStagePlane]; // image r, g, b, then target r, g, b
-  __shared__ float s_h[5][3][kSpan];
+  __shared__ float s_in[6][kStage]; // image r, g, b, then target r, g, b
+  __shared__ float s_h[15][kSpan];  // sums x, y, x^2, y^2, xy, three channels each
   __shared__ float s_warp[kTilePixels / 32];
   const int tile = blockIdx.x;
-  const ViewParams &cam = views.v[view_of_tile(views, tile)];
-  const int local = tile - cam.tileBase;
-  const int W = cam.width, H = cam.height;
-  const int x0 = (local % cam.gridW) * kTileSize, y0 = (local / cam.gridW) * kTileSize;
+  const TileOrigin origin = tile_origin(views, tile);
+  const ViewParams &cam = *origin.cam;
+  const int W = cam.width, H = cam.height, x0 = origin.x0, y0 = origin.y0;
   const size_t base = (size_t)cam.pixelBase;
   const size_t plane = (size_t)views.totalPixels;
 
@@ -87,94 +189,46 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
       a4 = image[at];
       b3 = unpack_unorm(target[at]);
     }
-    const int o = stage_row(r) + c;
-    s_in[0][o] = a4.x;
-    s_in[1][o] = a4.y;
-    s_in[2][o] = a4.z;
-    s_in[3][o] = b3.x;
-    s_in[4][o] = b3.y;
-    s_in[5][o] = b3.z;
+    s_in[0][i] = a4.x;
+    s_in[1][i] = a4.y;
+    s_in[2][i] = a4.z;
+    s_in[3][i] = b3.x;
+    s_in[4][i] = b3.y;
+    s_in[5][i] = b3.z;
   }
   __syncthreads();
-
-  // Horizontal pass: tile columns, tile rows plus the halo rows, two
-  // neighbouring columns per thread.
-  for (int i = threadIdx.x; i < kPairs; i += kTilePixels) {
-    const int r = i / (kTileSize / 2), c = 2 * (i % (kTileSize / 2));
-    const int y = y0 + r - kHalo, x = x0 + c;
-    float m[2][5][3] = {};
-    if (y >= 0 && y < H && x < W) {
-      const int row = stage_row(r) + c;
-#pragma unroll
-      for (int u = 0; u < 12; ++u) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const float a = s_in[k][row + u], b = s_in[3 + k][row + u];
-#pragma unroll
-          for (int o = 0; o < 2; ++o) {
-            const int tap = u - o; // output c + o takes staged column c + o + tap
-            if (tap < 0 || tap > 10) continue;
-            const float w = c_weights[tap];
-            const float wa = w * a;
-            m[o][0][k] = fmaf(w, a, m[o][0][k]);
-            m[o][1][k] = fmaf(w, b, m[o][1][k]);
-            m[o][2][k] = fmaf(wa, a, m[o][2][k]);
-            m[o][3][k] = fmaf(w * b, b, m[o][3][k]);
-            m[o][4][k] = fmaf(wa, b, m[o][4][k]);
-          }
-        }
-      }
-#pragma unroll
-      for (int o = 0; o < 2; ++o) {
-        const float inv = x + o < W ? 1.0f / window_norm(x + o, W) : 0.0f;
-#pragma unroll
-        for (int q = 0; q < 5; ++q)
-#pragma unroll
-          for (int k = 0; k < 3; ++k) m[o][q][k] *= inv;
-      }
-    }
-#pragma unroll
-    for (int o = 0; o < 2; ++o)
-#pragma unroll
-      for (int q = 0; q < 5; ++q)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) s_h[q][k][r * kTileSize + c + o] = m[o][q][k];
-  }
+  horizontal_pass<true>(s_in, s_h);
   __syncthreads();
 
-  const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
   float own = 0.0f;
-  if (px < W && py < H) {
-    const float rowNorm = window_norm(py, H);
-    float m[5][3] = {};
-    const int v0 = max(py - 5, 0), v1 = min(py + 5, H - 1);
-    for (int v = v0; v <= v1; ++v) {
-      const float w = c_weights[v - py + 5];
-      const int at = (v - y0 + kHalo) * kTileSize + (threadIdx.x & 15);
+  if (threadIdx.x < 3 * kVerticalItems) {
+    const int c = threadIdx.x % kTileSize, g = (threadIdx.x / kTileSize) % kGroups, k = threadIdx.x / kVerticalItems;
+    const int px = x0 + c, row0 = g * kGroup;
+    float m[kGroup][5];
+    vertical_sums<5>(s_h, k, c, row0, m);
+    if (px < W) {
+      const float invCol = 1.0f / norm_of(px, W);
 #pragma unroll
-      for (int q = 0; q < 5; ++q)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_h[q][k][at], m[q][k]);
-    }
-    const float invRow = 1.0f / rowNorm;
-    const float invNorm = 1.0f / (rowNorm * window_norm(px, W));
-    const size_t pixel = base + (size_t)py * W + px;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float mx = m[0][k] * invRow, my = m[1][k] * invRow;
-      const float vx = m[2][k] * invRow - mx * mx, vy = m[3][k] * invRow - my * my, cxy = m[4][k] * invRow - mx * my;
-      const float n1 = 2.0f * mx * my + kC1, n2 = 2.0f * cxy + kC2;
-      const float d1 = mx * mx + my * my + kC1, d2 = vx + vy + kC2;
-      const float invD = 1.0f / (d1 * d2), invD1 = 1.0f / d1, invD2 = 1.0f / d2;
-      const float s = (n1 * n2) * invD;
-      own += s;
-      // n1 and n2 cancelled by hand, as the reference does: n2 can be zero.
-      const float dMu = 2.0f * my * n2 * invD - s * 2.0f * mx * invD1;
-      const float dVar = -s * invD2;
-      const float dCov = 2.0f * n1 * invD;
-      fields[(0 * 3 + k) * plane + pixel] = (dMu - 2.0f * mx * dVar - my * dCov) * invNorm;
-      fields[(1 * 3 + k) * plane + pixel] = dVar * invNorm;
-      fields[(2 * 3 + k) * plane + pixel] = dCov * invNorm;
+      for (int o = 0; o < kGroup; ++o) {
+        const int py = y0 + row0 + o;
+        if (py >= H) continue;
+        const float inv = invCol / norm_of(py, H);
+        const float mx = m[o][0] * inv, my = m[o][1] * inv;
+        const float vx = fmaf(m[o][2], inv, -mx * mx), vy = fmaf(m[o][3], inv, -my * my), cxy = fmaf(m[o][4], inv, -mx * my);
+        const float n1 = fmaf(2.0f * mx, my, kC1), n2 = fmaf(2.0f, cxy, kC2);
+        const float d1 = fmaf(mx, mx, fmaf(my, my, kC1)), d2 = vx + vy + kC2;
+        const float invD = 1.0f / (d1 * d2), invD1 = d2 * invD, invD2 = d1 * invD;
+        const float ssim = (n1 * n2) * invD;
+        own += ssim;
+        // n1 and n2 cancelled by hand, as the reference does: n2 can be zero.
+        const float dMu = 2.0f * my * n2 * invD - ssim * 2.0f * mx * invD1;
+        const float dVar = -ssim * invD2;
+        const float dCov = 2.0f * n1 * invD;
+        const size_t pixel = base + (size_t)py * W + px;
+        fields[(0 * 3 + k) * plane + pixel] = (dMu - 2.0f * mx * dVar - my * dCov) * inv;
+        fields[(1 * 3 + k) * plane + pixel] = dVar * inv;
+        fields[(2 * 3 + k) * plane + pixel] = dCov * inv;
+      }
     }
   }
   const float total = block_sum(own, s_warp);
@@ -185,14 +239,14 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
                                                       const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
                                                       float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials) {
   const ViewSet &views = *viewsPtr;
-  __shared__ float s_in[9][kStagePlane]; // the nine field planes
-  __shared__ float s_h[3][3][kSpan];
+  __shared__ float s_in[9][kStage]; // the nine field planes
+  __shared__ float s_h[9][kSpan];
+  __shared__ float s_result[3][kTilePixels];
   __shared__ float s_warp[kTilePixels / 32];
   const int tile = blockIdx.x;
-  const ViewParams &cam = views.v[view_of_tile(views, tile)];
-  const int local = tile - cam.tileBase;
-  const int W = cam.width, H = cam.height;
-  const int x0 = (local % cam.gridW) * kTileSize, y0 = (local / cam.gridW) * kTileSize;
+  const TileOrigin origin = tile_origin(views, tile);
+  const ViewParams &cam = *origin.cam;
+  const int W = cam.width, H = cam.height, x0 = origin.x0, y0 = origin.y0;
   const size_t base = (size_t)cam.pixelBase;
   const size_t plane = (size_t)views.totalPixels;
 
@@ -201,75 +255,44 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
     const int y = y0 + r - kHalo, x = x0 + c - kHalo;
     const bool in = y >= 0 && y < H && x >= 0 && x < W;
     const size_t at = in ? base + (size_t)y * W + x : 0;
-    const int o = stage_row(r) + c;
 #pragma unroll
-    for (int f = 0; f < 9; ++f) s_in[f][o] = in ? fields[f * plane + at] : 0.0f;
+    for (int f = 0; f < 9; ++f) s_in[f][i] = in ? fields[f * plane + at] : 0.0f;
   }
   __syncthreads();
-
-  for (int i = threadIdx.x; i < kPairs; i += kTilePixels) {
-    const int r = i / (kTileSize / 2), c = 2 * (i % (kTileSize / 2));
-    const int y = y0 + r - kHalo, x = x0 + c;
-    float m[2][3][3] = {};
-    if (y >= 0 && y < H && x < W) {
-      const int row = stage_row(r) + c;
-#pragma unroll
-      for (int u = 0; u < 12; ++u) {
-#pragma unroll
-        for (int f = 0; f < 9; ++f) {
-          const float v = s_in[f][row + u];
-#pragma unroll
-          for (int o = 0; o < 2; ++o) {
-            const int tap = u - o;
-            if (tap < 0 || tap > 10) continue;
-            m[o][f / 3][f % 3] = fmaf(c_weights[tap], v, m[o][f / 3][f % 3]);
-          }
-        }
-      }
-      if (x + 1 >= W) {
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-#pragma unroll
-          for (int k = 0; k < 3; ++k) m[1][q][k] = 0.0f;
-      }
-    }
-#pragma unroll
-    for (int o = 0; o < 2; ++o)
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) s_h[q][k][r * kTileSize + c + o] = m[o][q][k];
-  }
+  horizontal_pass<false>(s_in, s_h);
   __syncthreads();
 
-  const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
   float own = 0.0f;
-  if (px < W && py < H) {
+  if (threadIdx.x < 3 * kVerticalItems) {
+    const int c = threadIdx.x % kTileSize, g = (threadIdx.x / kTileSize) % kGroups, k = threadIdx.x / kVerticalItems;
+    const int px = x0 + c, row0 = g * kGroup;
+    float m[kGroup][3];
+    vertical_sums<3>(s_h, k, c, row0, m);
     const float perValue = cam.perPixel;
-    const size_t pixel = base + (size_t)py * W + px;
-    const float4 x4 = image[pixel];
-    const float3 y3 = unpack_unorm(target[pixel]);
-    const float xv[3] = {x4.x, x4.y, x4.z}, yv[3] = {y3.x, y3.y, y3.z};
-    float m[3][3] = {};
-    const int v0 = max(py - 5, 0), v1 = min(py + 5, H - 1);
-    for (int v = v0; v <= v1; ++v) {
-      const float w = c_weights[v - py + 5];
-      const int at = (v - y0 + kHalo) * kTileSize + (threadIdx.x & 15);
+    const float *imageF = reinterpret_cast<const float *>(image);
 #pragma unroll
-      for (int q = 0; q < 3; ++q)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) m[q][k] = fmaf(w, s_h[q][k][at], m[q][k]);
+    for (int o = 0; o < kGroup; ++o) {
+      const int py = y0 + row0 + o;
+      float result = 0.0f;
+      if (px < W && py < H) {
+        const size_t pixel = base + (size_t)py * W + px;
+        const float xv = imageF[pixel * 4 + k];
+        const float yv = (float)((target[pixel] >> (8 * k)) & 0xFFu) / 255.0f;
+        const float d = xv - yv;
+        own += fabsf(d);
+        const float sgn = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
+        const float ssimPart = m[o][0] + 2.0f * xv * m[o][1] + yv * m[o][2];
+        result = ((1.0f - lambda) * sgn - lambda * ssimPart) * perValue;
+      }
+      s_result[k][(row0 + o) * kTileSize + c] = result;
     }
-    float result[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float d = xv[k] - yv[k];
-      own += fabsf(d);
-      const float sgn = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
-      const float ssimPart = m[0][k] + 2.0f * xv[k] * m[1][k] + yv[k] * m[2][k];
-      result[k] = ((1.0f - lambda) * sgn - lambda * ssimPart) * perValue;
-    }
-    adjoint[pixel] = make_float4(result[0], result[1], result[2], 0.0f);
+  }
+  __syncthreads();
+  {
+    const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
+    if (px < W && py < H)
+      adjoint[base + (size_t)py * W + px] =
+          make_float4(s_result[0][threadIdx.x], s_result[1][threadIdx.x], s_result[2][threadIdx.x], 0.0f);
   }
   const float total = block_sum(own, s_warp);
   if (threadIdx.x == 0) partials[tile].y = total;
