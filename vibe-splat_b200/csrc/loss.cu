@@ -77,6 +77,15 @@ constexpr int kGroups = kTileSize / kGroup;
 constexpr int kHorizontalItems = kRows * kGroups;      // per channel
 constexpr int kVerticalItems = kTileSize * kGroups;    // per channel
 static_assert(3 * kVerticalItems <= kTilePixels, "one vertical item per thread");
+static_assert(kTileSize == 16 && kGroup == 4, "h_index's swizzle assumes 16-wide rows and 4-row groups");
+
+// Where the horizontal sum of (row, column) lives in its plane: rows in pairs
+// of 32 words, a pair's two 16-word halves swapped where bit 2 of the row is
+// set, so that the two half-warps of the vertical pass, four rows apart, read
+// opposite halves of the banks.
+__device__ __forceinline__ int h_index(int row, int col) {
+  return (row >> 1) * 32 + ((((row & 1) << 4) | col) ^ (((row >> 2) & 1) << 4));
+}
 
 // The window norms of a row or column (the sum of the taps inside the image).
 __device__ __forceinline__ float norm_of(int at, int size) {
@@ -127,7 +136,7 @@ __device__ __forceinline__ void horizontal_pass(const float (*s_in)[kStage], flo
 #pragma unroll
     for (int o = 0; o < kGroup; ++o)
 #pragma unroll
-      for (int q = 0; q < kOut; ++q) s_h[q * 3 + k][r * kTileSize + c + o] = m[o][q];
+      for (int q = 0; q < kOut; ++q) s_h[q * 3 + k][h_index(r, c + o)] = m[o][q];
   }
 }
 
@@ -143,7 +152,7 @@ __device__ __forceinline__ void vertical_sums(const float (*s_h)[kSpan], int k, 
   for (int v = 0; v < kGroup + 10; ++v) {
     float h[kOut];
 #pragma unroll
-    for (int q = 0; q < kOut; ++q) h[q] = s_h[q * 3 + k][(row0 + v) * kTileSize + c];
+    for (int q = 0; q < kOut; ++q) h[q] = s_h[q * 3 + k][h_index(row0 + v, c)];
 #pragma unroll
     for (int o = 0; o < kGroup; ++o) {
       const int tap = v - o;
@@ -179,7 +188,10 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
   const size_t base = (size_t)cam.pixelBase;
   const size_t plane = (size_t)views.totalPixels;
 
-  for (int i = threadIdx.x; i < kStage; i += kTilePixels) {
+#pragma unroll
+  for (int round = 0; round < (kStage + kTilePixels - 1) / kTilePixels; ++round) {
+    const int i = round * kTilePixels + threadIdx.x;
+    if (i >= kStage) break;
     const int r = i / kSpanCols, c = i % kSpanCols;
     const int y = y0 + r - kHalo, x = x0 + c - kHalo;
     float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -249,8 +261,28 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   const int W = cam.width, H = cam.height, x0 = origin.x0, y0 = origin.y0;
   const size_t base = (size_t)cam.pixelBase;
   const size_t plane = (size_t)views.totalPixels;
+  // This thread's epilogue pixels (kGroup rows of one column, one channel):
+  // their image and target values are asked for first, so that they arrive
+  // while the fields are staged and filtered.
+  const bool epilogue = threadIdx.x < 3 * kVerticalItems;
+  const int ec = threadIdx.x % kTileSize, eg = (threadIdx.x / kTileSize) % kGroups, ek = threadIdx.x / kVerticalItems;
+  float xs[kGroup], ys[kGroup];
+#pragma unroll
+  for (int o = 0; o < kGroup; ++o) {
+    const int px = x0 + ec, py = y0 + eg * kGroup + o;
+    xs[o] = 0.0f;
+    ys[o] = 0.0f;
+    if (epilogue && px < W && py < H) {
+      const size_t pixel = base + (size_t)py * W + px;
+      xs[o] = reinterpret_cast<const float *>(image)[pixel * 4 + ek];
+      ys[o] = (float)((target[pixel] >> (8 * ek)) & 0xFFu) / 255.0f;
+    }
+  }
 
-  for (int i = threadIdx.x; i < kStage; i += kTilePixels) {
+#pragma unroll
+  for (int round = 0; round < (kStage + kTilePixels - 1) / kTilePixels; ++round) {
+    const int i = round * kTilePixels + threadIdx.x;
+    if (i >= kStage) break;
     const int r = i / kSpanCols, c = i % kSpanCols;
     const int y = y0 + r - kHalo, x = x0 + c - kHalo;
     const bool in = y >= 0 && y < H && x >= 0 && x < W;
@@ -263,21 +295,18 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   __syncthreads();
 
   float own = 0.0f;
-  if (threadIdx.x < 3 * kVerticalItems) {
-    const int c = threadIdx.x % kTileSize, g = (threadIdx.x / kTileSize) % kGroups, k = threadIdx.x / kVerticalItems;
-    const int px = x0 + c, row0 = g * kGroup;
+  if (epilogue) {
+    const int c = ec, k = ek;
+    const int px = x0 + c, row0 = eg * kGroup;
     float m[kGroup][3];
     vertical_sums<3>(s_h, k, c, row0, m);
     const float perValue = cam.perPixel;
-    const float *imageF = reinterpret_cast<const float *>(image);
 #pragma unroll
     for (int o = 0; o < kGroup; ++o) {
       const int py = y0 + row0 + o;
       float result = 0.0f;
       if (px < W && py < H) {
-        const size_t pixel = base + (size_t)py * W + px;
-        const float xv = imageF[pixel * 4 + k];
-        const float yv = (float)((target[pixel] >> (8 * k)) & 0xFFu) / 255.0f;
+        const float xv = xs[o], yv = ys[o];
         const float d = xv - yv;
         own += fabsf(d);
         const float sgn = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
