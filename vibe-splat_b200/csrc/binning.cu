@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kCountThreads)
     k_bin_count(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
                 const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
                 uint32_t *__restrict__ counts, uint32_t *__restrict__ masks, uint32_t *counters) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ ColTangents s_cols[kCountThreads / 32][kTableMax];
   __shared__ RowTangents s_rows[kCountThreads / 32][kTableMax];
@@ -250,6 +251,7 @@ __global__ void __launch_bounds__(kCountThreads)
 __global__ void __launch_bounds__(kScanThreads)
     k_offsets_scan(uint32_t items, uint32_t *__restrict__ offsets, uint32_t *counters, uint32_t capacity,
                    unsigned long long *status, uint32_t *ticket, uint32_t *error) {
+  chain_enter();
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ unsigned long long s_exclusive;
@@ -348,6 +350,7 @@ __global__ void __launch_bounds__(256)
                const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ masks, uint32_t capacity,
                uint32_t *__restrict__ tileKeys32, unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues,
                uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ ColTangents s_cols[8][kTableMax];
   __shared__ RowTangents s_rows[8][kTableMax];
@@ -456,6 +459,7 @@ constexpr uint32_t kRangesPerThread = 4;
 __global__ void __launch_bounds__(256) k_tile_ranges(const uint32_t *__restrict__ keys32, const unsigned long long *__restrict__ keys64,
                                                      const uint32_t *deviceCount, uint32_t tileLimit, uint2 *__restrict__ ranges,
                                                      uint32_t *error) {
+  chain_enter();
   const uint32_t count = *deviceCount;
   auto tile_of = [&](uint32_t i) { return keys64 != nullptr ? (uint32_t)(keys64[i] >> 32) : keys32[i]; };
   const uint32_t stride = gridDim.x * blockDim.x * kRangesPerThread;
@@ -494,9 +498,9 @@ void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
   cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
-  k_bin_count<<<div_up(items, kCountThreads), kCountThreads, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews,
+  launch_chained(k_bin_count, dim3(div_up(items, kCountThreads)), dim3(kCountThreads), 0, stream, splats, reach, itemKeys, itemSplat, items, n, dViews,
                                                                         offsets, masks, counters);
-  k_offsets_scan<<<tiles, kScanThreads, 0, stream>>>(items, offsets, counters, capacity, status, ticket, error);
+  launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, offsets, counters, capacity, status, ticket, error);
 }
 
 void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
@@ -504,7 +508,7 @@ void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *it
                      const uint32_t *masks, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
                      uint32_t *entryValues, uint32_t *error, cudaStream_t stream) {
   if (items == 0) return;
-  k_bin_emit<<<div_up(items, 256), 256, 0, stream>>>(splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks, capacity,
+  launch_chained(k_bin_emit, dim3(div_up(items, 256)), dim3(256), 0, stream, splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks, capacity,
                                                      tileKeys32, tileKeys64, entryValues, error);
 }
 
@@ -512,7 +516,7 @@ void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *ti
                         uint32_t capacity, uint32_t tileLimit, uint2 *ranges, uint32_t *error, cudaStream_t stream) {
   if (capacity == 0) return;
   const uint32_t blocks = std::min<uint32_t>(div_up(div_up(capacity, kRangesPerThread), 256), 148u * 8u);
-  k_tile_ranges<<<blocks, 256, 0, stream>>>(tileKeys32, tileKeys64, deviceCount, tileLimit, ranges, error);
+  launch_chained(k_tile_ranges, dim3(blocks), dim3(256), 0, stream, tileKeys32, tileKeys64, deviceCount, tileLimit, ranges, error);
 }
 
 void launch_exclusive_scan(uint32_t items, uint32_t *values, uint32_t *counters, void *scratch, uint32_t *error,
@@ -522,7 +526,7 @@ void launch_exclusive_scan(uint32_t items, uint32_t *values, uint32_t *counters,
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
   cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
-  k_offsets_scan<<<tiles, kScanThreads, 0, stream>>>(items, values, counters, 0xFFFFFFFFu, status, ticket, error);
+  launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, values, counters, 0xFFFFFFFFu, status, ticket, error);
 }
 
 } // namespace sb

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "chain.cuh"
 #include "splat_detmath.h"
 
 namespace sb {

@@ -177,6 +177,7 @@ __device__ __forceinline__ TileOrigin tile_origin(const ViewSet &views, int tile
 __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
                                                       const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
                                                       float2 *__restrict__ partials) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ float s_in[6][kStage]; // image r, g, b, then target r, g, b
   __shared__ float s_h[15][kSpan];  // sums x, y, x^2, y^2, xy, three channels each
@@ -250,6 +251,7 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
 __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
                                                       const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
                                                       float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ float s_in[9][kStage]; // the nine field planes
   __shared__ float s_h[9][kSpan];
@@ -329,6 +331,7 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
 
 __global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ partials, const ViewSet *__restrict__ viewsPtr,
                                                      LossTotals *totals) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ double s_ssim[256], s_l1[256];
   const int v = blockIdx.x;
@@ -360,18 +363,18 @@ __global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ 
 void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
                  cudaStream_t stream) {
   if (views.totalTiles == 0) return;
-  k_ssim<<<views.totalTiles, kTilePixels, 0, stream>>>(image, target, dViews, reinterpret_cast<float *>(fields), partials);
+  launch_chained(k_ssim, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, dViews, reinterpret_cast<float *>(fields), partials);
 }
 
 void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
                  float4 *adjoint, float2 *partials, cudaStream_t stream) {
   if (views.totalTiles == 0) return;
-  k_loss<<<views.totalTiles, kTilePixels, 0, stream>>>(image, target, reinterpret_cast<const float *>(fields), dViews, lambda,
+  launch_chained(k_loss, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, reinterpret_cast<const float *>(fields), dViews, lambda,
                                                        adjoint, partials);
 }
 
 void launch_loss_totals(const float2 *partials, const ViewSet &views, const ViewSet *dViews, LossTotals *totals, cudaStream_t stream) {
-  k_loss_totals<<<views.count, 256, 0, stream>>>(partials, dViews, totals);
+  launch_chained(k_loss_totals, dim3(views.count), dim3(256), 0, stream, partials, dViews, totals);
 }
 
 } // namespace sb

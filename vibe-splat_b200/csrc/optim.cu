@@ -331,6 +331,7 @@ __global__ void __launch_bounds__(128, 4) k_chain(Params p, const ViewSet *__res
                                                   OptimState state, GradientsOut grads, bool storeGradients,
                                                   float4 *__restrict__ shGrad, float *__restrict__ densifyStats,
                                                   const uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.n) return;
@@ -435,6 +436,7 @@ __global__ void __launch_bounds__(128, 4) k_chain(Params p, const ViewSet *__res
 // as one: [positions 3n | scales 3n | rotations 4n | opacities n].
 __global__ void __launch_bounds__(256) k_adam_geometry(Params p, const ChainArgs *__restrict__ argsPtr, OptimState state,
                                                        GradientsOut grads, const uint32_t *error) {
+  chain_enter();
   const size_t n = p.n;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 11 * n) return;
@@ -477,6 +479,7 @@ template <ShStore S, bool MULTI>
 __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__restrict__ viewsPtr, const float4 *__restrict__ shGrad,
                                                  const ChainArgs *__restrict__ argsPtr, OptimState state, GradientsOut grads,
                                                  bool storeGradients, const uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   const uint32_t n = p.n;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -635,6 +638,7 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
                                                                 const void *__restrict__ rawIn, const Splat *__restrict__ splats,
                                                                 const ChainArgs *__restrict__ argsPtr, OptimState state,
                                                                 float *__restrict__ densifyStats, uint32_t *error) {
+  chain_enter();
   constexpr uint32_t kShBytes = S == ShStore::F32 ? 4u : 2u;
   extern __shared__ __align__(128) unsigned char s_stage[];
   __shared__ __align__(8) uint64_t s_bar;
@@ -853,7 +857,7 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
 #define SB_STEP(ST, FIX)                                                                                           \
   {                                                                                                                  \
     cudaFuncSetAttribute(k_chain_step<S, ST, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
-    k_chain_step<S, ST, FIX><<<stepBlocks, kStepThreads, smem, stream>>>(p, dViews, raw, splats, dArgs, state, densifyStats, \
+    launch_chained(k_chain_step<S, ST, FIX>, dim3(stepBlocks), dim3(kStepThreads), smem, stream, p, dViews, raw, splats, dArgs, state, densifyStats, \
                                                                         error);                                      \
   }
     const bool f32 = state.store == StateStore::F32;
@@ -866,7 +870,7 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
     return;
   }
 #define SB_CHAIN(F, M) \
-  k_chain<S, F, M><<<blocks, 128, 0, stream>>>(p, dViews, raw, splats, dArgs, state, g, store, shGrad, densifyStats, error)
+  launch_chained(k_chain<S, F, M>, dim3(blocks), dim3(128), 0, stream, p, dViews, raw, splats, dArgs, state, g, store, shGrad, densifyStats, error)
   if (args.fixedPoint) {
     if (multi) SB_CHAIN(true, true);
     else SB_CHAIN(true, false);
@@ -876,10 +880,10 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
   }
 #undef SB_CHAIN
   if (args.mode == ChainMode::Statistics) return;
-  if (!store) k_adam_geometry<<<(uint32_t)((11 * (size_t)p.n + 255) / 256), 256, 0, stream>>>(p, dArgs, state, g, error);
+  if (!store) launch_chained(k_adam_geometry, dim3((uint32_t)((11 * (size_t)p.n + 255) / 256)), dim3(256), 0, stream, p, dArgs, state, g, error);
   const dim3 shGrid(div_up(p.n, 256), div_up(p.shCoeffs, kShGroup));
-  if (multi) k_sh_step<S, true><<<shGrid, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
-  else k_sh_step<S, false><<<shGrid, 256, 0, stream>>>(p, dViews, shGrad, dArgs, state, g, store, error);
+  if (multi) launch_chained(k_sh_step<S, true>, dim3(shGrid), dim3(256), 0, stream, p, dViews, shGrad, dArgs, state, g, store, error);
+  else launch_chained(k_sh_step<S, false>, dim3(shGrid), dim3(256), 0, stream, p, dViews, shGrad, dArgs, state, g, store, error);
 }
 
 } // namespace

@@ -18,6 +18,7 @@ template <ShStore S>
 __global__ void __launch_bounds__(256, 3) k_preprocess(Params p, const ViewSet *__restrict__ viewsPtr, Splat *__restrict__ splats,
                                                     float *__restrict__ reachOut, uint32_t *__restrict__ depthKeys,
                                                     uint32_t *__restrict__ values) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
@@ -137,13 +138,13 @@ void launch_preprocess(const Params &p, const ViewSet &views, const ViewSet *dVi
   const dim3 grid(div_up(p.n, 256), views.count);
   switch (p.shStore) {
   case ShStore::BF16:
-    k_preprocess<ShStore::BF16><<<grid, 256, 0, stream>>>(p, dViews, splats, reach, depthKeys, values);
+    launch_chained(k_preprocess<ShStore::BF16>, dim3(grid), dim3(256), 0, stream, p, dViews, splats, reach, depthKeys, values);
     break;
   case ShStore::F16:
-    k_preprocess<ShStore::F16><<<grid, 256, 0, stream>>>(p, dViews, splats, reach, depthKeys, values);
+    launch_chained(k_preprocess<ShStore::F16>, dim3(grid), dim3(256), 0, stream, p, dViews, splats, reach, depthKeys, values);
     break;
   default:
-    k_preprocess<ShStore::F32><<<grid, 256, 0, stream>>>(p, dViews, splats, reach, depthKeys, values);
+    launch_chained(k_preprocess<ShStore::F32>, dim3(grid), dim3(256), 0, stream, p, dViews, splats, reach, depthKeys, values);
     break;
   }
 }

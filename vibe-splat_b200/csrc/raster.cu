@@ -177,6 +177,7 @@ __global__ void __launch_bounds__(kTilePixels) k_forward(const Splat *__restrict
                                                          float bgR, float bgG, float bgB, float4 *__restrict__ image,
                                                          uint32_t *__restrict__ stops, BlendLists lists, uint32_t splatLimit,
                                                          uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
   __shared__ uint32_t s_cover[kTilePixels / 32][kBatch / 32];
@@ -294,6 +295,7 @@ __global__ void __launch_bounds__(kTilePixels, 4)
                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, void *__restrict__ rawOut,
                uint32_t splatLimit, uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
   __shared__ uint32_t s_acc[kBatch * kAccStride];
@@ -427,6 +429,7 @@ __global__ void __launch_bounds__(kTilePixels, 4)
                      const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                      const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, BlendLists lists,
                      float *__restrict__ raw, uint32_t splatLimit, uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
   __shared__ float s_acc[kBatch * kAccStride];
@@ -625,6 +628,7 @@ __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restri
                                                         const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
                                                         float bgR, float bgG, float bgB, float4 *__restrict__ image,
                                                         uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
   __shared__ uint32_t s_cover[kHalfTile / 32][kBatch / 32];
@@ -693,6 +697,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
                 const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                 const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
                 uint32_t splatLimit, uint32_t *error) {
+  chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
   __shared__ float s_acc[kBatch * kAccStride];
@@ -815,7 +820,7 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
   if (listMode != 0) {
 #define SB_FORWARD_LISTS(MATH, MODE)                                                                                         \
-  k_forward<MATH, MODE><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops, \
+  launch_chained(k_forward<MATH, MODE>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, stops, \
                                                                      lists, splatLimit, error)
     if (cfg.exactMath) {
       if (listMode == 1) SB_FORWARD_LISTS(ExactMath, 1);
@@ -829,17 +834,17 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
   }
   if (cfg.forwardPixels == 2) {
     if (cfg.exactMath)
-      k_forward2<ExactMath><<<views.totalTiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
+      launch_chained(k_forward2<ExactMath>, dim3(views.totalTiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, stops,
                                                                        splatLimit, error);
     else
-      k_forward2<FastMath><<<views.totalTiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, stops,
+      launch_chained(k_forward2<FastMath>, dim3(views.totalTiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, stops,
                                                                       splatLimit, error);
   } else {
     if (cfg.exactMath)
-      k_forward<ExactMath, 0><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+      launch_chained(k_forward<ExactMath, 0>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image,
                                                                            stops, BlendLists{}, splatLimit, error);
     else
-      k_forward<FastMath, 0><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+      launch_chained(k_forward<FastMath, 0>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image,
                                                                           stops, BlendLists{}, splatLimit, error);
   }
 }
@@ -854,15 +859,15 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
   if (!fixedPoint && cfg.backwardPixels == 2) {
     float *rawF = static_cast<float *>(raw);
     if (cfg.exactMath)
-      k_backward2<ExactMath><<<tiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
+      launch_chained(k_backward2<ExactMath>, dim3(tiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
                                                              rawF, splatLimit, error);
     else
-      k_backward2<FastMath><<<tiles, kHalfTile, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
+      launch_chained(k_backward2<FastMath>, dim3(tiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
                                                             rawF, splatLimit, error);
     return;
   }
 #define SB_BACKWARD(MATH, FIX) \
-  k_backward<MATH, FIX><<<tiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops, \
+  launch_chained(k_backward<MATH, FIX>, dim3(tiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops, \
                                                           raw, splatLimit, error)
   if (cfg.exactMath) {
     if (fixedPoint) SB_BACKWARD(ExactMath, true);
@@ -881,10 +886,10 @@ void launch_backward_lists(const Splat *splats, const uint32_t *entryValues, con
   if (views.totalTiles == 0) return;
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
   if (cfg.exactMath)
-    k_backward_lists<ExactMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+    launch_chained(k_backward_lists<ExactMath>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image,
                                                                              adjoint, stops, lists, raw, splatLimit, error);
   else
-    k_backward_lists<FastMath><<<views.totalTiles, kTilePixels, 0, stream>>>(splats, entryValues, ranges, dViews, r, g, b, image,
+    launch_chained(k_backward_lists<FastMath>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image,
                                                                             adjoint, stops, lists, raw, splatLimit, error);
 }
 

@@ -90,6 +90,7 @@ template <typename K, int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_histogram(const K *__restrict__ keys, const uint32_t *deviceCount,
                                                             uint32_t hostCount, int firstBit, int passes,
                                                             uint32_t *__restrict__ hist) {
+  chain_enter();
   constexpr int kBins = 1 << BITS;
   constexpr uint32_t kMask = kBins - 1;
   constexpr int kPerVec = 16 / sizeof(K);
@@ -149,6 +150,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
                                                               const uint32_t *deviceCount, uint32_t hostCount,
                                                               const uint32_t *__restrict__ passHist, uint32_t *lookback,
                                                               uint32_t *tileCounter, int shift, uint32_t *error) {
+  chain_enter();
   constexpr int kBins = 1 << BITS;
   constexpr uint32_t kMask = kBins - 1;
   extern __shared__ __align__(128) unsigned char s_dynamic[];
@@ -379,7 +381,7 @@ template <typename K, int BITS> size_t onesweep_smem() { return kSortTileKeys * 
 template <typename K, int BITS>
 int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, size_t capacity, uint32_t hostCount,
                     const uint32_t *deviceCount, int firstBit, int bits, void *scratch, uint32_t *error,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, bool clearScratch) {
   constexpr int kBins = 1 << BITS;
   const int passes = (bits + BITS - 1) / BITS;
   if (capacity == 0 || passes == 0) return 0;
@@ -389,7 +391,7 @@ int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, 
   uint32_t *hist = reinterpret_cast<uint32_t *>(base + l.hist);
   uint32_t *counters = reinterpret_cast<uint32_t *>(base + l.counters);
   uint32_t *lookback = reinterpret_cast<uint32_t *>(base + l.lookback);
-  cudaMemsetAsync(scratch, 0, l.total, stream);
+  if (clearScratch) cudaMemsetAsync(scratch, 0, l.total, stream);
 
   const uint32_t launchKeys = deviceCount != nullptr ? (uint32_t)capacity : hostCount;
   const uint32_t tiles = div_up(launchKeys, kSortTileKeys);
@@ -405,12 +407,12 @@ int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, 
                          (int)(kHistogramCopies * kMaxPasses * kBins * 4));
     configured = true;
   }
-  k_histogram<K, BITS><<<std::max(histBlocks, 1u), kSortThreads, histSmem, stream>>>(keys, deviceCount, hostCount, firstBit,
+  launch_chained(k_histogram<K, BITS>, dim3(std::max(histBlocks, 1u)), dim3(kSortThreads), histSmem, stream, keys, deviceCount, hostCount, firstBit,
                                                                                      passes, hist);
   K *srcK = keys, *dstK = tmpKeys;
   uint32_t *srcV = values, *dstV = tmpValues;
   for (int p = 0; p < passes; ++p) {
-    k_onesweep<K, BITS><<<tiles, kSortThreads, smem, stream>>>(srcK, srcV, dstK, dstV, deviceCount, hostCount,
+    launch_chained(k_onesweep<K, BITS>, dim3(tiles), dim3(kSortThreads), smem, stream, srcK, srcV, dstK, dstV, deviceCount, hostCount,
                                                                hist + p * kBins, lookback + (size_t)p * tiles * kBins,
                                                                counters + p, firstBit + p * BITS, error);
     K *tk = srcK;
@@ -431,33 +433,33 @@ size_t sort_scratch_bytes(size_t capacity, int /*keyBytes*/, int bits, int digit
 
 int sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t *tmpKeys, uint32_t *tmpValues, size_t capacity,
                    uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits, void *scratch,
-                   uint32_t *error, cudaStream_t stream) {
+                   uint32_t *error, cudaStream_t stream, bool clearScratch) {
   switch (digitBits) {
   case 6:
     return sort_pairs_impl<uint32_t, 6>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount, firstBit, bits,
-                                        scratch, error, stream);
+                                        scratch, error, stream, clearScratch);
   case 7:
     return sort_pairs_impl<uint32_t, 7>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount, firstBit, bits,
-                                        scratch, error, stream);
+                                        scratch, error, stream, clearScratch);
   default:
     return sort_pairs_impl<uint32_t, 8>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount, firstBit, bits,
-                                        scratch, error, stream);
+                                        scratch, error, stream, clearScratch);
   }
 }
 
 int sort_pairs_u64(unsigned long long *keys, uint32_t *values, unsigned long long *tmpKeys, uint32_t *tmpValues,
                    size_t capacity, uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
-                   void *scratch, uint32_t *error, cudaStream_t stream) {
+                   void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch) {
   switch (digitBits) {
   case 6:
     return sort_pairs_impl<unsigned long long, 6>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount,
-                                                  firstBit, bits, scratch, error, stream);
+                                                  firstBit, bits, scratch, error, stream, clearScratch);
   case 7:
     return sort_pairs_impl<unsigned long long, 7>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount,
-                                                  firstBit, bits, scratch, error, stream);
+                                                  firstBit, bits, scratch, error, stream, clearScratch);
   default:
     return sort_pairs_impl<unsigned long long, 8>(keys, values, tmpKeys, tmpValues, capacity, hostCount, deviceCount,
-                                                  firstBit, bits, scratch, error, stream);
+                                                  firstBit, bits, scratch, error, stream, clearScratch);
   }
 }
 

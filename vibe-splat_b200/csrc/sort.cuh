@@ -48,13 +48,15 @@ size_t sort_scratch_bytes(size_t capacity, int keyBytes, int bits, int digitBits
 // the sorted pairs ended in keys/values, 1 if in tmpKeys/tmpValues. The count is
 // read from *deviceCount when it is not null (CUDA-graph friendly; capacity
 // bounds the launch), else hostCount is used. scratch must hold
-// sort_scratch_bytes(capacity, ...) bytes; error is a device word that gets
-// kErrLookbackTimeout if a wait ran out. Supported digitBits: 6, 7, 8.
+// sort_scratch_bytes(capacity, ...) bytes, cleared by the sort itself unless
+// clearScratch is false, when the caller has already set those bytes to zero;
+// error is a device word that gets kErrLookbackTimeout if a wait ran out.
+// Supported digitBits: 6, 7, 8.
 int sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t *tmpKeys, uint32_t *tmpValues, size_t capacity,
                    uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
-                   void *scratch, uint32_t *error, cudaStream_t stream);
+                   void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch = true);
 int sort_pairs_u64(unsigned long long *keys, uint32_t *values, unsigned long long *tmpKeys, uint32_t *tmpValues,
                    size_t capacity, uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
-                   void *scratch, uint32_t *error, cudaStream_t stream);
+                   void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch = true);
 
 } // namespace sb

@@ -153,6 +153,11 @@ public:
   int digitBits = 8;
   int forwardPixels = 1, backwardPixels = 2; // pixels per thread of the compositing and float backward kernels
   cudaStream_t stream = nullptr;
+  // The step's clears run on a second stream, forked from and joined back to
+  // the first (branches of the same graph when captured).
+  cudaStream_t side = nullptr;
+  cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
+  bool entryScratchClear = false; // the entry sort's scratch was cleared for this step
 
   DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
   DeviceBuffer state[5], grads[5], densifyStats;
@@ -203,8 +208,9 @@ public:
   OptimState optim_state();
   void upload_targets(const uint8_t *const *targets, const size_t *bytes, int count);
   void stage_prefetch();
-  void record_prepare();
+  void record_prepare(bool backward);
   void record_forward();
+  int entry_sort_bits() const;
   void record_backward_and_chain(ChainMode mode, bool statistics);
   void record_readback();
   void begin(int stage);
@@ -259,6 +265,9 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   if (backwardPixels != 1 && backwardPixels != 2)
     throw Failure{SPLAT_ERR_INVALID, "backward_pixels_per_thread must be 1 or 2"};
   SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  SB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  SB_CUDA(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
   for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
 
   const size_t nn = n;
@@ -329,6 +338,9 @@ Trainer::~Trainer() {
   clear_graphs();
   for (auto &e : events)
     if (e != nullptr) cudaEventDestroy(e);
+  if (forkEvent != nullptr) cudaEventDestroy(forkEvent);
+  if (joinEvent != nullptr) cudaEventDestroy(joinEvent);
+  if (side != nullptr) cudaStreamDestroy(side);
   if (stream != nullptr) cudaStreamDestroy(stream);
 }
 
@@ -523,6 +535,7 @@ void Trainer::ensure_entries(uint32_t total) {
   for (int d = 6; d <= 8; ++d) scratch = std::max(scratch, sort_scratch_bytes(cap, (int)keyBytes, std::max<uint32_t>(bits, 32 + 24), d));
   sortScratchEntries.ensure(scratch);
   entryCapacity = (uint32_t)cap;
+  entryScratchClear = false;
   clear_graphs();
 }
 
@@ -569,21 +582,44 @@ void Trainer::end(int stage) {
   if (timing) SB_CUDA(cudaEventRecord(events[2 * stage + 1], stream));
 }
 
-void Trainer::record_prepare() {
+// The entry sort's key bits and digit width for the current views and form.
+int Trainer::entry_sort_bits() const {
+  return oneSort ? 32 + (int)bits_for((uint32_t)views.totalTiles) : (int)bits_for((uint32_t)views.totalTiles);
+}
+
+void Trainer::record_prepare(bool backward) {
   const Params p = params();
   SB_CUDA(cudaMemcpyAsync(dViews.get(), hViews.get(), sizeof(ViewSet), cudaMemcpyHostToDevice, stream));
   SB_CUDA(cudaMemsetAsync(dReadback.get(), 0, sizeof(StepReadback), stream));
   StepReadback *rb = dReadback.get<StepReadback>();
   uint32_t *counters = rb->counters, *error = &rb->error;
+  // What the step clears, cleared on the second stream while the projection
+  // runs: the backward pass's sums (not for a render, which keeps the last
+  // ones for apply_gradients), the tile ranges and both sorts' scratch. The
+  // kernels between the projection and the chain rule then follow one
+  // another with nothing in between.
+  SB_CUDA(cudaEventRecord(forkEvent, stream));
+  SB_CUDA(cudaStreamWaitEvent(side, forkEvent, 0));
+  if (backward) SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, side));
+  SB_CUDA(cudaMemsetAsync(ranges.get(), 0, (size_t)views.totalTiles * 8, side));
+  if (!oneSort) SB_CUDA(cudaMemsetAsync(sortScratchDepth.get(), 0, sort_scratch_bytes(n, 4, 32, digitBits), side));
+  entryScratchClear = entryKeys.get() != nullptr;
+  if (entryScratchClear) {
+    const int bits = entry_sort_bits();
+    SB_CUDA(cudaMemsetAsync(sortScratchEntries.get(), 0,
+                            sort_scratch_bytes(entryCapacity, oneSort ? 8 : 4, bits, entry_digits(bits, digitBits)), side));
+  }
+  SB_CUDA(cudaEventRecord(joinEvent, side));
   begin(0);
   launch_preprocess(p, views, dViews.get<ViewSet>(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
                     oneSort ? nullptr : values.get<uint32_t>(), stream);
   end(0);
+  SB_CUDA(cudaStreamWaitEvent(stream, joinEvent, 0));
   begin(1);
   if (!oneSort) {
     depthInTmp = sort_pairs_u32(depthKeys.get<uint32_t>(), values.get<uint32_t>(), tmpKeys.get<uint32_t>(),
                                 tmpValues.get<uint32_t>(), n, n, nullptr, 0, 32, digitBits, sortScratchDepth.get(), error,
-                                stream) == 1;
+                                stream, false) == 1;
   }
   end(1);
   begin(2);
@@ -607,19 +643,20 @@ void Trainer::record_forward() {
                   offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, entryCapacity,
                   oneSort ? nullptr : entryKeys.get<uint32_t>(),
                   oneSort ? entryKeys.get<unsigned long long>() : nullptr, entryValues.get<uint32_t>(), error, stream);
+  // The scratch was cleared with the step's other clears unless the entry
+  // buffers were (re)made after them.
+  const int bits = entry_sort_bits();
   if (oneSort) {
-    const int bits = 32 + (int)bits_for((uint32_t)views.totalTiles);
     entriesInTmp = sort_pairs_u64(entryKeys.get<unsigned long long>(), entryValues.get<uint32_t>(),
                                   tmpEntryKeys.get<unsigned long long>(), tmpEntryValues.get<uint32_t>(), entryCapacity, 0,
                                   &counters[2], 0, bits, entry_digits(bits, digitBits), sortScratchEntries.get(), error,
-                                  stream) == 1;
+                                  stream, !entryScratchClear) == 1;
   } else {
-    const int bits = (int)bits_for((uint32_t)views.totalTiles);
     entriesInTmp = sort_pairs_u32(entryKeys.get<uint32_t>(), entryValues.get<uint32_t>(), tmpEntryKeys.get<uint32_t>(),
                                   tmpEntryValues.get<uint32_t>(), entryCapacity, 0, &counters[2], 0, bits,
-                                  entry_digits(bits, digitBits), sortScratchEntries.get(), error, stream) == 1;
+                                  entry_digits(bits, digitBits), sortScratchEntries.get(), error, stream,
+                                  !entryScratchClear) == 1;
   }
-  SB_CUDA(cudaMemsetAsync(ranges.get(), 0, (size_t)views.totalTiles * 8, stream));
   const void *keys = entriesInTmp ? tmpEntryKeys.get() : entryKeys.get();
   launch_tile_ranges(oneSort ? nullptr : static_cast<const uint32_t *>(keys),
                      oneSort ? static_cast<const unsigned long long *>(keys) : nullptr, &counters[2], entryCapacity,
@@ -673,7 +710,6 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
               adjoint.get<float4>(), partials.get<float2>(), stream);
   launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, stream);
   end(5);
-  SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, stream));
   RasterConfig cfg;
   cfg.exactMath = exactMath ? 1 : 0;
   cfg.forwardPixels = forwardPixels;
@@ -803,7 +839,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
         cudaGraph_t graph = nullptr;
         SB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         try {
-          record_prepare();
+          record_prepare(true);
           record_forward();
           record_backward_and_chain(mode, statistics);
           record_readback();
@@ -832,7 +868,7 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
     }
     if (!graphDone) throw Failure{SPLAT_ERR_DEVICE, "the entry pool kept overflowing"};
   } else {
-    record_prepare();
+    record_prepare(true);
     // The reference's host wait: read the entry count and size the entry buffers.
     SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
     SB_CUDA(cudaStreamSynchronize(stream));
@@ -965,7 +1001,7 @@ void Trainer::render(const splat_camera *camera, float *out) {
   set_views(camera, 1);
   ensure_view_buffers();
   std::memcpy(hViews.get(), &views, sizeof(ViewSet));
-  record_prepare();
+  record_prepare(false);
   SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
   SB_CUDA(cudaStreamSynchronize(stream));
   const uint32_t total = hReadback.get<StepReadback>()->counters[1];
