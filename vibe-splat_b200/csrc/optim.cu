@@ -31,16 +31,20 @@ constexpr int kMaxCoeffs = 16;
 __device__ __forceinline__ float bf16_load(uint32_t word, int slot) {
   return __uint_as_float(slot == 0 ? word << 16 : word & 0xFFFF0000u);
 }
-__device__ __forceinline__ uint32_t bf16_round(float x) {
-  const uint32_t bits = __float_as_uint(x);
-  return (bits + 0x7FFFu + ((bits >> 16) & 1u)) >> 16;
-}
 __device__ __forceinline__ uint32_t bf16_stochastic(float x, uint32_t index, uint32_t seed) {
   const uint32_t word = pcg_word(index, seed);
   return (__float_as_uint(x) + (((word >> 22u) ^ word) & 0xFFFFu)) >> 16;
 }
-__device__ __forceinline__ uint32_t bf16_store(uint32_t word, int slot, uint32_t bits) {
-  return slot == 0 ? (word & 0xFFFF0000u) | bits : (word & 0xFFFFu) | (bits << 16);
+// The state word of a BF16 pair: m rounded to nearest even in the low half,
+// v rounded at random (as bf16_stochastic) in the high half. The random
+// rounding is done on v's bits first, which leaves a value the conversion
+// keeps exactly; one conversion then rounds m and packs both.
+__device__ __forceinline__ uint32_t bf16_pair(float m, float v, uint32_t index, uint32_t seed) {
+  const uint32_t word = pcg_word(index, seed);
+  const float vRounded = __uint_as_float((__float_as_uint(v) + (((word >> 22u) ^ word) & 0xFFFFu)) & 0xFFFF0000u);
+  uint32_t packed;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(packed) : "f"(vRounded), "f"(m));
+  return packed;
 }
 
 // Half floats rounded at random, in proportion to the distance to each neighbour.
@@ -66,14 +70,15 @@ __device__ __forceinline__ AdamArgs adam_args(const ChainArgs &c) {
 
 __device__ __forceinline__ float sqrt_sfu(float x) {
   float r;
-  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
 
 // Adam on one parameter (step_parameter with radius < 0): the bias
 // corrections as multiplications by their reciprocals, the square root and
 // the step's division on the SFU (the reference's GLSL sqrt and division are
-// not correctly rounded either).
+// not correctly rounded either); the square root flushes subnormal inputs to
+// zero, where the step's denominator is the epsilon either way.
 __device__ __forceinline__ void adam(float &value, float &m, float &v, float g, float rate, const AdamArgs &a) {
   m = a.beta1 * m + (1.0f - a.beta1) * g;
   v = a.beta2 * v + (1.0f - a.beta2) * g * g;
@@ -95,7 +100,7 @@ __device__ __forceinline__ void step_state(float &value, void *state, StateStore
     const uint32_t word = s[at];
     float m = bf16_load(word, 0), v = bf16_load(word, 1);
     adam(value, m, v, g, rate, a);
-    s[at] = bf16_store(bf16_store(word, 0, bf16_round(m)), 1, bf16_stochastic(v, hashIndex, a.seed));
+    s[at] = bf16_pair(m, v, hashIndex, a.seed);
   }
 }
 
@@ -566,8 +571,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
         static_cast<float *>(state.state[4])[t] = m[kk][c];
         static_cast<float *>(state.state[4])[count + t] = vv[kk][c];
       } else {
-        static_cast<uint32_t *>(state.state[4])[t] =
-            bf16_store(bf16_store(word[kk][c], 0, bf16_round(m[kk][c])), 1, bf16_stochastic(vv[kk][c], hashIndex, a.seed));
+        static_cast<uint32_t *>(state.state[4])[t] = bf16_pair(m[kk][c], vv[kk][c], hashIndex, a.seed);
       }
       if (k == 0) {
         p.shDc[t] = value[kk][c];
@@ -612,7 +616,7 @@ __device__ __forceinline__ void store_state(void *st, StateStore store, uint32_t
     static_cast<float *>(st)[at] = m;
     static_cast<float *>(st)[count + at] = v;
   } else {
-    static_cast<uint32_t *>(st)[at] = bf16_store(bf16_store(word, 0, bf16_round(m)), 1, bf16_stochastic(v, hashIndex, seed));
+    static_cast<uint32_t *>(st)[at] = bf16_pair(m, v, hashIndex, seed);
   }
 }
 
@@ -814,7 +818,7 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
       const uint32_t word = s_statew[plane * kStepThreads + tid];
       float m = bf16_load(word, 0), v = bf16_load(word, 1);
       adam(val, m, v, g, rate, a);
-      stateOut[(size_t)plane * ps] = bf16_round(m) | (bf16_stochastic(v, hashBase + plane * 5u, a.seed) << 16);
+      stateOut[(size_t)plane * ps] = bf16_pair(m, v, hashBase + plane * 5u, a.seed);
     }
   };
 #pragma unroll

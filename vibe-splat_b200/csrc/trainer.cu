@@ -158,6 +158,12 @@ public:
   cudaStream_t side = nullptr;
   cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
   bool entryScratchClear = false; // the entry sort's scratch was cleared for this step
+  // The next step's target on its way to the device: copied to pinned memory
+  // and on to targetNext by copyStream while this step runs (copied is
+  // recorded after that copy, consumed after the step that used it took it).
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t copied = nullptr, consumed = nullptr;
+  DeviceBuffer targetNext;
 
   DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
   DeviceBuffer state[5], grads[5], densifyStats;
@@ -208,6 +214,8 @@ public:
   OptimState optim_state();
   void upload_targets(const uint8_t *const *targets, const size_t *bytes, int count);
   void stage_prefetch();
+  void prefetch(const uint8_t *next, size_t bytes);
+  bool take_prefetched(const uint8_t *const *targets, const size_t *bytes, int count);
   void record_prepare(bool backward);
   void record_forward();
   int entry_sort_bits() const;
@@ -268,6 +276,9 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   SB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
   SB_CUDA(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+  SB_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&consumed, cudaEventDisableTiming));
   for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
 
   const size_t nn = n;
@@ -341,6 +352,12 @@ Trainer::~Trainer() {
   if (forkEvent != nullptr) cudaEventDestroy(forkEvent);
   if (joinEvent != nullptr) cudaEventDestroy(joinEvent);
   if (side != nullptr) cudaStreamDestroy(side);
+  if (copyStream != nullptr) {
+    cudaStreamSynchronize(copyStream);
+    cudaStreamDestroy(copyStream);
+  }
+  if (copied != nullptr) cudaEventDestroy(copied);
+  if (consumed != nullptr) cudaEventDestroy(consumed);
   if (stream != nullptr) cudaStreamDestroy(stream);
 }
 
@@ -348,12 +365,14 @@ Trainer::~Trainer() {
 // only that from the old Gaussians).
 void Trainer::release_transient() {
   clear_graphs();
+  SB_CUDA(cudaStreamSynchronize(copyStream)); // a prefetch may still be landing in targetNext
   for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities, &shDc, &shRest, &grads[0], &grads[1], &grads[2], &grads[3],
                           &grads[4], &densifyStats, &splats, &reach, &depthKeys, &values, &tmpKeys, &tmpValues, &offsets, &raw,
                           &shGrad, &entryKeys, &entryValues, &tmpEntryKeys, &tmpEntryValues, &image, &stops, &adjoint, &fields,
-                          &target, &ranges, &partials, &listCounts, &listOffsets, &listPool, &listScratch, &sortScratchDepth,
-                          &sortScratchEntries, &scanScratch})
+                          &target, &targetNext, &ranges, &partials, &listCounts, &listOffsets, &listPool, &listScratch,
+                          &sortScratchDepth, &sortScratchEntries, &scanScratch})
     b->release();
+  prefetched = nullptr;
   entryCapacity = 0;
   viewSlots = 0;
 }
@@ -406,7 +425,7 @@ uint64_t Trainer::entry_bytes(uint64_t entries) const {
 
 uint64_t Trainer::gpu_bytes() const {
   uint64_t total = bytes_per_gaussian() * n;
-  for (const DeviceBuffer *b : {&image, &stops, &adjoint, &fields, &target, &ranges, &partials, &entryKeys, &entryValues,
+  for (const DeviceBuffer *b : {&image, &stops, &adjoint, &fields, &target, &targetNext, &ranges, &partials, &entryKeys, &entryValues,
                                 &tmpEntryKeys, &tmpEntryValues, &sortScratchDepth, &sortScratchEntries, &scanScratch,
                                 &listCounts, &listOffsets, &listPool, &listScratch, &listCounters})
     total += b->bytes();
@@ -539,15 +558,37 @@ void Trainer::ensure_entries(uint32_t total) {
   clear_graphs();
 }
 
-// Copies the target named for the next step into the second pinned buffer;
-// run() calls it once the step's work is queued, so the copy overlaps it.
+// Copies the target named for the next step into the second pinned buffer
+// and from there, on copyStream, into targetNext; run() calls it once the
+// step's work is queued, so both copies overlap the step.
 void Trainer::stage_prefetch() {
   if (pendingPrefetch == nullptr) return;
-  stagingNext.ensure(pendingPrefetchBytes);
-  std::memcpy(stagingNext.get(), pendingPrefetch, pendingPrefetchBytes);
-  prefetched = pendingPrefetch;
-  prefetchedBytes = pendingPrefetchBytes;
+  prefetch(pendingPrefetch, pendingPrefetchBytes);
   pendingPrefetch = nullptr;
+}
+
+void Trainer::prefetch(const uint8_t *next, size_t bytes) {
+  // The last copy out of the pinned buffer has ended, and the step that took
+  // targetNext has copied it away, before either is written again.
+  SB_CUDA(cudaEventSynchronize(copied));
+  SB_CUDA(cudaStreamWaitEvent(copyStream, consumed, 0));
+  stagingNext.ensure(bytes);
+  std::memcpy(stagingNext.get(), next, bytes);
+  targetNext.ensure(bytes);
+  SB_CUDA(cudaMemcpyAsync(targetNext.get(), stagingNext.get(), bytes, cudaMemcpyHostToDevice, copyStream));
+  SB_CUDA(cudaEventRecord(copied, copyStream));
+  prefetched = next;
+  prefetchedBytes = bytes;
+}
+
+// Whether this step's single target is the one prefetched: then it is (or
+// soon will be) in targetNext.
+bool Trainer::take_prefetched(const uint8_t *const *targets, const size_t *bytes, int count) {
+  if (count != 1 || prefetched == nullptr || prefetched != targets[0] || prefetchedBytes != bytes[0]) return false;
+  const size_t want = (size_t)views.v[0].width * views.v[0].height * 4;
+  if (bytes[0] != want) throw Failure{SPLAT_ERR_INVALID, "the target image does not match the camera"};
+  prefetched = nullptr;
+  return true;
 }
 
 void Trainer::upload_targets(const uint8_t *const *targets, const size_t *bytes, int count) {
@@ -557,17 +598,11 @@ void Trainer::upload_targets(const uint8_t *const *targets, const size_t *bytes,
     if (bytes[k] != want || targets[k] == nullptr) throw Failure{SPLAT_ERR_INVALID, "the target image does not match the camera"};
     total += want;
   }
-  if (count == 1 && prefetched == targets[0] && prefetchedBytes == bytes[0]) {
-    // Staged during the previous step.
-    swap(staging, stagingNext);
-    prefetched = nullptr;
-  } else {
-    staging.ensure(total);
-    size_t off = 0;
-    for (int k = 0; k < count; ++k) {
-      std::memcpy(staging.get<uint8_t>() + off, targets[k], bytes[k]);
-      off += bytes[k];
-    }
+  staging.ensure(total);
+  size_t off = 0;
+  for (int k = 0; k < count; ++k) {
+    std::memcpy(staging.get<uint8_t>() + off, targets[k], bytes[k]);
+    off += bytes[k];
   }
 }
 
@@ -825,6 +860,10 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
       SB_CUDA(cudaMemcpyAsync(target.get<uint8_t>() + off, targets[k], want, cudaMemcpyDeviceToDevice, stream));
       off += want;
     }
+  } else if (take_prefetched(targets, bytes, count)) {
+    SB_CUDA(cudaStreamWaitEvent(stream, copied, 0));
+    SB_CUDA(cudaMemcpyAsync(target.get(), targetNext.get(), bytes[0], cudaMemcpyDeviceToDevice, stream));
+    SB_CUDA(cudaEventRecord(consumed, stream));
   } else {
     upload_targets(targets, bytes, count);
     SB_CUDA(cudaMemcpyAsync(target.get(), staging.get(), (size_t)views.totalPixels * 4, cudaMemcpyHostToDevice, stream));
@@ -1219,10 +1258,7 @@ int splat_trainer_prefetch_target(splat_trainer *trainer, const uint8_t *target,
   return guarded([&] {
     Trainer *t = impl_of(trainer);
     if (target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null target"};
-    t->stagingNext.ensure(target_bytes);
-    std::memcpy(t->stagingNext.get(), target, target_bytes);
-    t->prefetched = target;
-    t->prefetchedBytes = target_bytes;
+    t->prefetch(target, target_bytes);
   });
 }
 
