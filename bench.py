@@ -523,9 +523,15 @@ def our_arm(args) -> None:
     # which the library copies to pinned memory while the step runs.
     stream = trainer.stream()
     k = len(cams)
-    e2e_ms = time_steps(torch, trainer, lambda i: trainer.step(cams[i % k], host_targets[i % k], rates,
-                                                               next_target=host_targets[(i + 1) % k]),
-                        args.steps, stream)
+
+    def host_step(i):
+        return trainer.step(cams[i % k], host_targets[i % k], rates, next_target=host_targets[(i + 1) % k])
+
+    # Warm-up through the same call: the first ones allocate the pinned and
+    # device prefetch buffers and have no prefetched target yet.
+    for i in range(args.warmup):
+        host_step(i)
+    e2e_ms = time_steps(torch, trainer, lambda i: host_step(args.warmup + i), args.steps, stream)
     if dist is not None:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
