@@ -49,7 +49,7 @@ struct Params {
 // splats[v n + i], reach[v n + i], depthKeys[v n + i] (kInvisible when culled)
 // and, if values is not null, values[v n + i] = i.
 void launch_preprocess(const Params &p, const ViewSet &views, const ViewSet *dViews, Splat *splats, float *reach, uint32_t *depthKeys,
-                       uint32_t *values, cudaStream_t stream);
+                       uint32_t *values, cudaStream_t stream, uint32_t *error = nullptr);
 
 // train_bin_count.comp + record_scan(coverage): for every item r (a sorted
 // splat in the depth-sorted form, v n + i in the single-sort form) counts the

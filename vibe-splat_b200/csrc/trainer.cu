@@ -647,7 +647,7 @@ void Trainer::record_prepare(bool backward) {
   SB_CUDA(cudaEventRecord(joinEvent, side));
   begin(0);
   launch_preprocess(p, views, dViews.get<ViewSet>(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
-                    oneSort ? nullptr : values.get<uint32_t>(), stream);
+                    oneSort ? nullptr : values.get<uint32_t>(), stream, error);
   end(0);
   SB_CUDA(cudaStreamWaitEvent(stream, joinEvent, 0));
   begin(1);
