@@ -477,6 +477,11 @@ def our_arm(args) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    # The SM pipes' measured throughput: the roofline of the issue-bound kernels.
+    try:
+        sm_peaks = splat.measure_sm_peaks()
+    except Exception:
+        sm_peaks = {}
     pos, sc, rot, op, sh = make_scene(args.gaussians)
     cloud = splat.GaussianCloud(DEGREE, pos, sc, rot, op, sh)
     cams = [splat.Camera(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in hemisphere_views()][: args.views]
@@ -557,10 +562,12 @@ def our_arm(args) -> None:
     digits_used = tuned.get("digit_bits", chosen.digit_bits)
     depth_passes = math.ceil(32 / digits_used)
     algorithmic = stage_bytes(n, visible, entries, pixels, depth_passes)
-    # The SM issue rate: 148 SMs x 4 warp-instructions per clock, at the SM
+    # The SM issue rate: measured by the library's FMA microbenchmark on this
+    # GPU when it ran, else 148 SMs x 4 warp-instructions per clock at the SM
     # clock sampled during the timed steps (the maximum if none was sampled).
     sm_mhz = (clocks.get("sm_mhz") if isinstance(clocks, dict) else None) or 1965.0
-    issue_peak = 148 * 4 * sm_mhz * 1e6
+    issue_peak = sm_peaks.get("warp_instructions") or 148 * 4 * sm_mhz * 1e6
+    issue_source = "measured (splat_measure_sm_peaks)" if sm_peaks.get("warp_instructions") else "148 SMs x 4 per clock"
     stage_roof = {}
     for name, ms_stage in stages.items():
         b = algorithmic.get(name)
@@ -572,7 +579,7 @@ def our_arm(args) -> None:
         if inst:
             rate = inst / (ms_stage * 1e-3)
             stage_roof[name]["issue"] = {"warp_inst_per_s": rate, "peak": issue_peak, "frac": rate / issue_peak,
-                                         "instructions": inst}
+                                         "instructions": inst, "peak_source": issue_source}
     roof = None
     if dominant is not None and dominant in stage_roof:
         r = stage_roof[dominant]
@@ -582,8 +589,8 @@ def our_arm(args) -> None:
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
         if dominant in ("backward", "composite"):
             roof["note"] = ("issue-bound, not HBM-bound: the SM instruction issue rate is the limit; 'issue' gives "
-                            "the kernel's warp-instructions (ncu, profiles/) over its live time against 148 SMs x 4 "
-                            "per clock; the HBM fraction is given for the record")
+                            "the kernel's warp-instructions (ncu, profiles/) over its live time against the measured "
+                            "issue rate (the FMA microbenchmark's); the HBM fraction is given for the record")
             if "issue" in r:
                 roof["issue"] = r["issue"]
 
@@ -642,6 +649,7 @@ def our_arm(args) -> None:
                    "l2": "inputs larger than L2 (1M-Gaussian parameters and state, 64 x 4 MB targets)",
                    "tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "sm_peaks": sm_peaks,
         "roofline": roof,
         "stage_roofline": stage_roof,
         "stages_ms": stages,

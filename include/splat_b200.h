@@ -301,6 +301,21 @@ int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, u
 int splat_radix_sort_u32_noalloc(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, uint32_t *tmp_values,
                                  uint32_t count, int32_t key_bits, int32_t digit_bits, void *stream);
 
+/* Throughput the SM pipes reach on the current GPU, measured by
+ * microbenchmarks that keep one pipe busy on every SM (a few milliseconds in
+ * all): FP32 fused multiply-adds in FLOP/s (two per FMA), the SFU's ex2 in
+ * results/s, conflict-free 16-byte shared-memory loads in bytes/s, and the
+ * warp instructions the FMA benchmark issues per second. These, not HBM, bound
+ * the compositing and backward kernels; the bench reports their issue rates
+ * against them. This entry point has no counterpart in the reference. */
+typedef struct splat_sm_peaks {
+  double fp32_flops;
+  double sfu_ops;
+  double shared_bytes;
+  double warp_instructions;
+} splat_sm_peaks;
+int splat_measure_sm_peaks(splat_sm_peaks *out);
+
 /* Evaluates the deterministic exp and log of splat_detmath.h on the device, for
  * the check that they agree bit for bit with the host. Device pointers. */
 int splat_debug_detmath(const float *in, float *out_exp, float *out_log, uint32_t count);

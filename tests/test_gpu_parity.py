@@ -606,3 +606,16 @@ def test_gradients_against_central_differences(splat, oracle, fixed):
     # Fixed point: the reference's tolerance for its quantised sums (cosine > 0.97, 10%).
     cos, ratio = (0.97, 0.1) if fixed else (0.999, 0.01)
     check_close(ours[smooth], fd[smooth], "parameters vs central differences", cos, ratio)
+
+
+@pytest.mark.gpu
+def test_sm_peaks_are_plausible(splat):
+    # The microbenchmarks behind the issue-bound kernels' roofline: each figure
+    # between a tenth of and twice the B200's nominal rate at its top clock
+    # (148 SMs, 1965 MHz: FP32 74 TFLOP/s, SFU 4.65 T ex2/s, shared memory
+    # 37 TB/s, 4 warp instructions per clock per SM).
+    peaks = splat.measure_sm_peaks()
+    nominal = {"fp32_flops": 148 * 128 * 2 * 1.965e9, "sfu_ops": 148 * 16 * 1.965e9,
+               "shared_bytes": 148 * 128 * 1.965e9, "warp_instructions": 148 * 4 * 1.965e9}
+    for key, value in nominal.items():
+        assert 0.1 * value < peaks[key] < 2.0 * value, (key, peaks[key], value)

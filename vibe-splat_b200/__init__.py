@@ -169,6 +169,14 @@ _lib.splat_radix_sort_u32.argtypes = [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_
 _lib.splat_radix_sort_u64.argtypes = [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, _P]
 _lib.splat_debug_detmath.argtypes = [_P, _P, _P, ctypes.c_uint32]
 
+
+class _SmPeaks(ctypes.Structure):
+    _fields_ = [("fp32_flops", ctypes.c_double), ("sfu_ops", ctypes.c_double), ("shared_bytes", ctypes.c_double),
+                ("warp_instructions", ctypes.c_double)]
+
+
+_lib.splat_measure_sm_peaks.argtypes = [ctypes.POINTER(_SmPeaks)]
+
 # ----------------------------------------------------------------- errors
 
 
@@ -634,6 +642,15 @@ def radix_sort_device(keys_ptr: int, values_ptr: int, tmp_keys_ptr: int, tmp_val
 
 def detmath_device(in_ptr: int, exp_ptr: int, log_ptr: int, count: int) -> None:
     _check(_lib.splat_debug_detmath(_P(in_ptr), _P(exp_ptr), _P(log_ptr), count))
+
+
+def measure_sm_peaks() -> dict:
+    """splat_measure_sm_peaks: FP32 FLOP/s, SFU ex2 results/s, shared-memory
+    bytes/s and warp instructions issued per second, measured on the current GPU."""
+    r = _SmPeaks()
+    _check(_lib.splat_measure_sm_peaks(ctypes.byref(r)))
+    return {"fp32_flops": r.fp32_flops, "sfu_ops": r.sfu_ops, "shared_bytes": r.shared_bytes,
+            "warp_instructions": r.warp_instructions}
 
 
 def library():
