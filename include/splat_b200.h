@@ -167,6 +167,16 @@ int splat_trainer_render(splat_trainer *trainer, const splat_camera *camera, flo
  * gradients stored for splat_trainer_get_gradients. */
 int splat_trainer_compute_gradients(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
                                     size_t target_bytes, splat_step_stats *stats);
+/* Trainer::score_view (trainer.hpp:111, trainer.cpp:521-532): the FastGS
+ * scoring pass. A statistics pass over the view that marks the pixels whose
+ * mean absolute error is at least error_share of the view's worst
+ * (train_loss.comp:101-107, train_error_mask.comp), then adds to each
+ * Gaussian's densification statistics the marked pixels it reached, that count
+ * times the view's loss, and its edge score (the target's luminance Laplacian
+ * times the blending weight), all in pixels times pixel_weight
+ * (train_score.comp). error_share must be above 0; not with blend_lists. */
+int splat_trainer_score_view(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
+                             float error_share, float pixel_weight, splat_step_stats *stats);
 /* Trainer::collect_statistics (trainer.hpp:106). */
 int splat_trainer_collect_statistics(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
                                      size_t target_bytes, splat_step_stats *stats);

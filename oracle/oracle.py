@@ -197,6 +197,22 @@ def ref_contributions(cloud: Cloud, view: View, background=(0.0, 0.0, 0.0), near
     return out
 
 
+def ref_marked_pixels(cloud: Cloud, view: View, target: np.ndarray, share: float, background=(0.0, 0.0, 0.0),
+                      near: float = 0.01) -> np.ndarray:
+    """reference_marked_pixels: per Gaussian, the pixels it reaches whose mean
+    error is at least `share` of the worst (target RGBA8)."""
+    lib = ref_lib()
+    keep, cargs = _cloud_args(cloud)
+    ckeep, camargs = _camera_args(view)
+    out = np.zeros(cloud.count)
+    bg = np.array(background, np.float32)
+    t = np.ascontiguousarray(target, np.uint8)
+    assert lib.ref_marked_pixels(ctypes.c_int(cloud.count), ctypes.c_int(cloud.sh_degree), *cargs, *camargs,
+                                 t.ctypes.data_as(_U8), ctypes.c_double(share), _fp(bg), ctypes.c_float(near),
+                                 _dp(out)) == 0
+    return out
+
+
 def ref_loss(rgb: np.ndarray, width: int, height: int, target: np.ndarray, lam: float):
     """reference_loss: (loss, l1, ssim, adjoint [P,3])."""
     lib = ref_lib()

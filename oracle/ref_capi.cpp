@@ -104,6 +104,25 @@ int ref_contributions(int n, int degree, const float *positions, const float *sc
   }
 }
 
+// reference_marked_pixels (reference.cpp:248-276): per Gaussian, the pixels it
+// reaches whose mean error is at least `share` of the image's worst; target RGBA8.
+int ref_marked_pixels(int n, int degree, const float *positions, const float *scales, const float *rotations,
+                      const float *opacities, const float *sh, const float *view16, const float *position3,
+                      const float *intrinsics4, int width, int height, const std::uint8_t *target, double share,
+                      const float *background, float nearPlane, double *out) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    const Camera camera = make_camera(view16, position3, intrinsics4, width, height);
+    const std::vector<std::uint8_t> t(target, target + static_cast<std::size_t>(width) * height * 4);
+    const std::vector<double> c =
+        reference_marked_pixels(cloud, camera, t, share, make_options(background, nearPlane, 0, 0.f, 0.f, nullptr, n));
+    std::memcpy(out, c.data(), c.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
 // rgb: 3 doubles per pixel; target RGBA8; adjoint out: 3 doubles per pixel; totals out: loss, l1, ssim.
 int ref_loss(int width, int height, const double *rgb, const std::uint8_t *target, double lambda, double *adjoint,
              double *totals) {

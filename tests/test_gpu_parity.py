@@ -619,3 +619,67 @@ def test_sm_peaks_are_plausible(splat):
                "shared_bytes": 148 * 128 * 1.965e9, "warp_instructions": 148 * 4 * 1.965e9}
     for key, value in nominal.items():
         assert 0.1 * value < peaks[key] < 2.0 * value, (key, peaks[key], value)
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+def test_score_view_counts_the_marked_pixels(splat, oracle, fixed):
+    # tests/test_train.cpp:588-621: 72x56, 60 Gaussians degree 1 seed 47,
+    # target seed 43, share 0.5, pixel weight 2; against the reference's
+    # reference_marked_pixels, a pixel either way (the worst error is kept to
+    # 1/65535, which moves the limit a little).
+    view = oracle.train_camera(72, 56)
+    target = oracle.smooth_target(72, 56, 43)
+    cloud = oracle.random_cloud(60, 1, 47)
+    cpu = oracle.ref_marked_pixels(cloud, view, target, 0.5)
+    assert cpu.sum() > 0.0
+    trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=fixed))
+    # An ordinary iteration counts nothing.
+    trainer.compute_gradients(to_camera(view), target)
+    assert np.all(trainer.densify_stats().marked_pixels == 0.0)
+    stats = trainer.score_view(to_camera(view), target, 0.5, 2.0)
+    scored = trainer.densify_stats()
+    np.testing.assert_allclose(scored.marked_pixels, 2.0 * cpu, atol=3.0)
+    np.testing.assert_allclose(scored.marked_loss, 2.0 * cpu * stats.loss, atol=3.0)
+    # Back to counting nothing, and the same again adds up.
+    trainer.compute_gradients(to_camera(view), target)
+    np.testing.assert_array_equal(trainer.densify_stats().marked_pixels, scored.marked_pixels)
+
+
+def test_score_view_accumulates_the_edge_score(splat, oracle):
+    # tests/test_train.cpp:623-659: a vertical edge down the middle of a
+    # 96x64 target (dark left, bright right); eight small Gaussians on it and
+    # eight 24 pixels to its right. The edge score is positive on the edge and
+    # zero away from it; every Gaussian reaches marked pixels (the whole image
+    # is wrong).
+    w, h = 96, 64
+    view = oracle.train_camera(w, h)  # identity pose, focal 60: pixel x = 30 x + 48 at depth 2
+    target = np.full(w * h * 4, 255, np.uint8)
+    for y in range(h):
+        for x in range(w):
+            at = (y * w + x) * 4
+            target[at:at + 3] = 40 if x < w // 2 else 220
+    n = 16
+    positions = np.zeros((n, 3), np.float32)
+    for i in range(n):
+        positions[i] = (0.0 if i < 8 else 0.8, (i % 8 - 3.5) * 0.1, 2.0)
+    scales = np.full((n, 3), np.log(0.02), np.float32)
+    rotations = np.zeros((n, 4), np.float32)
+    rotations[:, 0] = 1.0
+    cloud = splat.GaussianCloud(0, positions.ravel(), scales.ravel(), rotations.ravel(), np.zeros(n, np.float32),
+                                np.zeros(n * 3, np.float32))
+    trainer = splat.Trainer(cloud)
+    trainer.score_view(to_camera(view), target, 0.5, 1.0)
+    scored = trainer.densify_stats()
+    assert scored.edge_score[:8].sum() > 0.0
+    assert scored.edge_score[8:].sum() == 0.0
+    assert np.all(scored.marked_pixels > 0.0)
+
+
+def test_score_view_refuses_bad_arguments(splat, oracle):
+    view = oracle.train_camera(72, 56)
+    target = oracle.smooth_target(72, 56, 43)
+    trainer = splat.Trainer(to_cloud(oracle.random_cloud(60, 1, 47)))
+    with pytest.raises(splat.SplatError):
+        trainer.score_view(to_camera(view), target, 0.0)
+    with pytest.raises(splat.SplatError):
+        trainer.score_view(to_camera(view), target, float("nan"))

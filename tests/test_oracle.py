@@ -169,3 +169,19 @@ def test_golden_fixtures(O):
     from tests.golden.check import check_golden
 
     check_golden(O)
+
+
+@needs_reference
+def test_reference_marked_pixels_count_what_the_image_gets_wrong(O):
+    # reference.cpp:248-276, the expectation of Trainer::score_view's test
+    # (tests/test_train.cpp:588-621): a Gaussian's count is at most the
+    # pixels of the image, every count is whole, a share above 1 marks
+    # nothing and a lower share marks at least as much.
+    view = O.train_camera(72, 56)
+    target = O.smooth_target(72, 56, 43)
+    cloud = O.random_cloud(60, 1, 47)
+    half = O.ref_marked_pixels(cloud, view, target, 0.5)
+    assert half.sum() > 0.0
+    assert np.all(half == np.round(half)) and np.all(half <= 72 * 56)
+    assert O.ref_marked_pixels(cloud, view, target, 1.5).sum() == 0.0
+    assert np.all(O.ref_marked_pixels(cloud, view, target, 0.25) >= half)

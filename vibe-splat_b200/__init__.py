@@ -130,6 +130,8 @@ _lib.splat_trainer_destroy.argtypes = [_P]
 _lib.splat_trainer_render.argtypes = [_P, ctypes.POINTER(_Camera), _FP]
 _lib.splat_trainer_compute_gradients.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Stats)]
 _lib.splat_trainer_collect_statistics.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Stats)]
+_lib.splat_trainer_score_view.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_float,
+                                         ctypes.c_float, ctypes.POINTER(_Stats)]
 _lib.splat_trainer_apply_gradients.argtypes = [_P, ctypes.POINTER(_Rates)]
 _lib.splat_trainer_step.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.POINTER(_Rates), _P,
                                     ctypes.c_size_t, ctypes.POINTER(_Stats)]
@@ -479,6 +481,17 @@ class Trainer:
         t, p, n = _target_ptr(target)
         s = _Stats()
         _check(_lib.splat_trainer_collect_statistics(self._h, ctypes.byref(camera._c()), p, n, ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def score_view(self, camera: Camera, target, error_share: float, pixel_weight: float = 1.0) -> StepStats:
+        """Trainer::score_view: a statistics pass that marks the pixels whose mean
+        error is at least error_share of the view's worst and adds, per Gaussian,
+        the marked pixels it reaches, that count times the loss and its edge
+        score to the densification statistics (in pixels times pixel_weight)."""
+        t, p, n = _target_ptr(target)
+        s = _Stats()
+        _check(_lib.splat_trainer_score_view(self._h, ctypes.byref(camera._c()), p, n, float(error_share),
+                                             float(pixel_weight), ctypes.byref(s)))
         return StepStats._from(s)
 
     def apply_gradients(self, rates: LearningRates) -> None:

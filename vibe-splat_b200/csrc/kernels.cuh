@@ -107,8 +107,19 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
 // partials: 2 floats per global tile (SSIM sum, L1 sum).
 void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
                  cudaStream_t stream);
+// A scored view (Trainer::score_view): with edge not null the loss also leaves
+// each pixel's mean absolute error in the adjoint's alpha, the view's worst
+// error (in 1/65535) in *errorMax (cleared by the caller) and the target's
+// edge weight in edge (one float per pixel).
+struct LossScoring {
+  float *edge = nullptr;
+  uint32_t *errorMax = nullptr;
+};
 void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
-                 float4 *adjoint, float2 *partials, cudaStream_t stream);
+                 float4 *adjoint, float2 *partials, cudaStream_t stream, LossScoring scoring = LossScoring{});
+// train_error_mask.comp over one view's pixels: the adjoint's alpha becomes 1
+// where the error is at least `share` of the worst, else 0.
+void launch_error_mask(float4 *adjoint, uint32_t pixels, const uint32_t *errorMax, float share, cudaStream_t stream);
 // FP64 sums of the per-tile partials into stats (see LossTotals).
 struct LossTotals {
   double ssimSum[kMaxViews];
@@ -118,9 +129,13 @@ void launch_loss_totals(const float2 *partials, const ViewSet &views, const View
 
 // train_backward_{fixed,float}.comp: raw sums, kRawStride per splat per view
 // (int32 fixed point with each view's fixedScale, or float).
+// With edge not null (a scored view, Trainer::score_view) also values 12 and
+// 13: the pixels marked in the adjoint's alpha, and the edge weight (one
+// float per pixel) times the blending weight, each over 3 pixels.
 void launch_backward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
                      const RasterConfig &cfg, const float4 *image, const float4 *adjoint, const uint32_t *stops,
-                     bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream);
+                     bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream,
+                     const float *edge = nullptr);
 // The store-everything backward: float sums from the recorded blend lists.
 void launch_backward_lists(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views,
                            const ViewSet *dViews, const RasterConfig &cfg, const float4 *image, const float4 *adjoint,
@@ -154,6 +169,11 @@ struct OptimState {
 struct GradientsOut {
   float *g[5];         // positions, scales, rotations, opacities, sh (GaussianCloud layout)
 };
+// train_score.comp after a scored view: densifyStats[i * 8 + 5..7] += marked
+// pixels, marked pixels times the loss, edge score (raw values 12 and 13 of n
+// Gaussians, int32 fixed point with fixedScale or float, times toPixels).
+void launch_score(const void *raw, bool fixedPoint, float fixedScale, uint32_t n, float toPixels, float loss, float *densifyStats,
+                  cudaStream_t stream);
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad,
                   float *densifyStats, uint32_t *error, cudaStream_t stream);

@@ -248,9 +248,34 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
   if (threadIdx.x == 0) partials[tile].x = total;
 }
 
+// The target's luminance at (x, y), clamped to the image (train_loss.comp:34-39).
+__device__ __forceinline__ float target_luminance(const uint32_t *target, size_t base, int W, int H, int x, int y) {
+  x = min(max(x, 0), W - 1);
+  y = min(max(y, 0), H - 1);
+  const float3 t = unpack_unorm(target[base + (size_t)y * W + x]);
+  return t.x * 0.299f + t.y * 0.587f + t.z * 0.114f;
+}
+
+// The edge weight of the edge-aware score: a Laplacian of the target's
+// luminance, as differences so that a flat patch gives exactly zero, clamped
+// to [0, 0.999] (train_loss.comp:41-50).
+__device__ __forceinline__ float target_edge(const uint32_t *target, size_t base, int W, int H, int x, int y) {
+  const float centre = target_luminance(target, base, W, H, x, y);
+  const float laplacian = (target_luminance(target, base, W, H, x - 1, y) - centre) +
+                          (target_luminance(target, base, W, H, x + 1, y) - centre) +
+                          (target_luminance(target, base, W, H, x, y - 1) - centre) +
+                          (target_luminance(target, base, W, H, x, y + 1) - centre);
+  return fminf(fmaxf(fabsf(laplacian) / 4.0f, 0.0f), 0.999f);
+}
+
+// SCORE (a scored view, train_loss.comp:101-107): the adjoint's alpha gets the
+// pixel's mean absolute error over its three channels, errorMax the view's
+// worst (in 1/65535), edge the target's edge weight.
+template <bool SCORE>
 __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
                                                       const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
-                                                      float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials) {
+                                                      float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials,
+                                                      LossScoring scoring) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ float s_in[9][kStage]; // the nine field planes
@@ -321,12 +346,34 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   __syncthreads();
   {
     const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
-    if (px < W && py < H)
-      adjoint[base + (size_t)py * W + px] =
-          make_float4(s_result[0][threadIdx.x], s_result[1][threadIdx.x], s_result[2][threadIdx.x], 0.0f);
+    if (px < W && py < H) {
+      const size_t pixel = base + (size_t)py * W + px;
+      float alpha = 0.0f;
+      if constexpr (SCORE) {
+        const float4 x4 = image[pixel];
+        const float3 y3 = unpack_unorm(target[pixel]);
+        const float own3 = fabsf(x4.x - y3.x) + fabsf(x4.y - y3.y) + fabsf(x4.z - y3.z);
+        alpha = own3 / 3.0f;
+        atomicMax(scoring.errorMax, (uint32_t)(fminf(fmaxf(alpha, 0.0f), 1.0f) * 65535.0f));
+        scoring.edge[pixel] = target_edge(target, base, W, H, px, py);
+      }
+      adjoint[pixel] = make_float4(s_result[0][threadIdx.x], s_result[1][threadIdx.x], s_result[2][threadIdx.x], alpha);
+    }
   }
   const float total = block_sum(own, s_warp);
   if (threadIdx.x == 0) partials[tile].y = total;
+}
+
+// train_error_mask.comp: the adjoint's alpha becomes 1 where the pixel's
+// error is at least `share` of the view's worst, else 0.
+__global__ void __launch_bounds__(256) k_error_mask(float4 *__restrict__ adjoint, uint32_t pixels, const uint32_t *__restrict__ errorMax,
+                                                    float share) {
+  chain_enter();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pixels) return;
+  const uint32_t worst = *errorMax;
+  const float error = adjoint[i].w;
+  adjoint[i].w = worst > 0u && error >= share * (float)worst / 65535.0f ? 1.0f : 0.0f;
 }
 
 __global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ partials, const ViewSet *__restrict__ viewsPtr,
@@ -367,10 +414,20 @@ void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &vie
 }
 
 void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
-                 float4 *adjoint, float2 *partials, cudaStream_t stream) {
+                 float4 *adjoint, float2 *partials, cudaStream_t stream, LossScoring scoring) {
   if (views.totalTiles == 0) return;
-  launch_chained(k_loss, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, reinterpret_cast<const float *>(fields), dViews, lambda,
-                                                       adjoint, partials);
+  const float *f = reinterpret_cast<const float *>(fields);
+  if (scoring.edge != nullptr)
+    launch_chained(k_loss<true>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
+                   partials, scoring);
+  else
+    launch_chained(k_loss<false>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
+                   partials, scoring);
+}
+
+void launch_error_mask(float4 *adjoint, uint32_t pixels, const uint32_t *errorMax, float share, cudaStream_t stream) {
+  if (pixels == 0) return;
+  launch_chained(k_error_mask, dim3(div_up(pixels, 256)), dim3(256), 0, stream, adjoint, pixels, errorMax, share);
 }
 
 void launch_loss_totals(const float2 *partials, const ViewSet &views, const ViewSet *dViews, LossTotals *totals, cudaStream_t stream) {

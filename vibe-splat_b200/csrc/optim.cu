@@ -846,6 +846,24 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   }
 }
 
+// train_score.comp: to each Gaussian's statistics, the marked pixels it
+// reached (raw value 12, in pixels), that count times the view's loss, and its
+// edge score (raw value 13, in pixels).
+__global__ void __launch_bounds__(256) k_score(const void *__restrict__ rawIn, bool fixedPoint, float fixedScale, uint32_t n,
+                                               float toPixels, float loss, float *__restrict__ densifyStats) {
+  chain_enter();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t *words = static_cast<const uint32_t *>(rawIn) + (size_t)i * kRawStride;
+  const float marked = fixedPoint ? (float)(int)words[12] / fixedScale : __uint_as_float(words[12]);
+  const float edge = fixedPoint ? (float)(int)words[13] / fixedScale : __uint_as_float(words[13]);
+  float *st = densifyStats + (size_t)i * kStatStride;
+  const float pixels = marked * toPixels;
+  st[5] += pixels;
+  st[6] += pixels * loss;
+  st[7] += edge * toPixels;
+}
+
 template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                     const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
@@ -891,6 +909,12 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
 }
 
 } // namespace
+
+void launch_score(const void *raw, bool fixedPoint, float fixedScale, uint32_t n, float toPixels, float loss, float *densifyStats,
+                  cudaStream_t stream) {
+  if (n == 0) return;
+  launch_chained(k_score, dim3(div_up(n, 256)), dim3(256), 0, stream, raw, fixedPoint, fixedScale, n, toPixels, loss, densifyStats);
+}
 
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,

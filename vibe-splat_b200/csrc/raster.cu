@@ -285,20 +285,39 @@ __device__ __forceinline__ float butterfly12(float v[12]) {
   SB_HALVE(2, 8)
   SB_HALVE(4, 4)
   SB_HALVE(8, 2)
-#undef SB_HALVE
   return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 16);
 }
 
-template <class M, bool FIXED>
+// The same over all 16 values (a scored view's 14, padded with zeros as the
+// reference pads them): lane l (< 16) ends up with the warp total of value
+// bitreverse4(l); the totals of values 0-11 are those of butterfly12.
+__device__ __forceinline__ float butterfly16(float v[16]) {
+  const uint32_t lane = threadIdx.x & 31u;
+  SB_HALVE(1, 16)
+  SB_HALVE(2, 8)
+  SB_HALVE(4, 4)
+  SB_HALVE(8, 2)
+  return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 16);
+}
+#undef SB_HALVE
+
+// SCORE (a scored view): also values 12 and 13, the pixels marked as high
+// error in the adjoint's alpha and the edge weight times the blending weight,
+// each over 3 pixels of the image (train_backward.glsl:125-126).
+template <bool SCORE> __host__ __device__ constexpr int score_values() { return SCORE ? kGradValues + 2 : kGradValues; }
+template <bool SCORE> __host__ __device__ constexpr int score_stride() { return SCORE ? kGradValues + 3 : kAccStride; }
+
+template <class M, bool FIXED, bool SCORE>
 __global__ void __launch_bounds__(kTilePixels, 4)
     k_backward(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, void *__restrict__ rawOut,
-               uint32_t splatLimit, uint32_t *error) {
+               uint32_t splatLimit, uint32_t *error, const float *__restrict__ edge) {
   chain_enter();
+  constexpr int kValues = score_values<SCORE>(), kStride = score_stride<SCORE>();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
-  __shared__ uint32_t s_acc[kBatch * kAccStride];
+  __shared__ uint32_t s_acc[kBatch * kStride];
   __shared__ uint32_t s_min[kTilePixels / 32];
   __shared__ uint32_t s_cover[kTilePixels / 32][kBatch / 32];
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
@@ -313,13 +332,14 @@ __global__ void __launch_bounds__(kTilePixels, 4)
   const size_t at = inside ? (size_t)cam.pixelBase + (size_t)y * cam.width + x : 0;
   const float logTotal = inside ? image[at].w : 0.0f;
   float4 A = inside ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float edgeWeight = SCORE && inside ? edge[at] : 0.0f;
   const float perPixel = cam.perPixel;
   const float scale = cam.fixedScale;
   const uint2 range = ranges[tile];
   const uint32_t stop = inside ? stops[at] : range.y;
   const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, stop);
   if (lane == 0) s_min[t >> 5] = warpMin;
-  for (int i = t; i < kBatch * kAccStride; i += kTilePixels) s_acc[i] = 0u;
+  for (int i = t; i < kBatch * kStride; i += kTilePixels) s_acc[i] = 0u;
   __syncthreads();
   uint32_t tileStop = s_min[0];
 #pragma unroll
@@ -365,7 +385,12 @@ __global__ void __launch_bounds__(kTilePixels, 4)
       const float logRest = M::log(1.0f - aAct);
       const float T = M::exp((logTotal - logBehind) - logRest);
       const float wA = act ? T * alpha : 0.0f;
-      float g[12];
+      float g[SCORE ? 16 : 12];
+      if constexpr (SCORE) {
+        g[12] = act ? A.w * perPixel : 0.0f;
+        g[13] = edgeWeight * wA * perPixel;
+        g[14] = g[15] = 0.0f;
+      }
       g[6] = wA * A.x;
       g[7] = wA * A.y;
       g[8] = wA * A.z;
@@ -387,9 +412,11 @@ __global__ void __launch_bounds__(kTilePixels, 4)
       Bg = fmaf(aAct, s.g - Bg, Bg);
       Bb = fmaf(aAct, s.b - Bb, Bb);
       logBehind = logBehind + logRest;
-      const float total = butterfly12(g);
-      if (lane < 16 && held < (uint32_t)kGradValues && total != 0.0f) {
-        uint32_t *slot = &s_acc[k * kAccStride + held];
+      float total;
+      if constexpr (SCORE) total = butterfly16(g);
+      else total = butterfly12(g);
+      if (lane < 16 && held < (uint32_t)kValues && total != 0.0f) {
+        uint32_t *slot = &s_acc[k * kStride + held];
         if (FIXED) {
           atomicAdd(reinterpret_cast<int *>(slot), __float2int_rn(fminf(fmaxf(total * scale, -1.0e9f), 1.0e9f)));
         } else {
@@ -402,15 +429,15 @@ __global__ void __launch_bounds__(kTilePixels, 4)
     if (t < count && s_batch[t].mask != 0u) {
       const size_t base = ((size_t)s_batch[t].index) * kRawStride;
 #pragma unroll
-      for (int j = 0; j < kGradValues; ++j) {
-        const uint32_t v = s_acc[t * kAccStride + j];
+      for (int j = 0; j < kValues; ++j) {
+        const uint32_t v = s_acc[t * kStride + j];
         if (v != 0u) {
           if (FIXED) {
             atomicAdd(reinterpret_cast<int *>(raw32 + base + j), (int)v);
           } else {
             atomicAdd(reinterpret_cast<float *>(raw32 + base + j), __uint_as_float(v));
           }
-          s_acc[t * kAccStride + j] = 0u;
+          s_acc[t * kStride + j] = 0u;
         }
       }
     }
@@ -691,16 +718,17 @@ __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restri
 }
 
 // Float sums only: each lane adds its two pixels' values before one butterfly.
-template <class M>
+template <class M, bool SCORE>
 __global__ void __launch_bounds__(kHalfTile, 6)
     k_backward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
                 const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                 const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
-                uint32_t splatLimit, uint32_t *error) {
+                uint32_t splatLimit, uint32_t *error, const float *__restrict__ edge) {
   chain_enter();
+  constexpr int kValues = score_values<SCORE>(), kStride = score_stride<SCORE>();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[kBatch];
-  __shared__ float s_acc[kBatch * kAccStride];
+  __shared__ float s_acc[kBatch * kStride];
   __shared__ uint32_t s_min[kHalfTile / 32];
   __shared__ uint32_t s_cover[kHalfTile / 32][kBatch / 32];
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
@@ -714,7 +742,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   // walked (those behind), kept as one running value. behind: the adjoint
   // dotted with the colour the splats behind (and the background) give, the
   // one thing of that colour the alpha gradient needs.
-  float front[2], Ax[2], Ay[2], Az[2], behind[2];
+  float front[2], Ax[2], Ay[2], Az[2], behind[2], marked[2], edgeWeight[2];
   uint32_t stop[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
@@ -726,11 +754,13 @@ __global__ void __launch_bounds__(kHalfTile, 6)
     Az[q] = a.z;
     stop[q] = pp.inside[q] ? stops[at] : range.y;
     behind[q] = fmaf(a.z, bgB, fmaf(a.y, bgG, a.x * bgR));
+    marked[q] = a.w;
+    edgeWeight[q] = SCORE && pp.inside[q] ? edge[at] : 0.0f;
   }
   const float perPixel = cam.perPixel;
   const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
   if (lane == 0) s_min[t >> 5] = warpMin;
-  for (int i = t; i < kBatch * kAccStride; i += kHalfTile) s_acc[i] = 0.0f;
+  for (int i = t; i < kBatch * kStride; i += kHalfTile) s_acc[i] = 0.0f;
   __syncthreads();
   uint32_t tileStop = s_min[0];
 #pragma unroll
@@ -760,9 +790,9 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         act[q] = start + k >= stop[q] && (mask & pp.bits[q]) == pp.bits[q] && !(power > 0.0f) && alpha[q] >= kAlphaMin;
       }
       if (!__any_sync(0xFFFFFFFFu, act[0] || act[1])) continue;
-      float g[12];
+      float g[SCORE ? 16 : 12];
 #pragma unroll
-      for (int j = 0; j < 12; ++j) g[j] = 0.0f;
+      for (int j = 0; j < (SCORE ? 16 : 12); ++j) g[j] = 0.0f;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const float aAct = act[q] ? alpha[q] : 0.0f;
@@ -774,6 +804,10 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         g[7] = fmaf(wA, Ay[q], g[7]);
         g[8] = fmaf(wA, Az[q], g[8]);
         g[9] = fmaf(wA, perPixel, g[9]);
+        if constexpr (SCORE) {
+          g[12] = fmaf(act[q] ? marked[q] : 0.0f, perPixel, g[12]);
+          g[13] = fmaf(edgeWeight[q] * wA, perPixel, g[13]);
+        }
         const float ahead = fmaf(Az[q], s.b, fmaf(Ay[q], s.g, Ax[q] * s.r)) - behind[q];
         const float dAlpha = (act[q] && oe[q] < kAlphaMax) ? T * ahead : 0.0f;
         g[0] = fmaf(dAlpha, ep[q], g[0]);
@@ -791,8 +825,10 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         behind[q] = fmaf(aAct, ahead, behind[q]);
         front[q] = front[q] - logRest;
       }
-      const float total = butterfly12(g);
-      if (lane < 16 && held < (uint32_t)kGradValues && total != 0.0f) atomicAdd(&s_acc[k * kAccStride + held], total);
+      float total;
+      if constexpr (SCORE) total = butterfly16(g);
+      else total = butterfly12(g);
+      if (lane < 16 && held < (uint32_t)kValues && total != 0.0f) atomicAdd(&s_acc[k * kStride + held], total);
     }
     __syncthreads();
     // One global atomic per (splat, value) for the whole tile.
@@ -800,11 +836,11 @@ __global__ void __launch_bounds__(kHalfTile, 6)
       if (s_batch[j].mask == 0u) continue;
       float *dst = raw + (size_t)s_batch[j].index * kRawStride;
 #pragma unroll
-      for (int v = 0; v < kGradValues; ++v) {
-        const float x = s_acc[j * kAccStride + v];
+      for (int v = 0; v < kValues; ++v) {
+        const float x = s_acc[j * kStride + v];
         if (x != 0.0f) {
           atomicAdd(dst + v, v >= 3 && v <= 5 ? 0.5f * x : x);
-          s_acc[j * kAccStride + v] = 0.0f;
+          s_acc[j * kStride + v] = 0.0f;
         }
       }
     }
@@ -851,31 +887,41 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
 
 void launch_backward(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
                      const RasterConfig &cfg, const float4 *image, const float4 *adjoint, const uint32_t *stops,
-                     bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream) {
+                     bool fixedPoint, void *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream, const float *edge) {
   if (views.totalTiles == 0) return;
   const float r = cfg.background[0], g = cfg.background[1], b = cfg.background[2];
   const uint32_t tiles = views.totalTiles;
+  const bool score = edge != nullptr;
   // The fixed-point sums keep the reference's 32-lane groups: one pixel per thread.
   if (!fixedPoint && cfg.backwardPixels == 2) {
     float *rawF = static_cast<float *>(raw);
-    if (cfg.exactMath)
-      launch_chained(k_backward2<ExactMath>, dim3(tiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
-                                                             rawF, splatLimit, error);
-    else
-      launch_chained(k_backward2<FastMath>, dim3(tiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops,
-                                                            rawF, splatLimit, error);
+#define SB_BACKWARD2(MATH, SCORE)                                                                                       \
+  launch_chained(k_backward2<MATH, SCORE>, dim3(tiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, \
+                 image, adjoint, stops, rawF, splatLimit, error, edge)
+    if (cfg.exactMath) {
+      if (score) SB_BACKWARD2(ExactMath, true);
+      else SB_BACKWARD2(ExactMath, false);
+    } else {
+      if (score) SB_BACKWARD2(FastMath, true);
+      else SB_BACKWARD2(FastMath, false);
+    }
+#undef SB_BACKWARD2
     return;
   }
-#define SB_BACKWARD(MATH, FIX) \
-  launch_chained(k_backward<MATH, FIX>, dim3(tiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, adjoint, stops, \
-                                                          raw, splatLimit, error)
-  if (cfg.exactMath) {
-    if (fixedPoint) SB_BACKWARD(ExactMath, true);
-    else SB_BACKWARD(ExactMath, false);
-  } else {
-    if (fixedPoint) SB_BACKWARD(FastMath, true);
-    else SB_BACKWARD(FastMath, false);
+#define SB_BACKWARD(MATH, FIX, SCORE)                                                                                   \
+  launch_chained(k_backward<MATH, FIX, SCORE>, dim3(tiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, \
+                 b, image, adjoint, stops, raw, splatLimit, error, edge)
+#define SB_BACKWARD_FIX(MATH, FIX)           \
+  {                                          \
+    if (score) SB_BACKWARD(MATH, FIX, true);  \
+    else SB_BACKWARD(MATH, FIX, false);       \
   }
+  if (cfg.exactMath) {
+    if (fixedPoint) SB_BACKWARD_FIX(ExactMath, true) else SB_BACKWARD_FIX(ExactMath, false)
+  } else {
+    if (fixedPoint) SB_BACKWARD_FIX(FastMath, true) else SB_BACKWARD_FIX(FastMath, false)
+  }
+#undef SB_BACKWARD_FIX
 #undef SB_BACKWARD
 }
 

@@ -164,6 +164,10 @@ public:
   cudaStream_t copyStream = nullptr;
   cudaEvent_t copied = nullptr, consumed = nullptr;
   DeviceBuffer targetNext;
+  // A scored view (score_view): above 0, the share of the worst error that
+  // marks a pixel; the target's edge weights and the worst error.
+  float scoreShare = 0.0f;
+  DeviceBuffer scoreEdge, scoreMax;
 
   DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
   DeviceBuffer state[5], grads[5], densifyStats;
@@ -225,6 +229,8 @@ public:
   void end(int stage);
   void clear_graphs();
   void release_transient();
+  void score_view(const splat_camera *camera, const uint8_t *target, size_t bytes, float share, float pixelWeight,
+                  splat_step_stats *stats);
   std::string graph_key(ChainMode mode, bool statistics) const;
   void run(const splat_camera *cameras, const uint8_t *const *targets, const size_t *bytes, int count, ChainMode mode,
            const splat_learning_rates *rates, bool statistics, splat_step_stats *stats, bool deviceTargets = false);
@@ -370,7 +376,7 @@ void Trainer::release_transient() {
                           &grads[4], &densifyStats, &splats, &reach, &depthKeys, &values, &tmpKeys, &tmpValues, &offsets, &raw,
                           &shGrad, &entryKeys, &entryValues, &tmpEntryKeys, &tmpEntryValues, &image, &stops, &adjoint, &fields,
                           &target, &targetNext, &ranges, &partials, &listCounts, &listOffsets, &listPool, &listScratch,
-                          &sortScratchDepth, &sortScratchEntries, &scanScratch})
+                          &sortScratchDepth, &sortScratchEntries, &scanScratch, &scoreEdge, &scoreMax})
     b->release();
   prefetched = nullptr;
   entryCapacity = 0;
@@ -421,6 +427,33 @@ uint64_t Trainer::bytes_per_gaussian() const {
 uint64_t Trainer::entry_bytes(uint64_t entries) const {
   // Keys and values with their copies, plus the sort's look-back words.
   return entries * ((oneSort ? 16 : 8) + 8) + entries / 16;
+}
+
+// Trainer::score_view (trainer.cpp:521-532): a statistics pass over the view
+// with the high-error pixels marked and the target's edge weights kept, then
+// the marked-pixel count, that count times the view's loss and the edge score
+// added to each Gaussian's statistics, in pixels times pixelWeight.
+void Trainer::score_view(const splat_camera *camera, const uint8_t *targetImage, size_t bytes, float share, float pixelWeight,
+                         splat_step_stats *stats) {
+  if (!(share > 0.0f) || !std::isfinite(share)) throw Failure{SPLAT_ERR_INVALID, "error_share must be above 0"};
+  if (!std::isfinite(pixelWeight)) throw Failure{SPLAT_ERR_INVALID, "pixel_weight must be finite"};
+  if (blendLists) throw Failure{SPLAT_ERR_UNSUPPORTED, "scoring a view does not run with blend lists"};
+  splat_step_stats own{};
+  const uint8_t *targets[1] = {targetImage};
+  const size_t sizes[1] = {bytes};
+  scoreShare = share;
+  try {
+    run(camera, targets, sizes, 1, ChainMode::Statistics, nullptr, true, &own);
+  } catch (...) {
+    scoreShare = 0.0f;
+    throw;
+  }
+  scoreShare = 0.0f;
+  // The raw sums are over 3 pixels of the image, like the derivatives.
+  const float toPixels = 3.0f * (float)camera->width * (float)camera->height * pixelWeight;
+  launch_score(raw.get(), fixedPoint, views.v[0].fixedScale, n, toPixels, (float)own.loss, densifyStats.get<float>(), stream);
+  SB_CUDA(cudaStreamSynchronize(stream));
+  if (stats != nullptr) *stats = own;
 }
 
 uint64_t Trainer::gpu_bytes() const {
@@ -741,8 +774,18 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   begin(5);
   launch_ssim(image.get<float4>(), target.get<uint32_t>(), views, dViews.get<ViewSet>(), fields.get<float4>(),
               partials.get<float2>(), stream);
+  LossScoring scoring;
+  if (scoreShare > 0.0f) {
+    scoreEdge.ensure((size_t)views.totalPixels * 4);
+    scoreMax.ensure(4);
+    SB_CUDA(cudaMemsetAsync(scoreMax.get(), 0, 4, stream));
+    scoring.edge = scoreEdge.get<float>();
+    scoring.errorMax = scoreMax.get<uint32_t>();
+  }
   launch_loss(image.get<float4>(), target.get<uint32_t>(), fields.get<float4>(), views, dViews.get<ViewSet>(), opt.lambda_ssim,
-              adjoint.get<float4>(), partials.get<float2>(), stream);
+              adjoint.get<float4>(), partials.get<float2>(), stream, scoring);
+  if (scoreShare > 0.0f)
+    launch_error_mask(adjoint.get<float4>(), (uint32_t)views.totalPixels, scoreMax.get<uint32_t>(), scoreShare, stream);
   launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, stream);
   end(5);
   RasterConfig cfg;
@@ -763,7 +806,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   } else {
     launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
                     adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
-                    stream);
+                    stream, scoreShare > 0.0f ? scoreEdge.get<float>() : nullptr);
   }
   end(6);
   ChainArgs args{};
@@ -870,7 +913,8 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
   }
 
   bool graphDone = false;
-  if (useGraph && !blendLists && entryKeys.get() != nullptr && !timing) {
+  // A scored view runs the plain form (it is rare, and its loss and backward differ).
+  if (useGraph && !blendLists && entryKeys.get() != nullptr && !timing && scoreShare <= 0.0f) {
     for (int attempt = 0; attempt < 3 && !graphDone; ++attempt) {
       const std::string key = graph_key(mode, statistics);
       auto it = graphs.find(key);
@@ -1191,6 +1235,14 @@ int splat_trainer_compute_gradients(splat_trainer *trainer, const splat_camera *
 int splat_trainer_collect_statistics(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
                                      size_t target_bytes, splat_step_stats *stats) {
   return run_one(trainer, camera, target, target_bytes, sb::ChainMode::Statistics, nullptr, true, stats);
+}
+
+int splat_trainer_score_view(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
+                             float error_share, float pixel_weight, splat_step_stats *stats) {
+  return guarded([&] {
+    if (camera == nullptr || target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    impl_of(trainer)->score_view(camera, target, target_bytes, error_share, pixel_weight, stats);
+  });
 }
 
 int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_rates *rates) {
