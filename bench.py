@@ -543,6 +543,14 @@ def our_arm(args) -> None:
         e2e_ms = float(t.item())
     e2e = world * 1000.0 * args.steps / e2e_ms
 
+    # The FastGS scoring pass (score_view: a statistics pass with the
+    # high-error pixels marked, plus the score kernel), host target, plain form.
+    for i in range(2):
+        trainer.score_view(cams[i % k], host_targets[i % k], 0.5)
+    score_ms = time_steps(torch, trainer, lambda i: trainer.score_view(cams[i % k], host_targets[i % k], 0.5),
+                          max(3, min(args.steps, 10)), stream) / max(3, min(args.steps, 10))
+    trainer.reset_densify_stats()
+
     # Per-stage device times (serialising events, plain launches) for the roofline.
     trainer.set_timing(True)
     for i in range(max(3, min(args.steps, 10))):
@@ -650,6 +658,7 @@ def our_arm(args) -> None:
                    "tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "sm_peaks": sm_peaks,
+        "score_view_ms": score_ms,
         "roofline": roof,
         "stage_roofline": stage_roof,
         "stages_ms": stages,
