@@ -30,8 +30,8 @@
  *   - A handle is used by one thread at a time, as the reference's Trainer.
  * Options the reference has but this library has no kernel for (the Mip
  * filters, SH dropout, second-order steps, pose gradients, position noise,
- * exposure, scoring) are refused with SPLAT_ERR_UNSUPPORTED; nothing falls
- * back to the CPU.
+ * exposure) are refused with SPLAT_ERR_UNSUPPORTED; nothing falls back to the
+ * CPU.
  */
 #ifndef SPLAT_B200_H
 #define SPLAT_B200_H
@@ -278,6 +278,21 @@ int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint6
  * to 128). Copies min(bytes, size) bytes; *size gets the
  * buffer's size in bytes. */
 int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size);
+
+/* 3DGS .ply files (src/splat/gaussian_cloud.hpp:60-67, load_ply and
+ * save_ply), host memory only. splat_cloud_load_ply reads a binary
+ * little-endian or ASCII file (properties a cloud has no use for, such as
+ * normals, are skipped; the SH degree follows from the number of f_rest_*
+ * properties: 0, 9, 24 or 45). With every array null it reads only the header
+ * and sets *count and *sh_degree; then call it again with arrays of 3, 3, 4, 1
+ * and 3 (degree + 1)^2 floats per Gaussian. A file that cannot be read or is
+ * not a splat file returns SPLAT_ERR_INVALID with the reason, as the
+ * reference's std::runtime_error. splat_cloud_save_ply writes the standard
+ * binary little-endian layout (x y z, zero normals, f_dc, f_rest channel-major,
+ * opacity, scales, rotations). */
+int splat_cloud_load_ply(const char *path, int32_t *count, int32_t *sh_degree, float *positions, float *scales,
+                         float *rotations, float *opacities, float *sh);
+int splat_cloud_save_ply(const char *path, const splat_cloud *cloud);
 
 /* Stage-level entry points on device memory, for the reference's operator
  * tests (tests/test_radix_sort.cpp) and for callers with their own buffers. */

@@ -197,6 +197,24 @@ def ref_contributions(cloud: Cloud, view: View, background=(0.0, 0.0, 0.0), near
     return out
 
 
+def ref_save_ply(cloud: Cloud, path) -> None:
+    """The reference's save_ply (gaussian_cloud.cpp:330-365)."""
+    keep, cargs = _cloud_args(cloud)
+    assert ref_lib().ref_save_ply(str(path).encode(), ctypes.c_int(cloud.count), ctypes.c_int(cloud.sh_degree), *cargs) == 0
+
+
+def ref_load_ply(path) -> Cloud:
+    """The reference's load_ply (gaussian_cloud.cpp:236-328); raises ValueError
+    where it throws."""
+    lib = ref_lib()
+    n, d = ctypes.c_int(), ctypes.c_int()
+    if lib.ref_load_ply(str(path).encode(), ctypes.byref(n), ctypes.byref(d), None, None, None, None, None) != 0:
+        raise ValueError(f"the reference's load_ply refused {path}")
+    arrays = [np.zeros(n.value * k, np.float32) for k in (3, 3, 4, 1, 3 * (d.value + 1) ** 2)]
+    assert lib.ref_load_ply(str(path).encode(), ctypes.byref(n), ctypes.byref(d), *[_fp(a) for a in arrays]) == 0
+    return Cloud(d.value, *arrays)
+
+
 def ref_marked_pixels(cloud: Cloud, view: View, target: np.ndarray, share: float, background=(0.0, 0.0, 0.0),
                       near: float = 0.01) -> np.ndarray:
     """reference_marked_pixels: per Gaussian, the pixels it reaches whose mean

@@ -104,6 +104,38 @@ int ref_contributions(int n, int degree, const float *positions, const float *sc
   }
 }
 
+// save_ply (gaussian_cloud.cpp:330-365): the reference's writer.
+int ref_save_ply(const char *path, int n, int degree, const float *positions, const float *scales, const float *rotations,
+                 const float *opacities, const float *sh) {
+  try {
+    save_ply(make_cloud(n, degree, positions, scales, rotations, opacities, sh), path);
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// load_ply (gaussian_cloud.cpp:236-328): the reference's reader. With null
+// arrays only the count and degree; then again with arrays sized for them.
+int ref_load_ply(const char *path, int *n, int *degree, float *positions, float *scales, float *rotations, float *opacities,
+                 float *sh) {
+  try {
+    const GaussianCloud c = load_ply(path);
+    *n = static_cast<int>(c.size());
+    *degree = c.shDegree;
+    if (positions != nullptr) {
+      std::memcpy(positions, c.positions.data(), c.positions.size() * sizeof(float));
+      std::memcpy(scales, c.scales.data(), c.scales.size() * sizeof(float));
+      std::memcpy(rotations, c.rotations.data(), c.rotations.size() * sizeof(float));
+      std::memcpy(opacities, c.opacities.data(), c.opacities.size() * sizeof(float));
+      std::memcpy(sh, c.sh.data(), c.sh.size() * sizeof(float));
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
 // reference_marked_pixels (reference.cpp:248-276): per Gaussian, the pixels it
 // reaches whose mean error is at least `share` of the image's worst; target RGBA8.
 int ref_marked_pixels(int n, int degree, const float *positions, const float *scales, const float *rotations,

@@ -178,6 +178,9 @@ class _SmPeaks(ctypes.Structure):
 
 
 _lib.splat_measure_sm_peaks.argtypes = [ctypes.POINTER(_SmPeaks)]
+_lib.splat_cloud_load_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                      _FP, _FP, _FP, _FP, _FP]
+_lib.splat_cloud_save_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(_Cloud)]
 
 # ----------------------------------------------------------------- errors
 
@@ -655,6 +658,23 @@ def radix_sort_device(keys_ptr: int, values_ptr: int, tmp_keys_ptr: int, tmp_val
 
 def detmath_device(in_ptr: int, exp_ptr: int, log_ptr: int, count: int) -> None:
     _check(_lib.splat_debug_detmath(_P(in_ptr), _P(exp_ptr), _P(log_ptr), count))
+
+
+def load_ply(path) -> GaussianCloud:
+    """load_ply: a 3DGS .ply (binary little-endian or ASCII) as a GaussianCloud."""
+    name = str(path).encode()
+    count, degree = ctypes.c_int32(), ctypes.c_int32()
+    _check(_lib.splat_cloud_load_ply(name, ctypes.byref(count), ctypes.byref(degree), None, None, None, None, None))
+    n, d = count.value, degree.value
+    arrays = [np.empty(n * k, np.float32) for k in (3, 3, 4, 1, 3 * (d + 1) ** 2)]
+    _check(_lib.splat_cloud_load_ply(name, ctypes.byref(count), ctypes.byref(degree), *[_fptr(a) for a in arrays]))
+    return GaussianCloud(d, *arrays)
+
+
+def save_ply(cloud: GaussianCloud, path) -> None:
+    """save_ply: the standard binary little-endian 3DGS layout."""
+    c, keep = cloud._c()
+    _check(_lib.splat_cloud_save_ply(str(path).encode(), ctypes.byref(c)))
 
 
 def measure_sm_peaks() -> dict:
