@@ -229,6 +229,33 @@ int splat_trainer_reset_opacity(splat_trainer *trainer, float maximum);
  * the old trainer's other buffers are freed before the new ones are made. */
 int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud, const int32_t *source);
 
+/* Trainer::remove_largest_gaussians, remove_least_contributing_gaussians,
+ * remove_least_opaque_gaussians (trainer.hpp:174-183, trainer.cpp:731-747;
+ * remove_largest, remove_least_contributing, remove_least_opaque of
+ * densify.cpp:70-113): removes ceil(share * count) Gaussians, at most
+ * count - 1, the highest first by their largest log-scale, by minus their
+ * contribution (densification statistics column 3) or by minus their opacity
+ * logit, ties in index order. The survivors keep their order, parameters and
+ * optimiser state; the densification statistics start anew. On the GPU: the
+ * keys, a stable radix sort, a scan and gathers; nothing goes through the host.
+ * share in [0, 1]; *removed gets the count (may be null). */
+int splat_trainer_remove_largest(splat_trainer *trainer, double share, uint64_t *removed);
+int splat_trainer_remove_least_contributing(splat_trainer *trainer, double share, uint64_t *removed);
+int splat_trainer_remove_least_opaque(splat_trainer *trainer, double share, uint64_t *removed);
+
+/* Trainer methods with no kernel in this library, for callers that set them
+ * unconditionally: the neutral setting is accepted and changes nothing, any
+ * other returns SPLAT_ERR_UNSUPPORTED. set_exposure (trainer.hpp:154): the
+ * identity rows {1,0,0,0, 0,1,0,0, 0,0,1,0}; set_sh_dropout: probability 0;
+ * set_filter3d: count 0; add_position_noise: scaler 0; enable_second_order and
+ * update_curvature: never accepted. */
+int splat_trainer_set_exposure(splat_trainer *trainer, const float exposure[12]);
+int splat_trainer_set_sh_dropout(splat_trainer *trainer, float probability, int32_t retained_degree, uint32_t seed);
+int splat_trainer_set_filter3d(splat_trainer *trainer, const float *filter, size_t count);
+int splat_trainer_add_position_noise(splat_trainer *trainer, float scaler, uint32_t iteration);
+int splat_trainer_enable_second_order(splat_trainer *trainer);
+int splat_trainer_update_curvature(splat_trainer *trainer);
+
 /* Trainer::gaussian_count, sh_degree, active_sh_degree, uses_fixed_point,
  * gpu_bytes, bytes_per_gaussian (trainer.hpp:138-193). */
 int splat_trainer_info(splat_trainer *trainer, int64_t *gaussians, int32_t *sh_degree, int32_t *active_sh_degree,

@@ -197,6 +197,19 @@ def ref_contributions(cloud: Cloud, view: View, background=(0.0, 0.0, 0.0), near
     return out
 
 
+def ref_prune(kind: int, cloud: Cloud, share: float, contribution=None) -> np.ndarray:
+    """The reference's remove_largest (kind 0), remove_least_contributing (1) or
+    remove_least_opaque (2), densify.cpp:95-113: the survivors' old indices."""
+    keep, cargs = _cloud_args(cloud)
+    c = np.ascontiguousarray(contribution if contribution is not None else np.zeros(cloud.count), np.float32)
+    source = np.zeros(cloud.count, np.int64)
+    count = ctypes.c_int()
+    assert ref_lib().ref_prune(ctypes.c_int(kind), ctypes.c_int(cloud.count), ctypes.c_int(cloud.sh_degree), *cargs, _fp(c),
+                               ctypes.c_double(share), source.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                               ctypes.byref(count)) == 0
+    return source[:count.value]
+
+
 def ref_save_ply(cloud: Cloud, path) -> None:
     """The reference's save_ply (gaussian_cloud.cpp:330-365)."""
     keep, cargs = _cloud_args(cloud)

@@ -9,6 +9,7 @@
 // log-scales 3, quaternions (w,x,y,z) 4, opacity logits 1, SH [k][rgb].
 // The camera is the reference's Camera (src/render/camera.hpp:84-89): a
 // column-major world->camera matrix, the camera centre, fx, fy, cx, cy, size.
+#include "train/densify.hpp"
 #include "train/reference.hpp"
 
 #include <cstdint>
@@ -98,6 +99,26 @@ int ref_contributions(int n, int degree, const float *positions, const float *sc
     const std::vector<double> c =
         reference_contributions(cloud, camera, make_options(background, nearPlane, flags, 0.f, 0.f, nullptr, n));
     std::memcpy(out, c.data(), c.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// remove_largest / remove_least_contributing / remove_least_opaque
+// (densify.cpp:95-113): kind 0, 1, 2. source gets, per survivor, the old index
+// (count = survivors); contribution is read for kind 1.
+int ref_prune(int kind, int n, int degree, const float *positions, const float *scales, const float *rotations,
+              const float *opacities, const float *sh, const float *contribution, double share, std::int64_t *source,
+              int *count) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    DensifyResult r;
+    if (kind == 0) r = remove_largest(cloud, share);
+    else if (kind == 1) r = remove_least_contributing(cloud, std::vector<float>(contribution, contribution + n), share);
+    else r = remove_least_opaque(cloud, share);
+    *count = static_cast<int>(r.source.size());
+    std::memcpy(source, r.source.data(), r.source.size() * sizeof(std::int64_t));
     return 0;
   } catch (const std::exception &) {
     return 1;

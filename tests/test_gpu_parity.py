@@ -4,6 +4,8 @@ restatement (bit for bit on integer results, given the device's own projected
 splats). Every call goes through the C ABI."""
 from __future__ import annotations
 
+import math
+
 import numpy as np
 import pytest
 
@@ -683,3 +685,68 @@ def test_score_view_refuses_bad_arguments(splat, oracle):
         trainer.score_view(to_camera(view), target, 0.0)
     with pytest.raises(splat.SplatError):
         trainer.score_view(to_camera(view), target, float("nan"))
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_pruning_keeps_the_references_survivors_and_their_state(splat, oracle, kind):
+    # Trainer::remove_largest_gaussians / remove_least_contributing_gaussians /
+    # remove_least_opaque_gaussians (trainer.cpp:731-747) on the GPU: the same
+    # survivors as the reference's remove_* (densify.cpp:70-113) on the same
+    # cloud and statistics, in their order, with their parameters and Adam
+    # state bit for bit; the statistics start anew; training goes on.
+    view = oracle.train_camera(72, 56)
+    target = oracle.smooth_target(72, 56, 5)
+    cloud = oracle.random_cloud(300, 2, 29)
+    trainer = splat.Trainer(to_cloud(cloud))
+    trainer.step(to_camera(view), target, splat.LearningRates())
+    trainer.collect_statistics(to_camera(view), target)
+    before = trainer.cloud()
+    stats = trainer.densify_stats()
+    states = [trainer.debug_download(splat.DEBUG_STATE + g, np.uint32) for g in range(5)]
+    host = oracle.Cloud(2, before.positions, before.scales, before.rotations, before.opacities, before.sh)
+    source = oracle.ref_prune(kind, host, 0.15, stats.contribution)
+    prune = (trainer.remove_largest_gaussians, trainer.remove_least_contributing_gaussians,
+             trainer.remove_least_opaque_gaussians)[kind]
+    assert prune(0.15) == 300 - len(source) == 45
+    after = trainer.cloud()
+    for name, width in (("positions", 3), ("scales", 3), ("rotations", 4), ("opacities", 1), ("sh", 27)):
+        old = np.asarray(getattr(before, name)).reshape(300, width)
+        new = np.asarray(getattr(after, name)).reshape(len(source), width)
+        np.testing.assert_array_equal(new.view(np.uint32), old[source].view(np.uint32), name)
+    for g, width in enumerate((3, 3, 4, 1)):
+        new = trainer.debug_download(splat.DEBUG_STATE + g, np.uint32).reshape(len(source), width)
+        np.testing.assert_array_equal(new, states[g].reshape(300, width)[source], f"state group {g}")
+    old_stride, new_stride = 384, 256  # Gaussian counts rounded up to 128
+    new_sh = trainer.debug_download(splat.DEBUG_STATE + 4, np.uint32).reshape(-1, new_stride)[:, : len(source)]
+    old_sh = states[4].reshape(-1, old_stride)[:, source]
+    np.testing.assert_array_equal(new_sh, old_sh, "SH state")
+    assert np.all(trainer.densify_stats().contribution == 0.0)
+    assert math.isfinite(trainer.step(to_camera(view), target, splat.LearningRates()).loss)
+
+
+def test_pruning_shares_and_ties(splat, oracle):
+    # Equal sizes: the lowest indices go first, as a stable sort leaves them;
+    # share 0 removes nothing, share 1 all but one; a share outside [0, 1] is refused.
+    cloud = oracle.random_cloud(40, 0, 3)
+    cloud.scales[:] = -2.0
+    trainer = splat.Trainer(to_cloud(cloud))
+    assert trainer.remove_largest_gaussians(0.0) == 0
+    assert trainer.remove_largest_gaussians(0.1) == 4
+    np.testing.assert_array_equal(trainer.cloud().positions.reshape(-1, 3), cloud.positions.reshape(-1, 3)[4:])
+    with pytest.raises(splat.SplatError):
+        trainer.remove_largest_gaussians(1.5)
+    assert trainer.remove_least_opaque_gaussians(1.0) == 35
+    assert trainer.cloud().size() == 1
+
+
+def test_settings_without_a_kernel_accept_only_neutral_values(splat, oracle):
+    trainer = splat.Trainer(to_cloud(oracle.random_cloud(20, 0, 1)))
+    trainer.set_exposure([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0])
+    trainer.set_sh_dropout(0.0)
+    trainer.set_filter3d([])
+    trainer.add_position_noise(0.0)
+    for call in (lambda: trainer.set_exposure([2, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0]), lambda: trainer.set_sh_dropout(0.5),
+                 lambda: trainer.set_filter3d(np.ones(20)), lambda: trainer.add_position_noise(1.0),
+                 trainer.enable_second_order, trainer.update_curvature):
+        with pytest.raises(splat.UnsupportedOption):
+            call()

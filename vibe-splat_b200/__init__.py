@@ -181,6 +181,14 @@ _lib.splat_measure_sm_peaks.argtypes = [ctypes.POINTER(_SmPeaks)]
 _lib.splat_cloud_load_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                       _FP, _FP, _FP, _FP, _FP]
 _lib.splat_cloud_save_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(_Cloud)]
+for _name in ("splat_trainer_remove_largest", "splat_trainer_remove_least_contributing", "splat_trainer_remove_least_opaque"):
+    getattr(_lib, _name).argtypes = [_P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64)]
+_lib.splat_trainer_set_exposure.argtypes = [_P, _FP]
+_lib.splat_trainer_set_sh_dropout.argtypes = [_P, ctypes.c_float, ctypes.c_int32, ctypes.c_uint32]
+_lib.splat_trainer_set_filter3d.argtypes = [_P, _FP, ctypes.c_size_t]
+_lib.splat_trainer_add_position_noise.argtypes = [_P, ctypes.c_float, ctypes.c_uint32]
+_lib.splat_trainer_enable_second_order.argtypes = [_P]
+_lib.splat_trainer_update_curvature.argtypes = [_P]
 
 # ----------------------------------------------------------------- errors
 
@@ -583,6 +591,44 @@ class Trainer:
 
     def reset_densify_stats(self) -> None:
         _check(_lib.splat_trainer_reset_densify_stats(self._h))
+
+    def _prune(self, fn, share: float) -> int:
+        removed = ctypes.c_uint64()
+        _check(fn(self._h, float(share), ctypes.byref(removed)))
+        self._count -= removed.value
+        return removed.value
+
+    def remove_largest_gaussians(self, share: float) -> int:
+        """Trainer::remove_largest_gaussians: the largest first (GPU)."""
+        return self._prune(_lib.splat_trainer_remove_largest, share)
+
+    def remove_least_contributing_gaussians(self, share: float) -> int:
+        """Trainer::remove_least_contributing_gaussians: by the collected contribution (GPU)."""
+        return self._prune(_lib.splat_trainer_remove_least_contributing, share)
+
+    def remove_least_opaque_gaussians(self, share: float) -> int:
+        """Trainer::remove_least_opaque_gaussians: the least opaque first (GPU)."""
+        return self._prune(_lib.splat_trainer_remove_least_opaque, share)
+
+    def set_exposure(self, exposure) -> None:
+        e = np.ascontiguousarray(np.asarray(exposure, np.float32).ravel())
+        _check(_lib.splat_trainer_set_exposure(self._h, _fptr(e)))
+
+    def set_sh_dropout(self, probability: float, retained_degree: int = 0, seed: int = 0) -> None:
+        _check(_lib.splat_trainer_set_sh_dropout(self._h, float(probability), int(retained_degree), int(seed)))
+
+    def set_filter3d(self, filter_values) -> None:
+        f = np.ascontiguousarray(np.asarray(filter_values, np.float32).ravel())
+        _check(_lib.splat_trainer_set_filter3d(self._h, _fptr(f) if f.size else None, f.size))
+
+    def add_position_noise(self, scaler: float, iteration: int = 0) -> None:
+        _check(_lib.splat_trainer_add_position_noise(self._h, float(scaler), int(iteration)))
+
+    def enable_second_order(self) -> None:
+        _check(_lib.splat_trainer_enable_second_order(self._h))
+
+    def update_curvature(self) -> None:
+        _check(_lib.splat_trainer_update_curvature(self._h))
 
     def reset_opacity(self, maximum: float) -> None:
         _check(_lib.splat_trainer_reset_opacity(self._h, float(maximum)))

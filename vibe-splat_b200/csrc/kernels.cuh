@@ -186,6 +186,18 @@ void launch_gather_rows(const int32_t *source, const uint32_t *in, uint32_t *out
                         uint32_t stride, uint32_t copies, cudaStream_t stream);
 void launch_gather_planes(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t newStride,
                           uint32_t oldStride, uint32_t planes, cudaStream_t stream);
+void launch_gather_planes16(const int32_t *source, const uint16_t *in, uint16_t *out, uint32_t newCount, uint32_t newStride,
+                            uint32_t oldStride, uint32_t planes, cudaStream_t stream);
+
+// Pruning on the GPU (remove_highest, src/train/densify.cpp:70-90): keys whose
+// ascending stable sort puts first the Gaussians to remove (kind 0 largest
+// log-scale, 1 least contribution, 2 least opacity), values = indices; then
+// keep flags from the sorted order, and the survivors' source table from the
+// exclusive scan of the flags.
+void launch_prune_keys(int kind, const float *scales, const float *opacities, const float *densifyStats, uint32_t n, uint32_t *keys,
+                       uint32_t *values, cudaStream_t stream);
+void launch_prune_keep(const uint32_t *order, uint32_t removed, uint32_t n, uint32_t *keep, cudaStream_t stream);
+void launch_survivor_sources(const uint32_t *keep, const uint32_t *place, uint32_t n, int32_t *source, cudaStream_t stream);
 
 } // namespace sb
 

@@ -139,7 +139,9 @@ uint32_t bits_for(uint32_t values) {
 
 class Trainer {
 public:
-  Trainer(const splat_cloud &cloud, const splat_trainer_options &options);
+  // upload false: only sizes the buffers (the cloud's arrays may be null) and
+  // leaves the parameters zero, for a caller that fills them on the device.
+  Trainer(const splat_cloud &cloud, const splat_trainer_options &options, bool upload = true);
   ~Trainer();
 
   splat_trainer_options opt;
@@ -228,7 +230,7 @@ public:
   void begin(int stage);
   void end(int stage);
   void clear_graphs();
-  void release_transient();
+  void release_transient(bool keepParameters = false);
   void score_view(const splat_camera *camera, const uint8_t *target, size_t bytes, float share, float pixelWeight,
                   splat_step_stats *stats);
   std::string graph_key(ChainMode mode, bool statistics) const;
@@ -243,11 +245,11 @@ public:
 
 // ---------------------------------------------------------------- set-up
 
-Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options) : opt(options) {
+Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options, bool upload) : opt(options) {
   if (cloud.count <= 0) throw Failure{SPLAT_ERR_INVALID, "nothing to train: the cloud is empty"};
   if (cloud.sh_degree < 0 || cloud.sh_degree > 3) throw Failure{SPLAT_ERR_INVALID, "GaussianCloud: SH degree must be 0..3"};
-  if (cloud.positions == nullptr || cloud.scales == nullptr || cloud.rotations == nullptr || cloud.opacities == nullptr ||
-      cloud.sh == nullptr) {
+  if (upload && (cloud.positions == nullptr || cloud.scales == nullptr || cloud.rotations == nullptr || cloud.opacities == nullptr ||
+                 cloud.sh == nullptr)) {
     throw Failure{SPLAT_ERR_INVALID, "GaussianCloud: inconsistent array sizes"};
   }
   if (opt.position_noise != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "position noise has no kernel in this library"};
@@ -299,6 +301,9 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
   shRest.ensure(std::max<size_t>(rest * (shStore == ShStore::F32 ? 4 : 2), 4));
   SB_CUDA(cudaMemset(shDc.get(), 0, shDc.bytes()));
   SB_CUDA(cudaMemset(shRest.get(), 0, shRest.bytes()));
+  if (!upload) {
+    for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities}) SB_CUDA(cudaMemset(b->get(), 0, b->bytes()));
+  } else {
   SB_CUDA(cudaMemcpy(positions.get(), cloud.positions, nn * 12, cudaMemcpyHostToDevice));
   SB_CUDA(cudaMemcpy(scales.get(), cloud.scales, nn * 12, cudaMemcpyHostToDevice));
   SB_CUDA(cudaMemcpy(rotations.get(), cloud.rotations, nn * 16, cudaMemcpyHostToDevice));
@@ -330,6 +335,7 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options)
         SB_CUDA(cudaMemcpy(shRest.get(), half.data(), rest * 2, cudaMemcpyHostToDevice));
       }
     }
+  }
   }
   const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, ps * 3 * shCoeffs};
   for (int g = 0; g < 5; ++g) {
@@ -369,10 +375,12 @@ Trainer::~Trainer() {
 
 // Frees every device buffer except the optimiser state (densification keeps
 // only that from the old Gaussians).
-void Trainer::release_transient() {
+void Trainer::release_transient(bool keepParameters) {
   clear_graphs();
   SB_CUDA(cudaStreamSynchronize(copyStream)); // a prefetch may still be landing in targetNext
-  for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities, &shDc, &shRest, &grads[0], &grads[1], &grads[2], &grads[3],
+  if (!keepParameters)
+    for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities, &shDc, &shRest}) b->release();
+  for (DeviceBuffer *b : {&grads[0], &grads[1], &grads[2], &grads[3],
                           &grads[4], &densifyStats, &splats, &reach, &depthKeys, &values, &tmpKeys, &tmpValues, &offsets, &raw,
                           &shGrad, &entryKeys, &entryValues, &tmpEntryKeys, &tmpEntryValues, &image, &stops, &adjoint, &fields,
                           &target, &targetNext, &ranges, &partials, &listCounts, &listOffsets, &listPool, &listScratch,
@@ -1443,6 +1451,166 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
     }
     delete t;
     trainer->impl = fresh;
+  });
+}
+
+namespace {
+
+// remove_highest on the GPU (densify.cpp:70-90, Trainer::apply_changes,
+// trainer.cpp:749-787): removes ceil(share n) Gaussians (at most n - 1) by the
+// key of `kind`, highest first, ties in index order; the survivors keep
+// their order, parameters and optimiser state, gathered on the device through
+// the source table; the densification statistics start anew. Returns how
+// many were removed.
+uint64_t prune_gaussians(splat_trainer *handle, int kind, double share) {
+  Trainer *t = impl_of(handle);
+  if (!(share >= 0.0 && share <= 1.0)) throw Failure{SPLAT_ERR_INVALID, "share must be in [0, 1]"};
+  const uint32_t oldN = t->n;
+  const uint32_t removed = (uint32_t)std::min<double>((double)oldN - 1.0, std::ceil((double)oldN * share));
+  if (removed == 0) return 0;
+  const uint32_t newN = oldN - removed;
+  cudaStream_t s = t->stream;
+  SB_CUDA(cudaStreamSynchronize(s));
+  sb::DeviceBuffer keys, values, tmpKeys, tmpValues, keep, place, table, scratch, scanScratch, counters;
+  keys.ensure((size_t)oldN * 4);
+  values.ensure((size_t)oldN * 4);
+  tmpKeys.ensure((size_t)oldN * 4);
+  tmpValues.ensure((size_t)oldN * 4);
+  keep.ensure((size_t)oldN * 4);
+  place.ensure((size_t)oldN * 4);
+  table.ensure((size_t)newN * 4);
+  scratch.ensure(sb::sort_scratch_bytes(oldN, 4, 32, 8));
+  scanScratch.ensure(sb::bin_scan_scratch_bytes(oldN));
+  counters.ensure(16);
+  SB_CUDA(cudaMemsetAsync(counters.get(), 0, 16, s));
+  uint32_t *error = counters.get<uint32_t>() + 3;
+  const float *stats = kind == 1 ? t->densifyStats.get<float>() : nullptr;
+  if (kind == 1 && stats == nullptr) throw Failure{SPLAT_ERR_STATE, "no densification statistics to prune by"};
+  sb::launch_prune_keys(kind, t->scales.get<float>(), t->opacities.get<float>(), stats, oldN, keys.get<uint32_t>(),
+                        values.get<uint32_t>(), s);
+  const int where = sb::sort_pairs_u32(keys.get<uint32_t>(), values.get<uint32_t>(), tmpKeys.get<uint32_t>(), tmpValues.get<uint32_t>(),
+                                       oldN, oldN, nullptr, 0, 32, 8, scratch.get(), error, s);
+  const uint32_t *order = where == 1 ? tmpValues.get<uint32_t>() : values.get<uint32_t>();
+  sb::launch_prune_keep(order, removed, oldN, keep.get<uint32_t>(), s);
+  SB_CUDA(cudaMemcpyAsync(place.get(), keep.get(), (size_t)oldN * 4, cudaMemcpyDeviceToDevice, s));
+  sb::launch_exclusive_scan(oldN, place.get<uint32_t>(), counters.get<uint32_t>(), scanScratch.get(), error, s);
+  sb::launch_survivor_sources(keep.get<uint32_t>(), place.get<uint32_t>(), oldN, table.get<int32_t>(), s);
+  uint32_t status[4] = {0, 0, 0, 0};
+  SB_CUDA(cudaMemcpyAsync(status, counters.get(), 16, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  if (status[3] != 0u) throw Failure{SPLAT_ERR_DEVICE, "the pruning sort's look-back gave up waiting"};
+  if (status[1] != newN) throw Failure{SPLAT_ERR_DEVICE, "the pruning kept an unexpected number of Gaussians"};
+  // Everything but the parameters and the optimiser state goes before the new
+  // trainer is made, for the sake of the budget.
+  t->release_transient(true);
+
+  splat_cloud sizes{};
+  sizes.count = (int32_t)newN;
+  sizes.sh_degree = t->shDegree;
+  Trainer *fresh = new Trainer(sizes, t->opt, false);
+  fresh->adamStep = t->adamStep;
+  fresh->activeDegree = t->activeDegree;
+  try {
+    cudaStream_t f = fresh->stream;
+    const int32_t *src = table.get<int32_t>();
+    const uint32_t strides[4] = {3, 3, 4, 1};
+    sb::DeviceBuffer *from[4] = {&t->positions, &t->scales, &t->rotations, &t->opacities};
+    sb::DeviceBuffer *to[4] = {&fresh->positions, &fresh->scales, &fresh->rotations, &fresh->opacities};
+    for (int g = 0; g < 4; ++g)
+      sb::launch_gather_rows(src, from[g]->get<uint32_t>(), to[g]->get<uint32_t>(), newN, oldN, strides[g], 1u, f);
+    sb::launch_gather_planes(src, t->shDc.get<uint32_t>(), fresh->shDc.get<uint32_t>(), newN, fresh->planeStride, t->planeStride, 3u, f);
+    const uint32_t restPlanes = 3u * (uint32_t)(t->shCoeffs - 1);
+    if (t->shStore == sb::ShStore::F32)
+      sb::launch_gather_planes(src, t->shRest.get<uint32_t>(), fresh->shRest.get<uint32_t>(), newN, fresh->planeStride,
+                               t->planeStride, restPlanes, f);
+    else
+      sb::launch_gather_planes16(src, t->shRest.get<uint16_t>(), fresh->shRest.get<uint16_t>(), newN, fresh->planeStride,
+                                 t->planeStride, restPlanes, f);
+    const uint32_t copies = t->stateStore == sb::StateStore::F32 ? 2u : 1u;
+    for (int g = 0; g < 4; ++g)
+      sb::launch_gather_rows(src, t->state[g].get<uint32_t>(), fresh->state[g].get<uint32_t>(), newN, oldN, strides[g], copies, f);
+    sb::launch_gather_planes(src, t->state[4].get<uint32_t>(), fresh->state[4].get<uint32_t>(), newN, fresh->planeStride,
+                             t->planeStride, 3u * (uint32_t)t->shCoeffs * copies, f);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(f));
+  } catch (...) {
+    delete fresh;
+    throw;
+  }
+  delete t;
+  handle->impl = fresh;
+  return removed;
+}
+
+} // namespace
+
+int splat_trainer_remove_largest(splat_trainer *trainer, double share, uint64_t *removed) {
+  return guarded([&] {
+    const uint64_t r = prune_gaussians(trainer, 0, share);
+    if (removed != nullptr) *removed = r;
+  });
+}
+
+int splat_trainer_remove_least_contributing(splat_trainer *trainer, double share, uint64_t *removed) {
+  return guarded([&] {
+    const uint64_t r = prune_gaussians(trainer, 1, share);
+    if (removed != nullptr) *removed = r;
+  });
+}
+
+int splat_trainer_remove_least_opaque(splat_trainer *trainer, double share, uint64_t *removed) {
+  return guarded([&] {
+    const uint64_t r = prune_gaussians(trainer, 2, share);
+    if (removed != nullptr) *removed = r;
+  });
+}
+
+int splat_trainer_set_exposure(splat_trainer *trainer, const float exposure[12]) {
+  return guarded([&] {
+    (void)impl_of(trainer);
+    if (exposure == nullptr) throw Failure{SPLAT_ERR_INVALID, "null exposure"};
+    static const float neutral[12] = {1.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f};
+    for (int k = 0; k < 12; ++k)
+      if (exposure[k] != neutral[k]) throw Failure{SPLAT_ERR_UNSUPPORTED, "exposure has no kernel in this library"};
+  });
+}
+
+int splat_trainer_set_sh_dropout(splat_trainer *trainer, float probability, int32_t retained_degree, uint32_t seed) {
+  return guarded([&] {
+    (void)impl_of(trainer);
+    (void)retained_degree;
+    (void)seed;
+    if (probability > 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "SH dropout has no kernel in this library"};
+  });
+}
+
+int splat_trainer_set_filter3d(splat_trainer *trainer, const float *filter, size_t count) {
+  return guarded([&] {
+    (void)impl_of(trainer);
+    (void)filter;
+    if (count != 0) throw Failure{SPLAT_ERR_UNSUPPORTED, "the 3D filter has no kernel in this library"};
+  });
+}
+
+int splat_trainer_add_position_noise(splat_trainer *trainer, float scaler, uint32_t iteration) {
+  return guarded([&] {
+    (void)impl_of(trainer);
+    (void)iteration;
+    if (scaler != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "position noise has no kernel in this library"};
+  });
+}
+
+int splat_trainer_enable_second_order(splat_trainer *trainer) {
+  return guarded([&] {
+    (void)impl_of(trainer);
+    throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
+  });
+}
+
+int splat_trainer_update_curvature(splat_trainer *trainer) {
+  return guarded([&] {
+    (void)impl_of(trainer);
+    throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
   });
 }
 
