@@ -602,6 +602,12 @@ def our_arm(args) -> None:
             if "issue" in r:
                 roof["issue"] = r["issue"]
 
+    # Pruning on the GPU (remove_largest_gaussians, 1 % of the Gaussians):
+    # keys, sort, scan and the gathers of parameters and optimiser state.
+    t0 = time.perf_counter()
+    pruned = trainer.remove_largest_gaussians(0.01)
+    prune = {"removed": pruned, "ms": (time.perf_counter() - t0) * 1000.0, "of": n}
+
     plain = None
     if not args.no_plain:
         del trainer
@@ -659,6 +665,7 @@ def our_arm(args) -> None:
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "sm_peaks": sm_peaks,
         "score_view_ms": score_ms,
+        "prune": prune,
         "roofline": roof,
         "stage_roofline": stage_roof,
         "stages_ms": stages,
