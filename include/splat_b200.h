@@ -219,6 +219,10 @@ int splat_trainer_set_active_sh_degree(splat_trainer *trainer, int32_t degree);
  * gradient sum, marked pixels, marked loss, edge score. */
 int splat_trainer_get_densify_stats(splat_trainer *trainer, float *out);
 /* Trainer::reset_densify_stats (trainer.hpp:178). */
+/* Replaces the densification statistics (8 floats per Gaussian, the layout
+ * splat_trainer_get_densify_stats reads), as restoring a paused run or a
+ * test that sets them needs. */
+int splat_trainer_set_densify_stats(splat_trainer *trainer, const float *raw);
 int splat_trainer_reset_densify_stats(splat_trainer *trainer);
 /* Trainer::reset_opacity (trainer.hpp:163, trainer.cpp:810-819). */
 int splat_trainer_reset_opacity(splat_trainer *trainer, float maximum);
@@ -242,6 +246,56 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
 int splat_trainer_remove_largest(splat_trainer *trainer, double share, uint64_t *removed);
 int splat_trainer_remove_least_contributing(splat_trainer *trainer, double share, uint64_t *removed);
 int splat_trainer_remove_least_opaque(splat_trainer *trainer, double share, uint64_t *removed);
+
+/* The random generator densification draws from: a std::mt19937, whose
+ * state carries over from call to call as the reference's session keeps one
+ * (TrainSession::densifyRng_, train.hpp:254) and passes it to every round. */
+typedef struct splat_rng splat_rng;
+int splat_rng_create(uint32_t seed, splat_rng **out);
+int splat_rng_destroy(splat_rng *rng);
+/* std::uniform_int_distribution<std::size_t>(0, count - 1)(rng), as the
+ * session draws the views it scores (train.cpp:690-692); count >= 1. */
+int splat_rng_pick(splat_rng *rng, uint64_t count, uint64_t *out);
+
+/* DensifyOptions (densify.hpp:23-50). */
+typedef struct splat_densify_options {
+  float gradient_threshold;  /* 2e-4 */
+  float dense_scale;         /* 0: larger than this along any axis splits, otherwise clones */
+  float prune_opacity;       /* 0.005 */
+  int32_t prune_large;       /* 0: also remove the oversized, below */
+  float max_screen_radius;   /* 20 */
+  float max_world_scale;     /* 0 */
+  uint64_t max_gaussians;    /* UINT64_MAX */
+  float split_threshold;     /* 0; above 0 large Gaussians split on the absolute gradient (AbsGS) */
+  int32_t scored_views;      /* 0; above 0 only Gaussians in high-error pixels densify (FastGS) */
+  float min_marked_pixels;   /* 5 */
+  double transparent_share;  /* 1: the share of the too transparent removed, the least useful first */
+  uint64_t explore_splits;   /* 0: random large Gaussians split each round */
+  uint64_t explore_seeds;    /* 0: new Gaussians placed at random in the cloud's bounding box */
+  int32_t edge_split;        /* 0: 1 splits candidates along their longest axis with probability edge score / best */
+} splat_densify_options;
+void splat_densify_options_default(splat_densify_options *options);
+
+/* DensifyResult's counts (densify.hpp:52-62); count is the new size. */
+typedef struct splat_densify_result {
+  uint64_t count, cloned, split, seeded, pruned, held_back;
+} splat_densify_result;
+
+/* Trainer::densify (trainer.cpp:710-715, densify_cloud of densify.cpp:115-326
+ * and apply_changes): clones, splits, prunes and seeds by the densification
+ * statistics, the new cloud being the survivors in their order, then per old
+ * index a copy per clone and two children per split, then the seeds. The
+ * survivors keep their optimiser state, the new ones start fresh, and the
+ * statistics start anew. On the GPU: the decisions, stable radix sorts for
+ * the transparent share and the count limit, scans and gathers; only the
+ * rows that take random draws (split children, seeds) and the lists those
+ * draws pick from are made on the host, drawing from rng in the reference's
+ * order. source (may be null): if source_capacity >= result->count, the old
+ * index whose state each new Gaussian keeps, or -1. A result with no
+ * Gaussian is SPLAT_ERR_INVALID and leaves the trainer as it was (rng has
+ * drawn, as in the reference). */
+int splat_trainer_densify(splat_trainer *trainer, const splat_densify_options *options, splat_rng *rng,
+                          splat_densify_result *result, int64_t *source, uint64_t source_capacity);
 
 /* Trainer methods with no kernel in this library, for callers that set them
  * unconditionally: the neutral setting is accepted and changes nothing, any

@@ -210,6 +210,61 @@ def ref_prune(kind: int, cloud: Cloud, share: float, contribution=None) -> np.nd
     return source[:count.value]
 
 
+class RefRng:
+    """A std::mt19937 kept by the reference side across ref_densify calls."""
+
+    def __init__(self, seed: int):
+        lib = ref_lib()
+        lib.ref_rng_create.restype = ctypes.c_void_p
+        lib.ref_rng_create.argtypes = [ctypes.c_uint32]
+        lib.ref_rng_destroy.argtypes = [ctypes.c_void_p]
+        self._h = ctypes.c_void_p(lib.ref_rng_create(ctypes.c_uint32(seed & 0xFFFFFFFF)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            ref_lib().ref_rng_destroy(self._h)
+            self._h = None
+
+
+def ref_rng_pick(rng: RefRng, count: int) -> int:
+    """std::uniform_int_distribution<std::size_t>(0, count - 1) on the reference side."""
+    lib = ref_lib()
+    lib.ref_rng_pick.restype = ctypes.c_uint64
+    lib.ref_rng_pick.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+    return int(lib.ref_rng_pick(rng._h, count))
+
+
+@dataclass
+class RefDensified:
+    cloud: Cloud
+    source: np.ndarray
+    counts: dict
+
+
+def ref_densify(cloud: Cloud, raw_stats: np.ndarray, options, rng: RefRng) -> RefDensified:
+    """The reference's densify_cloud (densify.cpp:115-326) on the trainer's raw
+    statistics (8 floats per Gaussian). options: a ctypes structure laid out
+    as DensifyOptions in the product's field order. Raises ValueError where
+    the reference throws."""
+    keep, cargs = _cloud_args(cloud)
+    raw = np.ascontiguousarray(raw_stats, np.float32).ravel()
+    assert raw.size == cloud.count * 8
+    room = 2 * cloud.count + int(options.explore_seeds)
+    coeffs = (cloud.sh_degree + 1) ** 2
+    out = [np.zeros(room * k, np.float32) for k in (3, 3, 4, 1, 3 * coeffs)]
+    source = np.zeros(room, np.int64)
+    counts = np.zeros(6, np.uint64)
+    status = ref_lib().ref_densify(ctypes.c_int(cloud.count), ctypes.c_int(cloud.sh_degree), *cargs, _fp(raw), ctypes.byref(options),
+                                   rng._h, *[_fp(a) for a in out], source.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                   counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+    if status != 0:
+        raise ValueError("the reference's densify_cloud threw")
+    n = int(counts[0])
+    result = Cloud(cloud.sh_degree, out[0][: n * 3], out[1][: n * 3], out[2][: n * 4], out[3][:n], out[4][: n * 3 * coeffs])
+    names = ("count", "cloned", "split", "seeded", "pruned", "held_back")
+    return RefDensified(result, source[:n], {k: int(v) for k, v in zip(names, counts)})
+
+
 def ref_save_ply(cloud: Cloud, path) -> None:
     """The reference's save_ply (gaussian_cloud.cpp:330-365)."""
     keep, cargs = _cloud_args(cloud)

@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <random>
 
 using namespace splat;
 
@@ -224,6 +225,79 @@ int ref_gradients(int n, int degree, const float *positions, const float *scales
     std::memcpy(gOpacities, g.opacities.data(), g.opacities.size() * sizeof(double));
     std::memcpy(gSh, g.sh.data(), g.sh.size() * sizeof(double));
     std::memcpy(absoluteCentre, g.absoluteCentre.data(), g.absoluteCentre.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// A std::mt19937 that lives across ref_densify calls, as the reference's
+// session keeps one (train.hpp:254).
+void *ref_rng_create(std::uint32_t seed) { return new std::mt19937(seed); }
+void ref_rng_destroy(void *rng) { delete static_cast<std::mt19937 *>(rng); }
+// The session's pick of a view to score (train.cpp:690-692).
+std::uint64_t ref_rng_pick(void *rng, std::uint64_t count) {
+  return std::uniform_int_distribution<std::size_t>(0, count - 1)(*static_cast<std::mt19937 *>(rng));
+}
+
+// DensifyOptions (densify.hpp:23-50), in the field order of the product's
+// splat_densify_options so that one ctypes structure serves both.
+struct RefDensifyOptions {
+  float gradientThreshold, denseScale, pruneOpacity;
+  std::int32_t pruneLarge;
+  float maxScreenRadius, maxWorldScale;
+  std::uint64_t maxGaussians;
+  float splitThreshold;
+  std::int32_t scoredViews;
+  float minMarkedPixels;
+  double transparentShare;
+  std::uint64_t exploreSplits, exploreSeeds;
+  std::int32_t edgeSplit;
+};
+
+// densify_cloud (densify.cpp:115-326) on the cloud and the trainer's raw
+// statistics (8 floats per Gaussian, trainer.cpp:686-708). The new cloud goes
+// to the out* arrays (room for 2n + exploreSeeds Gaussians), the source
+// table to source, counts = {count, cloned, split, seeded, pruned, heldBack}.
+// Returns 0, or 1 if the reference threw.
+int ref_densify(int n, int degree, const float *positions, const float *scales, const float *rotations, const float *opacities,
+                const float *sh, const float *raw, const RefDensifyOptions *o, void *rng, float *outPositions,
+                float *outScales, float *outRotations, float *outOpacities, float *outSh, std::int64_t *source,
+                std::uint64_t *counts) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    DensifyStats stats;
+    std::vector<float> *columns[8] = {&stats.gradientSum, &stats.visits, &stats.maxRadius, &stats.contribution,
+                                      &stats.absoluteGradientSum, &stats.markedPixels, &stats.markedLoss, &stats.edgeScore};
+    for (int c = 0; c < 8; ++c) {
+      columns[c]->resize(static_cast<std::size_t>(n));
+      for (int i = 0; i < n; ++i) (*columns[c])[static_cast<std::size_t>(i)] = raw[i * 8 + c];
+    }
+    DensifyOptions options;
+    options.gradientThreshold = o->gradientThreshold;
+    options.denseScale = o->denseScale;
+    options.pruneOpacity = o->pruneOpacity;
+    options.pruneLarge = o->pruneLarge != 0;
+    options.maxScreenRadius = o->maxScreenRadius;
+    options.maxWorldScale = o->maxWorldScale;
+    options.maxGaussians = o->maxGaussians;
+    options.splitThreshold = o->splitThreshold;
+    options.scoredViews = o->scoredViews;
+    options.minMarkedPixels = o->minMarkedPixels;
+    options.transparentShare = o->transparentShare;
+    options.exploreSplits = o->exploreSplits;
+    options.exploreSeeds = o->exploreSeeds;
+    options.edgeSplit = o->edgeSplit != 0;
+    const DensifyResult r = densify_cloud(cloud, stats, options, *static_cast<std::mt19937 *>(rng));
+    const GaussianCloud &c = r.cloud;
+    std::memcpy(outPositions, c.positions.data(), c.positions.size() * sizeof(float));
+    std::memcpy(outScales, c.scales.data(), c.scales.size() * sizeof(float));
+    std::memcpy(outRotations, c.rotations.data(), c.rotations.size() * sizeof(float));
+    std::memcpy(outOpacities, c.opacities.data(), c.opacities.size() * sizeof(float));
+    std::memcpy(outSh, c.sh.data(), c.sh.size() * sizeof(float));
+    std::memcpy(source, r.source.data(), r.source.size() * sizeof(std::int64_t));
+    const std::uint64_t out[6] = {c.size(), r.cloned, r.split, r.seeded, r.pruned, r.heldBack};
+    std::memcpy(counts, out, sizeof(out));
     return 0;
   } catch (const std::exception &) {
     return 1;

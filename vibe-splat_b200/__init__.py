@@ -156,6 +156,7 @@ _lib.splat_trainer_get_cloud.argtypes = [_P, _FP, _FP, _FP, _FP, _FP]
 _lib.splat_trainer_set_active_sh_degree.argtypes = [_P, ctypes.c_int32]
 _lib.splat_trainer_get_densify_stats.argtypes = [_P, _FP]
 _lib.splat_trainer_reset_densify_stats.argtypes = [_P]
+_lib.splat_trainer_set_densify_stats.argtypes = [_P, _FP]
 _lib.splat_trainer_reset_opacity.argtypes = [_P, ctypes.c_float]
 _lib.splat_trainer_apply_changes.argtypes = [_P, ctypes.POINTER(_Cloud), ctypes.POINTER(ctypes.c_int32)]
 _lib.splat_trainer_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32),
@@ -184,6 +185,26 @@ _lib.splat_cloud_save_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(_Cloud)]
 for _name in ("splat_trainer_remove_largest", "splat_trainer_remove_least_contributing", "splat_trainer_remove_least_opaque"):
     getattr(_lib, _name).argtypes = [_P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64)]
 _lib.splat_trainer_set_exposure.argtypes = [_P, _FP]
+
+
+class _DensifyOptions(ctypes.Structure):
+    _fields_ = [("gradient_threshold", ctypes.c_float), ("dense_scale", ctypes.c_float), ("prune_opacity", ctypes.c_float),
+                ("prune_large", ctypes.c_int32), ("max_screen_radius", ctypes.c_float), ("max_world_scale", ctypes.c_float),
+                ("max_gaussians", ctypes.c_uint64), ("split_threshold", ctypes.c_float), ("scored_views", ctypes.c_int32),
+                ("min_marked_pixels", ctypes.c_float), ("transparent_share", ctypes.c_double),
+                ("explore_splits", ctypes.c_uint64), ("explore_seeds", ctypes.c_uint64), ("edge_split", ctypes.c_int32)]
+
+
+class _DensifyResult(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in ("count", "cloned", "split", "seeded", "pruned", "held_back")]
+
+
+_lib.splat_rng_create.argtypes = [ctypes.c_uint32, ctypes.POINTER(_P)]
+_lib.splat_rng_destroy.argtypes = [_P]
+_lib.splat_rng_pick.argtypes = [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+_lib.splat_densify_options_default.argtypes = [ctypes.POINTER(_DensifyOptions)]
+_lib.splat_trainer_densify.argtypes = [_P, ctypes.POINTER(_DensifyOptions), _P, ctypes.POINTER(_DensifyResult),
+                                       ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64]
 _lib.splat_trainer_set_sh_dropout.argtypes = [_P, ctypes.c_float, ctypes.c_int32, ctypes.c_uint32]
 _lib.splat_trainer_set_filter3d.argtypes = [_P, _FP, ctypes.c_size_t]
 _lib.splat_trainer_add_position_noise.argtypes = [_P, ctypes.c_float, ctypes.c_uint32]
@@ -388,6 +409,71 @@ class LearningRates:
 
 
 @dataclass
+class DensifyOptions:
+    """DensifyOptions (densify.hpp:23-50)."""
+
+    gradient_threshold: float = 2e-4
+    dense_scale: float = 0.0
+    prune_opacity: float = 0.005
+    prune_large: bool = False
+    max_screen_radius: float = 20.0
+    max_world_scale: float = 0.0
+    max_gaussians: int = 2**64 - 1
+    split_threshold: float = 0.0
+    scored_views: int = 0
+    min_marked_pixels: float = 5.0
+    transparent_share: float = 1.0
+    explore_splits: int = 0
+    explore_seeds: int = 0
+    edge_split: bool = False
+
+    def _c(self) -> _DensifyOptions:
+        o = _DensifyOptions()
+        for name, _ in _DensifyOptions._fields_:
+            value = getattr(self, name)
+            setattr(o, name, int(value) if isinstance(value, bool) else value)
+        return o
+
+
+@dataclass
+class DensifyResult:
+    """DensifyResult (densify.hpp:52-62): the counts and, per new Gaussian, the
+    old index whose optimiser state it keeps (-1 for a new one)."""
+
+    count: int
+    cloned: int
+    split: int
+    seeded: int
+    pruned: int
+    held_back: int
+    source: np.ndarray
+
+
+class Rng:
+    """The std::mt19937 densification draws from; its state carries over from
+    round to round, as the reference's session keeps one (train.hpp:254)."""
+
+    def __init__(self, seed: int):
+        h = _P()
+        _check(_lib.splat_rng_create(ctypes.c_uint32(seed & 0xFFFFFFFF), ctypes.byref(h)))
+        self._h = h
+
+    def pick(self, count: int) -> int:
+        """std::uniform_int_distribution<std::size_t>(0, count - 1)(rng)."""
+        out = ctypes.c_uint64()
+        _check(_lib.splat_rng_pick(self._h, int(count), ctypes.byref(out)))
+        return out.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.splat_rng_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+@dataclass
 class StepStats:
     """StepStats (trainer.hpp:63-73)."""
 
@@ -589,6 +675,13 @@ class Trainer:
         r = raw.reshape(-1, 8)
         return DensifyStats(*(r[:, k].copy() for k in range(8)))
 
+    def set_densify_stats(self, raw) -> None:
+        """Replaces the statistics: 8 floats per Gaussian, the layout densify_stats reads."""
+        r = np.ascontiguousarray(np.asarray(raw, np.float32).ravel())
+        if r.size != self._count * 8:
+            raise ValueError("8 statistics per Gaussian expected")
+        _check(_lib.splat_trainer_set_densify_stats(self._h, _fptr(r)))
+
     def reset_densify_stats(self) -> None:
         _check(_lib.splat_trainer_reset_densify_stats(self._h))
 
@@ -597,6 +690,17 @@ class Trainer:
         _check(fn(self._h, float(share), ctypes.byref(removed)))
         self._count -= removed.value
         return removed.value
+
+    def densify(self, options: DensifyOptions, rng: Rng) -> DensifyResult:
+        """Trainer::densify (trainer.cpp:710-715): clone, split, prune and seed
+        by the densification statistics, on the GPU."""
+        capacity = 2 * self._count + int(options.explore_seeds)
+        source = np.empty(capacity, np.int64)
+        r = _DensifyResult()
+        _check(_lib.splat_trainer_densify(self._h, ctypes.byref(options._c()), rng._h, ctypes.byref(r),
+                                          source.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), capacity))
+        self._count = r.count
+        return DensifyResult(r.count, r.cloned, r.split, r.seeded, r.pruned, r.held_back, source[:r.count].copy())
 
     def remove_largest_gaussians(self, share: float) -> int:
         """Trainer::remove_largest_gaussians: the largest first (GPU)."""

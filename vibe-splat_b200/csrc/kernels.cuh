@@ -199,5 +199,55 @@ void launch_prune_keys(int kind, const float *scales, const float *opacities, co
 void launch_prune_keep(const uint32_t *order, uint32_t removed, uint32_t n, uint32_t *keep, cudaStream_t stream);
 void launch_survivor_sources(const uint32_t *keep, const uint32_t *place, uint32_t n, int32_t *source, cudaStream_t stream);
 
+// Adaptive density control (densify_cloud, densify.cpp:115-326). Actions
+// per Gaussian, and the options the kernels read. worldLog and denseLog are
+// the smallest largest-log-scales whose exp exceeds max_world_scale and the
+// dense scale (NaN: none does); opacityLogit the smallest logit whose
+// sigmoid is not below the opacity limit.
+enum : uint32_t { kDensifyKeep = 0, kDensifyPrune = 1, kDensifyClone = 2, kDensifySplit = 3, kDensifyLongAxis = 4 };
+struct DensifyArgs {
+  float gradientThreshold, splitThreshold, maxScreenRadius, minMarkedPixels;
+  float worldLog, denseLog, opacityLogit;
+  int pruneLarge, scoredViews, allTransparent, edgeSplit;
+};
+// A row computed on the host for a new Gaussian's slot.
+enum : uint32_t { kPatchRotation = 1, kPatchOpacity = 2, kPatchShRest = 4 };
+struct DensifyPatch {
+  uint32_t slot, what;
+  float position[3], scale[3], rotation[4], opacity;
+};
+// action = prune (oversized, non-finite, or too transparent when all such go)
+// or keep; transparent flags the too transparent otherwise, with the
+// ascending sort key of their share.
+void launch_densify_classify(const Params &p, const float *stats, const DensifyArgs &a, uint32_t *action, uint32_t *transparent,
+                             uint32_t *transparentKey, cudaStream_t stream);
+// kept, candidate flags and the ascending sort key of the candidates' priority.
+void launch_densify_candidates(const float *scales, const float *stats, const DensifyArgs &a, uint32_t n, const uint32_t *action,
+                               uint32_t *kept, uint32_t *candidate, uint32_t *priorityKey, cudaStream_t stream);
+// flag[order[r]] = value for r < count.
+void launch_set_first(const uint32_t *order, uint32_t count, uint32_t value, uint32_t *flag, cudaStream_t stream);
+// out[place[i]] = i, keysOut[place[i]] = keys[i] (if keysOut) where flag[i].
+void launch_compact(const uint32_t *flag, const uint32_t *place, const uint32_t *keys, uint32_t n, uint32_t *out, uint32_t *keysOut,
+                    cudaStream_t stream);
+// The chosen candidates' actions: long-axis split, split or clone.
+void launch_densify_choose(const float *scales, const DensifyArgs &a, uint32_t n, const uint32_t *chosen, uint32_t *action,
+                           cudaStream_t stream);
+// Flags the kept Gaussians larger than the dense scale.
+void launch_densify_large(const float *scales, const DensifyArgs &a, uint32_t n, const uint32_t *action, uint32_t *large,
+                          cudaStream_t stream);
+// Survivor, added-slot and patched-children flags from the actions.
+void launch_densify_flags(uint32_t n, const uint32_t *action, uint32_t *survivor, uint32_t *added, uint32_t *patched,
+                          cudaStream_t stream);
+// The new cloud's parameter and state source tables, the split parents in
+// index order and their first child's slot.
+void launch_densify_tables(uint32_t n, uint32_t survivors, const uint32_t *action, const uint32_t *survivorPlace,
+                           const uint32_t *addedPlace, const uint32_t *patchedPlace, int32_t *paramSource, int32_t *stateSource,
+                           uint32_t *parents, uint32_t *childSlot, cudaStream_t stream);
+// Writes host-computed rows into their slots (shRest: restPlanes planes of
+// planeStride elements of shBytes bytes).
+void launch_densify_patch(const DensifyPatch *patches, uint32_t count, float *positions, float *scales, float *rotations,
+                          float *opacities, void *shRest, uint32_t restPlanes, uint32_t planeStride, uint32_t shBytes,
+                          cudaStream_t stream);
+
 } // namespace sb
 

@@ -15,8 +15,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <new>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -240,6 +242,9 @@ public:
   void finish_stats(splat_step_stats *stats, int count);
   void fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates);
   void set_sort(bool single, int digits);
+  // Carries the step counter, active SH degree and the sort and layout
+  // choices over to a trainer made for a changed cloud.
+  void inherit(const Trainer &old);
   void autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats, splat_autotune_result *out);
 };
 
@@ -1003,6 +1008,16 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
 
 // Switches the tile sort's form and digit width; the entry buffers (whose key
 // width may change) and the captured graphs are rebuilt on the next step.
+void Trainer::inherit(const Trainer &old) {
+  adamStep = old.adamStep;
+  activeDegree = old.activeDegree;
+  oneSort = old.oneSort;
+  digitBits = old.digitBits;
+  forwardPixels = old.forwardPixels;
+  backwardPixels = old.backwardPixels;
+  timing = old.timing;
+}
+
 void Trainer::set_sort(bool single, int digits) {
   if (single == oneSort && digits == digitBits) return;
   SB_CUDA(cudaStreamSynchronize(stream));
@@ -1392,6 +1407,15 @@ int splat_trainer_get_densify_stats(splat_trainer *trainer, float *out) {
   });
 }
 
+int splat_trainer_set_densify_stats(splat_trainer *trainer, const float *raw) {
+  return guarded([&] {
+    Trainer *t = impl_of(trainer);
+    if (raw == nullptr) throw Failure{SPLAT_ERR_INVALID, "null input"};
+    SB_CUDA(cudaStreamSynchronize(t->stream));
+    SB_CUDA(cudaMemcpy(t->densifyStats.get(), raw, (size_t)t->n * sb::kStatStride * 4, cudaMemcpyHostToDevice));
+  });
+}
+
 int splat_trainer_reset_densify_stats(splat_trainer *trainer) {
   return guarded([&] {
     Trainer *t = impl_of(trainer);
@@ -1430,8 +1454,7 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
     t->release_transient();
     const splat_trainer_options o = t->opt;
     Trainer *fresh = new Trainer(*cloud, o);
-    fresh->adamStep = t->adamStep;
-    fresh->activeDegree = t->activeDegree;
+    fresh->inherit(*t);
     try {
       sb::DeviceBuffer table;
       table.ensure(newN * sizeof(int32_t));
@@ -1455,6 +1478,54 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
 }
 
 namespace {
+
+// Replaces the trainer by one of newN Gaussians gathered on the device from
+// the old one (Trainer::apply_changes, trainer.cpp:749-787): the parameters
+// through paramSource, the optimiser state through stateSource (-1: fresh,
+// zero). Everything but the parameters and the optimiser state goes before
+// the new trainer is made, for the sake of the budget; its densification
+// statistics start at zero. Returns the new trainer, installed in handle.
+Trainer *regather(splat_trainer *handle, const int32_t *paramSource, const int32_t *stateSource, uint32_t newN) {
+  Trainer *t = impl_of(handle);
+  const uint32_t oldN = t->n;
+  t->release_transient(true);
+  splat_cloud sizes{};
+  sizes.count = (int32_t)newN;
+  sizes.sh_degree = t->shDegree;
+  Trainer *fresh = new Trainer(sizes, t->opt, false);
+  fresh->inherit(*t);
+  try {
+    cudaStream_t f = fresh->stream;
+    const uint32_t strides[4] = {3, 3, 4, 1};
+    sb::DeviceBuffer *from[4] = {&t->positions, &t->scales, &t->rotations, &t->opacities};
+    sb::DeviceBuffer *to[4] = {&fresh->positions, &fresh->scales, &fresh->rotations, &fresh->opacities};
+    for (int g = 0; g < 4; ++g)
+      sb::launch_gather_rows(paramSource, from[g]->get<uint32_t>(), to[g]->get<uint32_t>(), newN, oldN, strides[g], 1u, f);
+    sb::launch_gather_planes(paramSource, t->shDc.get<uint32_t>(), fresh->shDc.get<uint32_t>(), newN, fresh->planeStride,
+                             t->planeStride, 3u, f);
+    const uint32_t restPlanes = 3u * (uint32_t)(t->shCoeffs - 1);
+    if (t->shStore == sb::ShStore::F32)
+      sb::launch_gather_planes(paramSource, t->shRest.get<uint32_t>(), fresh->shRest.get<uint32_t>(), newN, fresh->planeStride,
+                               t->planeStride, restPlanes, f);
+    else
+      sb::launch_gather_planes16(paramSource, t->shRest.get<uint16_t>(), fresh->shRest.get<uint16_t>(), newN, fresh->planeStride,
+                                 t->planeStride, restPlanes, f);
+    const uint32_t copies = t->stateStore == sb::StateStore::F32 ? 2u : 1u;
+    for (int g = 0; g < 4; ++g)
+      sb::launch_gather_rows(stateSource, t->state[g].get<uint32_t>(), fresh->state[g].get<uint32_t>(), newN, oldN, strides[g],
+                             copies, f);
+    sb::launch_gather_planes(stateSource, t->state[4].get<uint32_t>(), fresh->state[4].get<uint32_t>(), newN, fresh->planeStride,
+                             t->planeStride, 3u * (uint32_t)t->shCoeffs * copies, f);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(f));
+  } catch (...) {
+    delete fresh;
+    throw;
+  }
+  delete t;
+  handle->impl = fresh;
+  return fresh;
+}
 
 // remove_highest on the GPU (densify.cpp:70-90, Trainer::apply_changes,
 // trainer.cpp:749-787): removes ceil(share n) Gaussians (at most n - 1) by the
@@ -1500,49 +1571,484 @@ uint64_t prune_gaussians(splat_trainer *handle, int kind, double share) {
   SB_CUDA(cudaStreamSynchronize(s));
   if (status[3] != 0u) throw Failure{SPLAT_ERR_DEVICE, "the pruning sort's look-back gave up waiting"};
   if (status[1] != newN) throw Failure{SPLAT_ERR_DEVICE, "the pruning kept an unexpected number of Gaussians"};
-  // Everything but the parameters and the optimiser state goes before the new
-  // trainer is made, for the sake of the budget.
-  t->release_transient(true);
-
-  splat_cloud sizes{};
-  sizes.count = (int32_t)newN;
-  sizes.sh_degree = t->shDegree;
-  Trainer *fresh = new Trainer(sizes, t->opt, false);
-  fresh->adamStep = t->adamStep;
-  fresh->activeDegree = t->activeDegree;
-  try {
-    cudaStream_t f = fresh->stream;
-    const int32_t *src = table.get<int32_t>();
-    const uint32_t strides[4] = {3, 3, 4, 1};
-    sb::DeviceBuffer *from[4] = {&t->positions, &t->scales, &t->rotations, &t->opacities};
-    sb::DeviceBuffer *to[4] = {&fresh->positions, &fresh->scales, &fresh->rotations, &fresh->opacities};
-    for (int g = 0; g < 4; ++g)
-      sb::launch_gather_rows(src, from[g]->get<uint32_t>(), to[g]->get<uint32_t>(), newN, oldN, strides[g], 1u, f);
-    sb::launch_gather_planes(src, t->shDc.get<uint32_t>(), fresh->shDc.get<uint32_t>(), newN, fresh->planeStride, t->planeStride, 3u, f);
-    const uint32_t restPlanes = 3u * (uint32_t)(t->shCoeffs - 1);
-    if (t->shStore == sb::ShStore::F32)
-      sb::launch_gather_planes(src, t->shRest.get<uint32_t>(), fresh->shRest.get<uint32_t>(), newN, fresh->planeStride,
-                               t->planeStride, restPlanes, f);
-    else
-      sb::launch_gather_planes16(src, t->shRest.get<uint16_t>(), fresh->shRest.get<uint16_t>(), newN, fresh->planeStride,
-                                 t->planeStride, restPlanes, f);
-    const uint32_t copies = t->stateStore == sb::StateStore::F32 ? 2u : 1u;
-    for (int g = 0; g < 4; ++g)
-      sb::launch_gather_rows(src, t->state[g].get<uint32_t>(), fresh->state[g].get<uint32_t>(), newN, oldN, strides[g], copies, f);
-    sb::launch_gather_planes(src, t->state[4].get<uint32_t>(), fresh->state[4].get<uint32_t>(), newN, fresh->planeStride,
-                             t->planeStride, 3u * (uint32_t)t->shCoeffs * copies, f);
-    SB_CUDA(cudaGetLastError());
-    SB_CUDA(cudaStreamSynchronize(f));
-  } catch (...) {
-    delete fresh;
-    throw;
-  }
-  delete t;
-  handle->impl = fresh;
+  regather(handle, table.get<int32_t>(), table.get<int32_t>(), newN);
   return removed;
 }
 
+
 } // namespace
+} // extern "C"
+
+namespace {
+
+// ------------------------------------------------------------ densification
+
+// The smallest float x, in the order -inf .. +inf, for which holds(x), when
+// holds is false below some point and true from it on; NaN if it holds
+// nowhere. A bisection over the floats' bit patterns.
+template <class F> float first_holding(F holds) {
+  const auto from_key = [](uint32_t k) {
+    const uint32_t bits = (k & 0x80000000u) != 0u ? (k ^ 0x80000000u) : ~k;
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+  };
+  uint32_t lo = 0x007FFFFFu, hi = 0xFF800000u; // -inf, +inf
+  if (!holds(from_key(hi))) return std::numeric_limits<float>::quiet_NaN();
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (holds(from_key(mid))) hi = mid;
+    else lo = mid + 1;
+  }
+  return from_key(lo);
+}
+
+// Thresholds on the device's side of the comparisons densify_cloud makes
+// through the host's exp (densify.cpp:17,130,135,138): a Gaussian is larger
+// than s exactly when its largest log-scale is at least the first x with
+// exp(x) > s, and too transparent exactly when its logit is below the first
+// x whose sigmoid is not below the limit. The device then compares floats
+// only, and decides as the reference does bit for bit.
+float log_threshold(float scale) {
+  return first_holding([&](float x) { return std::exp(x) > scale; });
+}
+float logit_threshold(float limit) {
+  const float x = first_holding([&](float o) { return !(1.f / (1.f + std::exp(-o)) < limit); });
+  return std::isnan(x) ? std::numeric_limits<float>::infinity() : x;
+}
+
+// The Gaussian's rotation as a matrix, identity for a degenerate quaternion:
+// the same float arithmetic as densify.cpp:42-59, since the children's
+// positions are compared bit for bit.
+void rotation_matrix(const float q[4], float R[3][3]) {
+  float w = q[0], x = q[1], y = q[2], z = q[3];
+  const float length = std::sqrt(w * w + x * x + y * y + z * z);
+  if (length > 0.f) {
+    w /= length;
+    x /= length;
+    y /= length;
+    z /= length;
+  } else {
+    w = 1.f;
+    x = y = z = 0.f;
+  }
+  R[0][0] = 1.f - 2.f * (y * y + z * z);
+  R[0][1] = 2.f * (x * y - w * z);
+  R[0][2] = 2.f * (x * z + w * y);
+  R[1][0] = 2.f * (x * y + w * z);
+  R[1][1] = 1.f - 2.f * (x * x + z * z);
+  R[1][2] = 2.f * (y * z - w * x);
+  R[2][0] = 2.f * (x * z - w * y);
+  R[2][1] = 2.f * (y * z + w * x);
+  R[2][2] = 1.f - 2.f * (x * x + y * y);
+}
+
+// Rows of the old cloud gathered to the host for a list of indices.
+struct HostRows {
+  std::vector<float> positions, scales, rotations, opacities;
+  std::vector<uint32_t> actions;
+};
+
+} // namespace
+
+struct splat_rng {
+  std::mt19937 engine;
+};
+
+namespace {
+
+struct DensifyRun {
+  Trainer *t;
+  cudaStream_t s;
+  uint32_t n;
+  sb::DeviceBuffer counters, scanScratch, sortScratch, tmpKeys, tmpValues, rows;
+
+  explicit DensifyRun(Trainer *trainer) : t(trainer), s(trainer->stream), n(trainer->n) {
+    counters.ensure(64 * 4);
+    SB_CUDA(cudaMemsetAsync(counters.get(), 0, 64 * 4, s));
+    scanScratch.ensure(sb::bin_scan_scratch_bytes(n));
+    sortScratch.ensure(sb::sort_scratch_bytes(n, 4, 32, 8));
+    tmpKeys.ensure((size_t)n * 4);
+    tmpValues.ensure((size_t)n * 4);
+  }
+  uint32_t *error() { return counters.get<uint32_t>() + 63; }
+  // Exclusive scan of flags into place (both n words); the total lands in
+  // counter block `block` (word 1).
+  void scan(const sb::DeviceBuffer &flags, sb::DeviceBuffer &place, int block) {
+    SB_CUDA(cudaMemcpyAsync(place.get(), flags.get(), (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    sb::launch_exclusive_scan(n, place.get<uint32_t>(), counters.get<uint32_t>() + 4 * block, scanScratch.get(), error(), s);
+  }
+  // The counters, after the stream's work so far.
+  std::vector<uint32_t> read() {
+    std::vector<uint32_t> h(64);
+    SB_CUDA(cudaMemcpyAsync(h.data(), counters.get(), 64 * 4, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (h[63] != 0u) throw Failure{SPLAT_ERR_DEVICE, "a densification scan or sort gave up waiting"};
+    return h;
+  }
+  // Stable ascending sort of count (key, index) pairs; returns the indices.
+  const uint32_t *sort(sb::DeviceBuffer &keys, sb::DeviceBuffer &indices, uint32_t count) {
+    if (count <= 1) return indices.get<uint32_t>();
+    const int where = sb::sort_pairs_u32(keys.get<uint32_t>(), indices.get<uint32_t>(), tmpKeys.get<uint32_t>(),
+                                         tmpValues.get<uint32_t>(), n, count, nullptr, 0, 32, 8, sortScratch.get(), error(), s);
+    return where == 1 ? tmpValues.get<uint32_t>() : indices.get<uint32_t>();
+  }
+  // Downloads a device list of count indices.
+  std::vector<uint32_t> download(const uint32_t *list, uint32_t count) {
+    std::vector<uint32_t> h(count);
+    if (count > 0) SB_CUDA(cudaMemcpyAsync(h.data(), list, (size_t)count * 4, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    return h;
+  }
+  // The rows of `stride` words of `in` (n rows) for the count listed indices.
+  std::vector<float> gather(const int32_t *list, const void *in, uint32_t count, uint32_t stride) {
+    std::vector<float> h((size_t)count * stride);
+    if (count == 0) return h;
+    rows.ensure((size_t)count * stride * 4);
+    sb::launch_gather_rows(list, static_cast<const uint32_t *>(in), rows.get<uint32_t>(), count, n, stride, 1u, s);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaMemcpyAsync(h.data(), rows.get(), h.size() * 4, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    return h;
+  }
+};
+
+// Trainer::densify on the GPU (trainer.cpp:710-715; densify_cloud,
+// densify.cpp:115-326; apply_changes). Every per-Gaussian decision, both
+// global selections and the tables run on the device; the host draws from
+// rng in the reference's order (edge splits, the exploration shuffle, the
+// split children in index order, the seeds) over lists the device compacted.
+void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, std::mt19937 &rng, splat_densify_result *result,
+                       int64_t *source, uint64_t sourceCapacity) {
+  Trainer *t = impl_of(handle);
+  if (o.transparent_share < 0.0) throw Failure{SPLAT_ERR_INVALID, "transparent_share must not be negative"};
+  SB_CUDA(cudaStreamSynchronize(t->stream));
+  if (t->densifyStats.get() == nullptr) throw Failure{SPLAT_ERR_STATE, "no densification statistics"};
+  DensifyRun run(t);
+  cudaStream_t s = run.s;
+  const uint32_t n = run.n;
+  const float *stats = t->densifyStats.get<float>();
+  const float *scales = t->scales.get<float>();
+
+  sb::DensifyArgs a{};
+  a.gradientThreshold = o.gradient_threshold;
+  a.splitThreshold = o.split_threshold;
+  a.maxScreenRadius = o.max_screen_radius;
+  a.minMarkedPixels = o.min_marked_pixels;
+  a.worldLog = log_threshold(o.max_world_scale);
+  a.denseLog = log_threshold(o.dense_scale);
+  a.opacityLogit = logit_threshold(o.prune_opacity);
+  a.pruneLarge = o.prune_large != 0 ? 1 : 0;
+  a.scoredViews = o.scored_views;
+  a.allTransparent = o.transparent_share < 1.0 ? 0 : 1;
+  a.edgeSplit = o.edge_split != 0 ? 1 : 0;
+
+  sb::DeviceBuffer action, flags, keys, place, list, keyList, kept, keptPlace, candidate, candidatePlace, priority, chosen;
+  for (sb::DeviceBuffer *b : {&action, &flags, &keys, &place, &list, &keyList, &kept, &keptPlace, &candidate, &candidatePlace,
+                              &priority, &chosen})
+    b->ensure((size_t)n * 4);
+
+  // The oversized, the non-finite and the too transparent.
+  sb::launch_densify_classify(t->params(), stats, a, action.get<uint32_t>(), flags.get<uint32_t>(), keys.get<uint32_t>(), s);
+  if (!a.allTransparent) {
+    run.scan(flags, place, 0);
+    const uint32_t clear = run.read()[1];
+    sb::launch_compact(flags.get<uint32_t>(), place.get<uint32_t>(), keys.get<uint32_t>(), n, list.get<uint32_t>(),
+                       keyList.get<uint32_t>(), s);
+    const uint32_t *order = run.sort(keyList, list, clear);
+    const auto removed = (uint32_t)std::ceil((double)clear * o.transparent_share);
+    sb::launch_set_first(order, std::min(removed, clear), sb::kDensifyPrune, action.get<uint32_t>(), s);
+  }
+
+  // Candidates, and the count limit.
+  sb::launch_densify_candidates(scales, stats, a, n, action.get<uint32_t>(), kept.get<uint32_t>(), candidate.get<uint32_t>(),
+                                priority.get<uint32_t>(), s);
+  run.scan(kept, keptPlace, 1);
+  run.scan(candidate, candidatePlace, 2);
+  std::vector<uint32_t> c = run.read();
+  const uint64_t keptCount = c[5], candidates = c[9];
+  const uint64_t room = o.max_gaussians > keptCount ? o.max_gaussians - keptCount : 0;
+  uint64_t chosenCount = candidates, heldBack = 0;
+  if (candidates > room) {
+    sb::launch_compact(candidate.get<uint32_t>(), candidatePlace.get<uint32_t>(), priority.get<uint32_t>(), n, list.get<uint32_t>(),
+                       keyList.get<uint32_t>(), s);
+    const uint32_t *order = run.sort(keyList, list, (uint32_t)candidates);
+    SB_CUDA(cudaMemsetAsync(chosen.get(), 0, (size_t)n * 4, s));
+    sb::launch_set_first(order, (uint32_t)room, 1u, chosen.get<uint32_t>(), s);
+    heldBack = candidates - room;
+    chosenCount = room;
+  } else {
+    SB_CUDA(cudaMemcpyAsync(chosen.get(), candidate.get(), (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  }
+
+  // Edge splits (densify.cpp:181-190): each chosen candidate stays with
+  // probability score / best, drawn in index order.
+  if (a.edgeSplit && chosenCount > 0) {
+    run.scan(chosen, place, 3);
+    sb::launch_compact(chosen.get<uint32_t>(), place.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
+    const std::vector<uint32_t> listed = run.download(list.get<uint32_t>(), (uint32_t)chosenCount);
+    const std::vector<float> rowsOf = run.gather(list.get<int32_t>(), stats, (uint32_t)chosenCount, sb::kStatStride);
+    float best = 0.f;
+    for (size_t k = 0; k < listed.size(); ++k) best = std::max(best, rowsOf[k * sb::kStatStride + 7]);
+    if (best > 0.f) {
+      std::uniform_real_distribution<float> draw(0.f, 1.f);
+      std::vector<uint32_t> stay;
+      for (size_t k = 0; k < listed.size(); ++k)
+        if (!(draw(rng) > rowsOf[k * sb::kStatStride + 7] / best)) stay.push_back(listed[k]);
+      SB_CUDA(cudaMemsetAsync(chosen.get(), 0, (size_t)n * 4, s));
+      if (!stay.empty()) {
+        SB_CUDA(cudaMemcpyAsync(list.get(), stay.data(), stay.size() * 4, cudaMemcpyHostToDevice, s));
+        sb::launch_set_first(list.get<uint32_t>(), (uint32_t)stay.size(), 1u, chosen.get<uint32_t>(), s);
+      }
+      SB_CUDA(cudaStreamSynchronize(s));
+      chosenCount = stay.size();
+    }
+  }
+  sb::launch_densify_choose(scales, a, n, chosen.get<uint32_t>(), action.get<uint32_t>(), s);
+
+  // Exploration (densify.cpp:207-224): of the large Gaussians left alone,
+  // the larger half by summed log-scale, shuffled, and the first few split.
+  uint64_t left = room - chosenCount, exploreSplits = 0;
+  if (o.explore_splits > 0 && left > 0) {
+    sb::launch_densify_large(scales, a, n, action.get<uint32_t>(), flags.get<uint32_t>(), s);
+    run.scan(flags, place, 4);
+    const uint32_t count = run.read()[17];
+    sb::launch_compact(flags.get<uint32_t>(), place.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
+    const std::vector<uint32_t> listed = run.download(list.get<uint32_t>(), count);
+    const std::vector<float> rowsOf = run.gather(list.get<int32_t>(), scales, count, 3);
+    std::vector<float> sums(n);
+    for (size_t k = 0; k < listed.size(); ++k) sums[listed[k]] = rowsOf[k * 3] + rowsOf[k * 3 + 1] + rowsOf[k * 3 + 2];
+    std::vector<size_t> large(listed.begin(), listed.end());
+    const auto middle = large.begin() + static_cast<std::ptrdiff_t>(large.size() / 2);
+    std::nth_element(large.begin(), middle, large.end(), [&](size_t x, size_t y) { return sums[x] > sums[y]; });
+    large.resize((large.size() + 1) / 2);
+    std::shuffle(large.begin(), large.end(), rng);
+    exploreSplits = std::min<uint64_t>({o.explore_splits, (uint64_t)large.size(), left});
+    if (exploreSplits > 0) {
+      std::vector<uint32_t> picked(large.begin(), large.begin() + static_cast<std::ptrdiff_t>(exploreSplits));
+      SB_CUDA(cudaMemcpyAsync(list.get(), picked.data(), picked.size() * 4, cudaMemcpyHostToDevice, s));
+      sb::launch_set_first(list.get<uint32_t>(), (uint32_t)picked.size(), sb::kDensifySplit, action.get<uint32_t>(), s);
+      SB_CUDA(cudaStreamSynchronize(s));
+    }
+    left -= exploreSplits;
+  }
+
+  // Seeds (densify.cpp:226-251): the survivors' box and median mean
+  // log-scale, from their rows.
+  uint64_t seeded = std::min<uint64_t>(o.explore_seeds, left);
+  std::vector<uint32_t> survivors;
+  float low[3], high[3], seedScale = 0.f;
+  if (seeded > 0) {
+    if (keptCount == 0) {
+      seeded = 0;
+    } else {
+      sb::launch_compact(kept.get<uint32_t>(), keptPlace.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
+      survivors = run.download(list.get<uint32_t>(), (uint32_t)keptCount);
+      const std::vector<float> at = run.gather(list.get<int32_t>(), t->positions.get(), (uint32_t)keptCount, 3);
+      const std::vector<float> sc = run.gather(list.get<int32_t>(), scales, (uint32_t)keptCount, 3);
+      std::fill(low, low + 3, std::numeric_limits<float>::max());
+      std::fill(high, high + 3, std::numeric_limits<float>::lowest());
+      std::vector<float> means;
+      means.reserve(survivors.size());
+      for (size_t k = 0; k < survivors.size(); ++k) {
+        for (size_t d = 0; d < 3; ++d) {
+          low[d] = std::min(low[d], at[k * 3 + d]);
+          high[d] = std::max(high[d], at[k * 3 + d]);
+        }
+        means.push_back((sc[k * 3] + sc[k * 3 + 1] + sc[k * 3 + 2]) / 3.f);
+      }
+      std::nth_element(means.begin(), means.begin() + static_cast<std::ptrdiff_t>(means.size() / 2), means.end());
+      seedScale = means[means.size() / 2];
+    }
+  }
+
+  // The new cloud's layout.
+  sb::DeviceBuffer &survivor = kept, &survivorPlace = keptPlace, &added = candidate, &addedPlace = candidatePlace;
+  sb::DeviceBuffer &patched = flags, &patchedPlace = place;
+  sb::launch_densify_flags(n, action.get<uint32_t>(), survivor.get<uint32_t>(), added.get<uint32_t>(), patched.get<uint32_t>(), s);
+  run.scan(survivor, survivorPlace, 5);
+  run.scan(added, addedPlace, 6);
+  run.scan(patched, patchedPlace, 7);
+  c = run.read();
+  const uint64_t survivorCount = c[21], addedCount = c[25], parentsCount = c[29];
+  const uint64_t newCount = survivorCount + addedCount + seeded;
+  if (newCount == 0) throw Failure{SPLAT_ERR_INVALID, "densification removed every Gaussian"};
+  if (newCount > 0x7FFFFFFFull) throw Failure{SPLAT_ERR_INVALID, "densification would exceed 2^31 - 1 Gaussians"};
+  const auto newN = (uint32_t)newCount;
+  sb::DeviceBuffer paramSource, stateSource, parents, childSlot, patches;
+  paramSource.ensure((size_t)newN * 4);
+  stateSource.ensure((size_t)newN * 4);
+  parents.ensure(std::max<size_t>(parentsCount, 1) * 4);
+  childSlot.ensure(std::max<size_t>(parentsCount, 1) * 4);
+  sb::launch_densify_tables(n, (uint32_t)survivorCount, action.get<uint32_t>(), survivorPlace.get<uint32_t>(),
+                            addedPlace.get<uint32_t>(), patchedPlace.get<uint32_t>(), paramSource.get<int32_t>(),
+                            stateSource.get<int32_t>(), parents.get<uint32_t>(), childSlot.get<uint32_t>(), s);
+
+  // Split children (densify.cpp:264-299), in index order: samples of the
+  // parent shrunk by 1.6, or two halves along the longest axis.
+  std::vector<sb::DensifyPatch> rowsOut;
+  const std::vector<uint32_t> parentList = run.download(parents.get<uint32_t>(), (uint32_t)parentsCount);
+  const std::vector<uint32_t> slots = run.download(childSlot.get<uint32_t>(), (uint32_t)parentsCount);
+  uint64_t splits = 0, longAxis = 0;
+  if (parentsCount > 0) {
+    const auto *listed = parents.get<int32_t>();
+    const std::vector<float> at = run.gather(listed, t->positions.get(), (uint32_t)parentsCount, 3);
+    const std::vector<float> sc = run.gather(listed, scales, (uint32_t)parentsCount, 3);
+    const std::vector<float> rot = run.gather(listed, t->rotations.get(), (uint32_t)parentsCount, 4);
+    const std::vector<float> op = run.gather(listed, t->opacities.get(), (uint32_t)parentsCount, 1);
+    const std::vector<float> acts = run.gather(listed, action.get(), (uint32_t)parentsCount, 1);
+    const float shrink = std::log(1.6f);
+    for (size_t k = 0; k < parentList.size(); ++k) {
+      uint32_t act;
+      std::memcpy(&act, &acts[k], 4);
+      float R[3][3];
+      if (act == sb::kDensifySplit) {
+        ++splits;
+        for (uint32_t child = 0; child < 2; ++child) {
+          sb::DensifyPatch q{};
+          q.slot = slots[k] + child;
+          std::normal_distribution<float> normal(0.f, 1.f);
+          const float local[3] = {normal(rng) * std::exp(sc[k * 3]), normal(rng) * std::exp(sc[k * 3 + 1]),
+                                  normal(rng) * std::exp(sc[k * 3 + 2])};
+          rotation_matrix(&rot[k * 4], R);
+          for (int r = 0; r < 3; ++r) {
+            q.position[r] = at[k * 3 + r] + R[r][0] * local[0] + R[r][1] * local[1] + R[r][2] * local[2];
+            q.scale[r] = sc[k * 3 + r] - shrink;
+          }
+          rowsOut.push_back(q);
+        }
+      } else {
+        ++longAxis;
+        // Tangent to the parent at its ends: 0.45 of the semi-axis out, 0.55
+        // of it long, the other axes shrunk to stay inside, 0.6 of the opacity.
+        constexpr float kOffset = 0.45f;
+        const float *own = &sc[k * 3];
+        const int axis = (int)(std::max_element(own, own + 3) - own);
+        rotation_matrix(&rot[k * 4], R);
+        const float length = std::exp(own[axis]);
+        const double opacity = 0.6 * (1.f / (1.f + std::exp(-op[k])));
+        const float sides[2] = {-1.f, 1.f};
+        for (uint32_t child = 0; child < 2; ++child) {
+          sb::DensifyPatch q{};
+          q.slot = slots[k] + child;
+          q.what = sb::kPatchOpacity;
+          for (int d = 0; d < 3; ++d) {
+            q.position[d] = at[k * 3 + d] + sides[child] * kOffset * length * R[d][axis];
+            q.scale[d] = own[d] + (d == axis ? std::log(1.f - kOffset) : 0.5f * std::log(1.f - kOffset * kOffset));
+          }
+          q.opacity = static_cast<float>(std::log(opacity / (1.0 - opacity)));
+          rowsOut.push_back(q);
+        }
+      }
+    }
+  }
+
+  // Seeds: a random survivor's colour at a random place in the box, of the
+  // median size, unrotated, opacity 0.1, the same colour from all sides.
+  std::vector<int32_t> seedSources;
+  for (uint64_t k = 0; k < seeded; ++k) {
+    const size_t pick = std::uniform_int_distribution<size_t>(0, survivors.size() - 1)(rng);
+    seedSources.push_back((int32_t)survivors[pick]);
+    sb::DensifyPatch q{};
+    q.slot = (uint32_t)(survivorCount + addedCount + k);
+    q.what = sb::kPatchRotation | sb::kPatchOpacity | sb::kPatchShRest;
+    for (int d = 0; d < 3; ++d) {
+      q.position[d] = std::uniform_real_distribution<float>(low[d], high[d])(rng);
+      q.scale[d] = seedScale;
+    }
+    q.rotation[0] = 1.f;
+    q.opacity = std::log(0.1f / 0.9f);
+    rowsOut.push_back(q);
+  }
+  if (!seedSources.empty()) {
+    const std::vector<int32_t> fresh(seedSources.size(), -1);
+    const size_t offset = (size_t)(survivorCount + addedCount) * 4;
+    SB_CUDA(cudaMemcpyAsync(paramSource.get<uint8_t>() + offset, seedSources.data(), seedSources.size() * 4, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(stateSource.get<uint8_t>() + offset, fresh.data(), fresh.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  if (!rowsOut.empty()) {
+    patches.ensure(rowsOut.size() * sizeof(sb::DensifyPatch));
+    SB_CUDA(cudaMemcpyAsync(patches.get(), rowsOut.data(), rowsOut.size() * sizeof(sb::DensifyPatch), cudaMemcpyHostToDevice, s));
+  }
+  std::vector<int32_t> table;
+  if (source != nullptr && sourceCapacity >= newCount) {
+    table.resize(newN);
+    SB_CUDA(cudaMemcpyAsync(table.data(), stateSource.get(), (size_t)newN * 4, cudaMemcpyDeviceToHost, s));
+  }
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaStreamSynchronize(s));
+
+  Trainer *fresh = regather(handle, paramSource.get<int32_t>(), stateSource.get<int32_t>(), newN);
+  if (!rowsOut.empty()) {
+    const uint32_t restPlanes = 3u * (uint32_t)(fresh->shCoeffs - 1);
+    sb::launch_densify_patch(patches.get<sb::DensifyPatch>(), (uint32_t)rowsOut.size(), fresh->positions.get<float>(),
+                             fresh->scales.get<float>(), fresh->rotations.get<float>(), fresh->opacities.get<float>(),
+                             fresh->shRest.get(), restPlanes, fresh->planeStride, fresh->shStore == sb::ShStore::F32 ? 4u : 2u,
+                             fresh->stream);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(fresh->stream));
+  }
+  for (size_t i = 0; i < table.size(); ++i) source[i] = table[i];
+  if (result != nullptr) {
+    result->count = newCount;
+    result->cloned = addedCount - 2 * parentsCount;
+    result->split = splits + longAxis;
+    result->seeded = seeded;
+    result->pruned = n - keptCount;
+    result->held_back = heldBack;
+  }
+}
+
+} // namespace
+
+extern "C" {
+
+int splat_rng_create(uint32_t seed, splat_rng **out) {
+  return guarded([&] {
+    if (out == nullptr) throw Failure{SPLAT_ERR_INVALID, "null output"};
+    *out = new splat_rng{std::mt19937(seed)};
+  });
+}
+
+int splat_rng_destroy(splat_rng *rng) {
+  delete rng;
+  return SPLAT_OK;
+}
+
+int splat_rng_pick(splat_rng *rng, uint64_t count, uint64_t *out) {
+  return guarded([&] {
+    if (rng == nullptr || out == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    if (count == 0) throw Failure{SPLAT_ERR_INVALID, "nothing to pick from"};
+    *out = std::uniform_int_distribution<size_t>(0, (size_t)count - 1)(rng->engine);
+  });
+}
+
+void splat_densify_options_default(splat_densify_options *options) {
+  if (options == nullptr) return;
+  *options = splat_densify_options{};
+  options->gradient_threshold = 2e-4f;
+  options->dense_scale = 0.f;
+  options->prune_opacity = 0.005f;
+  options->prune_large = 0;
+  options->max_screen_radius = 20.f;
+  options->max_world_scale = 0.f;
+  options->max_gaussians = UINT64_MAX;
+  options->split_threshold = 0.f;
+  options->scored_views = 0;
+  options->min_marked_pixels = 5.f;
+  options->transparent_share = 1.0;
+  options->explore_splits = 0;
+  options->explore_seeds = 0;
+  options->edge_split = 0;
+}
+
+int splat_trainer_densify(splat_trainer *trainer, const splat_densify_options *options, splat_rng *rng,
+                          splat_densify_result *result, int64_t *source, uint64_t source_capacity) {
+  return guarded([&] {
+    if (options == nullptr || rng == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    densify_gaussians(trainer, *options, rng->engine, result, source, source_capacity);
+  });
+}
 
 int splat_trainer_remove_largest(splat_trainer *trainer, double share, uint64_t *removed) {
   return guarded([&] {
