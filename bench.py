@@ -602,6 +602,35 @@ def our_arm(args) -> None:
             if "issue" in r:
                 roof["issue"] = r["issue"]
 
+    # Densification on the GPU with the statistics the timed steps collected:
+    # the session's dense scale (1 % of the scene extent) and a count cap of
+    # 5 % growth. The reference's own densify_cloud on the same cloud and
+    # statistics is timed beside it on the host (its download of the cloud
+    # and upload of the result not included).
+    densify = None
+    if not args.no_densify:
+        held = trainer.cloud()
+        raw = trainer.densify_stats_raw()
+        centre = held.positions.reshape(-1, 3).mean(axis=0)
+        extent = float(np.linalg.norm(held.positions.reshape(-1, 3) - centre, axis=1).max())
+        d_opts = splat.DensifyOptions(dense_scale=0.01 * extent, max_gaussians=int(n * 1.05))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = trainer.densify(d_opts, splat.Rng(1))
+        d_ms = (time.perf_counter() - t0) * 1000.0
+        densify = {"ms": d_ms, "of": n, "count": r.count, "cloned": r.cloned, "split": r.split, "pruned": r.pruned,
+                   "held_back": r.held_back}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            from oracle import oracle as O
+
+            if O.have_reference():
+                c = O.Cloud(DEGREE, held.positions, held.scales, held.rotations, held.opacities, held.sh)
+                t0 = time.perf_counter()
+                ref = O.ref_densify(c, raw, d_opts._c(), O.RefRng(1))
+                densify["reference_cpu_ms"] = (time.perf_counter() - t0) * 1000.0
+                densify["reference_same_result"] = bool(np.array_equal(ref.source, r.source))
+        del held, raw
+
     # Pruning on the GPU (remove_largest_gaussians, 1 % of the Gaussians):
     # keys, sort, scan and the gathers of parameters and optimiser state.
     t0 = time.perf_counter()
@@ -665,6 +694,7 @@ def our_arm(args) -> None:
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "sm_peaks": sm_peaks,
         "score_view_ms": score_ms,
+        "densify": densify,
         "prune": prune,
         "roofline": roof,
         "stage_roofline": stage_roof,
@@ -693,6 +723,7 @@ def main() -> None:
                              "recompute vs store-everything backward; batched: 3M Gaussians, 8 uneven views per step")
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
+    parser.add_argument("--no-densify", action="store_true", help="skip the densification timing")
     parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
     parser.add_argument("--no-autotune", action="store_true", help="keep the chosen form's sort settings")
     parser.add_argument("--sort-form", type=int, choices=[0, 1], default=None,

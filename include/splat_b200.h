@@ -297,6 +297,28 @@ typedef struct splat_densify_result {
 int splat_trainer_densify(splat_trainer *trainer, const splat_densify_options *options, splat_rng *rng,
                           splat_densify_result *result, int64_t *source, uint64_t source_capacity);
 
+/* RelocateOptions (densify.hpp:87-91). */
+typedef struct splat_relocate_options {
+  float min_opacity;      /* 0.005: at or below, dead, to be relocated */
+  double growth;          /* 0.05: share of the count added per round, within max_gaussians */
+  uint64_t max_gaussians; /* UINT64_MAX */
+} splat_relocate_options;
+void splat_relocate_options_default(splat_relocate_options *options);
+
+/* Trainer::relocate (trainer.cpp:717-722, relocate_cloud of densify.cpp:
+ * 328-420, 3DGS-MCMC): the dead (opacity at or below min_opacity, or a value
+ * not finite) move onto live Gaussians drawn in proportion to opacity, then
+ * the count grows by growth the same way; a target that becomes N copies
+ * takes opacity 1 - (1 - o)^(1/N) and its scale times o / D (gsplat's
+ * divisor). Copies and targets start with fresh optimiser state; result
+ * counts the relocated as cloned and the growth as seeded. The dead/alive
+ * split and the gathers run on the GPU; the draws and the opacity and scale
+ * updates, a sequential chain over std::discrete_distribution, on the host
+ * from rng in the reference's order. With nothing alive the cloud stays and
+ * only the statistics start anew. source as splat_trainer_densify. */
+int splat_trainer_relocate(splat_trainer *trainer, const splat_relocate_options *options, splat_rng *rng,
+                           splat_densify_result *result, int64_t *source, uint64_t source_capacity);
+
 /* Trainer methods with no kernel in this library, for callers that set them
  * unconditionally: the neutral setting is accepted and changes nothing, any
  * other returns SPLAT_ERR_UNSUPPORTED. set_exposure (trainer.hpp:154): the

@@ -265,6 +265,26 @@ def ref_densify(cloud: Cloud, raw_stats: np.ndarray, options, rng: RefRng) -> Re
     return RefDensified(result, source[:n], {k: int(v) for k, v in zip(names, counts)})
 
 
+def ref_relocate(cloud: Cloud, options, rng: RefRng) -> RefDensified:
+    """The reference's relocate_cloud (densify.cpp:328-420). options: a ctypes
+    structure laid out as RelocateOptions in the product's field order."""
+    keep, cargs = _cloud_args(cloud)
+    room = cloud.count + int(max(0.0, options.growth) * cloud.count) + 1
+    coeffs = (cloud.sh_degree + 1) ** 2
+    out = [np.zeros(room * k, np.float32) for k in (3, 3, 4, 1, 3 * coeffs)]
+    source = np.zeros(room, np.int64)
+    counts = np.zeros(6, np.uint64)
+    status = ref_lib().ref_relocate(ctypes.c_int(cloud.count), ctypes.c_int(cloud.sh_degree), *cargs, ctypes.byref(options),
+                                    rng._h, *[_fp(a) for a in out], source.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                    counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+    if status != 0:
+        raise ValueError("the reference's relocate_cloud threw")
+    n = int(counts[0])
+    result = Cloud(cloud.sh_degree, out[0][: n * 3], out[1][: n * 3], out[2][: n * 4], out[3][:n], out[4][: n * 3 * coeffs])
+    names = ("count", "cloned", "split", "seeded", "pruned", "held_back")
+    return RefDensified(result, source[:n], {k: int(v) for k, v in zip(names, counts)})
+
+
 def ref_save_ply(cloud: Cloud, path) -> None:
     """The reference's save_ply (gaussian_cloud.cpp:330-365)."""
     keep, cargs = _cloud_args(cloud)

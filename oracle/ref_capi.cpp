@@ -304,4 +304,38 @@ int ref_densify(int n, int degree, const float *positions, const float *scales, 
   }
 }
 
+// RelocateOptions (densify.hpp:87-91) in the product's field order.
+struct RefRelocateOptions {
+  float minOpacity;
+  double growth;
+  std::uint64_t maxGaussians;
+};
+
+// relocate_cloud (densify.cpp:328-420): the out* arrays have room for
+// n + growth n + 1 Gaussians; counts as ref_densify.
+int ref_relocate(int n, int degree, const float *positions, const float *scales, const float *rotations, const float *opacities,
+                 const float *sh, const RefRelocateOptions *o, void *rng, float *outPositions, float *outScales,
+                 float *outRotations, float *outOpacities, float *outSh, std::int64_t *source, std::uint64_t *counts) {
+  try {
+    const GaussianCloud cloud = make_cloud(n, degree, positions, scales, rotations, opacities, sh);
+    RelocateOptions options;
+    options.minOpacity = o->minOpacity;
+    options.growth = o->growth;
+    options.maxGaussians = o->maxGaussians;
+    const DensifyResult r = relocate_cloud(cloud, options, *static_cast<std::mt19937 *>(rng));
+    const GaussianCloud &c = r.cloud;
+    std::memcpy(outPositions, c.positions.data(), c.positions.size() * sizeof(float));
+    std::memcpy(outScales, c.scales.data(), c.scales.size() * sizeof(float));
+    std::memcpy(outRotations, c.rotations.data(), c.rotations.size() * sizeof(float));
+    std::memcpy(outOpacities, c.opacities.data(), c.opacities.size() * sizeof(float));
+    std::memcpy(outSh, c.sh.data(), c.sh.size() * sizeof(float));
+    std::memcpy(source, r.source.data(), r.source.size() * sizeof(std::int64_t));
+    const std::uint64_t out[6] = {c.size(), r.cloned, r.split, r.seeded, r.pruned, r.heldBack};
+    std::memcpy(counts, out, sizeof(out));
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
 } // extern "C"

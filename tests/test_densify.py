@@ -357,3 +357,96 @@ def test_densify_keeps_the_generator_across_rounds_and_refuses_an_empty_result(s
     with pytest.raises(splat.SplatError):
         trainer.densify(options_of(), splat.Rng(1))
     assert trainer.cloud().opacities.size == 3
+
+
+# ----------------------------------------------------------------- relocation
+
+
+def logit(p):
+    return np.float32(np.log(np.float32(p) / (np.float32(1.0) - np.float32(p))))
+
+
+def relocation_scenarios(O):
+    """(name, cloud, RelocateOptions changes, seed, expected) after test_densify.cpp:355-415."""
+    splat = splat_module()
+    out = []
+    c = line_of(O, 2, 0.1)
+    c.opacities[:] = [logit(0.9), logit(0.001)]
+    out.append(("dead onto live", c, splat.RelocateOptions(max_gaussians=2), 1, dict(count=2, cloned=1, seeded=0)))
+    c = line_of(O, 1002, 0.1)
+    c.opacities[:] = logit(0.001)
+    c.opacities[0], c.opacities[1] = logit(0.9), logit(0.09)
+    out.append(("in proportion", c, splat.RelocateOptions(max_gaussians=1002), 1, dict(count=1002)))
+    out.append(("growth", line_of(O, 1000, 0.1), splat.RelocateOptions(max_gaussians=1030), 1,
+                dict(count=1030, seeded=30, cloned=0)))
+    out.append(("growth capped", line_of(O, 1000, 0.1), splat.RelocateOptions(max_gaussians=1000), 1,
+                dict(count=1000, seeded=0)))
+    out.append(("nothing alive", line_of(O, 5, 0.1, 0.001), splat.RelocateOptions(), 1, dict(count=5, cloned=0)))
+    c = line_of(O, 4, 0.1)
+    c.positions[3] = np.nan
+    c.sh[2 * 3 + 1] = np.inf
+    out.append(("non-finite are dead", c, splat.RelocateOptions(max_gaussians=4), 3, dict(count=4, cloned=2)))
+    return out
+
+
+@needs_reference
+def test_reference_relocation_matches_its_own_tests(O):
+    # relocate_cloud through the oracle wrapper, against the reference's tests:
+    # the relocated pair's opacity 1 - sqrt(1 - 0.9) and scale 0.1 * 0.9 / D,
+    # targets drawn in proportion to opacity, growth within the cap.
+    for name, cloud, options, seed, expected in relocation_scenarios(O):
+        r = O.ref_relocate(cloud, options._c(), O.RefRng(seed))
+        _check_expected(name, r, expected)
+        if name == "dead onto live":
+            fresh = 1.0 - math.sqrt(1.0 - 0.9)
+            d = sum(math.comb(i - 1, k) * (-1) ** k * fresh ** (k + 1) / math.sqrt(k + 1)
+                    for i in range(1, 3) for k in range(i))
+            for i in range(2):
+                assert abs(1.0 / (1.0 + math.exp(-r.cloud.opacities[i])) - fresh) < 1e-5
+                assert abs(math.exp(r.cloud.scales[i * 3]) - 0.1 * 0.9 / d) < 1e-5
+                assert r.source[i] == -1
+        if name == "in proportion":
+            on_first = int(np.sum(r.cloud.positions.reshape(-1, 3)[2:, 0] == 0.0))
+            assert 850 < on_first < 950
+
+
+@pytest.mark.gpu
+def test_relocation_matches_the_reference(splat, O):
+    # Trainer::relocate on the GPU and host against relocate_cloud: the
+    # reference's scenarios, then a random cloud with dead and non-finite
+    # Gaussians over two rounds on one generator, F16 and F32 SH: the same
+    # counts, source table, new cloud bit for bit, and the untouched
+    # Gaussians' Adam state.
+    for name, cloud, options, seed, expected in relocation_scenarios(O):
+        trainer, held = _trainer_for(splat, O, cloud, stats_of(cloud.count, 0.0))
+        ref = O.ref_relocate(held, options._c(), O.RefRng(seed))
+        r = trainer.relocate(options, splat.Rng(seed))
+        for key in ("count", "cloned", "seeded"):
+            assert getattr(r, key) == ref.counts[key], f"{name}: {key}"
+        np.testing.assert_array_equal(r.source, ref.source, name)
+        _assert_same_cloud(name, trainer.cloud(), ref.cloud)
+    for storage in (splat.SH_F16, splat.SH_F32):
+        cloud, raw = _random_case(O, 4000, 2, 77)
+        trainer, held = _trainer_for(splat, O, cloud, raw, storage)
+        view = O.train_camera(72, 56)
+        target = O.smooth_target(72, 56, 5)
+        trainer.step(to_camera(view), target, splat.LearningRates())
+        rng, ref_rng = splat.Rng(21), O.RefRng(21)
+        options = splat.RelocateOptions(min_opacity=0.01, growth=0.05, max_gaussians=4300)
+        for round_ in range(2):
+            before = trainer.cloud()
+            held = O.Cloud(2, before.positions, before.scales, before.rotations, before.opacities, before.sh)
+            m0 = held.count
+            states = [trainer.debug_download(splat.DEBUG_STATE + g, np.uint32) for g in range(4)]
+            ref = O.ref_relocate(held, options._c(), ref_rng)
+            r = trainer.relocate(options, rng)
+            assert (r.count, r.cloned, r.seeded) == (ref.counts["count"], ref.counts["cloned"], ref.counts["seeded"])
+            assert r.cloned > 0
+            np.testing.assert_array_equal(r.source, ref.source)
+            _assert_same_cloud(f"random round {round_}", trainer.cloud(), ref.cloud)
+            kept = r.source >= 0
+            for g, width in enumerate((3, 3, 4, 1)):
+                new = trainer.debug_download(splat.DEBUG_STATE + g, np.uint32).reshape(r.count, width)
+                np.testing.assert_array_equal(new[kept], states[g].reshape(m0, width)[r.source[kept]])
+                assert np.all(new[~kept] == 0)
+        assert math.isfinite(trainer.step(to_camera(view), target, splat.LearningRates()).loss)

@@ -199,6 +199,13 @@ class _DensifyResult(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in ("count", "cloned", "split", "seeded", "pruned", "held_back")]
 
 
+class _RelocateOptions(ctypes.Structure):
+    _fields_ = [("min_opacity", ctypes.c_float), ("growth", ctypes.c_double), ("max_gaussians", ctypes.c_uint64)]
+
+
+_lib.splat_relocate_options_default.argtypes = [ctypes.POINTER(_RelocateOptions)]
+_lib.splat_trainer_relocate.argtypes = [_P, ctypes.POINTER(_RelocateOptions), _P, ctypes.POINTER(_DensifyResult),
+                                        ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64]
 _lib.splat_rng_create.argtypes = [ctypes.c_uint32, ctypes.POINTER(_P)]
 _lib.splat_rng_destroy.argtypes = [_P]
 _lib.splat_rng_pick.argtypes = [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
@@ -433,6 +440,18 @@ class DensifyOptions:
             value = getattr(self, name)
             setattr(o, name, int(value) if isinstance(value, bool) else value)
         return o
+
+
+@dataclass
+class RelocateOptions:
+    """RelocateOptions (densify.hpp:87-91)."""
+
+    min_opacity: float = 0.005
+    growth: float = 0.05
+    max_gaussians: int = 2**64 - 1
+
+    def _c(self) -> _RelocateOptions:
+        return _RelocateOptions(self.min_opacity, self.growth, int(self.max_gaussians))
 
 
 @dataclass
@@ -675,6 +694,12 @@ class Trainer:
         r = raw.reshape(-1, 8)
         return DensifyStats(*(r[:, k].copy() for k in range(8)))
 
+    def densify_stats_raw(self) -> np.ndarray:
+        """The statistics as stored: 8 floats per Gaussian (trainer.cpp:686-708)."""
+        raw = np.empty(self._count * 8, np.float32)
+        _check(_lib.splat_trainer_get_densify_stats(self._h, _fptr(raw)))
+        return raw.reshape(-1, 8)
+
     def set_densify_stats(self, raw) -> None:
         """Replaces the statistics: 8 floats per Gaussian, the layout densify_stats reads."""
         r = np.ascontiguousarray(np.asarray(raw, np.float32).ravel())
@@ -699,6 +724,17 @@ class Trainer:
         r = _DensifyResult()
         _check(_lib.splat_trainer_densify(self._h, ctypes.byref(options._c()), rng._h, ctypes.byref(r),
                                           source.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), capacity))
+        self._count = r.count
+        return DensifyResult(r.count, r.cloned, r.split, r.seeded, r.pruned, r.held_back, source[:r.count].copy())
+
+    def relocate(self, options: RelocateOptions, rng: Rng) -> DensifyResult:
+        """Trainer::relocate (trainer.cpp:717-722): 3DGS-MCMC relocation of the
+        dead onto live Gaussians, then growth."""
+        capacity = self._count + int(max(0.0, options.growth) * self._count) + 1
+        source = np.empty(capacity, np.int64)
+        r = _DensifyResult()
+        _check(_lib.splat_trainer_relocate(self._h, ctypes.byref(options._c()), rng._h, ctypes.byref(r),
+                                           source.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), capacity))
         self._count = r.count
         return DensifyResult(r.count, r.cloned, r.split, r.seeded, r.pruned, r.held_back, source[:r.count].copy())
 

@@ -206,6 +206,19 @@ __global__ void __launch_bounds__(128) k_densify_patch(const DensifyPatch *__res
 }
 
 
+// Relocation's split (relocate_cloud, densify.cpp:335-337): dead where the
+// opacity is at or below the limit (the logit below deadLogit) or a value is
+// not finite; alive otherwise.
+template <ShStore S>
+__global__ void __launch_bounds__(256) k_relocate_flags(Params p, float deadLogit, uint32_t *__restrict__ dead,
+                                                        uint32_t *__restrict__ alive) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n) return;
+  const bool gone = !finite_gaussian<S>(p, i) || p.opacities[i] < deadLogit;
+  dead[i] = gone ? 1u : 0u;
+  alive[i] = gone ? 0u : 1u;
+}
+
 } // namespace
 
 void launch_densify_classify(const Params &p, const float *stats, const DensifyArgs &a, uint32_t *action, uint32_t *transparent,
@@ -216,6 +229,16 @@ void launch_densify_classify(const Params &p, const float *stats, const DensifyA
   case ShStore::BF16: k_densify_classify<ShStore::BF16><<<blocks, 256, 0, stream>>>(p, stats, a, action, transparent, transparentKey); break;
   case ShStore::F16: k_densify_classify<ShStore::F16><<<blocks, 256, 0, stream>>>(p, stats, a, action, transparent, transparentKey); break;
   default: k_densify_classify<ShStore::F32><<<blocks, 256, 0, stream>>>(p, stats, a, action, transparent, transparentKey); break;
+  }
+}
+
+void launch_relocate_flags(const Params &p, float deadLogit, uint32_t *dead, uint32_t *alive, cudaStream_t stream) {
+  if (p.n == 0) return;
+  const uint32_t blocks = div_up(p.n, 256);
+  switch (p.shStore) {
+  case ShStore::BF16: k_relocate_flags<ShStore::BF16><<<blocks, 256, 0, stream>>>(p, deadLogit, dead, alive); break;
+  case ShStore::F16: k_relocate_flags<ShStore::F16><<<blocks, 256, 0, stream>>>(p, deadLogit, dead, alive); break;
+  default: k_relocate_flags<ShStore::F32><<<blocks, 256, 0, stream>>>(p, deadLogit, dead, alive); break;
   }
 }
 

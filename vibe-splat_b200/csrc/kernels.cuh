@@ -243,6 +243,9 @@ void launch_densify_flags(uint32_t n, const uint32_t *action, uint32_t *survivor
 void launch_densify_tables(uint32_t n, uint32_t survivors, const uint32_t *action, const uint32_t *survivorPlace,
                            const uint32_t *addedPlace, const uint32_t *patchedPlace, int32_t *paramSource, int32_t *stateSource,
                            uint32_t *parents, uint32_t *childSlot, cudaStream_t stream);
+// Relocation (relocate_cloud, densify.cpp:328-420): dead and alive flags,
+// dead where the logit is below deadLogit or a value is not finite.
+void launch_relocate_flags(const Params &p, float deadLogit, uint32_t *dead, uint32_t *alive, cudaStream_t stream);
 // Writes host-computed rows into their slots (shRest: restPlanes planes of
 // planeStride elements of shBytes bytes).
 void launch_densify_patch(const DensifyPatch *patches, uint32_t count, float *positions, float *scales, float *rotations,

@@ -75,11 +75,21 @@ public:
   }
   template <class T = void> T *get() const { return static_cast<T *>(ptr_); }
   size_t bytes() const { return bytes_; }
+  friend void swap(DeviceBuffer &a, DeviceBuffer &b) noexcept {
+    std::swap(a.ptr_, b.ptr_);
+    std::swap(a.bytes_, b.bytes_);
+  }
 
 private:
   void *ptr_ = nullptr;
   size_t bytes_ = 0;
 };
+
+// Makes buffer at least `bytes` long, with a quarter to spare when it must
+// grow, for buffers that follow a Gaussian count that grows by steps.
+void grow(DeviceBuffer &buffer, size_t bytes) {
+  if (buffer.get() == nullptr || buffer.bytes() < bytes) buffer.ensure(bytes + bytes / 4);
+}
 
 class PinnedBuffer {
 public:
@@ -175,6 +185,11 @@ public:
 
   DeviceBuffer positions, scales, rotations, opacities, shDc, shRest;
   DeviceBuffer state[5], grads[5], densifyStats;
+  // Edits of the cloud (densify, relocate, prune): the next parameter and
+  // state buffers, gathered into and swapped with the current ones; and the
+  // scratch, tables and host-computed rows of an edit. Kept from one edit to
+  // the next, so that a training run's edits allocate little.
+  DeviceBuffer spareParams[6], spareState[5], editScratch, editTables, editRows;
   bool haveGradients = false, haveRaw = false;
 
   // Per (view, Gaussian).
@@ -245,6 +260,8 @@ public:
   // Carries the step counter, active SH degree and the sort and layout
   // choices over to a trainer made for a changed cloud.
   void inherit(const Trainer &old);
+  // Replaces the Gaussians, in place, by newN gathered from the current ones.
+  void replace_gaussians(const int32_t *paramSource, const int32_t *stateSource, uint32_t newN);
   void autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats, splat_autotune_result *out);
 };
 
@@ -1018,6 +1035,68 @@ void Trainer::inherit(const Trainer &old) {
   timing = old.timing;
 }
 
+// Trainer::apply_changes (trainer.cpp:749-787) for a cloud edited on the
+// device: the parameters are gathered through paramSource, the optimiser
+// state through stateSource (-1: fresh, zero), into the spare buffers, which
+// then take the current ones' place; the densification statistics start at
+// zero and the buffers sized by the count follow it at the next step. The
+// views' buffers, the tile entries and the targets stay. With a memory
+// budget the old buffers are freed at once; without one they are kept as the
+// next edit's spares.
+void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *stateSource, uint32_t newN) {
+  SB_CUDA(cudaStreamSynchronize(stream));
+  SB_CUDA(cudaStreamSynchronize(copyStream));
+  const uint32_t oldN = n, oldStride = planeStride;
+  const size_t nn = newN;
+  const uint32_t newStride = (uint32_t)(((nn + kPlaneAlign - 1) / kPlaneAlign) * kPlaneAlign);
+  const size_t restPlanes = 3 * (size_t)(shCoeffs - 1);
+  const size_t copies = stateStore == StateStore::F32 ? 2 : 1;
+  const size_t paramBytes[6] = {nn * 12, nn * 12, nn * 16, nn * 4, (size_t)newStride * 12,
+                                std::max<size_t>(restPlanes * newStride * (shStore == ShStore::F32 ? 4 : 2), 4)};
+  const size_t stateBytes[5] = {nn * 12 * copies, nn * 12 * copies, nn * 16 * copies, nn * 4 * copies,
+                                (size_t)newStride * 12 * shCoeffs * copies};
+  for (int g = 0; g < 6; ++g) grow(spareParams[g], paramBytes[g]);
+  for (int g = 0; g < 5; ++g) grow(spareState[g], stateBytes[g]);
+  const uint32_t strides[4] = {3, 3, 4, 1};
+  DeviceBuffer *params[4] = {&positions, &scales, &rotations, &opacities};
+  for (int g = 0; g < 4; ++g)
+    launch_gather_rows(paramSource, params[g]->get<uint32_t>(), spareParams[g].get<uint32_t>(), newN, oldN, strides[g], 1u, stream);
+  launch_gather_planes(paramSource, shDc.get<uint32_t>(), spareParams[4].get<uint32_t>(), newN, newStride, oldStride, 3u, stream);
+  if (shStore == ShStore::F32)
+    launch_gather_planes(paramSource, shRest.get<uint32_t>(), spareParams[5].get<uint32_t>(), newN, newStride, oldStride,
+                         (uint32_t)restPlanes, stream);
+  else
+    launch_gather_planes16(paramSource, shRest.get<uint16_t>(), spareParams[5].get<uint16_t>(), newN, newStride, oldStride,
+                           (uint32_t)restPlanes, stream);
+  for (int g = 0; g < 4; ++g)
+    launch_gather_rows(stateSource, state[g].get<uint32_t>(), spareState[g].get<uint32_t>(), newN, oldN, strides[g],
+                       (uint32_t)copies, stream);
+  launch_gather_planes(stateSource, state[4].get<uint32_t>(), spareState[4].get<uint32_t>(), newN, newStride, oldStride,
+                       (uint32_t)(3 * shCoeffs * copies), stream);
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaStreamSynchronize(stream));
+  for (int g = 0; g < 4; ++g) swap(*params[g], spareParams[g]);
+  swap(shDc, spareParams[4]);
+  swap(shRest, spareParams[5]);
+  for (int g = 0; g < 5; ++g) swap(state[g], spareState[g]);
+  if (opt.memory_budget != UINT64_MAX) {
+    for (DeviceBuffer &b : spareParams) b.release();
+    for (DeviceBuffer &b : spareState) b.release();
+  }
+  n = newN;
+  planeStride = newStride;
+  clear_graphs();
+  viewSlots = 0; // the per-view buffers follow the count, and the raw sums are cleared, at the next step
+  haveGradients = false;
+  haveRaw = false;
+  const size_t groupCounts[4] = {nn * 3, nn * 3, nn * 4, nn};
+  for (int g = 0; g < 4; ++g) grow(grads[g], groupCounts[g] * 4);
+  grow(densifyStats, nn * kStatStride * 4);
+  SB_CUDA(cudaMemsetAsync(densifyStats.get(), 0, nn * kStatStride * 4, stream));
+  SB_CUDA(cudaStreamSynchronize(stream));
+}
+
+
 void Trainer::set_sort(bool single, int digits) {
   if (single == oneSort && digits == digitBits) return;
   SB_CUDA(cudaStreamSynchronize(stream));
@@ -1176,6 +1255,31 @@ Trainer *impl_of(splat_trainer *t) {
   if (t == nullptr || t->impl == nullptr) throw Failure{SPLAT_ERR_INVALID, "null trainer"};
   return t->impl;
 }
+
+// A part of a device buffer.
+struct Slice {
+  void *p = nullptr;
+  template <class T = void> T *get() const { return static_cast<T *>(p); }
+};
+
+// An edit's scratch: 256-byte aligned slices of a device buffer the trainer
+// keeps, made large enough up front for everything the edit takes.
+class Arena {
+public:
+  Arena(sb::DeviceBuffer &buffer, size_t bytes) : buffer_(buffer), limit_(bytes) { sb::grow(buffer, bytes); }
+  Slice take(size_t bytes) {
+    const size_t size = (std::max<size_t>(bytes, 1) + 255) & ~size_t{255};
+    if (used_ + size > limit_) throw Failure{SPLAT_ERR_DEVICE, "an edit's scratch was sized too small"};
+    Slice s{buffer_.get<uint8_t>() + used_};
+    used_ += size;
+    return s;
+  }
+  static size_t room(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~size_t{255}; }
+
+private:
+  sb::DeviceBuffer &buffer_;
+  size_t limit_, used_ = 0;
+};
 
 } // namespace
 
@@ -1479,52 +1583,13 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
 
 namespace {
 
-// Replaces the trainer by one of newN Gaussians gathered on the device from
-// the old one (Trainer::apply_changes, trainer.cpp:749-787): the parameters
-// through paramSource, the optimiser state through stateSource (-1: fresh,
-// zero). Everything but the parameters and the optimiser state goes before
-// the new trainer is made, for the sake of the budget; its densification
-// statistics start at zero. Returns the new trainer, installed in handle.
+// The trainer's Gaussians replaced by newN gathered on the device
+// (Trainer::apply_changes, trainer.cpp:749-787): parameters through
+// paramSource, optimiser state through stateSource (-1: fresh, zero).
 Trainer *regather(splat_trainer *handle, const int32_t *paramSource, const int32_t *stateSource, uint32_t newN) {
   Trainer *t = impl_of(handle);
-  const uint32_t oldN = t->n;
-  t->release_transient(true);
-  splat_cloud sizes{};
-  sizes.count = (int32_t)newN;
-  sizes.sh_degree = t->shDegree;
-  Trainer *fresh = new Trainer(sizes, t->opt, false);
-  fresh->inherit(*t);
-  try {
-    cudaStream_t f = fresh->stream;
-    const uint32_t strides[4] = {3, 3, 4, 1};
-    sb::DeviceBuffer *from[4] = {&t->positions, &t->scales, &t->rotations, &t->opacities};
-    sb::DeviceBuffer *to[4] = {&fresh->positions, &fresh->scales, &fresh->rotations, &fresh->opacities};
-    for (int g = 0; g < 4; ++g)
-      sb::launch_gather_rows(paramSource, from[g]->get<uint32_t>(), to[g]->get<uint32_t>(), newN, oldN, strides[g], 1u, f);
-    sb::launch_gather_planes(paramSource, t->shDc.get<uint32_t>(), fresh->shDc.get<uint32_t>(), newN, fresh->planeStride,
-                             t->planeStride, 3u, f);
-    const uint32_t restPlanes = 3u * (uint32_t)(t->shCoeffs - 1);
-    if (t->shStore == sb::ShStore::F32)
-      sb::launch_gather_planes(paramSource, t->shRest.get<uint32_t>(), fresh->shRest.get<uint32_t>(), newN, fresh->planeStride,
-                               t->planeStride, restPlanes, f);
-    else
-      sb::launch_gather_planes16(paramSource, t->shRest.get<uint16_t>(), fresh->shRest.get<uint16_t>(), newN, fresh->planeStride,
-                                 t->planeStride, restPlanes, f);
-    const uint32_t copies = t->stateStore == sb::StateStore::F32 ? 2u : 1u;
-    for (int g = 0; g < 4; ++g)
-      sb::launch_gather_rows(stateSource, t->state[g].get<uint32_t>(), fresh->state[g].get<uint32_t>(), newN, oldN, strides[g],
-                             copies, f);
-    sb::launch_gather_planes(stateSource, t->state[4].get<uint32_t>(), fresh->state[4].get<uint32_t>(), newN, fresh->planeStride,
-                             t->planeStride, 3u * (uint32_t)t->shCoeffs * copies, f);
-    SB_CUDA(cudaGetLastError());
-    SB_CUDA(cudaStreamSynchronize(f));
-  } catch (...) {
-    delete fresh;
-    throw;
-  }
-  delete t;
-  handle->impl = fresh;
-  return fresh;
+  t->replace_gaussians(paramSource, stateSource, newN);
+  return t;
 }
 
 // remove_highest on the GPU (densify.cpp:70-90, Trainer::apply_changes,
@@ -1542,17 +1607,13 @@ uint64_t prune_gaussians(splat_trainer *handle, int kind, double share) {
   const uint32_t newN = oldN - removed;
   cudaStream_t s = t->stream;
   SB_CUDA(cudaStreamSynchronize(s));
-  sb::DeviceBuffer keys, values, tmpKeys, tmpValues, keep, place, table, scratch, scanScratch, counters;
-  keys.ensure((size_t)oldN * 4);
-  values.ensure((size_t)oldN * 4);
-  tmpKeys.ensure((size_t)oldN * 4);
-  tmpValues.ensure((size_t)oldN * 4);
-  keep.ensure((size_t)oldN * 4);
-  place.ensure((size_t)oldN * 4);
-  table.ensure((size_t)newN * 4);
-  scratch.ensure(sb::sort_scratch_bytes(oldN, 4, 32, 8));
-  scanScratch.ensure(sb::bin_scan_scratch_bytes(oldN));
-  counters.ensure(16);
+  const size_t words = Arena::room((size_t)oldN * 4);
+  Arena arena(t->editScratch, 7 * words + Arena::room(sb::sort_scratch_bytes(oldN, 4, 32, 8)) +
+                                  Arena::room(sb::bin_scan_scratch_bytes(oldN)) + Arena::room(16));
+  Slice keys = arena.take(words), values = arena.take(words), tmpKeys = arena.take(words), tmpValues = arena.take(words);
+  Slice keep = arena.take(words), place = arena.take(words), table = arena.take(words);
+  Slice scratch = arena.take(sb::sort_scratch_bytes(oldN, 4, 32, 8)), scanScratch = arena.take(sb::bin_scan_scratch_bytes(oldN));
+  Slice counters = arena.take(16);
   SB_CUDA(cudaMemsetAsync(counters.get(), 0, 16, s));
   uint32_t *error = counters.get<uint32_t>() + 3;
   const float *stats = kind == 1 ? t->densifyStats.get<float>() : nullptr;
@@ -1616,6 +1677,11 @@ float logit_threshold(float limit) {
   const float x = first_holding([&](float o) { return !(1.f / (1.f + std::exp(-o)) < limit); });
   return std::isnan(x) ? std::numeric_limits<float>::infinity() : x;
 }
+// The same for "at or below the limit" (relocation's dead, densify.cpp:336).
+float logit_threshold_inclusive(float limit) {
+  const float x = first_holding([&](float o) { return !(1.f / (1.f + std::exp(-o)) <= limit); });
+  return std::isnan(x) ? std::numeric_limits<float>::infinity() : x;
+}
 
 // The Gaussian's rotation as a matrix, identity for a degenerate quaternion:
 // the same float arithmetic as densify.cpp:42-59, since the children's
@@ -1661,20 +1727,30 @@ struct DensifyRun {
   Trainer *t;
   cudaStream_t s;
   uint32_t n;
-  sb::DeviceBuffer counters, scanScratch, sortScratch, tmpKeys, tmpValues, rows;
+  Arena arena;
+  Slice counters, scanScratch, sortScratch, tmpKeys, tmpValues, rows;
 
-  explicit DensifyRun(Trainer *trainer) : t(trainer), s(trainer->stream), n(trainer->n) {
-    counters.ensure(64 * 4);
-    SB_CUDA(cudaMemsetAsync(counters.get(), 0, 64 * 4, s));
-    scanScratch.ensure(sb::bin_scan_scratch_bytes(n));
-    sortScratch.ensure(sb::sort_scratch_bytes(n, 4, 32, 8));
-    tmpKeys.ensure((size_t)n * 4);
-    tmpValues.ensure((size_t)n * 4);
+  // arrays: how many further n-word arrays the edit takes (take()).
+  static size_t bytes(uint32_t n, int arrays) {
+    return Arena::room(64 * 4) + Arena::room(sb::bin_scan_scratch_bytes(n)) + Arena::room(sb::sort_scratch_bytes(n, 4, 32, 8)) +
+           (2 + 8 + (size_t)arrays) * Arena::room((size_t)n * 4 + 4);
   }
+  DensifyRun(Trainer *trainer, int arrays)
+      : t(trainer), s(trainer->stream), n(trainer->n), arena(trainer->editScratch, bytes(trainer->n, arrays)) {
+    counters = arena.take(64 * 4);
+    SB_CUDA(cudaMemsetAsync(counters.get(), 0, 64 * 4, s));
+    scanScratch = arena.take(sb::bin_scan_scratch_bytes(n));
+    sortScratch = arena.take(sb::sort_scratch_bytes(n, 4, 32, 8));
+    tmpKeys = take();
+    tmpValues = take();
+    rows = arena.take(8 * ((size_t)n * 4 + 4));
+  }
+  // An array of n + 1 words.
+  Slice take() { return arena.take((size_t)n * 4 + 4); }
   uint32_t *error() { return counters.get<uint32_t>() + 63; }
   // Exclusive scan of flags into place (both n words); the total lands in
   // counter block `block` (word 1).
-  void scan(const sb::DeviceBuffer &flags, sb::DeviceBuffer &place, int block) {
+  void scan(const Slice &flags, const Slice &place, int block) {
     SB_CUDA(cudaMemcpyAsync(place.get(), flags.get(), (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
     sb::launch_exclusive_scan(n, place.get<uint32_t>(), counters.get<uint32_t>() + 4 * block, scanScratch.get(), error(), s);
   }
@@ -1687,7 +1763,7 @@ struct DensifyRun {
     return h;
   }
   // Stable ascending sort of count (key, index) pairs; returns the indices.
-  const uint32_t *sort(sb::DeviceBuffer &keys, sb::DeviceBuffer &indices, uint32_t count) {
+  const uint32_t *sort(const Slice &keys, const Slice &indices, uint32_t count) {
     if (count <= 1) return indices.get<uint32_t>();
     const int where = sb::sort_pairs_u32(keys.get<uint32_t>(), indices.get<uint32_t>(), tmpKeys.get<uint32_t>(),
                                          tmpValues.get<uint32_t>(), n, count, nullptr, 0, 32, 8, sortScratch.get(), error(), s);
@@ -1700,11 +1776,11 @@ struct DensifyRun {
     SB_CUDA(cudaStreamSynchronize(s));
     return h;
   }
-  // The rows of `stride` words of `in` (n rows) for the count listed indices.
+  // The rows of `stride` (at most 8) words of `in` (n rows) for the count
+  // listed indices.
   std::vector<float> gather(const int32_t *list, const void *in, uint32_t count, uint32_t stride) {
     std::vector<float> h((size_t)count * stride);
     if (count == 0) return h;
-    rows.ensure((size_t)count * stride * 4);
     sb::launch_gather_rows(list, static_cast<const uint32_t *>(in), rows.get<uint32_t>(), count, n, stride, 1u, s);
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaMemcpyAsync(h.data(), rows.get(), h.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -1724,7 +1800,7 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
   if (o.transparent_share < 0.0) throw Failure{SPLAT_ERR_INVALID, "transparent_share must not be negative"};
   SB_CUDA(cudaStreamSynchronize(t->stream));
   if (t->densifyStats.get() == nullptr) throw Failure{SPLAT_ERR_STATE, "no densification statistics"};
-  DensifyRun run(t);
+  DensifyRun run(t, 14);
   cudaStream_t s = run.s;
   const uint32_t n = run.n;
   const float *stats = t->densifyStats.get<float>();
@@ -1743,10 +1819,9 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
   a.allTransparent = o.transparent_share < 1.0 ? 0 : 1;
   a.edgeSplit = o.edge_split != 0 ? 1 : 0;
 
-  sb::DeviceBuffer action, flags, keys, place, list, keyList, kept, keptPlace, candidate, candidatePlace, priority, chosen;
-  for (sb::DeviceBuffer *b : {&action, &flags, &keys, &place, &list, &keyList, &kept, &keptPlace, &candidate, &candidatePlace,
-                              &priority, &chosen})
-    b->ensure((size_t)n * 4);
+  Slice action = run.take(), flags = run.take(), keys = run.take(), place = run.take(), list = run.take(), keyList = run.take();
+  Slice kept = run.take(), keptPlace = run.take(), candidate = run.take(), candidatePlace = run.take(), priority = run.take();
+  Slice chosen = run.take(), parents = run.take(), childSlot = run.take();
 
   // The oversized, the non-finite and the too transparent.
   sb::launch_densify_classify(t->params(), stats, a, action.get<uint32_t>(), flags.get<uint32_t>(), keys.get<uint32_t>(), s);
@@ -1863,8 +1938,8 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
   }
 
   // The new cloud's layout.
-  sb::DeviceBuffer &survivor = kept, &survivorPlace = keptPlace, &added = candidate, &addedPlace = candidatePlace;
-  sb::DeviceBuffer &patched = flags, &patchedPlace = place;
+  const Slice &survivor = kept, &survivorPlace = keptPlace, &added = candidate, &addedPlace = candidatePlace;
+  const Slice &patched = flags, &patchedPlace = place;
   sb::launch_densify_flags(n, action.get<uint32_t>(), survivor.get<uint32_t>(), added.get<uint32_t>(), patched.get<uint32_t>(), s);
   run.scan(survivor, survivorPlace, 5);
   run.scan(added, addedPlace, 6);
@@ -1875,11 +1950,8 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
   if (newCount == 0) throw Failure{SPLAT_ERR_INVALID, "densification removed every Gaussian"};
   if (newCount > 0x7FFFFFFFull) throw Failure{SPLAT_ERR_INVALID, "densification would exceed 2^31 - 1 Gaussians"};
   const auto newN = (uint32_t)newCount;
-  sb::DeviceBuffer paramSource, stateSource, parents, childSlot, patches;
-  paramSource.ensure((size_t)newN * 4);
-  stateSource.ensure((size_t)newN * 4);
-  parents.ensure(std::max<size_t>(parentsCount, 1) * 4);
-  childSlot.ensure(std::max<size_t>(parentsCount, 1) * 4);
+  Arena tables(t->editTables, 2 * Arena::room((size_t)newN * 4));
+  const Slice paramSource = tables.take((size_t)newN * 4), stateSource = tables.take((size_t)newN * 4);
   sb::launch_densify_tables(n, (uint32_t)survivorCount, action.get<uint32_t>(), survivorPlace.get<uint32_t>(),
                             addedPlace.get<uint32_t>(), patchedPlace.get<uint32_t>(), paramSource.get<int32_t>(),
                             stateSource.get<int32_t>(), parents.get<uint32_t>(), childSlot.get<uint32_t>(), s);
@@ -1967,8 +2039,8 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
     SB_CUDA(cudaMemcpyAsync(stateSource.get<uint8_t>() + offset, fresh.data(), fresh.size() * 4, cudaMemcpyHostToDevice, s));
   }
   if (!rowsOut.empty()) {
-    patches.ensure(rowsOut.size() * sizeof(sb::DensifyPatch));
-    SB_CUDA(cudaMemcpyAsync(patches.get(), rowsOut.data(), rowsOut.size() * sizeof(sb::DensifyPatch), cudaMemcpyHostToDevice, s));
+    sb::grow(t->editRows, rowsOut.size() * sizeof(sb::DensifyPatch));
+    SB_CUDA(cudaMemcpyAsync(t->editRows.get(), rowsOut.data(), rowsOut.size() * sizeof(sb::DensifyPatch), cudaMemcpyHostToDevice, s));
   }
   std::vector<int32_t> table;
   if (source != nullptr && sourceCapacity >= newCount) {
@@ -1981,7 +2053,7 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
   Trainer *fresh = regather(handle, paramSource.get<int32_t>(), stateSource.get<int32_t>(), newN);
   if (!rowsOut.empty()) {
     const uint32_t restPlanes = 3u * (uint32_t)(fresh->shCoeffs - 1);
-    sb::launch_densify_patch(patches.get<sb::DensifyPatch>(), (uint32_t)rowsOut.size(), fresh->positions.get<float>(),
+    sb::launch_densify_patch(fresh->editRows.get<sb::DensifyPatch>(), (uint32_t)rowsOut.size(), fresh->positions.get<float>(),
                              fresh->scales.get<float>(), fresh->rotations.get<float>(), fresh->opacities.get<float>(),
                              fresh->shRest.get(), restPlanes, fresh->planeStride, fresh->shStore == sb::ShStore::F32 ? 4u : 2u,
                              fresh->stream);
@@ -1999,6 +2071,137 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
   }
 }
 
+
+// Trainer::relocate on the GPU and the host (trainer.cpp:717-722;
+// relocate_cloud, densify.cpp:328-420; apply_changes). The device splits the
+// Gaussians into dead and alive and gathers the new cloud and its optimiser
+// state; the draws (std::discrete_distribution over opacities, from rng in
+// the reference's order) and the opacity and scale updates of the drawn
+// targets, a sequential chain, run on the host over the opacities and
+// log-scales, the only values relocation changes.
+void relocate_gaussians(splat_trainer *handle, const splat_relocate_options &o, std::mt19937 &rng, splat_densify_result *result,
+                        int64_t *source, uint64_t sourceCapacity) {
+  Trainer *t = impl_of(handle);
+  if (!(o.growth >= 0.0)) throw Failure{SPLAT_ERR_INVALID, "growth must not be negative"};
+  SB_CUDA(cudaStreamSynchronize(t->stream));
+  DensifyRun run(t, 5);
+  cudaStream_t s = run.s;
+  const uint32_t n = run.n;
+  Slice dead = run.take(), alive = run.take(), deadPlace = run.take(), alivePlace = run.take(), list = run.take();
+  sb::launch_relocate_flags(t->params(), logit_threshold_inclusive(o.min_opacity), dead.get<uint32_t>(), alive.get<uint32_t>(), s);
+  run.scan(dead, deadPlace, 0);
+  run.scan(alive, alivePlace, 1);
+  const std::vector<uint32_t> c = run.read();
+  const uint32_t deadCount = c[1], aliveCount = c[5];
+  std::vector<int64_t> stateSource(n);
+  for (uint32_t i = 0; i < n; ++i) stateSource[i] = i;
+  splat_densify_result counts{};
+  counts.count = n;
+  if (aliveCount == 0) {
+    // Nothing to draw from: the cloud stays; its statistics start anew, as
+    // apply_changes leaves them.
+    SB_CUDA(cudaMemsetAsync(t->densifyStats.get(), 0, (size_t)n * sb::kStatStride * 4, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (source != nullptr && sourceCapacity >= n) std::copy(stateSource.begin(), stateSource.end(), source);
+    if (result != nullptr) *result = counts;
+    return;
+  }
+  sb::launch_compact(dead.get<uint32_t>(), deadPlace.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
+  const std::vector<uint32_t> deadList = run.download(list.get<uint32_t>(), deadCount);
+  sb::launch_compact(alive.get<uint32_t>(), alivePlace.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
+  const std::vector<uint32_t> aliveList = run.download(list.get<uint32_t>(), aliveCount);
+  std::vector<float> opacity(n), logScale((size_t)n * 3);
+  SB_CUDA(cudaMemcpyAsync(opacity.data(), t->opacities.get(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaMemcpyAsync(logScale.data(), t->scales.get(), (size_t)n * 12, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+
+  // origin[k]: the old Gaussian whose position, rotation and SH slot k holds.
+  std::vector<int32_t> origin(n);
+  for (uint32_t i = 0; i < n; ++i) origin[i] = (int32_t)i;
+  const auto sigmoid = [](float x) { return 1.f / (1.f + std::exp(-x)); };
+  // A target drawn m times becomes m + 1 equal copies (at most 51): opacity
+  // 1 - (1 - o)^(1/N) and scale times o / D, D the alternating binomial sum
+  // of 3DGS-MCMC (densify.cpp:342-364).
+  const auto update_targets = [&](const std::vector<size_t> &targets, size_t size) {
+    std::vector<int> times(size, 0);
+    for (const size_t k : targets) ++times[k];
+    for (size_t k = 0; k < size; ++k) {
+      if (times[k] == 0) continue;
+      const int copies = std::min(times[k] + 1, 51);
+      const double was = sigmoid(opacity[k]);
+      const double fresh = 1.0 - std::pow(1.0 - was, 1.0 / copies);
+      double divisor = 0.0;
+      for (int i = 1; i <= copies; ++i) {
+        double binom = 1.0;
+        for (int j = 0; j < i; ++j) {
+          if (j > 0) binom = binom * static_cast<double>(i - j) / j;
+          divisor += binom * (j % 2 == 0 ? 1.0 : -1.0) * std::pow(fresh, j + 1) / std::sqrt(static_cast<double>(j + 1));
+        }
+      }
+      const double clamped = std::clamp(fresh, static_cast<double>(o.min_opacity), 1.0 - 1e-6);
+      opacity[k] = static_cast<float>(std::log(clamped / (1.0 - clamped)));
+      const double factor = divisor > 0.0 ? was / divisor : 1.0;
+      for (size_t a = 0; a < 3; ++a) logScale[k * 3 + a] += static_cast<float>(std::log(factor));
+      stateSource[k] = -1;
+    }
+  };
+  const auto copy_into = [&](size_t from, size_t to) {
+    origin[to] = origin[from];
+    opacity[to] = opacity[from];
+    for (size_t a = 0; a < 3; ++a) logScale[to * 3 + a] = logScale[from * 3 + a];
+  };
+  const auto draw = [&](const auto &from, size_t count) {
+    std::vector<double> weights;
+    weights.reserve(from.size());
+    for (const auto k : from) weights.push_back(sigmoid(opacity[k]));
+    std::discrete_distribution<size_t> pick(weights.begin(), weights.end());
+    std::vector<size_t> targets(count);
+    for (size_t &k : targets) k = from[pick(rng)];
+    return targets;
+  };
+  if (deadCount > 0) {
+    const std::vector<size_t> targets = draw(aliveList, deadCount);
+    update_targets(targets, n);
+    for (size_t j = 0; j < deadList.size(); ++j) {
+      copy_into(targets[j], deadList[j]);
+      stateSource[deadList[j]] = -1;
+    }
+    counts.cloned = deadCount;
+  }
+  const uint64_t room = o.max_gaussians > n ? o.max_gaussians - n : 0;
+  const double share = o.growth * static_cast<double>(n);
+  const uint64_t wanted = share >= static_cast<double>(room) ? room : std::min<uint64_t>(static_cast<size_t>(share), room);
+  if (wanted + n > 0x7FFFFFFFull) throw Failure{SPLAT_ERR_INVALID, "relocation would exceed 2^31 - 1 Gaussians"};
+  if (wanted > 0) {
+    std::vector<size_t> everyone(n);
+    for (uint32_t i = 0; i < n; ++i) everyone[i] = i;
+    const std::vector<size_t> targets = draw(everyone, wanted);
+    update_targets(targets, n);
+    origin.resize(n + wanted);
+    opacity.resize(n + wanted);
+    logScale.resize((n + wanted) * 3);
+    for (size_t k = 0; k < targets.size(); ++k) {
+      copy_into(targets[k], n + k);
+      stateSource.push_back(-1);
+    }
+    counts.seeded = wanted;
+  }
+  const auto newN = (uint32_t)(n + wanted);
+  counts.count = newN;
+  std::vector<int32_t> state32(newN);
+  for (uint32_t k = 0; k < newN; ++k) state32[k] = (int32_t)stateSource[k];
+  Arena tables(t->editTables, 2 * Arena::room((size_t)newN * 4));
+  const Slice paramTable = tables.take((size_t)newN * 4), stateTable = tables.take((size_t)newN * 4);
+  SB_CUDA(cudaMemcpyAsync(paramTable.get(), origin.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(stateTable.get(), state32.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  Trainer *fresh = regather(handle, paramTable.get<int32_t>(), stateTable.get<int32_t>(), newN);
+  SB_CUDA(cudaMemcpyAsync(fresh->opacities.get(), opacity.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, fresh->stream));
+  SB_CUDA(cudaMemcpyAsync(fresh->scales.get(), logScale.data(), (size_t)newN * 12, cudaMemcpyHostToDevice, fresh->stream));
+  SB_CUDA(cudaStreamSynchronize(fresh->stream));
+  if (source != nullptr && sourceCapacity >= newN) std::copy(stateSource.begin(), stateSource.end(), source);
+  if (result != nullptr) *result = counts;
+}
 } // namespace
 
 extern "C" {
@@ -2047,6 +2250,22 @@ int splat_trainer_densify(splat_trainer *trainer, const splat_densify_options *o
   return guarded([&] {
     if (options == nullptr || rng == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
     densify_gaussians(trainer, *options, rng->engine, result, source, source_capacity);
+  });
+}
+
+void splat_relocate_options_default(splat_relocate_options *options) {
+  if (options == nullptr) return;
+  *options = splat_relocate_options{};
+  options->min_opacity = 0.005f;
+  options->growth = 0.05;
+  options->max_gaussians = UINT64_MAX;
+}
+
+int splat_trainer_relocate(splat_trainer *trainer, const splat_relocate_options *options, splat_rng *rng,
+                           splat_densify_result *result, int64_t *source, uint64_t source_capacity) {
+  return guarded([&] {
+    if (options == nullptr || rng == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    relocate_gaussians(trainer, *options, rng->engine, result, source, source_capacity);
   });
 }
 
@@ -2207,7 +2426,13 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     case 11: src = t->partials.get(); have = (size_t)t->views.totalTiles * 8; break;
     case 12: src = &rb->error; have = 4; break;
     case 13: src = t->listCounts.get(); have = t->blendLists ? (size_t)t->views.totalPixels * 4 : 0; break;
-    case 14: case 15: case 16: case 17: case 18: src = t->state[which - 14].get(); have = t->state[which - 14].bytes(); break;
+    case 14: case 15: case 16: case 17: case 18: {
+      const size_t g = t->n;
+      const size_t counts[5] = {g * 3, g * 3, g * 4, g, (size_t)t->planeStride * 3 * t->shCoeffs};
+      src = t->state[which - 14].get();
+      have = counts[which - 14] * (t->stateStore == sb::StateStore::F32 ? 8 : 4);
+      break;
+    }
     default: throw Failure{SPLAT_ERR_INVALID, "unknown buffer"};
     }
     if (size) *size = have;
