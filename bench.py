@@ -630,6 +630,13 @@ def our_arm(args) -> None:
                 densify["reference_cpu_ms"] = (time.perf_counter() - t0) * 1000.0
                 densify["reference_same_result"] = bool(np.array_equal(ref.source, r.source))
         del held, raw
+        # 3DGS-MCMC relocation (dead onto live, 5 % growth): the dead/alive
+        # split and the gathers on the GPU, the draws on the host.
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = trainer.relocate(splat.RelocateOptions(), splat.Rng(2))
+        densify["relocate"] = {"ms": (time.perf_counter() - t0) * 1000.0, "count": r.count, "relocated": r.cloned,
+                               "grown": r.seeded}
 
     # Pruning on the GPU (remove_largest_gaussians, 1 % of the Gaussians):
     # keys, sort, scan and the gathers of parameters and optimiser state.

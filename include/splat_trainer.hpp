@@ -58,6 +58,45 @@ inline splat_learning_rates default_rates() {
   return r;
 }
 
+// The generator densification draws from (std::mt19937 inside), kept by
+// the caller across rounds as the reference's session keeps densifyRng_.
+class Rng {
+public:
+  explicit Rng(std::uint32_t seed) { check(splat_rng_create(seed, &handle_)); }
+  ~Rng() { splat_rng_destroy(handle_); }
+  Rng(const Rng &) = delete;
+  Rng &operator=(const Rng &) = delete;
+  // std::uniform_int_distribution<std::size_t>(0, count - 1)(rng).
+  std::size_t pick(std::size_t count) {
+    std::uint64_t out = 0;
+    check(splat_rng_pick(handle_, count, &out));
+    return static_cast<std::size_t>(out);
+  }
+  [[nodiscard]] splat_rng *handle() const noexcept { return handle_; }
+
+private:
+  splat_rng *handle_ = nullptr;
+};
+
+inline splat_densify_options default_densify_options() {
+  splat_densify_options o;
+  splat_densify_options_default(&o);
+  return o;
+}
+
+inline splat_relocate_options default_relocate_options() {
+  splat_relocate_options o;
+  splat_relocate_options_default(&o);
+  return o;
+}
+
+// DensifyResult (densify.hpp:52-62) without the cloud, which stays on the GPU
+// (Trainer::cloud() downloads it).
+struct DensifyResult {
+  std::vector<std::int64_t> source;
+  std::size_t cloned = 0, split = 0, seeded = 0, pruned = 0, heldBack = 0;
+};
+
 class Trainer {
 public:
   explicit Trainer(const Cloud &initial, const splat_trainer_options &options = default_options())
@@ -134,6 +173,29 @@ public:
     check(splat_trainer_apply_changes(handle_, &c, source.data()));
     count_ = next.size();
   }
+  // Trainer::score_view: the FastGS scoring pass.
+  splat_step_stats score_view(const splat_camera &camera, std::span<const std::uint8_t> target, float errorShare,
+                              float pixelWeight = 1.f) {
+    splat_step_stats s{};
+    check(splat_trainer_score_view(handle_, &camera, target.data(), target.size(), errorShare, pixelWeight, &s));
+    return s;
+  }
+  // Trainer::densify and Trainer::relocate, on the GPU.
+  DensifyResult densify(const splat_densify_options &options, Rng &rng) {
+    return edit([&](splat_densify_result *r, int64_t *source, uint64_t capacity) {
+      return splat_trainer_densify(handle_, &options, rng.handle(), r, source, capacity);
+    }, 2 * count_ + options.explore_seeds);
+  }
+  DensifyResult relocate(const splat_relocate_options &options, Rng &rng) {
+    const double growth = options.growth > 0.0 ? options.growth * static_cast<double>(count_) : 0.0;
+    return edit([&](splat_densify_result *r, int64_t *source, uint64_t capacity) {
+      return splat_trainer_relocate(handle_, &options, rng.handle(), r, source, capacity);
+    }, count_ + static_cast<std::size_t>(growth) + 1);
+  }
+  // Trainer::remove_largest_gaussians and its siblings: how many went.
+  std::size_t remove_largest_gaussians(double share) { return prune(splat_trainer_remove_largest, share); }
+  std::size_t remove_least_contributing_gaussians(double share) { return prune(splat_trainer_remove_least_contributing, share); }
+  std::size_t remove_least_opaque_gaussians(double share) { return prune(splat_trainer_remove_least_opaque, share); }
   [[nodiscard]] std::vector<float> densify_stats() const {
     std::vector<float> out(count_ * 8);
     check(splat_trainer_get_densify_stats(handle_, out.data()));
@@ -154,6 +216,27 @@ public:
   [[nodiscard]] splat_trainer *handle() const noexcept { return handle_; }
 
 private:
+  template <class F> DensifyResult edit(F call, std::size_t capacity) {
+    DensifyResult out;
+    out.source.resize(capacity);
+    splat_densify_result r{};
+    check(call(&r, out.source.data(), capacity));
+    count_ = static_cast<std::size_t>(r.count);
+    out.source.resize(count_);
+    out.cloned = r.cloned;
+    out.split = r.split;
+    out.seeded = r.seeded;
+    out.pruned = r.pruned;
+    out.heldBack = r.held_back;
+    return out;
+  }
+  std::size_t prune(int (*call)(splat_trainer *, double, uint64_t *), double share) {
+    uint64_t removed = 0;
+    check(call(handle_, share, &removed));
+    count_ -= static_cast<std::size_t>(removed);
+    return static_cast<std::size_t>(removed);
+  }
+
   splat_trainer *handle_ = nullptr;
   int shDegree_ = 0;
   std::size_t count_ = 0;

@@ -47,6 +47,18 @@ def test_defaults_are_the_reference_defaults():
     s._lib.splat_learning_rates_default(ctypes.byref(r))
     got = [r.position, r.scale, r.rotation, r.opacity, r.sh, r.sh_rest_scale, r.trust_region]
     np.testing.assert_allclose(got, [1.6e-4, 0.005, 0.001, 0.05, 0.025, 0.05, 0.0], rtol=1e-6)
+    # DensifyOptions and RelocateOptions (densify.hpp:23-50,87-91).
+    d = s._DensifyOptions()
+    s._lib.splat_densify_options_default(ctypes.byref(d))
+    assert (d.prune_large, d.max_gaussians, d.scored_views, d.transparent_share) == (0, 2**64 - 1, 0, 1.0)
+    assert (d.explore_splits, d.explore_seeds, d.edge_split) == (0, 0, 0)
+    np.testing.assert_allclose([d.gradient_threshold, d.dense_scale, d.prune_opacity, d.max_screen_radius, d.max_world_scale,
+                                d.split_threshold, d.min_marked_pixels], [2e-4, 0.0, 0.005, 20.0, 0.0, 0.0, 5.0], rtol=1e-6)
+    m = s._RelocateOptions()
+    s._lib.splat_relocate_options_default(ctypes.byref(m))
+    assert abs(m.min_opacity - 0.005) < 1e-9 and m.growth == 0.05 and m.max_gaussians == 2**64 - 1
+    py = s.DensifyOptions()._c()
+    assert [getattr(py, f) for f, _ in d._fields_] == [getattr(d, f) for f, _ in d._fields_]
 
 
 def _tiny_cloud(s, n=4, degree=0):
@@ -114,3 +126,31 @@ def test_sorts_refuse_unaligned_arrays():
     fn = s._lib.splat_radix_sort_u32_noalloc
     assert fn(s._P(0x1000), s._P(0x2008), s._P(0x3000), s._P(0x4000), 10, 16, 8, None) == s.SPLAT_ERR_INVALID
     assert "16-byte aligned" in s._lib.splat_last_error().decode()
+
+
+def test_cpp_face_compiles_links_and_draws_as_the_reference(tmp_path):
+    # include/splat_trainer.hpp, the reference-shaped C++ class over the ABI,
+    # compiles as C++20, links against the library and runs its host-only
+    # part: the generator's picks, which the CPU reference draws the same.
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no C++ compiler")
+    source = tmp_path / "face.cpp"
+    source.write_text('#include "splat_trainer.hpp"\n#include <cstdio>\n'
+                      "int main() {\n  splat_b200::Rng rng(8);\n"
+                      "  for (int k = 0; k < 5; ++k) std::printf(\"%zu \", rng.pick(1000));\n"
+                      "  splat_densify_options d = splat_b200::default_densify_options();\n"
+                      "  splat_relocate_options r = splat_b200::default_relocate_options();\n"
+                      "  std::printf(\"%g %g\\n\", d.gradient_threshold, r.growth);\n}\n")
+    lib = ROOT / "vibe-splat_b200"
+    exe = tmp_path / "face"
+    subprocess.run([gxx, "-std=c++20", "-I", str(ROOT / "include"), str(source), "-L", str(lib), "-lsplat_b200",
+                    f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    splat = splat_module()
+    rng = splat.Rng(8)
+    assert [int(v) for v in out[:5]] == [rng.pick(1000) for _ in range(5)]
+    assert float(out[5]) == pytest.approx(2e-4) and float(out[6]) == pytest.approx(0.05)
