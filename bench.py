@@ -614,11 +614,20 @@ def our_arm(args) -> None:
         centre = held.positions.reshape(-1, 3).mean(axis=0)
         extent = float(np.linalg.norm(held.positions.reshape(-1, 3) - centre, axis=1).max())
         d_opts = splat.DensifyOptions(dense_scale=0.01 * extent, max_gaussians=int(n * 1.05))
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = trainer.densify(d_opts, splat.Rng(1))
-        d_ms = (time.perf_counter() - t0) * 1000.0
-        densify = {"ms": d_ms, "of": n, "count": r.count, "cloned": r.cloned, "split": r.split, "pruned": r.pruned,
+        rng = splat.Rng(1)
+
+        def more_steps(count):
+            for i in range(count):
+                trainer.step_device_target(cams[i % len(cams)], device_targets[i % len(cams)].data_ptr(), rates)
+
+        def timed(edit):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = edit()
+            return r, (time.perf_counter() - t0) * 1000.0
+
+        r, d_ms = timed(lambda: trainer.densify(d_opts, rng))
+        densify = {"ms_first": d_ms, "of": n, "count": r.count, "cloned": r.cloned, "split": r.split, "pruned": r.pruned,
                    "held_back": r.held_back}
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             from oracle import oracle as O
@@ -630,13 +639,20 @@ def our_arm(args) -> None:
                 densify["reference_cpu_ms"] = (time.perf_counter() - t0) * 1000.0
                 densify["reference_same_result"] = bool(np.array_equal(ref.source, r.source))
         del held, raw
+        # A later round, once the edit's buffers exist: statistics of a few
+        # more steps, then densify again on the same generator.
+        more_steps(5)
+        r, d_ms = timed(lambda: trainer.densify(d_opts, rng))
+        densify["ms"] = d_ms
+        densify["count_second"] = r.count
         # 3DGS-MCMC relocation (dead onto live, 5 % growth): the dead/alive
-        # split and the gathers on the GPU, the draws on the host.
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = trainer.relocate(splat.RelocateOptions(), splat.Rng(2))
-        densify["relocate"] = {"ms": (time.perf_counter() - t0) * 1000.0, "count": r.count, "relocated": r.cloned,
-                               "grown": r.seeded}
+        # split and the gathers on the GPU, the draws on the host; first and
+        # a later round.
+        r, m_first = timed(lambda: trainer.relocate(splat.RelocateOptions(), rng))
+        more_steps(5)
+        r2, m_ms = timed(lambda: trainer.relocate(splat.RelocateOptions(), rng))
+        densify["relocate"] = {"ms_first": m_first, "ms": m_ms, "count": r2.count, "relocated": r2.cloned,
+                               "grown": r2.seeded}
 
     # Pruning on the GPU (remove_largest_gaussians, 1 % of the Gaussians):
     # keys, sort, scan and the gathers of parameters and optimiser state.

@@ -20,6 +20,7 @@
 #include <new>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_fp16.h>
@@ -190,6 +191,7 @@ public:
   // scratch, tables and host-computed rows of an edit. Kept from one edit to
   // the next, so that a training run's edits allocate little.
   DeviceBuffer spareParams[6], spareState[5], editScratch, editTables, editRows;
+  PinnedBuffer editHost;
   bool haveGradients = false, haveRaw = false;
 
   // Per (view, Gaussian).
@@ -2072,13 +2074,58 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
 }
 
 
+// f(begin, end) over [0, count), split across up to 16 host threads.
+template <class F> void parallel_ranges(size_t count, F f) {
+  const size_t cores = std::max(1u, std::thread::hardware_concurrency());
+  const size_t threads = count < 65536 ? 1 : std::min<size_t>(cores, 16);
+  if (threads <= 1) {
+    f(size_t{0}, count);
+    return;
+  }
+  const size_t chunk = (count + threads - 1) / threads;
+  std::vector<std::thread> pool;
+  for (size_t k = 0; k < threads && k * chunk < count; ++k) pool.emplace_back(f, k * chunk, std::min(count, (k + 1) * chunk));
+  for (std::thread &t : pool) t.join();
+}
+
+// Draws of std::discrete_distribution<std::size_t> over `weights` (m of
+// them, filled in by weight(k)), restated so that its parts that do not
+// depend on each other run in parallel: the weights normalised by their sum,
+// their running sum with the last entry set to 1, and per draw the first
+// entry not below std::generate_canonical<double, 53> of the generator, the
+// draws taken from it in order. With fewer than two weights every draw is 0
+// and takes nothing from the generator.
+template <class W>
+std::vector<size_t> discrete_draws(size_t m, W weight, size_t count, std::mt19937 &rng, std::vector<double> &cumulative) {
+  std::vector<size_t> picks(count, 0);
+  if (m < 2) return picks;
+  cumulative.resize(m);
+  parallel_ranges(m, [&](size_t b, size_t e) {
+    for (size_t k = b; k < e; ++k) cumulative[k] = weight(k);
+  });
+  double sum = 0.0;
+  for (size_t k = 0; k < m; ++k) sum += cumulative[k];
+  parallel_ranges(m, [&](size_t b, size_t e) {
+    for (size_t k = b; k < e; ++k) cumulative[k] = cumulative[k] / sum;
+  });
+  for (size_t k = 1; k < m; ++k) cumulative[k] = cumulative[k - 1] + cumulative[k];
+  cumulative[m - 1] = 1.0;
+  std::vector<double> p(count);
+  for (double &v : p) v = std::generate_canonical<double, std::numeric_limits<double>::digits>(rng);
+  parallel_ranges(count, [&](size_t b, size_t e) {
+    for (size_t j = b; j < e; ++j)
+      picks[j] = (size_t)(std::lower_bound(cumulative.begin(), cumulative.end(), p[j]) - cumulative.begin());
+  });
+  return picks;
+}
+
 // Trainer::relocate on the GPU and the host (trainer.cpp:717-722;
 // relocate_cloud, densify.cpp:328-420; apply_changes). The device splits the
 // Gaussians into dead and alive and gathers the new cloud and its optimiser
-// state; the draws (std::discrete_distribution over opacities, from rng in
-// the reference's order) and the opacity and scale updates of the drawn
-// targets, a sequential chain, run on the host over the opacities and
-// log-scales, the only values relocation changes.
+// state; the draws (from rng in the reference's order) and the opacity and
+// scale updates of the drawn targets run on the host, in parallel where
+// they do not depend on each other, over the opacities and log-scales, the
+// only values relocation changes, kept in pinned memory.
 void relocate_gaussians(splat_trainer *handle, const splat_relocate_options &o, std::mt19937 &rng, splat_densify_result *result,
                         int64_t *source, uint64_t sourceCapacity) {
   Trainer *t = impl_of(handle);
@@ -2093,8 +2140,11 @@ void relocate_gaussians(splat_trainer *handle, const splat_relocate_options &o, 
   run.scan(alive, alivePlace, 1);
   const std::vector<uint32_t> c = run.read();
   const uint32_t deadCount = c[1], aliveCount = c[5];
-  std::vector<int64_t> stateSource(n);
-  for (uint32_t i = 0; i < n; ++i) stateSource[i] = i;
+  // Growth, fixed by the count alone (densify.cpp:389-390).
+  const uint64_t room = o.max_gaussians > n ? o.max_gaussians - n : 0;
+  const double share = o.growth * static_cast<double>(n);
+  const uint64_t wanted = share >= static_cast<double>(room) ? room : std::min<uint64_t>(static_cast<size_t>(share), room);
+  if (wanted + n > 0x7FFFFFFFull) throw Failure{SPLAT_ERR_INVALID, "relocation would exceed 2^31 - 1 Gaussians"};
   splat_densify_result counts{};
   counts.count = n;
   if (aliveCount == 0) {
@@ -2102,104 +2152,97 @@ void relocate_gaussians(splat_trainer *handle, const splat_relocate_options &o, 
     // apply_changes leaves them.
     SB_CUDA(cudaMemsetAsync(t->densifyStats.get(), 0, (size_t)n * sb::kStatStride * 4, s));
     SB_CUDA(cudaStreamSynchronize(s));
-    if (source != nullptr && sourceCapacity >= n) std::copy(stateSource.begin(), stateSource.end(), source);
+    if (source != nullptr && sourceCapacity >= n)
+      for (uint32_t i = 0; i < n; ++i) source[i] = i;
     if (result != nullptr) *result = counts;
     return;
   }
+  const size_t capacity = (size_t)n + wanted;
+  const size_t hostBytes = capacity * 16 + (size_t)n * 8;
+  if (t->editHost.bytes() < hostBytes) t->editHost.ensure(hostBytes + hostBytes / 4);
+  float *opacity = t->editHost.get<float>();
+  float *logScale = opacity + capacity;
+  uint32_t *deadList = reinterpret_cast<uint32_t *>(logScale + capacity * 3);
+  uint32_t *aliveList = deadList + n;
   sb::launch_compact(dead.get<uint32_t>(), deadPlace.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
-  const std::vector<uint32_t> deadList = run.download(list.get<uint32_t>(), deadCount);
-  sb::launch_compact(alive.get<uint32_t>(), alivePlace.get<uint32_t>(), nullptr, n, list.get<uint32_t>(), nullptr, s);
-  const std::vector<uint32_t> aliveList = run.download(list.get<uint32_t>(), aliveCount);
-  std::vector<float> opacity(n), logScale((size_t)n * 3);
-  SB_CUDA(cudaMemcpyAsync(opacity.data(), t->opacities.get(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
-  SB_CUDA(cudaMemcpyAsync(logScale.data(), t->scales.get(), (size_t)n * 12, cudaMemcpyDeviceToHost, s));
+  if (deadCount > 0) SB_CUDA(cudaMemcpyAsync(deadList, list.get(), (size_t)deadCount * 4, cudaMemcpyDeviceToHost, s));
+  sb::launch_compact(alive.get<uint32_t>(), alivePlace.get<uint32_t>(), nullptr, n, deadPlace.get<uint32_t>(), nullptr, s);
+  SB_CUDA(cudaMemcpyAsync(aliveList, deadPlace.get(), (size_t)aliveCount * 4, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaMemcpyAsync(opacity, t->opacities.get(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaMemcpyAsync(logScale, t->scales.get(), (size_t)n * 12, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaGetLastError());
   SB_CUDA(cudaStreamSynchronize(s));
 
   // origin[k]: the old Gaussian whose position, rotation and SH slot k holds.
-  std::vector<int32_t> origin(n);
-  for (uint32_t i = 0; i < n; ++i) origin[i] = (int32_t)i;
+  std::vector<int32_t> origin(capacity), stateSource(capacity, -1);
+  for (uint32_t i = 0; i < n; ++i) origin[i] = stateSource[i] = (int32_t)i;
   const auto sigmoid = [](float x) { return 1.f / (1.f + std::exp(-x)); };
+  std::vector<int> times(n);
   // A target drawn m times becomes m + 1 equal copies (at most 51): opacity
   // 1 - (1 - o)^(1/N) and scale times o / D, D the alternating binomial sum
-  // of 3DGS-MCMC (densify.cpp:342-364).
-  const auto update_targets = [&](const std::vector<size_t> &targets, size_t size) {
-    std::vector<int> times(size, 0);
+  // of 3DGS-MCMC (densify.cpp:342-364). Each target's update is its own.
+  const auto update_targets = [&](const std::vector<size_t> &targets) {
+    std::fill(times.begin(), times.end(), 0);
     for (const size_t k : targets) ++times[k];
-    for (size_t k = 0; k < size; ++k) {
-      if (times[k] == 0) continue;
-      const int copies = std::min(times[k] + 1, 51);
-      const double was = sigmoid(opacity[k]);
-      const double fresh = 1.0 - std::pow(1.0 - was, 1.0 / copies);
-      double divisor = 0.0;
-      for (int i = 1; i <= copies; ++i) {
-        double binom = 1.0;
-        for (int j = 0; j < i; ++j) {
-          if (j > 0) binom = binom * static_cast<double>(i - j) / j;
-          divisor += binom * (j % 2 == 0 ? 1.0 : -1.0) * std::pow(fresh, j + 1) / std::sqrt(static_cast<double>(j + 1));
+    parallel_ranges(n, [&](size_t b, size_t e) {
+      for (size_t k = b; k < e; ++k) {
+        if (times[k] == 0) continue;
+        const int copies = std::min(times[k] + 1, 51);
+        const double was = sigmoid(opacity[k]);
+        const double fresh = 1.0 - std::pow(1.0 - was, 1.0 / copies);
+        double divisor = 0.0;
+        for (int i = 1; i <= copies; ++i) {
+          double binom = 1.0;
+          for (int j = 0; j < i; ++j) {
+            if (j > 0) binom = binom * static_cast<double>(i - j) / j;
+            divisor += binom * (j % 2 == 0 ? 1.0 : -1.0) * std::pow(fresh, j + 1) / std::sqrt(static_cast<double>(j + 1));
+          }
         }
+        const double clamped = std::clamp(fresh, static_cast<double>(o.min_opacity), 1.0 - 1e-6);
+        opacity[k] = static_cast<float>(std::log(clamped / (1.0 - clamped)));
+        const double factor = divisor > 0.0 ? was / divisor : 1.0;
+        for (size_t a = 0; a < 3; ++a) logScale[k * 3 + a] += static_cast<float>(std::log(factor));
+        stateSource[k] = -1;
       }
-      const double clamped = std::clamp(fresh, static_cast<double>(o.min_opacity), 1.0 - 1e-6);
-      opacity[k] = static_cast<float>(std::log(clamped / (1.0 - clamped)));
-      const double factor = divisor > 0.0 ? was / divisor : 1.0;
-      for (size_t a = 0; a < 3; ++a) logScale[k * 3 + a] += static_cast<float>(std::log(factor));
-      stateSource[k] = -1;
-    }
+    });
   };
   const auto copy_into = [&](size_t from, size_t to) {
     origin[to] = origin[from];
     opacity[to] = opacity[from];
     for (size_t a = 0; a < 3; ++a) logScale[to * 3 + a] = logScale[from * 3 + a];
   };
-  const auto draw = [&](const auto &from, size_t count) {
-    std::vector<double> weights;
-    weights.reserve(from.size());
-    for (const auto k : from) weights.push_back(sigmoid(opacity[k]));
-    std::discrete_distribution<size_t> pick(weights.begin(), weights.end());
-    std::vector<size_t> targets(count);
-    for (size_t &k : targets) k = from[pick(rng)];
-    return targets;
-  };
+  std::vector<double> cumulative;
   if (deadCount > 0) {
-    const std::vector<size_t> targets = draw(aliveList, deadCount);
-    update_targets(targets, n);
-    for (size_t j = 0; j < deadList.size(); ++j) {
+    std::vector<size_t> targets = discrete_draws(
+        aliveCount, [&](size_t k) { return (double)sigmoid(opacity[aliveList[k]]); }, deadCount, rng, cumulative);
+    for (size_t &k : targets) k = aliveList[k];
+    update_targets(targets);
+    for (size_t j = 0; j < deadCount; ++j) {
       copy_into(targets[j], deadList[j]);
       stateSource[deadList[j]] = -1;
     }
     counts.cloned = deadCount;
   }
-  const uint64_t room = o.max_gaussians > n ? o.max_gaussians - n : 0;
-  const double share = o.growth * static_cast<double>(n);
-  const uint64_t wanted = share >= static_cast<double>(room) ? room : std::min<uint64_t>(static_cast<size_t>(share), room);
-  if (wanted + n > 0x7FFFFFFFull) throw Failure{SPLAT_ERR_INVALID, "relocation would exceed 2^31 - 1 Gaussians"};
   if (wanted > 0) {
-    std::vector<size_t> everyone(n);
-    for (uint32_t i = 0; i < n; ++i) everyone[i] = i;
-    const std::vector<size_t> targets = draw(everyone, wanted);
-    update_targets(targets, n);
-    origin.resize(n + wanted);
-    opacity.resize(n + wanted);
-    logScale.resize((n + wanted) * 3);
-    for (size_t k = 0; k < targets.size(); ++k) {
-      copy_into(targets[k], n + k);
-      stateSource.push_back(-1);
-    }
+    const std::vector<size_t> targets = discrete_draws(n, [&](size_t k) { return (double)sigmoid(opacity[k]); }, wanted, rng,
+                                                       cumulative);
+    update_targets(targets);
+    for (size_t k = 0; k < targets.size(); ++k) copy_into(targets[k], n + k);
     counts.seeded = wanted;
   }
-  const auto newN = (uint32_t)(n + wanted);
+  const auto newN = (uint32_t)capacity;
   counts.count = newN;
-  std::vector<int32_t> state32(newN);
-  for (uint32_t k = 0; k < newN; ++k) state32[k] = (int32_t)stateSource[k];
   Arena tables(t->editTables, 2 * Arena::room((size_t)newN * 4));
   const Slice paramTable = tables.take((size_t)newN * 4), stateTable = tables.take((size_t)newN * 4);
   SB_CUDA(cudaMemcpyAsync(paramTable.get(), origin.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(stateTable.get(), state32.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(stateTable.get(), stateSource.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, s));
   SB_CUDA(cudaStreamSynchronize(s));
   Trainer *fresh = regather(handle, paramTable.get<int32_t>(), stateTable.get<int32_t>(), newN);
-  SB_CUDA(cudaMemcpyAsync(fresh->opacities.get(), opacity.data(), (size_t)newN * 4, cudaMemcpyHostToDevice, fresh->stream));
-  SB_CUDA(cudaMemcpyAsync(fresh->scales.get(), logScale.data(), (size_t)newN * 12, cudaMemcpyHostToDevice, fresh->stream));
+  SB_CUDA(cudaMemcpyAsync(fresh->opacities.get(), opacity, (size_t)newN * 4, cudaMemcpyHostToDevice, fresh->stream));
+  SB_CUDA(cudaMemcpyAsync(fresh->scales.get(), logScale, (size_t)newN * 12, cudaMemcpyHostToDevice, fresh->stream));
   SB_CUDA(cudaStreamSynchronize(fresh->stream));
-  if (source != nullptr && sourceCapacity >= newN) std::copy(stateSource.begin(), stateSource.end(), source);
+  if (source != nullptr && sourceCapacity >= newN)
+    for (uint32_t k = 0; k < newN; ++k) source[k] = stateSource[k];
   if (result != nullptr) *result = counts;
 }
 } // namespace
