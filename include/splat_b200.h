@@ -180,6 +180,12 @@ int splat_trainer_score_view(splat_trainer *trainer, const splat_camera *camera,
 /* Trainer::collect_statistics (trainer.hpp:106). */
 int splat_trainer_collect_statistics(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target,
                                      size_t target_bytes, splat_step_stats *stats);
+/* The same two passes with the target already in device memory (an RGBA8
+ * image the caller keeps in HBM, as the session keeps its views). */
+int splat_trainer_collect_statistics_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
+                                                   size_t target_bytes, splat_step_stats *stats);
+int splat_trainer_score_view_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
+                                           size_t target_bytes, float error_share, float pixel_weight, splat_step_stats *stats);
 /* Trainer::apply_gradients (trainer.hpp:121): one Adam step from the sums the last
  * compute_gradients left. */
 int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_rates *rates);
@@ -318,6 +324,110 @@ void splat_relocate_options_default(splat_relocate_options *options);
  * only the statistics start anew. source as splat_trainer_densify. */
 int splat_trainer_relocate(splat_trainer *trainer, const splat_relocate_options *options, splat_rng *rng,
                            splat_densify_result *result, int64_t *source, uint64_t source_capacity);
+
+/* The training session (TrainSession, src/train/train.hpp:193-270 and
+ * train.cpp:474-760, with the schedule of src/train/schedule.cpp): it owns a
+ * trainer made from starting points (initial_cloud, train.cpp:194-212: sizes
+ * from the 3 nearest neighbours, found on the GPU) and the training views,
+ * kept in HBM at full, half and quarter size (half_size, train.cpp:232-255,
+ * on the GPU), and runs the reference's schedule one iteration per
+ * splat_session_step: the shuffled view order, coarse to fine (quarter size
+ * until coarse_until[1] of the way, half until coarse_until[0]; from the
+ * photos' spectra with adaptive_schedule), the position rate's decay and the
+ * SH degree's ramp, densification rounds with scored views, the growth cap
+ * and opacity resets (or 3DGS-MCMC relocation), and the pruning rounds.
+ * Exposure, pose refinement, second order, SH dropout and the Mip filters
+ * are not offered: they have no kernel here. */
+typedef struct splat_session_options {
+  int32_t iterations;         /* 15000 */
+  int32_t sh_degree;          /* 2 */
+  uint32_t seed;              /* 1: the view order draws from mt19937(seed), densification from mt19937(seed + 1) */
+  int32_t report_every;       /* 500: the probe view's PSNR every this many iterations; 0 never */
+  int32_t densify;            /* 1 */
+  int32_t densify_mode;       /* 0: clone, split and prune (ADC); 1: relocation (3DGS-MCMC) */
+  int32_t full_adam;          /* 0 */
+  int32_t full_resolution;    /* 0: start at quarter, then half size */
+  int32_t adaptive_schedule;  /* 0: 1 sets the sizes from the photos' spectra and grows the cap with them */
+  float gradient_threshold;   /* 2e-4 */
+  float split_threshold;      /* 1.2e-3 */
+  double dense_fraction;      /* 0.001 of the extent: larger Gaussians split, smaller clone */
+  int32_t densify_interval;   /* 100 */
+  int32_t score_views;        /* 10 */
+  float score_min_pixels;     /* 5 */
+  int32_t explore;            /* 0 */
+  int32_t significance_prune; /* 0 */
+  int32_t edge_split;         /* 0 */
+  double threshold_rise;      /* 1 */
+  double prune_share;         /* 0 */
+  double recovery_prune;      /* 0 */
+  double max_growth;          /* -1: 4 per 7000 iterations */
+  uint64_t max_gaussians;     /* 0: as the memory budget allows */
+  double coarse_until[2];     /* 0.35, 0.15 */
+} splat_session_options;
+void splat_session_options_default(splat_session_options *options);
+
+/* TrainData (train.hpp:153-173) as host arrays: the starting points (3
+ * doubles and 3 colour bytes each), the training views (cameras and RGBA8
+ * images at full size), the scene's extent and typical depth (the near
+ * plane is 0.01 of it). */
+typedef struct splat_session_data {
+  const double *points;
+  const uint8_t *colors;
+  uint64_t point_count;
+  const splat_camera *cameras;
+  const uint8_t *const *images;
+  int32_t views;
+  double extent;
+  double typical_depth;
+} splat_session_data;
+
+/* What the session has done: the last iteration, its level (0 half, 1
+ * quarter, 2 full size) and view, the position rate it used, the Gaussian
+ * count, the losses, the last report's probe PSNR and mean loss, the
+ * densification rounds, and the coarse levels' ends. */
+typedef struct splat_session_state {
+  int32_t iteration;
+  int32_t level;
+  int32_t view;
+  float position_rate;
+  uint64_t gaussians;
+  float first_loss, last_loss;
+  int32_t report_iteration;
+  double probe_psnr, mean_loss;
+  int32_t densify_rounds;
+  double densify_seconds;
+  splat_densify_result last_densify;
+  uint64_t held_back_total, pruned_total;
+  double coarse_until[2];
+} splat_session_state;
+
+typedef struct splat_session splat_session;
+/* trainer_options may be null (the defaults); the session sets selective_adam
+ * from full_adam and the near plane from the typical depth. */
+int splat_session_create(const splat_session_data *data, const splat_session_options *options,
+                         const splat_trainer_options *trainer_options, splat_session **out);
+int splat_session_destroy(splat_session *session);
+/* TrainSession::step: SPLAT_ERR_STATE once every iteration has run. */
+int splat_session_step(splat_session *session, splat_step_stats *stats);
+int splat_session_get_state(splat_session *session, splat_session_state *out);
+/* The session's trainer, borrowed (render, cloud, save); not to be destroyed. */
+int splat_session_trainer(splat_session *session, splat_trainer **out);
+
+/* The schedule's parts on their own. frequency_energy (schedule.cpp:41-75)
+ * on the GPU: per factor, the spectrum magnitude of the image's brightness
+ * within the frequencies an image smaller by that factor holds (up to 8
+ * factors, images up to 4096 x 4096). resolution_switches
+ * (schedule.cpp:77-82). GrowthBudget (schedule.hpp:26-41) after the given
+ * observations: its limit at image_factor and progress, and its final count.
+ * half_size (train.cpp:232-255) and initial_cloud (train.cpp:194-212) on
+ * the GPU, host arrays in and out. */
+int splat_frequency_energy(const uint8_t *rgba, int32_t width, int32_t height, const int32_t *factors, int32_t count, double *out);
+int splat_resolution_switches(double full, double half, double quarter, double out[2]);
+int splat_growth_limit(double initial_count, double factor, const uint64_t *observed, int32_t observations, double image_factor,
+                       double progress, uint64_t *limit, double *final_count);
+int splat_half_size(const uint8_t *rgba, int32_t width, int32_t height, uint8_t *out);
+int splat_initial_cloud(const double *points, const uint8_t *colors, uint64_t count, int32_t sh_degree, float *positions, float *scales,
+                        float *rotations, float *opacities, float *sh);
 
 /* Trainer methods with no kernel in this library, for callers that set them
  * unconditionally: the neutral setting is accepted and changes nothing, any

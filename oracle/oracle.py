@@ -285,6 +285,83 @@ def ref_relocate(cloud: Cloud, options, rng: RefRng) -> RefDensified:
     return RefDensified(result, source[:n], {k: int(v) for k, v in zip(names, counts)})
 
 
+# ----------------------------------------------------------------- session schedule
+
+
+def ref_frequency_energy(rgba: np.ndarray, width: int, height: int, factors=(1, 2, 4)) -> np.ndarray:
+    """The reference's frequency_energy (schedule.cpp:41-75)."""
+    lib = ref_lib()
+    image = np.ascontiguousarray(rgba, np.uint8).ravel()
+    f = (ctypes.c_int * len(factors))(*factors)
+    out = np.zeros(len(factors), np.float64)
+    assert lib.ref_frequency_energy(image.ctypes.data_as(_U8), ctypes.c_int(width), ctypes.c_int(height), f,
+                                    ctypes.c_int(len(factors)), _dp(out)) == 0
+    return out
+
+
+def ref_resolution_switches(full: float, half: float, quarter: float) -> tuple:
+    """The reference's resolution_switches (schedule.cpp:77-82)."""
+    out = np.zeros(2, np.float64)
+    lib = ref_lib()
+    lib.ref_resolution_switches.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
+    lib.ref_resolution_switches(full, half, quarter, _dp(out))
+    return float(out[0]), float(out[1])
+
+
+def ref_growth_limit(initial: float, factor: float, observed, image_factor: float, progress: float) -> tuple:
+    """The reference's GrowthBudget (schedule.hpp:26-41): (limit, final count)."""
+    lib = ref_lib()
+    lib.ref_growth_limit.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64), _D]
+    obs = (ctypes.c_uint64 * max(len(observed), 1))(*observed)
+    limit, final = ctypes.c_uint64(), ctypes.c_double()
+    lib.ref_growth_limit(initial, factor, obs, len(observed), image_factor, progress, ctypes.byref(limit), ctypes.byref(final))
+    return limit.value, final.value
+
+
+def ref_view_order(seed: int, views: int, steps: int) -> list:
+    """TrainSession's view order (train.cpp:560-565, 580-586) over std::mt19937(seed)."""
+    out = (ctypes.c_int * steps)()
+    ref_lib().ref_view_order(ctypes.c_uint32(seed), ctypes.c_int(views), ctypes.c_int(steps), out)
+    return list(out)
+
+
+def half_size(rgba: np.ndarray, width: int, height: int) -> np.ndarray:
+    """half_size (train.cpp:232-255) restated: the rounded mean of each 2x2 block, per channel."""
+    w, h = width // 2, height // 2
+    img = np.asarray(rgba, np.uint32).reshape(height, width, 4)[: 2 * h, : 2 * w]
+    s = img[0::2, 0::2] + img[0::2, 1::2] + img[1::2, 0::2] + img[1::2, 1::2]
+    return ((s + 2) // 4).astype(np.uint8).ravel()
+
+
+def neighbour_distances(points: np.ndarray) -> np.ndarray:
+    """neighbour_distances (train.cpp:143-189) restated for small clouds: on the
+    reference's grid, the mean distance to the 3 nearest other points within
+    the cube of cells of radius r, for the first r of 1..4 that holds 3, else
+    the cell size; float32 of max(mean, 1e-7)."""
+    p = np.asarray(points, np.float64).reshape(-1, 3)
+    n = p.shape[0]
+    low, high = p.min(axis=0), p.max(axis=0)
+    size = high - low
+    cell = max(np.cbrt(max(size[0] * size[1] * size[2], 1e-30) / n * 8.0), max(size) / 512.0)
+    cells = ((p - low) / cell).astype(np.int64)
+    out = np.zeros(n, np.float32)
+    for i in range(n):
+        d = p - p[i]
+        dist = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        far = np.abs(cells - cells[i]).max(axis=1)
+        mean = cell
+        for r in range(1, 5):
+            mask = far <= r
+            mask[i] = False
+            if mask.sum() >= 3:
+                best = np.sort(dist[mask])[:3]
+                mean = (np.sqrt(best[0]) + np.sqrt(best[1]) + np.sqrt(best[2])) / 3.0
+                break
+        out[i] = np.float32(max(mean, 1e-7))
+    return out
+
+
 def ref_save_ply(cloud: Cloud, path) -> None:
     """The reference's save_ply (gaussian_cloud.cpp:330-365)."""
     keep, cargs = _cloud_args(cloud)

@@ -11,11 +11,16 @@
 // column-major world->camera matrix, the camera centre, fx, fy, cx, cy, size.
 #include "train/densify.hpp"
 #include "train/reference.hpp"
+#include "train/schedule.hpp"
 
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <algorithm>
+#include <array>
+#include <numeric>
 #include <random>
+#include <vector>
 
 using namespace splat;
 
@@ -335,6 +340,54 @@ int ref_relocate(int n, int degree, const float *positions, const float *scales,
     return 0;
   } catch (const std::exception &) {
     return 1;
+  }
+}
+
+// frequency_energy and resolution_switches (schedule.cpp:41-82): the
+// reference's own, for the schedule's parity.
+int ref_frequency_energy(const std::uint8_t *rgba, int width, int height, const int *factors, int count, double *out) {
+  try {
+    const std::vector<std::uint8_t> image(rgba, rgba + static_cast<std::size_t>(width) * height * 4);
+    const std::vector<double> e = frequency_energy(image, width, height, std::vector<int>(factors, factors + count));
+    std::copy(e.begin(), e.end(), out);
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+void ref_resolution_switches(double full, double half, double quarter, double *out) {
+  const std::array<double, 2> s = resolution_switches(full, half, quarter);
+  out[0] = s[0];
+  out[1] = s[1];
+}
+
+// GrowthBudget (schedule.hpp:26-41) after the observations: limit and final count.
+void ref_growth_limit(double initial, double factor, const std::uint64_t *observed, int observations, double imageFactor,
+                      double progress, std::uint64_t *limit, double *finalCount) {
+  GrowthBudget budget(static_cast<std::size_t>(initial), factor);
+  for (int k = 0; k < observations; ++k) budget.observe(observed[k]);
+  *limit = budget.limit(imageFactor, progress);
+  *finalCount = budget.final_count();
+}
+
+// The order TrainSession draws its views in (train.cpp:560-565, 580-586),
+// restated over the same generator and std::shuffle: for each of `steps`
+// iterations the view it trains on.
+void ref_view_order(std::uint32_t seed, int views, int steps, int *out) {
+  std::mt19937 rng(seed);
+  std::vector<std::size_t> order;
+  const auto refill = [&] {
+    if (!order.empty()) return;
+    order.resize(static_cast<std::size_t>(views));
+    std::iota(order.begin(), order.end(), std::size_t{0});
+    std::shuffle(order.begin(), order.end(), rng);
+  };
+  for (int i = 0; i < steps; ++i) {
+    refill();
+    out[i] = static_cast<int>(order.back());
+    order.pop_back();
+    refill();
   }
 }
 

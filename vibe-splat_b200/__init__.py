@@ -206,6 +206,51 @@ class _RelocateOptions(ctypes.Structure):
 _lib.splat_relocate_options_default.argtypes = [ctypes.POINTER(_RelocateOptions)]
 _lib.splat_trainer_relocate.argtypes = [_P, ctypes.POINTER(_RelocateOptions), _P, ctypes.POINTER(_DensifyResult),
                                         ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64]
+class _SessionOptions(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("sh_degree", ctypes.c_int32), ("seed", ctypes.c_uint32),
+                ("report_every", ctypes.c_int32), ("densify", ctypes.c_int32), ("densify_mode", ctypes.c_int32),
+                ("full_adam", ctypes.c_int32), ("full_resolution", ctypes.c_int32), ("adaptive_schedule", ctypes.c_int32),
+                ("gradient_threshold", ctypes.c_float), ("split_threshold", ctypes.c_float), ("dense_fraction", ctypes.c_double),
+                ("densify_interval", ctypes.c_int32), ("score_views", ctypes.c_int32), ("score_min_pixels", ctypes.c_float),
+                ("explore", ctypes.c_int32), ("significance_prune", ctypes.c_int32), ("edge_split", ctypes.c_int32),
+                ("threshold_rise", ctypes.c_double), ("prune_share", ctypes.c_double), ("recovery_prune", ctypes.c_double),
+                ("max_growth", ctypes.c_double), ("max_gaussians", ctypes.c_uint64), ("coarse_until", ctypes.c_double * 2)]
+
+
+class _SessionData(ctypes.Structure):
+    _fields_ = [("points", ctypes.POINTER(ctypes.c_double)), ("colors", ctypes.POINTER(ctypes.c_uint8)),
+                ("point_count", ctypes.c_uint64), ("cameras", ctypes.POINTER(_Camera)), ("images", ctypes.POINTER(_P)),
+                ("views", ctypes.c_int32), ("extent", ctypes.c_double), ("typical_depth", ctypes.c_double)]
+
+
+class _SessionState(ctypes.Structure):
+    _fields_ = [("iteration", ctypes.c_int32), ("level", ctypes.c_int32), ("view", ctypes.c_int32),
+                ("position_rate", ctypes.c_float), ("gaussians", ctypes.c_uint64), ("first_loss", ctypes.c_float),
+                ("last_loss", ctypes.c_float), ("report_iteration", ctypes.c_int32), ("probe_psnr", ctypes.c_double),
+                ("mean_loss", ctypes.c_double), ("densify_rounds", ctypes.c_int32), ("densify_seconds", ctypes.c_double),
+                ("last_densify", _DensifyResult), ("held_back_total", ctypes.c_uint64), ("pruned_total", ctypes.c_uint64),
+                ("coarse_until", ctypes.c_double * 2)]
+
+
+_lib.splat_session_options_default.argtypes = [ctypes.POINTER(_SessionOptions)]
+_lib.splat_session_create.argtypes = [ctypes.POINTER(_SessionData), ctypes.POINTER(_SessionOptions), ctypes.POINTER(_Options),
+                                      ctypes.POINTER(_P)]
+_lib.splat_session_destroy.argtypes = [_P]
+_lib.splat_session_step.argtypes = [_P, ctypes.POINTER(_Stats)]
+_lib.splat_session_get_state.argtypes = [_P, ctypes.POINTER(_SessionState)]
+_lib.splat_session_trainer.argtypes = [_P, ctypes.POINTER(_P)]
+_lib.splat_frequency_energy.argtypes = [_P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
+                                        ctypes.POINTER(ctypes.c_double)]
+_lib.splat_resolution_switches.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+_lib.splat_growth_limit.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32,
+                                    ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64),
+                                    ctypes.POINTER(ctypes.c_double)]
+_lib.splat_half_size.argtypes = [_P, ctypes.c_int32, ctypes.c_int32, _P]
+_lib.splat_initial_cloud.argtypes = [ctypes.POINTER(ctypes.c_double), _P, ctypes.c_uint64, ctypes.c_int32, _FP, _FP, _FP, _FP, _FP]
+_lib.splat_trainer_collect_statistics_device_target.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t,
+                                                                ctypes.POINTER(_Stats)]
+_lib.splat_trainer_score_view_device_target.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_float,
+                                                        ctypes.c_float, ctypes.POINTER(_Stats)]
 _lib.splat_rng_create.argtypes = [ctypes.c_uint32, ctypes.POINTER(_P)]
 _lib.splat_rng_destroy.argtypes = [_P]
 _lib.splat_rng_pick.argtypes = [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
@@ -562,10 +607,24 @@ class Trainer:
         self._degree = initial.sh_degree
         self._prefetch_keep = None
 
+    @classmethod
+    def _borrowed(cls, handle) -> "Trainer":
+        """A view of a trainer another object owns (a session's)."""
+        t = cls.__new__(cls)
+        t.options = None
+        t._keep = None
+        t._h = handle
+        t._owner = False
+        n, degree = ctypes.c_int64(), ctypes.c_int32()
+        _check(_lib.splat_trainer_info(handle, ctypes.byref(n), ctypes.byref(degree), None, None, None, None))
+        t._count, t._degree = n.value, degree.value
+        t._prefetch_keep = None
+        return t
+
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self, "_owner", True):
             _check(_lib.splat_trainer_destroy(self._h))
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -875,3 +934,144 @@ def measure_sm_peaks() -> dict:
 def library():
     """The loaded ctypes library, for callers that bind more entry points."""
     return _lib
+
+
+# ----------------------------------------------------------------- session
+
+
+@dataclass
+class SessionOptions:
+    """TrainOptions' training schedule (train.hpp:25-112) as the session takes it."""
+
+    iterations: int = 15000
+    sh_degree: int = 2
+    seed: int = 1
+    report_every: int = 500
+    densify: bool = True
+    densify_mode: int = 0  # 0 clone/split/prune, 1 relocation
+    full_adam: bool = False
+    full_resolution: bool = False
+    adaptive_schedule: bool = False
+    gradient_threshold: float = 2e-4
+    split_threshold: float = 1.2e-3
+    dense_fraction: float = 0.001
+    densify_interval: int = 100
+    score_views: int = 10
+    score_min_pixels: float = 5.0
+    explore: int = 0
+    significance_prune: bool = False
+    edge_split: bool = False
+    threshold_rise: float = 1.0
+    prune_share: float = 0.0
+    recovery_prune: float = 0.0
+    max_growth: float = -1.0
+    max_gaussians: int = 0
+    coarse_until: tuple = (0.35, 0.15)
+
+    def _c(self) -> _SessionOptions:
+        o = _SessionOptions()
+        for name, _ in _SessionOptions._fields_:
+            value = getattr(self, name)
+            if name == "coarse_until":
+                o.coarse_until[0], o.coarse_until[1] = float(value[0]), float(value[1])
+            else:
+                setattr(o, name, int(value) if isinstance(value, bool) else value)
+        return o
+
+
+class Session:
+    """TrainSession (train.hpp:193-270): the schedule around a trainer, one
+    iteration per step(), with the views resident on the device at three sizes."""
+
+    def __init__(self, points, colors, cameras, images, extent: float, typical_depth: float,
+                 options: SessionOptions | None = None, trainer_options: TrainerOptions | None = None):
+        self.options = options or SessionOptions()
+        self._points = np.ascontiguousarray(np.asarray(points, np.float64).reshape(-1, 3))
+        self._colors = np.ascontiguousarray(np.asarray(colors, np.uint8).reshape(-1, 3))
+        if self._points.shape[0] != self._colors.shape[0]:
+            raise ValueError("one colour per point")
+        cams = (_Camera * len(cameras))(*[c._c() for c in cameras])
+        self._images = [np.ascontiguousarray(np.asarray(im, np.uint8).ravel()) for im in images]
+        ptrs = (_P * len(self._images))(*[im.ctypes.data_as(_P) for im in self._images])
+        data = _SessionData(self._points.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            self._colors.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), self._points.shape[0], cams, ptrs,
+                            len(cameras), float(extent), float(typical_depth))
+        handle = _P()
+        topt = (trainer_options or TrainerOptions())._c()
+        _check(_lib.splat_session_create(ctypes.byref(data), ctypes.byref(self.options._c()), ctypes.byref(topt),
+                                         ctypes.byref(handle)))
+        self._h = handle
+        self._images = None
+
+    def step(self) -> StepStats:
+        s = _Stats()
+        _check(_lib.splat_session_step(self._h, ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def finished(self) -> bool:
+        return self.state().iteration >= self.options.iterations
+
+    def state(self) -> _SessionState:
+        st = _SessionState()
+        _check(_lib.splat_session_get_state(self._h, ctypes.byref(st)))
+        return st
+
+    def trainer(self) -> Trainer:
+        """The session's trainer, borrowed: valid while the session lives."""
+        h = _P()
+        _check(_lib.splat_session_trainer(self._h, ctypes.byref(h)))
+        return Trainer._borrowed(h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.splat_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def frequency_energy(rgba, width: int, height: int, factors=(1, 2, 4)) -> np.ndarray:
+    """frequency_energy (schedule.cpp:41-75), on the GPU."""
+    image = np.ascontiguousarray(np.asarray(rgba, np.uint8).ravel())
+    f = (ctypes.c_int32 * len(factors))(*factors)
+    out = np.zeros(len(factors), np.float64)
+    _check(_lib.splat_frequency_energy(image.ctypes.data_as(_P), width, height, f, len(factors),
+                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return out
+
+
+def resolution_switches(full: float, half: float, quarter: float) -> tuple:
+    """resolution_switches (schedule.cpp:77-82): until half size ends, until quarter size ends."""
+    out = (ctypes.c_double * 2)()
+    _check(_lib.splat_resolution_switches(full, half, quarter, out))
+    return out[0], out[1]
+
+
+def growth_limit(initial: float, factor: float, observed, image_factor: float, progress: float) -> tuple:
+    """GrowthBudget (schedule.hpp:26-41) after `observed` rounds: (limit, final count)."""
+    obs = (ctypes.c_uint64 * max(len(observed), 1))(*observed)
+    limit, final = ctypes.c_uint64(), ctypes.c_double()
+    _check(_lib.splat_growth_limit(initial, factor, obs, len(observed), image_factor, progress, ctypes.byref(limit),
+                                   ctypes.byref(final)))
+    return limit.value, final.value
+
+
+def half_size(rgba, width: int, height: int) -> np.ndarray:
+    """half_size (train.cpp:232-255), on the GPU."""
+    image = np.ascontiguousarray(np.asarray(rgba, np.uint8).ravel())
+    out = np.zeros((height // 2) * (width // 2) * 4, np.uint8)
+    _check(_lib.splat_half_size(image.ctypes.data_as(_P), width, height, out.ctypes.data_as(_P)))
+    return out
+
+
+def initial_cloud(points, colors, sh_degree: int) -> GaussianCloud:
+    """initial_cloud (train.cpp:194-212), the neighbour search on the GPU."""
+    p = np.ascontiguousarray(np.asarray(points, np.float64).reshape(-1, 3))
+    c = np.ascontiguousarray(np.asarray(colors, np.uint8).reshape(-1, 3))
+    n, f = p.shape[0], 3 * (sh_degree + 1) ** 2
+    out = GaussianCloud(sh_degree, *(np.empty(k, np.float32) for k in (n * 3, n * 3, n * 4, n, n * f)))
+    _check(_lib.splat_initial_cloud(p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), c.ctypes.data_as(_P), n, sh_degree,
+                                    _fptr(out.positions), _fptr(out.scales), _fptr(out.rotations), _fptr(out.opacities),
+                                    _fptr(out.sh)))
+    return out

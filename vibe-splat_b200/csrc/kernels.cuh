@@ -252,5 +252,22 @@ void launch_densify_patch(const DensifyPatch *patches, uint32_t count, float *po
                           float *opacities, void *shRest, uint32_t restPlanes, uint32_t planeStride, uint32_t shBytes,
                           cudaStream_t stream);
 
+// The coarse-to-fine schedule's device work (csrc/schedule.cu).
+// half_size (train.cpp:232-255): out is (width / 2) x (height / 2) RGBA8.
+void launch_half_size(const uint8_t *in, int width, int height, uint8_t *out, cudaStream_t stream);
+// frequency_energy (schedule.cpp:41-75) of an RGBA8 image on the device:
+// partials gets blocks x count sums (summed by the caller) for count <= 8
+// factors; scratch: spectrum_scratch_bytes; sizes up to 4096.
+size_t spectrum_scratch_bytes(int width, int height);
+bool spectrum_supported(int width, int height);
+void launch_frequency_energy(const uint8_t *rgba, int width, int height, const int *factors, int count, void *scratch, double *partials,
+                             int blocks, cudaStream_t stream);
+// neighbour_distances (train.cpp:143-189) of n host points (3 doubles each)
+// on the grid of `cell` from `low` with `dims` cells per axis; out (device)
+// gets the float distances. scratch: neighbour_scratch_bytes(n).
+size_t neighbour_scratch_bytes(uint32_t n);
+int neighbour_distances(const double *points, uint32_t n, double3 low, double cell, int3 dims, void *scratch, float *out, uint32_t *error,
+                        cudaStream_t stream);
+
 } // namespace sb
 

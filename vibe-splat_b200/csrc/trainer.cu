@@ -251,7 +251,7 @@ public:
   void clear_graphs();
   void release_transient(bool keepParameters = false);
   void score_view(const splat_camera *camera, const uint8_t *target, size_t bytes, float share, float pixelWeight,
-                  splat_step_stats *stats);
+                  splat_step_stats *stats, bool deviceTarget = false);
   std::string graph_key(ChainMode mode, bool statistics) const;
   void run(const splat_camera *cameras, const uint8_t *const *targets, const size_t *bytes, int count, ChainMode mode,
            const splat_learning_rates *rates, bool statistics, splat_step_stats *stats, bool deviceTargets = false);
@@ -466,7 +466,7 @@ uint64_t Trainer::entry_bytes(uint64_t entries) const {
 // the marked-pixel count, that count times the view's loss and the edge score
 // added to each Gaussian's statistics, in pixels times pixelWeight.
 void Trainer::score_view(const splat_camera *camera, const uint8_t *targetImage, size_t bytes, float share, float pixelWeight,
-                         splat_step_stats *stats) {
+                         splat_step_stats *stats, bool deviceTarget) {
   if (!(share > 0.0f) || !std::isfinite(share)) throw Failure{SPLAT_ERR_INVALID, "error_share must be above 0"};
   if (!std::isfinite(pixelWeight)) throw Failure{SPLAT_ERR_INVALID, "pixel_weight must be finite"};
   if (blendLists) throw Failure{SPLAT_ERR_UNSUPPORTED, "scoring a view does not run with blend lists"};
@@ -475,7 +475,7 @@ void Trainer::score_view(const splat_camera *camera, const uint8_t *targetImage,
   const size_t sizes[1] = {bytes};
   scoreShare = share;
   try {
-    run(camera, targets, sizes, 1, ChainMode::Statistics, nullptr, true, &own);
+    run(camera, targets, sizes, 1, ChainMode::Statistics, nullptr, true, &own, deviceTarget);
   } catch (...) {
     scoreShare = 0.0f;
     throw;
@@ -1371,6 +1371,24 @@ int splat_trainer_score_view(splat_trainer *trainer, const splat_camera *camera,
   return guarded([&] {
     if (camera == nullptr || target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
     impl_of(trainer)->score_view(camera, target, target_bytes, error_share, pixel_weight, stats);
+  });
+}
+
+int splat_trainer_collect_statistics_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
+                                                   size_t target_bytes, splat_step_stats *stats) {
+  return guarded([&] {
+    if (camera == nullptr || device_target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    const uint8_t *targets[1] = {device_target};
+    const size_t sizes[1] = {target_bytes};
+    impl_of(trainer)->run(camera, targets, sizes, 1, sb::ChainMode::Statistics, nullptr, true, stats, true);
+  });
+}
+
+int splat_trainer_score_view_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
+                                           size_t target_bytes, float error_share, float pixel_weight, splat_step_stats *stats) {
+  return guarded([&] {
+    if (camera == nullptr || device_target == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    impl_of(trainer)->score_view(camera, device_target, target_bytes, error_share, pixel_weight, stats, true);
   });
 }
 
