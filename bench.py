@@ -783,15 +783,65 @@ def our_arm(args) -> None:
         dist.destroy_process_group()
 
 
+def session_workload(args) -> None:
+    """The whole training session (coarse to fine, densification rounds with
+    scored views, the growth cap, the SH ramp) on the headline views: 200k
+    starting points (the bench scene's means with its DC colours), 64 views at
+    1237x822 kept in HBM at full, half and quarter size, 3000 iterations with
+    the reference's default schedule (quarter size until 15 %, half until 35 %,
+    densification every 100 iterations from 151 to 1500, 10 scored views a
+    round). Against the same session at full size throughout. Session
+    iterations/s by the wall clock around the loop, one JSON line."""
+    import torch
+
+    splat = importlib.import_module("vibe-splat_b200")
+    n = 200_000 if args.gaussians == GAUSSIANS else args.gaussians
+    iterations = 3000
+    pos, sc, rot, op, sh = make_scene(n)
+    colors = np.clip((sh.reshape(n, -1)[:, :3] * 0.28209479177387814 + 0.5) * 255.0, 0, 255).astype(np.uint8)
+    cams = [splat.Camera(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in hemisphere_views()]
+    images = list(make_targets(len(cams)))
+    out = {"metric": "session iters/s, coarse to fine", "unit": "iters/s", "higher_is_better": True,
+           "config": {"workload": f"{n} starting points, {len(cams)} views 1237x822 on a radius-5 hemisphere (synthetic), "
+                                  f"{iterations} iterations, SH degree 2, default schedule"}}
+    for name, full in (("coarse_to_fine", False), ("full_resolution", True)):
+        options = splat.SessionOptions(iterations=iterations, full_resolution=full, report_every=0, seed=1)
+        trainer_options = chosen_options(splat)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        session = splat.Session(pos.reshape(-1, 3).astype(np.float64), colors, cams, images, extent=5.5, typical_depth=5.0,
+                                options=options, trainer_options=trainer_options)
+        setup = time.perf_counter() - t0
+        levels = [0, 0, 0]
+        t0 = time.perf_counter()
+        while not session.finished():
+            session.step()
+            levels[session.state().level] += 1
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - t0
+        st = session.state()
+        out[name] = {"iters_per_s": iterations / seconds, "seconds": seconds, "setup_seconds": setup,
+                     "final_gaussians": st.gaussians, "densify_rounds": st.densify_rounds,
+                     "densify_seconds": st.densify_seconds, "iterations_by_level": {"half": levels[0], "quarter": levels[1],
+                                                                                   "full": levels[2]},
+                     "last_loss": st.last_loss}
+        session.close()
+        torch.cuda.empty_cache()
+    out["value"] = out["coarse_to_fine"]["iters_per_s"]
+    out["coarse_to_fine_speedup"] = out["coarse_to_fine"]["iters_per_s"] / out["full_resolution"]["iters_per_s"]
+    print(json.dumps(out))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=30)
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    parser.add_argument("--workload", choices=["step", "memory-adjoint", "batched"], default="step",
+    parser.add_argument("--workload", choices=["step", "memory-adjoint", "batched", "session"], default="step",
                         help="step: the headline one-view training step; memory-adjoint: 6M Gaussians at 3840x2160, "
-                             "recompute vs store-everything backward; batched: 3M Gaussians, 8 uneven views per step")
+                             "recompute vs store-everything backward; batched: 3M Gaussians, 8 uneven views per step; "
+                             "session: a 3000-iteration coarse-to-fine training session from 200k points")
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--no-densify", action="store_true", help="skip the densification timing")
@@ -808,6 +858,8 @@ def main() -> None:
         memory_adjoint_workload(args)
     elif args.workload == "batched":
         batched_workload(args)
+    elif args.workload == "session":
+        session_workload(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:
