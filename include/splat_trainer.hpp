@@ -242,6 +242,48 @@ private:
   std::size_t count_ = 0;
 };
 
+inline splat_session_options default_session_options() {
+  splat_session_options o;
+  splat_session_options_default(&o);
+  return o;
+}
+
+// TrainSession (train.hpp:193-270) over the C ABI: the schedule around a
+// trainer, one iteration per step(); the views live in device memory.
+class Session {
+public:
+  Session(const splat_session_data &data, const splat_session_options &options = default_session_options(),
+          const splat_trainer_options &trainerOptions = default_options())
+      : iterations_(options.iterations) {
+    check(splat_session_create(&data, &options, &trainerOptions, &handle_));
+  }
+  ~Session() { splat_session_destroy(handle_); }
+  Session(const Session &) = delete;
+  Session &operator=(const Session &) = delete;
+
+  splat_step_stats step() {
+    splat_step_stats s{};
+    check(splat_session_step(handle_, &s));
+    return s;
+  }
+  [[nodiscard]] splat_session_state state() const {
+    splat_session_state s{};
+    check(splat_session_get_state(handle_, &s));
+    return s;
+  }
+  [[nodiscard]] bool finished() const { return state().iteration >= iterations_; }
+  // The session's trainer, borrowed: its handle serves the C calls (render, get_cloud).
+  [[nodiscard]] splat_trainer *trainer() const {
+    splat_trainer *t = nullptr;
+    check(splat_session_trainer(handle_, &t));
+    return t;
+  }
+
+private:
+  splat_session *handle_ = nullptr;
+  int iterations_ = 0;
+};
+
 } // namespace splat_b200
 
 // Adapters from the reference's own types, available where its headers come first.

@@ -144,6 +144,8 @@ def test_cpp_face_compiles_links_and_draws_as_the_reference(tmp_path):
                       "  for (int k = 0; k < 5; ++k) std::printf(\"%zu \", rng.pick(1000));\n"
                       "  splat_densify_options d = splat_b200::default_densify_options();\n"
                       "  splat_relocate_options r = splat_b200::default_relocate_options();\n"
+                      "  splat_session_options so = splat_b200::default_session_options();\n"
+                      "  if (so.iterations != 15000) return 1;\n"
                       "  std::printf(\"%g %g\\n\", d.gradient_threshold, r.growth);\n}\n")
     lib = ROOT / "vibe-splat_b200"
     exe = tmp_path / "face"
