@@ -27,14 +27,19 @@ __device__ __forceinline__ float largest_log(const float *scales, uint32_t i) {
   return fmaxf(fmaxf(scales[(size_t)i * 3], scales[(size_t)i * 3 + 1]), scales[(size_t)i * 3 + 2]);
 }
 
+// Every value finite; all loads issued before any test, so that they overlap.
 template <ShStore S> __device__ bool finite_gaussian(const Params &p, uint32_t i) {
   bool ok = isfinite(p.opacities[i]);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) ok = ok && isfinite(p.positions[(size_t)i * 3 + a]) && isfinite(p.scales[(size_t)i * 3 + a]);
+  for (int a = 0; a < 3; ++a) ok &= isfinite(p.positions[(size_t)i * 3 + a]) & isfinite(p.scales[(size_t)i * 3 + a]);
 #pragma unroll
-  for (int a = 0; a < 4; ++a) ok = ok && isfinite(p.rotations[(size_t)i * 4 + a]);
-  for (int k = 0; k < p.shCoeffs && ok; ++k)
-    for (int c = 0; c < 3; ++c) ok = ok && isfinite(sh_coefficient<S>(p, i, k, c));
+  for (int a = 0; a < 4; ++a) ok &= isfinite(p.rotations[(size_t)i * 4 + a]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ok &= isfinite(p.shDc[(size_t)c * p.planeStride + i]);
+  for (int k = 1; k < p.shCoeffs; ++k) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ok &= isfinite(sh_coefficient<S>(p, i, k, c));
+  }
   return ok;
 }
 

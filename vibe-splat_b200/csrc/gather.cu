@@ -11,39 +11,56 @@ namespace sb {
 
 namespace {
 
+// A thread per (new Gaussian, copy): the source index read once, the row's
+// `stride` words copied (STRIDE 0: any stride).
+template <uint32_t STRIDE>
 __global__ void __launch_bounds__(256) k_gather_rows(const int32_t *__restrict__ source, const uint32_t *__restrict__ in,
                                                      uint32_t *__restrict__ out, uint32_t newCount, uint32_t oldCount,
-                                                     uint32_t stride, uint32_t copies) {
-  const size_t total = (size_t)newCount * stride;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total * copies; e += (size_t)gridDim.x * blockDim.x) {
-    const size_t copy = e / total, i = e - copy * total;
-    const size_t g = i / stride, k = i - g * stride;
-    const int32_t from = source[g];
-    out[e] = from < 0 ? 0u : in[copy * (size_t)oldCount * stride + (size_t)from * stride + k];
+                                                     uint32_t runtimeStride) {
+  const uint32_t stride = STRIDE != 0 ? STRIDE : runtimeStride;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x, copy = blockIdx.y;
+  if (g >= newCount) return;
+  const int32_t from = source[g];
+  uint32_t *dst = out + ((size_t)copy * newCount + g) * stride;
+  if (from < 0) {
+    for (uint32_t k = 0; k < stride; ++k) dst[k] = 0u;
+    return;
+  }
+  const uint32_t *src = in + ((size_t)copy * oldCount + (uint32_t)from) * stride;
+  if constexpr (STRIDE == 4) {
+    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
+  } else {
+#pragma unroll
+    for (uint32_t k = 0; k < (STRIDE != 0 ? STRIDE : 1u); ++k) dst[k] = src[k];
+    if constexpr (STRIDE == 0)
+      for (uint32_t k = 1; k < stride; ++k) dst[k] = src[k];
   }
 }
 
-__global__ void __launch_bounds__(256) k_gather_planes(const int32_t *__restrict__ source, const uint32_t *__restrict__ in,
-                                                       uint32_t *__restrict__ out, uint32_t newCount, uint32_t newStride,
-                                                       uint32_t oldStride, uint32_t planes) {
-  const size_t total = (size_t)planes * newStride;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const size_t q = e / newStride, g = e - q * newStride;
-    const int32_t from = g < newCount ? source[g] : -1;
-    out[e] = from < 0 ? 0u : in[q * oldStride + (size_t)from];
+// A thread per new Gaussian (padding included, zeroed): the source index read
+// once, then every plane's element for it, planes in groups of 8 loads in
+// flight.
+template <class T>
+__global__ void __launch_bounds__(256) k_gather_planes(const int32_t *__restrict__ source, const T *__restrict__ in, T *__restrict__ out,
+                                                       uint32_t newCount, uint32_t newStride, uint32_t oldStride, uint32_t planes) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= newStride) return;
+  const int32_t from = g < newCount ? source[g] : -1;
+  T *dst = out + g;
+  if (from < 0) {
+    for (uint32_t q = 0; q < planes; ++q) dst[(size_t)q * newStride] = T(0);
+    return;
   }
-}
-
-// The same for planes of 16-bit elements (SH above degree 0 in BF16 or FP16).
-__global__ void __launch_bounds__(256) k_gather_planes16(const int32_t *__restrict__ source, const uint16_t *__restrict__ in,
-                                                         uint16_t *__restrict__ out, uint32_t newCount, uint32_t newStride,
-                                                         uint32_t oldStride, uint32_t planes) {
-  const size_t total = (size_t)planes * newStride;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const size_t q = e / newStride, g = e - q * newStride;
-    const int32_t from = g < newCount ? source[g] : -1;
-    out[e] = from < 0 ? (uint16_t)0 : in[q * oldStride + (size_t)from];
+  const T *src = in + (uint32_t)from;
+  uint32_t q = 0;
+  for (; q + 8 <= planes; q += 8) {
+    T v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = src[(size_t)(q + j) * oldStride];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dst[(size_t)(q + j) * newStride] = v[j];
   }
+  for (; q < planes; ++q) dst[(size_t)q * newStride] = src[(size_t)q * oldStride];
 }
 
 // Pruning (remove_highest, src/train/densify.cpp:70-90): a key per Gaussian
@@ -84,32 +101,35 @@ __global__ void __launch_bounds__(256) k_survivor_sources(const uint32_t *__rest
   if (i < n && keep[i] != 0u) source[place[i]] = (int32_t)i;
 }
 
-uint32_t gather_blocks(size_t elements) {
-  const size_t blocks = (elements + 255) / 256;
-  return (uint32_t)(blocks < 148 * 16 ? (blocks > 0 ? blocks : 1) : 148 * 16);
-}
-
 } // namespace
 
 void launch_gather_rows(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t oldCount,
                         uint32_t stride, uint32_t copies, cudaStream_t stream) {
-  if (newCount == 0) return;
-  k_gather_rows<<<gather_blocks((size_t)newCount * stride * copies), 256, 0, stream>>>(source, in, out, newCount, oldCount,
-                                                                                       stride, copies);
+  if (newCount == 0 || stride == 0 || copies == 0) return;
+  const dim3 grid(div_up(newCount, 256), copies);
+  // Rows of 4 words move as one 16-byte access when both arrays keep 16-byte rows.
+  const bool aligned = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0u;
+  switch (stride) {
+  case 1: k_gather_rows<1><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 1); break;
+  case 3: k_gather_rows<3><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 3); break;
+  case 4:
+    if (aligned) k_gather_rows<4><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 4);
+    else k_gather_rows<0><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 4);
+    break;
+  default: k_gather_rows<0><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, stride); break;
+  }
 }
 
 void launch_gather_planes(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t newStride,
                           uint32_t oldStride, uint32_t planes, cudaStream_t stream) {
-  if (newCount == 0) return;
-  k_gather_planes<<<gather_blocks((size_t)planes * newStride), 256, 0, stream>>>(source, in, out, newCount, newStride, oldStride,
-                                                                                 planes);
+  if (newStride == 0 || planes == 0) return;
+  k_gather_planes<uint32_t><<<div_up(newStride, 256), 256, 0, stream>>>(source, in, out, newCount, newStride, oldStride, planes);
 }
 
 void launch_gather_planes16(const int32_t *source, const uint16_t *in, uint16_t *out, uint32_t newCount, uint32_t newStride,
                             uint32_t oldStride, uint32_t planes, cudaStream_t stream) {
-  if (newCount == 0 || planes == 0) return;
-  k_gather_planes16<<<gather_blocks((size_t)planes * newStride), 256, 0, stream>>>(source, in, out, newCount, newStride, oldStride,
-                                                                                   planes);
+  if (newStride == 0 || planes == 0) return;
+  k_gather_planes<uint16_t><<<div_up(newStride, 256), 256, 0, stream>>>(source, in, out, newCount, newStride, oldStride, planes);
 }
 
 void launch_prune_keys(int kind, const float *scales, const float *opacities, const float *densifyStats, uint32_t n, uint32_t *keys,
