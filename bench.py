@@ -510,6 +510,24 @@ def batched_workload(args) -> None:
     print(json.dumps(out))
 
 
+def slowest_over_ranks(ms: float, dist, device: str) -> float:
+    """The max over ranks of one rank's device time; every rank calls this at
+    the same point (a collective). Without a process group, the time itself."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_rank: float, slowest_ms: float) -> float:
+    """Replicas: every rank did the same units; the job's rate is all of them
+    over the slowest rank's time."""
+    return world * units_per_rank * 1000.0 / slowest_ms
+
+
 def our_arm(args) -> None:
     import torch
 
@@ -564,12 +582,9 @@ def our_arm(args) -> None:
     if args.sort_form is not None:
         chosen.sort_form = args.sort_form
     trainer, ms, clocks, stats = run_form(chosen, "chosen", tune=args.sort_form is None and not args.no_autotune)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = slowest_over_ranks(ms, dist, "cuda")
     ms_per_step = ms / args.steps
-    value = world * 1000.0 / ms_per_step
+    value = whole_job_rate(world, args.steps, ms)
 
     # e2e: the public step() with host targets (H2D of the target and the stats
     # read-back in the timed region). Each call names the next view's target,
@@ -585,11 +600,8 @@ def our_arm(args) -> None:
     for i in range(args.warmup):
         host_step(i)
     e2e_ms = time_steps(torch, trainer, lambda i: host_step(args.warmup + i), args.steps, stream)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * 1000.0 * args.steps / e2e_ms
+    e2e_ms = slowest_over_ranks(e2e_ms, dist, "cuda")
+    e2e = whole_job_rate(world, args.steps, e2e_ms)
 
     # The FastGS scoring pass (score_view: a statistics pass with the
     # high-error pixels marked, plus the score kernel), host target, plain form.
