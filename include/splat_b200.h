@@ -235,8 +235,9 @@ int splat_trainer_reset_opacity(splat_trainer *trainer, float maximum);
 /* Trainer::apply_changes (trainer.cpp:749-787): replaces the Gaussians by
  * `cloud`; source[i] is the old index whose optimiser state Gaussian i keeps,
  * or -1 for a new one (fresh, zero state); an index past the old count is
- * SPLAT_ERR_INVALID. The state is gathered on the GPU (train_gather.comp);
- * the old trainer's other buffers are freed before the new ones are made. */
+ * SPLAT_ERR_INVALID. The state is gathered on the GPU (train_gather.comp)
+ * into the trainer's spare buffers, which then take the current ones' place;
+ * the densification statistics start anew. */
 int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud, const int32_t *source);
 
 /* Trainer::remove_largest_gaussians, remove_least_contributing_gaussians,

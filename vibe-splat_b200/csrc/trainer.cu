@@ -253,7 +253,6 @@ public:
   void begin(int stage);
   void end(int stage);
   void clear_graphs();
-  void release_transient(bool keepParameters = false);
   void score_view(const splat_camera *camera, const uint8_t *target, size_t bytes, float share, float pixelWeight,
                   splat_step_stats *stats, bool deviceTarget = false);
   std::string graph_key(ChainMode mode, bool statistics) const;
@@ -263,15 +262,50 @@ public:
   void finish_stats(splat_step_stats *stats, int count);
   void fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates);
   void set_sort(bool single, int digits);
-  // Carries the step counter, active SH degree and the sort and layout
-  // choices over to a trainer made for a changed cloud.
-  void inherit(const Trainer &old);
-  // Replaces the Gaussians, in place, by newN gathered from the current ones.
-  void replace_gaussians(const int32_t *paramSource, const int32_t *stateSource, uint32_t newN);
+  // Replaces the Gaussians, in place, by newN gathered from the current ones
+  // (or, with a host cloud, uploaded from it; the state is gathered either way).
+  void replace_gaussians(const int32_t *paramSource, const int32_t *stateSource, uint32_t newN, const splat_cloud *host = nullptr);
   void autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats, splat_autotune_result *out);
 };
 
 // ---------------------------------------------------------------- set-up
+
+// The cloud's parameters into device buffers in the trainer's layout, `to`
+// = positions, scales, rotations, opacities (rows), SH DC and SH rest (planes
+// of `stride` elements, padding zero): DC as FP32, the rest in `store`,
+// rounded to nearest.
+void upload_cloud(const splat_cloud &cloud, int shCoeffs, ShStore store, uint32_t stride, DeviceBuffer *to[6]) {
+  const size_t nn = (size_t)cloud.count, ps = stride;
+  SB_CUDA(cudaMemcpy(to[0]->get(), cloud.positions, nn * 12, cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(to[1]->get(), cloud.scales, nn * 12, cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(to[2]->get(), cloud.rotations, nn * 16, cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(to[3]->get(), cloud.opacities, nn * 4, cudaMemcpyHostToDevice));
+  const int floats = 3 * shCoeffs;
+  std::vector<float> dc(ps * 3, 0.0f);
+  for (size_t i = 0; i < nn; ++i)
+    for (int c = 0; c < 3; ++c) dc[c * ps + i] = cloud.sh[i * floats + c];
+  SB_CUDA(cudaMemcpy(to[4]->get(), dc.data(), ps * 12, cudaMemcpyHostToDevice));
+  const size_t rest = ps * 3 * (size_t)(shCoeffs - 1);
+  if (rest == 0) return;
+  std::vector<float> planes(rest, 0.0f);
+  for (size_t i = 0; i < nn; ++i)
+    for (int j = 3; j < floats; ++j) planes[(size_t)(j - 3) * ps + i] = cloud.sh[i * floats + j];
+  if (store == ShStore::F32) {
+    SB_CUDA(cudaMemcpy(to[5]->get(), planes.data(), rest * 4, cudaMemcpyHostToDevice));
+    return;
+  }
+  std::vector<uint16_t> half(rest);
+  for (size_t k = 0; k < rest; ++k) {
+    if (store == ShStore::BF16) {
+      uint32_t bits;
+      std::memcpy(&bits, &planes[k], 4);
+      half[k] = (uint16_t)((bits + 0x7FFFu + ((bits >> 16) & 1u)) >> 16);
+    } else {
+      half[k] = __half_as_ushort(__float2half_rn(planes[k]));
+    }
+  }
+  SB_CUDA(cudaMemcpy(to[5]->get(), half.data(), rest * 2, cudaMemcpyHostToDevice));
+}
 
 Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options, bool upload) : opt(options) {
   if (cloud.count <= 0) throw Failure{SPLAT_ERR_INVALID, "nothing to train: the cloud is empty"};
@@ -332,38 +366,8 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   if (!upload) {
     for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities}) SB_CUDA(cudaMemset(b->get(), 0, b->bytes()));
   } else {
-  SB_CUDA(cudaMemcpy(positions.get(), cloud.positions, nn * 12, cudaMemcpyHostToDevice));
-  SB_CUDA(cudaMemcpy(scales.get(), cloud.scales, nn * 12, cudaMemcpyHostToDevice));
-  SB_CUDA(cudaMemcpy(rotations.get(), cloud.rotations, nn * 16, cudaMemcpyHostToDevice));
-  SB_CUDA(cudaMemcpy(opacities.get(), cloud.opacities, nn * 4, cudaMemcpyHostToDevice));
-  // SH to planes: DC as FP32, the rest in the chosen storage, rounded to nearest.
-  {
-    const int floats = 3 * shCoeffs;
-    std::vector<float> dc(ps * 3, 0.0f);
-    for (size_t i = 0; i < nn; ++i)
-      for (int c = 0; c < 3; ++c) dc[c * ps + i] = cloud.sh[i * floats + c];
-    SB_CUDA(cudaMemcpy(shDc.get(), dc.data(), ps * 12, cudaMemcpyHostToDevice));
-    if (rest > 0) {
-      std::vector<float> planes(rest, 0.0f);
-      for (size_t i = 0; i < nn; ++i)
-        for (int j = 3; j < floats; ++j) planes[(size_t)(j - 3) * ps + i] = cloud.sh[i * floats + j];
-      if (shStore == ShStore::F32) {
-        SB_CUDA(cudaMemcpy(shRest.get(), planes.data(), rest * 4, cudaMemcpyHostToDevice));
-      } else {
-        std::vector<uint16_t> half(rest);
-        for (size_t k = 0; k < rest; ++k) {
-          if (shStore == ShStore::BF16) {
-            uint32_t bits;
-            std::memcpy(&bits, &planes[k], 4);
-            half[k] = (uint16_t)((bits + 0x7FFFu + ((bits >> 16) & 1u)) >> 16);
-          } else {
-            half[k] = __half_as_ushort(__float2half_rn(planes[k]));
-          }
-        }
-        SB_CUDA(cudaMemcpy(shRest.get(), half.data(), rest * 2, cudaMemcpyHostToDevice));
-      }
-    }
-  }
+    DeviceBuffer *to[6] = {&positions, &scales, &rotations, &opacities, &shDc, &shRest};
+    upload_cloud(cloud, shCoeffs, shStore, planeStride, to);
   }
   const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, ps * 3 * shCoeffs};
   for (int g = 0; g < 5; ++g) {
@@ -399,24 +403,6 @@ Trainer::~Trainer() {
   if (copied != nullptr) cudaEventDestroy(copied);
   if (consumed != nullptr) cudaEventDestroy(consumed);
   if (stream != nullptr) cudaStreamDestroy(stream);
-}
-
-// Frees every device buffer except the optimiser state (densification keeps
-// only that from the old Gaussians).
-void Trainer::release_transient(bool keepParameters) {
-  clear_graphs();
-  SB_CUDA(cudaStreamSynchronize(copyStream)); // a prefetch may still be landing in targetNext
-  if (!keepParameters)
-    for (DeviceBuffer *b : {&positions, &scales, &rotations, &opacities, &shDc, &shRest}) b->release();
-  for (DeviceBuffer *b : {&grads[0], &grads[1], &grads[2], &grads[3],
-                          &grads[4], &densifyStats, &splats, &reach, &depthKeys, &values, &tmpKeys, &tmpValues, &offsets, &raw,
-                          &shGrad, &entryKeys, &entryValues, &tmpEntryKeys, &tmpEntryValues, &image, &stops, &adjoint, &fields,
-                          &target, &targetNext, &ranges, &partials, &listCounts, &listOffsets, &listPool, &listScratch,
-                          &sortScratchDepth, &sortScratchEntries, &scanScratch, &scoreEdge, &scoreMax})
-    b->release();
-  prefetched = nullptr;
-  entryCapacity = 0;
-  viewSlots = 0;
 }
 
 void Trainer::clear_graphs() {
@@ -1031,25 +1017,15 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
 
 // Switches the tile sort's form and digit width; the entry buffers (whose key
 // width may change) and the captured graphs are rebuilt on the next step.
-void Trainer::inherit(const Trainer &old) {
-  adamStep = old.adamStep;
-  activeDegree = old.activeDegree;
-  oneSort = old.oneSort;
-  digitBits = old.digitBits;
-  forwardPixels = old.forwardPixels;
-  backwardPixels = old.backwardPixels;
-  timing = old.timing;
-}
-
-// Trainer::apply_changes (trainer.cpp:749-787) for a cloud edited on the
-// device: the parameters are gathered through paramSource, the optimiser
-// state through stateSource (-1: fresh, zero), into the spare buffers, which
+// Trainer::apply_changes (trainer.cpp:749-787): the parameters are gathered
+// through paramSource (or uploaded from a host cloud), the optimiser state
+// through stateSource (-1: fresh, zero), into the spare buffers, which
 // then take the current ones' place; the densification statistics start at
 // zero and the buffers sized by the count follow it at the next step. The
 // views' buffers, the tile entries and the targets stay. With a memory
 // budget the old buffers are freed at once; without one they are kept as the
 // next edit's spares.
-void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *stateSource, uint32_t newN) {
+void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *stateSource, uint32_t newN, const splat_cloud *host) {
   SB_CUDA(cudaStreamSynchronize(stream));
   SB_CUDA(cudaStreamSynchronize(copyStream));
   const uint32_t oldN = n, oldStride = planeStride;
@@ -1065,15 +1041,20 @@ void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *state
   for (int g = 0; g < 5; ++g) grow(spareState[g], stateBytes[g]);
   const uint32_t strides[4] = {3, 3, 4, 1};
   DeviceBuffer *params[4] = {&positions, &scales, &rotations, &opacities};
-  for (int g = 0; g < 4; ++g)
-    launch_gather_rows(paramSource, params[g]->get<uint32_t>(), spareParams[g].get<uint32_t>(), newN, oldN, strides[g], 1u, stream);
-  launch_gather_planes(paramSource, shDc.get<uint32_t>(), spareParams[4].get<uint32_t>(), newN, newStride, oldStride, 3u, stream);
-  if (shStore == ShStore::F32)
-    launch_gather_planes(paramSource, shRest.get<uint32_t>(), spareParams[5].get<uint32_t>(), newN, newStride, oldStride,
-                         (uint32_t)restPlanes, stream);
-  else
-    launch_gather_planes16(paramSource, shRest.get<uint16_t>(), spareParams[5].get<uint16_t>(), newN, newStride, oldStride,
+  if (host != nullptr) {
+    DeviceBuffer *to[6] = {&spareParams[0], &spareParams[1], &spareParams[2], &spareParams[3], &spareParams[4], &spareParams[5]};
+    upload_cloud(*host, shCoeffs, shStore, newStride, to);
+  } else {
+    for (int g = 0; g < 4; ++g)
+      launch_gather_rows(paramSource, params[g]->get<uint32_t>(), spareParams[g].get<uint32_t>(), newN, oldN, strides[g], 1u, stream);
+    launch_gather_planes(paramSource, shDc.get<uint32_t>(), spareParams[4].get<uint32_t>(), newN, newStride, oldStride, 3u, stream);
+    if (shStore == ShStore::F32)
+      launch_gather_planes(paramSource, shRest.get<uint32_t>(), spareParams[5].get<uint32_t>(), newN, newStride, oldStride,
                            (uint32_t)restPlanes, stream);
+    else
+      launch_gather_planes16(paramSource, shRest.get<uint16_t>(), spareParams[5].get<uint16_t>(), newN, newStride, oldStride,
+                             (uint32_t)restPlanes, stream);
+  }
   for (int g = 0; g < 4; ++g)
     launch_gather_rows(stateSource, state[g].get<uint32_t>(), spareState[g].get<uint32_t>(), newN, oldN, strides[g],
                        (uint32_t)copies, stream);
@@ -1571,37 +1552,20 @@ int splat_trainer_apply_changes(splat_trainer *trainer, const splat_cloud *cloud
     if (cloud == nullptr || source == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
     if (cloud->count <= 0) throw Failure{SPLAT_ERR_INVALID, "densification removed every Gaussian"};
     if (cloud->sh_degree != t->shDegree) throw Failure{SPLAT_ERR_INVALID, "the SH degree cannot change"};
+    if (cloud->positions == nullptr || cloud->scales == nullptr || cloud->rotations == nullptr || cloud->opacities == nullptr ||
+        cloud->sh == nullptr)
+      throw Failure{SPLAT_ERR_INVALID, "GaussianCloud: inconsistent array sizes"};
     const size_t oldN = t->n, newN = (size_t)cloud->count;
     for (size_t i = 0; i < newN; ++i)
       if (source[i] >= (int64_t)oldN) throw Failure{SPLAT_ERR_INVALID, "a source index is past the old Gaussians"};
-    SB_CUDA(cudaStreamSynchronize(t->stream));
-    // The survivors keep their optimiser state, gathered on the GPU through the
-    // source table (train_gather.comp) so that the moments never cross to the
-    // host. Everything else the old trainer holds is freed first, for the
-    // sake of the budget; the new trainer starts from the new cloud.
-    t->release_transient();
-    const splat_trainer_options o = t->opt;
-    Trainer *fresh = new Trainer(*cloud, o);
-    fresh->inherit(*t);
-    try {
-      sb::DeviceBuffer table;
-      table.ensure(newN * sizeof(int32_t));
-      SB_CUDA(cudaMemcpyAsync(table.get(), source, newN * sizeof(int32_t), cudaMemcpyHostToDevice, fresh->stream));
-      const uint32_t copies = t->stateStore == sb::StateStore::F32 ? 2u : 1u;
-      const uint32_t strides[4] = {3, 3, 4, 1};
-      for (int g = 0; g < 4; ++g)
-        sb::launch_gather_rows(table.get<int32_t>(), t->state[g].get<uint32_t>(), fresh->state[g].get<uint32_t>(), (uint32_t)newN,
-                               (uint32_t)oldN, strides[g], copies, fresh->stream);
-      sb::launch_gather_planes(table.get<int32_t>(), t->state[4].get<uint32_t>(), fresh->state[4].get<uint32_t>(), (uint32_t)newN,
-                               fresh->planeStride, t->planeStride, 3u * (uint32_t)t->shCoeffs * copies, fresh->stream);
-      SB_CUDA(cudaGetLastError());
-      SB_CUDA(cudaStreamSynchronize(fresh->stream));
-    } catch (...) {
-      delete fresh;
-      throw;
-    }
-    delete t;
-    trainer->impl = fresh;
+    // The new cloud is uploaded into the spare buffers and the survivors'
+    // optimiser state gathered on the GPU through the source table
+    // (train_gather.comp), so that the moments never cross to the host; the
+    // densification statistics start anew.
+    sb::DeviceBuffer table;
+    table.ensure(newN * sizeof(int32_t));
+    SB_CUDA(cudaMemcpy(table.get(), source, newN * sizeof(int32_t), cudaMemcpyHostToDevice));
+    t->replace_gaussians(nullptr, table.get<int32_t>(), (uint32_t)newN, cloud);
   });
 }
 
