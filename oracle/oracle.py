@@ -327,7 +327,8 @@ def ref_view_order(seed: int, views: int, steps: int) -> list:
 
 
 def half_size(rgba: np.ndarray, width: int, height: int) -> np.ndarray:
-    """half_size (train.cpp:232-255) restated: the rounded mean of each 2x2 block, per channel."""
+    """half_size (train.cpp:232-255) restated: the rounded mean of each 2x2 block, per channel.
+    Pinned on a hand-computed case (train.cpp does not compile on its own)."""
     w, h = width // 2, height // 2
     img = np.asarray(rgba, np.uint32).reshape(height, width, 4)[: 2 * h, : 2 * w]
     s = img[0::2, 0::2] + img[0::2, 1::2] + img[1::2, 0::2] + img[1::2, 1::2]
@@ -338,7 +339,10 @@ def neighbour_distances(points: np.ndarray) -> np.ndarray:
     """neighbour_distances (train.cpp:143-189) restated for small clouds: on the
     reference's grid, the mean distance to the 3 nearest other points within
     the cube of cells of radius r, for the first r of 1..4 that holds 3, else
-    the cell size; float32 of max(mean, 1e-7)."""
+    the cell size; float32 of max(mean, 1e-7). Parity unpinned against the
+    reference's own code: train.cpp does not compile without its Vulkan tree,
+    so this restatement is pinned only on cases whose answer is known (a
+    lattice, tests/test_session.py)."""
     p = np.asarray(points, np.float64).reshape(-1, 3)
     n = p.shape[0]
     low, high = p.min(axis=0), p.max(axis=0)
