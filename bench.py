@@ -18,7 +18,12 @@ on one view, views in turn. Reported:
   plain  the plain FP32 form (FP32 SH and Adam state, the reference's
          two-sort order, host read-back of the entry count, no CUDA graph,
          deterministic exp/log) on the same views, for the 2x target;
-  roofline, cpu_baseline, clocks, gpu_launches.
+  roofline, cpu_baseline, clocks, gpu_launches;
+  score_view_ms, densify (densification rounds on the GPU, first and later,
+         beside the reference's densify_cloud on the same statistics;
+         relocation rounds), prune: the cloud edits after the timed steps.
+--workload memory-adjoint, batched and session run the other measured
+shapes (each prints its own JSON line).
 With --gpus N > 1 every rank trains its own replica (the path does not shard:
 replicas only), and value is the sum over ranks.
 --impl reference times the reference's own FP64 CPU twin (src/train/
