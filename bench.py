@@ -807,8 +807,10 @@ def session_workload(args) -> None:
     1237x822 kept in HBM at full, half and quarter size, 3000 iterations with
     the reference's default schedule (quarter size until 15 %, half until 35 %,
     densification every 100 iterations from 151 to 1500, 10 scored views a
-    round). Against the same session at full size throughout. Session
-    iterations/s by the wall clock around the loop, one JSON line."""
+    round). Against the same session at full size throughout, and with four
+    views per batched step (a quarter of the iterations, the same views).
+    Session iterations/s and views/s by the wall clock around the loop, one
+    JSON line."""
     import torch
 
     splat = importlib.import_module("vibe-splat_b200")
@@ -821,8 +823,9 @@ def session_workload(args) -> None:
     out = {"metric": "session iters/s, coarse to fine", "unit": "iters/s", "higher_is_better": True,
            "config": {"workload": f"{n} starting points, {len(cams)} views 1237x822 on a radius-5 hemisphere (synthetic), "
                                   f"{iterations} iterations, SH degree 2, default schedule"}}
-    for name, full in (("coarse_to_fine", False), ("full_resolution", True)):
-        options = splat.SessionOptions(iterations=iterations, full_resolution=full, report_every=0, seed=1)
+    for name, full, batch in (("coarse_to_fine", False, 1), ("full_resolution", True, 1), ("coarse_to_fine_4_views", False, 4)):
+        options = splat.SessionOptions(iterations=iterations if batch == 1 else iterations // batch, full_resolution=full,
+                                       report_every=0, seed=1, views_per_step=batch)
         trainer_options = chosen_options(splat)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -837,7 +840,9 @@ def session_workload(args) -> None:
         torch.cuda.synchronize()
         seconds = time.perf_counter() - t0
         st = session.state()
-        out[name] = {"iters_per_s": iterations / seconds, "seconds": seconds, "setup_seconds": setup,
+        steps = options.iterations
+        out[name] = {"iters_per_s": steps / seconds, "views_per_s": steps * batch / seconds, "seconds": seconds,
+                     "setup_seconds": setup,
                      "final_gaussians": st.gaussians, "densify_rounds": st.densify_rounds,
                      "densify_seconds": st.densify_seconds, "iterations_by_level": {"half": levels[0], "quarter": levels[1],
                                                                                    "full": levels[2]},

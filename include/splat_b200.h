@@ -208,6 +208,9 @@ int splat_trainer_stream(splat_trainer *trainer, void **stream);
  * step is taken. New in this library; stats receives one entry per view. */
 int splat_trainer_step_batch(splat_trainer *trainer, const splat_camera *cameras, const uint8_t *const *targets,
                              int32_t views, const splat_learning_rates *rates, splat_step_stats *stats);
+/* The same with the targets in device memory. */
+int splat_trainer_step_batch_device_targets(splat_trainer *trainer, const splat_camera *cameras, const uint8_t *const *device_targets,
+                                            int32_t views, const splat_learning_rates *rates, splat_step_stats *stats);
 /* Trainer::prefetch_target (trainer.hpp:129). */
 int splat_trainer_prefetch_target(splat_trainer *trainer, const uint8_t *target, size_t target_bytes);
 
@@ -364,6 +367,8 @@ typedef struct splat_session_options {
   double max_growth;          /* -1: 4 per 7000 iterations */
   uint64_t max_gaussians;     /* 0: as the memory budget allows */
   double coarse_until[2];     /* 0.35, 0.15 */
+  int32_t views_per_step;     /* 1: the reference's one view per iteration; 2..8: that many views of the
+                                 order in one batched step (64-bit tile|depth keys), one Adam step for all */
 } splat_session_options;
 void splat_session_options_default(splat_session_options *options);
 
@@ -389,7 +394,8 @@ typedef struct splat_session_data {
 typedef struct splat_session_state {
   int32_t iteration;
   int32_t level;
-  int32_t view;
+  int32_t view;               /* the last view the step trained on */
+  int32_t views_in_step;
   float position_rate;
   uint64_t gaussians;
   float first_loss, last_loss;

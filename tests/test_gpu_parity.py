@@ -750,3 +750,21 @@ def test_settings_without_a_kernel_accept_only_neutral_values(splat, oracle):
                  trainer.enable_second_order, trainer.update_curvature):
         with pytest.raises(splat.UnsupportedOption):
             call()
+
+
+def test_graph_follows_the_active_sh_degree(splat, oracle):
+    # A captured step serves one active SH degree: after set_active_sh_degree
+    # the graph form recaptures, and stays bit for bit with the form that
+    # launches every kernel itself (fixed-point sums, so both are exact).
+    view = oracle.train_camera(96, 72)
+    target = oracle.smooth_target(96, 72, 8)
+    cloud = oracle.random_cloud(3000, 3, 41)
+    clouds = []
+    for graph in (True, False):
+        t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(use_graph=graph, force_fixed_point=True, sh_storage=splat.SH_BF16))
+        for degree in (0, 0, 1, 1, 3, 2):
+            t.set_active_sh_degree(degree)
+            assert math.isfinite(t.step(to_camera(view), target, splat.LearningRates()).loss)
+        clouds.append(t.cloud())
+    for name in ("positions", "scales", "rotations", "opacities", "sh"):
+        np.testing.assert_array_equal(getattr(clouds[0], name), getattr(clouds[1], name), name)

@@ -220,3 +220,25 @@ def test_adaptive_session_sizes_come_from_the_spectra(splat, O):
         session.step()
     assert session.state().densify_rounds > 0
     assert np.isfinite(session.trainer().render(to_camera(O.train_camera(96, 64)))).all()
+
+
+@pytest.mark.gpu
+def test_multi_view_session_takes_the_reference_order_in_groups(splat, O):
+    # views_per_step = 4: each step trains on the next four views of the
+    # order TrainSession's shuffle gives, in one batched step (64-bit
+    # tile|depth keys), at the schedule's size for that iteration.
+    pts, colors, cams, images = _small_scene(O)
+    iterations, batch = 120, 4
+    options = splat.SessionOptions(iterations=iterations, seed=9, views_per_step=batch, densify_interval=40, score_views=2,
+                                   report_every=0, dense_fraction=0.01)
+    session = splat.Session(pts, colors, cams, images, extent=4.0, typical_depth=4.5, options=options)
+    order = O.ref_view_order(9, len(cams), iterations * batch)
+    for it in range(1, iterations + 1):
+        stats = session.step()
+        st = session.state()
+        assert math.isfinite(stats.loss)
+        assert st.views_in_step == batch and st.view == order[it * batch - 1], f"iteration {it}"
+        progress = (it - 1) / (iterations - 1)
+        assert st.level == (1 if progress < 0.15 else 0 if progress < 0.35 else 2)
+    assert session.state().densify_rounds == len([i for i in range(min(500, iterations // 20 + 1), iterations // 2 + 1)
+                                                  if i % 40 == 0])

@@ -214,7 +214,8 @@ class _SessionOptions(ctypes.Structure):
                 ("densify_interval", ctypes.c_int32), ("score_views", ctypes.c_int32), ("score_min_pixels", ctypes.c_float),
                 ("explore", ctypes.c_int32), ("significance_prune", ctypes.c_int32), ("edge_split", ctypes.c_int32),
                 ("threshold_rise", ctypes.c_double), ("prune_share", ctypes.c_double), ("recovery_prune", ctypes.c_double),
-                ("max_growth", ctypes.c_double), ("max_gaussians", ctypes.c_uint64), ("coarse_until", ctypes.c_double * 2)]
+                ("max_growth", ctypes.c_double), ("max_gaussians", ctypes.c_uint64), ("coarse_until", ctypes.c_double * 2),
+                ("views_per_step", ctypes.c_int32)]
 
 
 class _SessionData(ctypes.Structure):
@@ -225,7 +226,7 @@ class _SessionData(ctypes.Structure):
 
 class _SessionState(ctypes.Structure):
     _fields_ = [("iteration", ctypes.c_int32), ("level", ctypes.c_int32), ("view", ctypes.c_int32),
-                ("position_rate", ctypes.c_float), ("gaussians", ctypes.c_uint64), ("first_loss", ctypes.c_float),
+                ("views_in_step", ctypes.c_int32), ("position_rate", ctypes.c_float), ("gaussians", ctypes.c_uint64), ("first_loss", ctypes.c_float),
                 ("last_loss", ctypes.c_float), ("report_iteration", ctypes.c_int32), ("probe_psnr", ctypes.c_double),
                 ("mean_loss", ctypes.c_double), ("densify_rounds", ctypes.c_int32), ("densify_seconds", ctypes.c_double),
                 ("last_densify", _DensifyResult), ("held_back_total", ctypes.c_uint64), ("pruned_total", ctypes.c_uint64),
@@ -247,6 +248,8 @@ _lib.splat_growth_limit.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.POI
                                     ctypes.POINTER(ctypes.c_double)]
 _lib.splat_half_size.argtypes = [_P, ctypes.c_int32, ctypes.c_int32, _P]
 _lib.splat_initial_cloud.argtypes = [ctypes.POINTER(ctypes.c_double), _P, ctypes.c_uint64, ctypes.c_int32, _FP, _FP, _FP, _FP, _FP]
+_lib.splat_trainer_step_batch_device_targets.argtypes = [_P, ctypes.POINTER(_Camera), ctypes.POINTER(_P), ctypes.c_int32,
+                                                         ctypes.POINTER(_Rates), ctypes.POINTER(_Stats)]
 _lib.splat_trainer_collect_statistics_device_target.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t,
                                                                 ctypes.POINTER(_Stats)]
 _lib.splat_trainer_score_view_device_target.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_float,
@@ -967,6 +970,7 @@ class SessionOptions:
     max_growth: float = -1.0
     max_gaussians: int = 0
     coarse_until: tuple = (0.35, 0.15)
+    views_per_step: int = 1
 
     def _c(self) -> _SessionOptions:
         o = _SessionOptions()

@@ -32,6 +32,7 @@ enum DeviceError : uint32_t {
   kErrLookbackTimeout = 1u,   // a decoupled look-back gave up waiting on a predecessor
   kErrEntryOverflow = 2u,     // more tile entries than the entry pool holds
   kErrBadIndex = 4u,          // an index read from memory was out of range
+  kErrShStage = 8u,           // a view's SH coefficients in use exceed the staging its launch was given
 };
 
 // One view, as the kernels need it (src/train/trainer.cpp:29-36 GpuCamera,

@@ -47,7 +47,7 @@ template <ShStore S>
 __global__ void __launch_bounds__(kProjectThreads, 3) k_preprocess(Params p, const ViewSet *__restrict__ viewsPtr,
                                                                 Splat *__restrict__ splats, float *__restrict__ reachOut,
                                                                 uint32_t *__restrict__ depthKeys, uint32_t *__restrict__ values,
-                                                                uint32_t *error) {
+                                                                uint32_t *error, int stageCoeffs) {
   chain_enter();
   extern __shared__ __align__(128) unsigned char s_stage[];
   __shared__ __align__(8) uint64_t s_bar;
@@ -55,6 +55,17 @@ __global__ void __launch_bounds__(kProjectThreads, 3) k_preprocess(Params p, con
   const uint32_t tid = threadIdx.x, i0 = blockIdx.x * kProjectThreads, i = i0 + tid;
   const int v = blockIdx.y;
   const ViewParams &cam = views.v[v];
+  // The stage holds stageCoeffs coefficients (the launch's shared memory); a
+  // view using more is refused rather than staged past its end: its
+  // Gaussians are written as culled, and the error word tells the host.
+  if (cam.activeCoeffs > stageCoeffs) {
+    if (tid == 0 && error != nullptr) atomicOr(error, kErrShStage);
+    if (i < p.n) {
+      depthKeys[(size_t)v * p.n + i] = kInvisible;
+      if (values != nullptr) values[(size_t)v * p.n + i] = i;
+    }
+    return;
+  }
   const int coeffs = cam.activeCoeffs;
   if (tid == 0) {
     bulk_barrier_init(&s_bar, 1);
@@ -201,7 +212,8 @@ void launch_preprocess_s(const Params &p, const ViewSet &views, const ViewSet *d
     configured = project_stage_bytes<S>(kMaxShCoeffs);
   }
   const dim3 grid(div_up(p.n, kProjectThreads), views.count);
-  launch_chained(k_preprocess<S>, grid, dim3(kProjectThreads), smem, stream, p, dViews, splats, reach, depthKeys, values, error);
+  launch_chained(k_preprocess<S>, grid, dim3(kProjectThreads), smem, stream, p, dViews, splats, reach, depthKeys, values, error,
+                 coeffs);
 }
 
 } // namespace

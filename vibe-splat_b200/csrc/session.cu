@@ -304,12 +304,19 @@ struct splat_session {
 void splat_session::step(splat_step_stats *out) {
   if (iteration >= options.iterations) throw SessionFailure{SPLAT_ERR_STATE, "training has already finished"};
   const int it = ++iteration;
-  refill_order();
-  lastView = order.back();
-  const size_t viewIndex = lastView;
   const size_t level = coarse_level(it);
-  order.pop_back();
-  refill_order(); // the next view's draw, as the reference makes it for its prefetch
+  // The views of this step, drawn one after another as the reference draws
+  // one per iteration (refill, take the back, refill for the next).
+  const int batch = std::clamp(options.views_per_step, 1, 8);
+  size_t picked[8];
+  for (int b = 0; b < batch; ++b) {
+    refill_order();
+    picked[b] = order.back();
+    order.pop_back();
+    refill_order(); // the next view's draw, as the reference makes it for its prefetch
+  }
+  lastView = picked[batch - 1];
+  const size_t viewIndex = lastView;
 
   const double progress = static_cast<double>(it - 1) / std::max(options.iterations - 1, 1);
   const double held = options.adaptive_schedule != 0 && options.full_resolution == 0 ? coarseUntil[0] : 0.0;
@@ -318,10 +325,26 @@ void splat_session::step(splat_step_stats *out) {
   ok(splat_trainer_set_active_sh_degree(trainer, (it - 1) / shInterval));
   splat_step_stats stats{};
   const splat_camera &camera = cameras[level][viewIndex];
-  fitting([&] {
-    return splat_trainer_step_device_target(trainer, &camera, image_of(level, viewIndex), pixels_of(level, viewIndex) * 4, &rates,
-                                            &stats);
-  });
+  if (batch == 1) {
+    fitting([&] {
+      return splat_trainer_step_device_target(trainer, &camera, image_of(level, viewIndex), pixels_of(level, viewIndex) * 4, &rates,
+                                              &stats);
+    });
+  } else {
+    splat_camera group[8];
+    const uint8_t *targets[8];
+    splat_step_stats each[8];
+    for (int b = 0; b < batch; ++b) {
+      group[b] = cameras[level][picked[b]];
+      targets[b] = image_of(level, picked[b]);
+    }
+    fitting([&] { return splat_trainer_step_batch_device_targets(trainer, group, targets, batch, &rates, each); });
+    stats = each[0];
+    float loss = 0.f;
+    for (int b = 0; b < batch; ++b) loss += each[b].loss;
+    stats.loss = loss / (float)batch;
+  }
+  state.views_in_step = batch;
   if (!std::isfinite(stats.loss))
     throw SessionFailure{SPLAT_ERR_NONFINITE, "the loss became " + std::to_string(stats.loss) + " at iteration " + std::to_string(it)};
   if (it == 1) state.first_loss = stats.loss;
@@ -490,6 +513,7 @@ void splat_session_options_default(splat_session_options *o) {
   o->max_gaussians = 0;
   o->coarse_until[0] = 0.35;
   o->coarse_until[1] = 0.15;
+  o->views_per_step = 1;
 }
 
 int splat_session_create(const splat_session_data *data, const splat_session_options *options,
@@ -560,6 +584,9 @@ int splat_session_create(const splat_session_data *data, const splat_session_opt
 
       // The trainer (train.cpp:486-506), from the starting points.
       s->trainerOptions.selective_adam = options->full_adam != 0 ? 0 : 1;
+      if (options->views_per_step < 1 || options->views_per_step > 8)
+        throw SessionFailure{SPLAT_ERR_INVALID, "views_per_step must be 1..8"};
+      if (options->views_per_step > 1) s->trainerOptions.sort_form = SPLAT_SORT_TILE_DEPTH_64; // several views share one sort
       s->trainerOptions.near_plane = static_cast<float>(s->typicalDepth * 0.01);
       const HostCloud c = initial_cloud(data->points, data->colors, data->point_count, options->sh_degree, s->stream);
       splat_cloud cloud{(int32_t)data->point_count, options->sh_degree, c.positions.data(), c.scales.data(), c.rotations.data(),

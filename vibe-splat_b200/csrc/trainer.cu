@@ -889,7 +889,10 @@ void Trainer::fill_chain_args(ChainMode mode, bool statistics, const splat_learn
 }
 
 std::string Trainer::graph_key(ChainMode mode, bool statistics) const {
-  std::string key = std::to_string((int)mode) + (statistics ? "s" : "-") + std::to_string(views.count);
+  // The active SH degree sets the projection's staging (its shared memory), so
+  // a graph serves one degree only.
+  std::string key = std::to_string((int)mode) + (statistics ? "s" : "-") + std::to_string(views.count) + "d" +
+                    std::to_string(activeDegree);
   for (int k = 0; k < views.count; ++k) key += ":" + std::to_string(views.v[k].width) + "x" + std::to_string(views.v[k].height);
   return key;
 }
@@ -1435,6 +1438,18 @@ int splat_trainer_step_batch(splat_trainer *trainer, const splat_camera *cameras
     size_t sizes[sb::kMaxViews];
     for (int k = 0; k < views; ++k) sizes[k] = (size_t)cameras[k].width * cameras[k].height * 4;
     impl_of(trainer)->run(cameras, targets, sizes, views, sb::ChainMode::Step, rates, true, stats);
+  });
+}
+
+int splat_trainer_step_batch_device_targets(splat_trainer *trainer, const splat_camera *cameras, const uint8_t *const *device_targets,
+                                            int32_t views, const splat_learning_rates *rates, splat_step_stats *stats) {
+  return guarded([&] {
+    if (cameras == nullptr || device_targets == nullptr || rates == nullptr) throw Failure{SPLAT_ERR_INVALID, "null argument"};
+    if (rates->trust_region != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
+    if (views < 1 || views > sb::kMaxViews) throw Failure{SPLAT_ERR_INVALID, "between 1 and 8 views per step"};
+    size_t sizes[sb::kMaxViews];
+    for (int k = 0; k < views; ++k) sizes[k] = (size_t)cameras[k].width * cameras[k].height * 4;
+    impl_of(trainer)->run(cameras, device_targets, sizes, views, sb::ChainMode::Step, rates, true, stats, true);
   });
 }
 
