@@ -628,7 +628,21 @@ void Trainer::prefetch(const uint8_t *next, size_t bytes) {
   SB_CUDA(cudaEventSynchronize(copied));
   SB_CUDA(cudaStreamWaitEvent(copyStream, consumed, 0));
   stagingNext.ensure(bytes);
-  std::memcpy(stagingNext.get(), next, bytes);
+  // The host copy runs while the GPU works on this step; split over four
+  // threads it stays inside the step on a slow host.
+  uint8_t *dst = stagingNext.get<uint8_t>();
+  if (bytes >= (1u << 20)) {
+    const size_t quarter = (bytes / 4 + 63) & ~size_t{63};
+    std::thread helpers[3];
+    for (int k = 1; k < 4; ++k) {
+      const size_t from = std::min(bytes, (size_t)k * quarter), to = std::min(bytes, (size_t)(k + 1) * quarter);
+      helpers[k - 1] = std::thread([=] { std::memcpy(dst + from, next + from, to - from); });
+    }
+    std::memcpy(dst, next, std::min(bytes, quarter));
+    for (std::thread &h : helpers) h.join();
+  } else {
+    std::memcpy(dst, next, bytes);
+  }
   targetNext.ensure(bytes);
   SB_CUDA(cudaMemcpyAsync(targetNext.get(), stagingNext.get(), bytes, cudaMemcpyHostToDevice, copyStream));
   SB_CUDA(cudaEventRecord(copied, copyStream));
