@@ -768,3 +768,31 @@ def test_graph_follows_the_active_sh_degree(splat, oracle):
         clouds.append(t.cloud())
     for name in ("positions", "scales", "rotations", "opacities", "sh"):
         np.testing.assert_array_equal(getattr(clouds[0], name), getattr(clouds[1], name), name)
+
+
+def test_device_target_entry_points_match_the_host_ones(splat, oracle):
+    # collect_statistics, score_view and step_batch with the targets already
+    # on the device give what the host-target calls give (fixed-point sums,
+    # so bit for bit).
+    import torch
+
+    views = [oracle.train_camera(80, 64), oracle.train_camera(96, 72)]
+    targets = [oracle.smooth_target(80, 64, 2), oracle.smooth_target(96, 72, 3)]
+    device = [torch.from_numpy(t).cuda() for t in targets]
+    cloud = oracle.random_cloud(2000, 1, 17)
+    opts = splat.TrainerOptions(force_fixed_point=True, sort_form=splat.SORT_TILE_DEPTH_64)
+    out = []
+    for on_device in (False, True):
+        t = splat.Trainer(to_cloud(cloud), opts)
+        if on_device:
+            t.collect_statistics_device_target(to_camera(views[0]), device[0].data_ptr())
+            t.score_view_device_target(to_camera(views[1]), device[1].data_ptr(), 0.5)
+            t.step_batch_device_targets([to_camera(v) for v in views], [d.data_ptr() for d in device], splat.LearningRates())
+        else:
+            t.collect_statistics(to_camera(views[0]), targets[0])
+            t.score_view(to_camera(views[1]), targets[1], 0.5)
+            t.step_batch([to_camera(v) for v in views], targets, splat.LearningRates())
+        out.append((t.densify_stats_raw().copy(), t.cloud()))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for name in ("positions", "scales", "opacities", "sh"):
+        np.testing.assert_array_equal(getattr(out[0][1], name), getattr(out[1][1], name), name)

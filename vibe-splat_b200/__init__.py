@@ -715,6 +715,31 @@ class Trainer:
         _check(_lib.splat_trainer_stream(self._h, ctypes.byref(out)))
         return out.value or 0
 
+    def collect_statistics_device_target(self, camera: Camera, device_target_ptr: int) -> StepStats:
+        """collect_statistics with the target already in device memory."""
+        s = _Stats()
+        _check(_lib.splat_trainer_collect_statistics_device_target(self._h, ctypes.byref(camera._c()), _P(device_target_ptr),
+                                                                   camera.width * camera.height * 4, ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def score_view_device_target(self, camera: Camera, device_target_ptr: int, error_share: float,
+                                 pixel_weight: float = 1.0) -> StepStats:
+        """score_view with the target already in device memory."""
+        s = _Stats()
+        _check(_lib.splat_trainer_score_view_device_target(self._h, ctypes.byref(camera._c()), _P(device_target_ptr),
+                                                           camera.width * camera.height * 4, float(error_share),
+                                                           float(pixel_weight), ctypes.byref(s)))
+        return StepStats._from(s)
+
+    def step_batch_device_targets(self, cameras: list, device_target_ptrs: list, rates: LearningRates) -> list:
+        """step_batch with the targets already in device memory (device addresses)."""
+        k = len(cameras)
+        cams = (_Camera * k)(*[c._c() for c in cameras])
+        ptrs = (_P * k)(*[_P(int(a)) for a in device_target_ptrs])
+        stats = (_Stats * k)()
+        _check(_lib.splat_trainer_step_batch_device_targets(self._h, cams, ptrs, k, ctypes.byref(rates._c()), stats))
+        return [StepStats._from(x) for x in stats]
+
     def step_batch(self, cameras: list, targets: list, rates: LearningRates) -> list:
         """Several views in one step (new in this library): one Adam step from
         the summed gradients. Needs sort_form SORT_TILE_DEPTH_64."""
