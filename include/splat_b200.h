@@ -536,13 +536,13 @@ int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, u
  * reference. It allocates nothing: its scratch is one file-scope __device__
  * array of about 4 MiB that every GPU loading this library holds until the
  * process exits. Limit: count <= 4194304 keys (key_bits 1..32, digit_bits
- * 6..8); larger counts return SPLAT_ERR_INVALID with a message saying so. The
- * first call on a device looks up the array's device address with that device
- * current; make that first call before any stream capture. Every call shares
- * the one array (it clears what must start at zero), so calls that overlap on
- * the GPU, from any stream or thread, race and must be ordered by the caller.
- * Device pointers and the result as for splat_radix_sort_u32; the call waits
- * for the sort to finish. */
+ * 6..8); larger counts return SPLAT_ERR_INVALID with a message saying so.
+ * Every call looks up the array's device address with the caller's device
+ * current. Every call shares the one array (it clears what must start at
+ * zero), so calls that overlap on the GPU, from any stream or thread, race and
+ * must be ordered by the caller. Device pointers and the result as for
+ * splat_radix_sort_u32. The call reads its error word back and synchronises
+ * its stream before it returns, so it cannot be used inside stream capture. */
 int splat_radix_sort_u32_noalloc(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, uint32_t *tmp_values,
                                  uint32_t count, int32_t key_bits, int32_t digit_bits, void *stream);
 

@@ -7,7 +7,6 @@
 // file-scope __device__ array of a fixed size, which every GPU that loads this
 // library holds until the process exits.
 #include <cstring>
-#include <mutex>
 
 #include "common.cuh"
 #include "sort.cuh"
@@ -26,13 +25,12 @@ constexpr size_t kNoAllocBytes = kNoAllocSortBytes + 256;
 
 static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noAllocMutex;
-void *g_noAllocAddress[kMaxDevices] = {};
-
-// The device address of g_noAllocScratch on the current device. In host code
+// The device address of g_noAllocScratch in the current context. In host code
 // the array's name stands for a host-side shadow, not device memory, so the
-// address is asked for once per device, with that device current.
+// address is asked for with the device current, on every call: a cache keyed
+// by device index would go stale after cudaDeviceReset (the module is loaded
+// again, possibly elsewhere) or under another context on the same device, and
+// the lookup costs little next to the sort and its wait.
 int scratch_address(void **out, const char **message) {
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) {
@@ -40,21 +38,13 @@ int scratch_address(void **out, const char **message) {
     *message = "no current CUDA device";
     return SPLAT_ERR_DEVICE;
   }
-  if (device < 0 || device >= kMaxDevices) {
-    *message = "device index beyond the no-allocation sort's table";
+  void *address = nullptr;
+  if (cudaGetSymbolAddress(&address, g_noAllocScratch) != cudaSuccess || address == nullptr) {
+    cudaGetLastError();
+    *message = "cudaGetSymbolAddress of the no-allocation sort's scratch failed";
     return SPLAT_ERR_DEVICE;
   }
-  std::lock_guard<std::mutex> lock(g_noAllocMutex);
-  if (g_noAllocAddress[device] == nullptr) {
-    void *address = nullptr;
-    if (cudaGetSymbolAddress(&address, g_noAllocScratch) != cudaSuccess || address == nullptr) {
-      cudaGetLastError();
-      *message = "cudaGetSymbolAddress of the no-allocation sort's scratch failed";
-      return SPLAT_ERR_DEVICE;
-    }
-    g_noAllocAddress[device] = address;
-  }
-  *out = g_noAllocAddress[device];
+  *out = address;
   return SPLAT_OK;
 }
 
@@ -101,6 +91,7 @@ extern "C" int splat_radix_sort_u32_noalloc(uint32_t *keys, uint32_t *values, ui
   }
   const int where = sb::sort_pairs_u32(keys, values, tmp_keys, tmp_values, count, count, nullptr, 0, key_bits, digits, base,
                                        error, s);
+  if (cudaGetLastError() != cudaSuccess) return fail(SPLAT_ERR_DEVICE, "a launch of the sort's kernels failed");
   if (where == 1) {
     if (cudaMemcpyAsync(keys, tmp_keys, (size_t)count * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(values, tmp_values, (size_t)count * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {

@@ -2534,6 +2534,7 @@ int splat_radix_sort_u32(uint32_t *keys, uint32_t *values, uint32_t *tmp_keys, u
     SB_CUDA(cudaMemsetAsync(error.get(), 0, 4, s));
     const int where = sb::sort_pairs_u32(keys, values, tmp_keys, tmp_values, count, count, nullptr, 0, key_bits, digits,
                                          scratch.get(), error.get<uint32_t>(), s);
+    SB_CUDA(cudaGetLastError());
     if (where == 1) {
       SB_CUDA(cudaMemcpyAsync(keys, tmp_keys, (size_t)count * 4, cudaMemcpyDeviceToDevice, s));
       SB_CUDA(cudaMemcpyAsync(values, tmp_values, (size_t)count * 4, cudaMemcpyDeviceToDevice, s));
@@ -2563,6 +2564,7 @@ int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, u
     auto *tk = reinterpret_cast<unsigned long long *>(tmp_keys);
     const int where = sb::sort_pairs_u64(k, values, tk, tmp_values, count, count, nullptr, 0, key_bits, digits, scratch.get(),
                                          error.get<uint32_t>(), s);
+    SB_CUDA(cudaGetLastError());
     if (where == 1) {
       SB_CUDA(cudaMemcpyAsync(keys, tmp_keys, (size_t)count * 8, cudaMemcpyDeviceToDevice, s));
       SB_CUDA(cudaMemcpyAsync(values, tmp_values, (size_t)count * 4, cudaMemcpyDeviceToDevice, s));
