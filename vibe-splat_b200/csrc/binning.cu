@@ -243,14 +243,16 @@ __global__ void __launch_bounds__(kCountThreads)
   }
 }
 
-// Exclusive scan of the coverage counts, in place (counts become offsets):
+// Exclusive scan of the coverage counts into offsets:
 // a block of kScanThreads threads takes kScanTile consecutive items, claimed
 // in launch order through a ticket, and finds what precedes it by a
 // decoupled look-back. counters[1] gets the total, counters[2] the entries
 // that fit the capacity; a total above it sets kErrEntryOverflow.
+// With gather, item r's count is counts[gather[r]] (counts indexed by splat,
+// the items in depth order); otherwise counts[r], and counts may be offsets.
 __global__ void __launch_bounds__(kScanThreads)
-    k_offsets_scan(uint32_t items, uint32_t *__restrict__ offsets, uint32_t *counters, uint32_t capacity,
-                   unsigned long long *status, uint32_t *ticket, uint32_t *error) {
+    k_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *__restrict__ gather, uint32_t *offsets,
+                   uint32_t *counters, uint32_t capacity, unsigned long long *status, uint32_t *ticket, uint32_t *error) {
   chain_enter();
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanThreads / 32];
@@ -261,13 +263,13 @@ __global__ void __launch_bounds__(kScanThreads)
   const uint32_t tile = s_tile;
   const uint32_t numTiles = div_up(items, kScanTile);
   if (tile >= numTiles) return;
-  uint32_t counts[kScanItems];
+  uint32_t counts_[kScanItems];
   uint32_t threadSum = 0;
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
-    counts[j] = r < items ? offsets[r] : 0u;
-    threadSum += counts[j];
+    counts_[j] = r < items ? counts[gather != nullptr ? gather[r] : r] : 0u;
+    threadSum += counts_[j];
   }
   // Block scan of the thread sums.
   uint32_t inclusive = threadSum;
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(kScanThreads)
   for (int j = 0; j < kScanItems; ++j) {
     const uint32_t r = tile * kScanTile + t * kScanItems + j;
     if (r < items) offsets[r] = running;
-    running += counts[j];
+    running += counts_[j];
   }
 }
 
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(kScanThreads)
 __global__ void __launch_bounds__(256)
     k_bin_emit(const Splat *__restrict__ splats, const float *__restrict__ reach, const uint32_t *__restrict__ itemKeys,
                const uint32_t *__restrict__ itemSplat, uint32_t items, uint32_t n, const ViewSet *__restrict__ viewsPtr,
-               const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ masks, uint32_t capacity,
+               const uint32_t *__restrict__ offsets, const uint32_t *__restrict__ masks, bool masksBySplat, uint32_t capacity,
                uint32_t *__restrict__ tileKeys32, unsigned long long *__restrict__ tileKeys64, uint32_t *__restrict__ entryValues,
                uint32_t *error) {
   chain_enter();
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(256)
   if (valid) t = splat_tiles(splats[s].centerExtent, views.v[view].gridW, views.v[view].gridH);
   const uint32_t width = t.x1 - t.x0 + 1u, area = valid ? rect_area(t) : 0u;
   const bool big = area > 32u;
-  const uint32_t mask = valid && !big ? masks[r] : 0u;
+  const uint32_t mask = valid && !big ? masks[masksBySplat ? s : r] : 0u;
   const uint32_t first = valid ? offsets[r] : 0u;
   bool overflow = false;
   auto put = [&](uint32_t slot, int v, uint32_t x, uint32_t y, uint32_t key, uint32_t splat) {
@@ -490,26 +492,40 @@ size_t bin_scan_scratch_bytes(uint32_t items) {
   return (size_t)(div_up(items, kScanTile) + 1) * sizeof(unsigned long long) + 256;
 }
 
-void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
-                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *masks,
-                           uint32_t *counters, uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
+void launch_bin_count(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat, uint32_t items,
+                      uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *counts, uint32_t *masks, uint32_t *counters,
+                      cudaStream_t stream) {
+  if (items == 0) return;
+  launch_chained(k_bin_count, dim3(div_up(items, kCountThreads)), dim3(kCountThreads), 0, stream, splats, reach, itemKeys, itemSplat,
+                 items, n, dViews, counts, masks, counters);
+}
+
+void launch_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *gather, uint32_t *offsets, uint32_t *counters,
+                         uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
   if (items == 0) return;
   const uint32_t tiles = div_up(items, kScanTile);
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
   cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
-  launch_chained(k_bin_count, dim3(div_up(items, kCountThreads)), dim3(kCountThreads), 0, stream, splats, reach, itemKeys, itemSplat, items, n, dViews,
-                                                                        offsets, masks, counters);
-  launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, offsets, counters, capacity, status, ticket, error);
+  launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, counts, gather, offsets, counters, capacity, status,
+                 ticket, error);
+}
+
+void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
+                           uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *masks,
+                           uint32_t *counters, uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
+  if (items == 0) return;
+  launch_bin_count(splats, reach, itemKeys, itemSplat, items, n, views, dViews, offsets, masks, counters, stream);
+  launch_offsets_scan(items, offsets, nullptr, offsets, counters, capacity, scratch, error, stream);
 }
 
 void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
                      uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets,
-                     const uint32_t *masks, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
+                     const uint32_t *masks, bool masksBySplat, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
                      uint32_t *entryValues, uint32_t *error, cudaStream_t stream) {
   if (items == 0) return;
-  launch_chained(k_bin_emit, dim3(div_up(items, 256)), dim3(256), 0, stream, splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks, capacity,
-                                                     tileKeys32, tileKeys64, entryValues, error);
+  launch_chained(k_bin_emit, dim3(div_up(items, 256)), dim3(256), 0, stream, splats, reach, itemKeys, itemSplat, items, n, dViews, offsets, masks,
+                 masksBySplat, capacity, tileKeys32, tileKeys64, entryValues, error);
 }
 
 void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *tileKeys64, const uint32_t *deviceCount,
@@ -526,7 +542,8 @@ void launch_exclusive_scan(uint32_t items, uint32_t *values, uint32_t *counters,
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
   cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
-  launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, values, counters, 0xFFFFFFFFu, status, ticket, error);
+  launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, values, nullptr, values, counters, 0xFFFFFFFFu, status,
+                 ticket, error);
 }
 
 } // namespace sb

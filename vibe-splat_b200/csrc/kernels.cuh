@@ -63,13 +63,24 @@ void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32
                            uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *offsets, uint32_t *masks,
                            uint32_t *counters, uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream);
 size_t bin_scan_scratch_bytes(uint32_t items);
+// The two halves of launch_bin_count_scan, for the depth-sorted form, whose
+// counting runs per splat while the depth sort runs on another stream:
+// counts[r] and masks[r] of item r; then offsets[r] = the exclusive scan of
+// counts[gather[r]] (gather null: of counts[r]; counts may be offsets), with
+// counters[1], counters[2] and the overflow bit as above.
+void launch_bin_count(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat, uint32_t items,
+                      uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *counts, uint32_t *masks, uint32_t *counters,
+                      cudaStream_t stream);
+void launch_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *gather, uint32_t *offsets, uint32_t *counters,
+                         uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream);
 
 // train_bin_emit.comp. Depth-sorted form: tileKeys32[slot] = tile, entryValues[slot]
 // = splat. Single-sort form (tileKeys64 not null): tileKeys64[slot] = (global
-// tile << 32) | depth key.
+// tile << 32) | depth key. masks are indexed by item, or by splat with
+// masksBySplat (a count that ran per splat).
 void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,
                      uint32_t items, uint32_t n, const ViewSet &views, const ViewSet *dViews, const uint32_t *offsets,
-                     const uint32_t *masks, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
+                     const uint32_t *masks, bool masksBySplat, uint32_t capacity, uint32_t *tileKeys32, unsigned long long *tileKeys64,
                      uint32_t *entryValues, uint32_t *error, cudaStream_t stream);
 
 // train_tile_ranges.comp over the sorted keys; ranges (2 u32 per global tile)

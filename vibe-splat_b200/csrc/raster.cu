@@ -650,6 +650,27 @@ __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, co
   }
 }
 
+// Packed two-lane FP32 arithmetic (sm_100a): each lane of fma2/mul2/add2 is
+// rounded once, exactly as fmaf / * / + on that lane alone, so a pixel pair
+// computed this way gets the bits each pixel would get on its own.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// c - a, lane by lane. Written as a packed fused multiply-add by the constant
+// -1, it gave wrong sums inside k_backward2 with nvcc 12.9 for sm_100a (a
+// stand-alone kernel computed the same form correctly), so it stays scalar.
+__device__ __forceinline__ float2 rsub2(float2 a, float2 c) { return make_float2(c.x - a.x, c.y - a.y); }
+
+// The exponent of a staged splat at a lane's two pixels, which share their
+// column (dx) and sit 4 rows apart: splat_power() of each, in its rounding
+// order, with the column's products computed once.
+__device__ __forceinline__ float2 splat_power2(const Staged &s, float dx, float2 dy) {
+  const float hx = s.hqx * dx;
+  const float2 pxy = fma2(f2(s.nqy), dy, f2(hx));
+  return fma2(mul2(f2(s.hqz), dy), dy, mul2(pxy, f2(dx)));
+}
+
 template <class M>
 __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
                                                         const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
@@ -666,58 +687,72 @@ __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restri
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const PixelPair pp = pixel_pair(geo, cam, t);
   const uint2 range = ranges[tile];
-  float cr[2] = {0.f, 0.f}, cg[2] = {0.f, 0.f}, cb[2] = {0.f, 0.f}, T[2] = {1.f, 1.f}, logT[2] = {0.f, 0.f};
-  uint32_t stop[2] = {range.x, range.x};
-  bool done[2] = {!pp.inside[0], !pp.inside[1]};
+  const float px = pp.px[0];
+  const float2 py = make_float2(pp.py[0], pp.py[1]);
+  const float logMin = kLogMinTransmittance * M::kLogScale;
+  float2 cr = f2(0.0f), cg = f2(0.0f), cb = f2(0.0f), T = f2(1.0f), logT = f2(0.0f);
+  uint32_t stop0 = range.x, stop1 = range.x;
+  bool done0 = !pp.inside[0], done1 = !pp.inside[1];
   for (uint32_t end = range.y; end > range.x;) {
     const uint32_t count = min((uint32_t)kBatch, end - range.x);
     end -= count;
-    if (__syncthreads_count(done[0] && done[1]) == kHalfTile) break;
+    if (__syncthreads_count(done0 && done1) == kHalfTile) break;
     stage_pairs<M>(splats, entryValues + end, count, splatLimit, geo, error, s_batch, s_cover);
     __syncthreads();
-    for (int word = (int)((count - 1u) >> 5); word >= 0 && !(done[0] && done[1]); --word) {
+    for (int word = (int)((count - 1u) >> 5); word >= 0 && !(done0 && done1); --word) {
     for (uint32_t bits = s_cover[warp][word]; bits != 0u;) {
       const int bit = 31 - __clz(bits);
       bits ^= 1u << bit;
       const uint32_t k = (uint32_t)word * 32u + (uint32_t)bit;
       const Staged &s = s_batch[k];
       const uint32_t mask = s.mask;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        if (done[q] || (mask & pp.bits[q]) != pp.bits[q]) continue;
-        const float dx = pp.px[q] - s.cx, dy = pp.py[q] - s.cy;
-        const float power = splat_power(s, dx, dy);
-        if (power > 0.0f) continue;
-        const float alpha = fminf(kAlphaMax, s.opacity * M::exp(power));
-        if (!(alpha >= kAlphaMin)) continue;
-        const float oneMinus = 1.0f - alpha;
-        const float logRest = M::log(oneMinus);
-        if (logT[q] + logRest < kLogMinTransmittance * M::kLogScale) {
-          stop[q] = end + (uint32_t)k + 1u;
-          done[q] = true;
-          continue;
-        }
-        const float w = T[q] * alpha;
-        cr[q] = fmaf(w, s.r, cr[q]);
-        cg[q] = fmaf(w, s.g, cg[q]);
-        cb[q] = fmaf(w, s.b, cb[q]);
-        T[q] = T[q] * oneMinus;
-        logT[q] = logT[q] + logRest;
+      // Both pixels' tests of k_forward, the exponent and alpha packed.
+      const float dx = px - s.cx;
+      const float2 dy = add2(py, f2(-s.cy));
+      const float2 power = splat_power2(s, dx, dy);
+      const float2 oe = mul2(f2(s.opacity), make_float2(M::exp(power.x), M::exp(power.y)));
+      const float a0 = fminf(kAlphaMax, oe.x), a1 = fminf(kAlphaMax, oe.y);
+      const bool v0 = !done0 && (mask & pp.bits[0]) == pp.bits[0] && !(power.x > 0.0f) && a0 >= kAlphaMin;
+      const bool v1 = !done1 && (mask & pp.bits[1]) == pp.bits[1] && !(power.y > 0.0f) && a1 >= kAlphaMin;
+      if (!(v0 || v1)) continue;
+      const float2 oneMinus = rsub2(make_float2(a0, a1), f2(1.0f));
+      const float2 next = add2(logT, make_float2(M::log(oneMinus.x), M::log(oneMinus.y)));
+      // A pixel whose transmittance would fall below the floor stops here.
+      const bool s0 = v0 && next.x < logMin, s1 = v1 && next.y < logMin;
+      if (s0) {
+        stop0 = end + k + 1u;
+        done0 = true;
       }
-      if (done[0] && done[1]) break;
+      if (s1) {
+        stop1 = end + k + 1u;
+        done1 = true;
+      }
+      // A pixel that does not blend takes weight 0 and factor 1: exact no-ops.
+      const bool b0 = v0 && !s0, b1 = v1 && !s1;
+      const float2 w = mul2(T, make_float2(b0 ? a0 : 0.0f, b1 ? a1 : 0.0f));
+      cr = fma2(w, f2(s.r), cr);
+      cg = fma2(w, f2(s.g), cg);
+      cb = fma2(w, f2(s.b), cb);
+      T = mul2(T, make_float2(b0 ? oneMinus.x : 1.0f, b1 ? oneMinus.y : 1.0f));
+      logT = make_float2(b0 ? next.x : logT.x, b1 ? next.y : logT.y);
+      if (done0 && done1) break;
     }
     }
   }
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    if (!pp.inside[q]) continue;
-    const size_t at = (size_t)cam.pixelBase + (size_t)pp.y[q] * cam.width + pp.x[q];
-    image[at] = make_float4(fmaf(T[q], bgR, cr[q]), fmaf(T[q], bgG, cg[q]), fmaf(T[q], bgB, cb[q]), logT[q]);
-    stops[at] = stop[q];
+  if (pp.inside[0]) {
+    const size_t at = (size_t)cam.pixelBase + (size_t)pp.y[0] * cam.width + pp.x[0];
+    image[at] = make_float4(fmaf(T.x, bgR, cr.x), fmaf(T.x, bgG, cg.x), fmaf(T.x, bgB, cb.x), logT.x);
+    stops[at] = stop0;
+  }
+  if (pp.inside[1]) {
+    const size_t at = (size_t)cam.pixelBase + (size_t)pp.y[1] * cam.width + pp.x[1];
+    image[at] = make_float4(fmaf(T.y, bgR, cr.y), fmaf(T.y, bgG, cg.y), fmaf(T.y, bgB, cb.y), logT.y);
+    stops[at] = stop1;
   }
 }
 
 // Float sums only: each lane adds its two pixels' values before one butterfly.
+// The per-pixel arithmetic runs on both pixels at once in packed FP32.
 template <class M, bool SCORE>
 __global__ void __launch_bounds__(kHalfTile, 6)
     k_backward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
@@ -741,22 +776,27 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   // front: log T total minus the log transmittance of the splats already
   // walked (those behind), kept as one running value. behind: the adjoint
   // dotted with the colour the splats behind (and the background) give, the
-  // one thing of that colour the alpha gradient needs.
-  float front[2], Ax[2], Ay[2], Az[2], behind[2], marked[2], edgeWeight[2];
+  // one thing of that colour the alpha gradient needs. One lane per pixel.
+  float fr[2], ax[2], ay[2], az[2], bh[2], mk[2], ew[2];
   uint32_t stop[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const size_t at = pp.inside[q] ? (size_t)cam.pixelBase + (size_t)pp.y[q] * cam.width + pp.x[q] : 0;
-    front[q] = pp.inside[q] ? image[at].w : 0.0f;
+    fr[q] = pp.inside[q] ? image[at].w : 0.0f;
     const float4 a = pp.inside[q] ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
-    Ax[q] = a.x;
-    Ay[q] = a.y;
-    Az[q] = a.z;
+    ax[q] = a.x;
+    ay[q] = a.y;
+    az[q] = a.z;
     stop[q] = pp.inside[q] ? stops[at] : range.y;
-    behind[q] = fmaf(a.z, bgB, fmaf(a.y, bgG, a.x * bgR));
-    marked[q] = a.w;
-    edgeWeight[q] = SCORE && pp.inside[q] ? edge[at] : 0.0f;
+    bh[q] = fmaf(a.z, bgB, fmaf(a.y, bgG, a.x * bgR));
+    mk[q] = a.w;
+    ew[q] = SCORE && pp.inside[q] ? edge[at] : 0.0f;
   }
+  float2 front = make_float2(fr[0], fr[1]), behind = make_float2(bh[0], bh[1]);
+  const float2 Ax = make_float2(ax[0], ax[1]), Ay = make_float2(ay[0], ay[1]), Az = make_float2(az[0], az[1]);
+  const float2 marked = make_float2(mk[0], mk[1]), edgeWeight = make_float2(ew[0], ew[1]);
+  const float px = pp.px[0];
+  const float2 py = make_float2(pp.py[0], pp.py[1]);
   const float perPixel = cam.perPixel;
   const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
   if (lane == 0) s_min[t >> 5] = warpMin;
@@ -777,54 +817,56 @@ __global__ void __launch_bounds__(kHalfTile, 6)
       const uint32_t k = word * 32u + (uint32_t)(__ffs(bits) - 1);
       const Staged &s = s_batch[k];
       const uint32_t mask = s.mask;
-      float dx[2], dy[2], ep[2], oe[2], alpha[2];
-      bool act[2];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        dx[q] = pp.px[q] - s.cx;
-        dy[q] = pp.py[q] - s.cy;
-        const float power = splat_power(s, dx[q], dy[q]);
-        ep[q] = M::exp(fminf(power, 0.0f));
-        oe[q] = s.opacity * ep[q];
-        alpha[q] = fminf(kAlphaMax, oe[q]);
-        act[q] = start + k >= stop[q] && (mask & pp.bits[q]) == pp.bits[q] && !(power > 0.0f) && alpha[q] >= kAlphaMin;
-      }
-      if (!__any_sync(0xFFFFFFFFu, act[0] || act[1])) continue;
+      const float dx = px - s.cx;
+      const float2 dy = add2(py, f2(-s.cy));
+      const float2 power = splat_power2(s, dx, dy);
+      const float2 ep = make_float2(M::exp(fminf(power.x, 0.0f)), M::exp(fminf(power.y, 0.0f)));
+      const float2 oe = mul2(f2(s.opacity), ep);
+      const float2 alpha = make_float2(fminf(kAlphaMax, oe.x), fminf(kAlphaMax, oe.y));
+      const uint32_t entry = start + k;
+      const bool act0 = entry >= stop[0] && (mask & pp.bits[0]) == pp.bits[0] && !(power.x > 0.0f) && alpha.x >= kAlphaMin;
+      const bool act1 = entry >= stop[1] && (mask & pp.bits[1]) == pp.bits[1] && !(power.y > 0.0f) && alpha.y >= kAlphaMin;
+      if (!__any_sync(0xFFFFFFFFu, act0 || act1)) continue;
+      // An inactive pixel takes alpha 0: its front and behind stay as they
+      // were and it adds zeros to the sums.
+      const float2 aAct = make_float2(act0 ? alpha.x : 0.0f, act1 ? alpha.y : 0.0f);
+      const float2 oneMinus = rsub2(aAct, f2(1.0f));
+      const float2 logRest = make_float2(M::log(oneMinus.x), M::log(oneMinus.y));
+      const float2 nextFront = rsub2(logRest, front);
+      const float2 T = make_float2(M::exp(nextFront.x), M::exp(nextFront.y));
+      const float2 wA = mul2(T, aAct);
       float g[SCORE ? 16 : 12];
-#pragma unroll
-      for (int j = 0; j < (SCORE ? 16 : 12); ++j) g[j] = 0.0f;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const float aAct = act[q] ? alpha[q] : 0.0f;
-        const float logRest = M::log(1.0f - aAct);
-        const float T = M::exp(front[q] - logRest);
-        // Float sums only, so fused multiply-adds throughout.
-        const float wA = T * aAct;
-        g[6] = fmaf(wA, Ax[q], g[6]);
-        g[7] = fmaf(wA, Ay[q], g[7]);
-        g[8] = fmaf(wA, Az[q], g[8]);
-        g[9] = fmaf(wA, perPixel, g[9]);
-        if constexpr (SCORE) {
-          g[12] = fmaf(act[q] ? marked[q] : 0.0f, perPixel, g[12]);
-          g[13] = fmaf(edgeWeight[q] * wA, perPixel, g[13]);
-        }
-        const float ahead = fmaf(Az[q], s.b, fmaf(Ay[q], s.g, Ax[q] * s.r)) - behind[q];
-        const float dAlpha = (act[q] && oe[q] < kAlphaMax) ? T * ahead : 0.0f;
-        g[0] = fmaf(dAlpha, ep[q], g[0]);
-        const float dPower = dAlpha * alpha[q];
-        const float vx = fmaf(s.qy, dy[q], s.qx * dx[q]), vy = fmaf(s.qz, dy[q], s.qy * dx[q]);
-        const float g1 = dPower * vx, g2 = dPower * vy;
-        g[1] += g1;
-        g[2] += g2;
-        g[10] += fabsf(g1);
-        g[11] += fabsf(g2);
-        // Twice the conic sums; the flush halves them (exactly).
-        g[3] = fmaf(g1, vx, g[3]);
-        g[4] = fmaf(g1, vy, g[4]);
-        g[5] = fmaf(g2, vy, g[5]);
-        behind[q] = fmaf(aAct, ahead, behind[q]);
-        front[q] = front[q] - logRest;
+      const float2 c6 = mul2(wA, Ax), c7 = mul2(wA, Ay), c8 = mul2(wA, Az);
+      g[6] = c6.x + c6.y;
+      g[7] = c7.x + c7.y;
+      g[8] = c8.x + c8.y;
+      g[9] = (wA.x + wA.y) * perPixel;
+      if constexpr (SCORE) {
+        g[12] = ((act0 ? marked.x : 0.0f) + (act1 ? marked.y : 0.0f)) * perPixel;
+        const float2 e = mul2(edgeWeight, wA);
+        g[13] = (e.x + e.y) * perPixel;
+        g[14] = g[15] = 0.0f;
       }
+      const float2 ahead = rsub2(behind, fma2(Az, f2(s.b), fma2(Ay, f2(s.g), mul2(Ax, f2(s.r)))));
+      // At the 0.99 clamp alpha no longer depends on the parameters.
+      const float2 dT = mul2(T, ahead);
+      const float2 dAlpha = make_float2(act0 && oe.x < kAlphaMax ? dT.x : 0.0f, act1 && oe.y < kAlphaMax ? dT.y : 0.0f);
+      const float2 c0 = mul2(dAlpha, ep);
+      g[0] = c0.x + c0.y;
+      const float2 dPower = mul2(dAlpha, alpha);
+      const float2 vx = fma2(f2(s.qy), dy, f2(s.qx * dx)), vy = fma2(f2(s.qz), dy, f2(s.qy * dx));
+      const float2 g1 = mul2(dPower, vx), g2 = mul2(dPower, vy);
+      g[1] = g1.x + g1.y;
+      g[2] = g2.x + g2.y;
+      g[10] = fabsf(g1.x) + fabsf(g1.y);
+      g[11] = fabsf(g2.x) + fabsf(g2.y);
+      // Twice the conic sums; the flush halves them (exactly).
+      const float2 c3 = mul2(g1, vx), c4 = mul2(g1, vy), c5 = mul2(g2, vy);
+      g[3] = c3.x + c3.y;
+      g[4] = c4.x + c4.y;
+      g[5] = c5.x + c5.y;
+      behind = fma2(aAct, ahead, behind);
+      front = nextFront;
       float total;
       if constexpr (SCORE) total = butterfly16(g);
       else total = butterfly12(g);

@@ -171,7 +171,7 @@ public:
   // The step's clears run on a second stream, forked from and joined back to
   // the first (branches of the same graph when captured).
   cudaStream_t side = nullptr;
-  cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
+  cudaEvent_t forkEvent = nullptr, joinEvent = nullptr, countForkEvent = nullptr, countEvent = nullptr;
   bool entryScratchClear = false; // the entry sort's scratch was cleared for this step
   // The next step's target on its way to the device: copied to pinned memory
   // and on to targetNext by copyStream while this step runs (copied is
@@ -204,7 +204,7 @@ public:
   // Tile entries.
   uint32_t entryCapacity = 0;
   DeviceBuffer entryKeys, entryValues, tmpEntryKeys, tmpEntryValues;
-  bool entriesInTmp = false, depthInTmp = false;
+  bool entriesInTmp = false, depthInTmp = false, countOverlap = false;
   // Per pixel and per tile of the views of a step.
   DeviceBuffer image, stops, adjoint, fields, target, ranges, partials;
   // Store-everything variant: per-pixel blend counts, list offsets, the list pool, scan scratch and counters.
@@ -346,6 +346,8 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   SB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
   SB_CUDA(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&countForkEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&countEvent, cudaEventDisableTiming));
   SB_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
   SB_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&consumed, cudaEventDisableTiming));
@@ -395,6 +397,8 @@ Trainer::~Trainer() {
     if (e != nullptr) cudaEventDestroy(e);
   if (forkEvent != nullptr) cudaEventDestroy(forkEvent);
   if (joinEvent != nullptr) cudaEventDestroy(joinEvent);
+  if (countForkEvent != nullptr) cudaEventDestroy(countForkEvent);
+  if (countEvent != nullptr) cudaEventDestroy(countEvent);
   if (side != nullptr) cudaStreamDestroy(side);
   if (copyStream != nullptr) {
     cudaStreamSynchronize(copyStream);
@@ -544,7 +548,7 @@ void Trainer::ensure_view_buffers() {
     values.ensure(items * 4);
     tmpKeys.ensure(items * 4);
     tmpValues.ensure(items * 4);
-    offsets.ensure(items * 8); // entry offsets, then the reached-tile masks
+    offsets.ensure(items * 12); // entry offsets, the reached-tile masks, then (depth-sorted form) the counts per splat
     raw.ensure(items * kRawStride * 4);
     shGrad.ensure(items * 32);
     SB_CUDA(cudaMemset(raw.get(), 0, items * kRawStride * 4));
@@ -718,6 +722,20 @@ void Trainer::record_prepare(bool backward) {
   launch_preprocess(p, views, dViews.get<ViewSet>(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
                     oneSort ? nullptr : values.get<uint32_t>(), stream, error);
   end(0);
+  const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
+  uint32_t *offs = offsets.get<uint32_t>(), *masks = offs + items, *countsBySplat = offs + 2 * (size_t)items;
+  // Depth-sorted form: the tiles of each splat are counted per splat index on
+  // the second stream while the depth sort runs, and the scan gathers the
+  // counts in depth order; the two latency-bound passes overlap. With stage
+  // timing on, they run one after the other so that each is timed alone.
+  countOverlap = !oneSort && !timing;
+  if (countOverlap) {
+    SB_CUDA(cudaEventRecord(countForkEvent, stream));
+    SB_CUDA(cudaStreamWaitEvent(side, countForkEvent, 0));
+    launch_bin_count(splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(), nullptr, n, n, views,
+                     dViews.get<ViewSet>(), countsBySplat, masks, counters, side);
+    SB_CUDA(cudaEventRecord(countEvent, side));
+  }
   SB_CUDA(cudaStreamWaitEvent(stream, joinEvent, 0));
   begin(1);
   if (!oneSort) {
@@ -729,10 +747,13 @@ void Trainer::record_prepare(bool backward) {
   begin(2);
   const uint32_t *itemKeys = oneSort ? depthKeys.get<uint32_t>() : (depthInTmp ? tmpKeys.get<uint32_t>() : depthKeys.get<uint32_t>());
   const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
-  const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
-  launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
-                        offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, counters, entryCapacity, scanScratch.get(),
-                        error, stream);
+  if (countOverlap) {
+    SB_CUDA(cudaStreamWaitEvent(stream, countEvent, 0));
+    launch_offsets_scan(items, countsBySplat, itemSplat, offs, counters, entryCapacity, scanScratch.get(), error, stream);
+  } else {
+    launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(), offs,
+                          masks, counters, entryCapacity, scanScratch.get(), error, stream);
+  }
   end(2);
 }
 
@@ -744,7 +765,7 @@ void Trainer::record_forward() {
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
   begin(3);
   launch_bin_emit(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
-                  offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, entryCapacity,
+                  offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, countOverlap, entryCapacity,
                   oneSort ? nullptr : entryKeys.get<uint32_t>(),
                   oneSort ? entryKeys.get<unsigned long long>() : nullptr, entryValues.get<uint32_t>(), error, stream);
   // The scratch was cleared with the step's other clears unless the entry
