@@ -33,6 +33,7 @@ host cores instead.
 from __future__ import annotations
 
 import argparse
+import copy
 import importlib
 import json
 import math
@@ -95,6 +96,121 @@ def hemisphere_views(count: int = VIEWS, radius: float = 5.0, width: int = WIDTH
         view[:3, :3] = rot
         view[:3, 3] = -rot @ eye
         out.append((view.astype(np.float32), eye.astype(np.float32), fx, fx, width / 2, height / 2, width, height))
+    return out
+
+
+def ring_views(count: int = 16, radius: float = 6.0, width: int = 800, height: int = 800, lift: float = 0.5):
+    """Cameras on a horizontal ring of the given radius (at height `lift`)
+    looking at the origin, 60 degree horizontal field of view: the full
+    training step's 16 cameras. Same tuple layout as hemisphere_views."""
+    fx = (width / 2) / math.tan(math.radians(30.0))
+    out = []
+    for k in range(count):
+        a = 2.0 * math.pi * k / count
+        eye = np.array([radius * math.cos(a), radius * math.sin(a), lift])
+        forward = -eye / np.linalg.norm(eye)
+        right = np.cross(forward, np.array([0.0, 0.0, 1.0]))
+        right /= np.linalg.norm(right)
+        down = np.cross(forward, right)
+        rot = np.stack([right, down, forward])
+        view = np.eye(4)
+        view[:3, :3] = rot
+        view[:3, 3] = -rot @ eye
+        out.append((view.astype(np.float32), eye.astype(np.float32), fx, fx, width / 2, height / 2, width, height))
+    return out
+
+
+def config2_scene(n: int = 100_000, seed: int = 2):
+    """The full training step's scene: n Gaussians of SH degree 3, means
+    uniform in [-2, 2]^3, log-scales N(-3, 0.3), unit quaternions from
+    N(0, 1)^4, opacity logits N(0, 1), DC colour U(0, 1), higher SH
+    N(0, 0.05). GaussianCloud arrays (float32)."""
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32).ravel()
+    scales = rng.normal(-3.0, 0.3, (n, 3)).astype(np.float32).ravel()
+    q = rng.normal(size=(n, 4))
+    rot = (q / np.linalg.norm(q, axis=1, keepdims=True)).astype(np.float32).ravel()
+    opac = rng.normal(0.0, 1.0, n).astype(np.float32)
+    sh = np.zeros((n, 16, 3), np.float32)
+    sh[:, 0, :] = (rng.uniform(0.0, 1.0, (n, 3)) - 0.5) / SH_C0
+    sh[:, 1:, :] = rng.normal(0.0, 0.05, (n, 15, 3))
+    return pos, scales, rot, opac, sh.ravel()
+
+
+def fd_picks(rng, visible: np.ndarray, degree: int = DEGREE) -> list:
+    """256 parameters of Gaussians a view sees: 64 position, 48 log-scale, 48
+    rotation, 32 opacity and 64 SH coordinates, each of a random Gaussian."""
+    coeffs = (degree + 1) ** 2
+    picks = []
+    for group, count, per in (("positions", 64, 3), ("scales", 48, 3), ("rotations", 48, 4), ("opacities", 32, 1),
+                              ("sh", 64, 3 * coeffs)):
+        for g in rng.choice(visible, count, replace=False):
+            picks.append((group, int(g) * per + int(rng.integers(0, per))))
+    return picks
+
+
+def agreement(a, b) -> dict:
+    """The reference's gradient comparison (tests/test_train.cpp:38-54): cosine
+    and length ratio of a against b."""
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    aa, bb = float(a @ a), float(b @ b)
+    if aa == 0.0 or bb == 0.0:
+        return {"cosine": 0.0, "length_ratio": 0.0}
+    return {"cosine": float(a @ b) / math.sqrt(aa * bb), "length_ratio": math.sqrt(aa / bb)}
+
+
+def fd_config2(splat, torch, step: float = 1e-4, lam: float = 0.2) -> dict:
+    """The full training step's adjoint against central differences of the
+    FP64 oracle's loss (oracle/fp64.py, 0.8 L1 + 0.2 (1 - SSIM)) on 256
+    parameters, h = 1e-4, for both backward variants (fixed-point and float
+    sums), FP32 parameters, camera 0 of the ring, a seeded U(0, 1) target. A
+    checker run outside every timed region; the criteria are the reference
+    tests' (float: cosine > 0.999, length within 1 %, tests/test_train.cpp:99-112;
+    fixed point: cosine > 0.97, within 10 %, :286-291)."""
+    from oracle import fp64
+    from oracle import oracle as O
+
+    arrays = config2_scene()
+    cam = ring_views()[0]
+    view = O.View(*cam)
+    rng = np.random.default_rng(5)
+    target = rng.integers(0, 256, (800 * 800, 4), dtype=np.uint8)
+    target[:, 3] = 255
+    target = target.ravel()
+    dc = fp64.DeviceCloud(O.Cloud(DEGREE, *arrays))
+    out = {"workload": "100k Gaussians, SH degree 3, 800x800, camera 0 of 16 on a radius-6 ring, 256 parameters, h = 1e-4",
+           "differences": "central, of the FP64 loss with the base render's blended (splat, pixel) pairs held fixed"}
+    picks = None
+    fd = None
+    for fixed in (False, True):
+        opts = splat.TrainerOptions(force_fixed_point=fixed, sh_storage=splat.SH_F32, state_storage=splat.STATE_F32)
+        trainer = splat.Trainer(splat.GaussianCloud(DEGREE, *arrays), opts)
+        stats = trainer.compute_gradients(splat.Camera(*cam), target)
+        g = trainer.gradients()
+        del trainer
+        if picks is None:
+            visible = np.nonzero(np.abs(g.opacities) > 0)[0]
+            picks = fd_picks(np.random.default_rng(17), visible)
+            t0 = time.perf_counter()
+            fd = fp64.finite_differences(dc, view, target, lam, picks, step=step)
+            out["fd_seconds"] = time.perf_counter() - t0
+            base = fp64.render_full(dc, view)
+            loss64, _, _, adjoint = fp64.loss(base.rgb, target, view.width, view.height, lam)
+            out["loss_fp64"] = loss64
+            g64 = fp64.gradients(dc, view, base, adjoint)
+            out["fp64_adjoint"] = agreement([g64[gr][ix] for gr, ix in picks], fd)
+            del base, adjoint
+        analytic = np.array([getattr(g, group)[index] for group, index in picks], np.float64)
+        agree = agreement(analytic, fd)
+        agree["loss"] = stats.loss
+        agree["groups"] = {name: agreement(analytic[[k for k, (gr, _) in enumerate(picks) if gr == name]],
+                                           fd[[k for k, (gr, _) in enumerate(picks) if gr == name]])
+                           for name in ("positions", "scales", "rotations", "opacities", "sh")}
+        cos, ratio = (0.97, 0.1) if fixed else (0.999, 0.01)
+        agree["passes"] = agree["cosine"] > cos and abs(agree["length_ratio"] - 1.0) < ratio
+        out["fixed_point" if fixed else "float"] = agree
+    torch.cuda.empty_cache()
     return out
 
 
@@ -221,37 +337,61 @@ class ClockSampler:
 # ----------------------------------------------------------------- CPU reference
 
 
-def reference_iterations(oracle, cloud, views, targets, threads: int, rows_per_band: int | None = None) -> tuple:
-    """One training iteration's forward + loss + backward of the reference's
-    FP64 twin per view, the image split into `threads` horizontal bands that
-    run in parallel (each band a camera on those rows; every band projects all
-    Gaussians, as reference_render must). Returns (seconds, views done)."""
+def adam_step_fp64(params: dict, grads, rates: dict, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-15) -> None:
+    """One Adam step in FP64 from a zero state (a run's first iteration),
+    selective as the reference's (a parameter without a gradient stays), in
+    place on the float32 parameter arrays: the reference's step
+    (shaders/train_step.glsl, constants src/train/trainer.cpp:23) restated in
+    numpy, since the reference has it only as a shader. rates: per group; SH
+    above DC at rates['sh_rest']."""
+    c1, c2 = 1.0 - beta1, 1.0 - beta2
+    for group in ("positions", "scales", "rotations", "opacities", "sh"):
+        g = np.asarray(getattr(grads, group), np.float64)
+        m = (1.0 - beta1) * g
+        v = (1.0 - beta2) * g * g
+        lr = np.full(g.shape, rates[group])
+        if group == "sh":
+            coeffs = g.size // (params["opacities"].size * 3)
+            lr = lr.reshape(-1, coeffs, 3)
+            lr[:, 1:, :] = rates["sh_rest"]
+            lr = lr.ravel()
+        step = lr * (m / c1) / (np.sqrt(v / c2) + eps)
+        step[g == 0.0] = 0.0
+        params[group] -= step.astype(np.float32)
+
+
+def twin_views_per_core(oracle, arrays, views, targets, threads: int, adam: bool = True) -> dict:
+    """The reference's FP64 CPU twin (src/train/reference.cpp, compiled from its
+    sources into oracle/_ref) on whole views, one view per host thread, as many
+    views at once as there are threads: per view reference_render,
+    reference_loss and reference_gradients (which renders again), then, with
+    adam, an FP64 Adam step on a copy of the parameters. Returns the wall time,
+    the views done, and each view's own seconds (one thread's time for one
+    whole view)."""
     import concurrent.futures
 
-    def band_jobs(view, target):
-        W, H = view.width, view.height
-        rows = rows_per_band or math.ceil(H / threads)
-        jobs = []
-        for y0 in range(0, H, rows):
-            h = min(rows, H - y0)
-            v = oracle.View(view.view, view.position, view.fx, view.fy, view.cx, view.cy - y0, W, h)
-            t = target.reshape(H, W, 4)[y0:y0 + h].ravel()
-            jobs.append((v, t))
-        return jobs
+    pos, sc, rot, op, sh = arrays
+    rates = {"positions": 1.6e-4, "scales": 0.005, "rotations": 0.001, "opacities": 0.05, "sh": 0.025,
+             "sh_rest": 0.025 * 0.05}
 
-    def work(job):
-        v, t = job
-        rgb, _, _ = oracle.ref_render(cloud, v)
-        _, _, _, adjoint = oracle.ref_loss(rgb, v.width, v.height, t, 0.2)
-        oracle.ref_gradients(cloud, v, adjoint)
+    def one(job):
+        view, target = job
+        t0 = time.perf_counter()
+        cloud = oracle.Cloud(DEGREE, pos, sc, rot, op, sh)
+        rgb, _, _ = oracle.ref_render(cloud, view)
+        _, _, _, adjoint = oracle.ref_loss(rgb, view.width, view.height, target, 0.2)
+        grads = oracle.ref_gradients(cloud, view, adjoint)
+        if adam:
+            params = {"positions": pos.copy(), "scales": sc.copy(), "rotations": rot.copy(), "opacities": op.copy(),
+                      "sh": sh.copy()}
+            adam_step_fp64(params, grads, rates)
+        return time.perf_counter() - t0
 
-    jobs = []
-    for view, target in zip(views, targets):
-        jobs.extend(band_jobs(view, target))
+    jobs = list(zip(views, targets))
     start = time.perf_counter()
     with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as pool:
-        list(pool.map(work, jobs))
-    return time.perf_counter() - start, len(views)
+        per_view = list(pool.map(one, jobs))
+    return {"seconds": time.perf_counter() - start, "views": len(jobs), "per_view_seconds": per_view}
 
 
 def reference_arm(args) -> None:
@@ -264,32 +404,37 @@ def reference_arm(args) -> None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsplatref.so was not built "
                           "(the reference's src/train/reference.cpp compiles only where its tree is present)"}))
         return
-    pos, sc, rot, op, sh = make_scene()
-    cloud = O.Cloud(DEGREE, pos, sc, rot, op, sh)
-    cams = hemisphere_views()
-    targets = make_targets(8)
+    arrays = make_scene()
     threads = cpu_count()
-    views = [O.View(v, p, fx, fy, cx, cy, w, h) for (v, p, fx, fy, cx, cy, w, h) in cams]
-    for i in range(args.warmup if args.reference_warmup else 0):
-        reference_iterations(O, cloud, [views[i % VIEWS]], [targets[i % 8]], threads)
-    total_s, done = 0.0, 0
-    for i in range(args.steps):
-        s, d = reference_iterations(O, cloud, [views[i % VIEWS]], [targets[i % 8]], threads)
-        total_s += s
-        done += d
-    value = done / total_s
-    sample = (f"{args.steps} full training iterations (1M Gaussians, SH degree 3, 1237x822), each split into "
-              f"{threads} row bands run on {threads} threads; reference_render + reference_loss + "
-              "reference_gradients (which renders again) per band")
+    # K steps, each one whole view (render, loss, gradients, Adam) on one host
+    # thread, run as full rounds of one view per thread: K rounded up to a
+    # multiple of the thread count, so that no round leaves cores idle.
+    count = threads * math.ceil(max(args.steps, 1) / threads)
+    views = [O.View(*hemisphere_views()[i % VIEWS]) for i in range(count)]
+    targets = make_targets(8)
+    run = twin_views_per_core(O, arrays, views, [targets[i % 8] for i in range(count)], threads)
+    value = run["views"] / run["seconds"]
+    per_view = float(np.mean(run["per_view_seconds"]))
+    sample = (f"{run['views']} whole views (1M Gaussians, SH degree 3, 1237x822), one per host thread on {threads} threads "
+              f"({run['seconds']:.0f} s): reference_render + reference_loss + reference_gradients of the reference's FP64 "
+              f"twin and an FP64 Adam step; {per_view:.0f} s per view on one thread")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "iters/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / done,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * run["seconds"] / run["views"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "the reference's FP64 CPU twin (src/train/reference.cpp): render, "
-                                                "loss and gradients per view, no optimiser step"},
-        "cpu_baseline": {"value": value, "unit": "iters/s", "cores": threads, "kind": "reference", "sample": sample},
+        "config": bench_config(),
+        "form": "the reference's FP64 CPU twin (src/train/reference.cpp) per whole view, one view per core, with an "
+                "FP64 Adam step restated from its shader",
+        "cpu_baseline": {"value": value, "unit": "iters/s", "cores": threads, "kind": "reference", "sample": sample,
+                         "single_thread_seconds_per_view": per_view},
         "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def bench_config() -> dict:
+    """The workload both arms report as their config."""
+    return {"workload": WORKLOAD, "views": VIEWS, "loss": "0.8 L1 + 0.2 (1 - SSIM)", "optimiser": "Adam, one step per view",
+            "l2": "inputs larger than L2 (1M-Gaussian parameters and state, 64 x 4 MB targets)"}
 
 
 # ----------------------------------------------------------------- our arm
@@ -370,18 +515,26 @@ def psnr(image: np.ndarray, reference: np.ndarray) -> float:
     return 10.0 * math.log10(1.0 / max(mse, 1e-30))
 
 
+def tuned_options(chosen, tuned: dict):
+    """The chosen form's options with the autotuner's picks applied."""
+    opts = copy.copy(chosen)
+    if tuned:
+        opts.sort_form = tuned.get("sort_form", chosen.sort_form)
+        opts.digit_bits = tuned.get("digit_bits", chosen.digit_bits)
+        opts.forward_pixels_per_thread = tuned.get("forward_pixels_per_thread", chosen.forward_pixels_per_thread)
+        opts.backward_pixels_per_thread = tuned.get("backward_pixels_per_thread", chosen.backward_pixels_per_thread)
+        opts.tile_size = tuned.get("tile_size", chosen.tile_size)
+        opts.batch_depth = tuned.get("batch_depth", chosen.batch_depth)
+        opts.persistent_raster = bool(tuned.get("persistent_raster", chosen.persistent_raster))
+    return opts
+
+
 def precision_check(splat, torch, cloud, cams, host_targets, rates, chosen, tuned, steps: int = 20) -> dict:
     """The chosen form against the plain FP32 form from the same cloud: PSNR of
     one's render against the other's, then, after `steps` identical training
     steps (views in turn), each render's PSNR against the target and the
     difference."""
-    tuned_opts = chosen
-    if tuned:
-        tuned_opts.sort_form = tuned.get("sort_form", chosen.sort_form)
-        tuned_opts.digit_bits = tuned.get("digit_bits", chosen.digit_bits)
-        tuned_opts.forward_pixels_per_thread = tuned.get("forward_pixels_per_thread", chosen.forward_pixels_per_thread)
-        tuned_opts.backward_pixels_per_thread = tuned.get("backward_pixels_per_thread", chosen.backward_pixels_per_thread)
-    forms = {"chosen": tuned_opts, "plain": plain_options(splat)}
+    forms = {"chosen": tuned_options(chosen, tuned), "plain": plain_options(splat)}
     renders, after = {}, {}
     target0 = host_targets[0].reshape(-1, 4)[:, :3].astype(np.float64) / 255.0
     for name, opts in forms.items():
@@ -397,16 +550,55 @@ def precision_check(splat, torch, cloud, cams, host_targets, rates, chosen, tune
             "psnr_difference_db": abs(after["chosen"] - after["plain"])}
 
 
-def memory_adjoint_workload(args) -> None:
+def precision_vs_fp64(splat, torch, arrays, camera, view, target, forms: dict, lam: float = 0.2) -> dict:
+    """Each form's render, loss and gradients on one view against the FP64
+    oracle (oracle/fp64.py: the reference twin's render, loss and gradients
+    restated in double precision on the GPU, pinned against the twin by
+    tests/test_configs.py) on the same cloud, with the SH coefficients the
+    form stores (BF16-rounded for the BF16 form): per-group relative error
+    ||g - g64|| / ||g64||, the render's PSNR against the FP64 render, and both
+    losses. A checker run outside every timed region."""
+    from oracle import fp64
+    from oracle import oracle as O
+
+    pos, sc, rot, op, sh = arrays
+    out = {}
+    for name, opts in forms.items():
+        trainer = splat.Trainer(splat.GaussianCloud(DEGREE, pos, sc, rot, op, sh), opts)
+        image = trainer.render(camera).reshape(-1, 4)[:, :3].astype(np.float64)
+        stats = trainer.compute_gradients(camera, target)
+        g = trainer.gradients()
+        del trainer
+        torch.cuda.empty_cache()
+        storage = {splat.SH_BF16: "bf16", splat.SH_F16: "f16"}.get(opts.sh_storage, "f32")
+        held = sh if storage == "f32" else O.round_sh_like_device(sh, DEGREE, storage)
+        dc = fp64.DeviceCloud(O.Cloud(DEGREE, pos, sc, rot, op, held))
+        rendered = fp64.render_full(dc, view)
+        loss64, _, _, adjoint = fp64.loss(rendered.rgb, target, view.width, view.height, lam)
+        g64 = fp64.gradients(dc, view, rendered, adjoint)
+        rgb64 = rendered.rgb.cpu().numpy()
+        rel = {}
+        for group in ("positions", "scales", "rotations", "opacities", "sh"):
+            ref = g64[group]
+            rel[group] = float(np.linalg.norm(np.asarray(getattr(g, group), np.float64) - ref) / max(np.linalg.norm(ref), 1e-300))
+        out[name] = {"loss": stats.loss, "loss_fp64": loss64, "render_psnr_vs_fp64_db": psnr(image, rgb64),
+                     "gradient_rel_error": rel, "max_gradient_rel_error": max(rel.values()),
+                     "fp64_entries": rendered.entry_count}
+        del dc, rendered, adjoint
+        torch.cuda.empty_cache()
+    return out
+
+
+def memory_adjoint_summary(gaussians: int, steps: int, warmup: int) -> dict:
     """The memory-bound adjoint: 6M Gaussians of SH degree 3 (BF16 above DC),
     3840x2160 views, log-scales N(-4.5, 0.6) for heavy per-tile overlap. The
     reverse-sweep recompute (8 bytes of per-pixel state) against the
     store-everything variant (every blended (entry, alpha) pair kept per pixel):
-    iterations/s, device memory held, per-pixel state. One JSON line."""
+    iterations/s, device memory held, per-pixel state."""
     import torch
 
     splat = importlib.import_module("vibe-splat_b200")
-    n = 6_000_000 if args.gaussians == GAUSSIANS else args.gaussians
+    n = gaussians
     width, height, views = 3840, 2160, 4
     pos, sc, rot, op, sh = make_scene(n, log_scale=(-4.5, 0.6))
     cloud = splat.GaussianCloud(DEGREE, pos, sc, rot, op, sh)
@@ -419,7 +611,7 @@ def memory_adjoint_workload(args) -> None:
     out = {"metric": "memory-bound adjoint: recompute vs store-everything", "unit": "iters/s",
            "config": {"workload": f"{n} Gaussians, SH degree 3 (BF16 above DC), {width}x{height}, log-scales N(-4.5, 0.6), "
                                   f"{views} cameras on a radius-5 hemisphere, 60 deg horizontal fov (synthetic)"},
-           "steps": args.steps, "warmup": args.warmup}
+           "steps": steps, "warmup": warmup}
     for name, lists in (("recompute", False), ("store_everything", True)):
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
@@ -431,13 +623,13 @@ def memory_adjoint_workload(args) -> None:
         if lists:
             opts.backward_pixels_per_thread = 1
         trainer = splat.Trainer(cloud, opts)
-        for i in range(args.warmup):
+        for i in range(warmup):
             stats = trainer.step_device_target(cams[i % views], targets[i % views].data_ptr(), rates)
         ms = time_steps(torch, trainer, lambda i: trainer.step_device_target(cams[i % views], targets[i % views].data_ptr(),
-                                                                              rates), args.steps, trainer.stream())
+                                                                              rates), steps, trainer.stream())
         torch.cuda.synchronize()
         free1, _ = torch.cuda.mem_get_info()
-        entry = {"iters_per_s": 1000.0 * args.steps / ms, "ms_per_step": ms / args.steps,
+        entry = {"iters_per_s": 1000.0 * steps / ms, "ms_per_step": ms / steps,
                  "device_bytes_held": free0 - free1, "tile_entries": stats.tile_entries,
                  "mean_entries_per_tile": stats.tile_entries / tiles, "per_pixel_state_bytes": 8.0}
         if lists:
@@ -451,23 +643,25 @@ def memory_adjoint_workload(args) -> None:
     r, s = out["recompute"], out["store_everything"]
     out["memory_saved_bytes"] = s["device_bytes_held"] - r["device_bytes_held"]
     out["speed_ratio_recompute_over_store"] = r["iters_per_s"] / s["iters_per_s"]
-    print(json.dumps(out))
+    return out
 
 
-def batched_workload(args) -> None:
-    """The batched form: 3M Gaussians of SH degree 3 (BF16 above DC), 8 views of
-    uneven sizes per step (one launch per stage for all of them, 64-bit
-    tile|depth keys, CUDA graph), cameras at random points of a sphere of radius
-    4 to 8 looking at the origin. Against the same views one per step. Views/s,
-    one JSON line."""
-    import torch
+def memory_adjoint_workload(args) -> None:
+    n = 6_000_000 if args.gaussians == GAUSSIANS else args.gaussians
+    print(json.dumps(memory_adjoint_summary(n, args.steps, args.warmup)))
 
-    splat = importlib.import_module("vibe-splat_b200")
-    n = 3_000_000 if args.gaussians == GAUSSIANS else args.gaussians
-    sizes = [(640, 480), (800, 600), (1024, 768), (1237, 822), (1280, 720), (1600, 1200), (960, 540), (1920, 1080)]
+
+BATCHED_SIZES = [(640, 480), (800, 600), (1024, 768), (1237, 822), (1280, 720), (1600, 1200), (960, 540), (1920, 1080)]
+
+
+def batched_views():
+    """The batched form's 8 views of uneven sizes, cameras at random points of
+    a sphere of radius 4 to 8 looking at the origin (60 degree horizontal
+    field of view), and a seeded RGBA8 target each: (view tuples as
+    hemisphere_views gives them, targets)."""
     rng = np.random.default_rng(SEED + 7)
-    cams, targets = [], []
-    for (w, h) in sizes:
+    views, targets = [], []
+    for (w, h) in BATCHED_SIZES:
         d = rng.normal(size=3)
         d /= np.linalg.norm(d)
         eye = d * rng.uniform(4.0, 8.0)
@@ -481,10 +675,26 @@ def batched_workload(args) -> None:
         view[:3, :3] = rot
         view[:3, 3] = -rot @ eye
         fx = (w / 2) / math.tan(math.radians(30.0))
-        cams.append(splat.Camera(view.astype(np.float32), eye.astype(np.float32), fx, fx, w / 2, h / 2, w, h))
+        views.append((view.astype(np.float32), eye.astype(np.float32), fx, fx, w / 2, h / 2, w, h))
         t = rng.integers(0, 256, h * w * 4, dtype=np.uint8)
         t[3::4] = 255
         targets.append(t)
+    return views, targets
+
+
+def batched_summary(gaussians: int, steps: int, warmup: int) -> dict:
+    """The batched form: 3M Gaussians of SH degree 3 (BF16 above DC), 8 views of
+    uneven sizes per step (one launch per stage for all of them, the
+    rasterizer's two persistent, 64-bit tile|depth keys, CUDA graph), cameras
+    at random points of a sphere of radius
+    4 to 8 looking at the origin. Against the same views one per step: views/s."""
+    import torch
+
+    splat = importlib.import_module("vibe-splat_b200")
+    n = gaussians
+    views, targets = batched_views()
+    sizes = [(v[6], v[7]) for v in views]
+    cams = [splat.Camera(*v) for v in views]
     pos, sc, rot_, op, sh = make_scene(n)
     cloud = splat.GaussianCloud(DEGREE, pos, sc, rot_, op, sh)
     rates = splat.LearningRates()
@@ -492,27 +702,38 @@ def batched_workload(args) -> None:
            "config": {"workload": f"{n} Gaussians, SH degree 3 (BF16 above DC), 8 views "
                                   + ", ".join(f"{w}x{h}" for w, h in sizes)
                                   + ", random poses on a sphere of radius 4-8, 60 deg horizontal fov (synthetic)"},
-           "steps": args.steps, "warmup": args.warmup}
+           "steps": steps, "warmup": warmup}
+    # Every view's tiles in one persistent launch per rasterizer stage.
     opts = chosen_options(splat)
     opts.sort_form = splat.SORT_TILE_DEPTH_64
+    opts.forward_pixels_per_thread = opts.backward_pixels_per_thread = 2
+    opts.persistent_raster = True
     trainer = splat.Trainer(cloud, opts)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         stats = trainer.step_batch(cams, targets, rates)
-    ms = time_steps(torch, trainer, lambda i: trainer.step_batch(cams, targets, rates), args.steps, trainer.stream())
-    out["batched"] = {"views_per_s": 1000.0 * args.steps * len(cams) / ms, "ms_per_step": ms / args.steps,
+    ms = time_steps(torch, trainer, lambda i: trainer.step_batch(cams, targets, rates), steps, trainer.stream())
+    out["batched"] = {"views_per_s": 1000.0 * steps * len(cams) / ms, "ms_per_step": ms / steps,
                       "tile_entries": stats[0].tile_entries}  # every view's stats carry the batch's total
     del trainer
     torch.cuda.empty_cache()
-    single = splat.Trainer(cloud, chosen_options(splat))
-    for i in range(args.warmup * len(cams)):
+    one = chosen_options(splat)
+    one.sort_form = splat.SORT_DEPTH_THEN_TILE
+    one.forward_pixels_per_thread = one.backward_pixels_per_thread = 2
+    single = splat.Trainer(cloud, one)
+    for i in range(warmup * len(cams)):
         single.step(cams[i % len(cams)], targets[i % len(cams)], rates)
     k = len(cams)
     ms1 = time_steps(torch, single, lambda i: single.step(cams[i % k], targets[i % k], rates,
                                                           next_target=targets[(i + 1) % k]),
-                     args.steps * k, single.stream())
-    out["one_view_per_step"] = {"views_per_s": 1000.0 * args.steps * k / ms1, "ms_per_view": ms1 / (args.steps * k)}
+                     steps * k, single.stream())
+    out["one_view_per_step"] = {"views_per_s": 1000.0 * steps * k / ms1, "ms_per_view": ms1 / (steps * k)}
     out["value"] = out["batched"]["views_per_s"]
-    print(json.dumps(out))
+    return out
+
+
+def batched_workload(args) -> None:
+    n = 3_000_000 if args.gaussians == GAUSSIANS else args.gaussians
+    print(json.dumps(batched_summary(n, args.steps, args.warmup)))
 
 
 def slowest_over_ranks(ms: float, dist, device: str) -> float:
@@ -738,18 +959,39 @@ def our_arm(args) -> None:
     if not args.no_plain:
         precision = precision_check(splat, torch, cloud, cams, host_targets, rates, chosen, tuned)
 
+    # Checkers, outside every timed region: the forms against the FP64
+    # oracle on the headline view, and the full training step's adjoint
+    # against FP64 central differences.
+    if precision is not None and not args.no_checks:
+        (v0, p0, fx0, fy0, cx0, cy0, w0, h0) = hemisphere_views()[0]
+        from oracle import oracle as O
+
+        precision["vs_fp64"] = precision_vs_fp64(splat, torch, (pos, sc, rot, op, sh), cams[0],
+                                                 O.View(v0, p0, fx0, fy0, cx0, cy0, w0, h0), host_targets[0],
+                                                 {"chosen": tuned_options(chosen, tuned), "plain": plain_options(splat)})
+    fd2 = fd_config2(splat, torch) if not args.no_checks else None
+
+    # The other measured shapes, compact: 8 uneven views per step (3M
+    # Gaussians) and the memory-bound adjoint (6M Gaussians at 3840x2160).
+    batched = batched_summary(3_000_000, 5, 2) if not args.no_checks else None
+    torch.cuda.empty_cache()
+    memory_adjoint = memory_adjoint_summary(6_000_000, 3, 1) if not args.no_checks else None
+    torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
 
         if O.have_reference():
-            c = O.Cloud(DEGREE, pos, sc, rot, op, sh)
-            (v, p, fx, fy, cx, cy, w, h) = hemisphere_views()[0]
             threads = cpu_count()
-            secs, done = reference_iterations(O, c, [O.View(v, p, fx, fy, cx, cy, w, h)], [host_targets[0]], threads)
-            cpu = {"value": done / secs, "unit": "iters/s", "cores": threads, "kind": "reference",
-                   "sample": f"1 training iteration of the reference's FP64 twin on the same workload, split into "
-                             f"{threads} row bands on {threads} threads ({secs:.1f} s)"}
+            run = twin_views_per_core(O, (pos, sc, rot, op, sh), [O.View(*hemisphere_views()[i % VIEWS]) for i in range(threads)],
+                                      [host_targets[i % len(host_targets)] for i in range(threads)], threads)
+            per_view = float(np.mean(run["per_view_seconds"]))
+            cpu = {"value": run["views"] / run["seconds"], "unit": "iters/s", "cores": threads, "kind": "reference",
+                   "single_thread_seconds_per_view": per_view,
+                   "sample": f"{run['views']} whole views of the same workload, one per host thread on {threads} threads "
+                             f"({run['seconds']:.0f} s): the reference's FP64 twin (render, loss, gradients) and an FP64 "
+                             f"Adam step; {per_view:.0f} s per view on one thread"}
 
     h2d = nbytes + 1240 + 128
     d2h = 160
@@ -769,16 +1011,17 @@ def our_arm(args) -> None:
         "ms_per_step": ms_per_step, "fwd_bwd_ms": sum(stages.get(k, 0.0) for k in ("composite", "loss", "backward")),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; the bicycle photos are not available)",
-        "config": {"workload": WORKLOAD,
-                   "form": f"chosen: BF16 SH + BF16-pair Adam state, {form_name} with {digits}-bit digits, "
-                           f"{tuned.get('forward_pixels_per_thread', chosen.forward_pixels_per_thread)}-pixel compositing, "
-                           f"{tuned.get('backward_pixels_per_thread', chosen.backward_pixels_per_thread)}-pixel float "
-                           f"backward ({'autotuned' if tuned else 'fixed'}), fused one-view chain rule + Adam + SH "
-                           "step, CUDA graph, SFU exp/log",
-                   "autotune_ms": tuned.get("ms"), "layout_ms": tuned.get("layout_ms"),
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (1M-Gaussian parameters and state, 64 x 4 MB targets)",
-                   "tile_entries": entries, "visible_splats": visible},
+        "config": dict(bench_config(), parallelism=f"replicas x{world}"),
+        "form": f"chosen: BF16 SH + BF16-pair Adam state, {form_name} with {digits}-bit digits, "
+                f"{tuned.get('forward_pixels_per_thread', chosen.forward_pixels_per_thread)}-pixel compositing, "
+                f"{tuned.get('backward_pixels_per_thread', chosen.backward_pixels_per_thread)}-pixel float "
+                f"backward, {tuned.get('tile_size', chosen.tile_size)}x{tuned.get('tile_size', chosen.tile_size)} tiles, "
+                f"batches of {tuned.get('batch_depth', chosen.batch_depth)}, "
+                f"{'persistent' if tuned.get('persistent_raster', chosen.persistent_raster) else 'one block per tile'} "
+                f"({'autotuned' if tuned else 'fixed'}), fused one-view chain rule + Adam + SH "
+                "step, CUDA graph, SFU exp/log",
+        "autotune": {"ms": tuned.get("ms"), "layout_ms": tuned.get("layout_ms"), "tile_ms": tuned.get("tile_ms")},
+        "workload_counts": {"tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "sm_peaks": sm_peaks,
         "score_view_ms": score_ms,
@@ -789,6 +1032,9 @@ def our_arm(args) -> None:
         "stages_ms": stages,
         "plain_fp32": plain,
         "precision": precision,
+        "fd_config2": fd2,
+        "batched": batched,
+        "memory_adjoint": memory_adjoint,
         "speedup_vs_plain": (value / world) / plain["iters_per_s"] if plain else None,
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -867,6 +1113,8 @@ def main() -> None:
     parser.add_argument("--no-plain", action="store_true", help="skip the plain FP32 form")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--no-densify", action="store_true", help="skip the densification timing")
+    parser.add_argument("--no-checks", action="store_true",
+                        help="skip the FP64 checks and the batched and memory-bound summaries")
     parser.add_argument("--reference-warmup", action="store_true", help="run warm-up steps in the reference arm too")
     parser.add_argument("--no-autotune", action="store_true", help="keep the chosen form's sort settings")
     parser.add_argument("--sort-form", type=int, choices=[0, 1], default=None,

@@ -103,6 +103,13 @@ typedef struct splat_trainer_options {
                                  each, and the backward walks those lists (float sums, one view, no CUDA
                                  graph: the list total is read back before the recording pass). For
                                  comparison of memory and speed. */
+  int32_t tile_size;          /* rasterizer tile edge in pixels: 16 (the reference's; 0 picks it) or 32. 32
+                                 applies where both rasterizer kernels take two pixels per thread and the sums
+                                 are float (not with force_fixed_point or blend_lists); elsewhere the tile stays
+                                 16. Images are the same bits either way. */
+  int32_t batch_depth;        /* splats the two-pixel kernels stage per round: 128 or 256 (0 picks 256) */
+  int32_t persistent_raster;  /* 1: the two-pixel kernels run as persistent launches, resident blocks taking
+                                 the tiles of every view of the step from one counter; 0: one block per tile */
 } splat_trainer_options;
 
 /* LearningRates (src/train/trainer.hpp:51-61); trust_region must be 0. */
@@ -465,13 +472,21 @@ typedef struct splat_autotune_result {
   int32_t backward_pixels_per_thread; /* the backward layout kept */
   double ms[2][3];         /* milliseconds per gradient pass, [sort form][digit bits - 6], starting layouts */
   double layout_ms[2][2];  /* milliseconds per gradient pass, [forward pixels - 1][backward pixels - 1], best sort */
+  int32_t tile_size;       /* the rasterizer tile kept (16 unless both layouts take two pixels per thread) */
+  int32_t batch_depth;     /* the batch depth kept */
+  int32_t persistent_raster; /* the launch form kept */
+  double tile_ms[2][2][2]; /* milliseconds per gradient pass, [tile 16/32][batch 128/256][persistent 0/1], best
+                              layouts (0 where not timed) */
 } splat_autotune_result;
 
 /* The autotuner (new in this library; the reference has fixed 16x16 tiles and
  * 8-bit digits): times every tile-sort form and radix digit width on this view
  * with gradient passes (which change neither the parameters, the optimiser
- * state nor the densification statistics), `repeats` passes each, and keeps
- * the fastest for the following steps. */
+ * state nor the densification statistics), `repeats` passes each, then the
+ * rasterizer's pixel layouts, then, where both layouts take two pixels per
+ * thread and the sums are float, its tile edge (16, 32), batch depth (128,
+ * 256) and launch form (one block per tile, persistent), and keeps the
+ * fastest for the following steps. */
 int splat_trainer_autotune(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
                            int32_t repeats, splat_autotune_result *result);
 /* Turns per-stage CUDA-event timing on or off (off by default: it serialises). */
@@ -560,6 +575,15 @@ typedef struct splat_sm_peaks {
   double warp_instructions;
 } splat_sm_peaks;
 int splat_measure_sm_peaks(splat_sm_peaks *out);
+
+/* Sets how many times a radix sort pass polls a predecessor's look-back word
+ * before it gives up (the default, 2^20, when polls is negative). A pass that
+ * gives up sets the look-back timeout bit: the call returns SPLAT_ERR_DEVICE
+ * and its output is not sorted, but no write leaves the arrays. For the tests
+ * of that failure path; applies to sorts launched after the call (a captured
+ * step keeps the limit it was captured with). This entry point has no
+ * counterpart in the reference. */
+int splat_debug_set_wait_limit(int32_t polls);
 
 /* Evaluates the deterministic exp and log of splat_detmath.h on the device, for
  * the check that they agree bit for bit with the host. Device pointers. */

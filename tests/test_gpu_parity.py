@@ -377,6 +377,53 @@ def test_pixel_layouts_agree(splat, oracle, exact):
         check_close(getattr(out[0][2], name), getattr(out[1][2], name), name, 0.99999, 1e-4)
 
 
+@pytest.mark.parametrize("exact", [True, False])
+def test_tile_batch_and_launch_forms_agree(splat, oracle, exact):
+    # The two-pixel kernels at every tile edge, batch depth and launch form:
+    # each pixel blends the same splats in the same order with the same
+    # arithmetic, so the image is the same bits as the one-pixel reference
+    # layout's; float sums in another order, so gradients to rounding. The
+    # view (100x75) leaves partial tiles at both edges for either tile edge.
+    view = oracle.train_camera(100, 75)
+    target = oracle.smooth_target(100, 75, 5)
+    cloud = oracle.random_cloud(500, 1, 37)
+    base = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(exact_math=exact))
+    image0 = base.render(to_camera(view))
+    base.compute_gradients(to_camera(view), target)
+    g0 = base.gradients()
+    for tile in (16, 32):
+        for batch in (128, 256):
+            for persistent in (False, True):
+                opts = splat.TrainerOptions(exact_math=exact, forward_pixels_per_thread=2, backward_pixels_per_thread=2,
+                                            tile_size=tile, batch_depth=batch, persistent_raster=persistent)
+                t = splat.Trainer(to_cloud(cloud), opts)
+                image = t.render(to_camera(view))
+                np.testing.assert_array_equal(image.view(np.uint32), image0.view(np.uint32),
+                                              err_msg=f"tile {tile} batch {batch} persistent {persistent}")
+                t.compute_gradients(to_camera(view), target)
+                g = t.gradients()
+                for name in ("positions", "scales", "rotations", "opacities", "sh"):
+                    check_close(getattr(g, name), getattr(g0, name), f"{name} t{tile} b{batch} p{int(persistent)}",
+                                0.99999, 1e-4)
+
+
+def test_batched_persistent_matches_single_views(splat, oracle):
+    # Several views of uneven size in one persistent launch per stage, 32 x 32
+    # tiles: each view's loss equals that view's alone (the same tiles, lists
+    # and arithmetic), whichever block took which tile.
+    cloud = oracle.random_cloud(3000, 1, 19)
+    views = [oracle.train_camera(w, h) for (w, h) in ((64, 48), (100, 75), (48, 96))]
+    targets = [oracle.smooth_target(v.width, v.height, 3 + k) for k, v in enumerate(views)]
+    opts = splat.TrainerOptions(sort_form=splat.SORT_TILE_DEPTH_64, exact_math=False, forward_pixels_per_thread=2,
+                                backward_pixels_per_thread=2, tile_size=32, persistent_raster=True)
+    single = splat.Trainer(to_cloud(cloud), opts)
+    alone = [single.compute_gradients(to_camera(v), t).loss for v, t in zip(views, targets)]
+    batch = splat.Trainer(to_cloud(cloud), opts)
+    stats = batch.step_batch([to_camera(v) for v in views], targets, splat.LearningRates())
+    for a, b in zip([s.loss for s in stats], alone):
+        assert abs(a - b) < 1e-6
+
+
 def _relative_error(a, b) -> float:
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()

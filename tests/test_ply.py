@@ -73,7 +73,7 @@ def test_loader_refuses_files_that_are_not_splats(S, tmp_path):
     path = tmp_path / "mesh.ply"
     path.write_text("ply\nformat ascii 1.0\nelement vertex 1\nproperty float x\nproperty float y\nproperty float z\n"
                     "end_header\n0 0 0\n")
-    with pytest.raises(S.SplatError, match="missing property"):
+    with pytest.raises(S.SplatError, match="missing property: "):
         S.load_ply(path)
     with pytest.raises(S.SplatError):
         S.load_ply(tmp_path / "absent.ply")

@@ -73,6 +73,9 @@ class _Options(ctypes.Structure):
         ("backward_pixels_per_thread", ctypes.c_int32),
         ("split_step", ctypes.c_int32),
         ("blend_lists", ctypes.c_int32),
+        ("tile_size", ctypes.c_int32),
+        ("batch_depth", ctypes.c_int32),
+        ("persistent_raster", ctypes.c_int32),
     ]
 
 
@@ -146,7 +149,9 @@ _lib.splat_trainer_stream.argtypes = [_P, ctypes.POINTER(_P)]
 class _Autotune(ctypes.Structure):
     _fields_ = [("sort_form", ctypes.c_int32), ("digit_bits", ctypes.c_int32),
                 ("forward_pixels_per_thread", ctypes.c_int32), ("backward_pixels_per_thread", ctypes.c_int32),
-                ("ms", (ctypes.c_double * 3) * 2), ("layout_ms", (ctypes.c_double * 2) * 2)]
+                ("ms", (ctypes.c_double * 3) * 2), ("layout_ms", (ctypes.c_double * 2) * 2),
+                ("tile_size", ctypes.c_int32), ("batch_depth", ctypes.c_int32), ("persistent_raster", ctypes.c_int32),
+                ("tile_ms", ((ctypes.c_double * 2) * 2) * 2)]
 
 
 _lib.splat_trainer_autotune.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_int32,
@@ -425,6 +430,9 @@ class TrainerOptions:
     backward_pixels_per_thread: int = 2
     split_step: bool = False
     blend_lists: bool = False
+    tile_size: int = 16
+    batch_depth: int = 256
+    persistent_raster: bool = False
 
     def _c(self) -> _Options:
         o = _Options()
@@ -443,6 +451,8 @@ class TrainerOptions:
         o.backward_pixels_per_thread = self.backward_pixels_per_thread
         o.split_step = int(self.split_step)
         o.blend_lists = int(self.blend_lists)
+        o.tile_size, o.batch_depth = self.tile_size, self.batch_depth
+        o.persistent_raster = int(self.persistent_raster)
         return o
 
 
@@ -698,8 +708,9 @@ class Trainer:
 
     def autotune(self, camera: Camera, target, repeats: int = 3) -> dict:
         """Times each tile-sort form and radix digit width, then each forward and
-        backward pixel layout, on this view with gradient passes (no parameter
-        changes) and keeps the fastest."""
+        backward pixel layout, then (two-pixel float layouts) each tile edge,
+        batch depth and launch form, on this view with gradient passes (no
+        parameter changes) and keeps the fastest."""
         t, p, n = _target_ptr(target)
         r = _Autotune()
         _check(_lib.splat_trainer_autotune(self._h, ctypes.byref(camera._c()), p, n, int(repeats), ctypes.byref(r)))
@@ -707,7 +718,10 @@ class Trainer:
                 "forward_pixels_per_thread": r.forward_pixels_per_thread,
                 "backward_pixels_per_thread": r.backward_pixels_per_thread,
                 "ms": {f"form{f}/digits{d + 6}": r.ms[f][d] for f in range(2) for d in range(3)},
-                "layout_ms": {f"fwd{f + 1}/bwd{b + 1}": r.layout_ms[f][b] for f in range(2) for b in range(2)}}
+                "layout_ms": {f"fwd{f + 1}/bwd{b + 1}": r.layout_ms[f][b] for f in range(2) for b in range(2)},
+                "tile_size": r.tile_size, "batch_depth": r.batch_depth, "persistent_raster": r.persistent_raster,
+                "tile_ms": {f"tile{16 * (t + 1)}/batch{128 * (b + 1)}/persistent{q}": r.tile_ms[t][b][q]
+                            for t in range(2) for b in range(2) for q in range(2) if r.tile_ms[t][b][q] > 0}}
 
     def stream(self) -> int:
         """The cudaStream_t the trainer runs on, as an integer handle."""

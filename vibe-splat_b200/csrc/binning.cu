@@ -23,13 +23,15 @@ struct TileRect {
   uint32_t x0, y0, x1, y1; // inclusive
 };
 
-// Covered tiles of a splat, inclusive (splat_tiles).
-__device__ __forceinline__ TileRect splat_tiles(const float4 ce, int gridW, int gridH) {
+// Covered tiles of a splat, inclusive (splat_tiles), for tiles of T x T
+// pixels (the reference's 16, or 32; a power of two, so the divisions are
+// exact scalings and T = 16 gives the reference's expressions' bits).
+__device__ __forceinline__ TileRect splat_tiles(const float4 ce, int gridW, int gridH, float T) {
   const float lastX = (float)(gridW - 1), lastY = (float)(gridH - 1);
-  const float lx = fminf(fmaxf(floorf((ce.x - ce.z - 1.0f) / 16.0f), 0.0f), lastX);
-  const float ly = fminf(fmaxf(floorf((ce.y - ce.w - 1.0f) / 16.0f), 0.0f), lastY);
-  const float hx = fminf(fmaxf(floorf((ce.x + ce.z + 1.0f) / 16.0f), 0.0f), lastX);
-  const float hy = fminf(fmaxf(floorf((ce.y + ce.w + 1.0f) / 16.0f), 0.0f), lastY);
+  const float lx = fminf(fmaxf(floorf((ce.x - ce.z - 1.0f) / T), 0.0f), lastX);
+  const float ly = fminf(fmaxf(floorf((ce.y - ce.w - 1.0f) / T), 0.0f), lastY);
+  const float hx = fminf(fmaxf(floorf((ce.x + ce.z + 1.0f) / T), 0.0f), lastX);
+  const float hy = fminf(fmaxf(floorf((ce.y + ce.w + 1.0f) / T), 0.0f), lastY);
   return {(uint32_t)lx, (uint32_t)ly, (uint32_t)hx, (uint32_t)hy};
 }
 
@@ -47,19 +49,19 @@ struct RowTangents {
   float lowY, highY, uLow, uHigh; // edge offsets from the centre and their unclamped tangent x
 };
 
-__device__ __forceinline__ ColTangents col_tangents(const float4 q, const float4 ce, uint32_t tx) {
+__device__ __forceinline__ ColTangents col_tangents(const float4 q, const float4 ce, uint32_t tx, float T) {
   ColTangents c;
-  c.lowX = ((float)tx * 16.0f + 0.5f) - ce.x;
-  c.highX = c.lowX + 15.0f;
+  c.lowX = ((float)tx * T + 0.5f) - ce.x;
+  c.highX = c.lowX + (T - 1.0f);
   c.yLow = -q.y * c.lowX / q.z;
   c.yHigh = -q.y * c.highX / q.z;
   return c;
 }
 
-__device__ __forceinline__ RowTangents row_tangents(const float4 q, const float4 ce, uint32_t ty) {
+__device__ __forceinline__ RowTangents row_tangents(const float4 q, const float4 ce, uint32_t ty, float T) {
   RowTangents r;
-  r.lowY = ((float)ty * 16.0f + 0.5f) - ce.y;
-  r.highY = r.lowY + 15.0f;
+  r.lowY = ((float)ty * T + 0.5f) - ce.y;
+  r.highY = r.lowY + (T - 1.0f);
   r.uLow = -q.y * r.lowY / q.x;
   r.uHigh = -q.y * r.highY / q.x;
   return r;
@@ -95,11 +97,11 @@ __device__ __forceinline__ uint32_t rect_area(const TileRect &t) { return (t.x1 
 // A large rectangle's tangent tables, filled by the whole warp. False (and
 // nothing filled) when the rectangle is wider or taller than the tables.
 __device__ __forceinline__ bool fill_tables(const float4 q, const float4 ce, const TileRect &t, uint32_t lane, ColTangents *cols,
-                                            RowTangents *rows) {
+                                            RowTangents *rows, float T) {
   const uint32_t width = t.x1 - t.x0 + 1u, height = t.y1 - t.y0 + 1u;
   if (width > kTableMax || height > kTableMax) return false;
-  for (uint32_t c = lane; c < width; c += 32u) cols[c] = col_tangents(q, ce, t.x0 + c);
-  for (uint32_t r = lane; r < height; r += 32u) rows[r] = row_tangents(q, ce, t.y0 + r);
+  for (uint32_t c = lane; c < width; c += 32u) cols[c] = col_tangents(q, ce, t.x0 + c, T);
+  for (uint32_t r = lane; r < height; r += 32u) rows[r] = row_tangents(q, ce, t.y0 + r, T);
   __syncwarp();
   return true;
 }
@@ -110,7 +112,8 @@ __device__ __forceinline__ bool fill_tables(const float4 q, const float4 ce, con
 // 1/(2 width) from an integer, far more than the rounding error.
 __device__ __forceinline__ uint32_t warp_reach(const float4 q, const float4 ce, float reach, const TileRect &t, uint32_t width,
                                                float invWidth, uint32_t area, uint32_t base, uint32_t lane,
-                                               const ColTangents *cols, const RowTangents *rows, uint32_t &x, uint32_t &y) {
+                                               const ColTangents *cols, const RowTangents *rows, uint32_t &x, uint32_t &y,
+                                               float T) {
   const uint32_t li = base + lane;
   bool hit = false;
   if (li < area) {
@@ -119,7 +122,7 @@ __device__ __forceinline__ uint32_t warp_reach(const float4 q, const float4 ce, 
     x = t.x0 + c;
     y = t.y0 + r;
     hit = cols != nullptr ? reaches_tile(q, reach, cols[c], rows[r])
-                          : reaches_tile(q, reach, col_tangents(q, ce, x), row_tangents(q, ce, y));
+                          : reaches_tile(q, reach, col_tangents(q, ce, x, T), row_tangents(q, ce, y, T));
   }
   return __ballot_sync(0xFFFFFFFFu, hit);
 }
@@ -147,6 +150,7 @@ __global__ void __launch_bounds__(kCountThreads)
                 uint32_t *__restrict__ counts, uint32_t *__restrict__ masks, uint32_t *counters) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
+  const float T = (float)views.tileSize;
   __shared__ ColTangents s_cols[kCountThreads / 32][kTableMax];
   __shared__ RowTangents s_rows[kCountThreads / 32][kTableMax];
   __shared__ uint32_t s_mask[kCountThreads / 32][32];
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(kCountThreads)
     cq = splats[s].conicOpacity;
     rc = reach[s];
     const ViewParams &cam = views.v[item_view(s, n, views.count)];
-    rect = splat_tiles(ce, cam.gridW, cam.gridH);
+    rect = splat_tiles(ce, cam.gridW, cam.gridH, T);
     area = rect_area(rect);
   }
   const uint32_t visibleLanes = __ballot_sync(0xFFFFFFFFu, valid);
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(kCountThreads)
       const float oinv = __shfl_sync(0xFFFFFFFFu, invWidth, owner);
       if (f < total) {
         const uint32_t row = (uint32_t)(((float)li + 0.5f) * oinv), col = li - row * ow;
-        if (reaches_tile(oq, orc, col_tangents(oq, oce, ox0 + col), row_tangents(oq, oce, oy0 + row)))
+        if (reaches_tile(oq, orc, col_tangents(oq, oce, ox0 + col, T), row_tangents(oq, oce, oy0 + row, T)))
           atomicOr(&s_mask[warp][owner], 1u << li);
       }
     }
@@ -221,14 +225,14 @@ __global__ void __launch_bounds__(kCountThreads)
     const ViewParams &cam = views.v[item_view(bs, n, views.count)];
     const Splat sp = splats[bs];
     const float rcb = reach[bs];
-    const TileRect bt = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    const TileRect bt = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH, T);
     const uint32_t width = bt.x1 - bt.x0 + 1u, barea = rect_area(bt);
-    const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, bt, lane, s_cols[warp], s_rows[warp]);
+    const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, bt, lane, s_cols[warp], s_rows[warp], T);
     const float invWidth = 1.0f / (float)width;
     uint32_t total = 0, hits = 0, x = 0, y = 0;
     for (uint32_t base = 0; base < barea; base += 32u) {
       hits = warp_reach(sp.conicOpacity, sp.centerExtent, rcb, bt, width, invWidth, barea, base, lane,
-                        tables ? s_cols[warp] : nullptr, s_rows[warp], x, y);
+                        tables ? s_cols[warp] : nullptr, s_rows[warp], x, y, T);
       total += (uint32_t)__popc(hits);
     }
     __syncwarp(); // the tables are read before the next rectangle fills them
@@ -354,6 +358,7 @@ __global__ void __launch_bounds__(256)
                uint32_t *error) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
+  const float T = (float)views.tileSize;
   __shared__ ColTangents s_cols[8][kTableMax];
   __shared__ RowTangents s_rows[8][kTableMax];
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(256)
   const uint32_t s = valid ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
   const int view = valid ? item_view(s, n, views.count) : 0;
   TileRect t{0u, 0u, 0u, 0u};
-  if (valid) t = splat_tiles(splats[s].centerExtent, views.v[view].gridW, views.v[view].gridH);
+  if (valid) t = splat_tiles(splats[s].centerExtent, views.v[view].gridW, views.v[view].gridH, T);
   const uint32_t width = t.x1 - t.x0 + 1u, area = valid ? rect_area(t) : 0u;
   const bool big = area > 32u;
   const uint32_t mask = valid && !big ? masks[masksBySplat ? s : r] : 0u;
@@ -435,15 +440,15 @@ __global__ void __launch_bounds__(256)
     const ViewParams &cam = views.v[bView];
     const Splat sp = splats[bs];
     const float rc = reach[bs];
-    const TileRect bt = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH);
+    const TileRect bt = splat_tiles(sp.centerExtent, cam.gridW, cam.gridH, T);
     const uint32_t bWidth = bt.x1 - bt.x0 + 1u, bArea = rect_area(bt);
-    const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, bt, lane, s_cols[warp], s_rows[warp]);
+    const bool tables = fill_tables(sp.conicOpacity, sp.centerExtent, bt, lane, s_cols[warp], s_rows[warp], T);
     const float invWidth = 1.0f / (float)bWidth;
     uint32_t slot = bFirst;
     for (uint32_t base = 0; base < bArea; base += 32u) {
       uint32_t x = 0, y = 0;
       const uint32_t hits = warp_reach(sp.conicOpacity, sp.centerExtent, rc, bt, bWidth, invWidth, bArea, base, lane,
-                                       tables ? s_cols[warp] : nullptr, s_rows[warp], x, y);
+                                       tables ? s_cols[warp] : nullptr, s_rows[warp], x, y, T);
       if ((hits >> lane) & 1u) put(slot + (uint32_t)__popc(hits & ((1u << lane) - 1u)), bView, x, y, key, bs);
       slot += (uint32_t)__popc(hits);
     }

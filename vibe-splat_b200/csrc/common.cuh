@@ -14,6 +14,8 @@
 namespace sb {
 
 // Reference constants (shaders/train_types.glsl:6-15, src/train/trainer.cpp:22-24).
+// The reference's tile (16 x 16 pixels): the binning and rasterizer's default
+// and the loss's tile. The float two-pixel rasterizer also runs 32 x 32 tiles.
 constexpr int kTileSize = 16;
 constexpr int kTilePixels = kTileSize * kTileSize;
 constexpr uint32_t kInvisible = 0xFFFFFFFFu;
@@ -55,7 +57,10 @@ struct ViewParams {
   float fixedScale;    // 3 W H 64, the fixed-point resolution
   int activeDegree;    // SH degree in use
   int activeCoeffs;    // (degree + 1)^2
-  int pad[2];
+  // The loss's own grid of 16 x 16 tiles (the rasterizer's tile may be larger).
+  int lossGridW, lossGridH;
+  int lossTileBase;    // first global loss tile of this view
+  int lossTileCount;
 };
 
 // A projected splat, 48 bytes (shaders/train_types.glsl:26-31 TrainSplat):

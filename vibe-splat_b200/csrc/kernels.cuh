@@ -11,11 +11,17 @@
 namespace sb {
 
 constexpr int kMaxViews = 8;
+// Several views of one step. The rasterizer's tiles are tileSize x tileSize
+// pixels (16, the reference's, or 32), numbered view by view from each view's
+// tileBase; the loss works on its own grid of 16 x 16 tiles (lossTileBase,
+// totalLossTiles), whatever the rasterizer's tile.
 struct ViewSet {
   ViewParams v[kMaxViews];
   int count;
   int totalTiles;
   long long totalPixels;
+  int tileSize;
+  int totalLossTiles;
 };
 
 // SH storage of the coefficients above degree 0 (the DC term is always FP32).
@@ -103,6 +109,14 @@ struct RasterConfig {
   int forwardPixels = 1;
   int backwardPixels = 2; // float backward only; the fixed-point sums keep 1
   float background[3] = {0.f, 0.f, 0.f};
+  // The two-pixel kernels' tile edge (16 or 32; views.tileSize must agree)
+  // and batch depth (splats staged per round: 128 or 256), and, for a
+  // persistent launch, each kernel's tile counter (zeroed before the launch;
+  // null: one block per tile).
+  int tile = 16;
+  int batch = 256;
+  uint32_t *workForward = nullptr;
+  uint32_t *workBackward = nullptr;
 };
 
 // train_forward.comp: one block per tile of 16x16 pixels. image: 4 floats per
@@ -115,7 +129,7 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
                     cudaStream_t stream, int listMode = 0, BlendLists lists = BlendLists{});
 
 // train_ssim.comp + train_loss.comp: SSIM fields, then the adjoint and L1.
-// partials: 2 floats per global tile (SSIM sum, L1 sum).
+// partials: 2 floats per global loss tile (SSIM sum, L1 sum).
 void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
                  cudaStream_t stream);
 // A scored view (Trainer::score_view): with edge not null the loss also leaves

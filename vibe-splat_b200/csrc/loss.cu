@@ -45,7 +45,7 @@ __device__ __forceinline__ float3 unpack_unorm(uint32_t v) {
 
 __device__ __forceinline__ int view_of_tile(const ViewSet &views, int tile) {
   int v = 0;
-  while (v + 1 < views.count && tile >= views.v[v + 1].tileBase) ++v;
+  while (v + 1 < views.count && tile >= views.v[v + 1].lossTileBase) ++v;
   return v;
 }
 
@@ -170,8 +170,8 @@ struct TileOrigin {
 
 __device__ __forceinline__ TileOrigin tile_origin(const ViewSet &views, int tile) {
   const ViewParams &cam = views.v[view_of_tile(views, tile)];
-  const int local = tile - cam.tileBase;
-  return TileOrigin{&cam, (local % cam.gridW) * kTileSize, (local / cam.gridW) * kTileSize};
+  const int local = tile - cam.lossTileBase;
+  return TileOrigin{&cam, (local % cam.lossGridW) * kTileSize, (local / cam.lossGridW) * kTileSize};
 }
 
 __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
@@ -384,8 +384,8 @@ __global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ 
   const int v = blockIdx.x;
   const ViewParams &cam = views.v[v];
   double ssim = 0.0, l1 = 0.0;
-  for (int i = threadIdx.x; i < cam.tileCount; i += 256) {
-    const float2 p = partials[cam.tileBase + i];
+  for (int i = threadIdx.x; i < cam.lossTileCount; i += 256) {
+    const float2 p = partials[cam.lossTileBase + i];
     ssim += (double)p.x;
     l1 += (double)p.y;
   }
@@ -409,19 +409,19 @@ __global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ 
 
 void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
                  cudaStream_t stream) {
-  if (views.totalTiles == 0) return;
-  launch_chained(k_ssim, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, dViews, reinterpret_cast<float *>(fields), partials);
+  if (views.totalLossTiles == 0) return;
+  launch_chained(k_ssim, dim3(views.totalLossTiles), dim3(kTilePixels), 0, stream, image, target, dViews, reinterpret_cast<float *>(fields), partials);
 }
 
 void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
                  float4 *adjoint, float2 *partials, cudaStream_t stream, LossScoring scoring) {
-  if (views.totalTiles == 0) return;
+  if (views.totalLossTiles == 0) return;
   const float *f = reinterpret_cast<const float *>(fields);
   if (scoring.edge != nullptr)
-    launch_chained(k_loss<true>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
+    launch_chained(k_loss<true>, dim3(views.totalLossTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
                    partials, scoring);
   else
-    launch_chained(k_loss<false>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
+    launch_chained(k_loss<false>, dim3(views.totalLossTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
                    partials, scoring);
 }
 

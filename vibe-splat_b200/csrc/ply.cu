@@ -139,27 +139,33 @@ struct Layout {
 };
 
 Layout layout_of(const PlyHeader &h, const std::string &path) {
-  std::unordered_map<std::string, size_t> at;
-  for (size_t i = 0; i < h.columns.size(); ++i) at[h.columns[i].name] = i;
-  const auto need = [&](const std::string &name) {
-    const auto it = at.find(name);
-    if (it == at.end()) throw std::runtime_error(path + ": missing property '" + name + "' (is this a Gaussian splat file?)");
-    return it->second;
+  std::unordered_map<std::string, size_t> column;
+  for (size_t i = 0; i < h.columns.size(); ++i) column[h.columns[i].name] = i;
+  // Every property a splat needs, looked up at once; one message names all
+  // the missing ones.
+  std::string missing;
+  const auto find = [&](const std::string &name) -> size_t {
+    const auto it = column.find(name);
+    if (it != column.end()) return it->second;
+    missing += (missing.empty() ? "" : ", ") + name;
+    return 0;
   };
-  size_t rest = 0;
-  while (at.count("f_rest_" + std::to_string(rest))) ++rest;
   Layout l;
+  size_t rest = 0;
+  while (column.count("f_rest_" + std::to_string(rest)) != 0) ++rest;
   l.degree = degree_of_rest(rest);
-  if (l.degree < 0) throw std::runtime_error(path + ": unexpected number of f_rest properties (" + std::to_string(rest) + ")");
-  const char *axes = "xyz";
+  static const char *const kAxes[3] = {"x", "y", "z"};
   for (int a = 0; a < 3; ++a) {
-    l.position[a] = need(std::string(1, axes[a]));
-    l.scale[a] = need("scale_" + std::to_string(a));
-    l.dc[a] = need("f_dc_" + std::to_string(a));
+    l.position[a] = find(kAxes[a]);
+    l.scale[a] = find("scale_" + std::to_string(a));
+    l.dc[a] = find("f_dc_" + std::to_string(a));
   }
-  for (int a = 0; a < 4; ++a) l.rotation[a] = need("rot_" + std::to_string(a));
-  l.opacity = need("opacity");
-  for (size_t i = 0; i < rest; ++i) l.rest.push_back(at.at("f_rest_" + std::to_string(i)));
+  for (int a = 0; a < 4; ++a) l.rotation[a] = find("rot_" + std::to_string(a));
+  l.opacity = find("opacity");
+  if (!missing.empty()) throw std::runtime_error(path + ": not a Gaussian splat file, missing property: " + missing);
+  if (l.degree < 0)
+    throw std::runtime_error(path + ": " + std::to_string(rest) + " f_rest properties, where a splat file has 0, 9, 24 or 45");
+  for (size_t i = 0; i < rest; ++i) l.rest.push_back(column.at("f_rest_" + std::to_string(i)));
   return l;
 }
 
@@ -200,15 +206,21 @@ Cloud load(const std::string &path, bool headerOnly) {
   c.opacities.resize(c.count);
   c.sh.resize(c.count * coeffs * 3);
   std::vector<float> values(h.columns.size());
+  const auto short_file = [&](size_t read) {
+    return std::runtime_error(path + ": the file ends after " + std::to_string(read) + " of " + std::to_string(c.count) +
+                              " vertices");
+  };
   if (h.binary) {
-    constexpr size_t kChunk = 1 << 16;
-    std::vector<unsigned char> chunk(h.recordBytes * kChunk);
-    for (size_t first = 0; first < c.count; first += kChunk) {
-      const size_t n = std::min(kChunk, c.count - first);
-      in.read(reinterpret_cast<char *>(chunk.data()), (std::streamsize)(n * h.recordBytes));
-      if ((size_t)in.gcount() != n * h.recordBytes) throw std::runtime_error(path + ": file is truncated");
+    // Whole vertices in blocks of about 16 MB.
+    const size_t perBlock = std::max<size_t>(1, ((size_t)16 << 20) / std::max<size_t>(h.recordBytes, 1));
+    std::vector<unsigned char> block(h.recordBytes * std::min(perBlock, std::max<size_t>(c.count, 1)));
+    for (size_t first = 0; first < c.count; first += perBlock) {
+      const size_t n = std::min(perBlock, c.count - first);
+      in.read(reinterpret_cast<char *>(block.data()), (std::streamsize)(n * h.recordBytes));
+      const size_t got = (size_t)in.gcount();
+      if (got != n * h.recordBytes) throw short_file(first + got / std::max<size_t>(h.recordBytes, 1));
       for (size_t i = 0; i < n; ++i) {
-        const unsigned char *record = chunk.data() + i * h.recordBytes;
+        const unsigned char *record = block.data() + i * h.recordBytes;
         if (h.allFloat) {
           std::memcpy(values.data(), record, h.recordBytes);
         } else {
@@ -221,7 +233,7 @@ Cloud load(const std::string &path, bool headerOnly) {
     for (size_t v = 0; v < c.count; ++v) {
       for (size_t p = 0; p < h.columns.size(); ++p) {
         double d = 0.0;
-        if (!(in >> d)) throw std::runtime_error(path + ": file is truncated");
+        if (!(in >> d)) throw short_file(v);
         values[p] = (float)d;
       }
       store_vertex(l, values.data(), c, v);

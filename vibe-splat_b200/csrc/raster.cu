@@ -19,6 +19,11 @@
 //     reference's per-warp global atomics, with up to 8 times fewer of them.
 //     Float: the same shared-memory pre-aggregation (float atomics are not
 //     order-deterministic in the reference either).
+#include <algorithm>
+#include <mutex>
+#include <unordered_map>
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace sb {
@@ -41,7 +46,8 @@ struct __align__(16) Staged {
   float g, b, qx, qy;
   float qz;
   uint32_t index;
-  float pad0, pad1;
+  uint32_t maskHi; // 32 x 32 tiles: the row bits (the column bits are in mask)
+  float pad1;
 };
 
 __device__ __forceinline__ uint32_t to_u32_clamped(float v) { return (uint32_t)fminf(v, 4294967040.0f); }
@@ -72,8 +78,8 @@ __device__ __forceinline__ uint32_t pixel_masks(const Splat &s, uint32_t x0, uin
   return mask;
 }
 
-template <class M>
-__device__ __forceinline__ Staged stage(const Splat &s, uint32_t index, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+// Every field of a staged splat but its pixel masks.
+template <class M> __device__ __forceinline__ Staged stage_fields(const Splat &s, uint32_t index) {
   Staged out;
   out.cx = s.centerExtent.x;
   out.cy = s.centerExtent.y;
@@ -88,11 +94,57 @@ __device__ __forceinline__ Staged stage(const Splat &s, uint32_t index, uint32_t
   out.qx = s.conicOpacity.x;
   out.qy = s.conicOpacity.y;
   out.qz = s.conicOpacity.z;
-  out.mask = pixel_masks(s, x0, y0, x1, y1);
+  out.mask = 0u;
   out.index = index;
-  out.pad0 = 0.0f;
+  out.maskHi = 0u;
   out.pad1 = 0.0f;
   return out;
+}
+
+template <class M>
+__device__ __forceinline__ Staged stage(const Splat &s, uint32_t index, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+  Staged out = stage_fields<M>(s, index);
+  out.mask = pixel_masks(s, x0, y0, x1, y1);
+  return out;
+}
+
+// The tiles of the float two-pixel rasterizer: T x T pixels, T * T / 2
+// threads, one warp per 8 x 8 block of pixels (two pixels per lane). A
+// staged splat's pixel mask has T column bits then T row bits: 32 bits for
+// the reference's 16 x 16 tiles, 64 for 32 x 32 ones.
+template <int T> struct TileShape {
+  static constexpr int kThreads = T * T / 2;
+  static constexpr int kWarps = kThreads / 32;
+  static constexpr int kBlocksX = T / 8;
+  using Mask = typename std::conditional<(T > 16), unsigned long long, uint32_t>::type;
+};
+
+// splat_pixels() and the radius test of splat_at() per column and per row of
+// a tile of T pixels (pixel_masks for any T).
+template <int T>
+__device__ __forceinline__ typename TileShape<T>::Mask pixel_masks_t(const Splat &s, uint32_t x0, uint32_t y0, uint32_t x1,
+                                                                     uint32_t y1) {
+  using Mask = typename TileShape<T>::Mask;
+  const float cx = s.centerExtent.x, cy = s.centerExtent.y, ex = s.centerExtent.z, ey = s.centerExtent.w;
+  const float r = s.colorRadius.w;
+  const uint32_t ax0 = max(to_u32_clamped(fmaxf(cx - ex - 0.5f, 0.0f)), x0);
+  const uint32_t ay0 = max(to_u32_clamped(fmaxf(cy - ey - 0.5f, 0.0f)), y0);
+  const uint32_t ax1 = min(to_u32_clamped(fmaxf(cx + ex + 0.5f, 0.0f)) + 1u, x1);
+  const uint32_t ay1 = min(to_u32_clamped(fmaxf(cy + ey + 0.5f, 0.0f)) + 1u, y1);
+  Mask mask = 0;
+#pragma unroll
+  for (int l = 0; l < T; ++l) {
+    const uint32_t x = x0 + l, y = y0 + l;
+    const float dx = ((float)x + 0.5f) - cx, dy = ((float)y + 0.5f) - cy;
+    if (x >= ax0 && x < ax1 && !(fabsf(dx) > r)) mask |= (Mask)1 << l;
+    if (y >= ay0 && y < ay1 && !(fabsf(dy) > r)) mask |= (Mask)1 << (T + l);
+  }
+  return mask;
+}
+
+template <int T> __device__ __forceinline__ typename TileShape<T>::Mask staged_mask(const Staged &s) {
+  if constexpr (T > 16) return (unsigned long long)s.mask | ((unsigned long long)s.maskHi << 32);
+  else return s.mask;
 }
 
 // -0.5 (qxx dx^2 + qyy dy^2) - qxy dx dy, in this rounding order.
@@ -106,16 +158,16 @@ struct TileGeometry {
   uint32_t x0, y0, x1, y1; // pixels of the tile, upper bounds exclusive
 };
 
-__device__ __forceinline__ TileGeometry tile_geometry(const ViewSet &views, int tile) {
+__device__ __forceinline__ TileGeometry tile_geometry(const ViewSet &views, int tile, uint32_t T = kTileSize) {
   TileGeometry g;
   g.view = view_of_tile(views, tile);
   const ViewParams &cam = views.v[g.view];
   const int local = tile - cam.tileBase;
   const uint32_t tx = local % cam.gridW, ty = local / cam.gridW;
-  g.x0 = tx * kTileSize;
-  g.y0 = ty * kTileSize;
-  g.x1 = min(g.x0 + kTileSize, (uint32_t)cam.width);
-  g.y1 = min(g.y0 + kTileSize, (uint32_t)cam.height);
+  g.x0 = tx * T;
+  g.y0 = ty * T;
+  g.x1 = min(g.x0 + T, (uint32_t)cam.width);
+  g.y1 = min(g.y0 + T, (uint32_t)cam.height);
   return g;
 }
 
@@ -561,31 +613,34 @@ __global__ void __launch_bounds__(kTilePixels, 4)
 }
 
 // Two pixels per thread, for the forms whose sums need not follow the
-// reference's 32-lane groups: 128 threads per tile, warp w covering the 8x8
-// quadrant (w & 1, w >> 1) of the tile, lane l its pixels (l & 7, l >> 3) and
-// (l & 7, (l >> 3) + 4). The per-pixel arithmetic is that of k_forward and
-// k_backward; what changes is that a warp skips a splat that misses its 8x8
-// block, and that a staged splat's record and (backward) its reduction serve
-// two pixels per lane.
+// reference's 32-lane groups: T * T / 2 threads per tile of T x T pixels,
+// warp w covering the 8x8 block (w % (T / 8), w / (T / 8)), lane l its pixels
+// (l & 7, l >> 3) and (l & 7, (l >> 3) + 4). The per-pixel arithmetic is that
+// of k_forward and k_backward; what changes is that a warp skips a splat that
+// misses its 8x8 block, and that a staged splat's record and (backward) its
+// reduction serve two pixels per lane.
 constexpr int kHalfTile = kTilePixels / 2;
 
-struct PixelPair {
-  uint32_t x[2], y[2], bits[2];
+template <int T> struct PixelPair {
+  uint32_t x[2], y[2];
+  typename TileShape<T>::Mask bits[2];
   float px[2], py[2];
   bool inside[2];
 };
 
-__device__ __forceinline__ PixelPair pixel_pair(const TileGeometry &geo, const ViewParams &cam, uint32_t t) {
-  PixelPair pp;
+template <int T>
+__device__ __forceinline__ PixelPair<T> pixel_pair(const TileGeometry &geo, const ViewParams &cam, uint32_t t) {
+  using Mask = typename TileShape<T>::Mask;
+  PixelPair<T> pp;
   const uint32_t warp = t >> 5, lane = t & 31u;
-  const uint32_t bx = (warp & 1u) * 8u, by = (warp >> 1) * 8u;
+  const uint32_t bx = (warp % TileShape<T>::kBlocksX) * 8u, by = (warp / TileShape<T>::kBlocksX) * 8u;
   const uint32_t lx = bx + (lane & 7u), ly = by + (lane >> 3);
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const uint32_t yy = ly + 4u * q;
     pp.x[q] = geo.x0 + lx;
     pp.y[q] = geo.y0 + yy;
-    pp.bits[q] = (1u << lx) | (1u << (16 + yy));
+    pp.bits[q] = ((Mask)1 << lx) | ((Mask)1 << (T + yy));
     pp.px[q] = (float)pp.x[q] + 0.5f;
     pp.py[q] = (float)pp.y[q] + 0.5f;
     pp.inside[q] = pp.x[q] < (uint32_t)cam.width && pp.y[q] < (uint32_t)cam.height;
@@ -615,38 +670,74 @@ __device__ __forceinline__ bool ellipse_meets_rect(float qx, float qy, float qz,
   return least <= reach * 1.001f + 1e-3f;
 }
 
-// Stages `count` splats with 128 threads, two rounds, and publishes the
-// 8x8-block bitmaps: a block is listed when the splat's masks reach it and its
-// cutoff ellipse meets the block's pixel centres. With minStops (the backward
-// pass), also only when the splat's entry (first + j) is at or after the
-// least stop of the block's pixels: before it, every pixel there has stopped.
-template <class M>
+// The 8x8-block bitmaps of a T x T tile (publish_cover's kBlocks8x8 for any
+// T): word `word` of block w has bit b set when the staging warp's splat b
+// reaches a pixel row and column of block w and `met` (the caller's finer test)
+// has bit w. Every lane of the staging warp calls this.
+template <int T, int B>
+__device__ __forceinline__ void publish_blocks(typename TileShape<T>::Mask mask, uint32_t met, uint32_t word, uint32_t lane,
+                                               uint32_t (*cover)[B / 32]) {
+  using Mask = typename TileShape<T>::Mask;
+  constexpr int W = TileShape<T>::kWarps;
+  uint32_t mine = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const Mask cols = (Mask)0xFFu << (8 * (w % TileShape<T>::kBlocksX));
+    const Mask rows = (Mask)0xFFu << (T + 8 * (w / TileShape<T>::kBlocksX));
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, (mask & cols) != 0 && (mask & rows) != 0 && ((met >> w) & 1u) != 0u);
+    if (lane == (uint32_t)w) mine = b;
+  }
+  if (lane < (uint32_t)W) cover[lane][word] = mine;
+}
+
+// Stages `count` (at most B) splats with the tile's T * T / 2 threads and
+// publishes the 8x8-block bitmaps: a block is listed when the splat's masks
+// reach it and its cutoff ellipse meets the block's pixel centres. With
+// minStops (the backward pass), also only when the splat's entry (first + j)
+// is at or after the least stop of the block's pixels: before it, every pixel
+// there has stopped.
+template <class M, int T, int B>
 __device__ __forceinline__ void stage_pairs(const Splat *__restrict__ splats, const uint32_t *__restrict__ values, uint32_t count,
                                             uint32_t splatLimit, const TileGeometry &geo, uint32_t *error, Staged *batch,
-                                            uint32_t (*cover)[kBatch / 32], const uint32_t *minStops = nullptr,
+                                            uint32_t (*cover)[B / 32], const uint32_t *minStops = nullptr,
                                             uint32_t first = 0u) {
+  using Mask = typename TileShape<T>::Mask;
+  constexpr int kThreads = TileShape<T>::kThreads, W = TileShape<T>::kWarps;
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
 #pragma unroll
-  for (uint32_t round = 0; round < kBatch / kHalfTile; ++round) {
-    const uint32_t j = round * kHalfTile + t;
-    uint32_t mask = 0u, met = 0u;
+  for (uint32_t round = 0; round < (uint32_t)((B + kThreads - 1) / kThreads); ++round) {
+    const uint32_t j = round * kThreads + t;
+    Mask mask = 0;
+    uint32_t met = 0u;
     if (j < count) {
-      const Staged st = stage_checked<M>(splats, values[j], splatLimit, geo, error);
+      const uint32_t s = values[j];
+      Staged st{};
+      if (s >= splatLimit) {
+        atomicOr(error, kErrBadIndex);
+      } else {
+        const Splat sp = splats[s];
+        st = stage_fields<M>(sp, s);
+        const Mask full = pixel_masks_t<T>(sp, geo.x0, geo.y0, geo.x1, geo.y1);
+        st.mask = (uint32_t)full;
+        st.maskHi = (uint32_t)((unsigned long long)full >> 32);
+      }
       batch[j] = st;
-      mask = st.mask;
-      if (mask != 0u) {
+      mask = staged_mask<T>(st);
+      if (mask != 0) {
         // 2 ln(255 opacity): alpha >= 1/255 exactly where d' Q d <= reach.
         const float reach = 2.0f * __logf(255.0f * st.opacity);
 #pragma unroll
-        for (uint32_t w = 0; w < kHalfTile / 32; ++w) {
+        for (uint32_t w = 0; w < (uint32_t)W; ++w) {
           if (minStops != nullptr && first + j < minStops[w]) continue;
-          const float lowX = ((float)(geo.x0 + (w & 1u) * 8u) + 0.5f) - st.cx;
-          const float lowY = ((float)(geo.y0 + (w >> 1) * 8u) + 0.5f) - st.cy;
+          const float lowX = ((float)(geo.x0 + (w % TileShape<T>::kBlocksX) * 8u) + 0.5f) - st.cx;
+          const float lowY = ((float)(geo.y0 + (w / TileShape<T>::kBlocksX) * 8u) + 0.5f) - st.cy;
           if (ellipse_meets_rect(st.qx, st.qy, st.qz, reach, lowX, lowX + 7.0f, lowY, lowY + 7.0f)) met |= 1u << w;
         }
       }
     }
-    publish_cover<kBlocks8x8>(mask, round * (kHalfTile / 32) + warp, lane, cover, met);
+    // Only the warps whose 32 splats fall inside the batch publish.
+    const uint32_t word = round * (kThreads / 32) + warp;
+    if (word < (uint32_t)(B / 32)) publish_blocks<T, B>(mask, met, word, lane, cover);
   }
 }
 
@@ -671,33 +762,45 @@ __device__ __forceinline__ float2 splat_power2(const Staged &s, float dx, float2
   return fma2(mul2(f2(s.hqz), dy), dy, mul2(pxy, f2(dx)));
 }
 
-template <class M>
-__global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
-                                                        const uint2 *__restrict__ ranges, const ViewSet *__restrict__ viewsPtr,
-                                                        float bgR, float bgG, float bgB, float4 *__restrict__ image,
-                                                        uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error) {
-  chain_enter();
-  const ViewSet &views = *viewsPtr;
-  __shared__ Staged s_batch[kBatch];
-  __shared__ uint32_t s_cover[kHalfTile / 32][kBatch / 32];
-  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  const int tile = blockIdx.x;
-  const TileGeometry geo = tile_geometry(views, tile);
+// Blocks per SM the two-pixel kernels are compiled for, by tile edge.
+template <int T> constexpr int forward2_blocks() { return T > 16 ? 2 : 8; }
+template <int T> constexpr int backward2_blocks() { return T > 16 ? 1 : 6; }
+
+// The next tile of a launch: blockIdx.x the first time, then, for a
+// persistent launch (work not null: a grid of resident blocks), tiles of every
+// view claimed from the launch's counter until they run out. Every thread of
+// the block gets the same answer; -1 when the block is done.
+__device__ __forceinline__ int next_tile(uint32_t *work, uint32_t total, bool first, uint32_t *s_next) {
+  if (work == nullptr) return first ? (int)blockIdx.x : -1;
+  __syncthreads(); // the previous tile is finished with shared memory
+  if (threadIdx.x == 0) *s_next = atomicAdd(work, 1u);
+  __syncthreads();
+  const uint32_t tile = *s_next;
+  return tile < total ? (int)tile : -1;
+}
+
+template <class M, int T, int B>
+__device__ __forceinline__ void forward2_tile(int tile, const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
+                                              const uint2 *__restrict__ ranges, const ViewSet &views, float bgR, float bgG,
+                                              float bgB, float4 *__restrict__ image, uint32_t *__restrict__ stops,
+                                              uint32_t splatLimit, uint32_t *error, Staged *s_batch, uint32_t (*s_cover)[B / 32]) {
+  constexpr int kThreads = TileShape<T>::kThreads;
+  const TileGeometry geo = tile_geometry(views, tile, T);
   const ViewParams &cam = views.v[geo.view];
-  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-  const PixelPair pp = pixel_pair(geo, cam, t);
+  const uint32_t t = threadIdx.x, warp = t >> 5;
+  const PixelPair<T> pp = pixel_pair<T>(geo, cam, t);
   const uint2 range = ranges[tile];
   const float px = pp.px[0];
   const float2 py = make_float2(pp.py[0], pp.py[1]);
   const float logMin = kLogMinTransmittance * M::kLogScale;
-  float2 cr = f2(0.0f), cg = f2(0.0f), cb = f2(0.0f), T = f2(1.0f), logT = f2(0.0f);
+  float2 cr = f2(0.0f), cg = f2(0.0f), cb = f2(0.0f), Tr = f2(1.0f), logT = f2(0.0f);
   uint32_t stop0 = range.x, stop1 = range.x;
   bool done0 = !pp.inside[0], done1 = !pp.inside[1];
   for (uint32_t end = range.y; end > range.x;) {
-    const uint32_t count = min((uint32_t)kBatch, end - range.x);
+    const uint32_t count = min((uint32_t)B, end - range.x);
     end -= count;
-    if (__syncthreads_count(done0 && done1) == kHalfTile) break;
-    stage_pairs<M>(splats, entryValues + end, count, splatLimit, geo, error, s_batch, s_cover);
+    if (__syncthreads_count(done0 && done1) == kThreads) break;
+    stage_pairs<M, T, B>(splats, entryValues + end, count, splatLimit, geo, error, s_batch, s_cover);
     __syncthreads();
     for (int word = (int)((count - 1u) >> 5); word >= 0 && !(done0 && done1); --word) {
     for (uint32_t bits = s_cover[warp][word]; bits != 0u;) {
@@ -705,7 +808,7 @@ __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restri
       bits ^= 1u << bit;
       const uint32_t k = (uint32_t)word * 32u + (uint32_t)bit;
       const Staged &s = s_batch[k];
-      const uint32_t mask = s.mask;
+      const auto mask = staged_mask<T>(s);
       // Both pixels' tests of k_forward, the exponent and alpha packed.
       const float dx = px - s.cx;
       const float2 dy = add2(py, f2(-s.cy));
@@ -729,11 +832,11 @@ __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restri
       }
       // A pixel that does not blend takes weight 0 and factor 1: exact no-ops.
       const bool b0 = v0 && !s0, b1 = v1 && !s1;
-      const float2 w = mul2(T, make_float2(b0 ? a0 : 0.0f, b1 ? a1 : 0.0f));
+      const float2 w = mul2(Tr, make_float2(b0 ? a0 : 0.0f, b1 ? a1 : 0.0f));
       cr = fma2(w, f2(s.r), cr);
       cg = fma2(w, f2(s.g), cg);
       cb = fma2(w, f2(s.b), cb);
-      T = mul2(T, make_float2(b0 ? oneMinus.x : 1.0f, b1 ? oneMinus.y : 1.0f));
+      Tr = mul2(Tr, make_float2(b0 ? oneMinus.x : 1.0f, b1 ? oneMinus.y : 1.0f));
       logT = make_float2(b0 ? next.x : logT.x, b1 ? next.y : logT.y);
       if (done0 && done1) break;
     }
@@ -741,37 +844,52 @@ __global__ void __launch_bounds__(kHalfTile, 8) k_forward2(const Splat *__restri
   }
   if (pp.inside[0]) {
     const size_t at = (size_t)cam.pixelBase + (size_t)pp.y[0] * cam.width + pp.x[0];
-    image[at] = make_float4(fmaf(T.x, bgR, cr.x), fmaf(T.x, bgG, cg.x), fmaf(T.x, bgB, cb.x), logT.x);
+    image[at] = make_float4(fmaf(Tr.x, bgR, cr.x), fmaf(Tr.x, bgG, cg.x), fmaf(Tr.x, bgB, cb.x), logT.x);
     stops[at] = stop0;
   }
   if (pp.inside[1]) {
     const size_t at = (size_t)cam.pixelBase + (size_t)pp.y[1] * cam.width + pp.x[1];
-    image[at] = make_float4(fmaf(T.y, bgR, cr.y), fmaf(T.y, bgG, cg.y), fmaf(T.y, bgB, cb.y), logT.y);
+    image[at] = make_float4(fmaf(Tr.y, bgR, cr.y), fmaf(Tr.y, bgG, cg.y), fmaf(Tr.y, bgB, cb.y), logT.y);
     stops[at] = stop1;
   }
 }
 
-// Float sums only: each lane adds its two pixels' values before one butterfly.
-// The per-pixel arithmetic runs on both pixels at once in packed FP32.
-template <class M, bool SCORE>
-__global__ void __launch_bounds__(kHalfTile, 6)
-    k_backward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
-                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
-                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
-                uint32_t splatLimit, uint32_t *error, const float *__restrict__ edge) {
+// Compositing, two pixels per thread, tiles of T x T pixels, batches of B
+// staged splats; work: a persistent launch's tile counter (or null: one
+// block per tile).
+template <class M, int T, int B>
+__global__ void __launch_bounds__(TileShape<T>::kThreads, forward2_blocks<T>())
+    k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
+               const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, float4 *__restrict__ image,
+               uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error, uint32_t *work) {
   chain_enter();
-  constexpr int kValues = score_values<SCORE>(), kStride = score_stride<SCORE>();
   const ViewSet &views = *viewsPtr;
-  __shared__ Staged s_batch[kBatch];
-  __shared__ float s_acc[kBatch * kStride];
-  __shared__ uint32_t s_min[kHalfTile / 32];
-  __shared__ uint32_t s_cover[kHalfTile / 32][kBatch / 32];
+  __shared__ Staged s_batch[B];
+  __shared__ uint32_t s_cover[TileShape<T>::kWarps][B / 32];
+  __shared__ uint32_t s_next;
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  const int tile = blockIdx.x;
-  const TileGeometry geo = tile_geometry(views, tile);
+  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next); tile >= 0;
+       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next))
+    forward2_tile<M, T, B>(tile, splats, entryValues, ranges, views, bgR, bgG, bgB, image, stops, splatLimit, error, s_batch,
+                           s_cover);
+}
+
+// Float sums only: each lane adds its two pixels' values before one
+// butterfly. The per-pixel arithmetic runs on both pixels at once in packed
+// FP32. One tile of T x T pixels, batches of B staged splats.
+template <class M, bool SCORE, int T, int B>
+__device__ __forceinline__ void backward2_tile(int tile, const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
+                                               const uint2 *__restrict__ ranges, const ViewSet &views, float bgR, float bgG,
+                                               float bgB, const float4 *__restrict__ image, const float4 *__restrict__ adjoint,
+                                               const uint32_t *__restrict__ stops, float *__restrict__ raw, uint32_t splatLimit,
+                                               uint32_t *error, const float *__restrict__ edge, Staged *s_batch, float *s_acc,
+                                               uint32_t *s_min, uint32_t (*s_cover)[B / 32]) {
+  constexpr int kValues = score_values<SCORE>(), kStride = score_stride<SCORE>();
+  constexpr int kThreads = TileShape<T>::kThreads, W = TileShape<T>::kWarps;
+  const TileGeometry geo = tile_geometry(views, tile, T);
   const ViewParams &cam = views.v[geo.view];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-  const PixelPair pp = pixel_pair(geo, cam, t);
+  const PixelPair<T> pp = pixel_pair<T>(geo, cam, t);
   const uint2 range = ranges[tile];
   // front: log T total minus the log transmittance of the splats already
   // walked (those behind), kept as one running value. behind: the adjoint
@@ -800,23 +918,23 @@ __global__ void __launch_bounds__(kHalfTile, 6)
   const float perPixel = cam.perPixel;
   const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
   if (lane == 0) s_min[t >> 5] = warpMin;
-  for (int i = t; i < kBatch * kStride; i += kHalfTile) s_acc[i] = 0.0f;
+  for (int i = t; i < B * kStride; i += kThreads) s_acc[i] = 0.0f;
   __syncthreads();
   uint32_t tileStop = s_min[0];
 #pragma unroll
-  for (int w = 1; w < kHalfTile / 32; ++w) tileStop = min(tileStop, s_min[w]);
+  for (int w = 1; w < W; ++w) tileStop = min(tileStop, s_min[w]);
   const uint32_t held = __brev(lane) >> 28;
 
-  for (uint32_t start = tileStop; start < range.y; start += kBatch) {
-    const uint32_t count = min((uint32_t)kBatch, range.y - start);
+  for (uint32_t start = tileStop; start < range.y; start += B) {
+    const uint32_t count = min((uint32_t)B, range.y - start);
     __syncthreads();
-    stage_pairs<M>(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover, s_min, start);
+    stage_pairs<M, T, B>(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover, s_min, start);
     __syncthreads();
     for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
     for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
       const uint32_t k = word * 32u + (uint32_t)(__ffs(bits) - 1);
       const Staged &s = s_batch[k];
-      const uint32_t mask = s.mask;
+      const auto mask = staged_mask<T>(s);
       const float dx = px - s.cx;
       const float2 dy = add2(py, f2(-s.cy));
       const float2 power = splat_power2(s, dx, dy);
@@ -833,8 +951,8 @@ __global__ void __launch_bounds__(kHalfTile, 6)
       const float2 oneMinus = rsub2(aAct, f2(1.0f));
       const float2 logRest = make_float2(M::log(oneMinus.x), M::log(oneMinus.y));
       const float2 nextFront = rsub2(logRest, front);
-      const float2 T = make_float2(M::exp(nextFront.x), M::exp(nextFront.y));
-      const float2 wA = mul2(T, aAct);
+      const float2 Tf = make_float2(M::exp(nextFront.x), M::exp(nextFront.y));
+      const float2 wA = mul2(Tf, aAct);
       float g[SCORE ? 16 : 12];
       const float2 c6 = mul2(wA, Ax), c7 = mul2(wA, Ay), c8 = mul2(wA, Az);
       g[6] = c6.x + c6.y;
@@ -849,7 +967,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
       }
       const float2 ahead = rsub2(behind, fma2(Az, f2(s.b), fma2(Ay, f2(s.g), mul2(Ax, f2(s.r)))));
       // At the 0.99 clamp alpha no longer depends on the parameters.
-      const float2 dT = mul2(T, ahead);
+      const float2 dT = mul2(Tf, ahead);
       const float2 dAlpha = make_float2(act0 && oe.x < kAlphaMax ? dT.x : 0.0f, act1 && oe.y < kAlphaMax ? dT.y : 0.0f);
       const float2 c0 = mul2(dAlpha, ep);
       g[0] = c0.x + c0.y;
@@ -874,7 +992,7 @@ __global__ void __launch_bounds__(kHalfTile, 6)
     }
     __syncthreads();
     // One global atomic per (splat, value) for the whole tile.
-    for (uint32_t j = t; j < count; j += kHalfTile) {
+    for (uint32_t j = t; j < count; j += kThreads) {
       if (s_batch[j].mask == 0u) continue;
       float *dst = raw + (size_t)s_batch[j].index * kRawStride;
 #pragma unroll
@@ -886,6 +1004,80 @@ __global__ void __launch_bounds__(kHalfTile, 6)
         }
       }
     }
+  }
+}
+
+template <class M, bool SCORE, int T, int B>
+__global__ void __launch_bounds__(TileShape<T>::kThreads, backward2_blocks<T>())
+    k_backward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
+                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
+                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
+                uint32_t splatLimit, uint32_t *error, const float *__restrict__ edge, uint32_t *work) {
+  chain_enter();
+  const ViewSet &views = *viewsPtr;
+  __shared__ Staged s_batch[B];
+  __shared__ float s_acc[B * score_stride<SCORE>()];
+  __shared__ uint32_t s_min[TileShape<T>::kWarps];
+  __shared__ uint32_t s_cover[TileShape<T>::kWarps][B / 32];
+  __shared__ uint32_t s_next;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next); tile >= 0;
+       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next))
+    backward2_tile<M, SCORE, T, B>(tile, splats, entryValues, ranges, views, bgR, bgG, bgB, image, adjoint, stops, raw, splatLimit,
+                                   error, edge, s_batch, s_acc, s_min, s_cover);
+}
+
+// Blocks of a kernel that fit on the GPU at once (its occupancy times the
+// SMs): the grid of a persistent launch. Asked once per kernel.
+uint32_t resident_blocks(const void *kernel, int threads) {
+  static std::mutex lock;
+  static std::unordered_map<const void *, uint32_t> known;
+  std::lock_guard<std::mutex> guard(lock);
+  const auto hit = known.find(kernel);
+  if (hit != known.end()) return hit->second;
+  int device = 0, sms = 0, perSm = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0);
+  const uint32_t blocks = (uint32_t)std::max(1, sms * std::max(perSm, 1));
+  known.emplace(kernel, blocks);
+  return blocks;
+}
+
+template <class M, int T, int B>
+void launch_forward2(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,
+                     const RasterConfig &cfg, float4 *image, uint32_t *stops, uint32_t splatLimit, uint32_t *error,
+                     cudaStream_t stream) {
+  constexpr int kThreads = TileShape<T>::kThreads;
+  uint32_t grid = (uint32_t)views.totalTiles;
+  if (cfg.workForward != nullptr) grid = std::min(grid, resident_blocks((const void *)k_forward2<M, T, B>, kThreads));
+  launch_chained(k_forward2<M, T, B>, dim3(grid), dim3(kThreads), 0, stream, splats, entryValues, ranges, dViews, cfg.background[0],
+                 cfg.background[1], cfg.background[2], image, stops, splatLimit, error, cfg.workForward);
+}
+
+template <class M, bool SCORE, int T, int B>
+void launch_backward2(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views,
+                      const ViewSet *dViews, const RasterConfig &cfg, const float4 *image, const float4 *adjoint,
+                      const uint32_t *stops, float *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream,
+                      const float *edge) {
+  constexpr int kThreads = TileShape<T>::kThreads;
+  uint32_t grid = (uint32_t)views.totalTiles;
+  if (cfg.workBackward != nullptr) grid = std::min(grid, resident_blocks((const void *)k_backward2<M, SCORE, T, B>, kThreads));
+  launch_chained(k_backward2<M, SCORE, T, B>, dim3(grid), dim3(kThreads), 0, stream, splats, entryValues, ranges, dViews,
+                 cfg.background[0], cfg.background[1], cfg.background[2], image, adjoint, stops, raw, splatLimit, error, edge,
+                 cfg.workBackward);
+}
+
+// Calls f(tile edge, batch depth) with the two-pixel kernels' settings as
+// compile-time constants.
+template <class F> void dispatch_tile_batch(const RasterConfig &cfg, F &&f) {
+  using I = std::integral_constant<int, 16>;
+  if (cfg.tile == 32) {
+    if (cfg.batch == 128) f(std::integral_constant<int, 32>{}, std::integral_constant<int, 128>{});
+    else f(std::integral_constant<int, 32>{}, std::integral_constant<int, 256>{});
+  } else {
+    if (cfg.batch == 128) f(I{}, std::integral_constant<int, 128>{});
+    else f(I{}, std::integral_constant<int, 256>{});
   }
 }
 
@@ -911,12 +1103,14 @@ void launch_forward(const Splat *splats, const uint32_t *entryValues, const uint
     return;
   }
   if (cfg.forwardPixels == 2) {
-    if (cfg.exactMath)
-      launch_chained(k_forward2<ExactMath>, dim3(views.totalTiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, stops,
-                                                                       splatLimit, error);
-    else
-      launch_chained(k_forward2<FastMath>, dim3(views.totalTiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image, stops,
-                                                                      splatLimit, error);
+    dispatch_tile_batch(cfg, [&](auto T, auto B) {
+      if (cfg.exactMath)
+        launch_forward2<ExactMath, decltype(T)::value, decltype(B)::value>(splats, entryValues, ranges, views, dViews, cfg, image,
+                                                                           stops, splatLimit, error, stream);
+      else
+        launch_forward2<FastMath, decltype(T)::value, decltype(B)::value>(splats, entryValues, ranges, views, dViews, cfg, image,
+                                                                          stops, splatLimit, error, stream);
+    });
   } else {
     if (cfg.exactMath)
       launch_chained(k_forward<ExactMath, 0>, dim3(views.totalTiles), dim3(kTilePixels), 0, stream, splats, entryValues, ranges, dViews, r, g, b, image,
@@ -937,17 +1131,16 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
   // The fixed-point sums keep the reference's 32-lane groups: one pixel per thread.
   if (!fixedPoint && cfg.backwardPixels == 2) {
     float *rawF = static_cast<float *>(raw);
-#define SB_BACKWARD2(MATH, SCORE)                                                                                       \
-  launch_chained(k_backward2<MATH, SCORE>, dim3(tiles), dim3(kHalfTile), 0, stream, splats, entryValues, ranges, dViews, r, g, b, \
-                 image, adjoint, stops, rawF, splatLimit, error, edge)
-    if (cfg.exactMath) {
-      if (score) SB_BACKWARD2(ExactMath, true);
-      else SB_BACKWARD2(ExactMath, false);
-    } else {
-      if (score) SB_BACKWARD2(FastMath, true);
-      else SB_BACKWARD2(FastMath, false);
-    }
-#undef SB_BACKWARD2
+    dispatch_tile_batch(cfg, [&](auto T, auto B) {
+      constexpr int kT = decltype(T)::value, kB = decltype(B)::value;
+      if (cfg.exactMath) {
+        if (score) launch_backward2<ExactMath, true, kT, kB>(splats, entryValues, ranges, views, dViews, cfg, image, adjoint, stops, rawF, splatLimit, error, stream, edge);
+        else launch_backward2<ExactMath, false, kT, kB>(splats, entryValues, ranges, views, dViews, cfg, image, adjoint, stops, rawF, splatLimit, error, stream, edge);
+      } else {
+        if (score) launch_backward2<FastMath, true, kT, kB>(splats, entryValues, ranges, views, dViews, cfg, image, adjoint, stops, rawF, splatLimit, error, stream, edge);
+        else launch_backward2<FastMath, false, kT, kB>(splats, entryValues, ranges, views, dViews, cfg, image, adjoint, stops, rawF, splatLimit, error, stream, edge);
+      }
+    });
     return;
   }
 #define SB_BACKWARD(MATH, FIX, SCORE)                                                                                   \

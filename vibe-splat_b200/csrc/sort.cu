@@ -2,6 +2,7 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 #include "bulk.cuh"
 #include "common.cuh"
@@ -19,6 +20,9 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagInclusive = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
 constexpr int kLookbackSpinLimit = 1 << 20;
+// The limit the passes are launched with: kLookbackSpinLimit unless a caller
+// lowered it (set_lookback_limit, for the tests that make a wait run out).
+std::atomic<int> g_lookbackLimit{kLookbackSpinLimit};
 constexpr int kLookbackWindow = 8;
 
 struct ScratchLayout {
@@ -149,7 +153,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
                                                               K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
                                                               const uint32_t *deviceCount, uint32_t hostCount,
                                                               const uint32_t *__restrict__ passHist, uint32_t *lookback,
-                                                              uint32_t *tileCounter, int shift, uint32_t *error) {
+                                                              uint32_t *tileCounter, int shift, int spinLimit, uint32_t *error) {
   chain_enter();
   constexpr int kBins = 1 << BITS;
   constexpr uint32_t kMask = kBins - 1;
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
         }
         if (done) break;
         pred -= used;
-        if (used < kLookbackWindow && ++spins > kLookbackSpinLimit) {
+        if (used < kLookbackWindow && ++spins > spinLimit) {
           atomicOr(error, kErrLookbackTimeout);
           break;
         }
@@ -414,7 +418,8 @@ int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, 
   for (int p = 0; p < passes; ++p) {
     launch_chained(k_onesweep<K, BITS>, dim3(tiles), dim3(kSortThreads), smem, stream, srcK, srcV, dstK, dstV, deviceCount, hostCount,
                                                                hist + p * kBins, lookback + (size_t)p * tiles * kBins,
-                                                               counters + p, firstBit + p * BITS, error);
+                                                               counters + p, firstBit + p * BITS,
+                                                               g_lookbackLimit.load(std::memory_order_relaxed), error);
     K *tk = srcK;
     srcK = dstK;
     dstK = tk;
@@ -462,5 +467,7 @@ int sort_pairs_u64(unsigned long long *keys, uint32_t *values, unsigned long lon
                                                   firstBit, bits, scratch, error, stream, clearScratch);
   }
 }
+
+void set_lookback_limit(int polls) { g_lookbackLimit.store(polls < 0 ? kLookbackSpinLimit : polls, std::memory_order_relaxed); }
 
 } // namespace sb

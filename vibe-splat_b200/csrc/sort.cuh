@@ -20,8 +20,10 @@
 // tiles are ordered by their id, which is claimed in launch order through an
 // atomic counter, so a tile only ever waits on tiles that already run.
 //
-// Every look-back wait is bounded: after kLookbackSpinLimit polls the kernel
-// sets kErrLookbackTimeout in the error word, takes what it has and finishes.
+// Every look-back wait is bounded: after 2^20 polls the kernel sets
+// kErrLookbackTimeout in the error word, takes what it has and finishes; every
+// scattered position is then still checked against the count, so no write
+// leaves the arrays (a partial prefix only moves a key to a lower slot).
 #pragma once
 
 #include <cstddef>
@@ -58,5 +60,9 @@ int sort_pairs_u32(uint32_t *keys, uint32_t *values, uint32_t *tmpKeys, uint32_t
 int sort_pairs_u64(unsigned long long *keys, uint32_t *values, unsigned long long *tmpKeys, uint32_t *tmpValues,
                    size_t capacity, uint32_t hostCount, const uint32_t *deviceCount, int firstBit, int bits, int digitBits,
                    void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch = true);
+
+// The look-back poll limit of later sort launches; a negative value restores
+// the default. For the tests that make a wait run out on purpose.
+void set_lookback_limit(int polls);
 
 } // namespace sb

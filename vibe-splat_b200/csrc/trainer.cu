@@ -167,6 +167,9 @@ public:
   bool blendLists = false; // store-everything backward
   int digitBits = 8;
   int forwardPixels = 1, backwardPixels = 2; // pixels per thread of the compositing and float backward kernels
+  int tileSize = 16, batchDepth = 256;        // the two-pixel kernels' tile edge and staging batch
+  bool persistent = false;                    // the two-pixel kernels as persistent launches
+  DeviceBuffer workCounters;                  // their tile counters (2 words), cleared every step
   cudaStream_t stream = nullptr;
   // The step's clears run on a second stream, forked from and joined back to
   // the first (branches of the same graph when captured).
@@ -248,6 +251,8 @@ public:
   void record_prepare(bool backward);
   void record_forward();
   int entry_sort_bits() const;
+  int raster_tile() const;
+  RasterConfig raster_config();
   void record_backward_and_chain(ChainMode mode, bool statistics);
   void record_readback();
   void begin(int stage);
@@ -342,6 +347,11 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
     throw Failure{SPLAT_ERR_INVALID, "forward_pixels_per_thread must be 1 or 2"};
   if (backwardPixels != 1 && backwardPixels != 2)
     throw Failure{SPLAT_ERR_INVALID, "backward_pixels_per_thread must be 1 or 2"};
+  tileSize = opt.tile_size == 0 ? 16 : opt.tile_size;
+  if (tileSize != 16 && tileSize != 32) throw Failure{SPLAT_ERR_INVALID, "tile_size must be 16 or 32"};
+  batchDepth = opt.batch_depth == 0 ? 256 : opt.batch_depth;
+  if (batchDepth != 128 && batchDepth != 256) throw Failure{SPLAT_ERR_INVALID, "batch_depth must be 128 or 256"};
+  persistent = opt.persistent_raster != 0;
   SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   SB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
   SB_CUDA(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
@@ -497,7 +507,8 @@ void Trainer::set_views(const splat_camera *cameras, int count) {
   if (count < 1 || count > kMaxViews) throw Failure{SPLAT_ERR_INVALID, "between 1 and 8 views per step"};
   ViewSet vs{};
   vs.count = count;
-  int tileBase = 0;
+  const int tile = raster_tile();
+  int tileBase = 0, lossTileBase = 0;
   long long pixelBase = 0;
   for (int k = 0; k < count; ++k) {
     const splat_camera &c = cameras[k];
@@ -519,10 +530,15 @@ void Trainer::set_views(const splat_camera *cameras, int count) {
     v.tanY = 0.5f * (float)c.height / c.fy;
     v.width = c.width;
     v.height = c.height;
-    v.gridW = (int)div_up((uint32_t)c.width, kTileSize);
-    v.gridH = (int)div_up((uint32_t)c.height, kTileSize);
+    v.gridW = (int)div_up((uint32_t)c.width, (uint32_t)tile);
+    v.gridH = (int)div_up((uint32_t)c.height, (uint32_t)tile);
     v.tileBase = tileBase;
     v.tileCount = v.gridW * v.gridH;
+    v.lossGridW = (int)div_up((uint32_t)c.width, kTileSize);
+    v.lossGridH = (int)div_up((uint32_t)c.height, kTileSize);
+    v.lossTileBase = lossTileBase;
+    v.lossTileCount = v.lossGridW * v.lossGridH;
+    lossTileBase += v.lossTileCount;
     v.pixelBase = pixelBase;
     v.perPixel = 1.0f / (3.0f * (float)c.width * (float)c.height);
     v.fixedScale = 3.0f * (float)c.width * (float)c.height * 64.0f;
@@ -535,6 +551,8 @@ void Trainer::set_views(const splat_camera *cameras, int count) {
   if (!oneSort && tileBase > (1 << 24)) throw Failure{SPLAT_ERR_INVALID, "too many tiles for one step"};
   vs.totalTiles = tileBase;
   vs.totalPixels = pixelBase;
+  vs.tileSize = tile;
+  vs.totalLossTiles = lossTileBase;
   views = vs;
 }
 
@@ -563,7 +581,7 @@ void Trainer::ensure_view_buffers() {
   fields.ensure(pixels * 36);
   target.ensure(pixels * 4);
   ranges.ensure(tiles * 8);
-  partials.ensure(tiles * 8);
+  partials.ensure((size_t)views.totalLossTiles * 8);
   if (image.bytes() + target.bytes() + ranges.bytes() != before) clear_graphs();
   if (blendLists) {
     listCounts.ensure(pixels * 4);
@@ -695,6 +713,29 @@ int Trainer::entry_sort_bits() const {
   return oneSort ? 32 + (int)bits_for((uint32_t)views.totalTiles) : (int)bits_for((uint32_t)views.totalTiles);
 }
 
+// The rasterizer's tile edge: the option's where both kernels take two
+// pixels per thread with float sums (the kernels built for other edges),
+// else the reference's 16.
+int Trainer::raster_tile() const {
+  return forwardPixels == 2 && backwardPixels == 2 && !fixedPoint && !blendLists ? tileSize : kTileSize;
+}
+
+RasterConfig Trainer::raster_config() {
+  RasterConfig cfg;
+  cfg.exactMath = exactMath ? 1 : 0;
+  cfg.forwardPixels = forwardPixels;
+  cfg.backwardPixels = backwardPixels;
+  for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
+  cfg.tile = views.tileSize;
+  cfg.batch = batchDepth;
+  if (persistent) {
+    workCounters.ensure(16);
+    if (forwardPixels == 2) cfg.workForward = workCounters.get<uint32_t>();
+    if (backwardPixels == 2 && !fixedPoint) cfg.workBackward = workCounters.get<uint32_t>() + 1;
+  }
+  return cfg;
+}
+
 void Trainer::record_prepare(bool backward) {
   const Params p = params();
   SB_CUDA(cudaMemcpyAsync(dViews.get(), hViews.get(), sizeof(ViewSet), cudaMemcpyHostToDevice, stream));
@@ -710,6 +751,10 @@ void Trainer::record_prepare(bool backward) {
   SB_CUDA(cudaStreamWaitEvent(side, forkEvent, 0));
   if (backward) SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, side));
   SB_CUDA(cudaMemsetAsync(ranges.get(), 0, (size_t)views.totalTiles * 8, side));
+  if (persistent) {
+    workCounters.ensure(16);
+    SB_CUDA(cudaMemsetAsync(workCounters.get(), 0, 16, side));
+  }
   if (!oneSort) SB_CUDA(cudaMemsetAsync(sortScratchDepth.get(), 0, sort_scratch_bytes(n, 4, 32, digitBits), side));
   entryScratchClear = entryKeys.get() != nullptr;
   if (entryScratchClear) {
@@ -787,11 +832,7 @@ void Trainer::record_forward() {
                      oneSort ? static_cast<const unsigned long long *>(keys) : nullptr, &counters[2], entryCapacity,
                      (uint32_t)views.totalTiles, ranges.get<uint2>(), error, stream);
   end(3);
-  RasterConfig cfg;
-  cfg.exactMath = exactMath ? 1 : 0;
-  cfg.forwardPixels = forwardPixels;
-  cfg.backwardPixels = backwardPixels;
-  for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
+  const RasterConfig cfg = raster_config();
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
   begin(4);
   if (blendLists) {
@@ -845,11 +886,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
     launch_error_mask(adjoint.get<float4>(), (uint32_t)views.totalPixels, scoreMax.get<uint32_t>(), scoreShare, stream);
   launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, stream);
   end(5);
-  RasterConfig cfg;
-  cfg.exactMath = exactMath ? 1 : 0;
-  cfg.forwardPixels = forwardPixels;
-  cfg.backwardPixels = backwardPixels;
-  for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
+  const RasterConfig cfg = raster_config();
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
   begin(6);
   if (blendLists) {
@@ -1139,9 +1176,11 @@ void Trainer::set_sort(bool single, int digits) {
 
 // The autotuner: times every sort form and digit width on one view with
 // gradient passes, which change neither the parameters, the optimiser state
-// nor the densification statistics, and keeps the fastest. The tile size (16)
-// and the batch depth (one staged splat per pixel thread, 256) are fixed by
-// the kernels' thread-per-pixel design.
+// nor the densification statistics, and keeps the fastest; then the
+// rasterizer's pixel layouts; then, for the two-pixel float kernels, their
+// tile edge (16 or 32), batch depth (128 or 256) and launch form (a block per
+// tile or persistent). The one-pixel kernels keep the reference's 16 x 16
+// tiles and 256-splat batches, one staged splat per pixel thread.
 void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats,
                        splat_autotune_result *out) {
   if (repeats < 1) repeats = 1;
@@ -1204,6 +1243,44 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
   clear_graphs();
   result.forward_pixels_per_thread = bestForward;
   result.backward_pixels_per_thread = bestBackward;
+  // Then, where both layouts take two pixels per thread with float sums, the
+  // tile edge, the staging batch and the launch form of those kernels.
+  if (forwardPixels == 2 && backwardPixels == 2 && !fixedPoint && !blendLists) {
+    int bestTile = tileSize, bestBatch = batchDepth;
+    bool bestPersistent = persistent;
+    double bestMs = 1e30;
+    for (int ti = 0; ti < 2; ++ti) {
+      for (int bi = 0; bi < 2; ++bi) {
+        for (int pi = 0; pi < 2; ++pi) {
+          tileSize = 16 << ti;
+          batchDepth = 128 << bi;
+          persistent = pi == 1;
+          clear_graphs();
+          splat_step_stats s{};
+          run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+          run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+          const auto t0 = std::chrono::steady_clock::now();
+          for (int r = 0; r < repeats; ++r) run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
+          const double ms =
+              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
+          result.tile_ms[ti][bi][pi] = ms;
+          if (ms < bestMs) {
+            bestMs = ms;
+            bestTile = tileSize;
+            bestBatch = batchDepth;
+            bestPersistent = persistent;
+          }
+        }
+      }
+    }
+    tileSize = bestTile;
+    batchDepth = bestBatch;
+    persistent = bestPersistent;
+    clear_graphs();
+  }
+  result.tile_size = raster_tile();
+  result.batch_depth = batchDepth;
+  result.persistent_raster = persistent ? 1 : 0;
   if (out != nullptr) *out = result;
 }
 
@@ -1327,6 +1404,9 @@ void splat_trainer_options_default(splat_trainer_options *o) {
   o->digit_bits = 8;
   o->forward_pixels_per_thread = 1;
   o->backward_pixels_per_thread = 2;
+  o->tile_size = 16;
+  o->batch_depth = 256;
+  o->persistent_raster = 0;
 }
 
 void splat_learning_rates_default(splat_learning_rates *r) {
@@ -2522,7 +2602,7 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     case 8: src = t->adjoint.get(); have = (size_t)t->views.totalPixels * 16; break;
     case 9: src = t->raw.get(); have = items * sb::kRawStride * 4; break;
     case 10: src = rb->counters; have = 16; break;
-    case 11: src = t->partials.get(); have = (size_t)t->views.totalTiles * 8; break;
+    case 11: src = t->partials.get(); have = (size_t)t->views.totalLossTiles * 8; break;
     case 12: src = &rb->error; have = 4; break;
     case 13: src = t->listCounts.get(); have = t->blendLists ? (size_t)t->views.totalPixels * 4 : 0; break;
     case 14: case 15: case 16: case 17: case 18: {
@@ -2595,6 +2675,10 @@ int splat_radix_sort_u64(uint64_t *keys, uint32_t *values, uint64_t *tmp_keys, u
     SB_CUDA(cudaStreamSynchronize(s));
     if (err != 0) throw Failure{SPLAT_ERR_DEVICE, "the sort's look-back gave up waiting"};
   });
+}
+
+int splat_debug_set_wait_limit(int32_t polls) {
+  return guarded([&] { sb::set_lookback_limit(polls); });
 }
 
 int splat_debug_detmath(const float *in, float *out_exp, float *out_log, uint32_t count) {
