@@ -18,17 +18,31 @@ on one view, views in turn. Reported:
   plain  the plain FP32 form (FP32 SH and Adam state, the reference's
          two-sort order, host read-back of the entry count, no CUDA graph,
          deterministic exp/log) on the same views, for the 2x target;
-  roofline, cpu_baseline, clocks, gpu_launches;
+  roofline, clocks, gpu_launches;
+  cpu_baseline  the reference's FP64 CPU twin on whole views, one view per
+         host thread on every thread, with an FP64 Adam step: views/s, and
+         one thread's seconds for one whole view;
+  precision.vs_fp64  the chosen and the plain form's render, loss and
+         gradients on the first view against the FP64 oracle (oracle/fp64.py);
+  fd_config2  both backward variants against FP64 central differences on
+         256 parameters at the full training step's shape (100k Gaussians,
+         800x800);
+  batched, memory_adjoint  the other measured shapes, compact: 8 uneven
+         views per step at 3M Gaussians, and recompute against store-everything
+         at 6M Gaussians and 3840x2160;
   score_view_ms, densify (densification rounds on the GPU, first and later,
          beside the reference's densify_cloud on the same statistics;
          relocation rounds), prune: the cloud edits after the timed steps.
+The checkers (the FP64 oracle, central differences, the CPU twin) run outside
+every timed region.
 --workload memory-adjoint, batched and session run the other measured
-shapes (each prints its own JSON line).
+shapes at full length (each prints its own JSON line).
 With --gpus N > 1 every rank trains its own replica (the path does not shard:
 replicas only), and value is the sum over ranks.
 --impl reference times the reference's own FP64 CPU twin (src/train/
 reference.cpp, compiled from the reference's sources into oracle/_ref) on the
-host cores instead.
+host cores instead: whole views, one per thread, in full rounds covering the
+K steps, each with an FP64 Adam step.
 """
 from __future__ import annotations
 
