@@ -52,11 +52,12 @@ def test_sort_lookback_gives_up_within_bounds(splat):
     try:
         assert lib.splat_debug_set_wait_limit(0) == 0
         status = sort(*[p for _, p in bufs], count, 32, 8, None)
+        message = lib.splat_last_error()  # before the next call replaces it
     finally:
         lib.splat_debug_set_wait_limit(-1)
     torch.cuda.synchronize()
     assert status == splat.SPLAT_ERR_DEVICE
-    assert b"look-back" in lib.splat_last_error()
+    assert b"look-back" in message
     for buf, _ in bufs:
         host = buf.cpu().numpy().view(np.uint32)
         assert (host[:pad] == SENTINEL).all() and (host[-pad:] == SENTINEL).all()

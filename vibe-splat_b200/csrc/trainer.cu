@@ -359,6 +359,9 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   SB_CUDA(cudaEventCreateWithFlags(&countForkEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&countEvent, cudaEventDisableTiming));
   SB_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+  // The persistent launches' tile counters, made here: a step may be recorded
+  // into a graph, where nothing may be allocated.
+  workCounters.ensure(16);
   SB_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&consumed, cudaEventDisableTiming));
   for (auto &e : events) SB_CUDA(cudaEventCreate(&e));
@@ -729,7 +732,6 @@ RasterConfig Trainer::raster_config() {
   cfg.tile = views.tileSize;
   cfg.batch = batchDepth;
   if (persistent) {
-    workCounters.ensure(16);
     if (forwardPixels == 2) cfg.workForward = workCounters.get<uint32_t>();
     if (backwardPixels == 2 && !fixedPoint) cfg.workBackward = workCounters.get<uint32_t>() + 1;
   }
@@ -751,10 +753,7 @@ void Trainer::record_prepare(bool backward) {
   SB_CUDA(cudaStreamWaitEvent(side, forkEvent, 0));
   if (backward) SB_CUDA(cudaMemsetAsync(raw.get(), 0, (size_t)n * views.count * kRawStride * 4, side));
   SB_CUDA(cudaMemsetAsync(ranges.get(), 0, (size_t)views.totalTiles * 8, side));
-  if (persistent) {
-    workCounters.ensure(16);
-    SB_CUDA(cudaMemsetAsync(workCounters.get(), 0, 16, side));
-  }
+  if (persistent) SB_CUDA(cudaMemsetAsync(workCounters.get(), 0, 16, side));
   if (!oneSort) SB_CUDA(cudaMemsetAsync(sortScratchDepth.get(), 0, sort_scratch_bytes(n, 4, 32, digitBits), side));
   entryScratchClear = entryKeys.get() != nullptr;
   if (entryScratchClear) {
