@@ -549,6 +549,7 @@ def tuned_options(chosen, tuned: dict):
         opts.tile_size = tuned.get("tile_size", chosen.tile_size)
         opts.batch_depth = tuned.get("batch_depth", chosen.batch_depth)
         opts.persistent_raster = bool(tuned.get("persistent_raster", chosen.persistent_raster))
+        opts.grouped_backward = bool(tuned.get("grouped_backward", chosen.grouped_backward))
     return opts
 
 
@@ -1040,10 +1041,12 @@ def our_arm(args) -> None:
                 f"{tuned.get('backward_pixels_per_thread', chosen.backward_pixels_per_thread)}-pixel float "
                 f"backward, {tuned.get('tile_size', chosen.tile_size)}x{tuned.get('tile_size', chosen.tile_size)} tiles, "
                 f"batches of {tuned.get('batch_depth', chosen.batch_depth)}, "
-                f"{'persistent' if tuned.get('persistent_raster', chosen.persistent_raster) else 'one block per tile'} "
+                f"{'persistent' if tuned.get('persistent_raster', chosen.persistent_raster) else 'one block per tile'}, "
+                f"{'grouped' if tuned.get('grouped_backward', chosen.grouped_backward) else 'per-splat'} backward sums "
                 f"({'autotuned' if tuned else 'fixed'}), fused one-view chain rule + Adam + SH "
                 "step, CUDA graph, SFU exp/log",
-        "autotune": {"ms": tuned.get("ms"), "layout_ms": tuned.get("layout_ms"), "tile_ms": tuned.get("tile_ms")},
+        "autotune": {"ms": tuned.get("ms"), "layout_ms": tuned.get("layout_ms"), "tile_ms": tuned.get("tile_ms"),
+                     "grouped_ms": tuned.get("grouped_ms")},
         "workload_counts": {"tile_entries": entries, "visible_splats": visible},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "sm_peaks": sm_peaks,

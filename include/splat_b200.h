@@ -110,6 +110,10 @@ typedef struct splat_trainer_options {
   int32_t batch_depth;        /* splats the two-pixel kernels stage per round: 128 or 256 (0 picks 256) */
   int32_t persistent_raster;  /* 1: the two-pixel kernels run as persistent launches, resident blocks taking
                                  the tiles of every view of the step from one counter; 0: one block per tile */
+  int32_t grouped_backward;   /* the two-pixel float backward's sums. 0: each splat's twelve sums reduced over
+                                 the warp by a butterfly (the reference's way); 1: for groups of splats, the
+                                 pixels' two factors kept in shared memory and the sums made splat-parallel,
+                                 one lane per (splat, share of the warp's pixels). Scored views use 0. */
 } splat_trainer_options;
 
 /* LearningRates (src/train/trainer.hpp:51-61); trust_region must be 0. */
@@ -476,7 +480,9 @@ typedef struct splat_autotune_result {
   int32_t batch_depth;     /* the batch depth kept */
   int32_t persistent_raster; /* the launch form kept */
   double tile_ms[2][2][2]; /* milliseconds per gradient pass, [tile 16/32][batch 128/256][persistent 0/1], best
-                              layouts (0 where not timed) */
+                              layouts, the backward's sums as kept (0 where not timed) */
+  int32_t grouped_backward; /* the backward's sums kept */
+  double grouped_ms[2][2][2]; /* the same with grouped_backward 1 (0 where not timed) */
 } splat_autotune_result;
 
 /* The autotuner (new in this library; the reference has fixed 16x16 tiles and
@@ -485,8 +491,8 @@ typedef struct splat_autotune_result {
  * state nor the densification statistics), `repeats` passes each, then the
  * rasterizer's pixel layouts, then, where both layouts take two pixels per
  * thread and the sums are float, its tile edge (16, 32), batch depth (128,
- * 256) and launch form (one block per tile, persistent), and keeps the
- * fastest for the following steps. */
+ * 256), launch form (one block per tile, persistent) and the backward's sums
+ * (per splat, grouped), and keeps the fastest for the following steps. */
 int splat_trainer_autotune(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
                            int32_t repeats, splat_autotune_result *result);
 /* Turns per-stage CUDA-event timing on or off (off by default: it serialises). */

@@ -143,9 +143,14 @@ def test_config3_forms_against_fp64(splat, oracle):
     arrays = bench.make_scene()
     cam = bench.hemisphere_views()[0]
     target = bench.make_targets(1)[0]
-    forms = {"chosen": bench.chosen_options(splat), "plain": bench.plain_options(splat)}
+    forms = {"chosen": bench.chosen_options(splat), "plain": bench.plain_options(splat),
+             "chosen_grouped_32": bench.chosen_options(splat)}
     forms["chosen"].sort_form = splat.SORT_DEPTH_THEN_TILE
     forms["chosen"].forward_pixels_per_thread = 2
+    g = forms["chosen_grouped_32"]
+    g.sort_form = splat.SORT_DEPTH_THEN_TILE
+    g.forward_pixels_per_thread = g.backward_pixels_per_thread = 2
+    g.tile_size, g.grouped_backward, g.persistent_raster = 32, True, True
     result = bench.precision_vs_fp64(splat, torch, arrays, splat.Camera(*cam), oracle.View(*cam), target, forms)
     for name, r in result.items():
         print(f"  {name}: loss {r['loss']:.7f} vs {r['loss_fp64']:.7f}, PSNR {r['render_psnr_vs_fp64_db']:.1f} dB, "

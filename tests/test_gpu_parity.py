@@ -4,6 +4,7 @@ restatement (bit for bit on integer results, given the device's own projected
 splats). Every call goes through the C ABI."""
 from __future__ import annotations
 
+import itertools
 import math
 
 import numpy as np
@@ -379,7 +380,8 @@ def test_pixel_layouts_agree(splat, oracle, exact):
 
 @pytest.mark.parametrize("exact", [True, False])
 def test_tile_batch_and_launch_forms_agree(splat, oracle, exact):
-    # The two-pixel kernels at every tile edge, batch depth and launch form:
+    # The two-pixel kernels at every tile edge, batch depth, launch form and
+    # form of the backward's sums:
     # each pixel blends the same splats in the same order with the same
     # arithmetic, so the image is the same bits as the one-pixel reference
     # layout's; float sums in another order, so gradients to rounding. The
@@ -391,11 +393,10 @@ def test_tile_batch_and_launch_forms_agree(splat, oracle, exact):
     image0 = base.render(to_camera(view))
     base.compute_gradients(to_camera(view), target)
     g0 = base.gradients()
-    for tile in (16, 32):
-        for batch in (128, 256):
-            for persistent in (False, True):
+    for tile, batch, persistent, grouped in itertools.product((16, 32), (128, 256), (False, True), (False, True)):
                 opts = splat.TrainerOptions(exact_math=exact, forward_pixels_per_thread=2, backward_pixels_per_thread=2,
-                                            tile_size=tile, batch_depth=batch, persistent_raster=persistent)
+                                            tile_size=tile, batch_depth=batch, persistent_raster=persistent,
+                                            grouped_backward=grouped)
                 t = splat.Trainer(to_cloud(cloud), opts)
                 image = t.render(to_camera(view))
                 np.testing.assert_array_equal(image.view(np.uint32), image0.view(np.uint32),
@@ -403,8 +404,8 @@ def test_tile_batch_and_launch_forms_agree(splat, oracle, exact):
                 t.compute_gradients(to_camera(view), target)
                 g = t.gradients()
                 for name in ("positions", "scales", "rotations", "opacities", "sh"):
-                    check_close(getattr(g, name), getattr(g0, name), f"{name} t{tile} b{batch} p{int(persistent)}",
-                                0.99999, 1e-4)
+                    check_close(getattr(g, name), getattr(g0, name),
+                                f"{name} t{tile} b{batch} p{int(persistent)} g{int(grouped)}", 0.99999, 1e-4)
 
 
 def test_batched_persistent_matches_single_views(splat, oracle):

@@ -76,6 +76,7 @@ class _Options(ctypes.Structure):
         ("tile_size", ctypes.c_int32),
         ("batch_depth", ctypes.c_int32),
         ("persistent_raster", ctypes.c_int32),
+        ("grouped_backward", ctypes.c_int32),
     ]
 
 
@@ -151,7 +152,8 @@ class _Autotune(ctypes.Structure):
                 ("forward_pixels_per_thread", ctypes.c_int32), ("backward_pixels_per_thread", ctypes.c_int32),
                 ("ms", (ctypes.c_double * 3) * 2), ("layout_ms", (ctypes.c_double * 2) * 2),
                 ("tile_size", ctypes.c_int32), ("batch_depth", ctypes.c_int32), ("persistent_raster", ctypes.c_int32),
-                ("tile_ms", ((ctypes.c_double * 2) * 2) * 2)]
+                ("tile_ms", ((ctypes.c_double * 2) * 2) * 2), ("grouped_backward", ctypes.c_int32),
+                ("grouped_ms", ((ctypes.c_double * 2) * 2) * 2)]
 
 
 _lib.splat_trainer_autotune.argtypes = [_P, ctypes.POINTER(_Camera), _P, ctypes.c_size_t, ctypes.c_int32,
@@ -433,6 +435,7 @@ class TrainerOptions:
     tile_size: int = 16
     batch_depth: int = 256
     persistent_raster: bool = False
+    grouped_backward: bool = False
 
     def _c(self) -> _Options:
         o = _Options()
@@ -453,6 +456,7 @@ class TrainerOptions:
         o.blend_lists = int(self.blend_lists)
         o.tile_size, o.batch_depth = self.tile_size, self.batch_depth
         o.persistent_raster = int(self.persistent_raster)
+        o.grouped_backward = int(self.grouped_backward)
         return o
 
 
@@ -721,7 +725,10 @@ class Trainer:
                 "layout_ms": {f"fwd{f + 1}/bwd{b + 1}": r.layout_ms[f][b] for f in range(2) for b in range(2)},
                 "tile_size": r.tile_size, "batch_depth": r.batch_depth, "persistent_raster": r.persistent_raster,
                 "tile_ms": {f"tile{16 * (t + 1)}/batch{128 * (b + 1)}/persistent{q}": r.tile_ms[t][b][q]
-                            for t in range(2) for b in range(2) for q in range(2) if r.tile_ms[t][b][q] > 0}}
+                            for t in range(2) for b in range(2) for q in range(2) if r.tile_ms[t][b][q] > 0},
+                "grouped_backward": r.grouped_backward,
+                "grouped_ms": {f"tile{16 * (t + 1)}/batch{128 * (b + 1)}/persistent{q}": r.grouped_ms[t][b][q]
+                               for t in range(2) for b in range(2) for q in range(2) if r.grouped_ms[t][b][q] > 0}}
 
     def stream(self) -> int:
         """The cudaStream_t the trainer runs on, as an integer handle."""

@@ -117,6 +117,9 @@ struct RasterConfig {
   int batch = 256;
   uint32_t *workForward = nullptr;
   uint32_t *workBackward = nullptr;
+  // The two-pixel float backward's sums: a butterfly per (splat, warp), or,
+  // twoPhase, splat-parallel per group of splats (not for scored views).
+  bool twoPhase = false;
 };
 
 // train_forward.comp: one block per tile of 16x16 pixels. image: 4 floats per

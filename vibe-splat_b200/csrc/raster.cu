@@ -1027,6 +1027,224 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, backward2_blocks<T>())
                                    error, edge, s_batch, s_acc, s_min, s_cover);
 }
 
+// The float backward in two phases (new here; the reference sums each splat
+// over a 32-lane group, train_backward.glsl:51-76). A warp walks its 8x8
+// block's listed splats pixel-parallel exactly as k_backward2 does, but
+// keeps, instead of the splat's twelve sums, two numbers per pixel (dPower and
+// the blending weight wA) in shared memory, for a group of up to G splats
+// that reach any of its pixels. Then the group's sums are made splat-parallel:
+// lane i % G takes splat i, lane / G a share of the block's 64 pixels, and
+// walks only the pixels the splat reached, adding the twelve sums in
+// registers; the shares meet by shuffles, and one shared atomic per (splat,
+// value) adds the group's totals. The per-(splat, block) reduction of twelve
+// values over 32 lanes is gone; what remains per reached pixel is a dozen
+// fused multiply-adds. Float sums in another order than k_backward2's.
+// g0 = sum dAlpha e^power is taken as sum dPower / opacity (alpha = opacity
+// e^power wherever dAlpha is not zero).
+template <int T> __host__ __device__ constexpr int group_size() { return T > 16 ? 8 : 16; }
+
+template <int T> struct PairStore {
+  float2 v[group_size<T>()][64]; // per group splat, per pixel of the block: (dPower, wA)
+};
+
+template <int G, int T, int B>
+__device__ __forceinline__ void backward3_sums(int count, uint32_t myK, uint32_t myLo, uint32_t myHi, const Staged *s_batch,
+                                               const PairStore<T> &pairs, const float4 *pix, const float *pixAz, float perPixel,
+                                               float *s_acc) {
+  constexpr uint32_t P = 64u / (32u / G); // pixels of a lane's share
+  const uint32_t lane = threadIdx.x & 31u, i = lane % G, h = lane / G;
+  const uint32_t k = __shfl_sync(0xFFFFFFFFu, myK, i);
+  const uint32_t lo = __shfl_sync(0xFFFFFFFFu, myLo, i), hi = __shfl_sync(0xFFFFFFFFu, myHi, i);
+  float acc[12];
+#pragma unroll
+  for (int v = 0; v < 12; ++v) acc[v] = 0.0f;
+  if ((int)i < count) {
+    const Staged &s = s_batch[k];
+    const float cx = s.cx, cy = s.cy, qx = s.qx, qy = s.qy, qz = s.qz, invOp = 1.0f / s.opacity;
+    const uint32_t first = h * P;
+    uint32_t mask;
+    if constexpr (P == 32u) {
+      mask = h == 0u ? lo : hi;
+    } else {
+      const uint32_t word = first < 32u ? lo : hi;
+      mask = (word >> (first & 31u)) & ((1u << P) - 1u);
+    }
+    for (; mask != 0u; mask &= mask - 1u) {
+      const uint32_t p = first + (uint32_t)(__ffs(mask) - 1);
+      const float4 px = pix[p];
+      const float2 pd = pairs.v[i][p];
+      const float dx = px.x - cx, dy = px.y - cy;
+      const float vx = fmaf(qy, dy, qx * dx), vy = fmaf(qz, dy, qy * dx);
+      const float g1 = pd.x * vx, g2 = pd.x * vy;
+      acc[0] = fmaf(pd.x, invOp, acc[0]);
+      acc[1] += g1;
+      acc[2] += g2;
+      // Twice the conic sums; the flush halves them (exactly).
+      acc[3] = fmaf(g1, vx, acc[3]);
+      acc[4] = fmaf(g1, vy, acc[4]);
+      acc[5] = fmaf(g2, vy, acc[5]);
+      acc[6] = fmaf(pd.y, px.z, acc[6]);
+      acc[7] = fmaf(pd.y, px.w, acc[7]);
+      acc[8] = fmaf(pd.y, pixAz[p], acc[8]);
+      acc[9] += pd.y;
+      acc[10] += fabsf(g1);
+      acc[11] += fabsf(g2);
+    }
+  }
+#pragma unroll
+  for (uint32_t o = G; o < 32u; o <<= 1)
+#pragma unroll
+    for (int v = 0; v < 12; ++v) acc[v] += __shfl_xor_sync(0xFFFFFFFFu, acc[v], o);
+  if (h == 0u && (int)i < count) {
+    acc[9] *= perPixel;
+#pragma unroll
+    for (int v = 0; v < 12; ++v)
+      if (acc[v] != 0.0f) atomicAdd(&s_acc[k * kAccStride + v], acc[v]);
+  }
+}
+
+template <class M, int T, int B>
+__device__ __forceinline__ void backward3_tile(int tile, const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
+                                               const uint2 *__restrict__ ranges, const ViewSet &views, float bgR, float bgG,
+                                               float bgB, const float4 *__restrict__ image, const float4 *__restrict__ adjoint,
+                                               const uint32_t *__restrict__ stops, float *__restrict__ raw, uint32_t splatLimit,
+                                               uint32_t *error, Staged *s_batch, float *s_acc, uint32_t *s_min,
+                                               uint32_t (*s_cover)[B / 32], PairStore<T> *s_pairs, float4 (*s_pix)[64],
+                                               float (*s_az)[64]) {
+  constexpr int kThreads = TileShape<T>::kThreads, W = TileShape<T>::kWarps, G = group_size<T>();
+  const TileGeometry geo = tile_geometry(views, tile, T);
+  const ViewParams &cam = views.v[geo.view];
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const PixelPair<T> pp = pixel_pair<T>(geo, cam, t);
+  const uint2 range = ranges[tile];
+  float fr[2], ax[2], ay[2], az[2], bh[2];
+  uint32_t stop[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const size_t at = pp.inside[q] ? (size_t)cam.pixelBase + (size_t)pp.y[q] * cam.width + pp.x[q] : 0;
+    fr[q] = pp.inside[q] ? image[at].w : 0.0f;
+    const float4 a = pp.inside[q] ? adjoint[at] : make_float4(0.f, 0.f, 0.f, 0.f);
+    ax[q] = a.x;
+    ay[q] = a.y;
+    az[q] = a.z;
+    stop[q] = pp.inside[q] ? stops[at] : range.y;
+    bh[q] = fmaf(a.z, bgB, fmaf(a.y, bgG, a.x * bgR));
+    // The block's pixel table for the splat-parallel sums: pixel q * 32 + lane.
+    s_pix[warp][q * 32 + lane] = make_float4(pp.px[q], pp.py[q], a.x, a.y);
+    s_az[warp][q * 32 + lane] = a.z;
+  }
+  float2 front = make_float2(fr[0], fr[1]), behind = make_float2(bh[0], bh[1]);
+  const float2 Ax = make_float2(ax[0], ax[1]), Ay = make_float2(ay[0], ay[1]), Az = make_float2(az[0], az[1]);
+  const float px = pp.px[0];
+  const float2 py = make_float2(pp.py[0], pp.py[1]);
+  const float perPixel = cam.perPixel;
+  const uint32_t warpMin = __reduce_min_sync(0xFFFFFFFFu, min(stop[0], stop[1]));
+  if (lane == 0) s_min[warp] = warpMin;
+  for (int i = t; i < B * kAccStride; i += kThreads) s_acc[i] = 0.0f;
+  __syncthreads();
+  uint32_t tileStop = s_min[0];
+#pragma unroll
+  for (int w = 1; w < W; ++w) tileStop = min(tileStop, s_min[w]);
+  PairStore<T> &pairs = s_pairs[warp];
+
+  for (uint32_t start = tileStop; start < range.y; start += B) {
+    const uint32_t count = min((uint32_t)B, range.y - start);
+    __syncthreads();
+    stage_pairs<M, T, B>(splats, entryValues + start, count, splatLimit, geo, error, s_batch, s_cover, s_min, start);
+    __syncthreads();
+    int group = 0;
+    uint32_t myK = 0u, myLo = 0u, myHi = 0u; // lane i < group: the group's i-th splat and the pixels it reached
+    for (uint32_t word = 0; word <= ((count - 1u) >> 5); ++word)
+    for (uint32_t bits = s_cover[warp][word]; bits != 0u; bits &= bits - 1u) {
+      const uint32_t k = word * 32u + (uint32_t)(__ffs(bits) - 1);
+      const Staged &s = s_batch[k];
+      const auto mask = staged_mask<T>(s);
+      const float dx = px - s.cx;
+      const float2 dy = add2(py, f2(-s.cy));
+      const float2 power = splat_power2(s, dx, dy);
+      const float2 ep = make_float2(M::exp(fminf(power.x, 0.0f)), M::exp(fminf(power.y, 0.0f)));
+      const float2 oe = mul2(f2(s.opacity), ep);
+      const float2 alpha = make_float2(fminf(kAlphaMax, oe.x), fminf(kAlphaMax, oe.y));
+      const uint32_t entry = start + k;
+      const bool act0 = entry >= stop[0] && (mask & pp.bits[0]) == pp.bits[0] && !(power.x > 0.0f) && alpha.x >= kAlphaMin;
+      const bool act1 = entry >= stop[1] && (mask & pp.bits[1]) == pp.bits[1] && !(power.y > 0.0f) && alpha.y >= kAlphaMin;
+      const uint32_t lo = __ballot_sync(0xFFFFFFFFu, act0), hi = __ballot_sync(0xFFFFFFFFu, act1);
+      if ((lo | hi) == 0u) continue;
+      const float2 aAct = make_float2(act0 ? alpha.x : 0.0f, act1 ? alpha.y : 0.0f);
+      const float2 oneMinus = rsub2(aAct, f2(1.0f));
+      const float2 logRest = make_float2(M::log(oneMinus.x), M::log(oneMinus.y));
+      const float2 nextFront = rsub2(logRest, front);
+      const float2 Tf = make_float2(M::exp(nextFront.x), M::exp(nextFront.y));
+      const float2 wA = mul2(Tf, aAct);
+      const float2 ahead = rsub2(behind, fma2(Az, f2(s.b), fma2(Ay, f2(s.g), mul2(Ax, f2(s.r)))));
+      // At the 0.99 clamp alpha no longer depends on the parameters.
+      const float2 dT = mul2(Tf, ahead);
+      const float2 dAlpha = make_float2(act0 && oe.x < kAlphaMax ? dT.x : 0.0f, act1 && oe.y < kAlphaMax ? dT.y : 0.0f);
+      const float2 dPower = mul2(dAlpha, alpha);
+      behind = fma2(aAct, ahead, behind);
+      front = nextFront;
+      pairs.v[group][lane] = make_float2(dPower.x, wA.x);
+      pairs.v[group][32 + lane] = make_float2(dPower.y, wA.y);
+      if (lane == (uint32_t)group) {
+        myK = k;
+        myLo = lo;
+        myHi = hi;
+      }
+      if (++group == G) {
+        __syncwarp();
+        backward3_sums<G, T, B>(group, myK, myLo, myHi, s_batch, pairs, s_pix[warp], s_az[warp], perPixel, s_acc);
+        __syncwarp();
+        group = 0;
+      }
+    }
+    if (group > 0) {
+      __syncwarp();
+      backward3_sums<G, T, B>(group, myK, myLo, myHi, s_batch, pairs, s_pix[warp], s_az[warp], perPixel, s_acc);
+      __syncwarp();
+    }
+    __syncthreads();
+    // One global atomic per (splat, value) for the whole tile.
+    for (uint32_t j = t; j < count; j += kThreads) {
+      if (s_batch[j].mask == 0u && s_batch[j].maskHi == 0u) continue;
+      float *dst = raw + (size_t)s_batch[j].index * kRawStride;
+#pragma unroll
+      for (int v = 0; v < kGradValues; ++v) {
+        const float x = s_acc[j * kAccStride + v];
+        if (x != 0.0f) {
+          atomicAdd(dst + v, v >= 3 && v <= 5 ? 0.5f * x : x);
+          s_acc[j * kAccStride + v] = 0.0f;
+        }
+      }
+    }
+  }
+}
+
+template <class M, int T, int B>
+__global__ void __launch_bounds__(TileShape<T>::kThreads, T > 16 ? 1 : 4)
+    k_backward3(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
+                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
+                const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
+                uint32_t splatLimit, uint32_t *error, uint32_t *work) {
+  chain_enter();
+  constexpr int W = TileShape<T>::kWarps;
+  const ViewSet &views = *viewsPtr;
+  // Dynamic shared memory: each warp's pair store, then its pixel tables.
+  extern __shared__ __align__(16) unsigned char s_dynamic[];
+  PairStore<T> *s_pairs = reinterpret_cast<PairStore<T> *>(s_dynamic);
+  float4(*s_pix)[64] = reinterpret_cast<float4(*)[64]>(s_dynamic + W * sizeof(PairStore<T>));
+  float(*s_az)[64] = reinterpret_cast<float(*)[64]>(s_dynamic + W * (sizeof(PairStore<T>) + 64 * sizeof(float4)));
+  __shared__ Staged s_batch[B];
+  __shared__ float s_acc[B * kAccStride];
+  __shared__ uint32_t s_min[W];
+  __shared__ uint32_t s_cover[W][B / 32];
+  __shared__ uint32_t s_next;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next); tile >= 0;
+       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next))
+    backward3_tile<M, T, B>(tile, splats, entryValues, ranges, views, bgR, bgG, bgB, image, adjoint, stops, raw, splatLimit, error,
+                            s_batch, s_acc, s_min, s_cover, s_pairs, s_pix, s_az);
+}
+
 // Blocks of a kernel that fit on the GPU at once (its occupancy times the
 // SMs): the grid of a persistent launch. Asked once per kernel.
 uint32_t resident_blocks(const void *kernel, int threads) {
@@ -1065,6 +1283,34 @@ void launch_backward2(const Splat *splats, const uint32_t *entryValues, const ui
   if (cfg.workBackward != nullptr) grid = std::min(grid, resident_blocks((const void *)k_backward2<M, SCORE, T, B>, kThreads));
   launch_chained(k_backward2<M, SCORE, T, B>, dim3(grid), dim3(kThreads), 0, stream, splats, entryValues, ranges, dViews,
                  cfg.background[0], cfg.background[1], cfg.background[2], image, adjoint, stops, raw, splatLimit, error, edge,
+                 cfg.workBackward);
+}
+
+template <int T> constexpr size_t backward3_dynamic_bytes() {
+  return (size_t)TileShape<T>::kWarps * (sizeof(PairStore<T>) + 64 * sizeof(float4) + 64 * sizeof(float));
+}
+
+template <class M, int T, int B>
+void launch_backward3(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views,
+                      const ViewSet *dViews, const RasterConfig &cfg, const float4 *image, const float4 *adjoint,
+                      const uint32_t *stops, float *raw, uint32_t splatLimit, uint32_t *error, cudaStream_t stream) {
+  constexpr int kThreads = TileShape<T>::kThreads;
+  constexpr size_t kDynamic = backward3_dynamic_bytes<T>();
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_backward3<M, T, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDynamic);
+    configured = true;
+  }
+  uint32_t grid = (uint32_t)views.totalTiles;
+  if (cfg.workBackward != nullptr) {
+    int perSm = 0, device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_backward3<M, T, B>, kThreads, kDynamic);
+    grid = std::min(grid, (uint32_t)std::max(1, sms * std::max(perSm, 1)));
+  }
+  launch_chained(k_backward3<M, T, B>, dim3(grid), dim3(kThreads), kDynamic, stream, splats, entryValues, ranges, dViews,
+                 cfg.background[0], cfg.background[1], cfg.background[2], image, adjoint, stops, raw, splatLimit, error,
                  cfg.workBackward);
 }
 
@@ -1129,6 +1375,19 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
   const uint32_t tiles = views.totalTiles;
   const bool score = edge != nullptr;
   // The fixed-point sums keep the reference's 32-lane groups: one pixel per thread.
+  if (!fixedPoint && cfg.backwardPixels == 2 && cfg.twoPhase && !score) {
+    float *rawF = static_cast<float *>(raw);
+    dispatch_tile_batch(cfg, [&](auto T, auto B) {
+      constexpr int kT = decltype(T)::value, kB = decltype(B)::value;
+      if (cfg.exactMath)
+        launch_backward3<ExactMath, kT, kB>(splats, entryValues, ranges, views, dViews, cfg, image, adjoint, stops, rawF, splatLimit,
+                                            error, stream);
+      else
+        launch_backward3<FastMath, kT, kB>(splats, entryValues, ranges, views, dViews, cfg, image, adjoint, stops, rawF, splatLimit,
+                                           error, stream);
+    });
+    return;
+  }
   if (!fixedPoint && cfg.backwardPixels == 2) {
     float *rawF = static_cast<float *>(raw);
     dispatch_tile_batch(cfg, [&](auto T, auto B) {

@@ -169,6 +169,7 @@ public:
   int forwardPixels = 1, backwardPixels = 2; // pixels per thread of the compositing and float backward kernels
   int tileSize = 16, batchDepth = 256;        // the two-pixel kernels' tile edge and staging batch
   bool persistent = false;                    // the two-pixel kernels as persistent launches
+  bool groupedSums = false;                   // the two-pixel float backward's sums by groups
   DeviceBuffer workCounters;                  // their tile counters (2 words), cleared every step
   cudaStream_t stream = nullptr;
   // The step's clears run on a second stream, forked from and joined back to
@@ -352,6 +353,7 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   batchDepth = opt.batch_depth == 0 ? 256 : opt.batch_depth;
   if (batchDepth != 128 && batchDepth != 256) throw Failure{SPLAT_ERR_INVALID, "batch_depth must be 128 or 256"};
   persistent = opt.persistent_raster != 0;
+  groupedSums = opt.grouped_backward != 0;
   SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   SB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
   SB_CUDA(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
@@ -731,6 +733,7 @@ RasterConfig Trainer::raster_config() {
   for (int c = 0; c < 3; ++c) cfg.background[c] = opt.background[c];
   cfg.tile = views.tileSize;
   cfg.batch = batchDepth;
+  cfg.twoPhase = groupedSums;
   if (persistent) {
     if (forwardPixels == 2) cfg.workForward = workCounters.get<uint32_t>();
     if (backwardPixels == 2 && !fixedPoint) cfg.workBackward = workCounters.get<uint32_t>() + 1;
@@ -1246,14 +1249,16 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
   // tile edge, the staging batch and the launch form of those kernels.
   if (forwardPixels == 2 && backwardPixels == 2 && !fixedPoint && !blendLists) {
     int bestTile = tileSize, bestBatch = batchDepth;
-    bool bestPersistent = persistent;
+    bool bestPersistent = persistent, bestGrouped = groupedSums;
     double bestMs = 1e30;
+    for (int gi = 0; gi < 2; ++gi)
     for (int ti = 0; ti < 2; ++ti) {
       for (int bi = 0; bi < 2; ++bi) {
         for (int pi = 0; pi < 2; ++pi) {
           tileSize = 16 << ti;
           batchDepth = 128 << bi;
           persistent = pi == 1;
+          groupedSums = gi == 1;
           clear_graphs();
           splat_step_stats s{};
           run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
@@ -1262,12 +1267,13 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
           for (int r = 0; r < repeats; ++r) run(camera, targets, sizes, 1, ChainMode::Gradients, nullptr, false, &s);
           const double ms =
               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
-          result.tile_ms[ti][bi][pi] = ms;
+          (gi == 1 ? result.grouped_ms : result.tile_ms)[ti][bi][pi] = ms;
           if (ms < bestMs) {
             bestMs = ms;
             bestTile = tileSize;
             bestBatch = batchDepth;
             bestPersistent = persistent;
+            bestGrouped = groupedSums;
           }
         }
       }
@@ -1275,11 +1281,13 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
     tileSize = bestTile;
     batchDepth = bestBatch;
     persistent = bestPersistent;
+    groupedSums = bestGrouped;
     clear_graphs();
   }
   result.tile_size = raster_tile();
   result.batch_depth = batchDepth;
   result.persistent_raster = persistent ? 1 : 0;
+  result.grouped_backward = groupedSums ? 1 : 0;
   if (out != nullptr) *out = result;
 }
 
@@ -1406,6 +1414,7 @@ void splat_trainer_options_default(splat_trainer_options *o) {
   o->tile_size = 16;
   o->batch_depth = 256;
   o->persistent_raster = 0;
+  o->grouped_backward = 0;
 }
 
 void splat_learning_rates_default(splat_learning_rates *r) {
