@@ -831,7 +831,14 @@ def our_arm(args) -> None:
     chosen = chosen_options(splat)
     if args.sort_form is not None:
         chosen.sort_form = args.sort_form
-    trainer, ms, clocks, stats = run_form(chosen, "chosen", tune=args.sort_form is None and not args.no_autotune)
+    if args.form:
+        pixels, tile, batch, persistent, grouped = (int(v) for v in args.form.split(","))
+        chosen.sort_form = splat.SORT_DEPTH_THEN_TILE if args.sort_form is None else args.sort_form
+        chosen.forward_pixels_per_thread = chosen.backward_pixels_per_thread = pixels
+        chosen.tile_size, chosen.batch_depth = tile, batch
+        chosen.persistent_raster, chosen.grouped_backward = bool(persistent), bool(grouped)
+    trainer, ms, clocks, stats = run_form(chosen, "chosen",
+                                          tune=args.sort_form is None and not args.no_autotune and not args.form)
     ms = slowest_over_ranks(ms, dist, "cuda")
     ms_per_step = ms / args.steps
     value = whole_job_rate(world, args.steps, ms)
@@ -1145,6 +1152,9 @@ def main() -> None:
     parser.add_argument("--no-autotune", action="store_true", help="keep the chosen form's sort settings")
     parser.add_argument("--sort-form", type=int, choices=[0, 1], default=None,
                         help="override the chosen form's tile sort (0: depth then tile, 1: 64-bit tile|depth keys)")
+    parser.add_argument("--form", default=None,
+                        help="the chosen form's rasterizer settings instead of the autotuner's, as "
+                             "pixels,tile,batch,persistent,grouped (for example 2,32,128,1,1; for profiling runs)")
     parser.add_argument("--views", type=int, default=VIEWS,
                         help="cameras cycled through (default 64; fewer keep ncu captures small)")
     parser.add_argument("--gaussians", type=int, default=GAUSSIANS,
