@@ -506,12 +506,12 @@ void launch_bin_count(const Splat *splats, const float *reach, const uint32_t *i
 }
 
 void launch_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *gather, uint32_t *offsets, uint32_t *counters,
-                         uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream) {
+                         uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch) {
   if (items == 0) return;
   const uint32_t tiles = div_up(items, kScanTile);
   unsigned long long *status = static_cast<unsigned long long *>(scratch);
   uint32_t *ticket = reinterpret_cast<uint32_t *>(status + tiles);
-  cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
+  if (clearScratch) cudaMemsetAsync(scratch, 0, bin_scan_scratch_bytes(items), stream);
   launch_chained(k_offsets_scan, dim3(tiles), dim3(kScanThreads), 0, stream, items, counts, gather, offsets, counters, capacity, status,
                  ticket, error);
 }

@@ -77,8 +77,9 @@ size_t bin_scan_scratch_bytes(uint32_t items);
 void launch_bin_count(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat, uint32_t items,
                       uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *counts, uint32_t *masks, uint32_t *counters,
                       cudaStream_t stream);
+// clearScratch false: the caller cleared scratch (bin_scan_scratch_bytes) already.
 void launch_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *gather, uint32_t *offsets, uint32_t *counters,
-                         uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream);
+                         uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch = true);
 
 // train_bin_emit.comp. Depth-sorted form: tileKeys32[slot] = tile, entryValues[slot]
 // = splat. Single-sort form (tileKeys64 not null): tileKeys64[slot] = (global

@@ -779,6 +779,7 @@ void Trainer::record_prepare(bool backward) {
   if (countOverlap) {
     SB_CUDA(cudaEventRecord(countForkEvent, stream));
     SB_CUDA(cudaStreamWaitEvent(side, countForkEvent, 0));
+    SB_CUDA(cudaMemsetAsync(scanScratch.get(), 0, bin_scan_scratch_bytes(items), side));
     launch_bin_count(splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(), nullptr, n, n, views,
                      dViews.get<ViewSet>(), countsBySplat, masks, counters, side);
     SB_CUDA(cudaEventRecord(countEvent, side));
@@ -796,7 +797,7 @@ void Trainer::record_prepare(bool backward) {
   const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
   if (countOverlap) {
     SB_CUDA(cudaStreamWaitEvent(stream, countEvent, 0));
-    launch_offsets_scan(items, countsBySplat, itemSplat, offs, counters, entryCapacity, scanScratch.get(), error, stream);
+    launch_offsets_scan(items, countsBySplat, itemSplat, offs, counters, entryCapacity, scanScratch.get(), error, stream, false);
   } else {
     launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(), offs,
                           masks, counters, entryCapacity, scanScratch.get(), error, stream);
