@@ -491,13 +491,24 @@ def stage_bytes(n: int, visible: int, entries: int, pixels: int, depth_passes: i
     }
 
 
-def profile_figure(kind: str, stage: str):
+def form_key(opts) -> str:
+    """The rasterizer form a profile line must name for its figure to be used:
+    tile edge, batch depth, launch shape, backward sums and pixels per thread
+    decide which kernels the composite and backward stages launch."""
+    return (f"tile{opts.tile_size} batch{opts.batch_depth} {'persistent' if opts.persistent_raster else 'grid'} "
+            f"{'grouped' if opts.grouped_backward else 'atomic'} px{opts.forward_pixels_per_thread}/"
+            f"{opts.backward_pixels_per_thread}")
+
+
+def profile_figure(kind: str, stage: str, form: str):
     """A per-launch figure of the stage's kernel from the committed ncu summary
-    of the bench workload (profiles/*.md, a line '<kind> <stage>: N'): kind
-    'traffic' for DRAM bytes, 'instructions' for warp-instructions. Or None."""
+    of the bench workload (profiles/*.md, a line '<kind> <stage> [<form>]: N'):
+    kind 'traffic' for DRAM bytes, 'instructions' for warp-instructions. A line
+    taken on another rasterizer form (another kernel) is not used. Or None."""
+    head = f"{kind} {stage} [{form}]:"
     for path in sorted((ROOT / "profiles").glob("*.md")):
         for line in path.read_text().splitlines():
-            if line.startswith(f"{kind} {stage}:"):
+            if line.startswith(head):
                 try:
                     return int(line.split(":", 1)[1].strip().split()[0])
                 except ValueError:
@@ -505,8 +516,8 @@ def profile_figure(kind: str, stage: str):
     return None
 
 
-def measured_traffic(stage: str):
-    return profile_figure("traffic", stage)
+def measured_traffic(stage: str, form: str):
+    return profile_figure("traffic", stage, form)
 
 
 def chosen_options(splat):
@@ -887,6 +898,7 @@ def our_arm(args) -> None:
     digits_used = tuned.get("digit_bits", chosen.digit_bits)
     depth_passes = math.ceil(32 / digits_used)
     algorithmic = stage_bytes(n, visible, entries, pixels, depth_passes)
+    form = form_key(tuned_options(chosen, tuned))
     # The SM issue rate: measured by the library's FMA microbenchmark on this
     # GPU when it ran, else 148 SMs x 4 warp-instructions per clock at the SM
     # clock sampled during the timed steps (the maximum if none was sampled).
@@ -900,7 +912,7 @@ def our_arm(args) -> None:
             continue
         gbs = b / (ms_stage * 1e-3) / 1e9
         stage_roof[name] = {"bytes": b, "ms": ms_stage, "GB/s": gbs, "frac": gbs / hbm_peak}
-        inst = profile_figure("instructions", name)
+        inst = profile_figure("instructions", name, form)
         if inst:
             rate = inst / (ms_stage * 1e-3)
             stage_roof[name]["issue"] = {"warp_inst_per_s": rate, "peak": issue_peak, "frac": rate / issue_peak,
@@ -908,9 +920,9 @@ def our_arm(args) -> None:
     roof = None
     if dominant is not None and dominant in stage_roof:
         r = stage_roof[dominant]
-        traffic = measured_traffic(dominant)
+        traffic = measured_traffic(dominant, form)
         roof = {"kernel": dominant, "bound": "hbm", "achieved": r["GB/s"], "peak": hbm_peak, "unit": "GB/s",
-                "frac": r["frac"], "traffic": traffic, "ms": r["ms"],
+                "frac": r["frac"], "traffic": traffic, "ms": r["ms"], "form": form,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
         if dominant in ("backward", "composite"):
             roof["note"] = ("issue-bound, not HBM-bound: the SM instruction issue rate is the limit; 'issue' gives "
