@@ -223,11 +223,16 @@ def fd_config2(splat, torch, step: float = 1e-4, lam: float = 0.2) -> dict:
                            for name in ("positions", "scales", "rotations", "opacities", "sh")}
         if fixed:
             # Fixed-point sums resolve 1 / (3 W H 64) per warp total (the
-            # reference's scale): the criterion applies to the derivatives
-            # well above that resolution.
-            clear = np.abs(fd) > 1e-3 * np.abs(fd).max()
-            agree["above_resolution"] = dict(agreement(analytic[clear], fd[clear]), count=int(clear.sum()))
-            judged = agree["above_resolution"]
+            # reference's scale, about 8e-9 at 800x800). A warp's dL/dcov
+            # total, behind the scales and rotations, is mostly smaller and
+            # rounds away; the criterion applies to the groups it resolves.
+            resolved = np.isin(np.array([gr for gr, _ in picks]), ("positions", "opacities", "sh"))
+            agree["resolved_groups"] = dict(agreement(analytic[resolved], fd[resolved]), count=int(resolved.sum()),
+                                            groups=["positions", "opacities", "sh"])
+            agree["note"] = ("scales and rotations come from dL/dcov sums that mostly fall below the fixed scale "
+                             "1/(3 W H 64) per warp at 800x800 and round away (the reference's design); "
+                             "tests/test_configs.py checks splat by splat that this rounding is the whole difference")
+            judged = agree["resolved_groups"]
             cos, ratio = 0.97, 0.1
         else:
             judged, cos, ratio = agree, 0.999, 0.01
@@ -658,7 +663,9 @@ def memory_adjoint_summary(gaussians: int, steps: int, warmup: int) -> dict:
         if lists:
             opts.backward_pixels_per_thread = 1
         trainer = splat.Trainer(cloud, opts)
-        for i in range(warmup):
+        # Every view once at least, so that the entry and list buffers have
+        # grown to the largest view's before the timed steps.
+        for i in range(max(warmup, views)):
             stats = trainer.step_device_target(cams[i % views], targets[i % views].data_ptr(), rates)
         ms = time_steps(torch, trainer, lambda i: trainer.step_device_target(cams[i % views], targets[i % views].data_ptr(),
                                                                               rates), steps, trainer.stream())

@@ -12,7 +12,11 @@
   parameters, with the criteria of the reference's finite-difference test
   (tests/test_train.cpp:99-112: cosine > 0.999, length within 1 %) for the
   float sums and those of its fixed-point GPU test (:286-291: cosine > 0.97,
-  length within 10 %) for the fixed-point sums. The differences hold the
+  length within 10 %) for the fixed-point sums of positions, opacities and
+  SH. The fixed-point sums behind scales and rotations (dL/dcov) fall mostly
+  below the reference's fixed scale at this size and round away; that they
+  differ from the float form's sums by no more than that rounding is checked
+  splat by splat instead. The differences hold the
   base render's blended (splat, pixel) pairs fixed (oracle/fp64.py
   finite_differences): with the alpha cutoff live, pairs crossing 1/255
   jump the loss by more than the derivative carries at this size (the
@@ -82,6 +86,32 @@ def test_fp64_oracle_matches_the_twin(splat, oracle, case):
         assert rel < 1e-9, name
 
 
+def _fixed_sums_are_float_sums_rounded(splat, fixed_trainer, cloud, view, target, entries: int) -> None:
+    """Each splat's fixed-point sums (fixed_trainer's last gradient pass)
+    differ from the float form's by no more than their rounding: one
+    round-to-nearest of a warp's total per (warp, splat, value), 8 warps a
+    tile, so at most 4 tiles_j / scale for splat j, plus the float form's own
+    rounding (1e-4 relative, with a floor of 1e-6 of the value's largest
+    magnitude over the splats)."""
+    n = cloud.count
+    scale = 3.0 * view.width * view.height * 64.0
+    raw_fixed = fixed_trainer.debug_download(splat.DEBUG_RAW, np.int32)[: n * 16].reshape(n, 16)[:, :12]
+    values = fixed_trainer.debug_download(splat.DEBUG_ENTRY_VALUES, np.uint32)[:entries]
+    tiles = np.bincount(values, minlength=n).astype(np.float64)
+    float_trainer = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(sh_storage=splat.SH_F32,
+                                                                        state_storage=splat.STATE_F32))
+    float_trainer.compute_gradients(to_camera(view), target)
+    raw_float = float_trainer.debug_download(splat.DEBUG_RAW, np.float32)[: n * 16].reshape(n, 16)[:, :12]
+    raw_float = raw_float.astype(np.float64)
+    diff = np.abs(raw_fixed.astype(np.float64) / scale - raw_float)
+    bound = 4.0 * tiles[:, None] / scale + 1e-4 * np.abs(raw_float) + 1e-6 * np.abs(raw_float).max(axis=0)[None, :]
+    worst = diff / bound
+    print(f"  fixed vs float sums: worst |difference| / bound {worst.max():.3f} over {n} splats x 12 values")
+    kept = np.abs(raw_fixed[:, 3:6]).sum() / max(np.abs(raw_float[:, 3:6] * scale).sum(), 1.0)
+    print(f"  dL/dcov kept by the fixed scale: {kept:.3f} of the float form's magnitude")
+    assert (diff <= bound).all(), np.unravel_index(int(np.argmax(worst)), worst.shape)
+
+
 @pytest.mark.parametrize("fixed", [False, True])
 def test_config2_adjoint_against_fp64_central_differences(splat, oracle, fixed):
     import torch
@@ -114,16 +144,20 @@ def test_config2_adjoint_against_fp64_central_differences(splat, oracle, fixed):
     oracle_analytic = np.array([g64[group][index] for group, index in picks], np.float64)
     check_close(oracle_analytic, fd, "FP64 adjoint", 0.9999, 0.001)
     analytic = np.array([getattr(g, group)[index] for group, index in picks], np.float64)
+    groups = np.array([group for group, _ in picks])
     if fixed:
-        # Fixed-point sums resolve 1 / (3 W H 64) per warp total (the
-        # reference's scale, src/train/trainer.cpp:586-591): about 8e-9 here,
-        # the size of many SH derivatives at 800x800. The reference's
-        # fixed-point criterion applies where a derivative stands well above
-        # that; every pick's agreement is printed as well.
+        # The reference's fixed-point criterion (tests/test_train.cpp:286-291)
+        # on the groups whose per-warp sums stand above the fixed scale's
+        # resolution at this size. The covariance sums behind scales and
+        # rotations mostly do not: 1 / (3 W H 64) per warp total (the
+        # reference's scale, src/train/trainer.cpp:589) is about 8e-9 here,
+        # and a warp's dL/dcov total at 800x800 is often smaller, so it
+        # rounds away. That their deviation is this rounding and nothing else
+        # is checked below, against the float form's sums.
+        resolved = np.isin(groups, ("positions", "opacities", "sh"))
+        check_close(analytic[resolved], fd[resolved], "positions, opacities, SH", 0.97, 0.1)
         check_close(analytic, fd, "256 parameters (all)", -1.0, 1.0)
-        clear = np.abs(fd) > 1e-3 * np.abs(fd).max()
-        assert clear.sum() >= 64
-        check_close(analytic[clear], fd[clear], f"{int(clear.sum())} above resolution", 0.97, 0.1)
+        _fixed_sums_are_float_sums_rounded(splat, trainer, cloud, view, target, stats.tile_entries)
     else:
         check_close(analytic, fd, "256 parameters", 0.999, 0.01)
     for name in ("positions", "scales", "rotations", "opacities", "sh"):
