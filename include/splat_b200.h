@@ -492,7 +492,9 @@ typedef struct splat_autotune_result {
  * rasterizer's pixel layouts, then, where both layouts take two pixels per
  * thread and the sums are float, its tile edge (16, 32), batch depth (128,
  * 256), launch form (one block per tile, persistent) and the backward's sums
- * (per splat, grouped), and keeps the fastest for the following steps. */
+ * (per splat, grouped), and keeps the fastest for the following steps. A
+ * stage keeps the trainer's configured setting unless another is more than
+ * 1 % faster, so that timing noise does not flip the form between runs. */
 int splat_trainer_autotune(splat_trainer *trainer, const splat_camera *camera, const uint8_t *target, size_t target_bytes,
                            int32_t repeats, splat_autotune_result *result);
 /* Turns per-stage CUDA-event timing on or off (off by default: it serialises). */

@@ -265,6 +265,40 @@ def test_fused_step_matches_split_step(splat, oracle, sh_storage, state_storage,
         np.testing.assert_array_equal(getattr(results[0][1], name), getattr(results[1][1], name), err_msg=name)
 
 
+@pytest.mark.parametrize("fixed", [False, True])
+def test_selective_step_moves_exactly_the_reached_gaussians(splat, oracle, fixed):
+    # Selective Adam steps the Gaussians the view reached (some backward sum
+    # non-zero) from a list of them: with float and fixed-point sums, every
+    # Gaussian whose sums are all zero keeps its parameters bit for bit, and
+    # every reached one moves. Dense, opaque Gaussians hide most of the cloud.
+    view = oracle.train_camera(96, 80)
+    target = oracle.smooth_target(96, 80, 5)
+    cloud = oracle.random_cloud(6000, 3, 77)
+    cloud.opacities[:] = 4.0
+    rates = splat.LearningRates(position=1e-3)
+    t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(force_fixed_point=fixed))
+    t.step(to_camera(view), target, rates)
+    before = t.cloud()
+    t.step(to_camera(view), target, rates)
+    after = t.cloud()
+    n = cloud.count
+    raw = t.debug_download(splat.DEBUG_RAW, np.uint32)[: n * 16].reshape(n, 16)[:, :14]
+    if fixed:
+        reached = (raw != 0).any(axis=1)
+    else:
+        reached = (raw.view(np.float32) != 0.0).any(axis=1)
+    print(f"  {int(reached.sum())} of {n} Gaussians reached")
+    assert reached.sum() > 100 and (~reached).sum() > 100
+    for name, per in (("positions", 3), ("scales", 3), ("rotations", 4), ("opacities", 1)):
+        b = getattr(before, name).reshape(n, per)
+        a = getattr(after, name).reshape(n, per)
+        np.testing.assert_array_equal(a[~reached], b[~reached], err_msg=name)
+    moved = (after.positions.reshape(n, 3) != before.positions.reshape(n, 3)).any(axis=1)
+    assert moved[reached].mean() > 0.99
+    sh_b, sh_a = before.sh.reshape(n, -1), after.sh.reshape(n, -1)
+    np.testing.assert_array_equal(sh_a[~reached], sh_b[~reached])
+
+
 def test_training_lowers_the_loss(splat, oracle):
     # In the spirit of tests/test_train.cpp:493-520: fit a rendered view.
     view = oracle.train_camera(96, 72)

@@ -846,6 +846,193 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   }
 }
 
+// Selective Adam with no penalty leaves a Gaussian the view did not reach
+// (every backward sum zero) exactly as it was, and behind the front layers of
+// a scene most Gaussians are not reached: one thread per Gaussian would run
+// the chain rule and the step with a few lanes of each warp. So k_touched
+// lists the reached Gaussians and k_chain_touched runs the one-view step over
+// the list, one thread per listed Gaussian, full warps. The list's order
+// (warp-aggregated appends) varies from run to run and does not matter: a
+// Gaussian's step reads and writes its own values only, with its own hash
+// indices, so the results are those of k_chain_step, bit for bit.
+//
+// touched[0] is the count (cleared before k_touched), the list starts at
+// touched[kTouchedListStart].
+constexpr uint32_t kTouchedListStart = 32;
+
+template <bool FIXED>
+__global__ void __launch_bounds__(256) k_touched(const void *__restrict__ rawIn, uint32_t n, uint32_t *touched,
+                                                 const uint32_t *error) {
+  chain_enter();
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
+  bool reached = false;
+  if (i < n) {
+    const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4 w4 = r4[q];
+      const uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        // As k_chain_step's test raw[k] != 0.0f: an integer sum is non-zero
+        // exactly when its value is; a float sum of -0 counts as zero.
+        if (q * 4 + e < kRawPerSplat) reached = reached || (FIXED ? w[e] != 0u : __uint_as_float(w[e]) != 0.0f);
+      }
+    }
+  }
+  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, reached);
+  if (mask == 0u) return;
+  uint32_t base = 0;
+  if (lane == (uint32_t)(__ffs(mask) - 1)) base = atomicAdd(touched, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xFFFFFFFFu, base, __ffs(mask) - 1);
+  if (reached) touched[kTouchedListStart + base + __popc(mask & ((1u << lane) - 1u))] = i;
+}
+
+template <ShStore S, StateStore ST, bool FIXED>
+__global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSet *__restrict__ viewsPtr,
+                                                      const void *__restrict__ rawIn, const Splat *__restrict__ splats,
+                                                      const ChainArgs *__restrict__ argsPtr, OptimState state,
+                                                      float *__restrict__ densifyStats, const uint32_t *__restrict__ touched,
+                                                      const uint32_t *error) {
+  chain_enter();
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const ViewParams &cam = viewsPtr->v[0];
+  const uint32_t count = touched[0], n = p.n, ps = p.planeStride;
+  const ChainArgs args = *argsPtr;
+  const AdamArgs a = adam_args(args);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+    const uint32_t i = touched[kTouchedListStart + j];
+    const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
+    const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
+    const float rawOpacity = p.opacities[i];
+    const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
+    float raw[kRawPerSplat];
+    {
+      const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
+      uint32_t words[16];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint4 w4 = r4[q];
+        words[q * 4] = w4.x;
+        words[q * 4 + 1] = w4.y;
+        words[q * 4 + 2] = w4.z;
+        words[q * 4 + 3] = w4.w;
+      }
+#pragma unroll
+      for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
+    }
+    const float opacity = 1.0f / (1.0f + splat_expf(-rawOpacity));
+    float gP[3] = {0.f, 0.f, 0.f}, gScale[3] = {0.f, 0.f, 0.f}, gRot[4] = {0.f, 0.f, 0.f, 0.f}, gOpacity = 0.f;
+    float gColour[3] = {0.f, 0.f, 0.f}, dir[3] = {0.f, 0.f, 0.f}, gPv[3] = {0.f, 0.f, 0.f}, distance = 1.0f;
+    const float4 col = splats[i].colorRadius;
+    if (args.statistics) {
+      float4 *st = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
+      float4 sa = st[0], sb = st[1];
+      const float hx = 0.5f * cam.widthF, hy = 0.5f * cam.heightF;
+      const float ax = raw[1] * hx, ay = raw[2] * hy;
+      sa.x += sqrtf(fmaf(ay, ay, ax * ax));
+      sa.y += 1.0f;
+      sa.z = fmaxf(sa.z, col.w);
+      sa.w += raw[9] * 3.0f * cam.widthF * cam.heightF;
+      const float bx = raw[10] * hx, by = raw[11] * hy;
+      sb.x += sqrtf(fmaf(by, by, bx * bx));
+      st[0] = sa;
+      st[1] = sb;
+    }
+    chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
+    const int active = min(cam.activeCoeffs, p.shCoeffs);
+    if (cam.activeDegree > 0) {
+      float gDir[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 1; k < kMaxCoeffs; ++k) {
+        if (k >= active) break;
+        const float value[3] = {sh_coefficient<S>(p, i, k, 0), sh_coefficient<S>(p, i, k, 1), sh_coefficient<S>(p, i, k, 2)};
+        direction_term(k, value, gColour, dir, gDir);
+      }
+      add_direction_term(gDir, dir, distance, gPv);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
+
+    // Adam on the 11 geometry elements, as k_chain_step (selective: an
+    // element with a zero gradient is left alone).
+    {
+      float gv[11], value[11], m[11], vv[11];
+      uint32_t word[11];
+#pragma unroll
+      for (int e = 0; e < 11; ++e) {
+        const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+        const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+        const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+        const uint32_t idx = i * per + (uint32_t)a0;
+        gv[e] = group == 0 ? gP[a0] : group == 1 ? gScale[a0] : group == 2 ? gRot[a0] : gOpacity;
+        value[e] = group == 0 ? pos[a0] : group == 1 ? logScale[a0] : group == 3 ? rawOpacity
+                 : a0 == 0 ? rq.x : a0 == 1 ? rq.y : a0 == 2 ? rq.z : rq.w;
+        m[e] = vv[e] = 0.0f;
+        word[e] = 0u;
+        if (gv[e] == 0.0f) continue;
+        load_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e]);
+      }
+#pragma unroll
+      for (int e = 0; e < 11; ++e) {
+        const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+        const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+        const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+        const uint32_t idx = i * per + (uint32_t)a0;
+        if (gv[e] == 0.0f) continue;
+        adam(value[e], m[e], vv[e], gv[e], args.rates[group], a);
+        store_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e], idx * 5u + (uint32_t)group, a.seed);
+        float *values = group == 0 ? p.positions : group == 1 ? p.scales : group == 2 ? p.rotations : p.opacities;
+        values[idx] = value[e];
+      }
+    }
+
+    // The SH step: only the coefficients in use have a gradient.
+    const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
+    const uint32_t hashBase = i * shFloats * 5u + 4u;
+    uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + i;
+    const size_t stateCount = (size_t)ps * shFloats; // F32: the v planes follow the m planes
+    auto element = [&](uint32_t plane, float &val, float g, float rate) {
+      if constexpr (ST == StateStore::F32) {
+        float *sf = reinterpret_cast<float *>(stateWords);
+        float m = sf[(size_t)plane * ps], v = sf[stateCount + (size_t)plane * ps];
+        adam(val, m, v, g, rate, a);
+        sf[(size_t)plane * ps] = m;
+        sf[stateCount + (size_t)plane * ps] = v;
+      } else {
+        const uint32_t word = stateWords[(size_t)plane * ps];
+        float m = bf16_load(word, 0), v = bf16_load(word, 1);
+        adam(val, m, v, g, rate, a);
+        stateWords[(size_t)plane * ps] = bf16_pair(m, v, hashBase + plane * 5u, a.seed);
+      }
+    };
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float g = active > 0 ? fmaf(basis_one(0, dir[0], dir[1], dir[2]), gColour[c], 0.0f) : 0.0f;
+      if (g == 0.0f) continue;
+      float val = p.shDc[(size_t)c * ps + i];
+      element((uint32_t)c, val, g, args.rates[4]);
+      p.shDc[(size_t)c * ps + i] = val;
+    }
+    const float restRate = args.rates[4] * args.restScale;
+#pragma unroll 1
+    for (int k = 1; k < active; ++k) {
+      const float b = basis_one(k, dir[0], dir[1], dir[2]);
+      const uint32_t r = (uint32_t)(k - 1) * 3u;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float g = fmaf(b, gColour[c], 0.0f);
+        if (g == 0.0f) continue;
+        const uint32_t plane = r + 3u + (uint32_t)c;
+        float val = load_sh_rest<S>(p.shRest, (size_t)(r + (uint32_t)c) * ps + i);
+        element(plane, val, g, restRate);
+        store_sh_rest<S>(p.shRest, (size_t)(r + (uint32_t)c) * ps + i, val, hashBase + plane * 5u, args.seed);
+      }
+    }
+  }
+}
+
 // train_score.comp: to each Gaussian's statistics, the marked pixels it
 // reached (raw value 12, in pixels), that count times the view's loss, and its
 // edge score (raw value 13, in pixels).
@@ -867,13 +1054,33 @@ __global__ void __launch_bounds__(256) k_score(const void *__restrict__ rawIn, b
 template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                     const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
-                    uint32_t *error, cudaStream_t stream) {
+                    uint32_t *touched, uint32_t *error, cudaStream_t stream) {
   const GradientsOut g = *grads;
   const bool store = args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
   const bool multi = views.count > 1;
   // The fused form indexes the F32 SH state (two planes of n * 48 floats) in 32 bits.
   if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.planeStride * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
+    if (touched != nullptr && args.selective && args.opacityReg == 0.0f && args.scaleReg == 0.0f) {
+      // Only the reached Gaussians change: list them, then step the list.
+      cudaMemsetAsync(touched, 0, 4, stream);
+      if (args.fixedPoint) launch_chained(k_touched<true>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
+      else launch_chained(k_touched<false>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
+      const uint32_t grid = std::min<uint32_t>(blocks, resident_blocks((const void *)k_chain_touched<S, StateStore::BF16Pair, false>, 128));
+#define SB_TOUCHED(ST, FIX)                                                                                          \
+  launch_chained(k_chain_touched<S, ST, FIX>, dim3(grid), dim3(128), 0, stream, p, dViews, raw, splats, dArgs, state, \
+                 densifyStats, (const uint32_t *)touched, (const uint32_t *)error)
+      const bool f32 = state.store == StateStore::F32;
+      if (args.fixedPoint) {
+        if (f32) SB_TOUCHED(StateStore::F32, true);
+        else SB_TOUCHED(StateStore::BF16Pair, true);
+      } else {
+        if (f32) SB_TOUCHED(StateStore::F32, false);
+        else SB_TOUCHED(StateStore::BF16Pair, false);
+      }
+#undef SB_TOUCHED
+      return;
+    }
     const uint32_t smem = step_stage_bytes(p.shCoeffs, S == ShStore::F32 ? 4 : 2, state.store == StateStore::F32);
     const uint32_t stepBlocks = div_up(p.n, kStepThreads);
 #define SB_STEP(ST, FIX)                                                                                           \
@@ -918,17 +1125,17 @@ void launch_score(const void *raw, bool fixedPoint, float fixedScale, uint32_t n
 
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
-                  uint32_t *error, cudaStream_t stream) {
+                  uint32_t *touched, uint32_t *error, cudaStream_t stream) {
   if (p.n == 0) return;
   switch (p.shStore) {
   case ShStore::BF16:
-    launch_chain_s<ShStore::BF16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
+    launch_chain_s<ShStore::BF16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, touched, error, stream);
     break;
   case ShStore::F16:
-    launch_chain_s<ShStore::F16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
+    launch_chain_s<ShStore::F16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, touched, error, stream);
     break;
   default:
-    launch_chain_s<ShStore::F32>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
+    launch_chain_s<ShStore::F32>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, touched, error, stream);
     break;
   }
 }

@@ -1245,6 +1245,8 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, T > 16 ? 1 : 4)
                             s_batch, s_acc, s_min, s_cover, s_pairs, s_pix, s_az);
 }
 
+} // namespace
+
 // Blocks of a kernel that fit on the GPU at once (its occupancy times the
 // SMs): the grid of a persistent launch. Asked once per kernel.
 uint32_t resident_blocks(const void *kernel, int threads) {
@@ -1261,6 +1263,8 @@ uint32_t resident_blocks(const void *kernel, int threads) {
   known.emplace(kernel, blocks);
   return blocks;
 }
+
+namespace {
 
 template <class M, int T, int B>
 void launch_forward2(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views, const ViewSet *dViews,

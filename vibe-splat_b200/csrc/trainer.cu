@@ -205,6 +205,7 @@ public:
   // Per (view, Gaussian).
   int viewSlots = 0;
   DeviceBuffer splats, reach, depthKeys, values, tmpKeys, tmpValues, offsets, raw, shGrad;
+  DeviceBuffer touched; // the one-view selective step's count and list of reached Gaussians
   // Tile entries.
   uint32_t entryCapacity = 0;
   DeviceBuffer entryKeys, entryValues, tmpEntryKeys, tmpEntryValues;
@@ -458,11 +459,13 @@ uint64_t Trainer::bytes_per_gaussian() const {
   const uint64_t floats = 3 + 3 + 4 + 1 + 3ull * shCoeffs;
   const uint64_t params = (3 + 3 + 4 + 1 + 3) * 4 + rest;
   const uint64_t optimiser = floats * (stateStore == StateStore::F32 ? 8 : 4);
-  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets and
-  // reached-tile masks 8, raw sums 64, colour gradient and direction for the SH step 32.
-  const uint64_t perView = sizeof(Splat) + 4 + 16 + 8 + kRawStride * 4 + 32;
-  // Geometry gradients between the chain rule and Adam: 11 floats.
-  return params + optimiser + 11 * 4 + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
+  // Per view: splat 48, reach 4, keys/values and their copies 16, offsets,
+  // reached-tile masks and counts 12, raw sums 64, colour gradient and
+  // direction for the SH step 32.
+  const uint64_t perView = sizeof(Splat) + 4 + 16 + 12 + kRawStride * 4 + 32;
+  // Geometry gradients between the chain rule and Adam: 11 floats; the list
+  // of reached Gaussians: 1.
+  return params + optimiser + 12 * 4 + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
 }
 
 uint64_t Trainer::entry_bytes(uint64_t entries) const {
@@ -574,6 +577,7 @@ void Trainer::ensure_view_buffers() {
     offsets.ensure(items * 12); // entry offsets, the reached-tile masks, then (depth-sorted form) the counts per splat
     raw.ensure(items * kRawStride * 4);
     shGrad.ensure(items * 32);
+    touched.ensure(((size_t)n + 32) * 4);
     SB_CUDA(cudaMemset(raw.get(), 0, items * kRawStride * 4));
     viewSlots = count;
     clear_graphs();
@@ -919,7 +923,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   const GradientsOut *gp = &g;
   begin(7);
   launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
-               shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
+               shGrad.get<float4>(), densifyStats.get<float>(), touched.get<uint32_t>(), error, stream);
   end(7);
 }
 
@@ -1187,10 +1191,13 @@ void Trainer::set_sort(bool single, int digits) {
 void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t bytes, int repeats,
                        splat_autotune_result *out) {
   if (repeats < 1) repeats = 1;
-  const bool oldSingle = oneSort;
-  const int oldDigits = digitBits;
-  double best = 1e30;
-  int bestForm = oneSort ? 1 : 0, bestDigits = digitBits;
+  // A candidate replaces the configured setting of a stage only when it is
+  // more than kKeep faster: differences inside the timing noise do not flip
+  // the form from one run to the next.
+  constexpr double kKeep = 1.01;
+  const int oldForm = oneSort ? 1 : 0, oldDigits = digitBits;
+  double best = 1e30, configuredMs = -1.0;
+  int bestForm = oldForm, bestDigits = digitBits;
   const uint8_t *targets[1] = {target};
   const size_t sizes[1] = {bytes};
   splat_autotune_result result{};
@@ -1206,6 +1213,7 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
       const double ms =
           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
       result.ms[form][digits - 6] = ms;
+      if (form == oldForm && digits == oldDigits) configuredMs = ms;
       if (ms < best) {
         best = ms;
         bestForm = form;
@@ -1213,15 +1221,19 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
       }
     }
   }
-  (void)oldSingle;
-  (void)oldDigits;
+  if (configuredMs > 0.0 && configuredMs <= best * kKeep) {
+    bestForm = oldForm;
+    bestDigits = oldDigits;
+  }
   set_sort(bestForm == 1, bestDigits);
   result.sort_form = bestForm;
   result.digit_bits = bestDigits;
   // Then the rasterizer's layouts with that sort (the graphs are keyed by
   // shape only, so they are dropped before each change).
+  const int oldForward = forwardPixels, oldBackward = backwardPixels;
   int bestForward = forwardPixels, bestBackward = backwardPixels;
   double bestLayoutMs = 1e30;
+  configuredMs = -1.0;
   for (int fwd = 1; fwd <= 2; ++fwd) {
     for (int bwd = 1; bwd <= 2; ++bwd) {
       forwardPixels = fwd;
@@ -1234,12 +1246,17 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
       const double ms =
           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
       result.layout_ms[fwd - 1][bwd - 1] = ms;
+      if (fwd == oldForward && bwd == oldBackward) configuredMs = ms;
       if (ms < bestLayoutMs) {
         bestLayoutMs = ms;
         bestForward = fwd;
         bestBackward = bwd;
       }
     }
+  }
+  if (configuredMs > 0.0 && configuredMs <= bestLayoutMs * kKeep) {
+    bestForward = oldForward;
+    bestBackward = oldBackward;
   }
   forwardPixels = bestForward;
   backwardPixels = bestBackward;
@@ -1249,9 +1266,12 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
   // Then, where both layouts take two pixels per thread with float sums, the
   // tile edge, the staging batch and the launch form of those kernels.
   if (forwardPixels == 2 && backwardPixels == 2 && !fixedPoint && !blendLists) {
+    const int oldTile = tileSize, oldBatch = batchDepth;
+    const bool oldPersistent = persistent, oldGrouped = groupedSums;
     int bestTile = tileSize, bestBatch = batchDepth;
     bool bestPersistent = persistent, bestGrouped = groupedSums;
     double bestMs = 1e30;
+    configuredMs = -1.0;
     for (int gi = 0; gi < 2; ++gi)
     for (int ti = 0; ti < 2; ++ti) {
       for (int bi = 0; bi < 2; ++bi) {
@@ -1269,6 +1289,8 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
           const double ms =
               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / repeats;
           (gi == 1 ? result.grouped_ms : result.tile_ms)[ti][bi][pi] = ms;
+          if (tileSize == oldTile && batchDepth == oldBatch && persistent == oldPersistent && groupedSums == oldGrouped)
+            configuredMs = ms;
           if (ms < bestMs) {
             bestMs = ms;
             bestTile = tileSize;
@@ -1278,6 +1300,12 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
           }
         }
       }
+    }
+    if (configuredMs > 0.0 && configuredMs <= bestMs * kKeep) {
+      bestTile = oldTile;
+      bestBatch = oldBatch;
+      bestPersistent = oldPersistent;
+      bestGrouped = oldGrouped;
     }
     tileSize = bestTile;
     batchDepth = bestBatch;
@@ -1516,8 +1544,8 @@ int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_r
     sb::GradientsOut g{};
     for (int k = 0; k < 5; ++k) g.g[k] = t->grads[k].get<float>();
     sb::launch_chain(t->params(), t->views, t->dViews.get<sb::ViewSet>(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
-                     t->dArgs.get<sb::ChainArgs>(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
-                     t->stream);
+                     t->dArgs.get<sb::ChainArgs>(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(),
+                     t->touched.get<uint32_t>(), nullptr, t->stream);
     SB_CUDA(cudaStreamSynchronize(t->stream));
   });
 }
