@@ -22,18 +22,29 @@ __device__ __forceinline__ void chain_enter() {
   chain_release();
 }
 
+// The launch also carries its stream's priority, so that a kernel captured
+// into a graph keeps it: where two streams' kernels share the GPU (the depth
+// sort beside the tile count), blocks of the higher-priority one are placed
+// first as SM slots free up.
 template <typename... Params, typename... Args>
 inline void launch_chained(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args &&...args) {
-  cudaLaunchAttribute attribute[1];
+  cudaLaunchAttribute attribute[2];
   attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attribute[0].val.programmaticStreamSerializationAllowed = 1;
+  int priority = 0;
+  unsigned count = 1;
+  if (cudaStreamGetPriority(stream, &priority) == cudaSuccess) {
+    attribute[1].id = cudaLaunchAttributePriority;
+    attribute[1].val.priority = priority;
+    count = 2;
+  }
   cudaLaunchConfig_t config{};
   config.gridDim = grid;
   config.blockDim = block;
   config.dynamicSmemBytes = smem;
   config.stream = stream;
   config.attrs = attribute;
-  config.numAttrs = 1;
+  config.numAttrs = count;
   cudaLaunchKernelEx(&config, kernel, std::forward<Args>(args)...);
 }
 

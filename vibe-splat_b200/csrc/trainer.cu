@@ -355,8 +355,13 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   if (batchDepth != 128 && batchDepth != 256) throw Failure{SPLAT_ERR_INVALID, "batch_depth must be 128 or 256"};
   persistent = opt.persistent_raster != 0;
   groupedSums = opt.grouped_backward != 0;
-  SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  SB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  // The step's own stream at the greatest priority, the second stream (the
+  // clears and the tile count beside the depth sort) at the least: the sort's
+  // passes, one after another, are the longer chain.
+  int leastPriority = 0, greatestPriority = 0;
+  SB_CUDA(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+  SB_CUDA(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatestPriority));
+  SB_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, leastPriority));
   SB_CUDA(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&countForkEvent, cudaEventDisableTiming));
