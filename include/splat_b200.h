@@ -537,6 +537,49 @@ int splat_cloud_load_ply(const char *path, int32_t *count, int32_t *sh_degree, f
                          float *rotations, float *opacities, float *sh);
 int splat_cloud_save_ply(const char *path, const splat_cloud *cloud);
 
+/* CGC files (src/splat/cgc.hpp:15-50, save_cgc and load_cgc): the lossy
+ * layered format for viewing over the network. A file holds three importance
+ * layers (opacity times cross-section percentiles), each with its own
+ * precision: positions on a symlog grid around the scene's median, stored as
+ * gaps along a Morton curve; canonical axes; YCoCg colour; opacity; the higher
+ * SH bands as labels into a per-layer k-means codebook; every byte column its
+ * own LZMA stream. splat_cloud_save_cgc needs a CUDA device (the per-splat
+ * work, the order statistics, the Morton sort and the codebook run on it) and
+ * writes nothing when it fails; a cloud with a NaN or infinite value is refused
+ * with SPLAT_ERR_INVALID, as the reference throws. splat_cloud_load_cgc reads
+ * versions 1 and 2 on the host, with splat_cloud_load_ply's two-call protocol;
+ * splats come back layer by layer, each layer in Morton order, with their axes
+ * possibly permuted and flipped (the same ellipsoids). */
+enum { SPLAT_CGC_BALANCED = 0, SPLAT_CGC_SMALL = 1 };
+typedef struct splat_cgc_options {
+  int32_t preset; /* SPLAT_CGC_BALANCED (about 28x smaller than .ply) or SPLAT_CGC_SMALL (about 31x) */
+  int32_t fast;   /* much quicker and a little larger (training checkpoints) */
+} splat_cgc_options;
+typedef struct splat_cgc_stats {
+  uint64_t bytes;           /* size of the written file */
+  uint64_t layer_counts[3]; /* splats per layer, most important first */
+} splat_cgc_stats;
+/* options may be null (balanced, not fast); stats may be null. */
+int splat_cloud_save_cgc(const char *path, const splat_cloud *cloud, const splat_cgc_options *options, splat_cgc_stats *stats);
+int splat_cloud_load_cgc(const char *path, int32_t *count, int32_t *sh_degree, float *positions, float *scales,
+                         float *rotations, float *opacities, float *sh);
+/* The CGC pieces the reference exposes for its unit tests
+ * (cgc_detail::morton_code, canonicalize_axes, src/splat/cgc.hpp:50-58): the
+ * low 21 bits of x, y, z interleaved (x into bit 0); log scales sorted
+ * descending with the quaternion (w, x, y, z) rewritten so that w is its
+ * largest component and not negative (a zero quaternion is the identity). */
+uint64_t splat_cgc_morton_code(uint32_t x, uint32_t y, uint32_t z);
+int splat_cgc_canonicalize_axes(float *log_scales, float *wxyz);
+/* The reference's LZMA helpers (src/splat/lzma.hpp:10-17): an "alone" (.lzma)
+ * stream from preset `level` (0-9, extreme flag) with lc, lp, pb; *written
+ * gets its size, and min(capacity, size) bytes are copied when out is not
+ * null. splat_lzma_decompress fails (SPLAT_ERR_INVALID) on corrupt or
+ * truncated data and on any size but `expected`. liblzma.so.5 is loaded at
+ * the first call. */
+int splat_lzma_compress(const uint8_t *data, size_t size, int32_t level, int32_t extreme, int32_t lc, int32_t lp, int32_t pb,
+                        uint8_t *out, size_t capacity, size_t *written);
+int splat_lzma_decompress(const uint8_t *stream, size_t size, uint8_t *out, size_t expected);
+
 /* Stage-level entry points on device memory, for the reference's operator
  * tests (tests/test_radix_sort.cpp) and for callers with their own buffers. */
 

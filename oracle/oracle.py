@@ -384,6 +384,58 @@ def ref_load_ply(path) -> Cloud:
     return Cloud(d.value, *arrays)
 
 
+def ref_save_cgc(cloud: Cloud, path, preset: int = 0, fast: bool = False) -> dict:
+    """The reference's save_cgc (src/splat/cgc.cpp), with the LZMA shim."""
+    keep, cargs = _cloud_args(cloud)
+    stats = np.zeros(4, np.uint64)
+    lib = ref_lib()
+    status = lib.ref_save_cgc(str(path).encode(), ctypes.c_int(cloud.count), ctypes.c_int(cloud.sh_degree), *cargs,
+                              ctypes.c_int(preset), ctypes.c_int(int(fast)), stats.ctypes.data_as(ctypes.c_void_p))
+    if status != 0:
+        raise ValueError(f"the reference's save_cgc refused {path}")
+    return {"bytes": int(stats[0]), "layer_counts": [int(v) for v in stats[1:]]}
+
+
+def ref_load_cgc(path) -> Cloud:
+    """The reference's load_cgc (src/splat/cgc.cpp); raises ValueError where it throws."""
+    lib = ref_lib()
+    n, d = ctypes.c_int(), ctypes.c_int()
+    if lib.ref_load_cgc(str(path).encode(), ctypes.byref(n), ctypes.byref(d), None, None, None, None, None) != 0:
+        raise ValueError(f"the reference's load_cgc refused {path}")
+    arrays = [np.zeros(n.value * k, np.float32) for k in (3, 3, 4, 1, 3 * (d.value + 1) ** 2)]
+    assert lib.ref_load_cgc(str(path).encode(), ctypes.byref(n), ctypes.byref(d), *[_fp(a) for a in arrays]) == 0
+    return Cloud(d.value, *arrays)
+
+
+def ref_cgc_morton(x: int, y: int, z: int) -> int:
+    """cgc_detail::morton_code (src/splat/cgc.hpp:53-55)."""
+    lib = ref_lib()
+    lib.ref_cgc_morton.restype = ctypes.c_uint64
+    return int(lib.ref_cgc_morton(ctypes.c_uint32(x), ctypes.c_uint32(y), ctypes.c_uint32(z)))
+
+
+def ref_cgc_canonicalize(scales, wxyz):
+    """cgc_detail::canonicalize_axes (src/splat/cgc.hpp:57-58): new (scales, quaternion)."""
+    s = np.array(scales, np.float32)
+    q = np.array(wxyz, np.float32)
+    ref_lib().ref_cgc_canonicalize(_fp(s), _fp(q))
+    return s, q
+
+
+def ref_lzma_compress(data: bytes, level: int = 9, extreme: bool = True, lc: int = 3, lp: int = 0, pb: int = 2) -> bytes:
+    """lzma_compress (src/splat/lzma.hpp:13) over the shim."""
+    lib = ref_lib()
+    lib.ref_lzma_compress.restype = ctypes.c_longlong
+    buf = np.frombuffer(data, np.uint8) if data else np.zeros(1, np.uint8)
+    args = (buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(len(data)), ctypes.c_int(level), ctypes.c_int(int(extreme)),
+            ctypes.c_int(lc), ctypes.c_int(lp), ctypes.c_int(pb))
+    size = lib.ref_lzma_compress(*args, None, ctypes.c_size_t(0))
+    assert size >= 0
+    out = np.zeros(max(size, 1), np.uint8)
+    assert lib.ref_lzma_compress(*args, out.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(size)) == size
+    return out[:size].tobytes()
+
+
 def ref_marked_pixels(cloud: Cloud, view: View, target: np.ndarray, share: float, background=(0.0, 0.0, 0.0),
                       near: float = 0.01) -> np.ndarray:
     """reference_marked_pixels: per Gaussian, the pixels it reaches whose mean

@@ -9,6 +9,8 @@
 // log-scales 3, quaternions (w,x,y,z) 4, opacity logits 1, SH [k][rgb].
 // The camera is the reference's Camera (src/render/camera.hpp:84-89): a
 // column-major world->camera matrix, the camera centre, fx, fy, cx, cy, size.
+#include "splat/cgc.hpp"
+#include "splat/lzma.hpp"
 #include "train/densify.hpp"
 #include "train/reference.hpp"
 #include "train/schedule.hpp"
@@ -160,6 +162,68 @@ int ref_load_ply(const char *path, int *n, int *degree, float *positions, float 
     return 0;
   } catch (const std::exception &) {
     return 1;
+  }
+}
+
+// save_cgc (src/splat/cgc.cpp): the reference's CGC writer; preset 0
+// balanced, 1 small. stats: bytes, then the three layer counts.
+int ref_save_cgc(const char *path, int n, int degree, const float *positions, const float *scales, const float *rotations,
+                 const float *opacities, const float *sh, int preset, int fast, std::uint64_t *stats) {
+  try {
+    CgcOptions options;
+    options.preset = preset == 1 ? CgcPreset::Small : CgcPreset::Balanced;
+    options.fast = fast != 0;
+    const CgcStats s = save_cgc(make_cloud(n, degree, positions, scales, rotations, opacities, sh), path, options);
+    if (stats != nullptr) {
+      stats[0] = s.bytes;
+      for (int l = 0; l < 3; ++l) stats[1 + l] = s.layerCounts[static_cast<std::size_t>(l)];
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// load_cgc (src/splat/cgc.cpp): the reference's CGC reader, as ref_load_ply.
+int ref_load_cgc(const char *path, int *n, int *degree, float *positions, float *scales, float *rotations, float *opacities,
+                 float *sh) {
+  try {
+    const GaussianCloud c = load_cgc(path);
+    *n = static_cast<int>(c.size());
+    *degree = c.shDegree;
+    if (positions != nullptr) {
+      std::memcpy(positions, c.positions.data(), c.positions.size() * sizeof(float));
+      std::memcpy(scales, c.scales.data(), c.scales.size() * sizeof(float));
+      std::memcpy(rotations, c.rotations.data(), c.rotations.size() * sizeof(float));
+      std::memcpy(opacities, c.opacities.data(), c.opacities.size() * sizeof(float));
+      std::memcpy(sh, c.sh.data(), c.sh.size() * sizeof(float));
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return 1;
+  }
+}
+
+// cgc_detail::morton_code and canonicalize_axes (src/splat/cgc.hpp:53-58).
+std::uint64_t ref_cgc_morton(std::uint32_t x, std::uint32_t y, std::uint32_t z) { return cgc_detail::morton_code(x, y, z); }
+void ref_cgc_canonicalize(float *scales3, float *wxyz) {
+  std::array<float, 3> s = {scales3[0], scales3[1], scales3[2]};
+  std::array<float, 4> q = {wxyz[0], wxyz[1], wxyz[2], wxyz[3]};
+  cgc_detail::canonicalize_axes(s, q);
+  std::copy(s.begin(), s.end(), scales3);
+  std::copy(q.begin(), q.end(), wxyz);
+}
+
+// lzma_compress / lzma_decompress (src/splat/lzma.hpp), through the shim.
+// Returns the size written (or needed), or -1.
+long long ref_lzma_compress(const std::uint8_t *data, std::size_t size, int level, int extreme, int lc, int lp, int pb,
+                            std::uint8_t *out, std::size_t capacity) {
+  try {
+    const auto packed = lzma_compress(std::as_bytes(std::span(data, size)), level, extreme != 0, lc, lp, pb);
+    if (out != nullptr) std::memcpy(out, packed.data(), std::min(capacity, packed.size()));
+    return static_cast<long long>(packed.size());
+  } catch (const std::exception &) {
+    return -1;
   }
 }
 

@@ -1,0 +1,415 @@
+"""CGC files (src/splat/cgc.hpp, cgc.cpp) and the LZMA helpers
+(src/splat/lzma.hpp), against the reference's own writer and reader compiled
+from its sources into oracle/_ref (with oracle/lzma_shim.cpp in place of its
+liblzma wrapper, whose header the image lacks).
+
+CPU tests (host code of the library): LZMA streams byte for byte equal to the
+reference wrapper's; Morton codes and canonical axes bit for bit; the reader
+on files the reference wrote (every SH degree, sizes 0 to 1000, both presets,
+fast and full) equal to the reference's reader bit for bit, version 1 files
+included; malformed files refused by both. GPU tests: files this library
+writes read back identically by both readers, and the reference's round-trip
+quality cases (tests/test_cgc.cpp:140-330) on them.
+"""
+from __future__ import annotations
+
+import lzma
+import struct
+
+import numpy as np
+import pytest
+
+from tests.conftest import splat_module
+
+needs_reference = pytest.mark.skipif("not __import__('oracle.oracle', fromlist=['x']).have_reference()",
+                                     reason="the reference's FP64 twin was not built here")
+
+
+@pytest.fixture(scope="module")
+def S():
+    return splat_module()
+
+
+@pytest.fixture(scope="module")
+def O():
+    from oracle import oracle
+
+    return oracle
+
+
+def sample_data() -> bytes:
+    # tests/test_cgc.cpp:29-35: a periodic run, then noise (seeded here).
+    periodic = bytes(i % 7 * 31 for i in range(90_000))
+    noise = np.random.default_rng(7).integers(0, 256, 10_000, dtype=np.uint8).tobytes()
+    return periodic + noise
+
+
+def random_cloud(S, count: int, degree: int, seed: int):
+    """The shapes of tests/test_cgc.cpp:142-159's clouds, seeded numpy draws:
+    positions U(0, 10), log scales U(-6, -1), unit quaternions, opacity logits
+    U(-4, 4), DC U(-1.5, 1.5), higher SH U(-0.3, 0.3)."""
+    rng = np.random.default_rng(seed)
+    coeffs = (degree + 1) ** 2
+    q = rng.normal(size=(count, 4)).astype(np.float32)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    sh = rng.uniform(-0.3, 0.3, (count, coeffs, 3)).astype(np.float32)
+    sh[:, 0, :] = rng.uniform(-1.5, 1.5, (count, 3))
+    return S.GaussianCloud(degree, rng.uniform(0, 10, count * 3).astype(np.float32),
+                           rng.uniform(-6, -1, count * 3).astype(np.float32), q.ravel(),
+                           rng.uniform(-4, 4, count).astype(np.float32), sh.ravel())
+
+
+def to_oracle(O, cloud):
+    return O.Cloud(cloud.sh_degree, cloud.positions, cloud.scales, cloud.rotations, cloud.opacities, cloud.sh)
+
+
+def same_bits(a, b) -> None:
+    assert a.sh_degree == b.sh_degree
+    for name in ("positions", "scales", "rotations", "opacities", "sh"):
+        x = np.asarray(getattr(a, name), np.float32)
+        y = np.asarray(getattr(b, name), np.float32)
+        assert x.shape == y.shape, name
+        np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32), err_msg=name)
+
+
+# ----------------------------------------------------------------- CPU
+
+
+@needs_reference
+@pytest.mark.parametrize("level,extreme,lc,lp,pb", [(9, True, 3, 0, 2), (1, False, 3, 0, 2), (6, False, 0, 0, 0)])
+def test_lzma_streams_equal_the_reference_wrappers(S, O, level, extreme, lc, lp, pb):
+    data = sample_data()
+    packed = S.lzma_compress(data, level, extreme, lc, lp, pb)
+    assert packed == O.ref_lzma_compress(data, level, extreme, lc, lp, pb)
+    assert len(packed) < len(data)
+    assert S.lzma_decompress(packed, len(data)) == data
+    # Python's own liblzma binding gives the same "alone" stream.
+    filters = [{"id": lzma.FILTER_LZMA1, "preset": level | (lzma.PRESET_EXTREME if extreme else 0), "lc": lc, "lp": lp, "pb": pb}]
+    assert packed == lzma.compress(data, format=lzma.FORMAT_ALONE, filters=filters)
+
+
+def test_lzma_round_trips_empty_input_and_rejects_bad_input(S):
+    # tests/test_cgc.cpp:45-66.
+    assert S.lzma_decompress(S.lzma_compress(b""), 0) == b""
+    data = sample_data()
+    packed = S.lzma_compress(data)
+    with pytest.raises(S.SplatError):
+        S.lzma_decompress(packed[:-10], len(data))
+    bad = bytearray(packed)
+    bad[0] = 0xFF
+    with pytest.raises(S.SplatError):
+        S.lzma_decompress(bytes(bad), len(data))
+    with pytest.raises(S.SplatError):
+        S.lzma_decompress(packed, len(data) + 1)
+    with pytest.raises(S.SplatError):
+        S.lzma_decompress(packed, len(data) - 1)
+
+
+@needs_reference
+def test_morton_codes_interleave_bits(S, O):
+    # tests/test_cgc.cpp:68-74, then random triples against the reference.
+    assert S.cgc_morton_code(1, 0, 0) == 1
+    assert S.cgc_morton_code(0, 1, 0) == 2
+    assert S.cgc_morton_code(0, 0, 1) == 4
+    assert S.cgc_morton_code(3, 0, 0) == 9
+    assert S.cgc_morton_code(0x1FFFFF, 0x1FFFFF, 0x1FFFFF) == (1 << 63) - 1
+    rng = np.random.default_rng(1)
+    for x, y, z in rng.integers(0, 1 << 21, (500, 3)):
+        assert S.cgc_morton_code(int(x), int(y), int(z)) == O.ref_cgc_morton(int(x), int(y), int(z))
+
+
+@needs_reference
+def test_canonical_axes_equal_the_references(S, O):
+    # tests/test_cgc.cpp:113-135: 2000 random ellipsoids, and the zero quaternion.
+    rng = np.random.default_rng(3)
+    for _ in range(2000):
+        s = rng.uniform(-5, 1, 3).astype(np.float32)
+        if rng.random() < 0.1:
+            s[1] = s[0]  # ties keep their order
+        q = rng.normal(size=4).astype(np.float32)
+        ours = S.cgc_canonicalize_axes(s, q)
+        ref = O.ref_cgc_canonicalize(s, q)
+        np.testing.assert_array_equal(ours[0].view(np.uint32), ref[0].view(np.uint32))
+        np.testing.assert_array_equal(ours[1].view(np.uint32), ref[1].view(np.uint32))
+        assert ours[0][0] >= ours[0][1] >= ours[0][2]
+        assert ours[1][0] >= 0.0 and all(ours[1][0] >= abs(v) - 1e-5 for v in ours[1][1:])
+    s, q = S.cgc_canonicalize_axes([1.0, 2.0, 3.0], [0.0, 0.0, 0.0, 0.0])
+    assert list(s) == [3.0, 2.0, 1.0]
+    assert abs(float(q @ q) - 1.0) < 1e-5
+
+
+@needs_reference
+@pytest.mark.parametrize("count,degree,preset,fast", [
+    (0, 2, 0, False), (1, 2, 0, False), (2, 0, 0, False), (3, 3, 1, False), (257, 2, 0, True),
+    (1000, 0, 0, False), (1000, 1, 1, False), (1000, 2, 0, True), (1000, 3, 0, False)])
+def test_reader_decodes_the_references_files_as_the_reference(S, O, tmp_path, count, degree, preset, fast):
+    cloud = random_cloud(S, count, degree, 11 + degree + count)
+    path = tmp_path / "ref.cgc"
+    stats = O.ref_save_cgc(to_oracle(O, cloud), path, preset, fast)
+    assert sum(stats["layer_counts"]) == count
+    ours, theirs = S.load_cgc(path), O.ref_load_cgc(path)
+    assert ours.size() == count
+    same_bits(ours, theirs)
+
+
+def _v1_file(n: int, degrees: np.ndarray, seed: int) -> bytes:
+    """A version 1 file (the layout load_cgc still reads, src/splat/cgc.cpp
+    load_v1): a 16-byte header, then one LZMA stream of the count, colour and
+    SH ranges, per-256-splat boxes and byte planes."""
+    rng = np.random.default_rng(seed)
+    chunks = (n + 255) // 256
+
+    def planes(words: np.ndarray) -> bytes:
+        w = np.asarray(words, np.uint32)
+        return b"".join(((w >> (8 * b)) & 0xFF).astype(np.uint8).tobytes() for b in range(4))
+
+    lo = rng.uniform(-3, 0, (chunks, 6)).astype(np.float32)
+    box = np.concatenate([lo[:, :3], lo[:, :3] + rng.uniform(0.5, 4, (chunks, 3)).astype(np.float32),
+                          lo[:, 3:], lo[:, 3:] + rng.uniform(0.5, 2, (chunks, 3)).astype(np.float32)], axis=1)
+    payload = struct.pack("<I", n) + np.array([0.1, 0.0, 0.2, 0.9, 1.0, 0.8, 0.6, 0.4, 0.3], np.float32).tobytes()
+    payload += planes(box.astype(np.float32).view(np.uint32).ravel())
+    payload += planes(rng.integers(0, 1 << 32, n, dtype=np.uint64))
+    payload += planes(rng.integers(0, 1 << 32, n, dtype=np.uint64))
+    payload += rng.integers(0, 256, 7 * n, dtype=np.uint8).tobytes() + degrees.astype(np.uint8).tobytes()
+    for band in range(1, int(degrees.max(initial=0)) + 1):
+        members = int((degrees >= band).sum())
+        payload += rng.integers(0, 256, members * 3 * (2 * band + 1), dtype=np.uint8).tobytes()
+    stream = lzma.compress(payload, format=lzma.FORMAT_ALONE)
+    return b"CGC\0" + struct.pack("<IQ", 1, len(payload)) + stream
+
+
+@needs_reference
+@pytest.mark.parametrize("n", [1, 300, 600])
+def test_reader_decodes_version_1_files_as_the_reference(S, O, tmp_path, n):
+    degrees = np.random.default_rng(n).integers(0, 4, n)
+    path = tmp_path / "v1.cgc"
+    path.write_bytes(_v1_file(n, degrees, n))
+    same_bits(S.load_cgc(path), O.ref_load_cgc(path))
+
+
+@needs_reference
+def test_malformed_files_are_refused_by_both_readers(S, O, tmp_path):
+    cloud = random_cloud(S, 300, 2, 5)
+    good = tmp_path / "good.cgc"
+    O.ref_save_cgc(to_oracle(O, cloud), good)
+    data = good.read_bytes()
+    cases = {
+        "magic": b"XGC\0" + data[4:],
+        "version": data[:4] + struct.pack("<I", 7) + data[8:],
+        "truncated": data[:-20],
+        "trailing": data + b"\0",
+        "short": data[:6],
+        "stream": data[:200] + bytes(b ^ 0x5A for b in data[200:260]) + data[260:],
+    }
+    for name, bad in cases.items():
+        path = tmp_path / f"{name}.cgc"
+        path.write_bytes(bad)
+        with pytest.raises(S.SplatError) as refused:
+            S.load_cgc(path)
+        assert refused.value.status == S.SPLAT_ERR_INVALID, name
+        with pytest.raises(ValueError):
+            O.ref_load_cgc(path)
+    with pytest.raises(S.SplatError):
+        S.load_cgc(tmp_path / "missing.cgc")
+
+
+# ----------------------------------------------------------------- GPU
+
+
+def _covariances(scales: np.ndarray, rotations: np.ndarray) -> np.ndarray:
+    """R diag(exp(2 s)) R^T per splat, its 6 unique entries (tests/test_cgc.cpp:90-108)."""
+    q = rotations.reshape(-1, 4).astype(np.float64)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    r = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+                  np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+                  np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+    d = np.exp(2.0 * scales.reshape(-1, 3).astype(np.float64))
+    cov = np.einsum("nia,na,nja->nij", r, d, r)
+    iu = np.triu_indices(3)
+    return cov[:, iu[0], iu[1]]
+
+
+def _nearest(original, loaded) -> np.ndarray:
+    a = original.positions.reshape(-1, 3).astype(np.float64)
+    b = loaded.positions.reshape(-1, 3).astype(np.float64)
+    out = np.empty(len(b), np.int64)
+    for start in range(0, len(b), 512):
+        d = ((b[start:start + 512, None, :] - a[None, :, :]) ** 2).sum(-1)
+        out[start:start + 512] = d.argmin(1)
+    return out
+
+
+def check_round_trip(original, loaded, skip: int = -1) -> int:
+    """tests/test_cgc.cpp:184-211: each loaded splat against the nearest
+    original: position within 0.02, covariance within a quarter of the largest
+    axis's square, opacity within 1/32; returns the DC colours off by more
+    than 0.06."""
+    n = original.size()
+    assert loaded.size() == n and loaded.sh_degree == original.sh_degree
+    if n == 0:
+        return 0
+    i = _nearest(original, loaded)
+    keep = i != skip
+    i = i[keep]
+    pos_o = original.positions.reshape(-1, 3)[i]
+    pos_l = loaded.positions.reshape(-1, 3)[keep]
+    assert np.abs(pos_l - pos_o).max() <= 0.02
+    so, sl = original.scales.reshape(-1, 3)[i], loaded.scales.reshape(-1, 3)[keep]
+    biggest = np.exp(2.0 * so.max(axis=1).astype(np.float64))
+    ca = _covariances(so, original.rotations.reshape(-1, 4)[i])
+    cb = _covariances(sl, loaded.rotations.reshape(-1, 4)[keep])
+    assert (np.abs(ca - cb) <= 0.25 * biggest[:, None] + 1e-12).all()
+    sig = lambda v: 1.0 / (1.0 + np.exp(-v.astype(np.float64)))
+    assert (np.abs(sig(loaded.opacities[keep]) - sig(original.opacities[i])) <= 1.0 / 32.0 + 1e-5).all()
+    coeffs = (original.sh_degree + 1) ** 2
+    want = 0.28209479177387814 * original.sh.reshape(n, coeffs, 3)[i, 0, :] + 0.5
+    got = 0.28209479177387814 * loaded.sh.reshape(n, coeffs, 3)[keep, 0, :] + 0.5
+    return int((np.abs(want - got) > 0.06).sum())
+
+
+def _round_trip(S, cloud, path, **kw):
+    stats = S.save_cgc(cloud, path, **kw)
+    assert stats["bytes"] == path.stat().st_size
+    return S.load_cgc(path), stats
+
+
+@pytest.mark.gpu
+@needs_reference
+@pytest.mark.parametrize("count,degree,preset,fast", [
+    (0, 2, 0, False), (1, 2, 0, False), (2, 0, 0, False), (3, 3, 1, False), (256, 1, 0, False), (257, 2, 0, True),
+    (1000, 0, 0, False), (1000, 3, 1, False), (5000, 3, 0, True)])
+def test_written_files_read_identically_by_both_readers(splat, O, tmp_path, count, degree, preset, fast):
+    cloud = random_cloud(splat, count, degree, 31 + count)
+    path = tmp_path / "ours.cgc"
+    loaded, stats = _round_trip(splat, cloud, path, preset=preset, fast=fast)
+    assert sum(stats["layer_counts"]) == count
+    same_bits(loaded, O.ref_load_cgc(path))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("degree", [0, 1, 2, 3])
+def test_round_trip_within_the_quantisation_steps(splat, tmp_path, degree):
+    # tests/test_cgc.cpp:232-244.
+    cloud = random_cloud(splat, 1000, degree, 11 + degree)
+    loaded, stats = _round_trip(splat, cloud, tmp_path / "rt.cgc")
+    assert stats["bytes"] > 0 and sum(stats["layer_counts"]) == 1000
+    assert check_round_trip(cloud, loaded) <= 10
+    assert np.isfinite(loaded.sh).all()
+
+
+@pytest.mark.gpu
+def test_codebook_reproduces_a_few_distinct_patterns(splat, tmp_path):
+    # tests/test_cgc.cpp:246-258: 8 SH patterns over 4000 splats.
+    cloud = random_cloud(splat, 4000, 3, 5)
+    patterns = np.random.default_rng(6).normal(0.0, 0.2, (8, 45)).astype(np.float32)
+    sh = cloud.sh.reshape(4000, 48)
+    sh[:, 3:] = patterns[np.arange(4000) % 8]
+    loaded, _ = _round_trip(splat, cloud, tmp_path / "patterns.cgc")
+    i = _nearest(cloud, loaded)
+    rms = float(np.sqrt(((cloud.sh.reshape(4000, 48)[i, 3:] - loaded.sh.reshape(4000, 48)[:, 3:]) ** 2).mean()))
+    print(f"  SH rms error {rms:.4f}")
+    assert rms < 0.03
+
+
+@pytest.mark.gpu
+def test_empty_higher_bands_stay_empty(splat, tmp_path):
+    cloud = random_cloud(splat, 500, 3, 5)
+    cloud.sh.reshape(500, 48)[:, 3:] = 0.0
+    loaded, _ = _round_trip(splat, cloud, tmp_path / "dc.cgc")
+    assert (loaded.sh.reshape(500, 48)[:, 3:] == 0.0).all()
+
+
+@pytest.mark.gpu
+def test_a_colour_outlier_does_not_coarsen_the_others(splat, tmp_path):
+    # tests/test_cgc.cpp:272-288.
+    base = random_cloud(splat, 1000, 1, 21)
+    positions = np.concatenate([base.positions, np.float32([5, 5, 11])])
+    scales = np.full(1001 * 3, -3.0, np.float32)
+    rotations = np.concatenate([base.rotations, np.float32([1, 0, 0, 0])])
+    opacities = np.full(1001, 2.0, np.float32)
+    sh = np.concatenate([base.sh, np.float32([100, 100, 100] + [0] * 9)])
+    cloud = splat.GaussianCloud(1, positions, scales, rotations, opacities, sh)
+    loaded, _ = _round_trip(splat, cloud, tmp_path / "outlier.cgc")
+    assert check_round_trip(cloud, loaded, skip=1000) <= 10
+    assert np.isfinite(loaded.sh).all()
+
+
+@pytest.mark.gpu
+def test_small_degenerate_and_far_away_clouds(splat, tmp_path):
+    # tests/test_cgc.cpp:290-326.
+    for count in (0, 1, 2, 3, 256, 257):
+        cloud = random_cloud(splat, count, 2, 31)
+        loaded, _ = _round_trip(splat, cloud, tmp_path / "sizes.cgc")
+        assert loaded.size() == count
+        check_round_trip(cloud, loaded)
+    same = random_cloud(splat, 300, 1, 41)
+    same.positions.reshape(300, 3)[:] = (1.0, 2.0, 3.0)
+    same.scales[:] = -2.0
+    loaded, _ = _round_trip(splat, same, tmp_path / "flat.cgc")
+    assert np.abs(loaded.positions.reshape(300, 3) - np.float32([1, 2, 3])).max() < 1e-4
+    assert np.abs(loaded.scales.reshape(300, 3)[:, 0] + 2.0).max() < 0.1
+    floater = random_cloud(splat, 1000, 0, 73)
+    floater.positions[0] = 1e5
+    loaded, _ = _round_trip(splat, floater, tmp_path / "floater.cgc")
+    near = loaded.positions.reshape(-1, 3)[:, 0] <= 1000.0
+    i = _nearest(floater, loaded)[near]
+    assert np.abs(loaded.positions.reshape(-1, 3)[near] - floater.positions.reshape(-1, 3)[i]).max() <= 0.2
+
+
+@pytest.mark.gpu
+def test_extreme_values_stay_finite_and_non_finite_is_refused(splat, tmp_path):
+    # tests/test_cgc.cpp:328-361.
+    cloud = random_cloud(splat, 4, 0, 51)
+    cloud.opacities[:] = (50.0, -50.0, 0.0, 3.0)
+    cloud.scales[0], cloud.scales[1] = -30.0, 10.0
+    loaded, _ = _round_trip(splat, cloud, tmp_path / "extreme.cgc")
+    assert np.isfinite(loaded.opacities).all() and np.isfinite(loaded.scales).all()
+    for field, index, value in (("positions", 4, np.nan), ("sh", 7, np.inf)):
+        bad = random_cloud(splat, 10, 1, 61)
+        getattr(bad, field)[index] = value
+        path = tmp_path / f"{field}.cgc"
+        with pytest.raises(splat.SplatError) as refused:
+            splat.save_cgc(bad, path)
+        assert refused.value.status == splat.SPLAT_ERR_INVALID
+        assert not path.exists()
+
+
+@pytest.mark.gpu
+@needs_reference
+def test_against_the_reference_writer(splat, O, tmp_path):
+    # The same centre and radius (exact order statistics), the layers within
+    # a few splats of the reference's, a file within 15 % of its size, and the
+    # Small preset smaller than the Balanced one (tests/test_cgc.cpp:338-346).
+    cloud = random_cloud(splat, 20_000, 3, 74)
+    ours, theirs = tmp_path / "ours.cgc", tmp_path / "ref.cgc"
+    balanced = splat.save_cgc(cloud, ours)
+    ref = O.ref_save_cgc(to_oracle(O, cloud), theirs)
+    a, b = ours.read_bytes(), theirs.read_bytes()
+    assert a[:36] == b[:36]  # magic, version, count, degree, layers, centre, radius
+    for l in range(3):
+        assert abs(balanced["layer_counts"][l] - ref["layer_counts"][l]) <= 20
+    print(f"  {balanced['bytes']} bytes against the reference writer's {ref['bytes']}")
+    assert abs(balanced["bytes"] - ref["bytes"]) <= 0.15 * ref["bytes"]
+    small = splat.save_cgc(cloud, ours, preset=splat.CGC_SMALL)
+    assert small["bytes"] < balanced["bytes"] and small["layer_counts"][0] < balanced["layer_counts"][0]
+
+
+@pytest.mark.gpu
+def test_a_cgc_scene_renders_like_the_original(splat, tmp_path):
+    # tests/test_cgc.cpp:405-426 (through this library's renderer: 320x180,
+    # PSNR above 35 dB).
+    import bench
+
+    arrays = bench.make_scene(50_000)
+    original = splat.GaussianCloud(3, *arrays)
+    loaded, _ = _round_trip(splat, original, tmp_path / "scene.cgc")
+    view = bench.hemisphere_views(1, width=320, height=180)[0]
+    images = []
+    for cloud in (original, loaded):
+        trainer = splat.Trainer(cloud, splat.TrainerOptions(sh_storage=splat.SH_F32))
+        images.append(trainer.render(splat.Camera(*view)).reshape(-1, 4)[:, :3].astype(np.float64))
+    mse = float(((images[0] - images[1]) ** 2).mean())
+    value = 10.0 * np.log10(1.0 / max(mse, 1e-30))
+    print(f"  PSNR {value:.1f} dB")
+    assert value > 35.0

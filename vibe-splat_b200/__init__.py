@@ -189,6 +189,25 @@ _lib.splat_measure_sm_peaks.argtypes = [ctypes.POINTER(_SmPeaks)]
 _lib.splat_cloud_load_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                       _FP, _FP, _FP, _FP, _FP]
 _lib.splat_cloud_save_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(_Cloud)]
+
+
+class _CgcOptions(ctypes.Structure):
+    _fields_ = [("preset", ctypes.c_int32), ("fast", ctypes.c_int32)]
+
+
+class _CgcStats(ctypes.Structure):
+    _fields_ = [("bytes", ctypes.c_uint64), ("layer_counts", ctypes.c_uint64 * 3)]
+
+
+_lib.splat_cloud_save_cgc.argtypes = [ctypes.c_char_p, ctypes.POINTER(_Cloud), ctypes.POINTER(_CgcOptions),
+                                      ctypes.POINTER(_CgcStats)]
+_lib.splat_cloud_load_cgc.argtypes = _lib.splat_cloud_load_ply.argtypes
+_lib.splat_cgc_morton_code.argtypes = [ctypes.c_uint32] * 3
+_lib.splat_cgc_morton_code.restype = ctypes.c_uint64
+_lib.splat_cgc_canonicalize_axes.argtypes = [_FP, _FP]
+_lib.splat_lzma_compress.argtypes = [_P, ctypes.c_size_t] + [ctypes.c_int32] * 5 + [_P, ctypes.c_size_t,
+                                                                                     ctypes.POINTER(ctypes.c_size_t)]
+_lib.splat_lzma_decompress.argtypes = [_P, ctypes.c_size_t, _P, ctypes.c_size_t]
 for _name in ("splat_trainer_remove_largest", "splat_trainer_remove_least_contributing", "splat_trainer_remove_least_opaque"):
     getattr(_lib, _name).argtypes = [_P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64)]
 _lib.splat_trainer_set_exposure.argtypes = [_P, _FP]
@@ -969,6 +988,62 @@ def save_ply(cloud: GaussianCloud, path) -> None:
     """save_ply: the standard binary little-endian 3DGS layout."""
     c, keep = cloud._c()
     _check(_lib.splat_cloud_save_ply(str(path).encode(), ctypes.byref(c)))
+
+
+CGC_BALANCED, CGC_SMALL = 0, 1
+
+
+def save_cgc(cloud: GaussianCloud, path, preset: int = CGC_BALANCED, fast: bool = False) -> dict:
+    """save_cgc (src/splat/cgc.hpp:41-43): the layered, LZMA-compressed format;
+    needs a CUDA device. Returns the file's size and the splats per layer."""
+    c, keep = cloud._c()
+    stats = _CgcStats()
+    _check(_lib.splat_cloud_save_cgc(str(path).encode(), ctypes.byref(c), ctypes.byref(_CgcOptions(preset, int(fast))),
+                                     ctypes.byref(stats)))
+    return {"bytes": int(stats.bytes), "layer_counts": [int(v) for v in stats.layer_counts]}
+
+
+def load_cgc(path) -> GaussianCloud:
+    """load_cgc (src/splat/cgc.hpp:45-49): a CGC file of version 1 or 2 (host only)."""
+    name = str(path).encode()
+    count, degree = ctypes.c_int32(), ctypes.c_int32()
+    _check(_lib.splat_cloud_load_cgc(name, ctypes.byref(count), ctypes.byref(degree), None, None, None, None, None))
+    n, d = count.value, degree.value
+    arrays = [np.empty(n * k, np.float32) for k in (3, 3, 4, 1, 3 * (d + 1) ** 2)]
+    _check(_lib.splat_cloud_load_cgc(name, ctypes.byref(count), ctypes.byref(degree), *[_fptr(a) for a in arrays]))
+    return GaussianCloud(d, *arrays)
+
+
+def cgc_morton_code(x: int, y: int, z: int) -> int:
+    """cgc_detail::morton_code: the low 21 bits of x, y, z interleaved."""
+    return int(_lib.splat_cgc_morton_code(x, y, z))
+
+
+def cgc_canonicalize_axes(log_scales, wxyz):
+    """cgc_detail::canonicalize_axes: (scales descending, quaternion with w largest and not negative)."""
+    s = np.array(log_scales, np.float32)
+    q = np.array(wxyz, np.float32)
+    _check(_lib.splat_cgc_canonicalize_axes(_fptr(s), _fptr(q)))
+    return s, q
+
+
+def lzma_compress(data: bytes, level: int = 9, extreme: bool = True, lc: int = 3, lp: int = 0, pb: int = 2) -> bytes:
+    """lzma_compress (src/splat/lzma.hpp:13): an .lzma ("alone") stream."""
+    buf = ctypes.create_string_buffer(bytes(data), max(len(data), 1))
+    size = ctypes.c_size_t()
+    _check(_lib.splat_lzma_compress(buf, len(data), level, int(extreme), lc, lp, pb, None, 0, ctypes.byref(size)))
+    out = ctypes.create_string_buffer(max(size.value, 1))
+    _check(_lib.splat_lzma_compress(buf, len(data), level, int(extreme), lc, lp, pb, out, size.value, ctypes.byref(size)))
+    return out.raw[: size.value]
+
+
+def lzma_decompress(stream: bytes, expected: int) -> bytes:
+    """lzma_decompress (src/splat/lzma.hpp:17): raises SplatError on corrupt,
+    truncated or wrongly sized data."""
+    src = ctypes.create_string_buffer(bytes(stream), max(len(stream), 1))
+    out = ctypes.create_string_buffer(max(expected, 1))
+    _check(_lib.splat_lzma_decompress(src, len(stream), out, expected))
+    return out.raw[:expected]
 
 
 def measure_sm_peaks() -> dict:
