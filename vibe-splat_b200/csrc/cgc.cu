@@ -629,11 +629,14 @@ public:
   ~Dev() {
     if (p_ != nullptr) cudaFree(p_);
   }
+  // Grows only (a sort's temporaries are reused by the next sort on the
+  // same stream without being freed under its kernels).
   void resize(size_t bytes) {
+    if (p_ != nullptr && bytes <= bytes_) return;
     if (p_ != nullptr) cudaFree(p_);
     p_ = nullptr;
     CGC_CUDA(cudaMalloc(&p_, std::max<size_t>(bytes, 16)));
-    bytes_ = bytes;
+    bytes_ = std::max<size_t>(bytes, 16);
   }
   template <class T = void> T *get() const { return static_cast<T *>(p_); }
 
