@@ -283,20 +283,19 @@ def test_selective_step_moves_exactly_the_reached_gaussians(splat, oracle, fixed
     after = t.cloud()
     n = cloud.count
     raw = t.debug_download(splat.DEBUG_RAW, np.uint32)[: n * 16].reshape(n, 16)[:, :14]
-    if fixed:
-        reached = (raw != 0).any(axis=1)
-    else:
-        reached = (raw.view(np.float32) != 0.0).any(axis=1)
-    print(f"  {int(reached.sum())} of {n} Gaussians reached")
+    nonzero = raw != 0 if fixed else raw.view(np.float32) != 0.0
+    reached = nonzero.any(axis=1)
+    # Sums 0-8 feed the parameter gradients; 9-13 are statistics only.
+    steered = nonzero[:, :9].any(axis=1)
+    print(f"  {int(reached.sum())} of {n} Gaussians reached, {int(steered.sum())} with a parameter gradient")
     assert reached.sum() > 100 and (~reached).sum() > 100
-    for name, per in (("positions", 3), ("scales", 3), ("rotations", 4), ("opacities", 1)):
+    moved = np.zeros(n, bool)
+    for name, per in (("positions", 3), ("scales", 3), ("rotations", 4), ("opacities", 1), ("sh", 3 * 16)):
         b = getattr(before, name).reshape(n, per)
         a = getattr(after, name).reshape(n, per)
         np.testing.assert_array_equal(a[~reached], b[~reached], err_msg=name)
-    moved = (after.positions.reshape(n, 3) != before.positions.reshape(n, 3)).any(axis=1)
-    assert moved[reached].mean() > 0.99
-    sh_b, sh_a = before.sh.reshape(n, -1), after.sh.reshape(n, -1)
-    np.testing.assert_array_equal(sh_a[~reached], sh_b[~reached])
+        moved |= (a != b).any(axis=1)
+    assert moved[steered].mean() > 0.99
 
 
 def test_training_lowers_the_loss(splat, oracle):

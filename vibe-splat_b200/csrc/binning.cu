@@ -156,9 +156,12 @@ __global__ void __launch_bounds__(kCountThreads)
   __shared__ uint32_t s_mask[kCountThreads / 32][32];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t r = blockIdx.x * kCountThreads + threadIdx.x;
-  // Whole warps stay to the end: the loops below are warp-wide.
-  const bool valid = r < items && itemKeys[r] != kInvisible;
-  const uint32_t s = valid ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
+  // Whole warps stay to the end: the loops below are warp-wide. Without item
+  // keys (the count beside the depth sort, which permutes them), a culled
+  // splat is the one whose reach the projection left at minus infinity.
+  const uint32_t item = r < items ? (itemSplat != nullptr ? itemSplat[r] : r) : 0u;
+  const bool valid = r < items && (itemKeys != nullptr ? itemKeys[r] != kInvisible : reach[item] != -INFINITY);
+  const uint32_t s = valid ? item : 0u;
   float4 ce = make_float4(0.f, 0.f, 0.f, 0.f), cq = ce;
   float rc = 0.0f;
   TileRect rect{0u, 0u, 0u, 0u};

@@ -52,8 +52,9 @@ struct Params {
 };
 
 // train_preprocess.comp: projects every Gaussian into every view. Writes
-// splats[v n + i], reach[v n + i], depthKeys[v n + i] (kInvisible when culled)
-// and, if values is not null, values[v n + i] = i.
+// splats[v n + i], reach[v n + i], depthKeys[v n + i] (kInvisible, and a
+// reach of minus infinity, when culled) and, if values is not null,
+// values[v n + i] = i.
 void launch_preprocess(const Params &p, const ViewSet &views, const ViewSet *dViews, Splat *splats, float *reach, uint32_t *depthKeys,
                        uint32_t *values, cudaStream_t stream, uint32_t *error = nullptr);
 
@@ -62,7 +63,8 @@ void launch_preprocess(const Params &p, const ViewSet &views, const ViewSet *dVi
 // tiles the splat reaches and writes their exclusive scan to offsets[r].
 // counters[0] += visible items, counters[1] = total entries, counters[2] =
 // min(total, capacity). itemSplat: if not null, the splat of item r is
-// itemSplat[r] (sorted values); itemKeys: kInvisible marks culled items.
+// itemSplat[r] (sorted values); itemKeys: kInvisible marks culled items
+// (without keys, a reach of minus infinity does).
 // masks[r]: the reached tiles of a rectangle of at most 32 tiles, bit
 // (y - y0) * width + (x - x0), for the emission to replay (0 for larger ones).
 void launch_bin_count_scan(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat,

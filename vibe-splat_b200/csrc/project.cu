@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(kProjectThreads, 3) k_preprocess(Params p, con
     if (tid == 0 && error != nullptr) atomicOr(error, kErrShStage);
     if (i < p.n) {
       depthKeys[(size_t)v * p.n + i] = kInvisible;
+      reachOut[(size_t)v * p.n + i] = -INFINITY;
       if (values != nullptr) values[(size_t)v * p.n + i] = i;
     }
     return;
@@ -92,7 +93,10 @@ __global__ void __launch_bounds__(kProjectThreads, 3) k_preprocess(Params p, con
   };
   if (i < p.n) [&] {
     const size_t at = (size_t)v * p.n + i;
+    // Culled until shown otherwise: the key, and the reach (which the tile
+    // count may read while the depth sort permutes the keys).
     depthKeys[at] = kInvisible;
+    reachOut[at] = -INFINITY;
     if (values != nullptr) values[at] = i;
 
     // Every parameter load first, so that they are in flight together.

@@ -789,8 +789,9 @@ void Trainer::record_prepare(bool backward) {
     SB_CUDA(cudaEventRecord(countForkEvent, stream));
     SB_CUDA(cudaStreamWaitEvent(side, countForkEvent, 0));
     SB_CUDA(cudaMemsetAsync(scanScratch.get(), 0, bin_scan_scratch_bytes(items), side));
-    launch_bin_count(splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(), nullptr, n, n, views,
-                     dViews.get<ViewSet>(), countsBySplat, masks, counters, side);
+    // No keys: the depth sort permutes them in place meanwhile.
+    launch_bin_count(splats.get<Splat>(), reach.get<float>(), nullptr, nullptr, n, n, views, dViews.get<ViewSet>(),
+                     countsBySplat, masks, counters, side);
     SB_CUDA(cudaEventRecord(countEvent, side));
   }
   SB_CUDA(cudaStreamWaitEvent(stream, joinEvent, 0));
