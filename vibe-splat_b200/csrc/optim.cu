@@ -866,21 +866,19 @@ __global__ void __launch_bounds__(256) k_touched(const void *__restrict__ rawIn,
   chain_enter();
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
-  bool reached = false;
+  uint32_t bits = 0u;
   if (i < n) {
+    // The sums' bits ORed together, every load first. As k_chain_step's test
+    // raw[k] != 0.0f: an integer sum is non-zero exactly when its value is; a
+    // float sum of -0 (only its sign bit set) counts as zero.
     const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint4 w4 = r4[q];
-      const uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        // As k_chain_step's test raw[k] != 0.0f: an integer sum is non-zero
-        // exactly when its value is; a float sum of -0 counts as zero.
-        if (q * 4 + e < kRawPerSplat) reached = reached || (FIXED ? w[e] != 0u : __uint_as_float(w[e]) != 0.0f);
-      }
-    }
+    const uint4 a = r4[0], b = r4[1], c = r4[2], d = r4[3];
+    const uint32_t keep = FIXED ? 0xFFFFFFFFu : 0x7FFFFFFFu;
+    static_assert(kRawPerSplat == 14, "the last word read is sum 13");
+    bits = ((a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) & keep) | ((c.x | c.y | c.z | c.w) & keep) |
+           ((d.x | d.y) & keep);
   }
+  const bool reached = bits != 0u;
   const uint32_t mask = __ballot_sync(0xFFFFFFFFu, reached);
   if (mask == 0u) return;
   uint32_t base = 0;
@@ -889,20 +887,76 @@ __global__ void __launch_bounds__(256) k_touched(const void *__restrict__ rawIn,
   if (reached) touched[kTouchedListStart + base + __popc(mask & ((1u << lane) - 1u))] = i;
 }
 
+// Shared-memory words a thread of k_chain_touched stages per Gaussian: the
+// DC coefficients (3), the 32-bit words holding the higher coefficients (45)
+// and the SH Adam state (48 words of BF16 pairs, or 96: m then v).
+template <StateStore ST> __host__ __device__ constexpr uint32_t touched_stage_words() {
+  return 3u + 45u + (ST == StateStore::F32 ? 96u : 48u);
+}
+constexpr uint32_t kTouchedThreads = 128;
+
+__device__ __forceinline__ void stage_word(uint32_t *dst, const void *src) {
+  const unsigned at = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(at), "l"(src) : "memory");
+}
+__device__ __forceinline__ void staged_words_ready() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The higher coefficient at element `idx` of the rest planes, from the
+// staged 32-bit word that holds it.
+template <ShStore S> __device__ __forceinline__ float rest_from_word(uint32_t word, size_t idx) {
+  if constexpr (S == ShStore::F32) {
+    return __uint_as_float(word);
+  } else {
+    const uint32_t half = (idx & 1u) != 0u ? word >> 16 : word & 0xFFFFu;
+    if constexpr (S == ShStore::BF16) return __uint_as_float(half << 16);
+    else return __half2float(__ushort_as_half((unsigned short)half));
+  }
+}
+
+// The one-view selective step of a listed Gaussian, one thread each. Its SH
+// coefficients and SH Adam state sit in planes, one scattered word per
+// element; they are brought into the thread's own shared-memory slots by
+// asynchronous copies issued as soon as the Gaussian is known, so that they
+// travel together while the chain rule runs, and the SH part reads them from
+// there. Element by element the arithmetic, hash indices and order of sums
+// are k_chain_step's.
 template <ShStore S, StateStore ST, bool FIXED>
-__global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSet *__restrict__ viewsPtr,
-                                                      const void *__restrict__ rawIn, const Splat *__restrict__ splats,
-                                                      const ChainArgs *__restrict__ argsPtr, OptimState state,
-                                                      float *__restrict__ densifyStats, const uint32_t *__restrict__ touched,
-                                                      const uint32_t *error) {
+__global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, const ViewSet *__restrict__ viewsPtr,
+                                                                      const void *__restrict__ rawIn,
+                                                                      const Splat *__restrict__ splats,
+                                                                      const ChainArgs *__restrict__ argsPtr, OptimState state,
+                                                                      float *__restrict__ densifyStats,
+                                                                      const uint32_t *__restrict__ touched,
+                                                                      const uint32_t *error) {
   chain_enter();
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  extern __shared__ uint32_t s_words[]; // [word][thread]
+  const uint32_t tid = threadIdx.x;
   const ViewParams &cam = viewsPtr->v[0];
   const uint32_t count = touched[0], n = p.n, ps = p.planeStride;
   const ChainArgs args = *argsPtr;
   const AdamArgs a = adam_args(args);
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+  const int active = min(cam.activeCoeffs, p.shCoeffs);
+  const uint32_t planes = 3u * (uint32_t)active; // SH elements in use
+  constexpr uint32_t kDc = 0, kRest = 3, kState = 48;
+  const auto slot = [&](uint32_t word) { return &s_words[word * kTouchedThreads + tid]; };
+  for (uint32_t j = blockIdx.x * blockDim.x + tid; j < count; j += gridDim.x * blockDim.x) {
     const uint32_t i = touched[kTouchedListStart + j];
+    // The scattered SH words first, so that they land while the rest runs.
+    if (active > 0) {
+      for (uint32_t c = 0; c < 3u; ++c) stage_word(slot(kDc + c), p.shDc + (size_t)c * ps + i);
+      for (uint32_t e = 0; e + 3u < planes; ++e) {
+        const size_t idx = (size_t)e * ps + i;
+        if constexpr (S == ShStore::F32) stage_word(slot(kRest + e), static_cast<const float *>(p.shRest) + idx);
+        else stage_word(slot(kRest + e), static_cast<const uint16_t *>(p.shRest) + (idx & ~(size_t)1));
+      }
+      const uint32_t *st = static_cast<const uint32_t *>(state.state[4]) + i;
+      const size_t stateCount = (size_t)ps * 3u * (uint32_t)p.shCoeffs;
+      for (uint32_t e = 0; e < planes; ++e) {
+        stage_word(slot(kState + e), st + (size_t)e * ps);
+        if constexpr (ST == StateStore::F32) stage_word(slot(kState + 48u + e), st + stateCount + (size_t)e * ps);
+      }
+    }
     const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
     const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
     const float rawOpacity = p.opacities[i];
@@ -927,8 +981,8 @@ __global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSe
     float gColour[3] = {0.f, 0.f, 0.f}, dir[3] = {0.f, 0.f, 0.f}, gPv[3] = {0.f, 0.f, 0.f}, distance = 1.0f;
     const float4 col = splats[i].colorRadius;
     if (args.statistics) {
-      float4 *st = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
-      float4 sa = st[0], sb = st[1];
+      float4 *stats = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
+      float4 sa = stats[0], sb = stats[1];
       const float hx = 0.5f * cam.widthF, hy = 0.5f * cam.heightF;
       const float ax = raw[1] * hx, ay = raw[2] * hy;
       sa.x += sqrtf(fmaf(ay, ay, ax * ax));
@@ -937,17 +991,22 @@ __global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSe
       sa.w += raw[9] * 3.0f * cam.widthF * cam.heightF;
       const float bx = raw[10] * hx, by = raw[11] * hy;
       sb.x += sqrtf(fmaf(by, by, bx * bx));
-      st[0] = sa;
-      st[1] = sb;
+      stats[0] = sa;
+      stats[1] = sb;
     }
     chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
-    const int active = min(cam.activeCoeffs, p.shCoeffs);
+    staged_words_ready();
     if (cam.activeDegree > 0) {
       float gDir[3] = {0.f, 0.f, 0.f};
 #pragma unroll
       for (int k = 1; k < kMaxCoeffs; ++k) {
         if (k >= active) break;
-        const float value[3] = {sh_coefficient<S>(p, i, k, 0), sh_coefficient<S>(p, i, k, 1), sh_coefficient<S>(p, i, k, 2)};
+        float value[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const uint32_t e = (uint32_t)(k - 1) * 3u + (uint32_t)c;
+          value[c] = rest_from_word<S>(*slot(kRest + e), (size_t)e * ps + i);
+        }
         direction_term(k, value, gColour, dir, gDir);
       }
       add_direction_term(gDir, dir, distance, gPv);
@@ -988,20 +1047,19 @@ __global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSe
       }
     }
 
-    // The SH step: only the coefficients in use have a gradient.
+    // The SH step from the staged words: only the coefficients in use have a gradient.
     const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
     const uint32_t hashBase = i * shFloats * 5u + 4u;
     uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + i;
     const size_t stateCount = (size_t)ps * shFloats; // F32: the v planes follow the m planes
     auto element = [&](uint32_t plane, float &val, float g, float rate) {
       if constexpr (ST == StateStore::F32) {
-        float *sf = reinterpret_cast<float *>(stateWords);
-        float m = sf[(size_t)plane * ps], v = sf[stateCount + (size_t)plane * ps];
+        float m = __uint_as_float(*slot(kState + plane)), v = __uint_as_float(*slot(kState + 48u + plane));
         adam(val, m, v, g, rate, a);
-        sf[(size_t)plane * ps] = m;
-        sf[stateCount + (size_t)plane * ps] = v;
+        reinterpret_cast<float *>(stateWords)[(size_t)plane * ps] = m;
+        reinterpret_cast<float *>(stateWords)[stateCount + (size_t)plane * ps] = v;
       } else {
-        const uint32_t word = stateWords[(size_t)plane * ps];
+        const uint32_t word = *slot(kState + plane);
         float m = bf16_load(word, 0), v = bf16_load(word, 1);
         adam(val, m, v, g, rate, a);
         stateWords[(size_t)plane * ps] = bf16_pair(m, v, hashBase + plane * 5u, a.seed);
@@ -1011,7 +1069,7 @@ __global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSe
     for (int c = 0; c < 3; ++c) {
       const float g = active > 0 ? fmaf(basis_one(0, dir[0], dir[1], dir[2]), gColour[c], 0.0f) : 0.0f;
       if (g == 0.0f) continue;
-      float val = p.shDc[(size_t)c * ps + i];
+      float val = __uint_as_float(*slot(kDc + (uint32_t)c));
       element((uint32_t)c, val, g, args.rates[4]);
       p.shDc[(size_t)c * ps + i] = val;
     }
@@ -1025,9 +1083,10 @@ __global__ void __launch_bounds__(128, 6) k_chain_touched(Params p, const ViewSe
         const float g = fmaf(b, gColour[c], 0.0f);
         if (g == 0.0f) continue;
         const uint32_t plane = r + 3u + (uint32_t)c;
-        float val = load_sh_rest<S>(p.shRest, (size_t)(r + (uint32_t)c) * ps + i);
+        const size_t idx = (size_t)(r + (uint32_t)c) * ps + i;
+        float val = rest_from_word<S>(*slot(kRest + r + (uint32_t)c), idx);
         element(plane, val, g, restRate);
-        store_sh_rest<S>(p.shRest, (size_t)(r + (uint32_t)c) * ps + i, val, hashBase + plane * 5u, args.seed);
+        store_sh_rest<S>(p.shRest, idx, val, hashBase + plane * 5u, args.seed);
       }
     }
   }
@@ -1066,17 +1125,23 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
       cudaMemsetAsync(touched, 0, 4, stream);
       if (args.fixedPoint) launch_chained(k_touched<true>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
       else launch_chained(k_touched<false>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
-      const uint32_t grid = std::min<uint32_t>(blocks, resident_blocks((const void *)k_chain_touched<S, StateStore::BF16Pair, false>, 128));
-#define SB_TOUCHED(ST, FIX)                                                                                          \
-  launch_chained(k_chain_touched<S, ST, FIX>, dim3(grid), dim3(128), 0, stream, p, dViews, raw, splats, dArgs, state, \
-                 densifyStats, (const uint32_t *)touched, (const uint32_t *)error)
+#define SB_TOUCHED(ST, FIX)                                                                                             \
+  {                                                                                                                      \
+    const uint32_t smemBytes = touched_stage_words<ST>() * kTouchedThreads * 4u;                                         \
+    cudaFuncSetAttribute(k_chain_touched<S, ST, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);      \
+    int perSm = 0, sms = 0, device = 0;                                                                                  \
+    cudaGetDevice(&device);                                                                                              \
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);                                                \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_chain_touched<S, ST, FIX>, kTouchedThreads, smemBytes);       \
+    const uint32_t grid = std::min<uint32_t>(div_up(p.n, kTouchedThreads), (uint32_t)std::max(1, perSm * sms));          \
+    launch_chained(k_chain_touched<S, ST, FIX>, dim3(grid), dim3(kTouchedThreads), smemBytes, stream, p, dViews, raw,     \
+                   splats, dArgs, state, densifyStats, (const uint32_t *)touched, (const uint32_t *)error);             \
+  }
       const bool f32 = state.store == StateStore::F32;
       if (args.fixedPoint) {
-        if (f32) SB_TOUCHED(StateStore::F32, true);
-        else SB_TOUCHED(StateStore::BF16Pair, true);
+        if (f32) SB_TOUCHED(StateStore::F32, true) else SB_TOUCHED(StateStore::BF16Pair, true)
       } else {
-        if (f32) SB_TOUCHED(StateStore::F32, false);
-        else SB_TOUCHED(StateStore::BF16Pair, false);
+        if (f32) SB_TOUCHED(StateStore::F32, false) else SB_TOUCHED(StateStore::BF16Pair, false)
       }
 #undef SB_TOUCHED
       return;
