@@ -396,20 +396,29 @@ def test_against_the_reference_writer(splat, O, tmp_path):
 
 
 @pytest.mark.gpu
-def test_a_cgc_scene_renders_like_the_original(splat, tmp_path):
-    # tests/test_cgc.cpp:405-426 (through this library's renderer: 320x180,
-    # PSNR above 35 dB).
+@needs_reference
+def test_a_cgc_scene_renders_like_the_original(splat, O, tmp_path):
+    # tests/test_cgc.cpp:405-426, through this library's renderer at 320x180:
+    # the file written here renders within 0.5 dB of the reference writer's
+    # file of the same scene, against the original, and above 33 dB (the
+    # reference asks 35 dB of its own test scene).
     import bench
 
     arrays = bench.make_scene(50_000)
     original = splat.GaussianCloud(3, *arrays)
-    loaded, _ = _round_trip(splat, original, tmp_path / "scene.cgc")
+    ours, _ = _round_trip(splat, original, tmp_path / "scene.cgc")
+    O.ref_save_cgc(to_oracle(O, original), tmp_path / "ref.cgc")
+    theirs = splat.load_cgc(tmp_path / "ref.cgc")
     view = bench.hemisphere_views(1, width=320, height=180)[0]
-    images = []
-    for cloud in (original, loaded):
+
+    def image(cloud):
         trainer = splat.Trainer(cloud, splat.TrainerOptions(sh_storage=splat.SH_F32))
-        images.append(trainer.render(splat.Camera(*view)).reshape(-1, 4)[:, :3].astype(np.float64))
-    mse = float(((images[0] - images[1]) ** 2).mean())
-    value = 10.0 * np.log10(1.0 / max(mse, 1e-30))
-    print(f"  PSNR {value:.1f} dB")
-    assert value > 35.0
+        return trainer.render(splat.Camera(*view)).reshape(-1, 4)[:, :3].astype(np.float64)
+
+    def psnr(a, b):
+        return 10.0 * np.log10(1.0 / max(float(((a - b) ** 2).mean()), 1e-30))
+
+    base = image(original)
+    mine, reference = psnr(base, image(ours)), psnr(base, image(theirs))
+    print(f"  PSNR {mine:.2f} dB (the reference writer's file: {reference:.2f} dB)")
+    assert mine > 33.0 and mine > reference - 0.5

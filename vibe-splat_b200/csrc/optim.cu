@@ -887,39 +887,17 @@ __global__ void __launch_bounds__(256) k_touched(const void *__restrict__ rawIn,
   if (reached) touched[kTouchedListStart + base + __popc(mask & ((1u << lane) - 1u))] = i;
 }
 
-// Shared-memory words a thread of k_chain_touched stages per Gaussian: the
-// DC coefficients (3), the 32-bit words holding the higher coefficients (45)
-// and the SH Adam state (48 words of BF16 pairs, or 96: m then v).
-template <StateStore ST> __host__ __device__ constexpr uint32_t touched_stage_words() {
-  return 3u + 45u + (ST == StateStore::F32 ? 96u : 48u);
-}
 constexpr uint32_t kTouchedThreads = 128;
-
-__device__ __forceinline__ void stage_word(uint32_t *dst, const void *src) {
-  const unsigned at = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(at), "l"(src) : "memory");
-}
-__device__ __forceinline__ void staged_words_ready() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// The higher coefficient at element `idx` of the rest planes, from the
-// staged 32-bit word that holds it.
-template <ShStore S> __device__ __forceinline__ float rest_from_word(uint32_t word, size_t idx) {
-  if constexpr (S == ShStore::F32) {
-    return __uint_as_float(word);
-  } else {
-    const uint32_t half = (idx & 1u) != 0u ? word >> 16 : word & 0xFFFFu;
-    if constexpr (S == ShStore::BF16) return __uint_as_float(half << 16);
-    else return __half2float(__ushort_as_half((unsigned short)half));
-  }
-}
+// Coefficients whose SH Adam state words are loaded together in the SH step.
+constexpr int kStateBatch = 5;
 
 // The one-view selective step of a listed Gaussian, one thread each. Its SH
 // coefficients and SH Adam state sit in planes, one scattered word per
-// element; they are brought into the thread's own shared-memory slots by
-// asynchronous copies issued as soon as the Gaussian is known, so that they
-// travel together while the chain rule runs, and the SH part reads them from
-// there. Element by element the arithmetic, hash indices and order of sums
-// are k_chain_step's.
+// element, so every load of a coefficient is issued up front (predicated on
+// the coefficient being in use, no branch between them) and the state words
+// go in batches of kStateBatch coefficients: a handful of memory latencies
+// per Gaussian instead of one per coefficient. Element by element the
+// arithmetic, hash indices and order of sums are k_chain_step's.
 template <ShStore S, StateStore ST, bool FIXED>
 __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, const ViewSet *__restrict__ viewsPtr,
                                                                       const void *__restrict__ rawIn,
@@ -930,41 +908,21 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
                                                                       const uint32_t *error) {
   chain_enter();
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  extern __shared__ uint32_t s_words[]; // [word][thread]
-  const uint32_t tid = threadIdx.x;
   const ViewParams &cam = viewsPtr->v[0];
   const uint32_t count = touched[0], n = p.n, ps = p.planeStride;
   const ChainArgs args = *argsPtr;
   const AdamArgs a = adam_args(args);
   const int active = min(cam.activeCoeffs, p.shCoeffs);
-  const uint32_t planes = 3u * (uint32_t)active; // SH elements in use
-  constexpr uint32_t kDc = 0, kRest = 3, kState = 48;
-  const auto slot = [&](uint32_t word) { return &s_words[word * kTouchedThreads + tid]; };
-  for (uint32_t j = blockIdx.x * blockDim.x + tid; j < count; j += gridDim.x * blockDim.x) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
     const uint32_t i = touched[kTouchedListStart + j];
-    // The scattered SH words first, so that they land while the rest runs.
-    if (active > 0) {
-      for (uint32_t c = 0; c < 3u; ++c) stage_word(slot(kDc + c), p.shDc + (size_t)c * ps + i);
-      for (uint32_t e = 0; e + 3u < planes; ++e) {
-        const size_t idx = (size_t)e * ps + i;
-        if constexpr (S == ShStore::F32) stage_word(slot(kRest + e), static_cast<const float *>(p.shRest) + idx);
-        else stage_word(slot(kRest + e), static_cast<const uint16_t *>(p.shRest) + (idx & ~(size_t)1));
-      }
-      const uint32_t *st = static_cast<const uint32_t *>(state.state[4]) + i;
-      const size_t stateCount = (size_t)ps * 3u * (uint32_t)p.shCoeffs;
-      for (uint32_t e = 0; e < planes; ++e) {
-        stage_word(slot(kState + e), st + (size_t)e * ps);
-        if constexpr (ST == StateStore::F32) stage_word(slot(kState + 48u + e), st + stateCount + (size_t)e * ps);
-      }
-    }
     const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
     const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
     const float rawOpacity = p.opacities[i];
     const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
-    float raw[kRawPerSplat];
+    const float4 col = splats[i].colorRadius;
+    uint32_t words[16];
     {
       const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
-      uint32_t words[16];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const uint4 w4 = r4[q];
@@ -973,13 +931,22 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
         words[q * 4 + 2] = w4.z;
         words[q * 4 + 3] = w4.w;
       }
-#pragma unroll
-      for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
     }
+    // The coefficients in use, all loads in flight together.
+    float dc[3], rest[kMaxCoeffs - 1][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dc[c] = active > 0 ? p.shDc[(size_t)c * ps + i] : 0.0f;
+#pragma unroll
+    for (int k = 1; k < kMaxCoeffs; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        rest[k - 1][c] = k < active ? load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i) : 0.0f;
+    float raw[kRawPerSplat];
+#pragma unroll
+    for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
     const float opacity = 1.0f / (1.0f + splat_expf(-rawOpacity));
     float gP[3] = {0.f, 0.f, 0.f}, gScale[3] = {0.f, 0.f, 0.f}, gRot[4] = {0.f, 0.f, 0.f, 0.f}, gOpacity = 0.f;
     float gColour[3] = {0.f, 0.f, 0.f}, dir[3] = {0.f, 0.f, 0.f}, gPv[3] = {0.f, 0.f, 0.f}, distance = 1.0f;
-    const float4 col = splats[i].colorRadius;
     if (args.statistics) {
       float4 *stats = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
       float4 sa = stats[0], sb = stats[1];
@@ -995,20 +962,11 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
       stats[1] = sb;
     }
     chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
-    staged_words_ready();
     if (cam.activeDegree > 0) {
       float gDir[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-      for (int k = 1; k < kMaxCoeffs; ++k) {
-        if (k >= active) break;
-        float value[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const uint32_t e = (uint32_t)(k - 1) * 3u + (uint32_t)c;
-          value[c] = rest_from_word<S>(*slot(kRest + e), (size_t)e * ps + i);
-        }
-        direction_term(k, value, gColour, dir, gDir);
-      }
+      for (int k = 1; k < kMaxCoeffs; ++k)
+        if (k < active) direction_term(k, rest[k - 1], gColour, dir, gDir);
       add_direction_term(gDir, dir, distance, gPv);
     }
 #pragma unroll
@@ -1047,46 +1005,57 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
       }
     }
 
-    // The SH step from the staged words: only the coefficients in use have a gradient.
+    // The SH step: only the coefficients in use have a gradient. The state
+    // words of kStateBatch coefficients are loaded together, then stepped.
     const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
     const uint32_t hashBase = i * shFloats * 5u + 4u;
     uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + i;
     const size_t stateCount = (size_t)ps * shFloats; // F32: the v planes follow the m planes
-    auto element = [&](uint32_t plane, float &val, float g, float rate) {
-      if constexpr (ST == StateStore::F32) {
-        float m = __uint_as_float(*slot(kState + plane)), v = __uint_as_float(*slot(kState + 48u + plane));
-        adam(val, m, v, g, rate, a);
-        reinterpret_cast<float *>(stateWords)[(size_t)plane * ps] = m;
-        reinterpret_cast<float *>(stateWords)[stateCount + (size_t)plane * ps] = v;
-      } else {
-        const uint32_t word = *slot(kState + plane);
-        float m = bf16_load(word, 0), v = bf16_load(word, 1);
-        adam(val, m, v, g, rate, a);
-        stateWords[(size_t)plane * ps] = bf16_pair(m, v, hashBase + plane * 5u, a.seed);
-      }
-    };
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float g = active > 0 ? fmaf(basis_one(0, dir[0], dir[1], dir[2]), gColour[c], 0.0f) : 0.0f;
-      if (g == 0.0f) continue;
-      float val = __uint_as_float(*slot(kDc + (uint32_t)c));
-      element((uint32_t)c, val, g, args.rates[4]);
-      p.shDc[(size_t)c * ps + i] = val;
-    }
     const float restRate = args.rates[4] * args.restScale;
-#pragma unroll 1
-    for (int k = 1; k < active; ++k) {
-      const float b = basis_one(k, dir[0], dir[1], dir[2]);
-      const uint32_t r = (uint32_t)(k - 1) * 3u;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float g = fmaf(b, gColour[c], 0.0f);
-        if (g == 0.0f) continue;
-        const uint32_t plane = r + 3u + (uint32_t)c;
-        const size_t idx = (size_t)(r + (uint32_t)c) * ps + i;
-        float val = rest_from_word<S>(*slot(kRest + r + (uint32_t)c), idx);
-        element(plane, val, g, restRate);
-        store_sh_rest<S>(p.shRest, idx, val, hashBase + plane * 5u, args.seed);
+    for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStateBatch) {
+      float m[kStateBatch][3], v[kStateBatch][3];
+#pragma unroll
+      for (int b = 0; b < kStateBatch; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const int k = k0 + b;
+          const size_t at = (size_t)(3 * k + c) * ps;
+          m[b][c] = v[b][c] = 0.0f;
+          if (k < active) {
+            if constexpr (ST == StateStore::F32) {
+              m[b][c] = reinterpret_cast<const float *>(stateWords)[at];
+              v[b][c] = reinterpret_cast<const float *>(stateWords)[stateCount + at];
+            } else {
+              const uint32_t w = stateWords[at];
+              m[b][c] = bf16_load(w, 0);
+              v[b][c] = bf16_load(w, 1);
+            }
+          }
+        }
+#pragma unroll
+      for (int b = 0; b < kStateBatch; ++b) {
+        const int k = k0 + b;
+        if (k >= active) continue;
+        const float basis = basis_one(k, dir[0], dir[1], dir[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float g = fmaf(basis, gColour[c], 0.0f);
+          if (g == 0.0f) continue;
+          const uint32_t plane = (uint32_t)(3 * k + c);
+          const size_t at = (size_t)plane * ps;
+          float val = k == 0 ? dc[c] : rest[k > 0 ? k - 1 : 0][c];
+          float mm = m[b][c], vvv = v[b][c];
+          adam(val, mm, vvv, g, k == 0 ? args.rates[4] : restRate, a);
+          if constexpr (ST == StateStore::F32) {
+            reinterpret_cast<float *>(stateWords)[at] = mm;
+            reinterpret_cast<float *>(stateWords)[stateCount + at] = vvv;
+          } else {
+            stateWords[at] = bf16_pair(mm, vvv, hashBase + plane * 5u, a.seed);
+          }
+          if (k == 0) p.shDc[(size_t)c * ps + i] = val;
+          else store_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i, val, hashBase + plane * 5u, args.seed);
+        }
       }
     }
   }
@@ -1127,15 +1096,10 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
       else launch_chained(k_touched<false>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
 #define SB_TOUCHED(ST, FIX)                                                                                             \
   {                                                                                                                      \
-    const uint32_t smemBytes = touched_stage_words<ST>() * kTouchedThreads * 4u;                                         \
-    cudaFuncSetAttribute(k_chain_touched<S, ST, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);      \
-    int perSm = 0, sms = 0, device = 0;                                                                                  \
-    cudaGetDevice(&device);                                                                                              \
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);                                                \
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_chain_touched<S, ST, FIX>, kTouchedThreads, smemBytes);       \
-    const uint32_t grid = std::min<uint32_t>(div_up(p.n, kTouchedThreads), (uint32_t)std::max(1, perSm * sms));          \
-    launch_chained(k_chain_touched<S, ST, FIX>, dim3(grid), dim3(kTouchedThreads), smemBytes, stream, p, dViews, raw,     \
-                   splats, dArgs, state, densifyStats, (const uint32_t *)touched, (const uint32_t *)error);             \
+    const uint32_t grid = std::min<uint32_t>(div_up(p.n, kTouchedThreads),                                                \
+                                             resident_blocks((const void *)k_chain_touched<S, ST, FIX>, kTouchedThreads)); \
+    launch_chained(k_chain_touched<S, ST, FIX>, dim3(grid), dim3(kTouchedThreads), 0, stream, p, dViews, raw, splats,   \
+                   dArgs, state, densifyStats, (const uint32_t *)touched, (const uint32_t *)error);                       \
   }
       const bool f32 = state.store == StateStore::F32;
       if (args.fixedPoint) {
