@@ -797,9 +797,9 @@ def test_pruning_keeps_the_references_survivors_and_their_state(splat, oracle, k
     for g, width in enumerate((3, 3, 4, 1)):
         new = trainer.debug_download(splat.DEBUG_STATE + g, np.uint32).reshape(len(source), width)
         np.testing.assert_array_equal(new, states[g].reshape(300, width)[source], f"state group {g}")
-    old_stride, new_stride = 384, 256  # Gaussian counts rounded up to 128
-    new_sh = trainer.debug_download(splat.DEBUG_STATE + 4, np.uint32).reshape(-1, new_stride)[:, : len(source)]
-    old_sh = states[4].reshape(-1, old_stride)[:, source]
+    # SH state: a row of 27 words per Gaussian (degree 2), row counts rounded up to 128.
+    new_sh = trainer.debug_download(splat.DEBUG_STATE + 4, np.uint32).reshape(256, 27)[: len(source)]
+    old_sh = states[4].reshape(384, 27)[source]
     np.testing.assert_array_equal(new_sh, old_sh, "SH state")
     assert np.all(trainer.densify_stats().contribution == 0.0)
     assert math.isfinite(trainer.step(to_camera(view), target, splat.LearningRates()).loss)

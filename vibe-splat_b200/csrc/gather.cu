@@ -2,9 +2,13 @@
 // Trainer::apply_changes, src/train/trainer.cpp:749-787): element k of new
 // Gaussian g takes old element k of Gaussian source[g], or zero when source[g]
 // is negative (a new Gaussian starts with fresh moments). Two layouts: rows of
-// `stride` words per Gaussian (positions, scales, rotations, opacities) and
-// planes of one word per Gaussian (the SH state, planeStride apart). F32
-// state keeps its v words as a second copy of the layout after the m words.
+// `stride` words per Gaussian (positions, scales, rotations, opacities, and
+// the SH state, whose row count is rounded up to a multiple of 128: rows from
+// `valid` on are padding, zeroed) and planes of one word per Gaussian (the SH
+// coefficients, planeStride apart). F32 state keeps its v words as a second
+// copy of the layout after the m words.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace sb {
@@ -16,11 +20,11 @@ namespace {
 template <uint32_t STRIDE>
 __global__ void __launch_bounds__(256) k_gather_rows(const int32_t *__restrict__ source, const uint32_t *__restrict__ in,
                                                      uint32_t *__restrict__ out, uint32_t newCount, uint32_t oldCount,
-                                                     uint32_t runtimeStride) {
+                                                     uint32_t runtimeStride, uint32_t valid) {
   const uint32_t stride = STRIDE != 0 ? STRIDE : runtimeStride;
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x, copy = blockIdx.y;
   if (g >= newCount) return;
-  const int32_t from = source[g];
+  const int32_t from = g < valid ? source[g] : -1;
   uint32_t *dst = out + ((size_t)copy * newCount + g) * stride;
   if (from < 0) {
     for (uint32_t k = 0; k < stride; ++k) dst[k] = 0u;
@@ -104,19 +108,20 @@ __global__ void __launch_bounds__(256) k_survivor_sources(const uint32_t *__rest
 } // namespace
 
 void launch_gather_rows(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t oldCount,
-                        uint32_t stride, uint32_t copies, cudaStream_t stream) {
+                        uint32_t stride, uint32_t copies, cudaStream_t stream, uint32_t valid) {
   if (newCount == 0 || stride == 0 || copies == 0) return;
+  valid = std::min(valid, newCount);
   const dim3 grid(div_up(newCount, 256), copies);
   // Rows of 4 words move as one 16-byte access when both arrays keep 16-byte rows.
   const bool aligned = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0u;
   switch (stride) {
-  case 1: k_gather_rows<1><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 1); break;
-  case 3: k_gather_rows<3><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 3); break;
+  case 1: k_gather_rows<1><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 1, valid); break;
+  case 3: k_gather_rows<3><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 3, valid); break;
   case 4:
-    if (aligned) k_gather_rows<4><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 4);
-    else k_gather_rows<0><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 4);
+    if (aligned) k_gather_rows<4><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 4, valid);
+    else k_gather_rows<0><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, 4, valid);
     break;
-  default: k_gather_rows<0><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, stride); break;
+  default: k_gather_rows<0><<<grid, 256, 0, stream>>>(source, in, out, newCount, oldCount, stride, valid); break;
   }
 }
 

@@ -219,7 +219,8 @@ uint32_t resident_blocks(const void *kernel, int threads);
 // per Gaussian, `copies` consecutive copies of the layout (2 for F32 m and v).
 // Planes: `planes` planes of one word per Gaussian, newStride / oldStride apart.
 void launch_gather_rows(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t oldCount,
-                        uint32_t stride, uint32_t copies, cudaStream_t stream);
+                        uint32_t stride, uint32_t copies, cudaStream_t stream,
+                        uint32_t valid = 0xFFFFFFFFu);
 void launch_gather_planes(const int32_t *source, const uint32_t *in, uint32_t *out, uint32_t newCount, uint32_t newStride,
                           uint32_t oldStride, uint32_t planes, cudaStream_t stream);
 void launch_gather_planes16(const int32_t *source, const uint16_t *in, uint16_t *out, uint32_t newCount, uint32_t newStride,

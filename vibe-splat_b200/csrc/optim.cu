@@ -74,6 +74,14 @@ __device__ __forceinline__ float sqrt_sfu(float x) {
   return r;
 }
 
+// The SH Adam state lies in rows: element e (= 3 k + c) of Gaussian i at word
+// i S + e, S = 3 (degree + 1)^2 words per Gaussian, the row count rounded up
+// to a multiple of 128 (kPlaneAlign); F32 state keeps its v rows after the m
+// rows, planeStride S words later. A Gaussian's state is one contiguous
+// run, which a step touching a few Gaussians here and there reads and writes
+// in whole sectors.
+__host__ __device__ __forceinline__ size_t sh_state_at(uint32_t i, uint32_t e, uint32_t S) { return (size_t)i * S + e; }
+
 // Adam on one parameter (step_parameter with radius < 0): the bias
 // corrections as multiplications by their reciprocals, the square root and
 // the step's division on the SFU (the reference's GLSL sqrt and division are
@@ -543,13 +551,13 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       value[kk][c] = m[kk][c] = vv[kk][c] = 0.0f;
       word[kk][c] = 0u;
       if (k >= p.shCoeffs) continue;
-      const size_t t = (size_t)(k * 3 + c) * ps + i;
+      const size_t t = (size_t)(k * 3 + c) * ps + i, ts = sh_state_at(i, (uint32_t)(k * 3 + c), shFloats);
       value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3 * ps);
       if (state.store == StateStore::F32) {
-        m[kk][c] = static_cast<const float *>(state.state[4])[t];
-        vv[kk][c] = static_cast<const float *>(state.state[4])[count + t];
+        m[kk][c] = static_cast<const float *>(state.state[4])[ts];
+        vv[kk][c] = static_cast<const float *>(state.state[4])[count + ts];
       } else {
-        word[kk][c] = static_cast<const uint32_t *>(state.state[4])[t];
+        word[kk][c] = static_cast<const uint32_t *>(state.state[4])[ts];
         m[kk][c] = bf16_load(word[kk][c], 0);
         vv[kk][c] = bf16_load(word[kk][c], 1);
       }
@@ -564,14 +572,14 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
     for (int c = 0; c < 3; ++c) {
       if (g[kk][c] == 0.0f && !stepZeros) continue;
       const uint32_t plane = (uint32_t)(k * 3 + c);
-      const size_t t = (size_t)plane * ps + i;
+      const size_t t = (size_t)plane * ps + i, ts = sh_state_at(i, plane, shFloats);
       const uint32_t hashIndex = (i * (uint32_t)shFloats + plane) * 5u + 4u;
       adam(value[kk][c], m[kk][c], vv[kk][c], g[kk][c], rate, a);
       if (state.store == StateStore::F32) {
-        static_cast<float *>(state.state[4])[t] = m[kk][c];
-        static_cast<float *>(state.state[4])[count + t] = vv[kk][c];
+        static_cast<float *>(state.state[4])[ts] = m[kk][c];
+        static_cast<float *>(state.state[4])[count + ts] = vv[kk][c];
       } else {
-        static_cast<uint32_t *>(state.state[4])[t] = bf16_pair(m[kk][c], vv[kk][c], hashIndex, a.seed);
+        static_cast<uint32_t *>(state.state[4])[ts] = bf16_pair(m[kk][c], vv[kk][c], hashIndex, a.seed);
       }
       if (k == 0) {
         p.shDc[t] = value[kk][c];
@@ -661,7 +669,7 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
     // Warp 0 issues the copies: DC planes, rest planes, state planes (F32: m then v).
     if (tid == 0) bulk_expect(&s_bar, step_stage_bytes(p.shCoeffs, (int)kShBytes, stateF32));
     __syncwarp();
-    const uint32_t copies = planes + (stateF32 ? 2u : 1u) * planes;
+    const uint32_t copies = planes + (stateF32 ? 2u : 1u);
     for (uint32_t c = tid; c < copies; c += 32u) {
       if (c < 3u) {
         bulk_load(s_dc + c * kStepThreads, p.shDc + (size_t)c * ps + i0, kStepThreads * 4u, &s_bar);
@@ -671,9 +679,11 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
                   static_cast<const unsigned char *>(p.shRest) + ((size_t)r * ps + i0) * kShBytes, kStepThreads * kShBytes,
                   &s_bar);
       } else {
-        const uint32_t q = c - planes; // F32: planes m, then planes v (at planes * ps)
-        bulk_load(s_state + q * kStepThreads * 4u,
-                  static_cast<const unsigned char *>(state.state[4]) + ((size_t)q * ps + i0) * 4u, kStepThreads * 4u, &s_bar);
+        // The block's state rows, one copy (F32: the m rows, then the v rows).
+        const uint32_t q = c - planes;
+        bulk_load(s_state + q * kStepThreads * planes * 4u,
+                  static_cast<const unsigned char *>(state.state[4]) + ((size_t)q * ps + i0) * planes * 4u,
+                  kStepThreads * planes * 4u, &s_bar);
       }
     }
   }
@@ -803,22 +813,24 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   if (!(touched || stepZeros)) return;
   const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
   const uint32_t hashBase = i * shFloats * 5u + 4u;
-  const float *s_statef = reinterpret_cast<const float *>(s_state);
+  // The staged rows: this thread's row at tid * planes (F32: the v rows after
+  // the block's m rows).
+  const float *s_statef = reinterpret_cast<const float *>(s_state) + (size_t)tid * planes;
   const uint32_t *s_statew = reinterpret_cast<const uint32_t *>(s_statef);
-  uint32_t *stateOut = static_cast<uint32_t *>(state.state[4]) + i;
-  const size_t stateCount = (size_t)ps * shFloats; // F32: the v planes follow the m planes
+  uint32_t *stateOut = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, shFloats);
+  const size_t stateCount = (size_t)ps * shFloats; // F32: the v rows follow the m rows
   // One element: Adam from the staged state, the new state and value returned.
   auto element = [&](uint32_t plane, float &val, float g, float rate) {
     if constexpr (ST == StateStore::F32) {
-      float m = s_statef[plane * kStepThreads + tid], v = s_statef[(planes + plane) * kStepThreads + tid];
+      float m = s_statef[plane], v = s_statef[(size_t)kStepThreads * planes + plane];
       adam(val, m, v, g, rate, a);
-      reinterpret_cast<float *>(stateOut)[(size_t)plane * ps] = m;
-      reinterpret_cast<float *>(stateOut)[stateCount + (size_t)plane * ps] = v;
+      reinterpret_cast<float *>(stateOut)[plane] = m;
+      reinterpret_cast<float *>(stateOut)[stateCount + plane] = v;
     } else {
-      const uint32_t word = s_statew[plane * kStepThreads + tid];
+      const uint32_t word = s_statew[plane];
       float m = bf16_load(word, 0), v = bf16_load(word, 1);
       adam(val, m, v, g, rate, a);
-      stateOut[(size_t)plane * ps] = bf16_pair(m, v, hashBase + plane * 5u, a.seed);
+      stateOut[plane] = bf16_pair(m, v, hashBase + plane * 5u, a.seed);
     }
   };
 #pragma unroll
@@ -1009,8 +1021,8 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
     // words of kStateBatch coefficients are loaded together, then stepped.
     const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
     const uint32_t hashBase = i * shFloats * 5u + 4u;
-    uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + i;
-    const size_t stateCount = (size_t)ps * shFloats; // F32: the v planes follow the m planes
+    uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, shFloats);
+    const size_t stateCount = (size_t)ps * shFloats; // F32: the v rows follow the m rows
     const float restRate = args.rates[4] * args.restScale;
 #pragma unroll
     for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStateBatch) {
@@ -1020,7 +1032,7 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const int k = k0 + b;
-          const size_t at = (size_t)(3 * k + c) * ps;
+          const size_t at = (size_t)(3 * k + c);
           m[b][c] = v[b][c] = 0.0f;
           if (k < active) {
             if constexpr (ST == StateStore::F32) {
@@ -1043,7 +1055,7 @@ __global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, 
           const float g = fmaf(basis, gColour[c], 0.0f);
           if (g == 0.0f) continue;
           const uint32_t plane = (uint32_t)(3 * k + c);
-          const size_t at = (size_t)plane * ps;
+          const size_t at = plane;
           float val = k == 0 ? dc[c] : rest[k > 0 ? k - 1 : 0][c];
           float mm = m[b][c], vvv = v[b][c];
           adam(val, mm, vvv, g, k == 0 ? args.rates[4] : restRate, a);
@@ -1087,7 +1099,7 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
   const bool store = args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
   const bool multi = views.count > 1;
-  // The fused form indexes the F32 SH state (two planes of n * 48 floats) in 32 bits.
+  // The fused form indexes the F32 SH state (m and v rows of 48 floats a Gaussian) in 32 bits.
   if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.planeStride * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
     if (touched != nullptr && args.selective && args.opacityReg == 0.0f && args.scaleReg == 0.0f) {
       // Only the reached Gaussians change: list them, then step the list.

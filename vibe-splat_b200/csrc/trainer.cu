@@ -1146,8 +1146,10 @@ void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *state
   for (int g = 0; g < 4; ++g)
     launch_gather_rows(stateSource, state[g].get<uint32_t>(), spareState[g].get<uint32_t>(), newN, oldN, strides[g],
                        (uint32_t)copies, stream);
-  launch_gather_planes(stateSource, state[4].get<uint32_t>(), spareState[4].get<uint32_t>(), newN, newStride, oldStride,
-                       (uint32_t)(3 * shCoeffs * copies), stream);
+  // The SH state rows: the row counts are the plane strides, the rows from
+  // newN on padding.
+  launch_gather_rows(stateSource, state[4].get<uint32_t>(), spareState[4].get<uint32_t>(), newStride, oldStride,
+                     (uint32_t)(3 * shCoeffs), (uint32_t)copies, stream, newN);
   SB_CUDA(cudaGetLastError());
   SB_CUDA(cudaStreamSynchronize(stream));
   for (int g = 0; g < 4; ++g) swap(*params[g], spareParams[g]);
