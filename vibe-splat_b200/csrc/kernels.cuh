@@ -205,12 +205,9 @@ struct GradientsOut {
 // Gaussians, int32 fixed point with fixedScale or float, times toPixels).
 void launch_score(const void *raw, bool fixedPoint, float fixedScale, uint32_t n, float toPixels, float loss, float *densifyStats,
                   cudaStream_t stream);
-// touched: a word for the count and, from word 32 on, a list of up to n
-// Gaussian indices (the one-view selective step lists the Gaussians the view
-// reached and steps those alone), or null.
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad,
-                  float *densifyStats, uint32_t *touched, uint32_t *error, cudaStream_t stream);
+                  float *densifyStats, uint32_t *error, cudaStream_t stream);
 // Blocks of `threads` threads of `kernel` resident on the whole GPU at once.
 uint32_t resident_blocks(const void *kernel, int threads);
 

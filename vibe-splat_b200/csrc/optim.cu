@@ -861,216 +861,227 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
 // Selective Adam with no penalty leaves a Gaussian the view did not reach
 // (every backward sum zero) exactly as it was, and behind the front layers of
 // a scene most Gaussians are not reached: one thread per Gaussian would run
-// the chain rule and the step with a few lanes of each warp. So k_touched
-// lists the reached Gaussians and k_chain_touched runs the one-view step over
-// the list, one thread per listed Gaussian, full warps. The list's order
-// (warp-aggregated appends) varies from run to run and does not matter: a
-// Gaussian's step reads and writes its own values only, with its own hash
-// indices, so the results are those of k_chain_step, bit for bit.
-//
-// touched[0] is the count (cleared before k_touched), the list starts at
-// touched[kTouchedListStart].
-constexpr uint32_t kTouchedListStart = 32;
-
-template <bool FIXED>
-__global__ void __launch_bounds__(256) k_touched(const void *__restrict__ rawIn, uint32_t n, uint32_t *touched,
-                                                 const uint32_t *error) {
-  chain_enter();
-  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
-  uint32_t bits = 0u;
-  if (i < n) {
-    // The sums' bits ORed together, every load first. As k_chain_step's test
-    // raw[k] != 0.0f: an integer sum is non-zero exactly when its value is; a
-    // float sum of -0 (only its sign bit set) counts as zero.
-    const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
-    const uint4 a = r4[0], b = r4[1], c = r4[2], d = r4[3];
-    const uint32_t keep = FIXED ? 0xFFFFFFFFu : 0x7FFFFFFFu;
-    static_assert(kRawPerSplat == 14, "the last word read is sum 13");
-    bits = ((a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) & keep) | ((c.x | c.y | c.z | c.w) & keep) |
-           ((d.x | d.y) & keep);
-  }
-  const bool reached = bits != 0u;
-  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, reached);
-  if (mask == 0u) return;
-  uint32_t base = 0;
-  if (lane == (uint32_t)(__ffs(mask) - 1)) base = atomicAdd(touched, (uint32_t)__popc(mask));
-  base = __shfl_sync(0xFFFFFFFFu, base, __ffs(mask) - 1);
-  if (reached) touched[kTouchedListStart + base + __popc(mask & ((1u << lane) - 1u))] = i;
-}
-
+// the chain rule and the step with a few lanes of each warp. So each block of
+// k_chain_reached first lists the reached Gaussians of its chunk of
+// kReachChunk in shared memory, then its threads step that list, full warps.
+// The list's order (warp-aggregated appends) varies from run to run and does
+// not matter: a Gaussian's step reads and writes its own values only, with
+// its own hash indices, so the results are those of k_chain_step, bit for bit.
 constexpr uint32_t kTouchedThreads = 128;
+constexpr uint32_t kReachChunk = 2048;
 // Coefficients whose SH Adam state words are loaded together in the SH step.
 constexpr int kStateBatch = 5;
 
-// The one-view selective step of a listed Gaussian, one thread each. Its SH
-// coefficients and SH Adam state sit in planes, one scattered word per
-// element, so every load of a coefficient is issued up front (predicated on
-// the coefficient being in use, no branch between them) and the state words
-// go in batches of kStateBatch coefficients: a handful of memory latencies
-// per Gaussian instead of one per coefficient. Element by element the
-// arithmetic, hash indices and order of sums are k_chain_step's.
+// Whether Gaussian i's backward sums hold anything, as k_chain_step's test
+// raw[k] != 0.0f: an integer sum is non-zero exactly when its value is; a
+// float sum of -0 (only its sign bit set) counts as zero.
+template <bool FIXED> __device__ __forceinline__ uint32_t reached_bits(const void *rawIn, uint32_t i) {
+  const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
+  const uint4 a = r4[0], b = r4[1], c = r4[2], d = r4[3];
+  const uint32_t keep = FIXED ? 0xFFFFFFFFu : 0x7FFFFFFFu;
+  static_assert(kRawPerSplat == 14, "the last word read is sum 13");
+  return ((a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) & keep) | ((c.x | c.y | c.z | c.w) & keep) | ((d.x | d.y) & keep);
+}
+
+// The one-view selective step of a reached Gaussian. Its SH coefficients and
+// SH Adam state are reached through scattered words (the coefficients in
+// planes, the state in its row), so every load of a coefficient is issued up
+// front (predicated on the coefficient being in use, no branch between them)
+// and the state words go in batches of kStateBatch coefficients: a handful of
+// memory latencies per Gaussian instead of one per coefficient. Element by
+// element the arithmetic, hash indices and order of sums are k_chain_step's.
 template <ShStore S, StateStore ST, bool FIXED>
-__global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_touched(Params p, const ViewSet *__restrict__ viewsPtr,
-                                                                      const void *__restrict__ rawIn,
-                                                                      const Splat *__restrict__ splats,
-                                                                      const ChainArgs *__restrict__ argsPtr, OptimState state,
-                                                                      float *__restrict__ densifyStats,
-                                                                      const uint32_t *__restrict__ touched,
-                                                                      const uint32_t *error) {
-  chain_enter();
-  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  const ViewParams &cam = viewsPtr->v[0];
-  const uint32_t count = touched[0], n = p.n, ps = p.planeStride;
-  const ChainArgs args = *argsPtr;
-  const AdamArgs a = adam_args(args);
-  const int active = min(cam.activeCoeffs, p.shCoeffs);
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
-    const uint32_t i = touched[kTouchedListStart + j];
-    const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
-    const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
-    const float rawOpacity = p.opacities[i];
-    const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
-    const float4 col = splats[i].colorRadius;
-    uint32_t words[16];
-    {
-      const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
+__device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const ViewParams &cam, const ChainArgs &args,
+                                             const AdamArgs &a, int active, const void *__restrict__ rawIn,
+                                             const Splat *__restrict__ splats, const OptimState &state,
+                                             float *__restrict__ densifyStats) {
+  const uint32_t n = p.n, ps = p.planeStride;
+  const float pos[3] = {p.positions[i * 3], p.positions[i * 3 + 1], p.positions[i * 3 + 2]};
+  const float logScale[3] = {p.scales[i * 3], p.scales[i * 3 + 1], p.scales[i * 3 + 2]};
+  const float rawOpacity = p.opacities[i];
+  const float4 rq = reinterpret_cast<const float4 *>(p.rotations)[i];
+  const float4 col = splats[i].colorRadius;
+  uint32_t words[16];
+  {
+    const uint4 *r4 = reinterpret_cast<const uint4 *>(rawIn) + (size_t)i * (kRawStride / 4);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint4 w4 = r4[q];
-        words[q * 4] = w4.x;
-        words[q * 4 + 1] = w4.y;
-        words[q * 4 + 2] = w4.z;
-        words[q * 4 + 3] = w4.w;
-      }
+    for (int q = 0; q < 4; ++q) {
+      const uint4 w4 = r4[q];
+      words[q * 4] = w4.x;
+      words[q * 4 + 1] = w4.y;
+      words[q * 4 + 2] = w4.z;
+      words[q * 4 + 3] = w4.w;
     }
-    // The coefficients in use, all loads in flight together.
-    float dc[3], rest[kMaxCoeffs - 1][3];
+  }
+  // The coefficients in use, all loads in flight together.
+  float dc[3], rest[kMaxCoeffs - 1][3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) dc[c] = active > 0 ? p.shDc[(size_t)c * ps + i] : 0.0f;
+  for (int c = 0; c < 3; ++c) dc[c] = active > 0 ? p.shDc[(size_t)c * ps + i] : 0.0f;
+#pragma unroll
+  for (int k = 1; k < kMaxCoeffs; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      rest[k - 1][c] = k < active ? load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i) : 0.0f;
+  float raw[kRawPerSplat];
+#pragma unroll
+  for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
+  const float opacity = 1.0f / (1.0f + splat_expf(-rawOpacity));
+  float gP[3] = {0.f, 0.f, 0.f}, gScale[3] = {0.f, 0.f, 0.f}, gRot[4] = {0.f, 0.f, 0.f, 0.f}, gOpacity = 0.f;
+  float gColour[3] = {0.f, 0.f, 0.f}, dir[3] = {0.f, 0.f, 0.f}, gPv[3] = {0.f, 0.f, 0.f}, distance = 1.0f;
+  if (args.statistics) {
+    float4 *stats = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
+    float4 sa = stats[0], sb = stats[1];
+    const float hx = 0.5f * cam.widthF, hy = 0.5f * cam.heightF;
+    const float ax = raw[1] * hx, ay = raw[2] * hy;
+    sa.x += sqrtf(fmaf(ay, ay, ax * ax));
+    sa.y += 1.0f;
+    sa.z = fmaxf(sa.z, col.w);
+    sa.w += raw[9] * 3.0f * cam.widthF * cam.heightF;
+    const float bx = raw[10] * hx, by = raw[11] * hy;
+    sb.x += sqrtf(fmaf(by, by, bx * bx));
+    stats[0] = sa;
+    stats[1] = sb;
+  }
+  chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
+  if (cam.activeDegree > 0) {
+    float gDir[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int k = 1; k < kMaxCoeffs; ++k)
+      if (k < active) direction_term(k, rest[k - 1], gColour, dir, gDir);
+    add_direction_term(gDir, dir, distance, gPv);
+  }
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        rest[k - 1][c] = k < active ? load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i) : 0.0f;
-    float raw[kRawPerSplat];
-#pragma unroll
-    for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
-    const float opacity = 1.0f / (1.0f + splat_expf(-rawOpacity));
-    float gP[3] = {0.f, 0.f, 0.f}, gScale[3] = {0.f, 0.f, 0.f}, gRot[4] = {0.f, 0.f, 0.f, 0.f}, gOpacity = 0.f;
-    float gColour[3] = {0.f, 0.f, 0.f}, dir[3] = {0.f, 0.f, 0.f}, gPv[3] = {0.f, 0.f, 0.f}, distance = 1.0f;
-    if (args.statistics) {
-      float4 *stats = reinterpret_cast<float4 *>(densifyStats + (size_t)i * kStatStride);
-      float4 sa = stats[0], sb = stats[1];
-      const float hx = 0.5f * cam.widthF, hy = 0.5f * cam.heightF;
-      const float ax = raw[1] * hx, ay = raw[2] * hy;
-      sa.x += sqrtf(fmaf(ay, ay, ax * ax));
-      sa.y += 1.0f;
-      sa.z = fmaxf(sa.z, col.w);
-      sa.w += raw[9] * 3.0f * cam.widthF * cam.heightF;
-      const float bx = raw[10] * hx, by = raw[11] * hy;
-      sb.x += sqrtf(fmaf(by, by, bx * bx));
-      stats[0] = sa;
-      stats[1] = sb;
-    }
-    chain_view(cam, raw, col, pos, logScale, opacity, rq, gPv, gScale, gRot, gOpacity, gColour, dir, distance);
-    if (cam.activeDegree > 0) {
-      float gDir[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-      for (int k = 1; k < kMaxCoeffs; ++k)
-        if (k < active) direction_term(k, rest[k - 1], gColour, dir, gDir);
-      add_direction_term(gDir, dir, distance, gPv);
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
+  for (int c = 0; c < 3; ++c) gP[c] += gPv[c];
 
-    // Adam on the 11 geometry elements, as k_chain_step (selective: an
-    // element with a zero gradient is left alone).
-    {
-      float gv[11], value[11], m[11], vv[11];
-      uint32_t word[11];
+  // Adam on the 11 geometry elements, as k_chain_step (selective: an
+  // element with a zero gradient is left alone).
+  {
+    float gv[11], value[11], m[11], vv[11];
+    uint32_t word[11];
 #pragma unroll
-      for (int e = 0; e < 11; ++e) {
-        const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
-        const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
-        const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
-        const uint32_t idx = i * per + (uint32_t)a0;
-        gv[e] = group == 0 ? gP[a0] : group == 1 ? gScale[a0] : group == 2 ? gRot[a0] : gOpacity;
-        value[e] = group == 0 ? pos[a0] : group == 1 ? logScale[a0] : group == 3 ? rawOpacity
-                 : a0 == 0 ? rq.x : a0 == 1 ? rq.y : a0 == 2 ? rq.z : rq.w;
-        m[e] = vv[e] = 0.0f;
-        word[e] = 0u;
-        if (gv[e] == 0.0f) continue;
-        load_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e]);
-      }
-#pragma unroll
-      for (int e = 0; e < 11; ++e) {
-        const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
-        const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
-        const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
-        const uint32_t idx = i * per + (uint32_t)a0;
-        if (gv[e] == 0.0f) continue;
-        adam(value[e], m[e], vv[e], gv[e], args.rates[group], a);
-        store_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e], idx * 5u + (uint32_t)group, a.seed);
-        float *values = group == 0 ? p.positions : group == 1 ? p.scales : group == 2 ? p.rotations : p.opacities;
-        values[idx] = value[e];
-      }
+    for (int e = 0; e < 11; ++e) {
+      const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+      const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+      const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+      const uint32_t idx = i * per + (uint32_t)a0;
+      gv[e] = group == 0 ? gP[a0] : group == 1 ? gScale[a0] : group == 2 ? gRot[a0] : gOpacity;
+      value[e] = group == 0 ? pos[a0] : group == 1 ? logScale[a0] : group == 3 ? rawOpacity
+               : a0 == 0 ? rq.x : a0 == 1 ? rq.y : a0 == 2 ? rq.z : rq.w;
+      m[e] = vv[e] = 0.0f;
+      word[e] = 0u;
+      if (gv[e] == 0.0f) continue;
+      load_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e]);
     }
+#pragma unroll
+    for (int e = 0; e < 11; ++e) {
+      const int group = e < 3 ? 0 : e < 6 ? 1 : e < 10 ? 2 : 3;
+      const int a0 = e < 3 ? e : e < 6 ? e - 3 : e < 10 ? e - 6 : 0;
+      const uint32_t per = group == 2 ? 4u : group == 3 ? 1u : 3u;
+      const uint32_t idx = i * per + (uint32_t)a0;
+      if (gv[e] == 0.0f) continue;
+      adam(value[e], m[e], vv[e], gv[e], args.rates[group], a);
+      store_state(state.state[group], ST, per * n, idx, m[e], vv[e], word[e], idx * 5u + (uint32_t)group, a.seed);
+      float *values = group == 0 ? p.positions : group == 1 ? p.scales : group == 2 ? p.rotations : p.opacities;
+      values[idx] = value[e];
+    }
+  }
 
-    // The SH step: only the coefficients in use have a gradient. The state
-    // words of kStateBatch coefficients are loaded together, then stepped.
-    const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
-    const uint32_t hashBase = i * shFloats * 5u + 4u;
-    uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, shFloats);
-    const size_t stateCount = (size_t)ps * shFloats; // F32: the v rows follow the m rows
-    const float restRate = args.rates[4] * args.restScale;
+  // The SH step: only the coefficients in use have a gradient. The state
+  // words of kStateBatch coefficients are loaded together, then stepped.
+  const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
+  const uint32_t hashBase = i * shFloats * 5u + 4u;
+  uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, shFloats);
+  const size_t stateCount = (size_t)ps * shFloats; // F32: the v rows follow the m rows
+  const float restRate = args.rates[4] * args.restScale;
 #pragma unroll
-    for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStateBatch) {
-      float m[kStateBatch][3], v[kStateBatch][3];
+  for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStateBatch) {
+    float m[kStateBatch][3], v[kStateBatch][3];
 #pragma unroll
-      for (int b = 0; b < kStateBatch; ++b)
+    for (int b = 0; b < kStateBatch; ++b)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const int k = k0 + b;
-          const size_t at = (size_t)(3 * k + c);
-          m[b][c] = v[b][c] = 0.0f;
-          if (k < active) {
-            if constexpr (ST == StateStore::F32) {
-              m[b][c] = reinterpret_cast<const float *>(stateWords)[at];
-              v[b][c] = reinterpret_cast<const float *>(stateWords)[stateCount + at];
-            } else {
-              const uint32_t w = stateWords[at];
-              m[b][c] = bf16_load(w, 0);
-              v[b][c] = bf16_load(w, 1);
-            }
-          }
-        }
-#pragma unroll
-      for (int b = 0; b < kStateBatch; ++b) {
+      for (int c = 0; c < 3; ++c) {
         const int k = k0 + b;
-        if (k >= active) continue;
-        const float basis = basis_one(k, dir[0], dir[1], dir[2]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float g = fmaf(basis, gColour[c], 0.0f);
-          if (g == 0.0f) continue;
-          const uint32_t plane = (uint32_t)(3 * k + c);
-          const size_t at = plane;
-          float val = k == 0 ? dc[c] : rest[k > 0 ? k - 1 : 0][c];
-          float mm = m[b][c], vvv = v[b][c];
-          adam(val, mm, vvv, g, k == 0 ? args.rates[4] : restRate, a);
+        const size_t at = (size_t)(3 * k + c);
+        m[b][c] = v[b][c] = 0.0f;
+        if (k < active) {
           if constexpr (ST == StateStore::F32) {
-            reinterpret_cast<float *>(stateWords)[at] = mm;
-            reinterpret_cast<float *>(stateWords)[stateCount + at] = vvv;
+            m[b][c] = reinterpret_cast<const float *>(stateWords)[at];
+            v[b][c] = reinterpret_cast<const float *>(stateWords)[stateCount + at];
           } else {
-            stateWords[at] = bf16_pair(mm, vvv, hashBase + plane * 5u, a.seed);
+            const uint32_t w = stateWords[at];
+            m[b][c] = bf16_load(w, 0);
+            v[b][c] = bf16_load(w, 1);
           }
-          if (k == 0) p.shDc[(size_t)c * ps + i] = val;
-          else store_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i, val, hashBase + plane * 5u, args.seed);
         }
+      }
+#pragma unroll
+    for (int b = 0; b < kStateBatch; ++b) {
+      const int k = k0 + b;
+      if (k >= active) continue;
+      const float basis = basis_one(k, dir[0], dir[1], dir[2]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float g = fmaf(basis, gColour[c], 0.0f);
+        if (g == 0.0f) continue;
+        const uint32_t plane = (uint32_t)(3 * k + c);
+        const size_t at = plane;
+        float val = k == 0 ? dc[c] : rest[k > 0 ? k - 1 : 0][c];
+        float mm = m[b][c], vvv = v[b][c];
+        adam(val, mm, vvv, g, k == 0 ? args.rates[4] : restRate, a);
+        if constexpr (ST == StateStore::F32) {
+          reinterpret_cast<float *>(stateWords)[at] = mm;
+          reinterpret_cast<float *>(stateWords)[stateCount + at] = vvv;
+        } else {
+          stateWords[at] = bf16_pair(mm, vvv, hashBase + plane * 5u, a.seed);
+        }
+        if (k == 0) p.shDc[(size_t)c * ps + i] = val;
+        else store_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i, val, hashBase + plane * 5u, args.seed);
       }
     }
   }
+}
+
+template <ShStore S, StateStore ST, bool FIXED>
+__global__ void __launch_bounds__(kTouchedThreads, 4) k_chain_reached(Params p, const ViewSet *__restrict__ viewsPtr,
+                                                                      const void *__restrict__ rawIn,
+                                                                      const Splat *__restrict__ splats,
+                                                                      const ChainArgs *__restrict__ argsPtr, OptimState state,
+                                                                      float *__restrict__ densifyStats, const uint32_t *error) {
+  chain_enter();
+  __shared__ uint32_t s_list[kReachChunk];
+  __shared__ uint32_t s_count;
+  if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  const uint32_t first = blockIdx.x * kReachChunk, n = p.n;
+  if (tid == 0) s_count = 0u;
+  __syncthreads();
+  // The chunk's reached Gaussians, four loads of sums in flight per thread.
+  for (uint32_t r = 0; r < kReachChunk; r += 4 * kTouchedThreads) {
+    uint32_t bits[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t g = first + r + (uint32_t)q * kTouchedThreads + tid;
+      bits[q] = g < n ? reached_bits<FIXED>(rawIn, g) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t g = first + r + (uint32_t)q * kTouchedThreads + tid;
+      const uint32_t mask = __ballot_sync(0xFFFFFFFFu, bits[q] != 0u);
+      if (mask == 0u) continue;
+      uint32_t base = 0;
+      if (lane == (uint32_t)(__ffs(mask) - 1)) base = atomicAdd(&s_count, (uint32_t)__popc(mask));
+      base = __shfl_sync(0xFFFFFFFFu, base, __ffs(mask) - 1);
+      if (bits[q] != 0u) s_list[base + __popc(mask & ((1u << lane) - 1u))] = g;
+    }
+  }
+  __syncthreads();
+  const uint32_t count = s_count;
+  const ViewParams &cam = viewsPtr->v[0];
+  const ChainArgs args = *argsPtr;
+  const AdamArgs a = adam_args(args);
+  const int active = min(cam.activeCoeffs, p.shCoeffs);
+  for (uint32_t j = tid; j < count; j += kTouchedThreads)
+    step_reached<S, ST, FIXED>(s_list[j], p, cam, args, a, active, rawIn, splats, state, densifyStats);
 }
 
 // train_score.comp: to each Gaussian's statistics, the marked pixels it
@@ -1094,32 +1105,27 @@ __global__ void __launch_bounds__(256) k_score(const void *__restrict__ rawIn, b
 template <ShStore S>
 void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                     const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
-                    uint32_t *touched, uint32_t *error, cudaStream_t stream) {
+                    uint32_t *error, cudaStream_t stream) {
   const GradientsOut g = *grads;
   const bool store = args.mode == ChainMode::Gradients;
   const uint32_t blocks = div_up(p.n, 128);
   const bool multi = views.count > 1;
   // The fused form indexes the F32 SH state (m and v rows of 48 floats a Gaussian) in 32 bits.
   if (!multi && !args.splitStep && args.mode == ChainMode::Step && (size_t)p.planeStride * 3 * kMaxCoeffs * 2 < (size_t{1} << 32)) {
-    if (touched != nullptr && args.selective && args.opacityReg == 0.0f && args.scaleReg == 0.0f) {
-      // Only the reached Gaussians change: list them, then step the list.
-      cudaMemsetAsync(touched, 0, 4, stream);
-      if (args.fixedPoint) launch_chained(k_touched<true>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
-      else launch_chained(k_touched<false>, dim3(div_up(p.n, 256)), dim3(256), 0, stream, raw, p.n, touched, error);
-#define SB_TOUCHED(ST, FIX)                                                                                             \
-  {                                                                                                                      \
-    const uint32_t grid = std::min<uint32_t>(div_up(p.n, kTouchedThreads),                                                \
-                                             resident_blocks((const void *)k_chain_touched<S, ST, FIX>, kTouchedThreads)); \
-    launch_chained(k_chain_touched<S, ST, FIX>, dim3(grid), dim3(kTouchedThreads), 0, stream, p, dViews, raw, splats,   \
-                   dArgs, state, densifyStats, (const uint32_t *)touched, (const uint32_t *)error);                       \
-  }
+    if (args.selective && args.opacityReg == 0.0f && args.scaleReg == 0.0f) {
+      // Only the reached Gaussians change: each block lists its chunk's, then steps them.
+#define SB_REACHED(ST, FIX)                                                                                           \
+  launch_chained(k_chain_reached<S, ST, FIX>, dim3(div_up(p.n, kReachChunk)), dim3(kTouchedThreads), 0, stream, p,    \
+                 dViews, raw, splats, dArgs, state, densifyStats, (const uint32_t *)error)
       const bool f32 = state.store == StateStore::F32;
       if (args.fixedPoint) {
-        if (f32) SB_TOUCHED(StateStore::F32, true) else SB_TOUCHED(StateStore::BF16Pair, true)
+        if (f32) SB_REACHED(StateStore::F32, true);
+        else SB_REACHED(StateStore::BF16Pair, true);
       } else {
-        if (f32) SB_TOUCHED(StateStore::F32, false) else SB_TOUCHED(StateStore::BF16Pair, false)
+        if (f32) SB_REACHED(StateStore::F32, false);
+        else SB_REACHED(StateStore::BF16Pair, false);
       }
-#undef SB_TOUCHED
+#undef SB_REACHED
       return;
     }
     const uint32_t smem = step_stage_bytes(p.shCoeffs, S == ShStore::F32 ? 4 : 2, state.store == StateStore::F32);
@@ -1166,17 +1172,17 @@ void launch_score(const void *raw, bool fixedPoint, float fixedScale, uint32_t n
 
 void launch_chain(const Params &p, const ViewSet &views, const ViewSet *dViews, const void *raw, const Splat *splats, const ChainArgs &args,
                   const ChainArgs *dArgs, OptimState &state, const GradientsOut *grads, float4 *shGrad, float *densifyStats,
-                  uint32_t *touched, uint32_t *error, cudaStream_t stream) {
+                  uint32_t *error, cudaStream_t stream) {
   if (p.n == 0) return;
   switch (p.shStore) {
   case ShStore::BF16:
-    launch_chain_s<ShStore::BF16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, touched, error, stream);
+    launch_chain_s<ShStore::BF16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
     break;
   case ShStore::F16:
-    launch_chain_s<ShStore::F16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, touched, error, stream);
+    launch_chain_s<ShStore::F16>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
     break;
   default:
-    launch_chain_s<ShStore::F32>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, touched, error, stream);
+    launch_chain_s<ShStore::F32>(p, views, dViews, raw, splats, args, dArgs, state, grads, shGrad, densifyStats, error, stream);
     break;
   }
 }

@@ -205,7 +205,6 @@ public:
   // Per (view, Gaussian).
   int viewSlots = 0;
   DeviceBuffer splats, reach, depthKeys, values, tmpKeys, tmpValues, offsets, raw, shGrad;
-  DeviceBuffer touched; // the one-view selective step's count and list of reached Gaussians
   // Tile entries.
   uint32_t entryCapacity = 0;
   DeviceBuffer entryKeys, entryValues, tmpEntryKeys, tmpEntryValues;
@@ -468,9 +467,8 @@ uint64_t Trainer::bytes_per_gaussian() const {
   // reached-tile masks and counts 12, raw sums 64, colour gradient and
   // direction for the SH step 32.
   const uint64_t perView = sizeof(Splat) + 4 + 16 + 12 + kRawStride * 4 + 32;
-  // Geometry gradients between the chain rule and Adam: 11 floats; the list
-  // of reached Gaussians: 1.
-  return params + optimiser + 12 * 4 + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
+  // Geometry gradients between the chain rule and Adam: 11 floats.
+  return params + optimiser + 11 * 4 + kStatStride * 4 + perView * (uint64_t)std::max(viewSlots, 1);
 }
 
 uint64_t Trainer::entry_bytes(uint64_t entries) const {
@@ -582,7 +580,6 @@ void Trainer::ensure_view_buffers() {
     offsets.ensure(items * 12); // entry offsets, the reached-tile masks, then (depth-sorted form) the counts per splat
     raw.ensure(items * kRawStride * 4);
     shGrad.ensure(items * 32);
-    touched.ensure(((size_t)n + 32) * 4);
     SB_CUDA(cudaMemset(raw.get(), 0, items * kRawStride * 4));
     viewSlots = count;
     clear_graphs();
@@ -929,7 +926,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   const GradientsOut *gp = &g;
   begin(7);
   launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
-               shGrad.get<float4>(), densifyStats.get<float>(), touched.get<uint32_t>(), error, stream);
+               shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
   end(7);
 }
 
@@ -1552,8 +1549,8 @@ int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_r
     sb::GradientsOut g{};
     for (int k = 0; k < 5; ++k) g.g[k] = t->grads[k].get<float>();
     sb::launch_chain(t->params(), t->views, t->dViews.get<sb::ViewSet>(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
-                     t->dArgs.get<sb::ChainArgs>(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(),
-                     t->touched.get<uint32_t>(), nullptr, t->stream);
+                     t->dArgs.get<sb::ChainArgs>(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
+                     t->stream);
     SB_CUDA(cudaStreamSynchronize(t->stream));
   });
 }
