@@ -628,12 +628,14 @@ def test_apply_changes_gathers_the_state(splat, oracle, state):
         n = new[g][: copies * new_n * stride].reshape(copies, new_n, stride)
         np.testing.assert_array_equal(n[:, kept], o[:, source[kept]])
         assert not n[:, ~kept].any()
-    planes = 3 * 9 * copies
-    old_ps, new_ps = 512, ((new_n + 127) // 128) * 128
-    o = old[4][: planes * old_ps].reshape(planes, old_ps)
-    n = new[4][: planes * new_ps].reshape(planes, new_ps)
+    # The SH state: rows of 27 words (degree 2), row counts rounded up to 128.
+    width = 3 * 9
+    old_rows, new_rows = 512, ((new_n + 127) // 128) * 128
+    o = old[4][: copies * old_rows * width].reshape(copies, old_rows, width)
+    n = new[4][: copies * new_rows * width].reshape(copies, new_rows, width)
     np.testing.assert_array_equal(n[:, :new_n][:, kept], o[:, source[kept]])
     assert not n[:, :new_n][:, ~kept].any()
+    assert not n[:, new_n:].any()
     assert np.any(o[:, source[kept]])
     assert np.isfinite(t.step(to_camera(view), target, rates).loss)
 
