@@ -501,10 +501,11 @@ int splat_trainer_autotune(splat_trainer *trainer, const splat_camera *camera, c
 int splat_trainer_set_timing(splat_trainer *trainer, int32_t enabled);
 /* Trainer::parameters (trainer.hpp:137): the device address of a parameter
  * group (0 positions, 1 scales, 2 rotations, 3 opacities, 4 SH DC planes,
- * 5 SH rest planes), valid until the Gaussians change in number. SH is stored
- * in planes, one per coefficient and channel, each the Gaussian count rounded
- * up to a multiple of 128 elements long (FP32 for DC; the rest in the
- * sh_storage type). */
+ * 5 SH rest rows), valid until the Gaussians change in number. The DC is
+ * stored in 3 FP32 planes, one per channel, each the Gaussian count rounded
+ * up to a multiple of 128 elements long; the higher coefficients in one row
+ * per Gaussian (coefficient-major, channel-minor, in the sh_storage type),
+ * padded to a multiple of 16 bytes, as many rows as a plane is long. */
 int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint64_t *device_address, uint64_t *bytes);
 
 /* Debug access to the device buffers of the last step, for parity tests:

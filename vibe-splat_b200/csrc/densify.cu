@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) k_densify_tables(uint32_t n, uint32_t sur
 // and a zero SH rest where asked.
 __global__ void __launch_bounds__(128) k_densify_patch(const DensifyPatch *__restrict__ patches, uint32_t count, float *positions,
                                                        float *scales, float *rotations, float *opacities, void *shRest,
-                                                       uint32_t restPlanes, uint32_t planeStride, uint32_t shBytes) {
+                                                       uint32_t restElements, uint32_t restStride, uint32_t shBytes) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
   const DensifyPatch q = patches[k];
@@ -202,8 +202,8 @@ __global__ void __launch_bounds__(128) k_densify_patch(const DensifyPatch *__res
   }
   if ((q.what & kPatchOpacity) != 0u) opacities[at] = q.opacity;
   if ((q.what & kPatchShRest) != 0u) {
-    for (uint32_t plane = 0; plane < restPlanes; ++plane) {
-      const size_t e = (size_t)plane * planeStride + at;
+    for (uint32_t element = 0; element < restElements; ++element) {
+      const size_t e = at * restStride + element;
       if (shBytes == 4) static_cast<float *>(shRest)[e] = 0.0f;
       else static_cast<uint16_t *>(shRest)[e] = 0;
     }
@@ -291,11 +291,11 @@ void launch_densify_tables(uint32_t n, uint32_t survivors, const uint32_t *actio
 }
 
 void launch_densify_patch(const DensifyPatch *patches, uint32_t count, float *positions, float *scales, float *rotations,
-                          float *opacities, void *shRest, uint32_t restPlanes, uint32_t planeStride, uint32_t shBytes,
+                          float *opacities, void *shRest, uint32_t restElements, uint32_t restStride, uint32_t shBytes,
                           cudaStream_t stream) {
   if (count == 0) return;
-  k_densify_patch<<<div_up(count, 128), 128, 0, stream>>>(patches, count, positions, scales, rotations, opacities, shRest, restPlanes,
-                                                          planeStride, shBytes);
+  k_densify_patch<<<div_up(count, 128), 128, 0, stream>>>(patches, count, positions, scales, rotations, opacities, shRest,
+                                                          restElements, restStride, shBytes);
 }
 
 } // namespace sb

@@ -31,12 +31,20 @@ enum class ShStore : int { F32 = 0, BF16 = 1, F16 = 2 };
 enum class StateStore : int { F32 = 0, BF16Pair = 1 };
 
 // Trainable parameters, in this library's HBM layout: positions, log-scales and
-// quaternions per Gaussian (12, 12, 16 bytes), opacity logits (4 bytes), SH
-// planar: shDc[c * planeStride + i] and shRest[((k - 1) * 3 + c) * planeStride
-// + i]. planeStride is n rounded up to kPlaneAlign, so that every plane starts
-// 16-byte aligned at every multiple of kPlaneAlign Gaussians (bulk copies);
-// the SH Adam state uses the same planes.
+// quaternions per Gaussian (12, 12, 16 bytes), opacity logits (4 bytes), SH DC
+// planar: shDc[c * planeStride + i]; the higher SH coefficients in rows:
+// shRest[i * restStride + (k - 1) * 3 + c], restStride = 3 (coeffs - 1)
+// elements rounded up to 16 bytes (sh_rest_stride). planeStride is n rounded
+// up to kPlaneAlign, and the rows count as many, so that a block of
+// kPlaneAlign Gaussians starts every plane and its rows 16-byte aligned (bulk
+// copies). The SH Adam state is in rows too (sh_state_at).
 constexpr uint32_t kPlaneAlign = 128;
+
+// Elements in a Gaussian's row of higher SH coefficients.
+inline uint32_t sh_rest_stride(int shCoeffs, ShStore store) {
+  const uint32_t elements = 3u * (uint32_t)(shCoeffs - 1), bytes = store == ShStore::F32 ? 4u : 2u;
+  return elements == 0u ? 0u : (elements * bytes + 15u) / 16u * 16u / bytes;
+}
 struct Params {
   float *positions;
   float *scales;
@@ -47,6 +55,7 @@ struct Params {
   ShStore shStore;
   uint32_t n;
   uint32_t planeStride;
+  uint32_t restStride; // elements per row of shRest
   int shDegree;
   int shCoeffs;
 };
@@ -280,10 +289,10 @@ void launch_densify_tables(uint32_t n, uint32_t survivors, const uint32_t *actio
 // Relocation (relocate_cloud, densify.cpp:328-420): dead and alive flags,
 // dead where the logit is below deadLogit or a value is not finite.
 void launch_relocate_flags(const Params &p, float deadLogit, uint32_t *dead, uint32_t *alive, cudaStream_t stream);
-// Writes host-computed rows into their slots (shRest: restPlanes planes of
-// planeStride elements of shBytes bytes).
+// Writes host-computed rows into their slots (shRest: rows of restStride
+// elements of shBytes bytes, the first restElements in use).
 void launch_densify_patch(const DensifyPatch *patches, uint32_t count, float *positions, float *scales, float *rotations,
-                          float *opacities, void *shRest, uint32_t restPlanes, uint32_t planeStride, uint32_t shBytes,
+                          float *opacities, void *shRest, uint32_t restElements, uint32_t restStride, uint32_t shBytes,
                           cudaStream_t stream);
 
 // The coarse-to-fine schedule's device work (csrc/schedule.cu).

@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       word[kk][c] = 0u;
       if (k >= p.shCoeffs) continue;
       const size_t t = (size_t)(k * 3 + c) * ps + i, ts = sh_state_at(i, (uint32_t)(k * 3 + c), shFloats);
-      value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, t - 3 * ps);
+      value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride));
       if (state.store == StateStore::F32) {
         m[kk][c] = static_cast<const float *>(state.state[4])[ts];
         vv[kk][c] = static_cast<const float *>(state.state[4])[count + ts];
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       if (k == 0) {
         p.shDc[t] = value[kk][c];
       } else {
-        store_sh_rest<S>(p.shRest, t - 3 * ps, value[kk][c], hashIndex, args.seed);
+        store_sh_rest<S>(p.shRest, sh_rest_at(i, plane - 3u, p.restStride), value[kk][c], hashIndex, args.seed);
       }
     }
   }
@@ -628,11 +628,11 @@ __device__ __forceinline__ void store_state(void *st, StateStore store, uint32_t
   }
 }
 
-// Shared-memory bytes of a block's staged SH planes and state.
-__host__ __device__ inline uint32_t step_stage_bytes(int coeffs, int shBytes, bool stateF32) {
+// Shared-memory bytes of a block's staged SH: the DC planes, the rows of
+// higher coefficients (restStride elements each) and the state rows.
+__host__ __device__ inline uint32_t step_stage_bytes(int coeffs, int shBytes, bool stateF32, uint32_t restStride) {
   const uint32_t planes = 3u * (uint32_t)coeffs;
-  return 3u * kStepThreads * 4u + (planes - 3u) * kStepThreads * (uint32_t)shBytes +
-         (stateF32 ? 2u : 1u) * planes * kStepThreads * 4u;
+  return 3u * kStepThreads * 4u + restStride * kStepThreads * (uint32_t)shBytes + (stateF32 ? 2u : 1u) * planes * kStepThreads * 4u;
 }
 
 template <ShStore S> __device__ __forceinline__ float staged_sh_rest(const unsigned char *rest, uint32_t at) {
@@ -662,25 +662,24 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   constexpr bool stateF32 = ST == StateStore::F32;
   float *s_dc = reinterpret_cast<float *>(s_stage);
   unsigned char *s_rest = s_stage + 3u * kStepThreads * 4u;
-  unsigned char *s_state = s_rest + restPlanes * kStepThreads * kShBytes;
+  unsigned char *s_state = s_rest + p.restStride * kStepThreads * kShBytes;
   if (tid == 0) bulk_barrier_init(&s_bar, 1);
   __syncthreads();
   if (tid < 32u) {
     // Warp 0 issues the copies: DC planes, rest planes, state planes (F32: m then v).
-    if (tid == 0) bulk_expect(&s_bar, step_stage_bytes(p.shCoeffs, (int)kShBytes, stateF32));
+    if (tid == 0) bulk_expect(&s_bar, step_stage_bytes(p.shCoeffs, (int)kShBytes, stateF32, p.restStride));
     __syncwarp();
-    const uint32_t copies = planes + (stateF32 ? 2u : 1u);
+    // The DC planes, the block's rows of higher coefficients, its state rows.
+    const uint32_t rest = restPlanes > 0u ? 1u : 0u, copies = 3u + rest + (stateF32 ? 2u : 1u);
     for (uint32_t c = tid; c < copies; c += 32u) {
       if (c < 3u) {
         bulk_load(s_dc + c * kStepThreads, p.shDc + (size_t)c * ps + i0, kStepThreads * 4u, &s_bar);
-      } else if (c < planes) {
-        const uint32_t r = c - 3u;
-        bulk_load(s_rest + r * kStepThreads * kShBytes,
-                  static_cast<const unsigned char *>(p.shRest) + ((size_t)r * ps + i0) * kShBytes, kStepThreads * kShBytes,
-                  &s_bar);
+      } else if (c < 3u + rest) {
+        bulk_load(s_rest, static_cast<const unsigned char *>(p.shRest) + (size_t)i0 * p.restStride * kShBytes,
+                  kStepThreads * p.restStride * kShBytes, &s_bar);
       } else {
         // The block's state rows, one copy (F32: the m rows, then the v rows).
-        const uint32_t q = c - planes;
+        const uint32_t q = c - 3u - rest;
         bulk_load(s_state + q * kStepThreads * planes * 4u,
                   static_cast<const unsigned char *>(state.state[4]) + ((size_t)q * ps + i0) * planes * 4u,
                   kStepThreads * planes * 4u, &s_bar);
@@ -754,9 +753,9 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
     for (int k = 1; k < kMaxCoeffs; ++k) {
       if (k >= active) break;
       const uint32_t r = (uint32_t)(k - 1) * 3u;
-      const float value[3] = {staged_sh_rest<S>(s_rest, r * kStepThreads + tid),
-                              staged_sh_rest<S>(s_rest, (r + 1u) * kStepThreads + tid),
-                              staged_sh_rest<S>(s_rest, (r + 2u) * kStepThreads + tid)};
+      const float value[3] = {staged_sh_rest<S>(s_rest, tid * p.restStride + r),
+                              staged_sh_rest<S>(s_rest, tid * p.restStride + r + 1u),
+                              staged_sh_rest<S>(s_rest, tid * p.restStride + r + 2u)};
       direction_term(k, value, gColour, dir, gDir);
     }
     add_direction_term(gDir, dir, distance, gPv);
@@ -851,9 +850,9 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
       const float g = k < active ? fmaf(b, gColour[c], 0.0f) : 0.0f;
       if (g == 0.0f && !stepZeros) continue;
       const uint32_t plane = r + 3u + (uint32_t)c;
-      float val = staged_sh_rest<S>(s_rest, (r + (uint32_t)c) * kStepThreads + tid);
+      float val = staged_sh_rest<S>(s_rest, tid * p.restStride + r + (uint32_t)c);
       element(plane, val, g, restRate);
-      store_sh_rest<S>(p.shRest, (size_t)(r + (uint32_t)c) * ps + i, val, hashBase + plane * 5u, args.seed);
+      store_sh_rest<S>(p.shRest, sh_rest_at(i, r + (uint32_t)c, p.restStride), val, hashBase + plane * 5u, args.seed);
     }
   }
 }
@@ -921,7 +920,7 @@ __device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const 
   for (int k = 1; k < kMaxCoeffs; ++k)
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      rest[k - 1][c] = k < active ? load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i) : 0.0f;
+      rest[k - 1][c] = k < active ? load_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride)) : 0.0f;
   float raw[kRawPerSplat];
 #pragma unroll
   for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
@@ -1035,7 +1034,8 @@ __device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const 
           stateWords[at] = bf16_pair(mm, vvv, hashBase + plane * 5u, a.seed);
         }
         if (k == 0) p.shDc[(size_t)c * ps + i] = val;
-        else store_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * ps + i, val, hashBase + plane * 5u, args.seed);
+        else store_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride), val, hashBase + plane * 5u,
+                              args.seed);
       }
     }
   }
@@ -1128,7 +1128,7 @@ void launch_chain_s(const Params &p, const ViewSet &views, const ViewSet *dViews
 #undef SB_REACHED
       return;
     }
-    const uint32_t smem = step_stage_bytes(p.shCoeffs, S == ShStore::F32 ? 4 : 2, state.store == StateStore::F32);
+    const uint32_t smem = step_stage_bytes(p.shCoeffs, S == ShStore::F32 ? 4 : 2, state.store == StateStore::F32, p.restStride);
     const uint32_t stepBlocks = div_up(p.n, kStepThreads);
 #define SB_STEP(ST, FIX)                                                                                           \
   {                                                                                                                  \

@@ -22,22 +22,26 @@ constexpr int kShSpinLimit = 1 << 22;
 
 template <ShStore S> __host__ __device__ constexpr uint32_t sh_bytes() { return S == ShStore::F32 ? 4u : 2u; }
 
-// Shared-memory bytes of a block's staged SH planes: 3 DC planes (FP32) and
-// (coeffs - 1) x 3 planes of the rest, kProjectThreads Gaussians each.
-template <ShStore S> inline uint32_t project_stage_bytes(int coeffs) {
-  return kProjectThreads * (3u * 4u + 3u * (uint32_t)(coeffs - 1) * sh_bytes<S>());
+// Shared-memory bytes of a block's staged SH: 3 DC planes (FP32) and, when
+// the view uses higher coefficients, the block's rows of them (restStride
+// elements each), kProjectThreads Gaussians.
+template <ShStore S> inline uint32_t project_stage_bytes(int coeffs, uint32_t restStride) {
+  return kProjectThreads * (3u * 4u + (coeffs > 1 ? restStride * sh_bytes<S>() : 0u));
 }
 
-// One block's SH coefficients staged in shared memory: plane k * 3 + c.
-template <ShStore S>
-__device__ __forceinline__ float staged_coefficient(const unsigned char *stage, uint32_t tid, int k, int c) {
-  if (k == 0) return reinterpret_cast<const float *>(stage)[c * kProjectThreads + tid];
-  const unsigned char *rest = stage + 3u * kProjectThreads * 4u;
-  const uint32_t at = (uint32_t)((k - 1) * 3 + c) * kProjectThreads + tid;
-  if constexpr (S == ShStore::F32) return reinterpret_cast<const float *>(rest)[at];
-  else if constexpr (S == ShStore::BF16) return __uint_as_float((uint32_t)reinterpret_cast<const uint16_t *>(rest)[at] << 16);
-  else return __half2float(reinterpret_cast<const __half *>(rest)[at]);
-}
+// A thread's staged row of higher coefficients, read from shared memory in
+// 16-byte pieces (a row is a whole number of them); element e of it.
+constexpr int kMaxRowPieces = 12; // 48 FP32 elements
+template <ShStore S> struct StagedRow {
+  uint4 piece[kMaxRowPieces];
+  __device__ __forceinline__ float element(int e) const {
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(piece);
+    if constexpr (S == ShStore::F32) return __uint_as_float(w[e]);
+    const uint32_t half = (e & 1) != 0 ? w[e >> 1] >> 16 : w[e >> 1] & 0xFFFFu;
+    if constexpr (S == ShStore::BF16) return __uint_as_float(half << 16);
+    else return __half2float(__ushort_as_half((unsigned short)half));
+  }
+};
 
 // The block's SH planes (those of the view's coefficients in use) arrive by
 // bulk copies that thread 0 issues first, so they land while the projection
@@ -68,19 +72,18 @@ __global__ void __launch_bounds__(kProjectThreads, 3) k_preprocess(Params p, con
     return;
   }
   const int coeffs = cam.activeCoeffs;
+  const uint32_t rowBytes = p.restStride * sh_bytes<S>();
+  unsigned char *s_rest = s_stage + 3u * kProjectThreads * 4u;
   if (tid == 0) {
     bulk_barrier_init(&s_bar, 1);
-    // The last block's planes end at the plane stride (a multiple of 128).
+    // The last block's planes and rows end at the plane stride (a multiple of 128).
     const uint32_t count = min(kProjectThreads, p.planeStride - i0);
-    const uint32_t restPlanes = 3u * (uint32_t)(coeffs - 1);
-    bulk_expect(&s_bar, count * (3u * 4u + restPlanes * sh_bytes<S>()));
+    const uint32_t restBytes = coeffs > 1 ? count * rowBytes : 0u;
+    bulk_expect(&s_bar, count * 3u * 4u + restBytes);
     for (uint32_t c = 0; c < 3u; ++c)
       bulk_load(s_stage + c * kProjectThreads * 4u, p.shDc + (size_t)c * p.planeStride + i0, count * 4u, &s_bar);
-    unsigned char *rest = s_stage + 3u * kProjectThreads * 4u;
-    for (uint32_t r = 0; r < restPlanes; ++r)
-      bulk_load(rest + r * kProjectThreads * sh_bytes<S>(),
-                static_cast<const unsigned char *>(p.shRest) + ((size_t)r * p.planeStride + i0) * sh_bytes<S>(),
-                count * sh_bytes<S>(), &s_bar);
+    if (restBytes > 0u)
+      bulk_load(s_rest, static_cast<const unsigned char *>(p.shRest) + (size_t)i0 * rowBytes, restBytes, &s_bar);
   }
   __syncthreads();
   bool staged = false;
@@ -178,11 +181,17 @@ __global__ void __launch_bounds__(kProjectThreads, 3) k_preprocess(Params p, con
     // Unrolled to the largest count so that the coefficients' loads are issued
     // together; the sums run in coefficient order as before.
     wait_stage();
+    StagedRow<S> row;
+    const uint4 *mine = reinterpret_cast<const uint4 *>(s_rest + (size_t)tid * rowBytes);
+  #pragma unroll
+    for (int q = 0; q < kMaxRowPieces; ++q) row.piece[q] = coeffs > 1 && (uint32_t)q * 16u < rowBytes ? mine[q] : make_uint4(0u, 0u, 0u, 0u);
     float coef[kMaxShCoeffs][3];
   #pragma unroll
-    for (int k = 0; k < kMaxShCoeffs; ++k)
+    for (int ch = 0; ch < 3; ++ch) coef[0][ch] = reinterpret_cast<const float *>(s_stage)[ch * kProjectThreads + tid];
   #pragma unroll
-      for (int ch = 0; ch < 3; ++ch) coef[k][ch] = k < coeffs ? staged_coefficient<S>(s_stage, tid, k, ch) : 0.0f;
+    for (int k = 1; k < kMaxShCoeffs; ++k)
+  #pragma unroll
+      for (int ch = 0; ch < 3; ++ch) coef[k][ch] = k < coeffs ? row.element((k - 1) * 3 + ch) : 0.0f;
     float col[3] = {0.5f, 0.5f, 0.5f};
   #pragma unroll
     for (int k = 0; k < kMaxShCoeffs; ++k) {
@@ -209,11 +218,12 @@ void launch_preprocess_s(const Params &p, const ViewSet &views, const ViewSet *d
                          uint32_t *depthKeys, uint32_t *values, uint32_t *error, cudaStream_t stream) {
   int coeffs = 1;
   for (int k = 0; k < views.count; ++k) coeffs = std::max(coeffs, views.v[k].activeCoeffs);
-  const uint32_t smem = project_stage_bytes<S>(coeffs);
+  const uint32_t smem = project_stage_bytes<S>(coeffs, p.restStride);
   static uint32_t configured = 0;
+  const uint32_t most = project_stage_bytes<S>(kMaxShCoeffs, sh_rest_stride(kMaxShCoeffs, S));
   if (smem > configured) {
-    cudaFuncSetAttribute(k_preprocess<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)project_stage_bytes<S>(kMaxShCoeffs));
-    configured = project_stage_bytes<S>(kMaxShCoeffs);
+    cudaFuncSetAttribute(k_preprocess<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most);
+    configured = most;
   }
   const dim3 grid(div_up(p.n, kProjectThreads), views.count);
   launch_chained(k_preprocess<S>, grid, dim3(kProjectThreads), smem, stream, p, dViews, splats, reach, depthKeys, values, error,

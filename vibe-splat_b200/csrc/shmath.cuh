@@ -101,10 +101,15 @@ template <> __device__ __forceinline__ float load_sh_rest<ShStore::F16>(const vo
   return __half2float(static_cast<const __half *>(p)[idx]);
 }
 
+// Element e (= 3 (k - 1) + c) of Gaussian i's row of higher coefficients.
+__host__ __device__ __forceinline__ size_t sh_rest_at(uint32_t i, uint32_t e, uint32_t restStride) {
+  return (size_t)i * restStride + e;
+}
+
 // Coefficient k (0 = DC), channel c, of Gaussian i.
 template <ShStore S> __device__ __forceinline__ float sh_coefficient(const Params &p, uint32_t i, int k, int c) {
   if (k == 0) return p.shDc[(size_t)c * p.planeStride + i];
-  return load_sh_rest<S>(p.shRest, ((size_t)(k - 1) * 3 + c) * p.planeStride + i);
+  return load_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride));
 }
 
 } // namespace sb

@@ -277,9 +277,9 @@ public:
 // ---------------------------------------------------------------- set-up
 
 // The cloud's parameters into device buffers in the trainer's layout, `to`
-// = positions, scales, rotations, opacities (rows), SH DC and SH rest (planes
-// of `stride` elements, padding zero): DC as FP32, the rest in `store`,
-// rounded to nearest.
+// = positions, scales, rotations, opacities (rows), SH DC (planes of `stride`
+// elements) and SH rest (`stride` rows of sh_rest_stride elements), padding
+// zero: DC as FP32, the rest in `store`, rounded to nearest.
 void upload_cloud(const splat_cloud &cloud, int shCoeffs, ShStore store, uint32_t stride, DeviceBuffer *to[6]) {
   const size_t nn = (size_t)cloud.count, ps = stride;
   SB_CUDA(cudaMemcpy(to[0]->get(), cloud.positions, nn * 12, cudaMemcpyHostToDevice));
@@ -291,11 +291,11 @@ void upload_cloud(const splat_cloud &cloud, int shCoeffs, ShStore store, uint32_
   for (size_t i = 0; i < nn; ++i)
     for (int c = 0; c < 3; ++c) dc[c * ps + i] = cloud.sh[i * floats + c];
   SB_CUDA(cudaMemcpy(to[4]->get(), dc.data(), ps * 12, cudaMemcpyHostToDevice));
-  const size_t rest = ps * 3 * (size_t)(shCoeffs - 1);
+  const size_t rowStride = sh_rest_stride(shCoeffs, store), rest = ps * rowStride;
   if (rest == 0) return;
   std::vector<float> planes(rest, 0.0f);
   for (size_t i = 0; i < nn; ++i)
-    for (int j = 3; j < floats; ++j) planes[(size_t)(j - 3) * ps + i] = cloud.sh[i * floats + j];
+    for (int j = 3; j < floats; ++j) planes[i * rowStride + (size_t)(j - 3)] = cloud.sh[i * floats + j];
   if (store == ShStore::F32) {
     SB_CUDA(cudaMemcpy(to[5]->get(), planes.data(), rest * 4, cudaMemcpyHostToDevice));
     return;
@@ -381,7 +381,7 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   rotations.ensure(nn * 16);
   opacities.ensure(nn * 4);
   shDc.ensure(ps * 12);
-  const size_t rest = ps * 3 * (shCoeffs - 1);
+  const size_t rest = ps * sh_rest_stride(shCoeffs, shStore);
   shRest.ensure(std::max<size_t>(rest * (shStore == ShStore::F32 ? 4 : 2), 4));
   SB_CUDA(cudaMemset(shDc.get(), 0, shDc.bytes()));
   SB_CUDA(cudaMemset(shRest.get(), 0, shRest.bytes()));
@@ -446,6 +446,7 @@ Params Trainer::params() const {
   p.shStore = shStore;
   p.n = n;
   p.planeStride = planeStride;
+  p.restStride = sh_rest_stride(shCoeffs, shStore);
   p.shDegree = shDegree;
   p.shCoeffs = shCoeffs;
   return p;
@@ -1116,10 +1117,10 @@ void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *state
   const uint32_t oldN = n, oldStride = planeStride;
   const size_t nn = newN;
   const uint32_t newStride = (uint32_t)(((nn + kPlaneAlign - 1) / kPlaneAlign) * kPlaneAlign);
-  const size_t restPlanes = 3 * (size_t)(shCoeffs - 1);
   const size_t copies = stateStore == StateStore::F32 ? 2 : 1;
+  const uint32_t rowStride = sh_rest_stride(shCoeffs, shStore), rowWords = rowStride * (shStore == ShStore::F32 ? 4u : 2u) / 4u;
   const size_t paramBytes[6] = {nn * 12, nn * 12, nn * 16, nn * 4, (size_t)newStride * 12,
-                                std::max<size_t>(restPlanes * newStride * (shStore == ShStore::F32 ? 4 : 2), 4)};
+                                std::max<size_t>((size_t)newStride * rowWords * 4, 4)};
   const size_t stateBytes[5] = {nn * 12 * copies, nn * 12 * copies, nn * 16 * copies, nn * 4 * copies,
                                 (size_t)newStride * 12 * shCoeffs * copies};
   for (int g = 0; g < 6; ++g) grow(spareParams[g], paramBytes[g]);
@@ -1133,12 +1134,9 @@ void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *state
     for (int g = 0; g < 4; ++g)
       launch_gather_rows(paramSource, params[g]->get<uint32_t>(), spareParams[g].get<uint32_t>(), newN, oldN, strides[g], 1u, stream);
     launch_gather_planes(paramSource, shDc.get<uint32_t>(), spareParams[4].get<uint32_t>(), newN, newStride, oldStride, 3u, stream);
-    if (shStore == ShStore::F32)
-      launch_gather_planes(paramSource, shRest.get<uint32_t>(), spareParams[5].get<uint32_t>(), newN, newStride, oldStride,
-                           (uint32_t)restPlanes, stream);
-    else
-      launch_gather_planes16(paramSource, shRest.get<uint16_t>(), spareParams[5].get<uint16_t>(), newN, newStride, oldStride,
-                             (uint32_t)restPlanes, stream);
+    // The rows of higher coefficients, as words (a row is a whole number of 16-byte units).
+    launch_gather_rows(paramSource, shRest.get<uint32_t>(), spareParams[5].get<uint32_t>(), newStride, oldStride, rowWords, 1u,
+                       stream, newN);
   }
   for (int g = 0; g < 4; ++g)
     launch_gather_rows(stateSource, state[g].get<uint32_t>(), spareState[g].get<uint32_t>(), newN, oldN, strides[g],
@@ -1648,7 +1646,7 @@ int splat_trainer_get_cloud(splat_trainer *trainer, float *positions, float *sca
       SB_CUDA(cudaMemcpy(dc.data(), t->shDc.get(), ps * 12, cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < n; ++i)
         for (int c = 0; c < 3; ++c) sh[i * floats + c] = dc[c * ps + i];
-      const size_t rest = ps * 3 * (t->shCoeffs - 1);
+      const size_t rowStride = sh_rest_stride(t->shCoeffs, t->shStore), rest = ps * rowStride;
       if (rest > 0) {
         std::vector<float> planes(rest);
         if (t->shStore == sb::ShStore::F32) {
@@ -1666,7 +1664,7 @@ int splat_trainer_get_cloud(splat_trainer *trainer, float *positions, float *sca
           }
         }
         for (size_t i = 0; i < n; ++i)
-          for (int j = 3; j < floats; ++j) sh[i * floats + j] = planes[(size_t)(j - 3) * ps + i];
+          for (int j = 3; j < floats; ++j) sh[i * floats + j] = planes[i * rowStride + (size_t)(j - 3)];
       }
     }
   });
@@ -2215,7 +2213,8 @@ void densify_gaussians(splat_trainer *handle, const splat_densify_options &o, st
     const uint32_t restPlanes = 3u * (uint32_t)(fresh->shCoeffs - 1);
     sb::launch_densify_patch(fresh->editRows.get<sb::DensifyPatch>(), (uint32_t)rowsOut.size(), fresh->positions.get<float>(),
                              fresh->scales.get<float>(), fresh->rotations.get<float>(), fresh->opacities.get<float>(),
-                             fresh->shRest.get(), restPlanes, fresh->planeStride, fresh->shStore == sb::ShStore::F32 ? 4u : 2u,
+                             fresh->shRest.get(), restPlanes, sb::sh_rest_stride(fresh->shCoeffs, fresh->shStore),
+                             fresh->shStore == sb::ShStore::F32 ? 4u : 2u,
                              fresh->stream);
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaStreamSynchronize(fresh->stream));
