@@ -527,7 +527,8 @@ def measured_traffic(stage: str, form: str):
 
 def chosen_options(splat):
     return splat.TrainerOptions(sh_storage=splat.SH_BF16, state_storage=splat.STATE_BF16_PAIR,
-                                sort_form=splat.SORT_TILE_DEPTH_64, exact_math=False, use_graph=True, digit_bits=8)
+                                sort_form=splat.SORT_TILE_DEPTH_64, exact_math=False, use_graph=True, digit_bits=8,
+                                forward_pixels_per_thread=2, backward_pixels_per_thread=2)
 
 
 def plain_options(splat):
