@@ -519,7 +519,7 @@ int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint6
  * blend_lists only, else empty), 14-18 the Adam state of parameter groups 0-4
  * (positions, scales, rotations, opacities, SH; u32 words: BF16 pairs, or FP32
  * m values then v values; SH state in rows of 3 (degree + 1)^2 words per
- * Gaussian, the row count rounded up to 128). Copies min(bytes, size) bytes; *size gets the
+ * Gaussian rounded up to a multiple of 4, the row count rounded up to 128). Copies min(bytes, size) bytes; *size gets the
  * buffer's size in bytes. */
 int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size);
 

@@ -186,16 +186,20 @@ static void splat_tiles(const float *s, int gridW, int gridH, uint32_t t[4]) {
 
 static int splat_reaches_tile(const float *s, float reach, uint32_t tx, uint32_t ty) {
   const float qx = s[0], qy = s[1], qz = s[2];
+  /* The tangent points as products by the conic's diagonal reciprocals (the
+   * GLSL division is not correctly rounded either; the kernels take one
+   * correctly rounded reciprocal per splat). */
+  const float iqx = 1.0f / qx, iqz = 1.0f / qz;
   const float lowX = ((float)tx * 16.0f + 0.5f) - s[8], lowY = ((float)ty * 16.0f + 0.5f) - s[9];
   const float highX = lowX + 15.0f, highY = lowY + 15.0f;
   if (lowX <= 0.0f && lowY <= 0.0f && highX >= 0.0f && highY >= 0.0f) return 1;
   float least = 1e30f;
   for (int side = 0; side < 2; ++side) {
     const float x = side == 0 ? lowX : highX;
-    const float y = clampf(-qy * x / qz, lowY, highY);
+    const float y = clampf((-qy * x) * iqz, lowY, highY);
     least = fminf(least, qx * x * x + 2.0f * qy * x * y + qz * y * y);
     const float vv = side == 0 ? lowY : highY;
-    const float u = clampf(-qy * vv / qx, lowX, highX);
+    const float u = clampf((-qy * vv) * iqx, lowX, highX);
     least = fminf(least, qx * u * u + 2.0f * qy * u * vv + qz * vv * vv);
   }
   return least <= reach * 1.001f + 1e-3f;

@@ -628,8 +628,9 @@ def test_apply_changes_gathers_the_state(splat, oracle, state):
         n = new[g][: copies * new_n * stride].reshape(copies, new_n, stride)
         np.testing.assert_array_equal(n[:, kept], o[:, source[kept]])
         assert not n[:, ~kept].any()
-    # The SH state: rows of 27 words (degree 2), row counts rounded up to 128.
-    width = 3 * 9
+    # The SH state: rows of 28 words (27 at degree 2, padded to 16 bytes), row
+    # counts rounded up to 128.
+    width = 28
     old_rows, new_rows = 512, ((new_n + 127) // 128) * 128
     o = old[4][: copies * old_rows * width].reshape(copies, old_rows, width)
     n = new[4][: copies * new_rows * width].reshape(copies, new_rows, width)
@@ -799,9 +800,10 @@ def test_pruning_keeps_the_references_survivors_and_their_state(splat, oracle, k
     for g, width in enumerate((3, 3, 4, 1)):
         new = trainer.debug_download(splat.DEBUG_STATE + g, np.uint32).reshape(len(source), width)
         np.testing.assert_array_equal(new, states[g].reshape(300, width)[source], f"state group {g}")
-    # SH state: a row of 27 words per Gaussian (degree 2), row counts rounded up to 128.
-    new_sh = trainer.debug_download(splat.DEBUG_STATE + 4, np.uint32).reshape(256, 27)[: len(source)]
-    old_sh = states[4].reshape(384, 27)[source]
+    # SH state: a row of 28 words per Gaussian (27 at degree 2, padded to 16
+    # bytes), row counts rounded up to 128.
+    new_sh = trainer.debug_download(splat.DEBUG_STATE + 4, np.uint32).reshape(256, 28)[: len(source)]
+    old_sh = states[4].reshape(384, 28)[source]
     np.testing.assert_array_equal(new_sh, old_sh, "SH state")
     assert np.all(trainer.densify_stats().contribution == 0.0)
     assert math.isfinite(trainer.step(to_camera(view), target, splat.LearningRates()).loss)

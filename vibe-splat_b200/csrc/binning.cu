@@ -49,21 +49,29 @@ struct RowTangents {
   float lowY, highY, uLow, uHigh; // edge offsets from the centre and their unclamped tangent x
 };
 
-__device__ __forceinline__ ColTangents col_tangents(const float4 q, const float4 ce, uint32_t tx, float T) {
+// The conic's diagonal reciprocals, correctly rounded: the tangent points are
+// products by them (the reference's GLSL division is not correctly rounded
+// either), one reciprocal per splat instead of four divisions per tile.
+struct TangentScales {
+  float invX, invZ;
+};
+__device__ __forceinline__ TangentScales tangent_scales(const float4 q) { return {__frcp_rn(q.x), __frcp_rn(q.z)}; }
+
+__device__ __forceinline__ ColTangents col_tangents(const float4 q, const TangentScales k, const float4 ce, uint32_t tx, float T) {
   ColTangents c;
   c.lowX = ((float)tx * T + 0.5f) - ce.x;
   c.highX = c.lowX + (T - 1.0f);
-  c.yLow = -q.y * c.lowX / q.z;
-  c.yHigh = -q.y * c.highX / q.z;
+  c.yLow = (-q.y * c.lowX) * k.invZ;
+  c.yHigh = (-q.y * c.highX) * k.invZ;
   return c;
 }
 
-__device__ __forceinline__ RowTangents row_tangents(const float4 q, const float4 ce, uint32_t ty, float T) {
+__device__ __forceinline__ RowTangents row_tangents(const float4 q, const TangentScales k, const float4 ce, uint32_t ty, float T) {
   RowTangents r;
   r.lowY = ((float)ty * T + 0.5f) - ce.y;
   r.highY = r.lowY + (T - 1.0f);
-  r.uLow = -q.y * r.lowY / q.x;
-  r.uHigh = -q.y * r.highY / q.x;
+  r.uLow = (-q.y * r.lowY) * k.invX;
+  r.uHigh = (-q.y * r.highY) * k.invX;
   return r;
 }
 
@@ -100,8 +108,9 @@ __device__ __forceinline__ bool fill_tables(const float4 q, const float4 ce, con
                                             RowTangents *rows, float T) {
   const uint32_t width = t.x1 - t.x0 + 1u, height = t.y1 - t.y0 + 1u;
   if (width > kTableMax || height > kTableMax) return false;
-  for (uint32_t c = lane; c < width; c += 32u) cols[c] = col_tangents(q, ce, t.x0 + c, T);
-  for (uint32_t r = lane; r < height; r += 32u) rows[r] = row_tangents(q, ce, t.y0 + r, T);
+  const TangentScales k = tangent_scales(q);
+  for (uint32_t c = lane; c < width; c += 32u) cols[c] = col_tangents(q, k, ce, t.x0 + c, T);
+  for (uint32_t r = lane; r < height; r += 32u) rows[r] = row_tangents(q, k, ce, t.y0 + r, T);
   __syncwarp();
   return true;
 }
@@ -121,8 +130,9 @@ __device__ __forceinline__ uint32_t warp_reach(const float4 q, const float4 ce, 
     const uint32_t c = li - r * width;
     x = t.x0 + c;
     y = t.y0 + r;
+    const TangentScales k = tangent_scales(q);
     hit = cols != nullptr ? reaches_tile(q, reach, cols[c], rows[r])
-                          : reaches_tile(q, reach, col_tangents(q, ce, x, T), row_tangents(q, ce, y, T));
+                          : reaches_tile(q, reach, col_tangents(q, k, ce, x, T), row_tangents(q, k, ce, y, T));
   }
   return __ballot_sync(0xFFFFFFFFu, hit);
 }
@@ -193,6 +203,7 @@ __global__ void __launch_bounds__(kCountThreads)
     const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31), excl = incl - own;
     const uint32_t width = rect.x1 - rect.x0 + 1u;
     const float invWidth = 1.0f / (float)width;
+    const TangentScales ks = valid ? tangent_scales(cq) : TangentScales{0.f, 0.f};
     s_mask[warp][lane] = 0u;
     __syncwarp();
     for (uint32_t base = 0; base < total; base += 32u) {
@@ -209,9 +220,10 @@ __global__ void __launch_bounds__(kCountThreads)
       const uint32_t ox0 = __shfl_sync(0xFFFFFFFFu, rect.x0, owner), oy0 = __shfl_sync(0xFFFFFFFFu, rect.y0, owner);
       const uint32_t ow = __shfl_sync(0xFFFFFFFFu, width, owner);
       const float oinv = __shfl_sync(0xFFFFFFFFu, invWidth, owner);
+      const TangentScales ok = {__shfl_sync(0xFFFFFFFFu, ks.invX, owner), __shfl_sync(0xFFFFFFFFu, ks.invZ, owner)};
       if (f < total) {
         const uint32_t row = (uint32_t)(((float)li + 0.5f) * oinv), col = li - row * ow;
-        if (reaches_tile(oq, orc, col_tangents(oq, oce, ox0 + col, T), row_tangents(oq, oce, oy0 + row, T)))
+        if (reaches_tile(oq, orc, col_tangents(oq, ok, oce, ox0 + col, T), row_tangents(oq, ok, oce, oy0 + row, T)))
           atomicOr(&s_mask[warp][owner], 1u << li);
       }
     }

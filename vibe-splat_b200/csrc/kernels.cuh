@@ -40,6 +40,9 @@ enum class StateStore : int { F32 = 0, BF16Pair = 1 };
 // copies). The SH Adam state is in rows too (sh_state_at).
 constexpr uint32_t kPlaneAlign = 128;
 
+// Words in a Gaussian's row of SH Adam state: 3 coeffs, rounded up to 16 bytes.
+__host__ __device__ inline uint32_t sh_state_stride(int shCoeffs) { return (3u * (uint32_t)shCoeffs + 3u) & ~3u; }
+
 // Elements in a Gaussian's row of higher SH coefficients.
 inline uint32_t sh_rest_stride(int shCoeffs, ShStore store) {
   const uint32_t elements = 3u * (uint32_t)(shCoeffs - 1), bytes = store == ShStore::F32 ? 4u : 2u;

@@ -75,11 +75,11 @@ __device__ __forceinline__ float sqrt_sfu(float x) {
 }
 
 // The SH Adam state lies in rows: element e (= 3 k + c) of Gaussian i at word
-// i S + e, S = 3 (degree + 1)^2 words per Gaussian, the row count rounded up
-// to a multiple of 128 (kPlaneAlign); F32 state keeps its v rows after the m
-// rows, planeStride S words later. A Gaussian's state is one contiguous
-// run, which a step touching a few Gaussians here and there reads and writes
-// in whole sectors.
+// i S + e, S = sh_state_stride (3 (degree + 1)^2 words rounded up to 16
+// bytes), the row count rounded up to a multiple of 128 (kPlaneAlign); F32
+// state keeps its v rows after the m rows, planeStride S words later. A
+// Gaussian's state is one contiguous, 16-byte aligned run, which a step
+// touching a few Gaussians here and there reads and writes in whole sectors.
 __host__ __device__ __forceinline__ size_t sh_state_at(uint32_t i, uint32_t e, uint32_t S) { return (size_t)i * S + e; }
 
 // Adam on one parameter (step_parameter with radius < 0): the bias
@@ -537,7 +537,8 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
   const bool stepZeros = !args.selective;
   if (!touched && !stepZeros) return;
   const AdamArgs a = adam_args(args);
-  const size_t ps = p.planeStride, count = ps * shFloats;
+  const uint32_t stateStride = sh_state_stride(p.shCoeffs);
+  const size_t ps = p.planeStride, count = ps * stateStride;
   // Every load first, then the arithmetic, then the stores: the values and the
   // state are reached through plain pointers, so a load placed after a store
   // could not be moved before it, and the 12 updates would run one by one.
@@ -551,7 +552,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
       value[kk][c] = m[kk][c] = vv[kk][c] = 0.0f;
       word[kk][c] = 0u;
       if (k >= p.shCoeffs) continue;
-      const size_t t = (size_t)(k * 3 + c) * ps + i, ts = sh_state_at(i, (uint32_t)(k * 3 + c), shFloats);
+      const size_t t = (size_t)(k * 3 + c) * ps + i, ts = sh_state_at(i, (uint32_t)(k * 3 + c), stateStride);
       value[kk][c] = k == 0 ? p.shDc[t] : load_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride));
       if (state.store == StateStore::F32) {
         m[kk][c] = static_cast<const float *>(state.state[4])[ts];
@@ -572,7 +573,7 @@ __global__ void __launch_bounds__(256) k_sh_step(Params p, const ViewSet *__rest
     for (int c = 0; c < 3; ++c) {
       if (g[kk][c] == 0.0f && !stepZeros) continue;
       const uint32_t plane = (uint32_t)(k * 3 + c);
-      const size_t t = (size_t)plane * ps + i, ts = sh_state_at(i, plane, shFloats);
+      const size_t t = (size_t)plane * ps + i, ts = sh_state_at(i, plane, stateStride);
       const uint32_t hashIndex = (i * (uint32_t)shFloats + plane) * 5u + 4u;
       adam(value[kk][c], m[kk][c], vv[kk][c], g[kk][c], rate, a);
       if (state.store == StateStore::F32) {
@@ -631,8 +632,8 @@ __device__ __forceinline__ void store_state(void *st, StateStore store, uint32_t
 // Shared-memory bytes of a block's staged SH: the DC planes, the rows of
 // higher coefficients (restStride elements each) and the state rows.
 __host__ __device__ inline uint32_t step_stage_bytes(int coeffs, int shBytes, bool stateF32, uint32_t restStride) {
-  const uint32_t planes = 3u * (uint32_t)coeffs;
-  return 3u * kStepThreads * 4u + restStride * kStepThreads * (uint32_t)shBytes + (stateF32 ? 2u : 1u) * planes * kStepThreads * 4u;
+  return 3u * kStepThreads * 4u + restStride * kStepThreads * (uint32_t)shBytes +
+         (stateF32 ? 2u : 1u) * sh_state_stride(coeffs) * kStepThreads * 4u;
 }
 
 template <ShStore S> __device__ __forceinline__ float staged_sh_rest(const unsigned char *rest, uint32_t at) {
@@ -680,9 +681,10 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
       } else {
         // The block's state rows, one copy (F32: the m rows, then the v rows).
         const uint32_t q = c - 3u - rest;
-        bulk_load(s_state + q * kStepThreads * planes * 4u,
-                  static_cast<const unsigned char *>(state.state[4]) + ((size_t)q * ps + i0) * planes * 4u,
-                  kStepThreads * planes * 4u, &s_bar);
+        const uint32_t stride = sh_state_stride(p.shCoeffs);
+        bulk_load(s_state + q * kStepThreads * stride * 4u,
+                  static_cast<const unsigned char *>(state.state[4]) + ((size_t)q * ps + i0) * stride * 4u,
+                  kStepThreads * stride * 4u, &s_bar);
       }
     }
   }
@@ -812,16 +814,17 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
   if (!(touched || stepZeros)) return;
   const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
   const uint32_t hashBase = i * shFloats * 5u + 4u;
-  // The staged rows: this thread's row at tid * planes (F32: the v rows after
-  // the block's m rows).
-  const float *s_statef = reinterpret_cast<const float *>(s_state) + (size_t)tid * planes;
+  // The staged rows: this thread's row at tid * stateStride (F32: the v rows
+  // after the block's m rows).
+  const uint32_t stateStride = sh_state_stride(p.shCoeffs);
+  const float *s_statef = reinterpret_cast<const float *>(s_state) + (size_t)tid * stateStride;
   const uint32_t *s_statew = reinterpret_cast<const uint32_t *>(s_statef);
-  uint32_t *stateOut = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, shFloats);
-  const size_t stateCount = (size_t)ps * shFloats; // F32: the v rows follow the m rows
+  uint32_t *stateOut = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, stateStride);
+  const size_t stateCount = (size_t)ps * stateStride; // F32: the v rows follow the m rows
   // One element: Adam from the staged state, the new state and value returned.
   auto element = [&](uint32_t plane, float &val, float g, float rate) {
     if constexpr (ST == StateStore::F32) {
-      float m = s_statef[plane], v = s_statef[(size_t)kStepThreads * planes + plane];
+      float m = s_statef[plane], v = s_statef[(size_t)kStepThreads * stateStride + plane];
       adam(val, m, v, g, rate, a);
       reinterpret_cast<float *>(stateOut)[plane] = m;
       reinterpret_cast<float *>(stateOut)[stateCount + plane] = v;
@@ -882,7 +885,38 @@ template <bool FIXED> __device__ __forceinline__ uint32_t reached_bits(const voi
   return ((a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) & keep) | ((c.x | c.y | c.z | c.w) & keep) | ((d.x | d.y) & keep);
 }
 
-// The one-view selective step of a reached Gaussian. Its SH coefficients and
+// A Gaussian's row of higher SH coefficients in registers: up to 48 elements
+// (degree 3) in 16-byte pieces. get() reads element e; set() writes it as
+// the store of the SH step does (stochastic rounding to 16-bit types, the
+// reference's rule, with the element's hash index).
+template <ShStore S> struct ShRow {
+  static constexpr uint32_t kBytes = S == ShStore::F32 ? 4u : 2u;
+  static constexpr int kPieces = (int)(48u * kBytes / 16u);
+  uint4 piece[kPieces];
+  __device__ __forceinline__ uint32_t &word(int w) { return reinterpret_cast<uint32_t *>(piece)[w]; }
+  __device__ __forceinline__ float get(int e) {
+    if constexpr (S == ShStore::F32) {
+      return __uint_as_float(word(e));
+    } else {
+      const uint32_t half = (e & 1) != 0 ? word(e >> 1) >> 16 : word(e >> 1) & 0xFFFFu;
+      if constexpr (S == ShStore::BF16) return __uint_as_float(half << 16);
+      else return __half2float(__ushort_as_half((unsigned short)half));
+    }
+  }
+  __device__ __forceinline__ void set(int e, float value, uint32_t hashIndex, uint32_t seed) {
+    if constexpr (S == ShStore::F32) {
+      word(e) = __float_as_uint(value);
+    } else {
+      uint32_t bits;
+      if constexpr (S == ShStore::BF16) bits = bf16_stochastic(value, hashIndex, seed ^ 0x5DEECE66u) & 0xFFFFu;
+      else bits = __half_as_ushort(half_stochastic(value, hashIndex, seed ^ 0x5DEECE66u));
+      uint32_t &w = word(e >> 1);
+      w = (e & 1) != 0 ? (w & 0x0000FFFFu) | (bits << 16) : (w & 0xFFFF0000u) | bits;
+    }
+  }
+};
+
+// The one-view selective step of a reached Gaussian.// The one-view selective step of a reached Gaussian. Its SH coefficients and
 // SH Adam state are reached through scattered words (the coefficients in
 // planes, the state in its row), so every load of a coefficient is issued up
 // front (predicated on the coefficient being in use, no branch between them)
@@ -912,15 +946,17 @@ __device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const 
       words[q * 4 + 3] = w4.w;
     }
   }
-  // The coefficients in use, all loads in flight together.
-  float dc[3], rest[kMaxCoeffs - 1][3];
+  // The coefficients: the DC planes and the Gaussian's row of the rest, the
+  // row moved in 16-byte pieces (kept in registers for the step, written back
+  // whole).
+  float dc[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) dc[c] = active > 0 ? p.shDc[(size_t)c * ps + i] : 0.0f;
+  ShRow<S> row;
+  uint4 *rowAt = reinterpret_cast<uint4 *>(static_cast<unsigned char *>(p.shRest) + (size_t)i * p.restStride * ShRow<S>::kBytes);
+  const uint32_t pieces = active > 1 ? p.restStride * ShRow<S>::kBytes / 16u : 0u;
 #pragma unroll
-  for (int k = 1; k < kMaxCoeffs; ++k)
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      rest[k - 1][c] = k < active ? load_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride)) : 0.0f;
+  for (int q = 0; q < ShRow<S>::kPieces; ++q) row.piece[q] = (uint32_t)q < pieces ? rowAt[q] : make_uint4(0u, 0u, 0u, 0u);
   float raw[kRawPerSplat];
 #pragma unroll
   for (int k = 0; k < kRawPerSplat; ++k) raw[k] = FIXED ? (float)(int)words[k] / cam.fixedScale : __uint_as_float(words[k]);
@@ -945,8 +981,12 @@ __device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const 
   if (cam.activeDegree > 0) {
     float gDir[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-    for (int k = 1; k < kMaxCoeffs; ++k)
-      if (k < active) direction_term(k, rest[k - 1], gColour, dir, gDir);
+    for (int k = 1; k < kMaxCoeffs; ++k) {
+      if (k < active) {
+        const float value[3] = {row.get((k - 1) * 3), row.get((k - 1) * 3 + 1), row.get((k - 1) * 3 + 2)};
+        direction_term(k, value, gColour, dir, gDir);
+      }
+    }
     add_direction_term(gDir, dir, distance, gPv);
   }
 #pragma unroll
@@ -985,60 +1025,78 @@ __device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const 
     }
   }
 
-  // The SH step: only the coefficients in use have a gradient. The state
-  // words of kStateBatch coefficients are loaded together, then stepped.
+  // The SH step: only the coefficients in use have a gradient. The state row
+  // goes in batches of 16 words (16-byte loads and stores); each element in
+  // use is stepped in the reference's order, the values in the row kept in
+  // registers, and the batch and then the row are written back whole.
   const uint32_t shFloats = 3u * (uint32_t)p.shCoeffs;
   const uint32_t hashBase = i * shFloats * 5u + 4u;
-  uint32_t *stateWords = static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, shFloats);
-  const size_t stateCount = (size_t)ps * shFloats; // F32: the v rows follow the m rows
+  const uint32_t stateStride = sh_state_stride(p.shCoeffs);
+  uint4 *stateRow = reinterpret_cast<uint4 *>(static_cast<uint32_t *>(state.state[4]) + sh_state_at(i, 0u, stateStride));
+  const size_t vRows = (size_t)ps * stateStride / 4u; // F32: the v rows, in 16-byte pieces, after the m rows
   const float restRate = args.rates[4] * args.restScale;
+  float basis[kMaxCoeffs];
 #pragma unroll
-  for (int k0 = 0; k0 < kMaxCoeffs; k0 += kStateBatch) {
-    float m[kStateBatch][3], v[kStateBatch][3];
+  for (int k = 0; k < kMaxCoeffs; ++k) basis[k] = k < active ? basis_one(k, dir[0], dir[1], dir[2]) : 0.0f;
+  const uint32_t inUse = 3u * (uint32_t)active;
+  bool dcChanged[3] = {false, false, false};
 #pragma unroll
-    for (int b = 0; b < kStateBatch; ++b)
+  for (int b = 0; b < 3; ++b) {
+    if ((uint32_t)b * 16u >= inUse) break;
+    // Pieces past the row's end (a lower degree) are not touched.
+    const uint32_t rowPieces = stateStride / 4u;
+    uint4 m4[4], v4[4];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int k = k0 + b;
-        const size_t at = (size_t)(3 * k + c);
-        m[b][c] = v[b][c] = 0.0f;
-        if (k < active) {
-          if constexpr (ST == StateStore::F32) {
-            m[b][c] = reinterpret_cast<const float *>(stateWords)[at];
-            v[b][c] = reinterpret_cast<const float *>(stateWords)[stateCount + at];
-          } else {
-            const uint32_t w = stateWords[at];
-            m[b][c] = bf16_load(w, 0);
-            v[b][c] = bf16_load(w, 1);
-          }
-        }
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t at = (uint32_t)b * 4u + (uint32_t)q;
+      m4[q] = at < rowPieces ? stateRow[at] : make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (ST == StateStore::F32) v4[q] = at < rowPieces ? stateRow[vRows + at] : make_uint4(0u, 0u, 0u, 0u);
+    }
+    uint32_t *mw = reinterpret_cast<uint32_t *>(m4), *vw = reinterpret_cast<uint32_t *>(v4);
+#pragma unroll
+    for (int w = 0; w < 16; ++w) {
+      const int e = b * 16 + w, k = e / 3, c = e % 3;
+      if (k >= kMaxCoeffs || (uint32_t)e >= inUse) continue;
+      const float g = fmaf(basis[k], gColour[c], 0.0f);
+      if (g == 0.0f) continue;
+      float val = k == 0 ? dc[c] : row.get(e - 3);
+      float m, v;
+      if constexpr (ST == StateStore::F32) {
+        m = __uint_as_float(mw[w]);
+        v = __uint_as_float(vw[w]);
+      } else {
+        m = bf16_load(mw[w], 0);
+        v = bf16_load(mw[w], 1);
       }
+      adam(val, m, v, g, k == 0 ? args.rates[4] : restRate, a);
+      if constexpr (ST == StateStore::F32) {
+        mw[w] = __float_as_uint(m);
+        vw[w] = __float_as_uint(v);
+      } else {
+        mw[w] = bf16_pair(m, v, hashBase + (uint32_t)e * 5u, a.seed);
+      }
+      if (k == 0) {
+        dc[c] = val;
+        dcChanged[c] = true;
+      } else {
+        row.set(e - 3, val, hashBase + (uint32_t)e * 5u, args.seed);
+      }
+    }
 #pragma unroll
-    for (int b = 0; b < kStateBatch; ++b) {
-      const int k = k0 + b;
-      if (k >= active) continue;
-      const float basis = basis_one(k, dir[0], dir[1], dir[2]);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float g = fmaf(basis, gColour[c], 0.0f);
-        if (g == 0.0f) continue;
-        const uint32_t plane = (uint32_t)(3 * k + c);
-        const size_t at = plane;
-        float val = k == 0 ? dc[c] : rest[k > 0 ? k - 1 : 0][c];
-        float mm = m[b][c], vvv = v[b][c];
-        adam(val, mm, vvv, g, k == 0 ? args.rates[4] : restRate, a);
-        if constexpr (ST == StateStore::F32) {
-          reinterpret_cast<float *>(stateWords)[at] = mm;
-          reinterpret_cast<float *>(stateWords)[stateCount + at] = vvv;
-        } else {
-          stateWords[at] = bf16_pair(mm, vvv, hashBase + plane * 5u, a.seed);
-        }
-        if (k == 0) p.shDc[(size_t)c * ps + i] = val;
-        else store_sh_rest<S>(p.shRest, sh_rest_at(i, (uint32_t)((k - 1) * 3 + c), p.restStride), val, hashBase + plane * 5u,
-                              args.seed);
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t at = (uint32_t)b * 4u + (uint32_t)q;
+      if (at < rowPieces) {
+        stateRow[at] = m4[q];
+        if constexpr (ST == StateStore::F32) stateRow[vRows + at] = v4[q];
       }
     }
   }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    if (dcChanged[c]) p.shDc[(size_t)c * ps + i] = dc[c];
+#pragma unroll
+  for (int q = 0; q < ShRow<S>::kPieces; ++q)
+    if ((uint32_t)q < pieces) rowAt[q] = row.piece[q];
 }
 
 template <ShStore S, StateStore ST, bool FIXED>

@@ -391,7 +391,7 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
     DeviceBuffer *to[6] = {&positions, &scales, &rotations, &opacities, &shDc, &shRest};
     upload_cloud(cloud, shCoeffs, shStore, planeStride, to);
   }
-  const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, ps * 3 * shCoeffs};
+  const size_t groupCounts[5] = {nn * 3, nn * 3, nn * 4, nn, ps * sh_state_stride(shCoeffs)};
   for (int g = 0; g < 5; ++g) {
     const size_t bytes = groupCounts[g] * (stateStore == StateStore::F32 ? 8 : 4);
     state[g].ensure(bytes);
@@ -1122,7 +1122,7 @@ void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *state
   const size_t paramBytes[6] = {nn * 12, nn * 12, nn * 16, nn * 4, (size_t)newStride * 12,
                                 std::max<size_t>((size_t)newStride * rowWords * 4, 4)};
   const size_t stateBytes[5] = {nn * 12 * copies, nn * 12 * copies, nn * 16 * copies, nn * 4 * copies,
-                                (size_t)newStride * 12 * shCoeffs * copies};
+                                (size_t)newStride * sh_state_stride(shCoeffs) * 4 * copies};
   for (int g = 0; g < 6; ++g) grow(spareParams[g], paramBytes[g]);
   for (int g = 0; g < 5; ++g) grow(spareState[g], stateBytes[g]);
   const uint32_t strides[4] = {3, 3, 4, 1};
@@ -1144,7 +1144,7 @@ void Trainer::replace_gaussians(const int32_t *paramSource, const int32_t *state
   // The SH state rows: the row counts are the plane strides, the rows from
   // newN on padding.
   launch_gather_rows(stateSource, state[4].get<uint32_t>(), spareState[4].get<uint32_t>(), newStride, oldStride,
-                     (uint32_t)(3 * shCoeffs), (uint32_t)copies, stream, newN);
+                     sh_state_stride(shCoeffs), (uint32_t)copies, stream, newN);
   SB_CUDA(cudaGetLastError());
   SB_CUDA(cudaStreamSynchronize(stream));
   for (int g = 0; g < 4; ++g) swap(*params[g], spareParams[g]);
@@ -2648,7 +2648,7 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     case 13: src = t->listCounts.get(); have = t->blendLists ? (size_t)t->views.totalPixels * 4 : 0; break;
     case 14: case 15: case 16: case 17: case 18: {
       const size_t g = t->n;
-      const size_t counts[5] = {g * 3, g * 3, g * 4, g, (size_t)t->planeStride * 3 * t->shCoeffs};
+      const size_t counts[5] = {g * 3, g * 3, g * 4, g, (size_t)t->planeStride * sb::sh_state_stride(t->shCoeffs)};
       src = t->state[which - 14].get();
       have = counts[which - 14] * (t->stateStore == sb::StateStore::F32 ? 8 : 4);
       break;
