@@ -165,7 +165,10 @@ __global__ void __launch_bounds__(kCountThreads)
   __shared__ RowTangents s_rows[kCountThreads / 32][kTableMax];
   __shared__ uint32_t s_mask[kCountThreads / 32][32];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t r = blockIdx.x * kCountThreads + threadIdx.x;
+  // A grid smaller than the items (the count beside the depth sort) walks
+  // them in chunks of a block's width, leaving SM slots to the sort's passes.
+  for (uint32_t chunk = blockIdx.x; chunk * kCountThreads < items; chunk += gridDim.x) {
+  const uint32_t r = chunk * kCountThreads + threadIdx.x;
   // Whole warps stay to the end: the loops below are warp-wide. Without item
   // keys (the count beside the depth sort, which permutes them), a culled
   // splat is the one whose reach the projection left at minus infinity.
@@ -259,6 +262,8 @@ __global__ void __launch_bounds__(kCountThreads)
   if (r < items) {
     counts[r] = count;
     masks[r] = mask;
+  }
+  __syncwarp(); // the warp's tables and masks are reused by its next chunk
   }
 }
 
@@ -514,10 +519,17 @@ size_t bin_scan_scratch_bytes(uint32_t items) {
 
 void launch_bin_count(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat, uint32_t items,
                       uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *counts, uint32_t *masks, uint32_t *counters,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, uint32_t blocksPerSm) {
   if (items == 0) return;
-  launch_chained(k_bin_count, dim3(div_up(items, kCountThreads)), dim3(kCountThreads), 0, stream, splats, reach, itemKeys, itemSplat,
-                 items, n, dViews, counts, masks, counters);
+  uint32_t grid = div_up(items, kCountThreads);
+  if (blocksPerSm > 0) {
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    grid = std::min(grid, (uint32_t)std::max(sms, 1) * blocksPerSm);
+  }
+  launch_chained(k_bin_count, dim3(grid), dim3(kCountThreads), 0, stream, splats, reach, itemKeys, itemSplat, items, n, dViews,
+                 counts, masks, counters);
 }
 
 void launch_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *gather, uint32_t *offsets, uint32_t *counters,

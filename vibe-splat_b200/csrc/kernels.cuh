@@ -90,7 +90,8 @@ size_t bin_scan_scratch_bytes(uint32_t items);
 // counters[1], counters[2] and the overflow bit as above.
 void launch_bin_count(const Splat *splats, const float *reach, const uint32_t *itemKeys, const uint32_t *itemSplat, uint32_t items,
                       uint32_t n, const ViewSet &views, const ViewSet *dViews, uint32_t *counts, uint32_t *masks, uint32_t *counters,
-                      cudaStream_t stream);
+                      cudaStream_t stream,
+                      uint32_t blocksPerSm = 0);
 // clearScratch false: the caller cleared scratch (bin_scan_scratch_bytes) already.
 void launch_offsets_scan(uint32_t items, const uint32_t *counts, const uint32_t *gather, uint32_t *offsets, uint32_t *counters,
                          uint32_t capacity, void *scratch, uint32_t *error, cudaStream_t stream, bool clearScratch = true);

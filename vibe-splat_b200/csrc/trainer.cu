@@ -788,8 +788,10 @@ void Trainer::record_prepare(bool backward) {
     SB_CUDA(cudaStreamWaitEvent(side, countForkEvent, 0));
     SB_CUDA(cudaMemsetAsync(scanScratch.get(), 0, bin_scan_scratch_bytes(items), side));
     // No keys: the depth sort permutes them in place meanwhile.
+    // Two blocks per SM walk the splats: the sort's passes (one to two
+    // blocks per SM each) keep room beside them.
     launch_bin_count(splats.get<Splat>(), reach.get<float>(), nullptr, nullptr, n, n, views, dViews.get<ViewSet>(),
-                     countsBySplat, masks, counters, side);
+                     countsBySplat, masks, counters, side, 2u);
     SB_CUDA(cudaEventRecord(countEvent, side));
   }
   SB_CUDA(cudaStreamWaitEvent(stream, joinEvent, 0));
