@@ -468,11 +468,14 @@ def bench_config() -> dict:
 # ----------------------------------------------------------------- our arm
 
 
-def stage_bytes(n: int, visible: int, entries: int, pixels: int, depth_passes: int) -> dict:
+def stage_bytes(n: int, visible: int, entries: int, pixels: int, depth_passes: int, reached: float | None = None) -> dict:
     """Algorithmic HBM bytes per step of each timed stage, for the chosen form
     (BF16 SH above DC, BF16-pair Adam state): what each stage must read and
-    write at least once, not what it happens to move."""
+    write at least once, not what it happens to move. `reached`: the Gaussians
+    the one-view selective step moves (a non-zero backward sum), measured; the
+    visible count when it was not."""
     sh_bytes = 12 + 45 * 2  # DC in FP32, 45 higher coefficients in BF16
+    moved = visible if reached is None else reached
     return {
         # positions, scales, rotations, opacity (44 B) and SH in; splat (48),
         # reach, depth key and index (12) out.
@@ -490,10 +493,28 @@ def stage_bytes(n: int, visible: int, entries: int, pixels: int, depth_passes: i
         "loss": pixels * (16 + 4 + 36 + 36 + 16 + 16 + 4),
         # per entry index and splat; per pixel image, adjoint, stop; sums out.
         "backward": entries * 52 + pixels * 36 + visible * 56,
-        # sums, parameters and colour in for every Gaussian; SH, Adam state (59
-        # words) and parameters read and written for the touched ones.
-        "chain rule and step": n * (64 + 44) + visible * (16 + 2 * (44 + sh_bytes + 59 * 4)),
+        # the 64-byte row of backward sums of every Gaussian (the reached test);
+        # colour in, and densification statistics (8 words), parameters, SH
+        # and Adam state (59 words) read and written, for the reached ones.
+        "chain rule and step": n * 64 + moved * (16 + 2 * (32 + 44 + sh_bytes + 59 * 4)),
     }
+
+
+def reached_count(splat, trainer, cams, targets, rates, views: int = 4) -> float:
+    """Mean count of the Gaussians a view reaches: those with a backward sum
+    that is not zero (a float sum of -0 counts as zero), the test the
+    one-view selective step makes. Each view's gradients are applied
+    afterwards, so the trainer ends a whole step further on."""
+    n = trainer.gaussian_count()
+    counts = []
+    for i in range(views):
+        trainer.compute_gradients(cams[i % len(cams)], targets[i % len(cams)])
+        raw = trainer.debug_download(splat.DEBUG_RAW, np.uint32).reshape(-1, 16)[:n, :14]
+        if not trainer.uses_fixed_point():
+            raw = raw & np.uint32(0x7FFFFFFF)
+        counts.append(int(np.count_nonzero(raw.any(axis=1))))
+        trainer.apply_gradients(rates)
+    return float(np.mean(counts))
 
 
 def form_key(opts) -> str:
@@ -905,7 +926,8 @@ def our_arm(args) -> None:
     n = args.gaussians
     digits_used = tuned.get("digit_bits", chosen.digit_bits)
     depth_passes = math.ceil(32 / digits_used)
-    algorithmic = stage_bytes(n, visible, entries, pixels, depth_passes)
+    reached = reached_count(splat, trainer, cams, host_targets, rates)
+    algorithmic = stage_bytes(n, visible, entries, pixels, depth_passes, reached)
     form = form_key(tuned_options(chosen, tuned))
     # The SM issue rate: measured by the library's FMA microbenchmark on this
     # GPU when it ran, else 148 SMs x 4 warp-instructions per clock at the SM
@@ -1074,7 +1096,7 @@ def our_arm(args) -> None:
                 "step, CUDA graph, SFU exp/log",
         "autotune": {"ms": tuned.get("ms"), "layout_ms": tuned.get("layout_ms"), "tile_ms": tuned.get("tile_ms"),
                      "grouped_ms": tuned.get("grouped_ms")},
-        "workload_counts": {"tile_entries": entries, "visible_splats": visible},
+        "workload_counts": {"tile_entries": entries, "visible_splats": visible, "reached_gaussians": reached},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "sm_peaks": sm_peaks,
         "score_view_ms": score_ms,

@@ -871,8 +871,6 @@ __global__ void __launch_bounds__(kStepThreads, 6) k_chain_step(Params p, const 
 // its own hash indices, so the results are those of k_chain_step, bit for bit.
 constexpr uint32_t kTouchedThreads = 128;
 constexpr uint32_t kReachChunk = 2048;
-// Coefficients whose SH Adam state words are loaded together in the SH step.
-constexpr int kStateBatch = 5;
 
 // Whether Gaussian i's backward sums hold anything, as k_chain_step's test
 // raw[k] != 0.0f: an integer sum is non-zero exactly when its value is; a
@@ -916,13 +914,13 @@ template <ShStore S> struct ShRow {
   }
 };
 
-// The one-view selective step of a reached Gaussian.// The one-view selective step of a reached Gaussian. Its SH coefficients and
-// SH Adam state are reached through scattered words (the coefficients in
-// planes, the state in its row), so every load of a coefficient is issued up
-// front (predicated on the coefficient being in use, no branch between them)
-// and the state words go in batches of kStateBatch coefficients: a handful of
-// memory latencies per Gaussian instead of one per coefficient. Element by
-// element the arithmetic, hash indices and order of sums are k_chain_step's.
+// The one-view selective step of a reached Gaussian. Its loads are issued up
+// front: the row of backward sums, the DC coefficients (three planes) and the
+// row of higher coefficients (16-byte pieces, predicated on the degree in
+// use, no branch between them); the SH Adam state row goes in batches of 16
+// words. A handful of memory latencies per Gaussian instead of one per
+// coefficient. Element by element the arithmetic, hash indices and order of
+// sums are k_chain_step's.
 template <ShStore S, StateStore ST, bool FIXED>
 __device__ __forceinline__ void step_reached(uint32_t i, const Params &p, const ViewParams &cam, const ChainArgs &args,
                                              const AdamArgs &a, int active, const void *__restrict__ rawIn,
