@@ -55,30 +55,6 @@ __device__ __forceinline__ void store_volatile(uint32_t *p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Exclusive prefix sum over the 256 threads of the block; `total` gets the sum.
-// s_warp needs kSortWarps words. Contains two barriers.
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_warp, uint32_t &total) {
-  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  uint32_t inclusive = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t n = __shfl_up_sync(0xFFFFFFFFu, inclusive, o);
-    if (lane >= (uint32_t)o) inclusive += n;
-  }
-  if (lane == 31) s_warp[warp] = inclusive;
-  __syncthreads();
-  uint32_t before = 0, sum = 0;
-#pragma unroll
-  for (int w = 0; w < kSortWarps; ++w) {
-    const uint32_t t = s_warp[w];
-    before += (uint32_t)w < warp ? t : 0u;
-    sum += t;
-  }
-  __syncthreads();
-  total = sum;
-  return before + inclusive - v;
-}
-
 template <typename K> __device__ __forceinline__ uint32_t digit_of(K key, int shift, uint32_t mask) {
   return (uint32_t)(key >> shift) & mask;
 }
@@ -144,10 +120,57 @@ __global__ void __launch_bounds__(kSortThreads) k_histogram(const K *__restrict_
 // Polls of a tile's bulk-copy barrier before the kernel gives up on it.
 constexpr int kBulkSpinLimit = 1 << 22;
 
+// Named barrier 1 over the block's first `threads` threads (a multiple of
+// 32): the threads that own a digit wait for one another while the other
+// warps go on to the block barrier.
+__device__ __forceinline__ void digit_barrier(uint32_t threads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
+}
+
+// Two exclusive prefix sums at once over the first kBins threads (one digit
+// each), of a into exA and of b into exB. s_warp needs 2 x kBins / 32 words.
+// One named barrier.
+template <int kBins>
+__device__ __forceinline__ void digit_exclusive_scan2(uint32_t a, uint32_t b, uint32_t *s_warp, uint32_t &exA, uint32_t &exB) {
+  constexpr int kWarps = kBins / 32;
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  uint32_t inA = a, inB = b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t na = __shfl_up_sync(0xFFFFFFFFu, inA, o), nb = __shfl_up_sync(0xFFFFFFFFu, inB, o);
+    if (lane >= (uint32_t)o) {
+      inA += na;
+      inB += nb;
+    }
+  }
+  uint32_t beforeA = 0, beforeB = 0;
+  if constexpr (kWarps > 1) {
+    if (lane == 31) {
+      s_warp[warp] = inA;
+      s_warp[kWarps + warp] = inB;
+    }
+    digit_barrier(kBins);
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      beforeA += (uint32_t)w < warp ? s_warp[w] : 0u;
+      beforeB += (uint32_t)w < warp ? s_warp[kWarps + w] : 0u;
+    }
+  }
+  exA = beforeA + inA - a;
+  exB = beforeB + inB - b;
+}
+
 // One pass: rank, look back, scatter. Dynamic shared memory holds the tile's
-// keys (later the keys, then the values, in digit order), its values as read,
-// and one digit byte per key. A full tile's keys and values arrive by bulk
-// copy, issued first so that the values land while the keys are ranked.
+// keys (later the keys in digit order), its values as read, the values in
+// digit order (in the keys' place, after them, where kApart is false), and
+// one digit byte per key. A full tile's keys and values
+// arrive by bulk copy, issued first so that they land while the block's
+// first barrier and the ticket settle; each thread's wait on the copy's
+// barrier makes the data visible to it, so a full tile needs no block
+// barrier there. The digit-owning threads (the first kBins) combine the
+// warps' counts, scan and look back among themselves (named barrier 1); the
+// block meets four times in all for a full tile (six where the values take
+// the keys' place).
 template <typename K, int BITS>
 __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restrict__ keysIn, const uint32_t *__restrict__ valsIn,
                                                               K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
@@ -157,15 +180,21 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
   chain_enter();
   constexpr int kBins = 1 << BITS;
   constexpr uint32_t kMask = kBins - 1;
+  static_assert(kBins % 32 == 0 && kBins <= kSortThreads, "one thread per digit, whole warps");
+  // 32-bit keys with digits of up to 7 bits: the values in digit order get
+  // their own array, and keys and values go out together. Otherwise they take
+  // the keys' place once the keys are out: 64-bit keys would fit two blocks
+  // per SM instead of three, and the 8-bit passes measured slower with it.
+  constexpr bool kApart = sizeof(K) == 4 && BITS <= 7;
   extern __shared__ __align__(128) unsigned char s_dynamic[];
   K *s_keys = reinterpret_cast<K *>(s_dynamic);
-  uint32_t *s_out = reinterpret_cast<uint32_t *>(s_dynamic);
   uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_dynamic + kSortTileKeys * sizeof(K));
-  uint8_t *s_digit = s_dynamic + kSortTileKeys * (sizeof(K) + 4);
+  uint32_t *s_out = kApart ? s_vals + kSortTileKeys : reinterpret_cast<uint32_t *>(s_dynamic);
+  uint8_t *s_digit = s_dynamic + kSortTileKeys * (sizeof(K) + (kApart ? 8 : 4));
   __shared__ uint32_t s_warpHist[kSortWarps][kBins];
   __shared__ uint32_t s_digitBase[kBins];
   __shared__ uint32_t s_globalBase[kBins];
-  __shared__ uint32_t s_scan[kSortWarps];
+  __shared__ uint32_t s_scan[2 * (kBins / 32)];
   __shared__ uint32_t s_tile;
   __shared__ __align__(8) uint64_t s_bar;
 
@@ -174,7 +203,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
     s_tile = atomicAdd(tileCounter, 1u);
     bulk_barrier_init(&s_bar, 1);
   }
-  for (int i = t; i < kSortWarps * kBins; i += kSortThreads) (&s_warpHist[0][0])[i] = 0;
+  if constexpr (BITS > 7)
+    for (int i = t; i < kSortWarps * kBins; i += kSortThreads) (&s_warpHist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t count = deviceCount != nullptr ? *deviceCount : hostCount;
@@ -182,17 +212,14 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
   if (tileStart >= count) return; // the whole block leaves; no copy was issued
   const uint32_t tileKeys = count - tileStart < (size_t)kSortTileKeys ? (uint32_t)(count - tileStart) : (uint32_t)kSortTileKeys;
   const bool bulk = tileKeys == kSortTileKeys;
-  if (bulk && t == 0) {
-    bulk_expect(&s_bar, kSortTileKeys * (uint32_t)(sizeof(K) + 4));
-    bulk_load(s_keys, keysIn + tileStart, kSortTileKeys * sizeof(K), &s_bar);
-    bulk_load(s_vals, valsIn + tileStart, kSortTileKeys * 4, &s_bar);
-  }
-
-  // The pass's global digit offsets: an exclusive scan of its histogram.
-  uint32_t binTotal = 0;
-  const uint32_t passOffset = block_exclusive_scan(t < (uint32_t)kBins ? passHist[t] : 0u, s_scan, binTotal);
-
+  // The pass's digit total, asked for now so that it has arrived by the scan.
+  const uint32_t passTotal = t < (uint32_t)kBins ? passHist[t] : 0u;
   if (bulk) {
+    if (t == 0) {
+      bulk_expect(&s_bar, kSortTileKeys * (uint32_t)(sizeof(K) + 4));
+      bulk_load(s_keys, keysIn + tileStart, kSortTileKeys * sizeof(K), &s_bar);
+      bulk_load(s_vals, valsIn + tileStart, kSortTileKeys * 4, &s_bar);
+    }
     if (!bulk_wait(&s_bar, 0, kBulkSpinLimit)) {
       // Never leave with a copy still landing in this block's shared memory.
       if (t == 0) atomicOr(error, kErrLookbackTimeout);
@@ -203,8 +230,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
       s_keys[i] = keysIn[tileStart + i];
       s_vals[i] = valsIn[tileStart + i];
     }
+    __syncthreads();
   }
-  __syncthreads();
   // Warp w owns keys [w*kSortItems*32, (w+1)*kSortItems*32); item j of lane l
   // is at j*32 + l inside that chunk, so (warp, item, lane) is the input order.
   K key[kSortItems];
@@ -275,9 +302,9 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
   }
   __syncthreads();
 
-  // Per digit: exclusive offsets across warps, and the tile's total.
-  uint32_t digitTotal = 0;
   if (t < (uint32_t)kBins) {
+    // Per digit: exclusive offsets across warps, and the tile's total.
+    uint32_t digitTotal = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) {
       const uint32_t c = s_warpHist[w][t];
@@ -286,15 +313,15 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
     }
     // Publish this tile's aggregate (or, for tile 0, its inclusive prefix) early.
     store_volatile(&lookback[(size_t)tile * kBins + t], (tile == 0 ? kFlagInclusive : kFlagAggregate) | digitTotal);
-  }
-  uint32_t tileTotal;
-  const uint32_t digitBase = block_exclusive_scan(t < (uint32_t)kBins ? digitTotal : 0u, s_scan, tileTotal);
+    // The pass's global digit offsets (an exclusive scan of its histogram) and
+    // the digits' offsets inside the tile.
+    uint32_t passOffset, digitBase;
+    digit_exclusive_scan2<kBins>(passTotal, digitTotal, s_scan, passOffset, digitBase);
 
-  // Decoupled look-back, one thread per digit, kLookbackWindow predecessors
-  // per poll: the aggregates up to the nearest inclusive prefix are added; a
-  // predecessor that has published nothing yet stops the walk there, and the
-  // next poll starts from it.
-  if (t < (uint32_t)kBins) {
+    // Decoupled look-back, kLookbackWindow predecessors per poll: the
+    // aggregates up to the nearest inclusive prefix are added; a predecessor
+    // that has published nothing yet stops the walk there, and the next poll
+    // starts from it.
     uint32_t exclusive = 0;
     if (tile > 0) {
       int64_t pred = (int64_t)tile - 1;
@@ -329,8 +356,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
   }
   __syncthreads();
 
-  // Keys into shared memory in digit order, then out: the threads of a warp
-  // write consecutive addresses within each digit's run.
+  // Keys (and, kApart, values) into shared memory in digit order, then out:
+  // the threads of a warp write consecutive addresses within each digit's run.
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const uint32_t i = chunk + j * 32 + lane;
@@ -338,49 +365,54 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
       const uint32_t d = digit_of(key[j], shift, kMask);
       slot[j] += s_digitBase[d] + s_warpHist[warp][d];
       s_keys[slot[j]] = key[j];
+      if constexpr (kApart) s_out[slot[j]] = s_vals[i];
       s_digit[slot[j]] = (uint8_t)d;
     }
   }
   __syncthreads();
   // A position outside [0, count) can only come from a look-back that gave up
   // (kErrLookbackTimeout is set then): skip the write rather than fault.
-  if (tileKeys == kSortTileKeys) {
+  const bool full = tileKeys == kSortTileKeys;
+  auto write_out = [&](bool keys, bool values) {
+    if (full) {
+#pragma unroll
+      for (int j = 0; j < kSortItems; ++j) {
+        const uint32_t i = j * kSortThreads + t;
+        const uint32_t dst = s_globalBase[s_digit[i]] + i;
+        if (dst < count) {
+          if (keys) keysOut[dst] = s_keys[i];
+          if (values) valsOut[dst] = s_out[i];
+        }
+      }
+    } else {
+      for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
+        const uint32_t dst = s_globalBase[s_digit[i]] + i;
+        if (dst < count) {
+          if (keys) keysOut[dst] = s_keys[i];
+          if (values) valsOut[dst] = s_out[i];
+        }
+      }
+    }
+  };
+  if constexpr (kApart) {
+    write_out(true, true);
+  } else {
+    write_out(true, false);
+    __syncthreads();
+    // The same permutation for the values, straight from where they landed.
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-      const uint32_t i = j * kSortThreads + t;
-      const uint32_t dst = s_globalBase[s_digit[i]] + i;
-      if (dst < count) keysOut[dst] = s_keys[i];
+      const uint32_t i = chunk + j * 32 + lane;
+      if (i < tileKeys) s_out[slot[j]] = s_vals[i];
     }
-  } else {
-    for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
-      const uint32_t dst = s_globalBase[s_digit[i]] + i;
-      if (dst < count) keysOut[dst] = s_keys[i];
-    }
-  }
-  __syncthreads();
-  // The same permutation for the values, straight from where they landed.
-#pragma unroll
-  for (int j = 0; j < kSortItems; ++j) {
-    const uint32_t i = chunk + j * 32 + lane;
-    if (i < tileKeys) s_out[slot[j]] = s_vals[i];
-  }
-  __syncthreads();
-  if (tileKeys == kSortTileKeys) {
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-      const uint32_t i = j * kSortThreads + t;
-      const uint32_t dst = s_globalBase[s_digit[i]] + i;
-      if (dst < count) valsOut[dst] = s_out[i];
-    }
-  } else {
-    for (uint32_t i = t; i < tileKeys; i += kSortThreads) {
-      const uint32_t dst = s_globalBase[s_digit[i]] + i;
-      if (dst < count) valsOut[dst] = s_out[i];
-    }
+    __syncthreads();
+    write_out(false, true);
   }
 }
 
-template <typename K, int BITS> size_t onesweep_smem() { return kSortTileKeys * (sizeof(K) + 4) + kSortTileKeys; }
+template <typename K, int BITS> size_t onesweep_smem() {
+  return kSortTileKeys * (sizeof(K) + (sizeof(K) == 4 && BITS <= 7 ? 8 : 4)) + kSortTileKeys;
+}
 
 template <typename K, int BITS>
 int sort_pairs_impl(K *keys, uint32_t *values, K *tmpKeys, uint32_t *tmpValues, size_t capacity, uint32_t hostCount,
