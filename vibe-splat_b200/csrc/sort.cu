@@ -163,10 +163,9 @@ __device__ __forceinline__ void digit_exclusive_scan2(uint32_t a, uint32_t b, ui
 // One pass: rank, look back, scatter. Dynamic shared memory holds the tile's
 // keys (later the keys in digit order), its values as read, the values in
 // digit order (in the keys' place, after them, where kApart is false), and
-// one digit byte per key. A full tile's keys and values
-// arrive by bulk copy, issued first so that they land while the block's
-// first barrier and the ticket settle; each thread's wait on the copy's
-// barrier makes the data visible to it, so a full tile needs no block
+// one digit byte per key. A full tile's keys and values arrive by bulk copy,
+// issued as soon as the ticket names the tile; each thread's wait on the
+// copy's barrier makes the data visible to it, so a full tile needs no block
 // barrier there. The digit-owning threads (the first kBins) combine the
 // warps' counts, scan and look back among themselves (named barrier 1); the
 // block meets four times in all for a full tile (six where the values take
@@ -284,14 +283,17 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
 #pragma unroll
     for (int r = 0; r < kPerLane; ++r) s_warpHist[warp][lane + 32 * r] = run[r];
   } else {
-    // Eight-bit digits: match.any multi-split with the running counts in
-    // shared memory (eight registers a lane would not pay off).
+    // Eight-bit digits: the peers from the warp's ballots of the digit's bits
+    // (match.any measured slower), the running counts in shared memory
+    // (eight registers a lane would not pay off).
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
       const uint32_t i = chunk + j * 32 + lane;
       const bool valid = i < tileKeys;
-      const uint32_t d = valid ? digit_of(key[j], shift, kMask) : (uint32_t)kBins;
-      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+      const uint32_t d = valid ? digit_of(key[j], shift, kMask) : 0u;
+      uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+      for (int b = 0; b < BITS; ++b) peers &= __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u) ^ (((d >> b) & 1u) - 1u);
       const uint32_t before = __popc(peers & ((1u << lane) - 1u));
       const uint32_t prior = valid ? s_warpHist[warp][d] : 0u;
       __syncwarp();
