@@ -202,8 +202,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
     s_tile = atomicAdd(tileCounter, 1u);
     bulk_barrier_init(&s_bar, 1);
   }
-  if constexpr (BITS > 7)
-    for (int i = t; i < kSortWarps * kBins; i += kSortThreads) (&s_warpHist[0][0])[i] = 0;
+  for (int i = t; i < kSortWarps * kBins; i += kSortThreads) (&s_warpHist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t count = deviceCount != nullptr ? *deviceCount : hostCount;
@@ -242,65 +241,26 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K *__restric
     key[j] = i < tileKeys ? s_keys[i] : K(0);
   }
 
-  if constexpr (BITS <= 7) {
-    // Ballot multi-split, item by item in input order: the peers of a digit
-    // are the AND of the warp's ballots of its bits; the warp's running count
-    // of digit b lives in register b / 32 of lane b % 32 and grows by the
-    // popcount of that digit's peers. No shared memory until the end.
-    constexpr int kPerLane = kBins / 32;
-    uint32_t run[kPerLane];
+  // Multi-split by ballots, item by item in input order: the peers of a
+  // digit are the AND of the warp's ballots of its bits (match.any measured
+  // slower); the warp's running count of each digit lives in shared memory,
+  // read by every peer and advanced by the highest one. (Running counts in
+  // registers, lane b % 32 holding digit b, measured slower for 6-bit digits.)
 #pragma unroll
-    for (int r = 0; r < kPerLane; ++r) run[r] = 0u;
-    const uint32_t below = (1u << lane) - 1u;
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t i = chunk + j * 32 + lane;
+    const bool valid = i < tileKeys;
+    const uint32_t d = valid ? digit_of(key[j], shift, kMask) : 0u;
+    uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+    // x ^ (flag - 1): x where the flag is 1, ~x where it is 0.
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-      const uint32_t i = chunk + j * 32 + lane;
-      const uint32_t d = digit_of(key[j], shift, kMask);
-      const uint32_t valid = __ballot_sync(0xFFFFFFFFu, i < tileKeys);
-      uint32_t bit[BITS];
-#pragma unroll
-      for (int b = 0; b < BITS; ++b) bit[b] = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
-      // x ^ (flag - 1): x where the flag is 1, ~x where it is 0.
-      uint32_t peers = valid;
-#pragma unroll
-      for (int b = 0; b < BITS; ++b) peers &= bit[b] ^ (((d >> b) & 1u) - 1u);
-      uint32_t prior = 0u;
-#pragma unroll
-      for (int r = 0; r < kPerLane; ++r) {
-        const uint32_t x = __shfl_sync(0xFFFFFFFFu, run[r], d & 31u);
-        prior = (d >> 5) == (uint32_t)r ? x : prior;
-      }
-      slot[j] = prior + __popc(peers & below);
-#pragma unroll
-      for (int r = 0; r < kPerLane; ++r) {
-        const uint32_t bin = lane + 32u * (uint32_t)r;
-        uint32_t m = valid;
-#pragma unroll
-        for (int b = 0; b < BITS; ++b) m &= bit[b] ^ (((bin >> b) & 1u) - 1u);
-        run[r] += __popc(m);
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < kPerLane; ++r) s_warpHist[warp][lane + 32 * r] = run[r];
-  } else {
-    // Eight-bit digits: the peers from the warp's ballots of the digit's bits
-    // (match.any measured slower), the running counts in shared memory
-    // (eight registers a lane would not pay off).
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-      const uint32_t i = chunk + j * 32 + lane;
-      const bool valid = i < tileKeys;
-      const uint32_t d = valid ? digit_of(key[j], shift, kMask) : 0u;
-      uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
-#pragma unroll
-      for (int b = 0; b < BITS; ++b) peers &= __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u) ^ (((d >> b) & 1u) - 1u);
-      const uint32_t before = __popc(peers & ((1u << lane) - 1u));
-      const uint32_t prior = valid ? s_warpHist[warp][d] : 0u;
-      __syncwarp();
-      if (valid && lane == (uint32_t)(31 - __clz(peers))) s_warpHist[warp][d] = prior + __popc(peers);
-      __syncwarp();
-      slot[j] = prior + before;
-    }
+    for (int b = 0; b < BITS; ++b) peers &= __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u) ^ (((d >> b) & 1u) - 1u);
+    const uint32_t before = __popc(peers & ((1u << lane) - 1u));
+    const uint32_t prior = valid ? s_warpHist[warp][d] : 0u;
+    __syncwarp();
+    if (valid && lane == (uint32_t)(31 - __clz(peers))) s_warpHist[warp][d] = prior + __popc(peers);
+    __syncwarp();
+    slot[j] = prior + before;
   }
   __syncthreads();
 
