@@ -818,27 +818,45 @@ __device__ __forceinline__ void forward2_tile(int tile, const Splat *__restrict_
       const bool v0 = !done0 && (mask & pp.bits[0]) == pp.bits[0] && !(power.x > 0.0f) && a0 >= kAlphaMin;
       const bool v1 = !done1 && (mask & pp.bits[1]) == pp.bits[1] && !(power.y > 0.0f) && a1 >= kAlphaMin;
       if (!(v0 || v1)) continue;
-      const float2 oneMinus = rsub2(make_float2(a0, a1), f2(1.0f));
-      const float2 next = add2(logT, make_float2(M::log(oneMinus.x), M::log(oneMinus.y)));
-      // A pixel whose transmittance would fall below the floor stops here.
-      const bool s0 = v0 && next.x < logMin, s1 = v1 && next.y < logMin;
-      if (s0) {
-        stop0 = end + k + 1u;
-        done0 = true;
+      // A pixel that does not blend takes alpha 0: weight 0, factor 1 - 0 = 1
+      // and log 1 = 0 (exact in both forms), so its update is an exact no-op
+      // that needs no select. Its log T stays at or above the floor, so only
+      // a blending pixel can stop.
+      float2 alpha = make_float2(v0 ? a0 : 0.0f, v1 ? a1 : 0.0f);
+      float2 oneMinus = rsub2(alpha, f2(1.0f));
+      float2 next = add2(logT, make_float2(M::log(oneMinus.x), M::log(oneMinus.y)));
+      if (next.x < logMin || next.y < logMin) {
+        // A pixel whose transmittance would fall below the floor stops here,
+        // and this splat changes nothing in it.
+        if (next.x < logMin) {
+          stop0 = end + k + 1u;
+          done0 = true;
+          alpha.x = 0.0f;
+          oneMinus.x = 1.0f;
+          next.x = logT.x;
+        }
+        if (next.y < logMin) {
+          stop1 = end + k + 1u;
+          done1 = true;
+          alpha.y = 0.0f;
+          oneMinus.y = 1.0f;
+          next.y = logT.y;
+        }
+        const float2 w = mul2(Tr, alpha);
+        cr = fma2(w, f2(s.r), cr);
+        cg = fma2(w, f2(s.g), cg);
+        cb = fma2(w, f2(s.b), cb);
+        Tr = mul2(Tr, oneMinus);
+        logT = next;
+        if (done0 && done1) break;
+        continue;
       }
-      if (s1) {
-        stop1 = end + k + 1u;
-        done1 = true;
-      }
-      // A pixel that does not blend takes weight 0 and factor 1: exact no-ops.
-      const bool b0 = v0 && !s0, b1 = v1 && !s1;
-      const float2 w = mul2(Tr, make_float2(b0 ? a0 : 0.0f, b1 ? a1 : 0.0f));
+      const float2 w = mul2(Tr, alpha);
       cr = fma2(w, f2(s.r), cr);
       cg = fma2(w, f2(s.g), cg);
       cb = fma2(w, f2(s.b), cb);
-      Tr = mul2(Tr, make_float2(b0 ? oneMinus.x : 1.0f, b1 ? oneMinus.y : 1.0f));
-      logT = make_float2(b0 ? next.x : logT.x, b1 ? next.y : logT.y);
-      if (done0 && done1) break;
+      Tr = mul2(Tr, oneMinus);
+      logT = next;
     }
     }
   }
