@@ -110,6 +110,10 @@ void launch_bin_emit(const Splat *splats, const float *reach, const uint32_t *it
 void launch_tile_ranges(const uint32_t *tileKeys32, const unsigned long long *tileKeys64, const uint32_t *deviceCount,
                         uint32_t capacity, uint32_t tileLimit, uint2 *ranges, uint32_t *error, cudaStream_t stream);
 
+// The tiles of a launch, heaviest first, into order (tiles entries): the work
+// of tile i is tileWork[i], or, without tileWork, the length of ranges[i].
+void launch_tile_order(const uint2 *ranges, const uint32_t *tileWork, uint32_t tiles, uint32_t *order, cudaStream_t stream);
+
 // Per-pixel blend lists of the store-everything variant: counts[p] splats
 // blended at pixel p, recorded front to back at pool[offsets[p] ...] as
 // (entry index, alpha bits).
@@ -133,6 +137,12 @@ struct RasterConfig {
   int batch = 256;
   uint32_t *workForward = nullptr;
   uint32_t *workBackward = nullptr;
+  // The two-pixel kernels' tile orders, heaviest first (launch_tile_order;
+  // null: raster order), and where the two-pixel compositing records each
+  // tile's work for the backward's order (null: not recorded).
+  const uint32_t *orderForward = nullptr;
+  const uint32_t *orderBackward = nullptr;
+  uint32_t *tileWork = nullptr;
   // The two-pixel float backward's sums: a butterfly per (splat, warp), or,
   // twoPhase, splat-parallel per group of splats (not for scored views).
   bool twoPhase = false;

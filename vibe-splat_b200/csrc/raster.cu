@@ -770,20 +770,80 @@ template <int T> constexpr int backward2_blocks() { return T > 16 ? 1 : 6; }
 // persistent launch (work not null: a grid of resident blocks), tiles of every
 // view claimed from the launch's counter until they run out. Every thread of
 // the block gets the same answer; -1 when the block is done.
-__device__ __forceinline__ int next_tile(uint32_t *work, uint32_t total, bool first, uint32_t *s_next) {
-  if (work == nullptr) return first ? (int)blockIdx.x : -1;
+// With an order (not null), the i-th tile taken is order[i] (heaviest first,
+// k_tile_order) instead of tile i.
+__device__ __forceinline__ int next_tile(uint32_t *work, uint32_t total, bool first, uint32_t *s_next,
+                                         const uint32_t *order = nullptr) {
+  if (work == nullptr) {
+    if (!first) return -1;
+    return order != nullptr ? (int)order[blockIdx.x] : (int)blockIdx.x;
+  }
   __syncthreads(); // the previous tile is finished with shared memory
   if (threadIdx.x == 0) *s_next = atomicAdd(work, 1u);
   __syncthreads();
   const uint32_t tile = *s_next;
-  return tile < total ? (int)tile : -1;
+  if (tile >= total) return -1;
+  return order != nullptr ? (int)order[tile] : (int)tile;
+}
+
+// The rasterizer's tiles, heaviest first (new here; the reference launches its
+// tiles in raster order): tiles cost what they walk, from a few entries to
+// thousands, and a launch whose heavy tiles start last ends with most SMs idle
+// while those finish. Each tile's work (tileWork, or without it the length of
+// its entry range) is put into one of 32 half-octave classes, and the tiles are
+// listed class by class, heaviest class first; the order inside a class is
+// the order in which the block's threads claim places (it changes which block
+// takes which tile, not what any tile computes). One block.
+constexpr int kOrderThreads = 1024, kOrderClasses = 32;
+
+__device__ __forceinline__ uint32_t work_class(uint32_t work) {
+  return work == 0u ? 0u : min((uint32_t)kOrderClasses - 1u, 1u + (uint32_t)(2.0f * __log2f((float)work)));
+}
+
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order(const uint2 *__restrict__ ranges, const uint32_t *__restrict__ tileWork,
+                                                              uint32_t tiles, uint32_t *__restrict__ order) {
+  chain_enter();
+  __shared__ uint32_t s_count[kOrderClasses];
+  const uint32_t t = threadIdx.x, lane = t & 31u;
+  if (t < (uint32_t)kOrderClasses) s_count[t] = 0u;
+  __syncthreads();
+  const uint32_t rounds = div_up(tiles, kOrderThreads);
+  for (uint32_t r = 0; r < rounds; ++r) {
+    const uint32_t i = r * kOrderThreads + t;
+    const bool in = i < tiles;
+    const uint32_t c = in ? work_class(tileWork != nullptr ? tileWork[i] : ranges[i].y - ranges[i].x) : kOrderClasses;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, c);
+    if (in && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_count[c], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  if (t == 0) {
+    uint32_t run = 0;
+    for (int c = kOrderClasses - 1; c >= 0; --c) {
+      const uint32_t k = s_count[c];
+      s_count[c] = run;
+      run += k;
+    }
+  }
+  __syncthreads();
+  for (uint32_t r = 0; r < rounds; ++r) {
+    const uint32_t i = r * kOrderThreads + t;
+    const bool in = i < tiles;
+    const uint32_t c = in ? work_class(tileWork != nullptr ? tileWork[i] : ranges[i].y - ranges[i].x) : kOrderClasses;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, c);
+    const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+    uint32_t base = 0u;
+    if (in && lane == leader) base = atomicAdd(&s_count[c], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (in) order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
+  }
 }
 
 template <class M, int T, int B>
 __device__ __forceinline__ void forward2_tile(int tile, const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues,
                                               const uint2 *__restrict__ ranges, const ViewSet &views, float bgR, float bgG,
                                               float bgB, float4 *__restrict__ image, uint32_t *__restrict__ stops,
-                                              uint32_t splatLimit, uint32_t *error, Staged *s_batch, uint32_t (*s_cover)[B / 32]) {
+                                              uint32_t splatLimit, uint32_t *error, Staged *s_batch, uint32_t (*s_cover)[B / 32],
+                                              uint32_t *tileWork, uint32_t *s_least) {
   constexpr int kThreads = TileShape<T>::kThreads;
   const TileGeometry geo = tile_geometry(views, tile, T);
   const ViewParams &cam = views.v[geo.view];
@@ -870,6 +930,19 @@ __device__ __forceinline__ void forward2_tile(int tile, const Splat *__restrict_
     image[at] = make_float4(fmaf(Tr.y, bgR, cr.y), fmaf(Tr.y, bgG, cg.y), fmaf(Tr.y, bgB, cb.y), logT.y);
     stops[at] = stop1;
   }
+  if (tileWork != nullptr) {
+    // The entries the backward pass walks here: from the least stop of the
+    // tile's pixels to the end of its range.
+    const uint32_t least = __reduce_min_sync(0xFFFFFFFFu, min(pp.inside[0] ? stop0 : range.y, pp.inside[1] ? stop1 : range.y));
+    if ((t & 31u) == 0u) s_least[warp] = least;
+    __syncthreads();
+    if (t == 0) {
+      uint32_t m = s_least[0];
+#pragma unroll
+      for (int w = 1; w < TileShape<T>::kWarps; ++w) m = min(m, s_least[w]);
+      tileWork[tile] = range.y - m;
+    }
+  }
 }
 
 // Compositing, two pixels per thread, tiles of T x T pixels, batches of B
@@ -879,17 +952,19 @@ template <class M, int T, int B>
 __global__ void __launch_bounds__(TileShape<T>::kThreads, forward2_blocks<T>())
     k_forward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
                const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, float4 *__restrict__ image,
-               uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error, uint32_t *work) {
+               uint32_t *__restrict__ stops, uint32_t splatLimit, uint32_t *error, uint32_t *work, const uint32_t *order,
+               uint32_t *tileWork) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[B];
   __shared__ uint32_t s_cover[TileShape<T>::kWarps][B / 32];
+  __shared__ uint32_t s_least[TileShape<T>::kWarps];
   __shared__ uint32_t s_next;
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next); tile >= 0;
-       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next))
+  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next, order); tile >= 0;
+       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next, order))
     forward2_tile<M, T, B>(tile, splats, entryValues, ranges, views, bgR, bgG, bgB, image, stops, splatLimit, error, s_batch,
-                           s_cover);
+                           s_cover, tileWork, s_least);
 }
 
 // Float sums only: each lane adds its two pixels' values before one
@@ -1030,7 +1105,7 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, backward2_blocks<T>())
     k_backward2(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
                 const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                 const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
-                uint32_t splatLimit, uint32_t *error, const float *__restrict__ edge, uint32_t *work) {
+                uint32_t splatLimit, uint32_t *error, const float *__restrict__ edge, uint32_t *work, const uint32_t *order) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
   __shared__ Staged s_batch[B];
@@ -1039,8 +1114,8 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, backward2_blocks<T>())
   __shared__ uint32_t s_cover[TileShape<T>::kWarps][B / 32];
   __shared__ uint32_t s_next;
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next); tile >= 0;
-       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next))
+  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next, order); tile >= 0;
+       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next, order))
     backward2_tile<M, SCORE, T, B>(tile, splats, entryValues, ranges, views, bgR, bgG, bgB, image, adjoint, stops, raw, splatLimit,
                                    error, edge, s_batch, s_acc, s_min, s_cover);
 }
@@ -1242,7 +1317,7 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, T > 16 ? 1 : 4)
     k_backward3(const Splat *__restrict__ splats, const uint32_t *__restrict__ entryValues, const uint2 *__restrict__ ranges,
                 const ViewSet *__restrict__ viewsPtr, float bgR, float bgG, float bgB, const float4 *__restrict__ image,
                 const float4 *__restrict__ adjoint, const uint32_t *__restrict__ stops, float *__restrict__ raw,
-                uint32_t splatLimit, uint32_t *error, uint32_t *work) {
+                uint32_t splatLimit, uint32_t *error, uint32_t *work, const uint32_t *order) {
   chain_enter();
   constexpr int W = TileShape<T>::kWarps;
   const ViewSet &views = *viewsPtr;
@@ -1257,8 +1332,8 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, T > 16 ? 1 : 4)
   __shared__ uint32_t s_cover[W][B / 32];
   __shared__ uint32_t s_next;
   if (error != nullptr && (*error & kErrEntryOverflow) != 0u) return;
-  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next); tile >= 0;
-       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next))
+  for (int tile = next_tile(work, (uint32_t)views.totalTiles, true, &s_next, order); tile >= 0;
+       tile = next_tile(work, (uint32_t)views.totalTiles, false, &s_next, order))
     backward3_tile<M, T, B>(tile, splats, entryValues, ranges, views, bgR, bgG, bgB, image, adjoint, stops, raw, splatLimit, error,
                             s_batch, s_acc, s_min, s_cover, s_pairs, s_pix, s_az);
 }
@@ -1292,7 +1367,8 @@ void launch_forward2(const Splat *splats, const uint32_t *entryValues, const uin
   uint32_t grid = (uint32_t)views.totalTiles;
   if (cfg.workForward != nullptr) grid = std::min(grid, resident_blocks((const void *)k_forward2<M, T, B>, kThreads));
   launch_chained(k_forward2<M, T, B>, dim3(grid), dim3(kThreads), 0, stream, splats, entryValues, ranges, dViews, cfg.background[0],
-                 cfg.background[1], cfg.background[2], image, stops, splatLimit, error, cfg.workForward);
+                 cfg.background[1], cfg.background[2], image, stops, splatLimit, error, cfg.workForward, cfg.orderForward,
+                 cfg.tileWork);
 }
 
 template <class M, bool SCORE, int T, int B>
@@ -1305,7 +1381,7 @@ void launch_backward2(const Splat *splats, const uint32_t *entryValues, const ui
   if (cfg.workBackward != nullptr) grid = std::min(grid, resident_blocks((const void *)k_backward2<M, SCORE, T, B>, kThreads));
   launch_chained(k_backward2<M, SCORE, T, B>, dim3(grid), dim3(kThreads), 0, stream, splats, entryValues, ranges, dViews,
                  cfg.background[0], cfg.background[1], cfg.background[2], image, adjoint, stops, raw, splatLimit, error, edge,
-                 cfg.workBackward);
+                 cfg.workBackward, cfg.orderBackward);
 }
 
 template <int T> constexpr size_t backward3_dynamic_bytes() {
@@ -1333,7 +1409,7 @@ void launch_backward3(const Splat *splats, const uint32_t *entryValues, const ui
   }
   launch_chained(k_backward3<M, T, B>, dim3(grid), dim3(kThreads), kDynamic, stream, splats, entryValues, ranges, dViews,
                  cfg.background[0], cfg.background[1], cfg.background[2], image, adjoint, stops, raw, splatLimit, error,
-                 cfg.workBackward);
+                 cfg.workBackward, cfg.orderBackward);
 }
 
 // Calls f(tile edge, batch depth) with the two-pixel kernels' settings as
@@ -1439,6 +1515,11 @@ void launch_backward(const Splat *splats, const uint32_t *entryValues, const uin
   }
 #undef SB_BACKWARD_FIX
 #undef SB_BACKWARD
+}
+
+void launch_tile_order(const uint2 *ranges, const uint32_t *tileWork, uint32_t tiles, uint32_t *order, cudaStream_t stream) {
+  if (tiles == 0) return;
+  launch_chained(k_tile_order, dim3(1), dim3(kOrderThreads), 0, stream, ranges, tileWork, tiles, order);
 }
 
 void launch_backward_lists(const Splat *splats, const uint32_t *entryValues, const uint2 *ranges, const ViewSet &views,

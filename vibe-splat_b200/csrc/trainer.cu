@@ -592,7 +592,9 @@ void Trainer::ensure_view_buffers() {
   adjoint.ensure(pixels * 16);
   fields.ensure(pixels * 36);
   target.ensure(pixels * 4);
-  ranges.ensure(tiles * 8);
+  // The tile ranges, then per tile the compositing's work record and the
+  // backward's tile order (launch_tile_order).
+  ranges.ensure(tiles * 16);
   partials.ensure((size_t)views.totalLossTiles * 8);
   if (image.bytes() + target.bytes() + ranges.bytes() != before) clear_graphs();
   if (blendLists) {
@@ -875,7 +877,15 @@ void Trainer::record_forward() {
     launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
                    stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream, 2, lists);
   } else {
-    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+    RasterConfig c = cfg;
+    // The two-pixel compositing records what the backward pass will walk in
+    // each tile, for the backward's tile order. (Its own tiles stay in raster
+    // order: measured, ordering them by the length of their entry ranges
+    // made the compositing no faster; how far a tile's pixels walk before
+    // they stop is not known before it runs.)
+    if (forwardPixels == 2 && backwardPixels == 2 && !fixedPoint)
+      c.tileWork = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + views.totalTiles);
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), c, image.get<float4>(),
                    stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
   }
   end(4);
@@ -913,7 +923,16 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
                           adjoint.get<float4>(), stops.get<uint32_t>(), lists, raw.get<float>(), n * (uint32_t)views.count,
                           error, stream);
   } else {
-    launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+    RasterConfig c = cfg;
+    if (backwardPixels == 2 && !fixedPoint) {
+      // Heaviest tiles first, by the entries each walks (recorded by the
+      // two-pixel compositing), else by the length of their entry ranges.
+      const uint32_t tiles = (uint32_t)views.totalTiles;
+      uint32_t *extra = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + tiles);
+      launch_tile_order(ranges.get<uint2>(), forwardPixels == 2 ? extra : nullptr, tiles, extra + tiles, stream);
+      c.orderBackward = extra + tiles;
+    }
+    launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), c, image.get<float4>(),
                     adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
                     stream, scoreShare > 0.0f ? scoreEdge.get<float>() : nullptr);
   }
