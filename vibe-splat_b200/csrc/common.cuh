@@ -18,6 +18,8 @@ namespace sb {
 // and the loss's tile. The float two-pixel rasterizer also runs 32 x 32 tiles.
 constexpr int kTileSize = 16;
 constexpr int kTilePixels = kTileSize * kTileSize;
+// The loss kernels' own tiles: 16 pixels wide, 32 tall.
+constexpr int kLossTileW = 16, kLossTileH = 32;
 constexpr uint32_t kInvisible = 0xFFFFFFFFu;
 constexpr float kLogMinTransmittance = -9.210340372f;
 constexpr float kMinQuaternionLength = 1e-4f;
@@ -57,7 +59,7 @@ struct ViewParams {
   float fixedScale;    // 3 W H 64, the fixed-point resolution
   int activeDegree;    // SH degree in use
   int activeCoeffs;    // (degree + 1)^2
-  // The loss's own grid of 16 x 16 tiles (the rasterizer's tile may be larger).
+  // The loss's own grid of kLossTileW x kLossTileH tiles.
   int lossGridW, lossGridH;
   int lossTileBase;    // first global loss tile of this view
   int lossTileCount;

@@ -2,14 +2,20 @@
 // dL/dImage and L1 (shaders/train_loss.comp:52-113), for
 //   L = (1 - lambda) mean|image - target| + lambda (1 - mean SSIM)
 // over pixels and channels, 11x11 Gaussian window (sigma 1.5) cut off and
-// renormalised at the image border. Both kernels run one block per 16x16
-// tile: the tile and a 5-pixel halo are staged into shared memory once, a
-// horizontal pass over the tile plus 5 rows above and below goes into shared
-// memory, then a vertical pass out of it. Normalisations are multiplications
+// renormalised at the image border. Both kernels run one block of 512 threads
+// per loss tile of 16 x 32 pixels (the reference's passes run per pixel): the
+// tile and a 5-pixel halo are staged into shared memory once, a horizontal
+// pass over the tile plus 5 rows above and below goes into shared memory,
+// then a vertical pass out of it. The tall tile spends fewer of its
+// horizontal sums on halo rows (42 rows for 32 against 26 for 16), and its
+// horizontal items fill the block's threads in one round. Normalisations are multiplications
 // by reciprocals (the reference's GLSL division is not correctly rounded
 // either). The fields are stored as 9
 // FP32 planes (P, Q, R per channel; 36 bytes per pixel instead of the
 // reference's 48). Per-tile partial sums are added in FP64 on the GPU.
+#include <mutex>
+#include <set>
+
 #include "kernels.cuh"
 
 namespace sb {
@@ -17,8 +23,10 @@ namespace sb {
 namespace {
 
 constexpr int kHalo = 5;
-constexpr int kRows = kTileSize + 2 * kHalo;
-constexpr int kSpan = kRows * kTileSize;
+constexpr int kLossW = kLossTileW, kLossH = kLossTileH;
+constexpr int kLossThreads = kLossW * kLossH;
+constexpr int kRows = kLossH + 2 * kHalo;
+constexpr int kSpan = kRows * kLossW;
 constexpr float kC1 = 0.0001f, kC2 = 0.0009f;
 
 __constant__ float c_weights[11] = {0.00102838f, 0.00759876f, 0.03600077f, 0.10936069f, 0.21300554f, 0.26601172f,
@@ -49,7 +57,7 @@ __device__ __forceinline__ int view_of_tile(const ViewSet &views, int tile) {
   return v;
 }
 
-// Sum over the block of 256 threads; valid in thread 0.
+// Sum over the block's threads; valid in thread 0.
 __device__ __forceinline__ float block_sum(float v, float *s_warp) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
@@ -57,7 +65,7 @@ __device__ __forceinline__ float block_sum(float v, float *s_warp) {
   __syncthreads();
   float total = 0.0f;
   if (threadIdx.x == 0)
-    for (int w = 0; w < kTilePixels / 32; ++w) total += s_warp[w];
+    for (int w = 0; w < kLossThreads / 32; ++w) total += s_warp[w];
   return total;
 }
 
@@ -70,14 +78,16 @@ __device__ __forceinline__ float block_sum(float v, float *s_warp) {
 // applied, with the vertical one, in the epilogue. Both passes are register
 // blocked: a thread takes kGroup neighbouring outputs of one channel, which
 // share kGroup + 10 staged values per plane.
-constexpr int kSpanCols = kTileSize + 2 * kHalo;
+constexpr int kSpanCols = kLossW + 2 * kHalo;
 constexpr int kStage = kRows * kSpanCols;
 constexpr int kGroup = 4;
-constexpr int kGroups = kTileSize / kGroup;
-constexpr int kHorizontalItems = kRows * kGroups;      // per channel
-constexpr int kVerticalItems = kTileSize * kGroups;    // per channel
-static_assert(3 * kVerticalItems <= kTilePixels, "one vertical item per thread");
-static_assert(kTileSize == 16 && kGroup == 4, "h_index's swizzle assumes 16-wide rows and 4-row groups");
+constexpr int kGroupsX = kLossW / kGroup;               // horizontal items per row
+constexpr int kGroupsY = kLossH / kGroup;               // vertical items per column
+constexpr int kHorizontalItems = kRows * kGroupsX;      // per channel
+constexpr int kVerticalItems = kLossW * kGroupsY;       // per channel
+static_assert(3 * kHorizontalItems <= kLossThreads, "one horizontal item per thread");
+static_assert(3 * kVerticalItems <= kLossThreads, "one vertical item per thread");
+static_assert(kLossW == 16 && kGroup == 4 && kRows % 2 == 0, "h_index's swizzle assumes 16-wide rows and 4-row groups");
 
 // Where the horizontal sum of (row, column) lives in its plane: rows in pairs
 // of 32 words, a pair's two 16-word halves swapped where bit 2 of the row is
@@ -92,51 +102,38 @@ __device__ __forceinline__ float norm_of(int at, int size) {
   return (at >= kHalo && at + kHalo < size) ? c_weights_total() : window_norm(at, size);
 }
 
-// Horizontal window sums of `planes` staged planes into s_h, kGroup outputs
-// per item: FIELD sums x (one plane each); SSIM sums x, y, x^2, y^2, xy.
-template <bool SSIM>
+// Horizontal window sums x, y, x^2, y^2, xy of the staged image and target
+// planes into s_h, kGroup outputs per item.
 __device__ __forceinline__ void horizontal_pass(const float (*s_in)[kStage], float (*s_h)[kSpan]) {
-  constexpr int kOut = SSIM ? 5 : 3;
-  for (int item = threadIdx.x; item < 3 * kHorizontalItems; item += kTilePixels) {
+  for (int item = threadIdx.x; item < 3 * kHorizontalItems; item += kLossThreads) {
     const int k = item / kHorizontalItems, rem = item % kHorizontalItems;
-    const int r = rem / kGroups, c = (rem % kGroups) * kGroup;
+    const int r = rem / kGroupsX, c = (rem % kGroupsX) * kGroup;
     const int row = r * kSpanCols + c;
-    float m[kGroup][kOut];
+    float m[kGroup][5];
 #pragma unroll
     for (int o = 0; o < kGroup; ++o)
 #pragma unroll
-      for (int q = 0; q < kOut; ++q) m[o][q] = 0.0f;
+      for (int q = 0; q < 5; ++q) m[o][q] = 0.0f;
 #pragma unroll
     for (int u = 0; u < kGroup + 10; ++u) {
-      if constexpr (SSIM) {
-        const float a = s_in[k][row + u], b = s_in[3 + k][row + u];
+      const float a = s_in[k][row + u], b = s_in[3 + k][row + u];
 #pragma unroll
-        for (int o = 0; o < kGroup; ++o) {
-          const int tap = u - o; // output c + o takes staged column c + o + tap
-          if (tap < 0 || tap > 10) continue;
-          const float w = c_weights[tap];
-          const float wa = w * a, wb = w * b;
-          m[o][0] = fmaf(w, a, m[o][0]);
-          m[o][1] = fmaf(w, b, m[o][1]);
-          m[o][2] = fmaf(wa, a, m[o][2]);
-          m[o][3] = fmaf(wb, b, m[o][3]);
-          m[o][4] = fmaf(wa, b, m[o][4]);
-        }
-      } else {
-        const float v[3] = {s_in[k][row + u], s_in[3 + k][row + u], s_in[6 + k][row + u]};
-#pragma unroll
-        for (int o = 0; o < kGroup; ++o) {
-          const int tap = u - o;
-          if (tap < 0 || tap > 10) continue;
-#pragma unroll
-          for (int q = 0; q < 3; ++q) m[o][q] = fmaf(c_weights[tap], v[q], m[o][q]);
-        }
+      for (int o = 0; o < kGroup; ++o) {
+        const int tap = u - o; // output c + o takes staged column c + o + tap
+        if (tap < 0 || tap > 10) continue;
+        const float w = c_weights[tap];
+        const float wa = w * a, wb = w * b;
+        m[o][0] = fmaf(w, a, m[o][0]);
+        m[o][1] = fmaf(w, b, m[o][1]);
+        m[o][2] = fmaf(wa, a, m[o][2]);
+        m[o][3] = fmaf(wb, b, m[o][3]);
+        m[o][4] = fmaf(wa, b, m[o][4]);
       }
     }
 #pragma unroll
     for (int o = 0; o < kGroup; ++o)
 #pragma unroll
-      for (int q = 0; q < kOut; ++q) s_h[q * 3 + k][h_index(r, c + o)] = m[o][q];
+      for (int q = 0; q < 5; ++q) s_h[q * 3 + k][h_index(r, c + o)] = m[o][q];
   }
 }
 
@@ -171,17 +168,22 @@ struct TileOrigin {
 __device__ __forceinline__ TileOrigin tile_origin(const ViewSet &views, int tile) {
   const ViewParams &cam = views.v[view_of_tile(views, tile)];
   const int local = tile - cam.lossTileBase;
-  return TileOrigin{&cam, (local % cam.lossGridW) * kTileSize, (local / cam.lossGridW) * kTileSize};
+  return TileOrigin{&cam, (local % cam.lossGridW) * kLossW, (local / cam.lossGridW) * kLossH};
 }
 
-__global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
-                                                      const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
-                                                      float2 *__restrict__ partials) {
+// Dynamic shared memory of k_ssim: image r, g, b, then target r, g, b staged;
+// the horizontal sums x, y, x^2, y^2, xy, three channels each.
+constexpr size_t kSsimShared = sizeof(float) * (6 * kStage + 15 * kSpan);
+
+__global__ void __launch_bounds__(kLossThreads, 3) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
+                                                       const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
+                                                       float2 *__restrict__ partials) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
-  __shared__ float s_in[6][kStage]; // image r, g, b, then target r, g, b
-  __shared__ float s_h[15][kSpan];  // sums x, y, x^2, y^2, xy, three channels each
-  __shared__ float s_warp[kTilePixels / 32];
+  extern __shared__ __align__(16) float s_dynamic[];
+  float(*s_in)[kStage] = reinterpret_cast<float(*)[kStage]>(s_dynamic);
+  float(*s_h)[kSpan] = reinterpret_cast<float(*)[kSpan]>(s_dynamic + 6 * kStage);
+  __shared__ float s_warp[kLossThreads / 32];
   const int tile = blockIdx.x;
   const TileOrigin origin = tile_origin(views, tile);
   const ViewParams &cam = *origin.cam;
@@ -190,8 +192,8 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
   const size_t plane = (size_t)views.totalPixels;
 
 #pragma unroll
-  for (int round = 0; round < (kStage + kTilePixels - 1) / kTilePixels; ++round) {
-    const int i = round * kTilePixels + threadIdx.x;
+  for (int round = 0; round < (kStage + kLossThreads - 1) / kLossThreads; ++round) {
+    const int i = round * kLossThreads + threadIdx.x;
     if (i >= kStage) break;
     const int r = i / kSpanCols, c = i % kSpanCols;
     const int y = y0 + r - kHalo, x = x0 + c - kHalo;
@@ -210,12 +212,12 @@ __global__ void __launch_bounds__(kTilePixels) k_ssim(const float4 *__restrict__
     s_in[5][i] = b3.z;
   }
   __syncthreads();
-  horizontal_pass<true>(s_in, s_h);
+  horizontal_pass(s_in, s_h);
   __syncthreads();
 
   float own = 0.0f;
   if (threadIdx.x < 3 * kVerticalItems) {
-    const int c = threadIdx.x % kTileSize, g = (threadIdx.x / kTileSize) % kGroups, k = threadIdx.x / kVerticalItems;
+    const int c = threadIdx.x % kLossW, g = (threadIdx.x / kLossW) % kGroupsY, k = threadIdx.x / kVerticalItems;
     const int px = x0 + c, row0 = g * kGroup;
     float m[kGroup][5];
     vertical_sums<5>(s_h, k, c, row0, m);
@@ -268,20 +270,55 @@ __device__ __forceinline__ float target_edge(const uint32_t *target, size_t base
   return fminf(fmaxf(fabsf(laplacian) / 4.0f, 0.0f), 0.999f);
 }
 
+// Dynamic shared memory of k_loss: the nine field planes staged, their
+// horizontal sums, the adjoint's three channels.
+constexpr size_t kLossShared = sizeof(float) * (9 * kStage + 9 * kSpan + 3 * kLossThreads);
+
+// Horizontal window sums of the nine staged field planes into s_h, kGroup
+// outputs per item.
+__device__ __forceinline__ void horizontal_fields(const float (*s_in)[kStage], float (*s_h)[kSpan]) {
+  for (int item = threadIdx.x; item < 3 * kHorizontalItems; item += kLossThreads) {
+    const int k = item / kHorizontalItems, rem = item % kHorizontalItems;
+    const int r = rem / kGroupsX, c = (rem % kGroupsX) * kGroup;
+    const int row = r * kSpanCols + c;
+    float m[kGroup][3];
+#pragma unroll
+    for (int o = 0; o < kGroup; ++o)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) m[o][q] = 0.0f;
+#pragma unroll
+    for (int u = 0; u < kGroup + 10; ++u) {
+      const float v[3] = {s_in[k][row + u], s_in[3 + k][row + u], s_in[6 + k][row + u]};
+#pragma unroll
+      for (int o = 0; o < kGroup; ++o) {
+        const int tap = u - o;
+        if (tap < 0 || tap > 10) continue;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) m[o][q] = fmaf(c_weights[tap], v[q], m[o][q]);
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < kGroup; ++o)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) s_h[q * 3 + k][h_index(r, c + o)] = m[o][q];
+  }
+}
+
 // SCORE (a scored view, train_loss.comp:101-107): the adjoint's alpha gets the
 // pixel's mean absolute error over its three channels, errorMax the view's
 // worst (in 1/65535), edge the target's edge weight.
 template <bool SCORE>
-__global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
-                                                      const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
-                                                      float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials,
-                                                      LossScoring scoring) {
+__global__ void __launch_bounds__(kLossThreads, 3) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
+                                                       const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
+                                                       float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials,
+                                                       LossScoring scoring) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
-  __shared__ float s_in[9][kStage]; // the nine field planes
-  __shared__ float s_h[9][kSpan];
-  __shared__ float s_result[3][kTilePixels];
-  __shared__ float s_warp[kTilePixels / 32];
+  extern __shared__ __align__(16) float s_dynamic[];
+  float(*s_in)[kStage] = reinterpret_cast<float(*)[kStage]>(s_dynamic);
+  float(*s_h)[kSpan] = reinterpret_cast<float(*)[kSpan]>(s_dynamic + 9 * kStage);
+  float(*s_result)[kLossThreads] = reinterpret_cast<float(*)[kLossThreads]>(s_dynamic + 9 * kStage + 9 * kSpan);
+  __shared__ float s_warp[kLossThreads / 32];
   const int tile = blockIdx.x;
   const TileOrigin origin = tile_origin(views, tile);
   const ViewParams &cam = *origin.cam;
@@ -292,7 +329,7 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   // their image and target values are asked for first, so that they arrive
   // while the fields are staged and filtered.
   const bool epilogue = threadIdx.x < 3 * kVerticalItems;
-  const int ec = threadIdx.x % kTileSize, eg = (threadIdx.x / kTileSize) % kGroups, ek = threadIdx.x / kVerticalItems;
+  const int ec = threadIdx.x % kLossW, eg = (threadIdx.x / kLossW) % kGroupsY, ek = threadIdx.x / kVerticalItems;
   float xs[kGroup], ys[kGroup];
 #pragma unroll
   for (int o = 0; o < kGroup; ++o) {
@@ -307,8 +344,8 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
   }
 
 #pragma unroll
-  for (int round = 0; round < (kStage + kTilePixels - 1) / kTilePixels; ++round) {
-    const int i = round * kTilePixels + threadIdx.x;
+  for (int round = 0; round < (kStage + kLossThreads - 1) / kLossThreads; ++round) {
+    const int i = round * kLossThreads + threadIdx.x;
     if (i >= kStage) break;
     const int r = i / kSpanCols, c = i % kSpanCols;
     const int y = y0 + r - kHalo, x = x0 + c - kHalo;
@@ -318,7 +355,7 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
     for (int f = 0; f < 9; ++f) s_in[f][i] = in ? fields[f * plane + at] : 0.0f;
   }
   __syncthreads();
-  horizontal_pass<false>(s_in, s_h);
+  horizontal_fields(s_in, s_h);
   __syncthreads();
 
   float own = 0.0f;
@@ -340,12 +377,12 @@ __global__ void __launch_bounds__(kTilePixels) k_loss(const float4 *__restrict__
         const float ssimPart = m[o][0] + 2.0f * xv * m[o][1] + yv * m[o][2];
         result = ((1.0f - lambda) * sgn - lambda * ssimPart) * perValue;
       }
-      s_result[k][(row0 + o) * kTileSize + c] = result;
+      s_result[k][(row0 + o) * kLossW + c] = result;
     }
   }
   __syncthreads();
   {
-    const int px = x0 + (threadIdx.x & 15), py = y0 + (threadIdx.x >> 4);
+    const int px = x0 + (int)(threadIdx.x % kLossW), py = y0 + (int)(threadIdx.x / kLossW);
     if (px < W && py < H) {
       const size_t pixel = base + (size_t)py * W + px;
       float alpha = 0.0f;
@@ -407,22 +444,40 @@ __global__ void __launch_bounds__(256) k_loss_totals(const float2 *__restrict__ 
 
 } // namespace
 
+// The loss kernels' shared memory is above the static 48 KB: allowed once per
+// process and device.
+void allow_loss_shared() {
+  static std::mutex lock;
+  static std::set<int> done;
+  int device = 0;
+  cudaGetDevice(&device);
+  std::lock_guard<std::mutex> guard(lock);
+  if (done.count(device) != 0) return;
+  cudaFuncSetAttribute(k_ssim, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSsimShared);
+  cudaFuncSetAttribute(k_loss<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLossShared);
+  cudaFuncSetAttribute(k_loss<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLossShared);
+  done.insert(device);
+}
+
 void launch_ssim(const float4 *image, const uint32_t *target, const ViewSet &views, const ViewSet *dViews, float4 *fields, float2 *partials,
                  cudaStream_t stream) {
   if (views.totalLossTiles == 0) return;
-  launch_chained(k_ssim, dim3(views.totalLossTiles), dim3(kTilePixels), 0, stream, image, target, dViews, reinterpret_cast<float *>(fields), partials);
+  allow_loss_shared();
+  launch_chained(k_ssim, dim3(views.totalLossTiles), dim3(kLossThreads), kSsimShared, stream, image, target, dViews,
+                 reinterpret_cast<float *>(fields), partials);
 }
 
 void launch_loss(const float4 *image, const uint32_t *target, const float4 *fields, const ViewSet &views, const ViewSet *dViews, float lambda,
                  float4 *adjoint, float2 *partials, cudaStream_t stream, LossScoring scoring) {
   if (views.totalLossTiles == 0) return;
   const float *f = reinterpret_cast<const float *>(fields);
+  allow_loss_shared();
   if (scoring.edge != nullptr)
-    launch_chained(k_loss<true>, dim3(views.totalLossTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
-                   partials, scoring);
+    launch_chained(k_loss<true>, dim3(views.totalLossTiles), dim3(kLossThreads), kLossShared, stream, image, target, f, dViews, lambda,
+                   adjoint, partials, scoring);
   else
-    launch_chained(k_loss<false>, dim3(views.totalLossTiles), dim3(kTilePixels), 0, stream, image, target, f, dViews, lambda, adjoint,
-                   partials, scoring);
+    launch_chained(k_loss<false>, dim3(views.totalLossTiles), dim3(kLossThreads), kLossShared, stream, image, target, f, dViews, lambda,
+                   adjoint, partials, scoring);
 }
 
 void launch_error_mask(float4 *adjoint, uint32_t pixels, const uint32_t *errorMax, float share, cudaStream_t stream) {

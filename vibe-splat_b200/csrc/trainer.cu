@@ -546,8 +546,8 @@ void Trainer::set_views(const splat_camera *cameras, int count) {
     v.gridH = (int)div_up((uint32_t)c.height, (uint32_t)tile);
     v.tileBase = tileBase;
     v.tileCount = v.gridW * v.gridH;
-    v.lossGridW = (int)div_up((uint32_t)c.width, kTileSize);
-    v.lossGridH = (int)div_up((uint32_t)c.height, kTileSize);
+    v.lossGridW = (int)div_up((uint32_t)c.width, kLossTileW);
+    v.lossGridH = (int)div_up((uint32_t)c.height, kLossTileH);
     v.lossTileBase = lossTileBase;
     v.lossTileCount = v.lossGridW * v.lossGridH;
     lossTileBase += v.lossTileCount;
