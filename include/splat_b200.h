@@ -107,7 +107,7 @@ typedef struct splat_trainer_options {
                                  applies where both rasterizer kernels take two pixels per thread and the sums
                                  are float (not with force_fixed_point or blend_lists); elsewhere the tile stays
                                  16. Images are the same bits either way. */
-  int32_t batch_depth;        /* splats the two-pixel kernels stage per round: 128 or 256 (0 picks 256) */
+  int32_t batch_depth;        /* splats the two-pixel kernels stage per round: 128 or 256 (0 picks 128) */
   int32_t persistent_raster;  /* 1: the two-pixel kernels run as persistent launches, resident blocks taking
                                  the tiles of every view of the step from one counter; 0: one block per tile */
   int32_t grouped_backward;   /* the two-pixel float backward's sums. 0: each splat's twelve sums reduced over

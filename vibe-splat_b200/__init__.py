@@ -452,7 +452,7 @@ class TrainerOptions:
     split_step: bool = False
     blend_lists: bool = False
     tile_size: int = 16
-    batch_depth: int = 256
+    batch_depth: int = 128
     persistent_raster: bool = False
     grouped_backward: bool = False
 

@@ -167,7 +167,7 @@ public:
   bool blendLists = false; // store-everything backward
   int digitBits = 8;
   int forwardPixels = 1, backwardPixels = 2; // pixels per thread of the compositing and float backward kernels
-  int tileSize = 16, batchDepth = 256;        // the two-pixel kernels' tile edge and staging batch
+  int tileSize = 16, batchDepth = 128;        // the two-pixel kernels' tile edge and staging batch
   bool persistent = false;                    // the two-pixel kernels as persistent launches
   bool groupedSums = false;                   // the two-pixel float backward's sums by groups
   DeviceBuffer workCounters;                  // their tile counters (2 words), cleared every step
@@ -350,7 +350,7 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
     throw Failure{SPLAT_ERR_INVALID, "backward_pixels_per_thread must be 1 or 2"};
   tileSize = opt.tile_size == 0 ? 16 : opt.tile_size;
   if (tileSize != 16 && tileSize != 32) throw Failure{SPLAT_ERR_INVALID, "tile_size must be 16 or 32"};
-  batchDepth = opt.batch_depth == 0 ? 256 : opt.batch_depth;
+  batchDepth = opt.batch_depth == 0 ? 128 : opt.batch_depth;
   if (batchDepth != 128 && batchDepth != 256) throw Failure{SPLAT_ERR_INVALID, "batch_depth must be 128 or 256"};
   persistent = opt.persistent_raster != 0;
   groupedSums = opt.grouped_backward != 0;
@@ -1467,7 +1467,7 @@ void splat_trainer_options_default(splat_trainer_options *o) {
   o->forward_pixels_per_thread = 1;
   o->backward_pixels_per_thread = 2;
   o->tile_size = 16;
-  o->batch_depth = 256;
+  o->batch_depth = 128;
   o->persistent_raster = 0;
   o->grouped_backward = 0;
 }
