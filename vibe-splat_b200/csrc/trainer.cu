@@ -176,6 +176,14 @@ public:
   // the first (branches of the same graph when captured).
   cudaStream_t side = nullptr;
   cudaEvent_t forkEvent = nullptr, joinEvent = nullptr, countForkEvent = nullptr, countEvent = nullptr;
+  // The backward's tile order and the loss totals, made on the second stream
+  // beside the loss and the backward.
+  cudaEvent_t orderForkEvent = nullptr, orderEvent = nullptr, totalsForkEvent = nullptr, totalsEvent = nullptr;
+  bool orderPending = false, orderForked = false, totalsPending = false;
+  // Recording a CUDA graph: the forks onto the second stream above cost the
+  // one-launch-at-a-time forms more host time than they save, so only a
+  // captured step makes them.
+  bool capturing = false;
   bool entryScratchClear = false; // the entry sort's scratch was cleared for this step
   // The next step's target on its way to the device: copied to pinned memory
   // and on to targetNext by copyStream while this step runs (copied is
@@ -365,6 +373,10 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   SB_CUDA(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&countForkEvent, cudaEventDisableTiming));
   SB_CUDA(cudaEventCreateWithFlags(&countEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&orderForkEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&orderEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&totalsForkEvent, cudaEventDisableTiming));
+  SB_CUDA(cudaEventCreateWithFlags(&totalsEvent, cudaEventDisableTiming));
   SB_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
   // The persistent launches' tile counters, made here: a step may be recorded
   // into a graph, where nothing may be allocated.
@@ -419,6 +431,8 @@ Trainer::~Trainer() {
   if (joinEvent != nullptr) cudaEventDestroy(joinEvent);
   if (countForkEvent != nullptr) cudaEventDestroy(countForkEvent);
   if (countEvent != nullptr) cudaEventDestroy(countEvent);
+  for (cudaEvent_t e : {orderForkEvent, orderEvent, totalsForkEvent, totalsEvent})
+    if (e != nullptr) cudaEventDestroy(e);
   if (side != nullptr) cudaStreamDestroy(side);
   if (copyStream != nullptr) {
     cudaStreamSynchronize(copyStream);
@@ -753,6 +767,9 @@ RasterConfig Trainer::raster_config() {
 void Trainer::record_prepare(bool backward) {
   const Params p = params();
   SB_CUDA(cudaMemcpyAsync(dViews.get(), hViews.get(), sizeof(ViewSet), cudaMemcpyHostToDevice, stream));
+  // The chain rule's arguments too, here at the start, so that no copy sits
+  // between the backward pass and the chain rule.
+  SB_CUDA(cudaMemcpyAsync(dArgs.get(), hArgs.get(), sizeof(ChainArgs), cudaMemcpyHostToDevice, stream));
   SB_CUDA(cudaMemsetAsync(dReadback.get(), 0, sizeof(StepReadback), stream));
   StepReadback *rb = dReadback.get<StepReadback>();
   uint32_t *counters = rb->counters, *error = &rb->error;
@@ -887,6 +904,23 @@ void Trainer::record_forward() {
       c.tileWork = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + views.totalTiles);
     launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), c, image.get<float4>(),
                    stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
+    if (backwardPixels == 2 && !fixedPoint) {
+      // The backward's tiles, heaviest first (by the entries each walks, as
+      // the two-pixel compositing recorded them, else by the length of their
+      // entry ranges), ordered on the second stream while the loss runs.
+      const uint32_t tiles = (uint32_t)views.totalTiles;
+      uint32_t *extra = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + tiles);
+      cudaStream_t where = stream;
+      if (capturing) {
+        SB_CUDA(cudaEventRecord(orderForkEvent, stream));
+        SB_CUDA(cudaStreamWaitEvent(side, orderForkEvent, 0));
+        where = side;
+      }
+      launch_tile_order(ranges.get<uint2>(), forwardPixels == 2 ? extra : nullptr, tiles, extra + tiles, where);
+      if (capturing) SB_CUDA(cudaEventRecord(orderEvent, side));
+      orderPending = true;
+      orderForked = capturing;
+    }
   }
   end(4);
 }
@@ -909,7 +943,15 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
               adjoint.get<float4>(), partials.get<float2>(), stream, scoring);
   if (scoreShare > 0.0f)
     launch_error_mask(adjoint.get<float4>(), (uint32_t)views.totalPixels, scoreMax.get<uint32_t>(), scoreShare, stream);
-  launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, stream);
+  // The FP64 totals; in a captured step on the second stream beside the
+  // backward pass (only the step's read-back needs them).
+  totalsPending = capturing;
+  if (totalsPending) {
+    SB_CUDA(cudaEventRecord(totalsForkEvent, stream));
+    SB_CUDA(cudaStreamWaitEvent(side, totalsForkEvent, 0));
+  }
+  launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, totalsPending ? side : stream);
+  if (totalsPending) SB_CUDA(cudaEventRecord(totalsEvent, side));
   end(5);
   const RasterConfig cfg = raster_config();
   const uint32_t *vals = entriesInTmp ? tmpEntryValues.get<uint32_t>() : entryValues.get<uint32_t>();
@@ -924,13 +966,10 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
                           error, stream);
   } else {
     RasterConfig c = cfg;
-    if (backwardPixels == 2 && !fixedPoint) {
-      // Heaviest tiles first, by the entries each walks (recorded by the
-      // two-pixel compositing), else by the length of their entry ranges.
-      const uint32_t tiles = (uint32_t)views.totalTiles;
-      uint32_t *extra = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + tiles);
-      launch_tile_order(ranges.get<uint2>(), forwardPixels == 2 ? extra : nullptr, tiles, extra + tiles, stream);
-      c.orderBackward = extra + tiles;
+    if (orderPending) {
+      if (orderForked) SB_CUDA(cudaStreamWaitEvent(stream, orderEvent, 0));
+      c.orderBackward = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + views.totalTiles) + views.totalTiles;
+      orderPending = orderForked = false;
     }
     launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), c, image.get<float4>(),
                     adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
@@ -941,7 +980,6 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   std::memcpy(&args, hArgs.get(), sizeof(ChainArgs));
   (void)mode;
   (void)statistics;
-  SB_CUDA(cudaMemcpyAsync(dArgs.get(), hArgs.get(), sizeof(ChainArgs), cudaMemcpyHostToDevice, stream));
   OptimState st = optim_state();
   // The geometry gradients always pass through these buffers on their way to
   // Adam; compute_gradients() also keeps the SH ones there.
@@ -952,6 +990,10 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
                shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
   end(7);
+  if (totalsPending) {
+    SB_CUDA(cudaStreamWaitEvent(stream, totalsEvent, 0));
+    totalsPending = false;
+  }
 }
 
 void Trainer::record_readback() {
@@ -1052,12 +1094,15 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
       if (it == graphs.end()) {
         cudaGraph_t graph = nullptr;
         SB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
         try {
           record_prepare(true);
           record_forward();
           record_backward_and_chain(mode, statistics);
           record_readback();
+          capturing = false;
         } catch (...) {
+          capturing = false;
           cudaStreamEndCapture(stream, &graph);
           if (graph != nullptr) cudaGraphDestroy(graph);
           throw;
@@ -1364,6 +1409,11 @@ void Trainer::render(const splat_camera *camera, float *out) {
   timing = false;
   record_forward();
   timing = wasTiming;
+  if (orderPending) {
+    // No backward pass follows a render: take the order's stream back.
+    if (orderForked) SB_CUDA(cudaStreamWaitEvent(stream, orderEvent, 0));
+    orderPending = orderForked = false;
+  }
   record_readback();
   SB_CUDA(cudaStreamSynchronize(stream));
   if (hReadback.get<StepReadback>()->error != 0u) throw Failure{SPLAT_ERR_DEVICE, "device check failed during render"};
