@@ -519,8 +519,10 @@ int splat_trainer_device_parameters(splat_trainer *trainer, int32_t group, uint6
  * blend_lists only, else empty), 14-18 the Adam state of parameter groups 0-4
  * (positions, scales, rotations, opacities, SH; u32 words: BF16 pairs, or FP32
  * m values then v values; SH state in rows of 3 (degree + 1)^2 words per
- * Gaussian rounded up to a multiple of 4, the row count rounded up to 128). Copies min(bytes, size) bytes; *size gets the
- * buffer's size in bytes. */
+ * Gaussian rounded up to a multiple of 4, the row count rounded up to 128), 19 the two-pixel backward's
+ * tile schedule (u32 per tile: the entries each tile's backward walks, as the two-pixel compositing
+ * recorded them, then the order the backward took the tiles in). Copies min(bytes, size) bytes; *size
+ * gets the buffer's size in bytes. */
 int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *out, size_t bytes, size_t *size);
 
 /* 3DGS .ply files (src/splat/gaussian_cloud.hpp:60-67, load_ply and

@@ -441,6 +441,37 @@ def test_tile_batch_and_launch_forms_agree(splat, oracle, exact):
                                 f"{name} t{tile} b{batch} p{int(persistent)} g{int(grouped)}", 0.99999, 1e-4)
 
 
+@pytest.mark.parametrize("tile,persistent", [(16, False), (32, True)])
+def test_backward_takes_the_heaviest_tiles_first(splat, oracle, tile, persistent):
+    # The two-pixel compositing records, per tile, the entries its backward
+    # walks (range end minus the least stop of the tile's pixels); the
+    # backward takes the tiles in half-octave classes of that work, heaviest
+    # first: every tile once, and a later tile never more than a class above
+    # an earlier one (sqrt 2, plus slack for the SFU log2 at class edges).
+    view = oracle.train_camera(150, 100)
+    target = oracle.smooth_target(150, 100, 6)
+    cloud = oracle.random_cloud(4000, 1, 41)
+    t = splat.Trainer(to_cloud(cloud), splat.TrainerOptions(exact_math=False, forward_pixels_per_thread=2,
+                                                            backward_pixels_per_thread=2, tile_size=tile,
+                                                            persistent_raster=persistent))
+    t.compute_gradients(to_camera(view), target)
+    gw, gh = -(-150 // tile), -(-100 // tile)
+    tiles = gw * gh
+    schedule = t.debug_download(splat.DEBUG_TILE_SCHEDULE, np.uint32)[: 2 * tiles]
+    work, order = schedule[:tiles], schedule[tiles:]
+    assert np.array_equal(np.sort(order), np.arange(tiles, dtype=np.uint32))
+    ranges = t.debug_download(splat.DEBUG_RANGES, np.uint32)[: 2 * tiles].reshape(tiles, 2)
+    stops = t.debug_download(splat.DEBUG_STOPS, np.uint32)[: 150 * 100].reshape(100, 150)
+    for k in range(tiles):
+        ty, tx = divmod(k, gw)
+        least = stops[ty * tile:(ty + 1) * tile, tx * tile:(tx + 1) * tile].min()
+        assert work[k] == ranges[k, 1] - min(least, ranges[k, 1]), k
+    walked = work[order].astype(np.float64)
+    assert walked.max() > 0
+    lightest = np.minimum.accumulate(walked)
+    assert (walked[1:] <= 1.5 * lightest[:-1] + 1.0).all()
+
+
 def test_batched_persistent_matches_single_views(splat, oracle):
     # Several views of uneven size in one persistent launch per stage, 32 x 32
     # tiles: each view's loss equals that view's alone (the same tiles, lists

@@ -616,6 +616,7 @@ DEBUG_SPLATS, DEBUG_REACH, DEBUG_DEPTH_KEYS, DEBUG_ENTRY_KEYS, DEBUG_ENTRY_VALUE
 DEBUG_IMAGE, DEBUG_STOPS, DEBUG_ADJOINT, DEBUG_RAW, DEBUG_COUNTERS, DEBUG_PARTIALS, DEBUG_ERROR = range(6, 13)
 DEBUG_BLEND_COUNTS = 13
 DEBUG_STATE = 14  # + parameter group 0..4
+DEBUG_TILE_SCHEDULE = 19  # per tile: the backward's walk length, then its tile order
 
 
 def _target_ptr(target) -> tuple:

@@ -2719,6 +2719,10 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     case 11: src = t->partials.get(); have = (size_t)t->views.totalLossTiles * 8; break;
     case 12: src = &rb->error; have = 4; break;
     case 13: src = t->listCounts.get(); have = t->blendLists ? (size_t)t->views.totalPixels * 4 : 0; break;
+    case 19:
+      src = t->ranges.get<uint2>() + t->views.totalTiles;
+      have = (size_t)t->views.totalTiles * 8;
+      break;
     case 14: case 15: case 16: case 17: case 18: {
       const size_t g = t->n;
       const size_t counts[5] = {g * 3, g * 3, g * 4, g, (size_t)t->planeStride * sb::sh_state_stride(t->shCoeffs)};
