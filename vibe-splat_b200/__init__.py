@@ -394,13 +394,11 @@ class Camera:
     height: int = 1
 
     def _c(self) -> _Camera:
+        # Whole-array assignments: a step spends no more host time here than
+        # it must (the GPU waits on the host between synchronous steps).
         c = _Camera()
-        view = np.asarray(self.view, dtype=np.float32)
-        for col in range(4):
-            for row in range(4):
-                c.view[col * 4 + row] = float(view[row, col])
-        for a in range(3):
-            c.position[a] = float(self.position[a])
+        c.view[:] = np.asarray(self.view, dtype=np.float32).T.reshape(16).tolist()  # column-major
+        c.position[:] = np.asarray(self.position, dtype=np.float32).reshape(-1)[:3].tolist()
         c.fx, c.fy, c.cx, c.cy = float(self.fx), float(self.fy), float(self.cx), float(self.cy)
         c.width, c.height = int(self.width), int(self.height)
         return c
