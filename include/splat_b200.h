@@ -207,7 +207,8 @@ int splat_trainer_step(splat_trainer *trainer, const splat_camera *camera, const
                        const splat_learning_rates *rates, const uint8_t *next_target, size_t next_target_bytes,
                        splat_step_stats *stats);
 /* Trainer::step with the target already in device memory (device_target is a
- * device pointer of width * height * 4 bytes, read during the call). For
+ * device pointer of width * height * 4 bytes, read during the call: the loss
+ * reads it where it is, without a copy, when it is 4-byte aligned). For
  * callers that keep their photos resident in HBM. New in this library. */
 int splat_trainer_step_device_target(splat_trainer *trainer, const splat_camera *camera, const uint8_t *device_target,
                                      size_t target_bytes, const splat_learning_rates *rates, splat_step_stats *stats);

@@ -22,6 +22,10 @@ struct ViewSet {
   long long totalPixels;
   int tileSize;
   int totalLossTiles;
+  // A one-view step on a target already in device memory reads it where the
+  // caller keeps it (RGBA8, the view's width x height); null: the trainer's
+  // own target buffer.
+  const uint32_t *target;
 };
 
 // SH storage of the coefficients above degree 0 (the DC term is always FP32).

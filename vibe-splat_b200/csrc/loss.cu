@@ -175,11 +175,12 @@ __device__ __forceinline__ TileOrigin tile_origin(const ViewSet &views, int tile
 // the horizontal sums x, y, x^2, y^2, xy, three channels each.
 constexpr size_t kSsimShared = sizeof(float) * (6 * kStage + 15 * kSpan);
 
-__global__ void __launch_bounds__(kLossThreads, 3) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
+__global__ void __launch_bounds__(kLossThreads, 3) k_ssim(const float4 *__restrict__ image, const uint32_t *__restrict__ targetBuffer,
                                                        const ViewSet *__restrict__ viewsPtr, float *__restrict__ fields,
                                                        float2 *__restrict__ partials) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
+  const uint32_t *__restrict__ target = views.target != nullptr ? views.target : targetBuffer;
   extern __shared__ __align__(16) float s_dynamic[];
   float(*s_in)[kStage] = reinterpret_cast<float(*)[kStage]>(s_dynamic);
   float(*s_h)[kSpan] = reinterpret_cast<float(*)[kSpan]>(s_dynamic + 6 * kStage);
@@ -308,12 +309,13 @@ __device__ __forceinline__ void horizontal_fields(const float (*s_in)[kStage], f
 // pixel's mean absolute error over its three channels, errorMax the view's
 // worst (in 1/65535), edge the target's edge weight.
 template <bool SCORE>
-__global__ void __launch_bounds__(kLossThreads, 3) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ target,
+__global__ void __launch_bounds__(kLossThreads, 3) k_loss(const float4 *__restrict__ image, const uint32_t *__restrict__ targetBuffer,
                                                        const float *__restrict__ fields, const ViewSet *__restrict__ viewsPtr,
                                                        float lambda, float4 *__restrict__ adjoint, float2 *__restrict__ partials,
                                                        LossScoring scoring) {
   chain_enter();
   const ViewSet &views = *viewsPtr;
+  const uint32_t *__restrict__ target = views.target != nullptr ? views.target : targetBuffer;
   extern __shared__ __align__(16) float s_dynamic[];
   float(*s_in)[kStage] = reinterpret_cast<float(*)[kStage]>(s_dynamic);
   float(*s_h)[kSpan] = reinterpret_cast<float(*)[kSpan]>(s_dynamic + 9 * kStage);

@@ -222,8 +222,20 @@ public:
   // Store-everything variant: per-pixel blend counts, list offsets, the list pool, scan scratch and counters.
   DeviceBuffer listCounts, listOffsets, listPool, listScratch, listCounters;
   // Small things.
-  DeviceBuffer dViews, dArgs, dReadback, sortScratchDepth, sortScratchEntries, scanScratch;
-  PinnedBuffer hViews, hArgs, hReadback, staging, stagingNext;
+  // The step's small device inputs and outputs in one block, the views, the
+  // chain rule's arguments, then the read-back, so that one copy from the
+  // pinned block of the same layout (whose read-back part stays zero) sets
+  // the first two and clears the third at the start of a step.
+  DeviceBuffer dStep, sortScratchDepth, sortScratchEntries, scanScratch;
+  PinnedBuffer hStep, hReadback, staging, stagingNext;
+  static constexpr size_t kArgsAt = (sizeof(ViewSet) + 255) / 256 * 256;
+  static constexpr size_t kReadbackAt = kArgsAt + (sizeof(ChainArgs) + 255) / 256 * 256;
+  static constexpr size_t kStepBytes = kReadbackAt + sizeof(StepReadback);
+  ViewSet *d_views() const { return dStep.get<ViewSet>(); }
+  ChainArgs *d_args() const { return reinterpret_cast<ChainArgs *>(dStep.get<unsigned char>() + kArgsAt); }
+  StepReadback *d_readback() const { return reinterpret_cast<StepReadback *>(dStep.get<unsigned char>() + kReadbackAt); }
+  ViewSet *h_views() const { return hStep.get<ViewSet>(); }
+  ChainArgs *h_args() const { return reinterpret_cast<ChainArgs *>(hStep.get<unsigned char>() + kArgsAt); }
   const uint8_t *prefetched = nullptr;
   size_t prefetchedBytes = 0;
   const uint8_t *pendingPrefetch = nullptr; // the next step's target, copied during this step
@@ -414,11 +426,9 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   for (int g = 0; g < 4; ++g) grads[g].ensure(groupCounts[g] * 4);
   densifyStats.ensure(nn * kStatStride * 4);
   SB_CUDA(cudaMemset(densifyStats.get(), 0, nn * kStatStride * 4));
-  dViews.ensure(sizeof(ViewSet));
-  dArgs.ensure(sizeof(ChainArgs));
-  dReadback.ensure(sizeof(StepReadback));
-  hViews.ensure(sizeof(ViewSet));
-  hArgs.ensure(sizeof(ChainArgs));
+  dStep.ensure(kStepBytes);
+  hStep.ensure(kStepBytes);
+  std::memset(hStep.get(), 0, kStepBytes);
   hReadback.ensure(sizeof(StepReadback));
 }
 
@@ -766,12 +776,11 @@ RasterConfig Trainer::raster_config() {
 
 void Trainer::record_prepare(bool backward) {
   const Params p = params();
-  SB_CUDA(cudaMemcpyAsync(dViews.get(), hViews.get(), sizeof(ViewSet), cudaMemcpyHostToDevice, stream));
-  // The chain rule's arguments too, here at the start, so that no copy sits
-  // between the backward pass and the chain rule.
-  SB_CUDA(cudaMemcpyAsync(dArgs.get(), hArgs.get(), sizeof(ChainArgs), cudaMemcpyHostToDevice, stream));
-  SB_CUDA(cudaMemsetAsync(dReadback.get(), 0, sizeof(StepReadback), stream));
-  StepReadback *rb = dReadback.get<StepReadback>();
+  // The views, the chain rule's arguments (here at the start, so that no
+  // copy sits between the backward pass and the chain rule) and a cleared
+  // read-back, in one copy.
+  SB_CUDA(cudaMemcpyAsync(dStep.get(), hStep.get(), kStepBytes, cudaMemcpyHostToDevice, stream));
+  StepReadback *rb = d_readback();
   uint32_t *counters = rb->counters, *error = &rb->error;
   // What the step clears, cleared on the second stream while the projection
   // runs: the backward pass's sums (not for a render, which keeps the last
@@ -792,7 +801,7 @@ void Trainer::record_prepare(bool backward) {
   }
   SB_CUDA(cudaEventRecord(joinEvent, side));
   begin(0);
-  launch_preprocess(p, views, dViews.get<ViewSet>(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
+  launch_preprocess(p, views, d_views(), splats.get<Splat>(), reach.get<float>(), depthKeys.get<uint32_t>(),
                     oneSort ? nullptr : values.get<uint32_t>(), stream, error);
   end(0);
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
@@ -811,7 +820,7 @@ void Trainer::record_prepare(bool backward) {
     // passes (one to two blocks per SM each) room beside them: measured at
     // 1M splats, 1.509 ms a step against 1.519 with one block per chunk of
     // splats and 1.544 with two per SM.
-    launch_bin_count(splats.get<Splat>(), reach.get<float>(), nullptr, nullptr, n, n, views, dViews.get<ViewSet>(),
+    launch_bin_count(splats.get<Splat>(), reach.get<float>(), nullptr, nullptr, n, n, views, d_views(),
                      countsBySplat, masks, counters, side, 3u);
     SB_CUDA(cudaEventRecord(countEvent, side));
   }
@@ -830,20 +839,20 @@ void Trainer::record_prepare(bool backward) {
     SB_CUDA(cudaStreamWaitEvent(stream, countEvent, 0));
     launch_offsets_scan(items, countsBySplat, itemSplat, offs, counters, entryCapacity, scanScratch.get(), error, stream, false);
   } else {
-    launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(), offs,
+    launch_bin_count_scan(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, d_views(), offs,
                           masks, counters, entryCapacity, scanScratch.get(), error, stream);
   }
   end(2);
 }
 
 void Trainer::record_forward() {
-  StepReadback *rb = dReadback.get<StepReadback>();
+  StepReadback *rb = d_readback();
   uint32_t *counters = rb->counters, *error = &rb->error;
   const uint32_t *itemKeys = oneSort ? depthKeys.get<uint32_t>() : (depthInTmp ? tmpKeys.get<uint32_t>() : depthKeys.get<uint32_t>());
   const uint32_t *itemSplat = oneSort ? nullptr : (depthInTmp ? tmpValues.get<uint32_t>() : values.get<uint32_t>());
   const uint32_t items = oneSort ? n * (uint32_t)views.count : n;
   begin(3);
-  launch_bin_emit(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, dViews.get<ViewSet>(),
+  launch_bin_emit(splats.get<Splat>(), reach.get<float>(), itemKeys, itemSplat, items, n, views, d_views(),
                   offsets.get<uint32_t>(), offsets.get<uint32_t>() + items, countOverlap, entryCapacity,
                   oneSort ? nullptr : entryKeys.get<uint32_t>(),
                   oneSort ? entryKeys.get<unsigned long long>() : nullptr, entryValues.get<uint32_t>(), error, stream);
@@ -875,7 +884,7 @@ void Trainer::record_forward() {
     // the lists.
     BlendLists lists;
     lists.counts = listCounts.get<uint32_t>();
-    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, d_views(), cfg, image.get<float4>(),
                    stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream, 1, lists);
     const size_t pixels = (size_t)views.totalPixels;
     SB_CUDA(cudaMemcpyAsync(listOffsets.get(), listCounts.get(), pixels * 4, cudaMemcpyDeviceToDevice, stream));
@@ -891,7 +900,7 @@ void Trainer::record_forward() {
     }
     lists.offsets = listOffsets.get<uint32_t>();
     lists.pool = listPool.get<uint2>();
-    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, d_views(), cfg, image.get<float4>(),
                    stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream, 2, lists);
   } else {
     RasterConfig c = cfg;
@@ -902,7 +911,7 @@ void Trainer::record_forward() {
     // they stop is not known before it runs.)
     if (forwardPixels == 2 && backwardPixels == 2 && !fixedPoint)
       c.tileWork = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + views.totalTiles);
-    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), c, image.get<float4>(),
+    launch_forward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, d_views(), c, image.get<float4>(),
                    stops.get<uint32_t>(), n * (uint32_t)views.count, error, stream);
     if (backwardPixels == 2 && !fixedPoint) {
       // The backward's tiles, heaviest first (by the entries each walks, as
@@ -926,10 +935,10 @@ void Trainer::record_forward() {
 }
 
 void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
-  StepReadback *rb = dReadback.get<StepReadback>();
+  StepReadback *rb = d_readback();
   uint32_t *error = &rb->error;
   begin(5);
-  launch_ssim(image.get<float4>(), target.get<uint32_t>(), views, dViews.get<ViewSet>(), fields.get<float4>(),
+  launch_ssim(image.get<float4>(), target.get<uint32_t>(), views, d_views(), fields.get<float4>(),
               partials.get<float2>(), stream);
   LossScoring scoring;
   if (scoreShare > 0.0f) {
@@ -939,7 +948,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
     scoring.edge = scoreEdge.get<float>();
     scoring.errorMax = scoreMax.get<uint32_t>();
   }
-  launch_loss(image.get<float4>(), target.get<uint32_t>(), fields.get<float4>(), views, dViews.get<ViewSet>(), opt.lambda_ssim,
+  launch_loss(image.get<float4>(), target.get<uint32_t>(), fields.get<float4>(), views, d_views(), opt.lambda_ssim,
               adjoint.get<float4>(), partials.get<float2>(), stream, scoring);
   if (scoreShare > 0.0f)
     launch_error_mask(adjoint.get<float4>(), (uint32_t)views.totalPixels, scoreMax.get<uint32_t>(), scoreShare, stream);
@@ -950,7 +959,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
     SB_CUDA(cudaEventRecord(totalsForkEvent, stream));
     SB_CUDA(cudaStreamWaitEvent(side, totalsForkEvent, 0));
   }
-  launch_loss_totals(partials.get<float2>(), views, dViews.get<ViewSet>(), &rb->totals, totalsPending ? side : stream);
+  launch_loss_totals(partials.get<float2>(), views, d_views(), &rb->totals, totalsPending ? side : stream);
   if (totalsPending) SB_CUDA(cudaEventRecord(totalsEvent, side));
   end(5);
   const RasterConfig cfg = raster_config();
@@ -961,7 +970,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
     lists.counts = listCounts.get<uint32_t>();
     lists.offsets = listOffsets.get<uint32_t>();
     lists.pool = listPool.get<uint2>();
-    launch_backward_lists(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), cfg, image.get<float4>(),
+    launch_backward_lists(splats.get<Splat>(), vals, ranges.get<uint2>(), views, d_views(), cfg, image.get<float4>(),
                           adjoint.get<float4>(), stops.get<uint32_t>(), lists, raw.get<float>(), n * (uint32_t)views.count,
                           error, stream);
   } else {
@@ -971,13 +980,13 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
       c.orderBackward = reinterpret_cast<uint32_t *>(ranges.get<uint2>() + views.totalTiles) + views.totalTiles;
       orderPending = orderForked = false;
     }
-    launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, dViews.get<ViewSet>(), c, image.get<float4>(),
+    launch_backward(splats.get<Splat>(), vals, ranges.get<uint2>(), views, d_views(), c, image.get<float4>(),
                     adjoint.get<float4>(), stops.get<uint32_t>(), fixedPoint, raw.get(), n * (uint32_t)views.count, error,
                     stream, scoreShare > 0.0f ? scoreEdge.get<float>() : nullptr);
   }
   end(6);
   ChainArgs args{};
-  std::memcpy(&args, hArgs.get(), sizeof(ChainArgs));
+  std::memcpy(&args, h_args(), sizeof(ChainArgs));
   (void)mode;
   (void)statistics;
   OptimState st = optim_state();
@@ -987,7 +996,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
   for (int k = 0; k < 5; ++k) g.g[k] = grads[k].get<float>();
   const GradientsOut *gp = &g;
   begin(7);
-  launch_chain(params(), views, dViews.get<ViewSet>(), raw.get(), splats.get<Splat>(), args, dArgs.get<ChainArgs>(), st, gp,
+  launch_chain(params(), views, d_views(), raw.get(), splats.get<Splat>(), args, d_args(), st, gp,
                shGrad.get<float4>(), densifyStats.get<float>(), error, stream);
   end(7);
   if (totalsPending) {
@@ -997,7 +1006,7 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
 }
 
 void Trainer::record_readback() {
-  SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+  SB_CUDA(cudaMemcpyAsync(hReadback.get(), d_readback(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
 }
 
 void Trainer::fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates) {
@@ -1032,7 +1041,7 @@ void Trainer::fill_chain_args(ChainMode mode, bool statistics, const splat_learn
       }
     }
   }
-  std::memcpy(hArgs.get(), &a, sizeof(ChainArgs));
+  std::memcpy(h_args(), &a, sizeof(ChainArgs));
   lastArgs = a;
 }
 
@@ -1065,10 +1074,17 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
   if (count > 1 && !oneSort) throw Failure{SPLAT_ERR_UNSUPPORTED, "several views per step need sort_form SPLAT_SORT_TILE_DEPTH_64"};
   if (count > 1 && blendLists) throw Failure{SPLAT_ERR_UNSUPPORTED, "blend lists are for one view per step"};
   ensure_view_buffers();
-  std::memcpy(hViews.get(), &views, sizeof(ViewSet));
+  // One view on a device target: the loss reads it where it is, no copy.
+  const bool targetInPlace = deviceTargets && count == 1 && targets[0] != nullptr &&
+                             bytes[0] == (size_t)views.v[0].width * views.v[0].height * 4 &&
+                             reinterpret_cast<uintptr_t>(targets[0]) % 4 == 0;
+  views.target = targetInPlace ? reinterpret_cast<const uint32_t *>(targets[0]) : nullptr;
+  std::memcpy(h_views(), &views, sizeof(ViewSet));
   fill_chain_args(mode, statistics, rates);
   // The targets reach the device before the step's launches (and outside the graph).
-  if (deviceTargets) {
+  if (targetInPlace) {
+    // Nothing to copy: the loss reads views.target.
+  } else if (deviceTargets) {
     size_t off = 0;
     for (int k = 0; k < count; ++k) {
       const size_t want = (size_t)views.v[k].width * views.v[k].height * 4;
@@ -1129,15 +1145,15 @@ void Trainer::run(const splat_camera *cameras, const uint8_t *const *targets, co
   } else {
     record_prepare(true);
     // The reference's host wait: read the entry count and size the entry buffers.
-    SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+    SB_CUDA(cudaMemcpyAsync(hReadback.get(), d_readback(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
     SB_CUDA(cudaStreamSynchronize(stream));
     const uint32_t total = hReadback.get<StepReadback>()->counters[1];
     if (total > entryCapacity || entryKeys.get() == nullptr) {
       ensure_entries(total);
       // The count-and-scan pass wrote the clipped count for the old capacity.
       const uint32_t fix[2] = {total, total};
-      SB_CUDA(cudaMemcpyAsync(&dReadback.get<StepReadback>()->counters[1], fix, sizeof(fix), cudaMemcpyHostToDevice, stream));
-      uint32_t *err = &dReadback.get<StepReadback>()->error;
+      SB_CUDA(cudaMemcpyAsync(&d_readback()->counters[1], fix, sizeof(fix), cudaMemcpyHostToDevice, stream));
+      uint32_t *err = &d_readback()->error;
       SB_CUDA(cudaMemsetAsync(err, 0, 4, stream));
       SB_CUDA(cudaStreamSynchronize(stream));
     }
@@ -1394,16 +1410,16 @@ void Trainer::autotune(const splat_camera *camera, const uint8_t *target, size_t
 void Trainer::render(const splat_camera *camera, float *out) {
   set_views(camera, 1);
   ensure_view_buffers();
-  std::memcpy(hViews.get(), &views, sizeof(ViewSet));
+  std::memcpy(h_views(), &views, sizeof(ViewSet));
   record_prepare(false);
-  SB_CUDA(cudaMemcpyAsync(hReadback.get(), dReadback.get(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+  SB_CUDA(cudaMemcpyAsync(hReadback.get(), d_readback(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
   SB_CUDA(cudaStreamSynchronize(stream));
   const uint32_t total = hReadback.get<StepReadback>()->counters[1];
   if (total > entryCapacity || entryKeys.get() == nullptr) {
     ensure_entries(total);
     const uint32_t fix[2] = {total, total};
-    SB_CUDA(cudaMemcpyAsync(&dReadback.get<StepReadback>()->counters[1], fix, sizeof(fix), cudaMemcpyHostToDevice, stream));
-    SB_CUDA(cudaMemsetAsync(&dReadback.get<StepReadback>()->error, 0, 4, stream));
+    SB_CUDA(cudaMemcpyAsync(&d_readback()->counters[1], fix, sizeof(fix), cudaMemcpyHostToDevice, stream));
+    SB_CUDA(cudaMemsetAsync(&d_readback()->error, 0, 4, stream));
   }
   const bool wasTiming = timing;
   timing = false;
@@ -1615,12 +1631,12 @@ int splat_trainer_apply_gradients(splat_trainer *trainer, const splat_learning_r
     if (rates->trust_region != 0.f) throw Failure{SPLAT_ERR_UNSUPPORTED, "second-order steps have no kernel in this library"};
     if (!t->haveRaw) throw Failure{SPLAT_ERR_STATE, "no gradients: compute_gradients() leaves the sums apply_gradients() uses"};
     t->fill_chain_args(sb::ChainMode::Step, false, rates);
-    SB_CUDA(cudaMemcpyAsync(t->dArgs.get(), t->hArgs.get(), sizeof(sb::ChainArgs), cudaMemcpyHostToDevice, t->stream));
+    SB_CUDA(cudaMemcpyAsync(t->d_args(), t->h_args(), sizeof(sb::ChainArgs), cudaMemcpyHostToDevice, t->stream));
     sb::OptimState st = t->optim_state();
     sb::GradientsOut g{};
     for (int k = 0; k < 5; ++k) g.g[k] = t->grads[k].get<float>();
-    sb::launch_chain(t->params(), t->views, t->dViews.get<sb::ViewSet>(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
-                     t->dArgs.get<sb::ChainArgs>(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
+    sb::launch_chain(t->params(), t->views, t->d_views(), t->raw.get(), t->splats.get<sb::Splat>(), t->lastArgs,
+                     t->d_args(), st, &g, t->shGrad.get<float4>(), t->densifyStats.get<float>(), nullptr,
                      t->stream);
     SB_CUDA(cudaStreamSynchronize(t->stream));
   });
@@ -2686,7 +2702,7 @@ int splat_trainer_debug_download(splat_trainer *trainer, int32_t which, void *ou
     const size_t items = (size_t)t->n * std::max(t->views.count, 1);
     const void *src = nullptr;
     size_t have = 0;
-    sb::StepReadback *rb = t->dReadback.get<sb::StepReadback>();
+    sb::StepReadback *rb = t->d_readback();
     switch (which) {
     case 0: src = t->splats.get(); have = items * sizeof(sb::Splat); break;
     case 1: src = t->reach.get(); have = items * 4; break;
