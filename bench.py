@@ -852,9 +852,13 @@ def our_arm(args) -> None:
         trainer = splat.Trainer(cloud, options)
         stream = trainer.stream()
 
+        # The targets' device addresses, looked up once: the loop does no
+        # tensor indexing between the (synchronous) steps.
+        target_ptrs = [device_targets[k].data_ptr() for k in range(len(cams))]
+
         def resident(i):
             k = i % len(cams)
-            return trainer.step_device_target(cams[k], device_targets[k].data_ptr(), rates)
+            return trainer.step_device_target(cams[k], target_ptrs[k], rates)
 
         if tune:
             # The autotuner picks the sort form and digit width (gradient passes, no parameter change).
