@@ -912,3 +912,37 @@ def test_device_target_entry_points_match_the_host_ones(splat, oracle):
     np.testing.assert_array_equal(out[0][0], out[1][0])
     for name in ("positions", "scales", "opacities", "sh"):
         np.testing.assert_array_equal(getattr(out[0][1], name), getattr(out[1][1], name), name)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_step_on_a_device_target_matches_the_host_target(splat, oracle, graph):
+    # A one-view step reads a device target where it is (4-byte aligned) or
+    # copies it (any other address); either way the steps equal those on
+    # the host target, bit for bit with fixed-point sums, graph or not.
+    import torch
+
+    view = oracle.train_camera(90, 70)
+    target = oracle.smooth_target(90, 70, 4)
+    cloud = oracle.random_cloud(1500, 1, 29)
+    opts = splat.TrainerOptions(force_fixed_point=True, use_graph=graph)
+    rates = splat.LearningRates(position=1e-3)
+    size = target.size
+    padded = torch.zeros(size + 1, dtype=torch.uint8, device="cuda")
+    padded[1:] = torch.from_numpy(target.reshape(-1)).cuda()
+    aligned = torch.from_numpy(target.reshape(-1)).cuda()
+    results = []
+    for where in ("host", "aligned", "unaligned"):
+        t = splat.Trainer(to_cloud(cloud), opts)
+        losses = []
+        for _ in range(3):
+            if where == "host":
+                losses.append(t.step(to_camera(view), target, rates).loss)
+            elif where == "aligned":
+                losses.append(t.step_device_target(to_camera(view), aligned.data_ptr(), rates).loss)
+            else:
+                losses.append(t.step_device_target(to_camera(view), padded.data_ptr() + 1, rates).loss)
+        results.append((losses, t.cloud()))
+    for losses, c in results[1:]:
+        assert losses == results[0][0]
+        for name in ("positions", "scales", "rotations", "opacities", "sh"):
+            np.testing.assert_array_equal(getattr(c, name), getattr(results[0][1], name), name)
