@@ -131,6 +131,15 @@ struct StepReadback {
   LossTotals totals;
 };
 
+// The step's read-back written by a kernel straight into the pinned host
+// block (mapped into the device's address space), after the step's last
+// kernel: no copy node after the step, and the stream synchronisation that
+// follows makes the writes visible to the host.
+__global__ void __launch_bounds__(64) k_readback(const uint32_t *__restrict__ src, uint32_t *dst, uint32_t words) {
+  chain_enter();
+  for (uint32_t i = threadIdx.x; i < words; i += 64u) dst[i] = src[i];
+}
+
 constexpr int kStages = 8;
 const char *const kStageNames[kStages] = {"project", "depth sort", "count tiles", "tile lists",
                                           "composite", "loss", "backward", "chain rule and step"};
@@ -228,6 +237,7 @@ public:
   // the first two and clears the third at the start of a step.
   DeviceBuffer dStep, sortScratchDepth, sortScratchEntries, scanScratch;
   PinnedBuffer hStep, hReadback, staging, stagingNext;
+  void *hReadbackDevice = nullptr;
   static constexpr size_t kArgsAt = (sizeof(ViewSet) + 255) / 256 * 256;
   static constexpr size_t kReadbackAt = kArgsAt + (sizeof(ChainArgs) + 255) / 256 * 256;
   static constexpr size_t kStepBytes = kReadbackAt + sizeof(StepReadback);
@@ -430,6 +440,12 @@ Trainer::Trainer(const splat_cloud &cloud, const splat_trainer_options &options,
   hStep.ensure(kStepBytes);
   std::memset(hStep.get(), 0, kStepBytes);
   hReadback.ensure(sizeof(StepReadback));
+  // The read-back's address on the device side of the pinned block (null
+  // where the block is not mapped: the read-back is then copied).
+  if (cudaHostGetDevicePointer(&hReadbackDevice, hReadback.get(), 0) != cudaSuccess) {
+    cudaGetLastError();
+    hReadbackDevice = nullptr;
+  }
 }
 
 Trainer::~Trainer() {
@@ -1006,7 +1022,14 @@ void Trainer::record_backward_and_chain(ChainMode mode, bool statistics) {
 }
 
 void Trainer::record_readback() {
-  SB_CUDA(cudaMemcpyAsync(hReadback.get(), d_readback(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+  static_assert(sizeof(StepReadback) % 4 == 0, "the read-back goes as words");
+  if (hReadbackDevice == nullptr) {
+    SB_CUDA(cudaMemcpyAsync(hReadback.get(), d_readback(), sizeof(StepReadback), cudaMemcpyDeviceToHost, stream));
+    return;
+  }
+  launch_chained(k_readback, dim3(1), dim3(64), 0, stream, reinterpret_cast<const uint32_t *>(d_readback()),
+                 static_cast<uint32_t *>(hReadbackDevice), (uint32_t)(sizeof(StepReadback) / 4));
+  SB_CUDA(cudaGetLastError());
 }
 
 void Trainer::fill_chain_args(ChainMode mode, bool statistics, const splat_learning_rates *rates) {
